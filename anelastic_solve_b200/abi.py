@@ -1,0 +1,105 @@
+"""ctypes mirrors of the C-ABI structs declared in include/anel.h."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+MAX_LEVELS = 16
+
+OK = 0
+ERR_SIZE = -1
+ERR_BC = -2
+ERR_NOCONV = -3
+ERR_CUDA = -4
+ERR_TIMEOUT = -5
+ERR_ARG = -6
+ERR_NOMEM = -7
+ERR_UNSUPPORTED = -8
+ERR_NONFINITE = -9
+
+SMOOTHER_RBPGS = 0
+SMOOTHER_LJ = 1
+MODE_LITERAL = 0
+MODE_METRIC = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
+STOP_RELMAX = 0
+STOP_RESID = 1
+MEM_HOST = 0
+MEM_DEVICE = 1
+BC_PERIODIC = 0
+BC_NEUMANN = 1
+BC_DIRICHLET = 2
+
+_DP = C.POINTER(C.c_double)
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("xL", C.c_double), ("yL", C.c_double), ("zL", C.c_double),
+        ("xe", _DP), ("xc", _DP), ("dxe", _DP), ("dxc", _DP), ("rdxe", _DP), ("rdxc", _DP),
+        ("ye", _DP), ("yc", _DP), ("dye", _DP), ("dyc", _DP), ("rdye", _DP), ("rdyc", _DP),
+        ("ze", _DP), ("zc", _DP), ("dze", _DP), ("dzc", _DP), ("rdze", _DP), ("rdzc", _DP)]
+
+
+class MGParams(C.Structure):
+    _fields_ = [("levels", C.c_int32 * 3), ("maxcy", C.c_int32), ("tolmax", C.c_double),
+                ("smoother", C.c_int32), ("pre_relax", C.c_int32 * MAX_LEVELS),
+                ("post_relax", C.c_int32 * MAX_LEVELS), ("tbc", C.c_int32 * 6),
+                ("vbc", C.c_double * 6), ("mode", C.c_int32), ("precision", C.c_int32),
+                ("stop", C.c_int32), ("verbose", C.c_int32)]
+
+
+class MGReport(C.Structure):
+    _fields_ = [("iter", C.c_int32), ("status", C.c_int32), ("relmax", C.c_double),
+                ("resid", C.c_double), ("ms", C.c_double)]
+
+
+def dptr(a: np.ndarray):
+    """Pointer to the data of a C- or Fortran-contiguous float64 array."""
+    assert a.dtype == np.float64 and (a.flags.c_contiguous or a.flags.f_contiguous)
+    return a.ctypes.data_as(_DP)
+
+
+def make_grid_desc(grid):
+    """Build a GridDesc from an anelastic_solve_b200.grid.Grid; returns
+    (desc, keepalive) -- keep the second item alive while desc is used."""
+    keep = []
+    d = GridDesc()
+    d.nx, d.ny, d.nz = grid.x.n, grid.y.n, grid.z.n
+    d.xL, d.yL, d.zL = grid.x.L, grid.y.L, grid.z.L
+    for ax, pfx in ((grid.x, "x"), (grid.y, "y"), (grid.z, "z")):
+        for name, arr in zip(("e", "c", "de", "dc", "rde", "rdc"), ax.arrays()):
+            a = np.ascontiguousarray(arr, dtype=np.float64)
+            keep.append(a)
+            fld = {"e": f"{pfx}e", "c": f"{pfx}c", "de": f"d{pfx}e", "dc": f"d{pfx}c",
+                   "rde": f"rd{pfx}e", "rdc": f"rd{pfx}c"}[name]
+            setattr(d, fld, dptr(a))
+    return d, keep
+
+
+def make_mg_params(levels, maxcy=99, tolmax=1e-10, pre=None, post=None, tbc=(0, 1, 0, 1, 0, 0),
+                   vbc=(0.0,) * 6, smoother=SMOOTHER_RBPGS, mode=MODE_LITERAL,
+                   precision=PREC_FP64, stop=STOP_RELMAX, verbose=0) -> MGParams:
+    """``pre``/``post`` are per-level sweep counts listed coarsest -> finest,
+    as in the ini file; a scalar applies to every level."""
+    p = MGParams()
+    ngrid = max(levels)
+    for d in range(3):
+        p.levels[d] = int(levels[d])
+    p.maxcy = int(maxcy)
+    p.tolmax = float(tolmax)
+    p.smoother = int(smoother)
+    pre = [2] * ngrid if pre is None else ([pre] * ngrid if np.isscalar(pre) else list(pre))
+    post = [2] * ngrid if post is None else ([post] * ngrid if np.isscalar(post) else list(post))
+    if len(pre) != ngrid or len(post) != ngrid:
+        raise ValueError("pre/post must list one sweep count per level")
+    for l in range(ngrid):
+        p.pre_relax[l] = int(pre[l])
+        p.post_relax[l] = int(post[l])
+    for f in range(6):
+        p.tbc[f] = int(tbc[f])
+        p.vbc[f] = float(vbc[f])
+    p.mode, p.precision, p.stop, p.verbose = int(mode), int(precision), int(stop), int(verbose)
+    return p

@@ -1,0 +1,350 @@
+// mg_device.cuh -- device code of the multigrid V-cycle, templated on the
+// storage/arithmetic type T (double for the FP64 path, float for the FP32
+// inner cycle of the mixed-precision solver).
+//
+// Layout: every level array is ghosted and column-major like the reference
+// (i fastest); cell (i,j,k), 1-based with ghosts, sits at
+// (i-1) + X*((j-1) + Y*(k-1)).  The FP64 instantiation is compiled with
+// -fmad=false and evaluates every sum in the reference's left-to-right
+// order, so its results are bit-identical to the Fortran semantics.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "anel_internal.h"
+
+namespace anel {
+
+template <typename T>
+struct DevLevel {
+  int nx, ny, nz;  // interior cells
+  int X, Y, Z;     // ghosted dims
+  int64_t XY, G;
+  T* phi;
+  T* src;
+  const T* coef;   // cx1[X] cx2[X] cy3[Y] cy4[Y] cz5[Z] cz6[Z] dz5[Z] dz6[Z]
+  BdryRule rule;
+};
+
+template <typename T>
+__device__ __forceinline__ const T* cx1p(const DevLevel<T>& L) { return L.coef; }
+template <typename T>
+__device__ __forceinline__ const T* cx2p(const DevLevel<T>& L) { return L.coef + L.X; }
+template <typename T>
+__device__ __forceinline__ const T* cy3p(const DevLevel<T>& L) { return L.coef + 2 * L.X; }
+template <typename T>
+__device__ __forceinline__ const T* cy4p(const DevLevel<T>& L) { return L.coef + 2 * L.X + L.Y; }
+template <typename T>
+__device__ __forceinline__ const T* cz5p(const DevLevel<T>& L) { return L.coef + 2 * L.X + 2 * L.Y; }
+template <typename T>
+__device__ __forceinline__ const T* cz6p(const DevLevel<T>& L) {
+  return L.coef + 2 * L.X + 2 * L.Y + L.Z;
+}
+template <typename T>
+__device__ __forceinline__ const T* dz5p(const DevLevel<T>& L) {
+  return L.coef + 2 * L.X + 2 * L.Y + 2 * L.Z;
+}
+template <typename T>
+__device__ __forceinline__ const T* dz6p(const DevLevel<T>& L) {
+  return L.coef + 2 * L.X + 2 * L.Y + 3 * L.Z;
+}
+
+__device__ __forceinline__ int64_t cidx(int i, int j, int k, int X, int64_t XY) {
+  return (int64_t)(i - 1) + (int64_t)X * (j - 1) + XY * (k - 1);
+}
+
+// ------------------------------------------------------------ ghost rule
+// Final value of ghost cell (i,j,k) after the reference's serial mg_bdry
+// (mg_bdry.F90:72-190): full periodic wrap X1, X2, X3, then the wall faces
+// X2max, X3min, X2min, X3max, X1min, X1max, each over its full plane.  The
+// value is found by walking the phases backwards to the interior cell it
+// derives from, then replaying the Neumann additions forwards.  Reads only
+// interior cells, so it can run concurrently with other ghost writers.
+template <typename T>
+__device__ __forceinline__ T ghost_value(const DevLevel<T>& L, const T* __restrict__ phi, int i, int j,
+                                         int k) {
+  const BdryRule& R = L.rule;
+  T add[9];
+  int sgn[9];
+  int nops = 0;
+  int t = 9;
+  const int X = L.X, Y = L.Y, Z = L.Z;
+  T base = T(0);
+  for (;;) {
+    int p = 0;
+    if (t >= 9 && R.type[5] && i == X) p = 9;
+    else if (t >= 8 && R.type[4] && i == 1) p = 8;
+    else if (t >= 7 && R.type[3] && k == Z) p = 7;
+    else if (t >= 6 && R.type[2] && j == 1) p = 6;
+    else if (t >= 5 && R.type[1] && k == 1) p = 5;
+    else if (t >= 4 && R.type[0] && j == Y) p = 4;
+    else if (t >= 3 && (k == 1 || k == Z)) p = 3;
+    else if (t >= 2 && (j == 1 || j == Y)) p = 2;
+    else if (t >= 1 && (i == 1 || i == X)) p = 1;
+    if (p == 0) {
+      base = phi[cidx(i, j, k, X, L.XY)];
+      break;
+    }
+    if (p >= 4) {
+      const int face = p - 4;  // 0..5 in mg_bdry order
+      if (R.type[face] == 2) {
+        base = (T)R.val[face];
+        break;
+      }
+      // Neumann: ghost = neighbour +/- phibc*d (X2max, X3max, X1max add)
+      const T prod = (T)R.val[face] * (T)R.dist[face];
+      add[nops] = prod;
+      sgn[nops] = (face == 0 || face == 3 || face == 5) ? 1 : -1;
+      ++nops;
+      switch (face) {
+        case 0: j = Y - 1; break;
+        case 1: k = 2; break;
+        case 2: j = 2; break;
+        case 3: k = Z - 1; break;
+        case 4: i = 2; break;
+        default: i = X - 1; break;
+      }
+    } else if (p == 3) {
+      k = (k == 1) ? Z - 1 : 2;
+    } else if (p == 2) {
+      j = (j == 1) ? Y - 1 : 2;
+    } else {
+      i = (i == 1) ? X - 1 : 2;
+    }
+    t = p - 1;
+  }
+  T v = base;
+  for (int q = nops - 1; q >= 0; --q) v = (sgn[q] > 0) ? (v + add[q]) : (v - add[q]);
+  return v;
+}
+
+// Map a linear ghost id (0 .. G-N-1) to a ghost cell: k-ghost planes, then
+// j-ghost rows of interior k, then i-ghost columns of interior j,k.
+__device__ __forceinline__ void ghost_cell(int64_t g, int X, int Y, int Z, int& i, int& j, int& k) {
+  const int64_t XY = (int64_t)X * Y;
+  if (g < 2 * XY) {
+    const int64_t r = g % XY;
+    k = (g < XY) ? 1 : Z;
+    i = 1 + (int)(r % X);
+    j = 1 + (int)(r / X);
+    return;
+  }
+  g -= 2 * XY;
+  const int nz = Z - 2;
+  const int64_t Xnz = (int64_t)X * nz;
+  if (g < 2 * Xnz) {
+    const int64_t r = g % Xnz;
+    j = (g < Xnz) ? 1 : Y;
+    i = 1 + (int)(r % X);
+    k = 2 + (int)(r / X);
+    return;
+  }
+  g -= 2 * Xnz;
+  const int ny = Y - 2;
+  const int64_t nynz = (int64_t)ny * nz;
+  const int64_t r = g % nynz;
+  i = (g < nynz) ? 1 : X;
+  j = 2 + (int)(r % ny);
+  k = 2 + (int)(r / ny);
+}
+
+template <typename T>
+__global__ void k_bdry(DevLevel<T> L, T* __restrict__ phi) {
+  const int64_t nghost = L.G - (int64_t)L.nx * L.ny * L.nz;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < nghost;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    ghost_cell(g, L.X, L.Y, L.Z, i, j, k);
+    phi[cidx(i, j, k, L.X, L.XY)] = ghost_value(L, phi, i, j, k);
+  }
+}
+
+// ------------------------------------------------------------- RB sweep
+// One half-sweep of mg_relaxRB (mg_relax.F90:146-168): updates the cells
+// with (i+j+k) % 2 == color (pass 1 = colour 0).  Reads only the other
+// colour and ghosts, so the cells of one colour are independent.
+template <typename T>
+__device__ __forceinline__ T stencil_update(const DevLevel<T>& L, const T* __restrict__ phi, T s,
+                                            int64_t c, int i, int j, int k) {
+  const T a1 = cx1p(L)[i - 1], a2 = cx2p(L)[i - 1];
+  const T a3 = cy3p(L)[j - 1], a4 = cy4p(L)[j - 1];
+  const T a5 = cz5p(L)[k - 1], a6 = cz6p(L)[k - 1];
+  const T diag = -(a1 + a2 + a3 + a4 + dz5p(L)[k - 1] + dz6p(L)[k - 1]);
+  T acc = a1 * phi[c - 1];
+  acc = acc + a2 * phi[c + 1];
+  acc = acc + a3 * phi[c - L.X];
+  acc = acc + a4 * phi[c + L.X];
+  acc = acc + a5 * phi[c - L.XY];
+  acc = acc + a6 * phi[c + L.XY];
+  return (s - acc) / diag;
+}
+
+template <typename T>
+__global__ void k_rb_sweep(DevLevel<T> L, int color) {
+  const int hx = (L.nx + 1) >> 1;
+  const int64_t total = (int64_t)hx * L.ny * L.nz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(t % hx);
+    const int64_t r = t / hx;
+    const int j = 2 + (int)(r % L.ny);
+    const int k = 2 + (int)(r / L.ny);
+    const int i = 2 + ((color + j + k) & 1) + 2 * q;
+    if (i > L.nx + 1) continue;
+    const int64_t c = cidx(i, j, k, L.X, L.XY);
+    L.phi[c] = stencil_update(L, L.phi, L.src[c], c, i, j, k);
+  }
+}
+
+// ----------------------------------------------------- residual + restrict
+// mg_restr.F90:114-241.  One thread per coarse cell (ghosts included):
+// coarse phi <- 0 everywhere, coarse f <- 0 on ghosts and, on the interior,
+// the scaled sum of the children's residuals res = f - A phi, summed in the
+// reference order of the active variant.  cdir bit d set = direction d is
+// coarsened between the two levels.
+template <typename T>
+__device__ __forceinline__ T fine_resid(const DevLevel<T>& F, int i, int j, int k) {
+  const int64_t c = cidx(i, j, k, F.X, F.XY);
+  const T a1 = cx1p(F)[i - 1], a2 = cx2p(F)[i - 1];
+  const T a3 = cy3p(F)[j - 1], a4 = cy4p(F)[j - 1];
+  const T a5 = cz5p(F)[k - 1], a6 = cz6p(F)[k - 1];
+  const T diag = -(a1 + a2 + a3 + a4 + dz5p(F)[k - 1] + dz6p(F)[k - 1]);
+  const T* __restrict__ p = F.phi;
+  T acc = a1 * p[c - 1];
+  acc = acc + a2 * p[c + 1];
+  acc = acc + a3 * p[c - F.X];
+  acc = acc + a4 * p[c + F.X];
+  acc = acc + a5 * p[c - F.XY];
+  acc = acc + a6 * p[c + F.XY];
+  acc = acc + diag * p[c];
+  return F.src[c] - acc;
+}
+
+template <typename T>
+__global__ void k_restrict(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < Cl.G;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int ic = 1 + (int)(t % Cl.X);
+    const int64_t r = t / Cl.X;
+    const int jc = 1 + (int)(r % Cl.Y);
+    const int kc = 1 + (int)(r / Cl.Y);
+    Cl.phi[t] = T(0);
+    const bool interior =
+        ic >= 2 && ic <= Cl.nx + 1 && jc >= 2 && jc <= Cl.ny + 1 && kc >= 2 && kc <= Cl.nz + 1;
+    if (!interior) {
+      Cl.src[t] = T(0);
+      continue;
+    }
+    const bool cx = cdir & 1, cy = cdir & 2, cz = cdir & 4;
+    const int i = cx ? 2 * ic - 2 : ic;
+    const int j = cy ? 2 * jc - 2 : jc;
+    const int k = cz ? 2 * kc - 2 : kc;
+    T v;
+    if (cx && cy && cz) {
+      T s = fine_resid(F, i, j, k);
+      s = s + fine_resid(F, i, j + 1, k);
+      s = s + fine_resid(F, i, j, k + 1);
+      s = s + fine_resid(F, i, j + 1, k + 1);
+      s = s + fine_resid(F, i + 1, j, k);
+      s = s + fine_resid(F, i + 1, j + 1, k + 1);
+      s = s + fine_resid(F, i + 1, j + 1, k);
+      s = s + fine_resid(F, i + 1, j, k + 1);
+      v = T(0.125) * s;
+    } else if (!cx && !cy) {  // z only
+      v = T(0.5) * (fine_resid(F, i, j, k) + fine_resid(F, i, j, k + 1));
+    } else if (!cx && !cz) {  // y only
+      v = T(0.5) * (fine_resid(F, i, j, k) + fine_resid(F, i, j + 1, k));
+    } else if (!cy && !cz) {  // x only
+      v = T(0.5) * (fine_resid(F, i, j, k) + fine_resid(F, i + 1, j, k));
+    } else if (!cx) {  // y,z
+      T s = fine_resid(F, i, j, k);
+      s = s + fine_resid(F, i, j + 1, k);
+      s = s + fine_resid(F, i, j, k + 1);
+      s = s + fine_resid(F, i, j + 1, k + 1);
+      v = T(0.25) * s;
+    } else if (!cy) {  // x,z
+      T s = fine_resid(F, i, j, k);
+      s = s + fine_resid(F, i, j, k + 1);
+      s = s + fine_resid(F, i + 1, j, k);
+      s = s + fine_resid(F, i + 1, j, k + 1);
+      v = T(0.25) * s;
+    } else {  // x,y
+      T s = fine_resid(F, i, j, k);
+      s = s + fine_resid(F, i + 1, j, k);
+      s = s + fine_resid(F, i, j + 1, k);
+      s = s + fine_resid(F, i + 1, j + 1, k);
+      v = T(0.25) * s;
+    }
+    Cl.src[t] = v;
+  }
+}
+
+// -------------------------------------------------------------- prolong
+// mg_cor.F90:102-290 for the fine interior (fine ghosts are rebuilt by the
+// boundary pass that follows, as in the reference).  In a coarsened
+// direction fine index f uses coarse ic = (f+1)/2 (f odd, near point ic) or
+// ic = f/2 (f even, near point ic+1); weights 3 (near) and 1 (far).
+template <typename T>
+__global__ void k_prolong(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
+  const int64_t total = (int64_t)F.nx * F.ny * F.nz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = 2 + (int)(t % F.nx);
+    const int64_t r = t / F.nx;
+    const int j = 2 + (int)(r % F.ny);
+    const int k = 2 + (int)(r / F.ny);
+    const bool cx = cdir & 1, cy = cdir & 2, cz = cdir & 4;
+    const int ic = cx ? ((i & 1) ? (i + 1) >> 1 : i >> 1) : i;
+    const int jc = cy ? ((j & 1) ? (j + 1) >> 1 : j >> 1) : j;
+    const int kc = cz ? ((k & 1) ? (k + 1) >> 1 : k >> 1) : k;
+    // weight of coarse offset o (0/1) in each direction
+    const T wx0 = cx ? ((i & 1) ? T(3) : T(1)) : T(1), wx1 = cx ? ((i & 1) ? T(1) : T(3)) : T(0);
+    const T wy0 = cy ? ((j & 1) ? T(3) : T(1)) : T(1), wy1 = cy ? ((j & 1) ? T(1) : T(3)) : T(0);
+    const T wz0 = cz ? ((k & 1) ? T(3) : T(1)) : T(1), wz1 = cz ? ((k & 1) ? T(1) : T(3)) : T(0);
+    const int64_t c0 = cidx(ic, jc, kc, Cl.X, Cl.XY);
+    const T* __restrict__ pc = Cl.phi;
+    const int64_t ox = 1, oy = Cl.X, oz = Cl.XY;
+    T corr;
+    if (cx && cy && cz) {
+      // order (x,y,z) offsets: 000 010 001 011 100 110 101 111
+      T s = (wx0 * wy0 * wz0) * pc[c0];
+      s = s + (wx0 * wy1 * wz0) * pc[c0 + oy];
+      s = s + (wx0 * wy0 * wz1) * pc[c0 + oz];
+      s = s + (wx0 * wy1 * wz1) * pc[c0 + oy + oz];
+      s = s + (wx1 * wy0 * wz0) * pc[c0 + ox];
+      s = s + (wx1 * wy1 * wz0) * pc[c0 + ox + oy];
+      s = s + (wx1 * wy0 * wz1) * pc[c0 + ox + oz];
+      s = s + (wx1 * wy1 * wz1) * pc[c0 + ox + oy + oz];
+      corr = s / T(64);
+    } else if (!cx && !cy) {  // z only
+      corr = (wz0 * pc[c0] + wz1 * pc[c0 + oz]) / T(4);
+    } else if (!cx && !cz) {  // y only
+      corr = (wy0 * pc[c0] + wy1 * pc[c0 + oy]) / T(4);
+    } else if (!cy && !cz) {  // x only
+      corr = (wx0 * pc[c0] + wx1 * pc[c0 + ox]) / T(4);
+    } else if (!cx) {  // y,z: (y,z) 00 10 01 11
+      T s = (wy0 * wz0) * pc[c0];
+      s = s + (wy1 * wz0) * pc[c0 + oy];
+      s = s + (wy0 * wz1) * pc[c0 + oz];
+      s = s + (wy1 * wz1) * pc[c0 + oy + oz];
+      corr = s / T(16);
+    } else if (!cy) {  // x,z: (x,z) 00 10 01 11
+      T s = (wx0 * wz0) * pc[c0];
+      s = s + (wx1 * wz0) * pc[c0 + ox];
+      s = s + (wx0 * wz1) * pc[c0 + oz];
+      s = s + (wx1 * wz1) * pc[c0 + ox + oz];
+      corr = s / T(16);
+    } else {  // x,y: (x,y) 00 10 01 11
+      T s = (wx0 * wy0) * pc[c0];
+      s = s + (wx1 * wy0) * pc[c0 + ox];
+      s = s + (wx0 * wy1) * pc[c0 + oy];
+      s = s + (wx1 * wy1) * pc[c0 + ox + oy];
+      corr = s / T(16);
+    }
+    const int64_t cf = cidx(i, j, k, F.X, F.XY);
+    F.phi[cf] = F.phi[cf] + corr;
+  }
+}
+
+}  // namespace anel

@@ -1,0 +1,16 @@
+// mg_kernels32.cu -- FP32 instantiation of the multigrid kernels, used by
+// the inner V-cycle of the mixed-precision defect correction.  Compiled
+// with multiply-add contraction allowed (this path is not bit-matched to
+// the reference; its accuracy is set by the FP64 outer loop).
+#include "mg_launch_impl.cuh"
+
+namespace anel {
+
+template void launch_bdry<float>(const DevLevel<float>&, float*, cudaStream_t);
+template void launch_rb_sweep<float>(const DevLevel<float>&, int, cudaStream_t);
+template void launch_restrict<float>(const DevLevel<float>&, const DevLevel<float>&, int,
+                                     cudaStream_t);
+template void launch_prolong<float>(const DevLevel<float>&, const DevLevel<float>&, int,
+                                    cudaStream_t);
+
+}  // namespace anel

@@ -1,0 +1,157 @@
+// mg_kernels64.cu -- FP64 instantiation of the multigrid kernels plus the
+// FP64-only reductions.  Compiled with -fmad=false: no multiply-add
+// contraction, so every value is rounded exactly as the reference's
+// expressions evaluated left to right.
+#include "mg_launch_impl.cuh"
+
+namespace anel {
+
+template void launch_bdry<double>(const DevLevel<double>&, double*, cudaStream_t);
+template void launch_rb_sweep<double>(const DevLevel<double>&, int, cudaStream_t);
+template void launch_restrict<double>(const DevLevel<double>&, const DevLevel<double>&, int,
+                                      cudaStream_t);
+template void launch_prolong<double>(const DevLevel<double>&, const DevLevel<double>&, int,
+                                     cudaStream_t);
+
+// ------------------------------------------------------------- reductions
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+// Non-negative doubles order like their bit patterns, so the maxima are
+// accumulated exactly (and order-independently) with integer atomicMax.
+__global__ void k_relmax_copy(DevLevel<double> L, const double* __restrict__ phin,
+                              double* __restrict__ phio, unsigned long long* out) {
+  unsigned long long m1 = 0, m2 = 0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < L.G;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = 1 + (int)(t % L.X);
+    const int64_t r = t / L.X;
+    const int j = 1 + (int)(r % L.Y);
+    const int k = 1 + (int)(r / L.Y);
+    const double n = phin[t];
+    if (i >= 2 && i <= L.nx + 1 && j >= 2 && j <= L.ny + 1 && k >= 2 && k <= L.nz + 1) {
+      const unsigned long long a = __double_as_longlong(fabs(n));
+      const unsigned long long d = __double_as_longlong(fabs(n - phio[t]));
+      m1 = a > m1 ? a : m1;
+      m2 = d > m2 ? d : m2;
+    }
+    phio[t] = n;
+  }
+  m1 = warp_max_u64(m1);
+  m2 = warp_max_u64(m2);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, m1);
+    atomicMax(out + 1, m2);
+  }
+}
+
+void launch_relmax_copy(const DevLevel<double>& L, const double* phin, double* phio,
+                        unsigned long long* out, cudaStream_t s) {
+  k_relmax_copy<<<gs_blocks(L.G), 256, 0, s>>>(L, phin, phio, out);
+  count_launch();
+}
+
+static constexpr int kNormThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s += sh[q];
+  return s;
+}
+
+template <bool kStore>
+__global__ void k_resid_norm(DevLevel<double> L, const double* __restrict__ phi,
+                             const double* __restrict__ f, float* __restrict__ r32,
+                             double* __restrict__ part) {
+  __shared__ double sh[kNormThreads / 32];
+  double rr = 0.0, ff = 0.0;
+  const int64_t N = (int64_t)L.nx * L.ny * L.nz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = 2 + (int)(t % L.nx);
+    const int64_t r = t / L.nx;
+    const int j = 2 + (int)(r % L.ny);
+    const int k = 2 + (int)(r / L.ny);
+    const int64_t c = cidx(i, j, k, L.X, L.XY);
+    DevLevel<double> Lp = L;
+    Lp.phi = const_cast<double*>(phi);
+    Lp.src = const_cast<double*>(f);
+    const double res = fine_resid(Lp, i, j, k);
+    if (kStore) r32[c] = (float)res;
+    rr += res * res;
+    ff += f[c] * f[c];
+  }
+  const double s1 = block_sum(rr, sh);
+  const double s2 = block_sum(ff, sh);
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = s1;
+    part[2 * blockIdx.x + 1] = s2;
+  }
+}
+
+__global__ void k_fold(const double* __restrict__ part, int nb, double* out) {
+  __shared__ double sh[kNormThreads / 32];
+  double a = 0.0, b = 0.0;
+  for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+    a += part[2 * q];
+    b += part[2 * q + 1];
+  }
+  const double s1 = block_sum(a, sh);
+  const double s2 = block_sum(b, sh);
+  if (threadIdx.x == 0) {
+    out[0] = s1;
+    out[1] = s2;
+  }
+}
+
+int resid_norm_blocks(const DevLevel<double>& L) {
+  return gs_blocks((int64_t)L.nx * L.ny * L.nz, kNormThreads);
+}
+
+void launch_resid_norm(const DevLevel<double>& L, const double* phi, const double* f, double* part,
+                       double* out, cudaStream_t s) {
+  const int nb = resid_norm_blocks(L);
+  k_resid_norm<false><<<nb, kNormThreads, 0, s>>>(L, phi, f, nullptr, part);
+  k_fold<<<1, kNormThreads, 0, s>>>(part, nb, out);
+  count_launch(2);
+}
+
+void launch_resid_store(const DevLevel<double>& L, const double* phi, const double* f, float* r32,
+                        double* part, double* out, cudaStream_t s) {
+  const int nb = resid_norm_blocks(L);
+  k_resid_norm<true><<<nb, kNormThreads, 0, s>>>(L, phi, f, r32, part);
+  k_fold<<<1, kNormThreads, 0, s>>>(part, nb, out);
+  count_launch(2);
+}
+
+__global__ void k_add_correction(DevLevel<double> L, double* __restrict__ phi,
+                                 const float* __restrict__ e) {
+  const int64_t N = (int64_t)L.nx * L.ny * L.nz;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = 2 + (int)(t % L.nx);
+    const int64_t r = t / L.nx;
+    const int j = 2 + (int)(r % L.ny);
+    const int k = 2 + (int)(r / L.ny);
+    const int64_t c = cidx(i, j, k, L.X, L.XY);
+    phi[c] = phi[c] + (double)e[c];
+  }
+}
+
+void launch_add_correction(const DevLevel<double>& L, double* phi, const float* e, cudaStream_t s) {
+  k_add_correction<<<gs_blocks((int64_t)L.nx * L.ny * L.nz), 256, 0, s>>>(L, phi, e);
+  count_launch();
+}
+
+}  // namespace anel

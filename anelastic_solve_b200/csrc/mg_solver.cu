@@ -1,0 +1,799 @@
+// mg_solver.cu -- host side of the B200 multigrid pressure solver: level
+// maps (mg_init.F90), coarse metric hierarchy (mg_grids.F90, mg_coeff.F90),
+// level coefficients (mg_pfpde.F90, mg_phpde.F90), the V-cycle schedule
+// (mg_cycle.F90) and the solve loop (mg_solver.F90), all driving the
+// sm_100a kernels of mg_device.cuh.  Built with -ffp-contract=off for the
+// host compiler so the coefficients round exactly as the reference's.
+#include "mg_solver.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace anel {
+
+static inline int imax(int a, int b) { return a > b ? a : b; }
+
+// ------------------------------------------------------------------ init
+MGSolver* MGSolver::create(const anel_grid_desc* g, const anel_mg_params* p, int device,
+                           int* status) {
+  MGSolver* s = new MGSolver();
+  const int st = s->init(g, p, device);
+  if (status) *status = st;
+  if (st != ANEL_OK) {
+    delete s;
+    return nullptr;
+  }
+  return s;
+}
+
+int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device) {
+  if (!g || !p) {
+    set_error("null grid or params");
+    return ANEL_ERR_ARG;
+  }
+  prm_ = *p;
+  device_ = device;
+  nx_ = g->nx;
+  ny_ = g->ny;
+  nz_ = g->nz;
+  L_[0] = g->xL;
+  L_[1] = g->yL;
+  L_[2] = g->zL;
+  const int n[3] = {nx_, ny_, nz_};
+  if (nx_ < 1 || ny_ < 1 || nz_ < 1) {
+    set_error("grid sizes must be positive (got %d %d %d)", nx_, ny_, nz_);
+    return ANEL_ERR_SIZE;
+  }
+  if (p->smoother != ANEL_SMOOTHER_RBPGS && p->smoother != ANEL_SMOOTHER_LJ) {
+    set_error("unknown smoother %d", p->smoother);
+    return ANEL_ERR_ARG;
+  }
+  if (p->smoother == ANEL_SMOOTHER_LJ) {
+    set_error("the z-line (LJ) smoother is not available in this build");
+    return ANEL_ERR_UNSUPPORTED;
+  }
+  if (p->mode != ANEL_MODE_LITERAL && p->mode != ANEL_MODE_METRIC) {
+    set_error("unknown mode %d", p->mode);
+    return ANEL_ERR_ARG;
+  }
+  if (p->precision != ANEL_PREC_FP64 && p->precision != ANEL_PREC_MIXED) {
+    set_error("unknown precision %d", p->precision);
+    return ANEL_ERR_ARG;
+  }
+  if (p->maxcy < 1) {
+    set_error("maxcy must be >= 1");
+    return ANEL_ERR_ARG;
+  }
+  const double* src[3][6] = {{g->xe, g->xc, g->dxe, g->dxc, g->rdxe, g->rdxc},
+                             {g->ye, g->yc, g->dye, g->dyc, g->rdye, g->rdyc},
+                             {g->ze, g->zc, g->dze, g->dzc, g->rdze, g->rdzc}};
+  for (int d = 0; d < 3; ++d)
+    for (int a = 0; a < 6; ++a) {
+      if (!src[d][a]) {
+        set_error("grid metric array %d of direction %d is null", a, d);
+        return ANEL_ERR_ARG;
+      }
+      fm_[d][a].assign(src[d][a], src[d][a] + n[d] + 2);
+    }
+  // ---- level sizes and index maps (mg_init.F90:86-220) ----
+  ngrid_ = imax(p->levels[0], imax(p->levels[1], p->levels[2]));
+  if (ngrid_ < 2 || ngrid_ > ANEL_MAX_LEVELS) {
+    set_error("ngrid = %d; need 2..%d levels (a single level has no coarse grid)", ngrid_,
+              ANEL_MAX_LEVELS);
+    return ANEL_ERR_SIZE;
+  }
+  for (int d = 0; d < 3; ++d) {
+    const int Ld = p->levels[d];
+    if (Ld < 2) {
+      set_error("no coarsening in direction %d at the finest level (mg_check_size codes 10-12)",
+                d + 1);
+      return ANEL_ERR_SIZE;
+    }
+    nC_[d] = n[d] >> (Ld - 1);
+    if (nC_[d] < 1 || (nC_[d] << (Ld - 1)) != n[d]) {
+      set_error("n%d = %d is not nC*2^(levels-1) (mg_check_size codes 4-6)", d + 1, n[d]);
+      return ANEL_ERR_SIZE;
+    }
+  }
+  for (int l = 1; l <= ngrid_; ++l)
+    for (int d = 0; d < 3; ++d)
+      geo_[l].nk[d] = (nC_[d] << (imax(l + p->levels[d] - ngrid_, 1) - 1)) + 1;
+  for (int d = 0; d < 3; ++d) {
+    geo_[ngrid_].s[d] = 2;
+    geo_[ngrid_].e[d] = n[d] + 1;
+  }
+  for (int l = ngrid_ - 1; l >= 1; --l)
+    for (int d = 0; d < 3; ++d) {
+      const bool coarser = geo_[l].nk[d] < geo_[l + 1].nk[d];
+      geo_[l].s[d] = coarser ? geo_[l + 1].s[d] / 2 + 1 : geo_[l + 1].s[d];
+      geo_[l].e[d] = coarser ? (geo_[l + 1].e[d] - 1) / 2 + 1 : geo_[l + 1].e[d];
+    }
+  int64_t kp3 = 1;
+  int kx[3] = {1, 1, 1};
+  for (int l = ngrid_; l >= 1; --l) {
+    LevelGeom& G = geo_[l];
+    for (int d = 0; d < 3; ++d) G.n[d] = G.e[d] - G.s[d] + 1;
+    G.X = G.e[0] + 1;
+    G.Y = G.e[1] + 1;
+    G.Z = G.e[2] + 1;
+    G.G = (int64_t)G.X * G.Y * G.Z;
+    G.kp3d = kp3;
+    kp3 += G.G;
+    for (int d = 0; d < 3; ++d) {
+      G.kpx[d] = kx[d];
+      kx[d] += G.nk[d] + 1;
+    }
+  }
+  // ---- boundary codes (mg_init.F90:265-328) ----
+  for (int f = 0; f < 6; ++f)
+    if (p->tbc[f] < 0 || p->tbc[f] > 2) {
+      set_error("bad boundary type tbc(%d) = %d", f + 1, p->tbc[f]);
+      return ANEL_ERR_BC;
+    }
+  // periodic must be paired
+  if ((p->tbc[4] == 0) != (p->tbc[5] == 0) || (p->tbc[2] == 0) != (p->tbc[0] == 0) ||
+      (p->tbc[1] == 0) != (p->tbc[3] == 0)) {
+    set_error("a direction mixes periodic and wall faces");
+    return ANEL_ERR_BC;
+  }
+  std::memset(bd_, 0, sizeof(bd_));
+  bd_[9] = p->tbc[4];
+  bd_[18] = p->tbc[5];
+  bd_[5] = p->tbc[2];
+  bd_[1] = p->tbc[0];
+  bd_[3] = p->tbc[1];
+  bd_[7] = p->tbc[3];
+  for (int f = 0; f < 6; ++f) {
+    phibc_[ngrid_][f] = p->vbc[f];
+    for (int l = ngrid_ - 1; l >= 1; --l) phibc_[l][f] = 0.0;
+  }
+  build_metric_hierarchy();
+  // boundary rules; spacings indexed without the level offset, exactly as
+  // mg_bdry.F90:106-181 (dyck(eym) etc.)
+  for (int l = 1; l <= ngrid_; ++l) {
+    const LevelGeom& G = geo_[l];
+    BdryRule R;
+    const int bdf[6] = {bd_[1], bd_[3], bd_[5], bd_[7], bd_[9], bd_[18]};
+    const double dist[6] = {hDC_[1][G.e[1]], hDC_[2][G.s[2]], hDC_[1][G.s[1]],
+                            hDC_[2][G.e[2]], hDC_[0][G.s[0]], hDC_[0][G.e[0]]};
+    for (int f = 0; f < 6; ++f) {
+      R.type[f] = bdf[f];
+      R.val[f] = phibc_[l][f];
+      R.dist[f] = dist[f];
+    }
+    rule_[l] = R;
+    for (int f = 0; f < 6; ++f) R.val[f] = 0.0;
+    rule_hom_[l] = R;
+  }
+  // ---- device ----
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  ANEL_CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  ANEL_CUDA_TRY(cudaEventCreate(&ev0_));
+  ANEL_CUDA_TRY(cudaEventCreate(&ev1_));
+  const bool mixed = p->precision == ANEL_PREC_MIXED;
+  for (int l = 1; l <= ngrid_; ++l) {
+    const int64_t G = geo_[l].G;
+    const size_t ncoef = 2 * (size_t)geo_[l].X + 2 * (size_t)geo_[l].Y + 4 * (size_t)geo_[l].Z;
+    if (!mixed || l == ngrid_) {
+      ANEL_CUDA_TRY(cudaMalloc(&d_phi64_[l], G * sizeof(double)));
+      ANEL_CUDA_TRY(cudaMalloc(&d_src64_[l], G * sizeof(double)));
+      ANEL_CUDA_TRY(cudaMemset(d_phi64_[l], 0, G * sizeof(double)));
+      ANEL_CUDA_TRY(cudaMemset(d_src64_[l], 0, G * sizeof(double)));
+    }
+    ANEL_CUDA_TRY(cudaMalloc(&d_coef64_[l], ncoef * sizeof(double)));
+    if (mixed) {
+      ANEL_CUDA_TRY(cudaMalloc(&d_phi32_[l], G * sizeof(float)));
+      ANEL_CUDA_TRY(cudaMalloc(&d_src32_[l], G * sizeof(float)));
+      ANEL_CUDA_TRY(cudaMemset(d_phi32_[l], 0, G * sizeof(float)));
+      ANEL_CUDA_TRY(cudaMemset(d_src32_[l], 0, G * sizeof(float)));
+      ANEL_CUDA_TRY(cudaMalloc(&d_coef32_[l], ncoef * sizeof(float)));
+    }
+  }
+  ANEL_CUDA_TRY(cudaMalloc(&d_max_, 2 * sizeof(unsigned long long)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_part_, 2 * (size_t)gs_blocks(1LL << 40) * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_norm_, 2 * sizeof(double)));
+  ANEL_CUDA_TRY(cudaHostAlloc(&h_pin_, 4 * sizeof(double), cudaHostAllocDefault));
+  // default density r == 1
+  std::vector<double> rz(geo_[ngrid_].Z, 1.0);
+  int st = build_coefficients(rz);
+  if (st != ANEL_OK) return st;
+  return upload_coefficients();
+}
+
+MGSolver::~MGSolver() {
+  if (device_ >= 0) cudaSetDevice(device_);
+  for (int l = 0; l <= ANEL_MAX_LEVELS; ++l) {
+    cudaFree(d_phi64_[l]);
+    cudaFree(d_src64_[l]);
+    cudaFree(d_coef64_[l]);
+    cudaFree(d_phi32_[l]);
+    cudaFree(d_src32_[l]);
+    cudaFree(d_coef32_[l]);
+  }
+  cudaFree(d_max_);
+  cudaFree(d_part_);
+  cudaFree(d_norm_);
+  cudaFree(d_io_phi_);
+  cudaFree(d_io_rhs_);
+  if (h_pin_) cudaFreeHost(h_pin_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+// ------------------------------------------------- coarse metric hierarchy
+// mg_grids.F90:54-448 and mg_coeff.F90:77-145.  Arrays are 1-based
+// (index 0 unused) over the concatenated per-level 1-D workspace.
+void MGSolver::build_metric_hierarchy() {
+  const int tmin[3] = {prm_.tbc[4], prm_.tbc[2], prm_.tbc[1]};
+  const int tmax[3] = {prm_.tbc[5], prm_.tbc[0], prm_.tbc[3]};
+  for (int d = 0; d < 3; ++d) {
+    const int nw = geo_[1].kpx[d] + geo_[1].nk[d] + 1;  // nworkx
+    std::vector<double>& E = hE_[d];
+    std::vector<double>& C = hC_[d];
+    std::vector<double>& DC = hDC_[d];
+    std::vector<double>& DE = hDE_[d];
+    E.assign(nw + 1, 0.0);
+    C.assign(nw + 1, 0.0);
+    DC.assign(nw + 1, 99999999999.0);
+    DE.assign(nw + 1, 99999999999.0);
+    const int nf = geo_[ngrid_].nk[d];
+    const int k0 = geo_[ngrid_].kpx[d];
+    for (int q = 1; q <= nf + 1; ++q) {
+      E[q + k0 - 1] = fm_[d][0][q - 1];
+      C[q + k0 - 1] = fm_[d][1][q - 1];
+      DE[q + k0 - 1] = fm_[d][2][q - 1];
+      DC[q + k0 - 1] = fm_[d][3][q - 1];
+    }
+    const double LL = fm_[d][0][nf] - fm_[d][0][0];
+    const int Ld = prm_.levels[d];
+    for (int lvl = ngrid_; lvl >= ngrid_ - Ld + 2; --lvl) {
+      const int lC = lvl - 1;
+      const int nc = geo_[lC].nk[d], nfl = geo_[lvl].nk[d];
+      const int kc = geo_[lC].kpx[d], kf = geo_[lvl].kpx[d];
+      if (tmin[d] == 0) {
+        const double h = LL / (double)nc;
+        for (int q = 1; q <= nc + 1; ++q) E[q + kc - 1] = -h + h * (double)q;
+        for (int q = 2; q <= nc + 1; ++q) C[q + kc - 1] = (E[q + kc - 1] + E[q + kc - 2]) / 2.0;
+        C[kc] = E[kc] - 0.5 * h;
+        for (int q = 1; q <= nc + 1; ++q) {
+          DC[q + kc - 1] = h;
+          DE[q + kc - 1] = h;
+        }
+        continue;
+      }
+      E[kc] = E[kf];
+      for (int q = 2; q <= nc; ++q) {
+        const int f = (kf - 1) + 2 * q - 2, c = (kc - 1) + q;
+        C[c] = C[f] + DC[f] * 0.5;
+        E[c] = C[c] + DC[f];
+      }
+      C[kc] = (tmin[d] == 2) ? C[kf] : C[kf] - 0.5 * DE[kf + 1];
+      {
+        const int c = kc + nc, f = kf + nfl;
+        if (tmax[d] == 2) {
+          C[c] = C[f];
+          E[c] = E[f];
+        } else {
+          C[c] = C[f] + 0.5 * DE[f - 1];
+          E[c] = E[f] + 0.5 * DC[f - 1];
+        }
+      }
+      for (int q = 2; q <= nc; ++q) {
+        const int c = (kc - 1) + q;
+        DE[c] = C[c + 1] - C[c];
+        DC[c] = E[c] - E[c - 1];
+      }
+      DC[kc] = 0.0;
+      DE[kc] = (tmin[d] == 2) ? C[kc + 1] - C[kc] : DE[kc + 1];
+      {
+        const int c = kc + nc;
+        if (tmax[d] == 2) {
+          DE[c] = C[c] - C[c - 1];
+          DC[c] = E[c] - E[c - 1];
+        } else {
+          DE[c] = DE[c - 1];
+          DC[c] = DC[c - 1];
+        }
+      }
+    }
+    for (int lvl = ngrid_ - Ld + 1; lvl >= 2; --lvl) {
+      const int lC = lvl - 1;
+      const int nc = geo_[lC].nk[d];
+      const int kc = geo_[lC].kpx[d], kf = geo_[lvl].kpx[d];
+      for (int q = 1; q <= nc + 1; ++q) {
+        E[(kc - 1) + q] = E[(kf - 1) + q];
+        C[(kc - 1) + q] = C[(kf - 1) + q];
+        DE[(kc - 1) + q] = DE[(kf - 1) + q];
+        DC[(kc - 1) + q] = DC[(kf - 1) + q];
+      }
+    }
+    // pcf_(2d+1), pcf_(2d+2) of mg_coeff.F90:77-99
+    pA_[d].assign(nw + 1, 0.0);
+    pB_[d].assign(nw + 1, 0.0);
+    for (int l = 1; l <= ngrid_; ++l) {
+      const int s0 = geo_[l].kpx[d];
+      for (int q = 2; q <= geo_[l].nk[d]; ++q) {
+        const int gq = s0 + q - 1;
+        pA_[d][gq] = 1.0 / (DC[gq] * DE[gq - 1]);
+        pB_[d][gq] = 1.0 / (DC[gq] * DE[gq]);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------- coefficients
+// rz[k-1] = r(:,:,k) on the fine level, k = 1..nz+2.
+int MGSolver::build_coefficients(const std::vector<double>& rz) {
+  const int ng = ngrid_;
+  const int Zf = geo_[ng].Z;
+  auto R = [&](int k) {  // fine r at 1-based k; k < 1 clamps to the ghost plane
+    if (k < 1) k = 1;
+    if (k > Zf) k = Zf;
+    return rz[k - 1];
+  };
+  for (int l = 1; l <= ng; ++l) {
+    const LevelGeom& G = geo_[l];
+    LevelCoef& c = coef_[l];
+    c.cx1.assign(G.X, 0.0);
+    c.cx2.assign(G.X, 0.0);
+    c.cy3.assign(G.Y, 0.0);
+    c.cy4.assign(G.Y, 0.0);
+    c.cz5.assign(G.Z, 0.0);
+    c.cz6.assign(G.Z, 0.0);
+    c.dz5.assign(G.Z, 0.0);
+    c.dz6.assign(G.Z, 0.0);
+    const int kstep = (geo_[ng].nk[2] - 1) / (G.nk[2] - 1);
+    if (prm_.mode == ANEL_MODE_LITERAL) {
+      const double dlx = L_[0] / (double)(float)(G.nk[0] - 1);
+      const double ex = 1.0 / (dlx * dlx);
+      const double dly = L_[1] / (double)(float)(G.nk[1] - 1);
+      const double ey = 1.0 / (dly * dly);
+      const double dlz = L_[2] / (double)(float)(G.nk[2] - 1);
+      const double ez = 1.0 / (dlz * dlz);
+      for (int i = 1; i <= G.X; ++i) c.cx1[i - 1] = c.cx2[i - 1] = ex;
+      for (int j = 1; j <= G.Y; ++j) c.cy3[j - 1] = c.cy4[j - 1] = ey;
+      if (l == ng) {  // mgdpfpde (mg_pfpde.F90:41-60)
+        for (int k = G.s[2]; k <= G.e[2]; ++k) {
+          c.cz5[k - 1] = ez * 0.5 * (R(k) + R(k - 1)) / R(k - 1);
+          c.cz6[k - 1] = ez * 0.5 * (R(k) + R(k + 1)) / R(k + 1);
+          c.dz5[k - 1] = ez * 0.5 * (R(k) + R(k - 1)) / R(k);
+          c.dz6[k - 1] = ez * 0.5 * (R(k) + R(k + 1)) / R(k);
+        }
+      } else {  // mgdphpde (mg_phpde.F90:111-199)
+        int ks = 0;
+        for (int k = G.s[2]; k <= G.e[2]; ++k) {
+          const int km = 2 * kstep * k - 3 * (kstep - 1);
+          int q = (km - kstep) / 2;
+          c.cz5[k - 1] = ez * 0.5 * (R(q) + R(q - 1)) / R(q - 1);
+          q = (km + kstep) / 2;
+          c.cz6[k - 1] = ez * 0.5 * (R(q) + R(q + 1)) / R(q + 1);
+          ks = q;  // the value left over for the diagonal loop
+        }
+        if (bd_[9] == 1) c.cx1[G.s[0] - 1] = 0.0;
+        if (bd_[18] == 1) c.cx2[G.e[0] - 1] = 0.0;
+        if (bd_[5] == 1) c.cy3[G.s[1] - 1] = 0.0;
+        if (bd_[1] == 1) c.cy4[G.e[1] - 1] = 0.0;
+        if (bd_[3] == 1) c.cz5[G.s[2] - 1] = 0.0;
+        if (bd_[7] == 1) c.cz6[G.e[2] - 1] = 0.0;
+        const double d5 = ez * 0.5 * (R(ks) + R(ks - 1)) / R(ks);
+        const double d6 = ez * 0.5 * (R(ks) + R(ks + 1)) / R(ks);
+        for (int k = G.s[2]; k <= G.e[2]; ++k) {
+          c.dz5[k - 1] = d5;
+          c.dz6[k - 1] = d6;
+        }
+      }
+    } else {  // METRIC
+      const bool fine = (l == ng);
+      auto pcf = [&](int d, bool a, int q) {
+        const int gq = geo_[l].kpx[d] + q - 1;
+        return a ? pA_[d][gq] : pB_[d][gq];
+      };
+      for (int i = G.s[0]; i <= G.e[0]; ++i) {
+        double a1 = fine ? fm_[0][5][i - 1] * fm_[0][4][i - 2] : pcf(0, true, i);
+        double a2 = fine ? fm_[0][5][i - 1] * fm_[0][4][i - 1] : pcf(0, false, i);
+        if (bd_[9] == 1 && i == G.s[0]) a1 = 0.0;
+        if (bd_[18] == 1 && i == G.e[0]) a2 = 0.0;
+        c.cx1[i - 1] = a1;
+        c.cx2[i - 1] = a2;
+      }
+      for (int j = G.s[1]; j <= G.e[1]; ++j) {
+        double a3 = fine ? fm_[1][5][j - 1] * fm_[1][4][j - 2] : pcf(1, true, j);
+        double a4 = fine ? fm_[1][5][j - 1] * fm_[1][4][j - 1] : pcf(1, false, j);
+        if (bd_[5] == 1 && j == G.s[1]) a3 = 0.0;
+        if (bd_[1] == 1 && j == G.e[1]) a4 = 0.0;
+        c.cy3[j - 1] = a3;
+        c.cy4[j - 1] = a4;
+      }
+      for (int k = G.s[2]; k <= G.e[2]; ++k) {
+        double a5 = fine ? fm_[2][5][k - 1] * fm_[2][4][k - 2] : pcf(2, true, k);
+        double a6 = fine ? fm_[2][5][k - 1] * fm_[2][4][k - 1] : pcf(2, false, k);
+        if (bd_[3] == 1 && k == G.s[2]) a5 = 0.0;
+        if (bd_[7] == 1 && k == G.e[2]) a6 = 0.0;
+        const int km = 2 * kstep * k - 3 * (kstep - 1);
+        const int fk = fine ? k : km / 2;
+        const double rp = R(fk), rb = R(fk - 1), rt = R(fk + 1);
+        const double w5 = 0.5 * (rp + rb), w6 = 0.5 * (rp + rt);
+        c.cz5[k - 1] = a5 * w5 / rb;
+        c.cz6[k - 1] = a6 * w6 / rt;
+        c.dz5[k - 1] = a5 * w5 / rp;
+        c.dz6[k - 1] = a6 * w6 / rp;
+      }
+    }
+  }
+  coef_ready_ = true;
+  return ANEL_OK;
+}
+
+int MGSolver::upload_coefficients() {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  for (int l = 1; l <= ngrid_; ++l) {
+    const LevelCoef& c = coef_[l];
+    std::vector<double> packed;
+    for (const std::vector<double>* v :
+         {&c.cx1, &c.cx2, &c.cy3, &c.cy4, &c.cz5, &c.cz6, &c.dz5, &c.dz6})
+      packed.insert(packed.end(), v->begin(), v->end());
+    ANEL_CUDA_TRY(cudaMemcpy(d_coef64_[l], packed.data(), packed.size() * sizeof(double),
+                             cudaMemcpyHostToDevice));
+    if (d_coef32_[l]) {
+      std::vector<float> p32(packed.begin(), packed.end());
+      ANEL_CUDA_TRY(cudaMemcpy(d_coef32_[l], p32.data(), p32.size() * sizeof(float),
+                               cudaMemcpyHostToDevice));
+    }
+  }
+  return ANEL_OK;
+}
+
+int MGSolver::set_density_host(const double* r) {
+  if (!r) {
+    set_error("null density");
+    return ANEL_ERR_ARG;
+  }
+  const LevelGeom& F = geo_[ngrid_];
+  const int64_t XY = (int64_t)F.X * F.Y;
+  std::vector<double> rz(F.Z);
+  for (int k = 0; k < F.Z; ++k) {
+    const double* plane = r + (int64_t)k * XY;
+    const double v = plane[0];
+    for (int64_t q = 1; q < XY; ++q)
+      if (!(plane[q] == v)) {
+        set_error(
+            "density must be horizontally uniform r = r(z); plane k=%d differs at offset %lld",
+            k + 1, (long long)q);
+        return ANEL_ERR_UNSUPPORTED;
+      }
+    if (!std::isfinite(v) || v == 0.0) {
+      set_error("density plane k=%d is zero or not finite", k + 1);
+      return ANEL_ERR_NONFINITE;
+    }
+    rz[k] = v;
+  }
+  int st = build_coefficients(rz);
+  if (st != ANEL_OK) return st;
+  return upload_coefficients();
+}
+
+int MGSolver::set_density_device(const double* r, cudaStream_t s) {
+  const LevelGeom& F = geo_[ngrid_];
+  std::vector<double> h(F.G);
+  ANEL_CUDA_TRY(cudaMemcpyAsync(h.data(), r, F.G * sizeof(double), cudaMemcpyDeviceToHost,
+                                s ? s : stream_));
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s ? s : stream_));
+  return set_density_host(h.data());
+}
+
+// ------------------------------------------------------------ views
+DevLevel<double> MGSolver::L64(int l) const {
+  const LevelGeom& G = geo_[l];
+  DevLevel<double> L;
+  L.nx = G.n[0];
+  L.ny = G.n[1];
+  L.nz = G.n[2];
+  L.X = G.X;
+  L.Y = G.Y;
+  L.Z = G.Z;
+  L.XY = (int64_t)G.X * G.Y;
+  L.G = G.G;
+  L.phi = d_phi64_[l];
+  L.src = d_src64_[l];
+  L.coef = d_coef64_[l];
+  L.rule = rule_[l];
+  return L;
+}
+
+DevLevel<float> MGSolver::L32(int l, bool hom) const {
+  const LevelGeom& G = geo_[l];
+  DevLevel<float> L;
+  L.nx = G.n[0];
+  L.ny = G.n[1];
+  L.nz = G.n[2];
+  L.X = G.X;
+  L.Y = G.Y;
+  L.Z = G.Z;
+  L.XY = (int64_t)G.X * G.Y;
+  L.G = G.G;
+  L.phi = d_phi32_[l];
+  L.src = d_src32_[l];
+  L.coef = d_coef32_[l];
+  L.rule = hom ? rule_hom_[l] : rule_[l];
+  return L;
+}
+
+DevLevel<double> MGSolver::fine_view(double* phi, const double* src) const {
+  DevLevel<double> L = L64(ngrid_);
+  L.phi = phi;
+  L.src = const_cast<double*>(src);
+  return L;
+}
+
+int MGSolver::coarsen_dirs(int lC) const {
+  int m = 0;
+  for (int d = 0; d < 3; ++d)
+    if (geo_[lC].nk[d] < geo_[lC + 1].nk[d]) m |= 1 << d;
+  return m;
+}
+
+// ----------------------------------------------------------- V-cycle
+// mg_relaxRB: per iteration colour 0, boundary pass, colour 1, boundary
+// pass (mg_relax.F90:146-172); the extra final boundary pass of :176 is a
+// no-op after an iteration and is kept only when iters == 0.
+void MGSolver::relax64(int l, int iters, cudaStream_t s) {
+  const DevLevel<double> L = L64(l);
+  for (int it = 0; it < iters; ++it) {
+    launch_rb_sweep(L, 0, s);
+    launch_bdry(L, L.phi, s);
+    launch_rb_sweep(L, 1, s);
+    launch_bdry(L, L.phi, s);
+  }
+  if (iters == 0) launch_bdry(L, L.phi, s);
+}
+
+// mg_cycle.F90:186-325
+void MGSolver::cycle64(cudaStream_t s) {
+  const int ng = ngrid_;
+  const int* pre = prm_.pre_relax;
+  const int* post = prm_.post_relax;
+  relax64(ng, pre[ng - 1], s);
+  launch_restrict(L64(ng), L64(ng - 1), coarsen_dirs(ng - 1), s);
+  for (int l = ng - 1; l >= 2; --l) {
+    relax64(l, pre[l - 1], s);
+    launch_restrict(L64(l), L64(l - 1), coarsen_dirs(l - 1), s);
+  }
+  relax64(1, pre[0], s);
+  for (int l = 1; l <= ng - 1; ++l) {
+    relax64(l, post[l - 1], s);
+    const DevLevel<double> F = L64(l + 1);
+    launch_prolong(F, L64(l), coarsen_dirs(l), s);
+    launch_bdry(F, F.phi, s);
+  }
+  relax64(ng, post[ng - 1], s);
+}
+
+void MGSolver::relax32(int l, int iters, cudaStream_t s) {
+  const DevLevel<float> L = L32(l, true);
+  for (int it = 0; it < iters; ++it) {
+    launch_rb_sweep(L, 0, s);
+    launch_bdry(L, L.phi, s);
+    launch_rb_sweep(L, 1, s);
+    launch_bdry(L, L.phi, s);
+  }
+  if (iters == 0) launch_bdry(L, L.phi, s);
+}
+
+void MGSolver::cycle32(cudaStream_t s) {
+  const int ng = ngrid_;
+  const int* pre = prm_.pre_relax;
+  const int* post = prm_.post_relax;
+  relax32(ng, pre[ng - 1], s);
+  launch_restrict(L32(ng, true), L32(ng - 1, true), coarsen_dirs(ng - 1), s);
+  for (int l = ng - 1; l >= 2; --l) {
+    relax32(l, pre[l - 1], s);
+    launch_restrict(L32(l, true), L32(l - 1, true), coarsen_dirs(l - 1), s);
+  }
+  relax32(1, pre[0], s);
+  for (int l = 1; l <= ng - 1; ++l) {
+    relax32(l, post[l - 1], s);
+    const DevLevel<float> F = L32(l + 1, true);
+    launch_prolong(F, L32(l, true), coarsen_dirs(l), s);
+    launch_bdry(F, F.phi, s);
+  }
+  relax32(ng, post[ng - 1], s);
+}
+
+// ------------------------------------------------------------ solves
+double MGSolver::true_resid(const double* d_phi, const double* d_rhs, cudaStream_t s,
+                            double* fnorm) {
+  const DevLevel<double> F = fine_view(const_cast<double*>(d_phi), d_rhs);
+  launch_resid_norm(F, d_phi, d_rhs, d_part_, d_norm_, s);
+  cudaMemcpyAsync(h_pin_, d_norm_, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  if (fnorm) *fnorm = std::sqrt(h_pin_[1]);
+  return h_pin_[1] > 0.0 ? std::sqrt(h_pin_[0] / h_pin_[1]) : std::sqrt(h_pin_[0]);
+}
+
+int MGSolver::solve_device(double* d_phi, const double* d_rhs, cudaStream_t s,
+                           anel_mg_report* rep) {
+  if (!d_phi || !d_rhs) {
+    set_error("null phi or rhs");
+    return ANEL_ERR_ARG;
+  }
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  anel_mg_report r{};
+  ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
+  const int st = prm_.precision == ANEL_PREC_MIXED ? solve_mixed(d_phi, d_rhs, s, &r)
+                                                   : solve_fp64(d_phi, d_rhs, s, &r);
+  ANEL_CUDA_TRY(cudaEventRecord(ev1_, s));
+  ANEL_CUDA_TRY(cudaEventSynchronize(ev1_));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev0_, ev1_);
+  r.ms = ms;
+  if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
+  const int le = check_launch("mg solve");
+  if (le != ANEL_OK) return le;
+  r.resid = true_resid(d_phi, d_rhs, s, nullptr);
+  r.status = st;
+  if (rep) *rep = r;
+  return st;
+}
+
+int MGSolver::solve_fp64(double* d_phi, const double* d_rhs, cudaStream_t s,
+                         anel_mg_report* rep) {
+  const int ng = ngrid_;
+  const DevLevel<double> Fu = fine_view(d_phi, d_rhs);
+  const DevLevel<double> W = L64(ng);
+  launch_bdry(Fu, d_phi, s);  // mg_solver.F90:101
+  ANEL_CUDA_TRY(cudaMemcpyAsync(W.phi, d_phi, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  ANEL_CUDA_TRY(cudaMemcpyAsync(W.src, d_rhs, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  double relmax = 0.0, fn = 0.0;
+  int iter = 0;
+  bool conv = false;
+  const bool by_resid = prm_.stop == ANEL_STOP_RESID;
+  if (by_resid) {
+    // ||f|| once; ||f - A phi|| is taken on the work array after each cycle
+    true_resid(d_phi, d_rhs, s, &fn);
+  }
+  for (iter = 1; iter <= prm_.maxcy; ++iter) {
+    cycle64(s);
+    if (by_resid) {
+      const double res = true_resid(W.phi, d_rhs, s, nullptr);
+      relmax = res;
+      if (prm_.verbose) std::fprintf(stderr, "       Iteration: %5d  RESID= %22.15e\n", iter, res);
+      if (res <= prm_.tolmax) {
+        conv = true;
+        break;
+      }
+    } else {
+      ANEL_CUDA_TRY(cudaMemsetAsync(d_max_, 0, 2 * sizeof(unsigned long long), s));
+      launch_relmax_copy(W, W.phi, d_phi, d_max_, s);
+      ANEL_CUDA_TRY(cudaMemcpyAsync(h_pin_, d_max_, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+      ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+      const double v1 = h_pin_[0], v2 = h_pin_[1];  // bit patterns of the maxima
+      relmax = v1 > 0.0 ? v2 / v1 : 0.0;
+      if (prm_.verbose)
+        std::fprintf(stderr, "       Iteration: %5d  RESIDUAL= %22.15e\n", iter, relmax);
+      if (relmax <= prm_.tolmax) {
+        conv = true;
+        break;
+      }
+    }
+  }
+  if (by_resid)
+    ANEL_CUDA_TRY(cudaMemcpyAsync(d_phi, W.phi, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  launch_bdry(Fu, d_phi, s);  // mg_solver.F90:139
+  if (!conv) {
+    if (prm_.verbose)
+      std::fprintf(stderr, "WARNING: failed to achieve convergence in %6d cycles, RESIDUAL=%22.16f\n",
+                   prm_.maxcy, relmax);
+    iter = prm_.maxcy + 1;  // value of the Fortran DO variable after the loop
+  }
+  rep->iter = iter;
+  rep->relmax = relmax;
+  return conv ? ANEL_OK : ANEL_ERR_NOCONV;
+}
+
+// Mixed precision: FP64 defect correction around one FP32 V-cycle per
+// iteration.  FP64: fine residual, correction update, norms, boundary
+// pass of the solution.  FP32: smoothing, restriction, prolongation and
+// every coarse level, on the error equation (homogeneous wall values).
+int MGSolver::solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s,
+                          anel_mg_report* rep) {
+  const int ng = ngrid_;
+  const DevLevel<double> Fu = fine_view(d_phi, d_rhs);
+  const DevLevel<float> E = L32(ng, true);
+  launch_bdry(Fu, d_phi, s);
+  double rel = 0.0;
+  int iter = 0;
+  bool conv = false;
+  for (iter = 0; iter <= prm_.maxcy; ++iter) {
+    launch_resid_store(Fu, d_phi, d_rhs, E.src, d_part_, d_norm_, s);
+    ANEL_CUDA_TRY(cudaMemcpyAsync(h_pin_, d_norm_, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+    rel = h_pin_[1] > 0.0 ? std::sqrt(h_pin_[0] / h_pin_[1]) : std::sqrt(h_pin_[0]);
+    if (prm_.verbose) std::fprintf(stderr, "       Defect: %5d  RESID= %22.15e\n", iter, rel);
+    if (rel <= prm_.tolmax) {
+      conv = true;
+      break;
+    }
+    if (iter == prm_.maxcy) break;
+    ANEL_CUDA_TRY(cudaMemsetAsync(E.phi, 0, E.G * sizeof(float), s));
+    cycle32(s);
+    launch_add_correction(Fu, d_phi, E.phi, s);
+    launch_bdry(Fu, d_phi, s);
+  }
+  rep->iter = conv ? iter : prm_.maxcy + 1;
+  rep->relmax = rel;
+  return conv ? ANEL_OK : ANEL_ERR_NOCONV;
+}
+
+int MGSolver::solve_host(double* phi, const double* rhs, cudaStream_t s, anel_mg_report* rep) {
+  if (!phi || !rhs) {
+    set_error("null phi or rhs");
+    return ANEL_ERR_ARG;
+  }
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  const size_t bytes = geo_[ngrid_].G * sizeof(double);
+  if (!d_io_phi_) {
+    ANEL_CUDA_TRY(cudaMalloc(&d_io_phi_, bytes));
+    ANEL_CUDA_TRY(cudaMalloc(&d_io_rhs_, bytes));
+  }
+  ANEL_CUDA_TRY(cudaMemcpyAsync(d_io_phi_, phi, bytes, cudaMemcpyHostToDevice, s));
+  ANEL_CUDA_TRY(cudaMemcpyAsync(d_io_rhs_, rhs, bytes, cudaMemcpyHostToDevice, s));
+  const int st = solve_device(d_io_phi_, d_io_rhs_, s, rep);
+  if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
+  ANEL_CUDA_TRY(cudaMemcpyAsync(phi, d_io_phi_, bytes, cudaMemcpyDeviceToHost, s));
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  return st;
+}
+
+int MGSolver::debug_pass(int which, double* d_phi, const double* d_src, cudaStream_t s) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  const int ng = ngrid_;
+  const DevLevel<double> W = L64(ng);
+  if (which == 0 || which == 1) {
+    DevLevel<double> F = fine_view(d_phi, d_src);
+    if (which == 0) {
+      launch_rb_sweep(F, 0, s);
+      launch_bdry(F, d_phi, s);
+      launch_rb_sweep(F, 1, s);
+      launch_bdry(F, d_phi, s);
+    } else {
+      launch_bdry(F, d_phi, s);
+    }
+  } else if (which == 2) {
+    ANEL_CUDA_TRY(cudaMemcpyAsync(W.phi, d_phi, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    ANEL_CUDA_TRY(cudaMemcpyAsync(W.src, d_src, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    cycle64(s);
+    ANEL_CUDA_TRY(cudaMemcpyAsync(d_phi, W.phi, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  } else {
+    set_error("unknown debug pass %d", which);
+    return ANEL_ERR_ARG;
+  }
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  return check_launch("debug pass");
+}
+
+int MGSolver::levels_table(int32_t* out, int cap) const {
+  for (int l = 1; l <= ngrid_ && l <= cap; ++l) {
+    const LevelGeom& G = geo_[l];
+    int32_t* o = out + (l - 1) * 12;
+    o[0] = G.nk[0];
+    o[1] = G.nk[1];
+    o[2] = G.nk[2];
+    o[3] = G.s[0];
+    o[4] = G.e[0];
+    o[5] = G.s[1];
+    o[6] = G.e[1];
+    o[7] = G.s[2];
+    o[8] = G.e[2];
+    o[9] = (int32_t)G.kp3d;
+    o[10] = G.kpx[0];
+    o[11] = G.kpx[1];
+  }
+  return ngrid_;
+}
+
+}  // namespace anel

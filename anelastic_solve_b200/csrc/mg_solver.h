@@ -1,0 +1,91 @@
+// mg_solver.h -- host side of the B200 multigrid pressure solver.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "mg_launch.h"
+
+namespace anel {
+
+// The solver context: what MG_init builds (mg_init.F90:70-351) plus the
+// device workspaces.  Not thread-safe; calls are ordered on `stream_`.
+class MGSolver {
+ public:
+  static MGSolver* create(const anel_grid_desc* g, const anel_mg_params* p, int device,
+                          int* status);
+  ~MGSolver();
+
+  // Density Flow::r on the fine ghosted grid (host pointer).  Must be
+  // horizontally uniform, r = r(z), as every density profile of the
+  // reference is; otherwise ANEL_ERR_UNSUPPORTED.
+  int set_density_host(const double* r);
+  int set_density_device(const double* r, cudaStream_t s);
+
+  // mg_solver on device arrays: d_phi inout (ghosted FP64), d_rhs in.
+  int solve_device(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
+  // Same with host arrays (copies in and out through pinned staging).
+  int solve_host(double* phi, const double* rhs, cudaStream_t s, anel_mg_report* rep);
+
+  int debug_pass(int which, double* d_phi, const double* d_src, cudaStream_t s);
+  int levels_table(int32_t* out, int cap) const;
+
+  cudaStream_t stream() const { return stream_; }
+  int device() const { return device_; }
+  const LevelGeom& fine() const { return geo_[ngrid_]; }
+  int ngrid() const { return ngrid_; }
+  const anel_mg_params& params() const { return prm_; }
+  // Fine-level FP64 descriptor bound to the given arrays.
+  DevLevel<double> fine_view(double* phi, const double* src) const;
+
+ private:
+  MGSolver() = default;
+  int init(const anel_grid_desc* g, const anel_mg_params* p, int device);
+  void build_metric_hierarchy();
+  int build_coefficients(const std::vector<double>& rz);
+  int upload_coefficients();
+  void relax64(int l, int iters, cudaStream_t s);
+  void cycle64(cudaStream_t s);
+  void relax32(int l, int iters, cudaStream_t s);
+  void cycle32(cudaStream_t s);
+  int solve_fp64(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
+  int solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
+  int coarsen_dirs(int lC) const;
+  double true_resid(const double* d_phi, const double* d_rhs, cudaStream_t s, double* fnorm);
+
+  anel_mg_params prm_{};
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr;
+  int nx_ = 0, ny_ = 0, nz_ = 0;
+  double L_[3] = {0, 0, 0};
+  int ngrid_ = 0;
+  int nC_[3] = {0, 0, 0};
+  LevelGeom geo_[ANEL_MAX_LEVELS + 1];
+  int bd_[27] = {0};
+  double phibc_[ANEL_MAX_LEVELS + 1][6];
+  // fine metrics (n+2 each) and the coarse hierarchy (mg_grids.F90)
+  std::vector<double> fm_[3][6];          // xe xc dxe dxc rdxe rdxc
+  std::vector<double> hE_[3], hC_[3], hDC_[3], hDE_[3], pA_[3], pB_[3];
+  LevelCoef coef_[ANEL_MAX_LEVELS + 1];
+  BdryRule rule_[ANEL_MAX_LEVELS + 1];
+  BdryRule rule_hom_[ANEL_MAX_LEVELS + 1];  // same with phibc = 0 (error equation)
+  bool coef_ready_ = false;
+  // device memory
+  double* d_phi64_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  double* d_src64_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  double* d_coef64_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  float* d_phi32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  float* d_src32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  float* d_coef32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  unsigned long long* d_max_ = nullptr;   // 2 words
+  double* d_part_ = nullptr;              // norm partials
+  double* d_norm_ = nullptr;              // 2 doubles
+  double* d_io_phi_ = nullptr;            // staging for host-pointer solves
+  double* d_io_rhs_ = nullptr;
+  double* h_pin_ = nullptr;               // pinned small readback (4 doubles)
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  DevLevel<double> L64(int l) const;
+  DevLevel<float> L32(int l, bool hom) const;
+};
+
+}  // namespace anel

@@ -1,0 +1,167 @@
+/*
+ * anel.h -- C-ABI of the B200 (sm_100a) anelastic/Boussinesq hot path:
+ * the multigrid pressure-Poisson solve (mgMK) and the RK3 sub-step.
+ *
+ * Every entry point takes plain pointers and sizes.  Field arrays are the
+ * reference's ghost-layered, column-major (i fastest) FP64 arrays:
+ *   element (i,j,k), 1-based with ghosts, i = 1..nx+2 (interior 2..nx+1),
+ *   sits at offset (i-1) + (nx+2)*((j-1) + (ny+2)*(k-1)).
+ * 1-D grid metric arrays (xe, xc, dxe, dxc, rdxe, rdxc, ...) have n+2
+ * entries, entry 0 being the Fortran index 1, exactly as read from the
+ * reference's x?_grid.in files (ANELASTIC_SL/utils/loadGrid.F90:38-90).
+ *
+ * Two families of calls exist:
+ *  - drop-in calls with the reference's names and by-reference arguments
+ *    (anel_mg_init / anel_mg_solve / anel_mg_finalize, anel_rk_substep),
+ *    operating on one library-owned default context and on HOST arrays;
+ *  - context calls (anel_mg_ctx_*, anel_ns_ctx_*) that take a context
+ *    handle, a memory-space flag (host or device pointers) and a CUDA
+ *    stream, for device-resident use and for many independent members.
+ *
+ * Return codes are ANEL_OK (0) or a negative ANEL_ERR_*; no call exits the
+ * process.  anel_last_error() returns a message for the calling thread.
+ */
+#ifndef ANEL_H
+#define ANEL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ANEL_MAX_LEVELS 16
+
+/* ---- status codes ---------------------------------------------------- */
+enum {
+  ANEL_OK = 0,
+  ANEL_ERR_SIZE = -1,        /* level/size constraints (mg_check_size.F90:77-151) */
+  ANEL_ERR_BC = -2,          /* bad boundary-condition code (mg_init.F90:317-328) */
+  ANEL_ERR_NOCONV = -3,      /* maxcy reached before tolmax (mg_solver.F90:130-133) */
+  ANEL_ERR_CUDA = -4,        /* a CUDA runtime call failed */
+  ANEL_ERR_TIMEOUT = -5,     /* a bounded device-side loop gave up */
+  ANEL_ERR_ARG = -6,         /* null pointer / bad enum / not initialised */
+  ANEL_ERR_NOMEM = -7,       /* device allocation failed */
+  ANEL_ERR_UNSUPPORTED = -8, /* valid in the reference, not handled by this build */
+  ANEL_ERR_NONFINITE = -9    /* NaN/Inf found in an input field */
+};
+
+/* ---- enums ------------------------------------------------------------ */
+enum { ANEL_SMOOTHER_RBPGS = 0, ANEL_SMOOTHER_LJ = 1 };
+/* LITERAL: the reference's RBPGS operator (uniform spacing xL/nx, zL/nz,
+ *          mg_pfpde.F90 / mg_phpde.F90).  METRIC: the same V-cycle with
+ *          every level's 7-point operator built from the stretched metric
+ *          (mg_grids.F90 + mg_coeff.F90), consistent with Psource/Pgrad. */
+enum { ANEL_MODE_LITERAL = 0, ANEL_MODE_METRIC = 1 };
+/* FP64: every MG array FP64.  MIXED: FP32 V-cycle inside an FP64 defect-
+ *       correction loop (FP64 fine residual, correction and norms). */
+enum { ANEL_PREC_FP64 = 0, ANEL_PREC_MIXED = 1 };
+/* RELMAX: the reference's stop test max|phi_new-phi_old|/max|phi_new| <=
+ *         tolmax (mg_residual.F90:60-94).  RESID: ||f - A phi||_2/||f||_2
+ *         <= tolmax with the fine operator. */
+enum { ANEL_STOP_RELMAX = 0, ANEL_STOP_RESID = 1 };
+enum { ANEL_MEM_HOST = 0, ANEL_MEM_DEVICE = 1 };
+/* boundary types, tbc[] (mg_read_params.F90:96-99) */
+enum { ANEL_BC_PERIODIC = 0, ANEL_BC_NEUMANN = 1, ANEL_BC_DIRICHLET = 2 };
+
+/* ---- descriptors -------------------------------------------------------
+ * anel_grid_desc replaces the Domain and Grid modules
+ * (ANELASTIC_SL/include/modules.F90:17-39): interior sizes, domain lengths
+ * and the 18 metric arrays of length n+2. */
+typedef struct {
+  int32_t nx, ny, nz;
+  double xL, yL, zL;
+  const double *xe, *xc, *dxe, *dxc, *rdxe, *rdxc;
+  const double *ye, *yc, *dye, *dyc, *rdye, *rdyc;
+  const double *ze, *zc, *dze, *dzc, *rdze, *rdzc;
+} anel_grid_desc;
+
+/* anel_mg_params replaces the mgVars module inputs read by mg_read_params
+ * (ANELASTIC_SL/mgMK/mg_read_params.F90:43-214).  pre_relax/post_relax are
+ * indexed by level-1, level 1 = coarsest, exactly as the ini lists them.
+ * tbc/vbc use the reference face order 1=X2max 2=X3min 3=X2min 4=X3max
+ * 5=X1min 6=X1max (index 0..5 here). */
+typedef struct {
+  int32_t levels[3];               /* nxlevels, nylevels, nzlevels */
+  int32_t maxcy;                   /* maximum V-cycles */
+  double tolmax;                   /* stop tolerance */
+  int32_t smoother;                /* ANEL_SMOOTHER_* */
+  int32_t pre_relax[ANEL_MAX_LEVELS];
+  int32_t post_relax[ANEL_MAX_LEVELS];
+  int32_t tbc[6];
+  double vbc[6];
+  int32_t mode;                    /* ANEL_MODE_* */
+  int32_t precision;               /* ANEL_PREC_* */
+  int32_t stop;                    /* ANEL_STOP_* */
+  int32_t verbose;                 /* print per-cycle residuals to stderr */
+} anel_mg_params;
+
+/* Per-solve report (the reference prints the same numbers,
+ * NSsolver.F90:524 and mg_solver.F90:123). */
+typedef struct {
+  int32_t iter;        /* V-cycles (MIXED: defect-correction iterations) */
+  int32_t status;      /* ANEL_OK or ANEL_ERR_NOCONV / _TIMEOUT */
+  double relmax;       /* reference stop metric of the last cycle */
+  double resid;        /* ||f - A phi||_2 / ||f||_2 (fine operator) after the solve */
+  double ms;           /* device time of the solve (CUDA events) */
+} anel_mg_report;
+
+typedef struct anel_mg_ctx anel_mg_ctx;
+
+/* ---- library ------------------------------------------------------------ */
+const char* anel_last_error(void);
+int anel_version(void);
+/* Number of this library's kernels launched since load (all contexts). */
+int64_t anel_kernel_launch_count(void);
+
+/* ---- multigrid: drop-in calls ------------------------------------------ */
+
+/* Replaces mg_read_params + MG_init (mg_read_params.F90:1-218,
+ * mg_init.F90:1-351): level maps, workspace, coarse metrics.  Returns the
+ * reference's stat meaning as ANEL_OK / ANEL_ERR_SIZE / ANEL_ERR_BC. */
+int anel_mg_init(const anel_grid_desc* grid, const anel_mg_params* params);
+
+/* Sets the density Flow::r (host, ghosted G array) used to build the level
+ * coefficients (mg_solver.F90:81-97 rebuilds them from r on every call;
+ * here they are rebuilt only when r changes).  Before the first call r == 1. */
+int anel_mg_set_density(const double* r);
+
+/* Replaces mg_solver(phif,rhsf,iter,relmax) (mg_solver.F90:1-141), same
+ * argument order, Fortran by-reference, host arrays.  phif: inout, ghosted;
+ * its ghosts are set by the final boundary pass.  rhsf: in; the reference
+ * uses it as V-cycle scratch (mg_cycle.F90:33,84-85), so its contents on
+ * return are unspecified here as well.  iter: cycles used (maxcy when not
+ * converged).  relmax: last max|dphi|/max|phi|. */
+void anel_mg_solve(double* phif, double* rhsf, int32_t* iter, double* relmax);
+
+/* Replaces mg_end (mg_end.F90:1-42). */
+int anel_mg_finalize(void);
+
+/* ---- multigrid: context calls ------------------------------------------- */
+anel_mg_ctx* anel_mg_create(const anel_grid_desc* grid, const anel_mg_params* params,
+                            int32_t device, int32_t* status);
+void anel_mg_destroy(anel_mg_ctx* ctx);
+int anel_mg_ctx_set_density(anel_mg_ctx* ctx, const double* r, int32_t mem);
+/* phif/rhsf are host (ANEL_MEM_HOST) or device (ANEL_MEM_DEVICE) ghosted
+ * FP64 arrays; stream is a cudaStream_t (NULL = the context's stream).
+ * rhsf is read only (unlike the reference, it is not clobbered). */
+int anel_mg_ctx_solve(anel_mg_ctx* ctx, double* phif, const double* rhsf, int32_t mem,
+                      void* stream, anel_mg_report* report);
+/* Level table, for tests of the bit-exact index maps (mg_init.F90:125-220):
+ * out[l*12 + 0..11] = nxk nyk nzk sxk exk syk eyk szk ezk kp3d kpx1 kpx2
+ * for l = 0..ngrid-1 (level l+1); returns ngrid. */
+int anel_mg_ctx_levels(const anel_mg_ctx* ctx, int32_t* out, int32_t cap);
+
+/* Primitive passes on the finest level, device pointers, for parity tests
+ * of single kernels.  which: 0 = one RB-GS iteration (both colours + the
+ * boundary pass after each, mg_relax.F90:146-172), 1 = boundary pass only
+ * (mg_bdry.F90), 2 = one V-cycle with phif as initial guess
+ * (mg_cycle.F90). */
+int anel_mg_ctx_debug_pass(anel_mg_ctx* ctx, int32_t which, double* d_phi,
+                           const double* d_src, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ANEL_H */

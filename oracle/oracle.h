@@ -1,0 +1,57 @@
+/*
+ * oracle.h -- CPU FP64 restatement of the reference's hot path, used ONLY
+ * as test infrastructure: the parity tests, __graft_entry__.smoke() and the
+ * CPU-baseline leg of bench.py call it as the checker.  The product library
+ * (anelastic_solve_b200/libanel.so) never links, loads or calls it.
+ *
+ * Parity status: the Fortran reference cannot be compiled in this
+ * environment (no Fortran front end, no MPI), so this restatement is pinned
+ * by the reference's own known-answer cases (the six analytic problems of
+ * ANELASTIC_SL/mgMK/test/test.F90:149-382, whose exact solutions are at
+ * :471-564) and by manufactured solutions, not by reference binaries.
+ *
+ * Evaluation order follows the Fortran source left to right and the
+ * library is built with -ffp-contract=off so no FMA changes a rounding.
+ */
+#ifndef ANEL_ORACLE_H
+#define ANEL_ORACLE_H
+
+#include "../include/anel.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_mg orc_mg;
+
+/* MG_init + mg_read_params (values passed in directly).  *stat = 0 ok,
+ * the mg_check_size code (1..12) or -1 for a bad BC. */
+orc_mg* orc_mg_create(const anel_grid_desc* g, const anel_mg_params* p, int* stat);
+void orc_mg_destroy(orc_mg* m);
+
+/* Density Flow::r on the fine ghosted grid; default r == 1. */
+void orc_mg_set_density(orc_mg* m, const double* r);
+
+/* mg_solver(phif, rhsf, iter, relmax) with the reference semantics,
+ * including the clobbering of rhsf (mg_cycle.F90:84-85). */
+void orc_mg_solve(orc_mg* m, double* phif, double* rhsf, int* iter, double* relmax);
+
+/* Single passes on the finest level (for kernel parity tests).
+ * which: 0 = one mg_relaxRB iteration (iters=1), 1 = mg_bdry,
+ *        2 = one mg_cycle (with coefficients built first). */
+void orc_mg_debug_pass(orc_mg* m, int which, double* phi, double* src);
+
+/* Level table in the layout of anel_mg_ctx_levels(); returns ngrid. */
+int orc_mg_levels(const orc_mg* m, int* out, int cap);
+
+/* ||f - A phi||_2 / ||f||_2 over the fine interior with the fine operator
+ * of the context's mode (coefficients built from the current density). */
+double orc_mg_true_resid(orc_mg* m, const double* phi, const double* f);
+
+/* Apply the fine operator: out(interior) = A phi (phi ghosts must be set). */
+void orc_mg_apply(orc_mg* m, const double* phi, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,103 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+the CPU-baseline leg of bench.py, as the checker.  The product package
+never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from anelastic_solve_b200 import abi
+
+_HERE = Path(__file__).resolve().parent
+_LIB = None
+
+
+def build() -> Path:
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", str(_HERE)], check=True)
+    return _HERE / "liboracle.so"
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        so = _HERE / "liboracle.so"
+        if not so.exists():
+            build()
+        L = C.CDLL(str(so))
+        L.orc_mg_create.restype = C.c_void_p
+        L.orc_mg_create.argtypes = [C.POINTER(abi.GridDesc), C.POINTER(abi.MGParams),
+                                    C.POINTER(C.c_int)]
+        L.orc_mg_destroy.argtypes = [C.c_void_p]
+        L.orc_mg_set_density.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.orc_mg_solve.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.orc_mg_debug_pass.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double)]
+        L.orc_mg_levels.restype = C.c_int
+        L.orc_mg_levels.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_int]
+        L.orc_mg_true_resid.restype = C.c_double
+        L.orc_mg_true_resid.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_mg_apply.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        _LIB = L
+    return _LIB
+
+
+def _f(a: np.ndarray) -> np.ndarray:
+    if not (a.dtype == np.float64 and a.flags.f_contiguous):
+        raise TypeError("oracle fields must be Fortran-ordered float64 arrays")
+    return a
+
+
+class OracleMG:
+    """mg_read_params + MG_init + mg_solver of the reference, on the CPU."""
+
+    def __init__(self, grid, params: abi.MGParams):
+        self._desc, self._keep = abi.make_grid_desc(grid)
+        self.params = params
+        st = C.c_int(0)
+        self._h = lib().orc_mg_create(C.byref(self._desc), C.byref(params), C.byref(st))
+        self.stat = st.value
+        self.grid = grid
+        if self.stat != 0:
+            lib().orc_mg_destroy(self._h)
+            self._h = None
+            raise ValueError(f"oracle MG_init failed, stat={self.stat}")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_mg_destroy(self._h)
+            self._h = None
+
+    def set_density(self, r: np.ndarray):
+        lib().orc_mg_set_density(self._h, abi.dptr(_f(r)))
+
+    def solve(self, phi: np.ndarray, rhs: np.ndarray):
+        """In place on phi (and clobbers rhs, like the reference)."""
+        it = C.c_int(0)
+        rm = C.c_double(0)
+        lib().orc_mg_solve(self._h, abi.dptr(_f(phi)), abi.dptr(_f(rhs)), C.byref(it), C.byref(rm))
+        return it.value, rm.value
+
+    def debug_pass(self, which: int, phi: np.ndarray, src: np.ndarray):
+        lib().orc_mg_debug_pass(self._h, which, abi.dptr(_f(phi)), abi.dptr(_f(src)))
+
+    def levels(self) -> np.ndarray:
+        out = (C.c_int * (12 * abi.MAX_LEVELS))()
+        n = lib().orc_mg_levels(self._h, out, abi.MAX_LEVELS)
+        return np.array(out[: 12 * n], dtype=np.int64).reshape(n, 12)
+
+    def true_resid(self, phi, f) -> float:
+        return lib().orc_mg_true_resid(self._h, abi.dptr(_f(phi)), abi.dptr(_f(f)))
+
+    def apply(self, phi) -> np.ndarray:
+        out = np.zeros_like(phi, order="F")
+        lib().orc_mg_apply(self._h, abi.dptr(_f(phi)), abi.dptr(out))
+        return out

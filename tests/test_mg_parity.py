@@ -1,0 +1,148 @@
+"""GPU multigrid vs the CPU oracle, through the C-ABI.
+
+The FP64 path must be bit-identical to the oracle (the reference's
+algorithm evaluated in its own order): boundary pass, one red-black
+iteration, one V-cycle, and whole solves including iteration count and the
+reference stop metric.  The mixed-precision path must reach the FP64
+oracle's solution within 1e-9 relative L2 (after removing the mean, the
+problem being singular) with a true relative residual <= 1e-10.
+"""
+import numpy as np
+import pytest
+
+from anelastic_solve_b200 import abi
+from anelastic_solve_b200 import grid as G
+from anelastic_solve_b200.mg import MGSolver
+from oracle.pyoracle import OracleMG
+
+from .helpers import compatible, field, levels_for, mg_params, rel_l2, remove_mean, zeros
+
+pytestmark = pytest.mark.gpu
+
+
+def to_dev(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+
+
+def to_host(t):
+    return np.asfortranarray(t.cpu().numpy().T)
+
+
+CASES = {
+    # name: (grid, tbc, vbc, levels)
+    "shear_uniform": (lambda: G.shear_layer_grid(16, 8, 16, stretched=False), (0, 1, 0, 1, 0, 0),
+                      (0, 0, 0, 0, 0, 0), None),
+    "shear_stretched_vbc": (lambda: G.shear_layer_grid(32, 16, 32, stretched=True),
+                            (0, 1, 0, 1, 0, 0), (0, 0.25, 0, -0.5, 0, 0), None),
+    "walls_everywhere": (lambda: G.Grid(G.uniform_axis(16, 1.0), G.uniform_axis(12, 0.75),
+                                        G.uniform_axis(8, 0.5)),
+                         (1, 2, 2, 1, 1, 2), (0.3, 1.0, -1.0, 0.2, -0.4, 0.5), None),
+    "partial_coarsening": (lambda: G.shear_layer_grid(16, 8, 32, stretched=False), (0, 1, 0, 1, 0, 0),
+                           (0, 0, 0, 0, 0, 0), (3, 2, 5)),
+    "odd_coarse": (lambda: G.Grid(G.uniform_axis(12, 1.0), G.uniform_axis(6, 0.5),
+                                  G.uniform_axis(12, 1.0)), (0, 1, 0, 1, 0, 0), (0, 0, 0, 0, 0, 0),
+                   (3, 2, 3)),
+}
+
+
+def _pair(name, mode=abi.MODE_LITERAL, **kw):
+    mk, tbc, vbc, lv = CASES[name]
+    g = mk()
+    p = mg_params(g, levels=lv or levels_for(g), tbc=tbc, vbc=vbc, mode=mode, **kw)
+    return g, p, OracleMG(g, p), MGSolver(g, p)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_level_tables_match(name):
+    g, p, o, s = _pair(name)
+    np.testing.assert_array_equal(o.levels(), s.levels())
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_LITERAL, abi.MODE_METRIC])
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("which", [1, 0, 2])
+def test_single_pass_bitwise(name, mode, which):
+    """which: 1 = mg_bdry, 0 = one RB-GS iteration, 2 = one V-cycle."""
+    g, p, o, s = _pair(name, mode)
+    rng = np.random.default_rng(11 + which)
+    phi = field(g, rng)
+    src = field(g, rng)
+    ref = phi.copy(order="F")
+    o.debug_pass(which, ref, src.copy(order="F"))
+    dphi, dsrc = to_dev(phi), to_dev(src)
+    s.debug_pass(which, dphi, dsrc)
+    got = to_host(dphi)
+    np.testing.assert_array_equal(got, ref)
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_LITERAL, abi.MODE_METRIC])
+@pytest.mark.parametrize("name", list(CASES))
+def test_solve_bitwise(name, mode):
+    g, p, o, s = _pair(name, mode, maxcy=60, tolmax=1e-9)
+    rng = np.random.default_rng(5)
+    src = compatible(field(g, rng), g, mode)
+    phi0 = field(g, rng, 0.1)
+    ref = phi0.copy(order="F")
+    it_o, rm_o = o.solve(ref, src.copy(order="F"))
+    dphi, dsrc = to_dev(phi0), to_dev(src)
+    it_g, rm_g = s.solve(dphi, dsrc)
+    assert it_g == it_o
+    assert rm_g == rm_o
+    np.testing.assert_array_equal(to_host(dphi), ref)
+    # the right-hand side is read only on the device path
+    np.testing.assert_array_equal(to_host(dsrc), src)
+
+
+def test_host_path_equals_device_path():
+    g, p, o, s = _pair("shear_stretched_vbc", maxcy=40, tolmax=1e-10)
+    rng = np.random.default_rng(3)
+    src = remove_mean(field(g, rng))
+    phi_h = zeros(g)
+    it_h, rm_h = s.solve(phi_h, src.copy(order="F"))
+    dphi, dsrc = to_dev(zeros(g)), to_dev(src)
+    it_d, rm_d = s.solve(dphi, dsrc)
+    assert (it_h, rm_h) == (it_d, rm_d)
+    np.testing.assert_array_equal(phi_h, to_host(dphi))
+
+
+def test_nonconvergence_reports_like_reference():
+    """maxcy reached: the Fortran DO variable ends at maxcy+1
+    (mg_solver.F90:114-133) and the status is ANEL_ERR_NOCONV."""
+    g, p, o, s = _pair("shear_uniform", maxcy=1, tolmax=1e-30)
+    rng = np.random.default_rng(9)
+    src = remove_mean(field(g, rng))
+    ref = zeros(g)
+    it_o, rm_o = o.solve(ref, src.copy(order="F"))
+    dphi = to_dev(zeros(g))
+    it_g, rm_g = s.solve(dphi, to_dev(src))
+    assert it_o == it_g == 2
+    assert rm_g == rm_o
+    assert s.last_report.status == abi.ERR_NOCONV
+    with pytest.raises(Exception):
+        s.solve(to_dev(zeros(g)), to_dev(src), allow_noconv=False)
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_LITERAL, abi.MODE_METRIC])
+def test_mixed_precision_reaches_fp64_solution(mode):
+    g = G.shear_layer_grid(32, 16, 32, stretched=True)
+    lv = levels_for(g)
+    rng = np.random.default_rng(21)
+    src = compatible(field(g, rng), g, mode)
+    # FP64 oracle solved to the true-residual target
+    po = mg_params(g, levels=lv, mode=mode, maxcy=400, tolmax=1e-14)
+    o = OracleMG(g, po)
+    ref = zeros(g)
+    o.solve(ref, src.copy(order="F"))
+    assert o.true_resid(ref, src) < 1e-10
+    pm = mg_params(g, levels=lv, mode=mode, maxcy=100, tolmax=1e-10,
+                   precision=abi.PREC_MIXED, stop=abi.STOP_RESID)
+    s = MGSolver(g, pm)
+    dphi = to_dev(zeros(g))
+    it, res = s.solve(dphi, to_dev(src))
+    got = to_host(dphi)
+    assert s.last_report.status == abi.OK
+    assert s.last_report.resid <= 1e-10
+    assert o.true_resid(got, src) <= 1.01e-10
+    assert rel_l2(remove_mean(got), remove_mean(ref)) < 1e-9
