@@ -32,6 +32,7 @@ SIGNATURES = {
     "anel_mg_ctx_set_density": (C.c_int, [_P, _DP, C.c_int32]),
     "anel_mg_ctx_solve": (C.c_int, [_P, _DP, _DP, C.c_int32, _P, C.POINTER(abi.MGReport)]),
     "anel_mg_ctx_levels": (C.c_int, [_P, _IP, C.c_int32]),
+    "anel_mg_ctx_set_profiling": (C.c_int, [_P, C.c_int32]),
     "anel_mg_ctx_debug_pass": (C.c_int, [_P, C.c_int32, _DP, _DP, _P]),
 }
 

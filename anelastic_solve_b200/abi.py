@@ -53,7 +53,9 @@ class MGParams(C.Structure):
 
 class MGReport(C.Structure):
     _fields_ = [("iter", C.c_int32), ("status", C.c_int32), ("relmax", C.c_double),
-                ("resid", C.c_double), ("ms", C.c_double)]
+                ("resid", C.c_double), ("ms", C.c_double), ("launches", C.c_int64),
+                ("fine_sweeps", C.c_int32), ("reserved", C.c_int32),
+                ("fine_sweep_ms", C.c_double)]
 
 
 def dptr(a: np.ndarray):

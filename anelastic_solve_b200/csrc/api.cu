@@ -125,6 +125,11 @@ int anel_mg_ctx_solve(anel_mg_ctx* ctx, double* phif, const double* rhsf, int32_
                                 : ctx->s->solve_host(phif, rhsf, s, report);
 }
 
+int anel_mg_ctx_set_profiling(anel_mg_ctx* ctx, int32_t on) {
+  if (!ctx) return ANEL_ERR_ARG;
+  return ctx->s->set_profiling(on != 0);
+}
+
 int anel_mg_ctx_levels(const anel_mg_ctx* ctx, int32_t* out, int32_t cap) {
   if (!ctx || !out) return ANEL_ERR_ARG;
   return ctx->s->levels_table(out, cap);

@@ -149,6 +149,7 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
     for (int l = ngrid_ - 1; l >= 1; --l) phibc_[l][f] = 0.0;
   }
   build_metric_hierarchy();
+  build_agglomerated();
   // boundary rules; spacings indexed without the level offset, exactly as
   // mg_bdry.F90:106-181 (dyck(eym) etc.)
   for (int l = 1; l <= ngrid_; ++l) {
@@ -217,6 +218,7 @@ MGSolver::~MGSolver() {
   cudaFree(d_io_phi_);
   cudaFree(d_io_rhs_);
   if (h_pin_) cudaFreeHost(h_pin_);
+  for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -323,6 +325,45 @@ void MGSolver::build_metric_hierarchy() {
   }
 }
 
+// METRIC mode coarse metrics: cell-centred agglomeration (coarse edge q
+// is fine edge 2q-1; widths and centres from the edges; ghosts mirror their
+// interior neighbour).  The reference's mg_grids recursion is not used
+// here because its edges drift on strongly stretched grids.
+void MGSolver::build_agglomerated() {
+  const int ng = ngrid_;
+  for (int d = 0; d < 3; ++d) {
+    ag_[ng][d][0] = fm_[d][0];
+    ag_[ng][d][1] = fm_[d][1];
+    ag_[ng][d][2] = fm_[d][3];
+    ag_[ng][d][3] = fm_[d][2];
+    for (int l = ng - 1; l >= 1; --l) {
+      if (geo_[l].nk[d] == geo_[l + 1].nk[d]) {
+        for (int a = 0; a < 4; ++a) ag_[l][d][a] = ag_[l + 1][d][a];
+        continue;
+      }
+      const int n = geo_[l].nk[d] - 1;
+      std::vector<double> E(n + 2), C(n + 2), DC(n + 2), DE(n + 2);
+      const std::vector<double>& Ef = ag_[l + 1][d][0];
+      for (int q = 1; q <= n + 1; ++q) E[q - 1] = Ef[2 * q - 2];
+      for (int q = 2; q <= n + 1; ++q) {
+        DC[q - 1] = E[q - 1] - E[q - 2];
+        C[q - 1] = 0.5 * (E[q - 1] + E[q - 2]);
+      }
+      DC[0] = DC[1];
+      DC[n + 1] = DC[n];
+      C[0] = E[0] - 0.5 * DC[0];
+      E[n + 1] = E[n] + DC[n + 1];
+      C[n + 1] = E[n] + 0.5 * DC[n + 1];
+      for (int q = 1; q <= n + 1; ++q) DE[q - 1] = C[q] - C[q - 1];
+      DE[n + 1] = DE[n];
+      ag_[l][d][0] = E;
+      ag_[l][d][1] = C;
+      ag_[l][d][2] = DC;
+      ag_[l][d][3] = DE;
+    }
+  }
+}
+
 // ------------------------------------------------------- coefficients
 // rz[k-1] = r(:,:,k) on the fine level, k = 1..nz+2.
 int MGSolver::build_coefficients(const std::vector<double>& rz) {
@@ -386,9 +427,11 @@ int MGSolver::build_coefficients(const std::vector<double>& rz) {
       }
     } else {  // METRIC
       const bool fine = (l == ng);
+      // 1/(dxc(q)*dxe(q-1)) and 1/(dxc(q)*dxe(q)) on the agglomerated level
       auto pcf = [&](int d, bool a, int q) {
-        const int gq = geo_[l].kpx[d] + q - 1;
-        return a ? pA_[d][gq] : pB_[d][gq];
+        const std::vector<double>& DC = ag_[l][d][2];
+        const std::vector<double>& DE = ag_[l][d][3];
+        return a ? 1.0 / (DC[q - 1] * DE[q - 2]) : 1.0 / (DC[q - 1] * DE[q - 1]);
       };
       for (int i = G.s[0]; i <= G.e[0]; ++i) {
         double a1 = fine ? fm_[0][5][i - 1] * fm_[0][4][i - 2] : pcf(0, true, i);
@@ -540,11 +583,14 @@ int MGSolver::coarsen_dirs(int lC) const {
 // no-op after an iteration and is kept only when iters == 0.
 void MGSolver::relax64(int l, int iters, cudaStream_t s) {
   const DevLevel<double> L = L64(l);
+  const bool prof = prof_ && l == ngrid_;
   for (int it = 0; it < iters; ++it) {
-    launch_rb_sweep(L, 0, s);
-    launch_bdry(L, L.phi, s);
-    launch_rb_sweep(L, 1, s);
-    launch_bdry(L, L.phi, s);
+    for (int color = 0; color < 2; ++color) {
+      if (prof) prof_begin(s);
+      launch_rb_sweep(L, color, s);
+      if (prof) prof_end(s);
+      launch_bdry(L, L.phi, s);
+    }
   }
   if (iters == 0) launch_bdry(L, L.phi, s);
 }
@@ -572,11 +618,14 @@ void MGSolver::cycle64(cudaStream_t s) {
 
 void MGSolver::relax32(int l, int iters, cudaStream_t s) {
   const DevLevel<float> L = L32(l, true);
+  const bool prof = prof_ && l == ngrid_;
   for (int it = 0; it < iters; ++it) {
-    launch_rb_sweep(L, 0, s);
-    launch_bdry(L, L.phi, s);
-    launch_rb_sweep(L, 1, s);
-    launch_bdry(L, L.phi, s);
+    for (int color = 0; color < 2; ++color) {
+      if (prof) prof_begin(s);
+      launch_rb_sweep(L, color, s);
+      if (prof) prof_end(s);
+      launch_bdry(L, L.phi, s);
+    }
   }
   if (iters == 0) launch_bdry(L, L.phi, s);
 }
@@ -621,6 +670,8 @@ int MGSolver::solve_device(double* d_phi, const double* d_rhs, cudaStream_t s,
   ANEL_CUDA_TRY(cudaSetDevice(device_));
   if (!s) s = stream_;
   anel_mg_report r{};
+  const int64_t launches0 = g_launches.load();
+  prof_n_ = 0;
   ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
   const int st = prm_.precision == ANEL_PREC_MIXED ? solve_mixed(d_phi, d_rhs, s, &r)
                                                    : solve_fp64(d_phi, d_rhs, s, &r);
@@ -632,6 +683,9 @@ int MGSolver::solve_device(double* d_phi, const double* d_rhs, cudaStream_t s,
   if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
   const int le = check_launch("mg solve");
   if (le != ANEL_OK) return le;
+  r.launches = g_launches.load() - launches0;
+  const int pe = prof_collect(&r);
+  if (pe != ANEL_OK) return pe;
   r.resid = true_resid(d_phi, d_rhs, s, nullptr);
   r.status = st;
   if (rep) *rep = r;
@@ -774,6 +828,40 @@ int MGSolver::debug_pass(int which, double* d_phi, const double* d_src, cudaStre
   }
   ANEL_CUDA_TRY(cudaStreamSynchronize(s));
   return check_launch("debug pass");
+}
+
+int MGSolver::set_profiling(bool on) {
+  prof_ = on;
+  return ANEL_OK;
+}
+
+void MGSolver::prof_begin(cudaStream_t s) {
+  if (prof_ev_.size() < 2 * prof_n_ + 2) {
+    for (int q = 0; q < 64; ++q) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      prof_ev_.push_back(e);
+    }
+  }
+  cudaEventRecord(prof_ev_[2 * prof_n_], s);
+}
+
+void MGSolver::prof_end(cudaStream_t s) {
+  cudaEventRecord(prof_ev_[2 * prof_n_ + 1], s);
+  ++prof_n_;
+}
+
+int MGSolver::prof_collect(anel_mg_report* r) {
+  double ms = 0.0;
+  for (size_t q = 0; q < prof_n_; ++q) {
+    float t = 0.f;
+    ANEL_CUDA_TRY(cudaEventElapsedTime(&t, prof_ev_[2 * q], prof_ev_[2 * q + 1]));
+    ms += t;
+  }
+  r->fine_sweeps = (int32_t)prof_n_;
+  r->fine_sweep_ms = ms;
+  prof_n_ = 0;
+  return ANEL_OK;
 }
 
 int MGSolver::levels_table(int32_t* out, int cap) const {

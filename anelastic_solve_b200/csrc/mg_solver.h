@@ -28,6 +28,7 @@ class MGSolver {
   int solve_host(double* phi, const double* rhs, cudaStream_t s, anel_mg_report* rep);
 
   int debug_pass(int which, double* d_phi, const double* d_src, cudaStream_t s);
+  int set_profiling(bool on);
   int levels_table(int32_t* out, int cap) const;
 
   cudaStream_t stream() const { return stream_; }
@@ -66,6 +67,9 @@ class MGSolver {
   // fine metrics (n+2 each) and the coarse hierarchy (mg_grids.F90)
   std::vector<double> fm_[3][6];          // xe xc dxe dxc rdxe rdxc
   std::vector<double> hE_[3], hC_[3], hDC_[3], hDE_[3], pA_[3], pB_[3];
+  // METRIC mode hierarchy: per level/direction local E, C, DC, DE
+  std::vector<double> ag_[ANEL_MAX_LEVELS + 1][3][4];
+  void build_agglomerated();
   LevelCoef coef_[ANEL_MAX_LEVELS + 1];
   BdryRule rule_[ANEL_MAX_LEVELS + 1];
   BdryRule rule_hom_[ANEL_MAX_LEVELS + 1];  // same with phibc = 0 (error equation)
@@ -84,6 +88,13 @@ class MGSolver {
   double* d_io_rhs_ = nullptr;
   double* h_pin_ = nullptr;               // pinned small readback (4 doubles)
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  // profiling of finest-level smoother launches
+  bool prof_ = false;
+  std::vector<cudaEvent_t> prof_ev_;
+  size_t prof_n_ = 0;  // events used in the current solve (pairs)
+  void prof_begin(cudaStream_t s);
+  void prof_end(cudaStream_t s);
+  int prof_collect(anel_mg_report* r);
   DevLevel<double> L64(int l) const;
   DevLevel<float> L32(int l, bool hom) const;
 };

@@ -83,6 +83,9 @@ class MGSolver:
         self.last_report = rep
         return rep.iter, rep.relmax
 
+    def set_profiling(self, on: bool):
+        check(lib().anel_mg_ctx_set_profiling(self._h, 1 if on else 0))
+
     def levels(self) -> np.ndarray:
         out = (C.c_int32 * (12 * abi.MAX_LEVELS))()
         n = lib().anel_mg_ctx_levels(self._h, out, abi.MAX_LEVELS)

@@ -51,8 +51,10 @@ enum {
 enum { ANEL_SMOOTHER_RBPGS = 0, ANEL_SMOOTHER_LJ = 1 };
 /* LITERAL: the reference's RBPGS operator (uniform spacing xL/nx, zL/nz,
  *          mg_pfpde.F90 / mg_phpde.F90).  METRIC: the same V-cycle with
- *          every level's 7-point operator built from the stretched metric
- *          (mg_grids.F90 + mg_coeff.F90), consistent with Psource/Pgrad. */
+ *          every level's 7-point operator built from the stretched metric:
+ *          the fine level is exactly Psource(Pgrad(p)), coarse levels use
+ *          1/(dzc*dze) products (mg_coeff.F90 form) on a cell-centred
+ *          agglomeration of the grid, with consistent Neumann walls. */
 enum { ANEL_MODE_LITERAL = 0, ANEL_MODE_METRIC = 1 };
 /* FP64: every MG array FP64.  MIXED: FP32 V-cycle inside an FP64 defect-
  *       correction loop (FP64 fine residual, correction and norms). */
@@ -105,6 +107,10 @@ typedef struct {
   double relmax;       /* reference stop metric of the last cycle */
   double resid;        /* ||f - A phi||_2 / ||f||_2 (fine operator) after the solve */
   double ms;           /* device time of the solve (CUDA events) */
+  int64_t launches;    /* kernels of this library launched by the solve */
+  int32_t fine_sweeps; /* finest-level smoother launches timed (profiling on) */
+  int32_t reserved;
+  double fine_sweep_ms;/* their summed device time (CUDA events, profiling on) */
 } anel_mg_report;
 
 typedef struct anel_mg_ctx anel_mg_ctx;
@@ -131,8 +137,9 @@ int anel_mg_set_density(const double* r);
  * argument order, Fortran by-reference, host arrays.  phif: inout, ghosted;
  * its ghosts are set by the final boundary pass.  rhsf: in; the reference
  * uses it as V-cycle scratch (mg_cycle.F90:33,84-85), so its contents on
- * return are unspecified here as well.  iter: cycles used (maxcy when not
- * converged).  relmax: last max|dphi|/max|phi|. */
+ * return are unspecified here as well.  iter: cycles used (maxcy+1 when not
+ * converged, the value the reference's DO loop leaves).  relmax: last
+ * max|dphi|/max|phi|. */
 void anel_mg_solve(double* phif, double* rhsf, int32_t* iter, double* relmax);
 
 /* Replaces mg_end (mg_end.F90:1-42). */
@@ -148,6 +155,10 @@ int anel_mg_ctx_set_density(anel_mg_ctx* ctx, const double* r, int32_t mem);
  * rhsf is read only (unlike the reference, it is not clobbered). */
 int anel_mg_ctx_solve(anel_mg_ctx* ctx, double* phif, const double* rhsf, int32_t mem,
                       void* stream, anel_mg_report* report);
+/* Profiling: when on, every finest-level smoother launch of the following
+ * solves is bracketed by CUDA events on its stream, and the report carries
+ * their count and summed time (fine_sweeps, fine_sweep_ms). */
+int anel_mg_ctx_set_profiling(anel_mg_ctx* ctx, int32_t on);
 /* Level table, for tests of the bit-exact index maps (mg_init.F90:125-220):
  * out[l*12 + 0..11] = nxk nyk nzk sxk exk syk eyk szk ezk kp3d kpx1 kpx2
  * for l = 0..ngrid-1 (level l+1); returns ngrid. */

@@ -43,6 +43,9 @@ struct orc_mg {
   double* dck1[3];        /* dxck */
   double* dek1[3];        /* dxek */
   double* pcf[6];         /* pcf_1..pcf_6 (mg_coeff.F90) */
+  /* METRIC mode hierarchy: per level and direction, local arrays
+   * (index q-1 for the 1-based ghosted q) of E, C, DC, DE */
+  double* ag[ML][3][4];
   int bd[27];
   double phibc[ML][6];
   int tbc[6];
@@ -229,6 +232,44 @@ static void coeff_level(orc_mg* m, int lvl) {
     if (t[3] == 1) m->pcf[5][m->kpx[lvl][2] + m->nk[lvl][2] - 1 - 1] = 0.0;
   }
 }
+/* METRIC mode coarse metrics (a documented deviation): cell-centred
+ * agglomeration.  Coarse edge q is fine edge 2q-1, coarse widths and
+ * centres follow from the edges, ghost cells mirror their interior
+ * neighbour.  Directions not coarsened copy the finer level. */
+static void agglomerate(orc_mg* m) {
+  const int ng = m->ngrid;
+  for (int d = 0; d < 3; ++d) {
+    const int nf = m->nk[ng][d] - 1;
+    for (int a = 0; a < 4; ++a) m->ag[ng][d][a] = (double*)malloc(sizeof(double) * (nf + 2));
+    memcpy(m->ag[ng][d][0], m->fe[d], sizeof(double) * (nf + 2));
+    memcpy(m->ag[ng][d][1], m->fc[d], sizeof(double) * (nf + 2));
+    memcpy(m->ag[ng][d][2], m->fdc[d], sizeof(double) * (nf + 2));
+    memcpy(m->ag[ng][d][3], m->fde[d], sizeof(double) * (nf + 2));
+    for (int l = ng - 1; l >= 1; --l) {
+      const int n = m->nk[l][d] - 1;
+      for (int a = 0; a < 4; ++a) m->ag[l][d][a] = (double*)malloc(sizeof(double) * (n + 2));
+      double *E = m->ag[l][d][0], *C = m->ag[l][d][1], *DC = m->ag[l][d][2], *DE = m->ag[l][d][3];
+      const double* Ef = m->ag[l + 1][d][0];
+      if (m->nk[l][d] == m->nk[l + 1][d]) {
+        for (int a = 0; a < 4; ++a) memcpy(m->ag[l][d][a], m->ag[l + 1][d][a], sizeof(double) * (n + 2));
+        continue;
+      }
+      for (int q = 1; q <= n + 1; ++q) E[q - 1] = Ef[2 * q - 2];
+      for (int q = 2; q <= n + 1; ++q) {
+        DC[q - 1] = E[q - 1] - E[q - 2];
+        C[q - 1] = 0.5 * (E[q - 1] + E[q - 2]);
+      }
+      DC[0] = DC[1];
+      DC[n + 1] = DC[n];
+      C[0] = E[0] - 0.5 * DC[0];
+      E[n + 1] = E[n] + DC[n + 1];
+      C[n + 1] = E[n] + 0.5 * DC[n + 1];
+      for (int q = 1; q <= n + 1; ++q) DE[q - 1] = C[q] - C[q - 1];
+      DE[n + 1] = DE[n];
+    }
+  }
+}
+
 /* pcf_d(i) for local (level) index i */
 static inline double PCF(const orc_mg* m, int which, int lvl, int i) {
   const int d = which / 2;
@@ -329,6 +370,7 @@ orc_mg* orc_mg_create(const anel_grid_desc* g, const anel_mg_params* p, int* sta
   grids_dir(m, 1, m->tbc[2], m->tbc[0]);
   grids_dir(m, 2, m->tbc[1], m->tbc[3]);
   for (int l = 1; l <= ng; ++l) coeff_level(m, l);
+  agglomerate(m);
   /* bdMG (:265-305): serial, the domain touches every face */
   memset(m->bd, 0, sizeof(m->bd));
   m->bd[9] = m->tbc[4];
@@ -373,6 +415,9 @@ void orc_mg_destroy(orc_mg* m) {
     free(m->frde[d]);
     free(m->frdc[d]);
   }
+  for (int l = 1; l <= m->ngrid; ++l)
+    for (int d = 0; d < 3; ++d)
+      for (int a = 0; a < 4; ++a) free(m->ag[l][d][a]);
   free(m->r);
   free(m);
 }
@@ -529,8 +574,11 @@ static void phpde(orc_mg* m, int l) {
 /* METRIC mode (a documented deviation from the reference): every level's
  * operator is the 7-point stencil of the stretched metric.  Fine level:
  * rdxc(i)*rdxe(i-1) etc., i.e. exactly Psource(Pgrad(.)) of
- * NSsolver.F90:2060-2078,2212-2214 with r == 1; coarse levels: pcf_* of
- * mg_coeff on the mg_grids hierarchy.  Neumann faces zero the wall
+ * NSsolver.F90:2060-2078,2212-2214 with r == 1; coarse levels:
+ * 1/(dxc*dxe) products (the form of mg_coeff.F90:77-99) on the
+ * agglomerated hierarchy of agglomerate() -- the reference's mg_grids
+ * recursion drifts on strongly stretched grids and makes the V-cycle
+ * diverge there.  Neumann faces zero the wall
  * coefficient on every level and the diagonal is minus the sum of the six
  * off-diagonals, so the operator is the consistent Neumann operator.
  * The density factors are those of the literal fine formula, evaluated
@@ -559,12 +607,15 @@ static void metric_level(orc_mg* m, int l) {
           a5 = m->frdc[2][k - 1] * m->frde[2][k - 2];
           a6 = m->frdc[2][k - 1] * m->frde[2][k - 1];
         } else {
-          a1 = PCF(m, 0, l, i);
-          a2 = PCF(m, 1, l, i);
-          a3 = PCF(m, 2, l, j);
-          a4 = PCF(m, 3, l, j);
-          a5 = PCF(m, 4, l, k);
-          a6 = PCF(m, 5, l, k);
+          double* const* X_ = m->ag[l][0];
+          double* const* Y_ = m->ag[l][1];
+          double* const* Z_ = m->ag[l][2];
+          a1 = 1.0 / (X_[2][i - 1] * X_[3][i - 2]);
+          a2 = 1.0 / (X_[2][i - 1] * X_[3][i - 1]);
+          a3 = 1.0 / (Y_[2][j - 1] * Y_[3][j - 2]);
+          a4 = 1.0 / (Y_[2][j - 1] * Y_[3][j - 1]);
+          a5 = 1.0 / (Z_[2][k - 1] * Z_[3][k - 2]);
+          a6 = 1.0 / (Z_[2][k - 1] * Z_[3][k - 1]);
         }
         if (m->bd[9] == 1 && i == sxm) a1 = 0.0;
         if (m->bd[18] == 1 && i == exm) a2 = 0.0;
@@ -696,11 +747,17 @@ static void relax_rb(orc_mg* m, int l, double* phi, const double* src, int iters
   const int sym = m->sk[l][1], eym = m->ek[l][1];
   const int szm = m->sk[l][2], ezm = m->ek[l][2];
   for (int it = 1; it <= iters; ++it) {
-    int rb = sxm % 2;
     for (int ipass = 1; ipass <= 2; ++ipass) {
+      /* The reference toggles rb per j and per k starting from mod(sxm,2)
+       * (pass 1) or 1-mod(sxm,2) (pass 2); the start of row (j,k) is
+       * therefore sxm + (rb0 + (j-sym) + (k-szm)) mod 2.  Within a pass
+       * every update reads only the other colour and ghosts, so the rows
+       * are independent and may run in parallel. */
+      const int rb0 = (ipass == 1) ? sxm % 2 : 1 - sxm % 2;
+#pragma omp parallel for schedule(static)
       for (int k = szm; k <= ezm; ++k) {
-        const int rbs = rb;
         for (int j = sym; j <= eym; ++j) {
+          const int rb = (rb0 + (j - sym) + (k - szm)) & 1;
           for (int i = sxm + rb; i <= exm; i += 2) {
             const double pcfsum = AT(c[6], i, j, k);
             AT(phi, i, j, k) =
@@ -710,11 +767,8 @@ static void relax_rb(orc_mg* m, int l, double* phi, const double* src, int iters
                   AT(c[4], i, j, k) * AT(phi, i, j, k - 1) + AT(c[5], i, j, k) * AT(phi, i, j, k + 1))) /
                 pcfsum;
           }
-          rb = 1 - rb;
         }
-        rb = 1 - rbs;
       }
-      rb = 1 - sxm % 2;
       bdry(m, l, phi);
     }
   }
@@ -807,6 +861,7 @@ static void restr(orc_mg* m, int lC, int lF, double* res) {
     LVLDIMS(m, lF);
     const long Gf = lvl_size(m, lF);
     for (long q = 0; q < Gf; ++q) res[q] = 0.0;
+#pragma omp parallel for schedule(static)
     for (int k = m->sk[lF][2]; k <= m->ek[lF][2]; ++k)
       for (int j = m->sk[lF][1]; j <= m->ek[lF][1]; ++j)
         for (int i = m->sk[lF][0]; i <= m->ek[lF][0]; ++i)
@@ -827,6 +882,7 @@ static void restr(orc_mg* m, int lC, int lF, double* res) {
   const int syc = m->sk[lC][1], eyc = m->ek[lC][1];
   const int szc = m->sk[lC][2], ezc = m->ek[lC][2];
   if (nxc < nxf && nyc < nyf && nzc < nzf) {
+#pragma omp parallel for schedule(static)
     for (int kc = szc; kc <= ezc; ++kc) {
       const int k = 2 * kc - 2;
       for (int jc = syc; jc <= eyc; ++jc) {
@@ -905,6 +961,7 @@ static void cor(orc_mg* m, int lC, int lF) {
   const int syf = m->sk[lF][1], eyf = m->ek[lF][1];
   const int szf = m->sk[lF][2], ezf = m->ek[lF][2];
   if (nxc < nxf && nyc < nyf && nzc < nzf) {
+#pragma omp parallel for schedule(static)
     for (int kc = szc - 1; kc <= ezc; ++kc) {
       const int k = 2 * kc - 1;
       for (int jc = syc - 1; jc <= eyc; ++jc) {
@@ -1033,6 +1090,7 @@ static double residual(orc_mg* m, double* phio, const double* phin) {
   const int l = m->ngrid;
   LVLDIMS(m, l);
   double v1 = 0.0, v2 = 0.0;
+#pragma omp parallel for schedule(static) reduction(max : v1, v2)
   for (int k = m->sk[l][2]; k <= m->ek[l][2]; ++k)
     for (int j = m->sk[l][1]; j <= m->ek[l][1]; ++j)
       for (int i = m->sk[l][0]; i <= m->ek[l][0]; ++i) {

@@ -37,7 +37,7 @@ def test_python_signature_table_covers_header():
 def test_struct_layouts_match_header():
     # anel_grid_desc: 3 int32 + pad + 3 double + 18 pointers
     assert C.sizeof(abi.GridDesc) == 4 * 3 + 4 + 8 * 3 + 8 * 18
-    assert C.sizeof(abi.MGReport) == 4 + 4 + 8 + 8 + 8
+    assert C.sizeof(abi.MGReport) == 4 + 4 + 8 + 8 + 8 + 8 + 4 + 4 + 8
     # anel_mg_params: offsets of the first and last fields
     assert abi.MGParams.tolmax.offset == 16
     assert abi.MGParams.verbose.offset == C.sizeof(abi.MGParams) - 4 - 4 or \
