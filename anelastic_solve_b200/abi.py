@@ -20,6 +20,7 @@ ERR_NONFINITE = -9
 
 SMOOTHER_RBPGS = 0
 SMOOTHER_LJ = 1
+SMOOTHER_ZLINE = 2
 MODE_LITERAL = 0
 MODE_METRIC = 1
 PREC_FP64 = 0

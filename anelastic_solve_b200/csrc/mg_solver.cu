@@ -45,12 +45,13 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
     set_error("grid sizes must be positive (got %d %d %d)", nx_, ny_, nz_);
     return ANEL_ERR_SIZE;
   }
-  if (p->smoother != ANEL_SMOOTHER_RBPGS && p->smoother != ANEL_SMOOTHER_LJ) {
+  if (p->smoother != ANEL_SMOOTHER_RBPGS && p->smoother != ANEL_SMOOTHER_LJ &&
+      p->smoother != ANEL_SMOOTHER_ZLINE) {
     set_error("unknown smoother %d", p->smoother);
     return ANEL_ERR_ARG;
   }
-  if (p->smoother == ANEL_SMOOTHER_LJ) {
-    set_error("the z-line (LJ) smoother is not available in this build");
+  if (p->smoother != ANEL_SMOOTHER_RBPGS) {
+    set_error("the z-line smoothers (LJ, ZLINE) are not available in this build");
     return ANEL_ERR_UNSUPPORTED;
   }
   if (p->mode != ANEL_MODE_LITERAL && p->mode != ANEL_MODE_METRIC) {

@@ -48,7 +48,12 @@ enum {
 };
 
 /* ---- enums ------------------------------------------------------------ */
-enum { ANEL_SMOOTHER_RBPGS = 0, ANEL_SMOOTHER_LJ = 1 };
+/* RBPGS: red-black point Gauss-Seidel (mg_relax.F90:85-179, the runfile's
+ *        choice).  LJ: the reference's (i+j) red-black z-line smoother with
+ *        the pcf_* coefficients (mg_relax.F90:423-538).  ZLINE: (i+j)
+ *        red-black z-line Gauss-Seidel with the level's own 7-point
+ *        operator (an extension for stretched z grids). */
+enum { ANEL_SMOOTHER_RBPGS = 0, ANEL_SMOOTHER_LJ = 1, ANEL_SMOOTHER_ZLINE = 2 };
 /* LITERAL: the reference's RBPGS operator (uniform spacing xL/nx, zL/nz,
  *          mg_pfpde.F90 / mg_phpde.F90).  METRIC: the same V-cycle with
  *          every level's 7-point operator built from the stretched metric:

@@ -88,8 +88,9 @@ static int check_size(const orc_mg* m, const int nC[3]) {
     if (nF[d] + 1 != nC[d] * (1 << (m->L[d] - 1)) + 1) return 4 + d;
   }
   if (m->ngrid > 1) {
+    /* the ZLINE extension allows horizontal semi-coarsening (no z levels) */
     for (int d = 0; d < 3; ++d)
-      if (m->L[d] == 1) return 10 + d;
+      if (m->L[d] == 1 && !(d == 2 && m->smoother == ANEL_SMOOTHER_ZLINE)) return 10 + d;
   }
   /* a single level would make mg_cycle restrict into level 0
    * (mg_cycle.F90:226); that is rejected here (code 13, not in the
@@ -837,8 +838,54 @@ static void relax_lz(orc_mg* m, int l, double* phi, const double* src, int iters
   free(rhs);
 }
 
+/* ZLINE smoother (an extension, not in the reference): (i+j) red-black
+ * z-line Gauss-Seidel with the level's own 7-point coefficients (the
+ * operator the residual uses), each line solved by the Thomas algorithm of
+ * mg_relax.F90:541-595; boundary pass after each colour. */
+static void relax_zl(orc_mg* m, int l, double* phi, const double* src, int iters) {
+  LVLDIMS(m, l);
+  double* c[7];
+  for (int q = 0; q < 7; ++q) c[q] = lvl_ptr(m->workc[q], m, l);
+  const int sxm = m->sk[l][0], exm = m->ek[l][0];
+  const int sym = m->sk[l][1], eym = m->ek[l][1];
+  const int szm = m->sk[l][2], ezm = m->ek[l][2];
+  const int n = ezm - szm + 1;
+  for (int it = 1; it <= iters; ++it) {
+    for (int ipass = 1; ipass <= 2; ++ipass) {
+      const int rb0 = (ipass == 1) ? 0 : 1;
+#pragma omp parallel for schedule(static)
+      for (int j = sym; j <= eym; ++j) {
+        double* a = (double*)malloc(sizeof(double) * 4 * n);
+        double* b = a + n;
+        double* cc = b + n;
+        double* rhs = cc + n;
+        const int rb = (rb0 + (j - sym)) & 1;
+        for (int i = sxm + rb; i <= exm; i += 2) {
+          for (int k = szm; k <= ezm; ++k) {
+            const int q = k - szm;
+            a[q] = AT(c[4], i, j, k);
+            b[q] = AT(c[6], i, j, k);
+            cc[q] = AT(c[5], i, j, k);
+            rhs[q] = AT(src, i, j, k) -
+                     (AT(c[0], i, j, k) * AT(phi, i - 1, j, k) + AT(c[1], i, j, k) * AT(phi, i + 1, j, k) +
+                      AT(c[2], i, j, k) * AT(phi, i, j - 1, k) + AT(c[3], i, j, k) * AT(phi, i, j + 1, k));
+          }
+          rhs[0] = rhs[0] - a[0] * AT(phi, i, j, szm - 1);
+          rhs[n - 1] = rhs[n - 1] - cc[n - 1] * AT(phi, i, j, ezm + 1);
+          thomas(a, b, cc, rhs, n);
+          for (int k = szm; k <= ezm; ++k) AT(phi, i, j, k) = rhs[k - szm];
+        }
+        free(a);
+      }
+      bdry(m, l, phi);
+    }
+  }
+  bdry(m, l, phi);
+}
+
 static void relax(orc_mg* m, int l, double* phi, const double* src, int iters) {
   if (m->smoother == ANEL_SMOOTHER_LJ) relax_lz(m, l, phi, src, iters);
+  else if (m->smoother == ANEL_SMOOTHER_ZLINE) relax_zl(m, l, phi, src, iters);
   else relax_rb(m, l, phi, src, iters);
 }
 
