@@ -34,6 +34,22 @@ SIGNATURES = {
     "anel_mg_ctx_levels": (C.c_int, [_P, _IP, C.c_int32]),
     "anel_mg_ctx_set_profiling": (C.c_int, [_P, C.c_int32]),
     "anel_mg_ctx_debug_pass": (C.c_int, [_P, C.c_int32, _DP, _DP, _P]),
+    "anel_ns_create": (_P, [C.POINTER(abi.GridDesc), C.POINTER(abi.MGParams),
+                            C.POINTER(abi.NSParams), C.c_int32, _IP]),
+    "anel_ns_destroy": (None, [_P]),
+    "anel_ns_set_fields": (C.c_int, [_P, C.POINTER(abi.Fields), C.c_int32]),
+    "anel_ns_get_fields": (C.c_int, [_P, C.POINTER(abi.Fields), C.c_int32]),
+    "anel_ns_ctx_substep": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, _P, _IP, _DP]),
+    "anel_ns_ctx_step": (C.c_int, [_P, C.c_int32, _P, C.POINTER(abi.StepReport)]),
+    "anel_ns_ctx_set_clock": (C.c_int, [_P, C.c_double, C.c_int32]),
+    "anel_ns_ctx_project": (C.c_int, [_P, _IP, _DP]),
+    "anel_ns_ctx_divergence": (C.c_int, [_P, _DP]),
+    "anel_ns_init": (C.c_int, [C.POINTER(abi.GridDesc), C.POINTER(abi.MGParams),
+                               C.POINTER(abi.NSParams)]),
+    "anel_bind_fields": (C.c_int, [C.POINTER(abi.Fields)]),
+    "anel_rk_substep": (None, [_DP, _DP, _DP, _DP, _DP, _DP, _IP, _IP]),
+    "anel_ns_finalize": (C.c_int, []),
 }
 
 

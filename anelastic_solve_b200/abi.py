@@ -106,3 +106,79 @@ def make_mg_params(levels, maxcy=99, tolmax=1e-10, pre=None, post=None, tbc=(0, 
         p.vbc[f] = float(vbc[f])
     p.mode, p.precision, p.stop, p.verbose = int(mode), int(precision), int(stop), int(verbose)
     return p
+
+
+# ------------------------------------------------------------------ stepper
+MODEL_DNS = 0
+MODEL_SSM = 1
+DELTA_3ROOT = 0
+DELTA_2ROOT = 1
+DAMP_LITERAL = 0
+DAMP_NONE = 1
+
+# boundC variable index (1-based in the reference) -> name
+BC_VARS = ("U1", "U2", "U3", "P", "RHO", "FLUC", "TEMP", "SCAL1")
+
+
+class NSParams(C.Structure):
+    _fields_ = [("Re", C.c_double), ("Pr", C.c_double), ("Sc", C.c_double),
+                ("cfl", C.c_double), ("dtmax", C.c_double),
+                ("g_init", C.c_double), ("g_final", C.c_double), ("gt1", C.c_double),
+                ("gt2", C.c_double), ("vmodel", C.c_int32), ("rmodel", C.c_int32),
+                ("smodel", C.c_int32), ("les_delta", C.c_int32), ("les_damp", C.c_int32),
+                ("ssm_const", C.c_double), ("pr_sgs", C.c_double), ("les_start", C.c_int32),
+                ("les_freq", C.c_int32), ("tb", ((C.c_int32 * 8) * 2) * 3),
+                ("vb", ((C.c_double * 8) * 2) * 3), ("ew", C.c_int32), ("scal1_on", C.c_int32)]
+
+
+class Fields(C.Structure):
+    _fields_ = [(n, _DP) for n in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG",
+                                   "q_u", "q_v", "q_w", "q_rho", "q_s", "psrc",
+                                   "nuT", "kappaT", "nappaT")]
+
+
+FIELD_NAMES = [n for n, _ in Fields._fields_]
+
+
+class StepReport(C.Structure):
+    _fields_ = [("nstep", C.c_int32), ("mg_iter", C.c_int32 * 3), ("dt", C.c_double),
+                ("time", C.c_double), ("mg_relmax", C.c_double * 3), ("max_div", C.c_double),
+                ("avg_div", C.c_double), ("ms", C.c_double)]
+
+
+def free_slip_bcs(p: NSParams, rho_value=(0.0, 0.0)):
+    """x, y periodic; z walls free-slip: U1, U2 Neumann 0, U3 Dirichlet 0,
+    P Neumann 0, RHO Neumann (values), FLUC Neumann 0, SCAL1 Neumann 0,
+    temporaries Dirichlet 0 (BC.F90:741-742)."""
+    for d in range(2):
+        for f in range(2):
+            for v in range(8):
+                p.tb[d][f][v] = 3
+                p.vb[d][f][v] = -1.0
+    ztypes = {0: 2, 1: 2, 2: 1, 3: 2, 4: 2, 5: 2, 6: 1, 7: 2}
+    for f in range(2):
+        for v in range(8):
+            p.tb[2][f][v] = ztypes[v]
+            p.vb[2][f][v] = 0.0
+        p.vb[2][f][4] = float(rho_value[f])
+    return p
+
+
+def make_ns_params(Re=1000.0, Pr=1.0, Sc=1.0, cfl=1e6, dtmax=0.01, g=-0.12, les=False,
+                   ssm_const=0.0289, pr_sgs=0.7, les_start=0, les_freq=1,
+                   les_damp=DAMP_NONE, les_delta=DELTA_3ROOT, ew=1, scal1_on=1) -> NSParams:
+    """Shear-layer parameters: gravity constant g from t = 0 (Ginit = Gfinal
+    = g, GT1 = GT2 = 0), free-slip z walls, periodic x and y."""
+    p = NSParams()
+    p.Re, p.Pr, p.Sc = float(Re), float(Pr), float(Sc)
+    p.cfl, p.dtmax = float(cfl), float(dtmax)
+    p.g_init = p.g_final = float(g)
+    p.gt1 = p.gt2 = 0.0
+    m = MODEL_SSM if les else MODEL_DNS
+    p.vmodel = p.rmodel = p.smodel = m
+    p.les_delta, p.les_damp = int(les_delta), int(les_damp)
+    p.ssm_const, p.pr_sgs = float(ssm_const), float(pr_sgs)
+    p.les_start, p.les_freq = int(les_start), int(les_freq)
+    p.ew = int(ew)
+    p.scal1_on = int(scal1_on)
+    return free_slip_bcs(p)

@@ -28,6 +28,8 @@ SOURCES = {
     "mg_solver.cu": ["-fmad=false"],
     "mg_kernels64.cu": ["-fmad=false"],
     "mg_kernels32.cu": ["-fmad=true"],
+    "ns_kernels.cu": ["-fmad=false"],
+    "ns_solver.cu": ["-fmad=false"],
 }
 
 

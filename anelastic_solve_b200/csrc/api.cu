@@ -4,6 +4,7 @@
 #include <mutex>
 
 #include "mg_solver.h"
+#include "ns_solver.h"
 
 namespace anel {
 
@@ -32,10 +33,16 @@ int check_launch(const char* what) {
 struct anel_mg_ctx {
   anel::MGSolver* s;
 };
+struct anel_ns_ctx {
+  anel::NSSolver* s;
+};
 
 namespace {
 std::mutex g_default_mu;
 anel::MGSolver* g_default = nullptr;  // the drop-in calls' module state
+anel::NSSolver* g_ns = nullptr;       // drop-in stepper
+anel_fields g_bound{};                // bound host module arrays
+bool g_bound_ok = false;
 }  // namespace
 
 extern "C" {
@@ -139,6 +146,121 @@ int anel_mg_ctx_debug_pass(anel_mg_ctx* ctx, int32_t which, double* d_phi, const
                            void* stream) {
   if (!ctx) return ANEL_ERR_ARG;
   return ctx->s->debug_pass(which, d_phi, d_src, static_cast<cudaStream_t>(stream));
+}
+
+// ------------------------------------------------------------ stepper
+anel_ns_ctx* anel_ns_create(const anel_grid_desc* grid, const anel_mg_params* mg,
+                            const anel_ns_params* ns, int32_t device, int32_t* status) {
+  int st = ANEL_OK;
+  anel::NSSolver* s = anel::NSSolver::create(grid, mg, ns, device, &st);
+  if (status) *status = st;
+  if (!s) return nullptr;
+  return new anel_ns_ctx{s};
+}
+
+void anel_ns_destroy(anel_ns_ctx* ctx) {
+  if (!ctx) return;
+  delete ctx->s;
+  delete ctx;
+}
+
+int anel_ns_set_fields(anel_ns_ctx* ctx, const anel_fields* f, int32_t mem) {
+  if (!ctx) return ANEL_ERR_ARG;
+  return ctx->s->set_fields(f, mem, nullptr);
+}
+
+int anel_ns_get_fields(anel_ns_ctx* ctx, const anel_fields* f, int32_t mem) {
+  if (!ctx) return ANEL_ERR_ARG;
+  return ctx->s->get_fields(f, mem, nullptr);
+}
+
+int anel_ns_ctx_substep(anel_ns_ctx* ctx, double a1, double a2, double a3, double dt_rk, double dt,
+                        void* stream, int32_t* mg_iter, double* mg_relmax) {
+  if (!ctx) return ANEL_ERR_ARG;
+  int it = 0;
+  double rm = 0.0;
+  const int st = ctx->s->substep(a1, a2, a3, dt_rk, dt, static_cast<cudaStream_t>(stream), &it, &rm);
+  if (mg_iter) *mg_iter = it;
+  if (mg_relmax) *mg_relmax = rm;
+  return st;
+}
+
+int anel_ns_ctx_step(anel_ns_ctx* ctx, int32_t nsteps, void* stream, anel_step_report* report) {
+  if (!ctx || nsteps < 0) return ANEL_ERR_ARG;
+  return ctx->s->step(nsteps, static_cast<cudaStream_t>(stream), report);
+}
+
+int anel_ns_ctx_set_clock(anel_ns_ctx* ctx, double time, int32_t nstep) {
+  if (!ctx) return ANEL_ERR_ARG;
+  ctx->s->set_clock(time, nstep);
+  return ANEL_OK;
+}
+
+int anel_ns_ctx_divergence(anel_ns_ctx* ctx, double* out) {
+  if (!ctx || !out) return ANEL_ERR_ARG;
+  return ctx->s->divergence(nullptr, out);
+}
+
+int anel_ns_ctx_project(anel_ns_ctx* ctx, int32_t* mg_iter, double* mg_relmax) {
+  if (!ctx) return ANEL_ERR_ARG;
+  int it = 0;
+  double rm = 0.0;
+  const int st = ctx->s->project(nullptr, &it, &rm);
+  if (mg_iter) *mg_iter = it;
+  if (mg_relmax) *mg_relmax = rm;
+  return st;
+}
+
+// drop-in stepper
+int anel_ns_init(const anel_grid_desc* grid, const anel_mg_params* mg, const anel_ns_params* ns) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  delete g_ns;
+  g_ns = nullptr;
+  int st = ANEL_OK;
+  g_ns = anel::NSSolver::create(grid, mg, ns, 0, &st);
+  return st;
+}
+
+int anel_bind_fields(const anel_fields* f) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (!f) return ANEL_ERR_ARG;
+  g_bound = *f;
+  g_bound_ok = true;
+  // r and densityBG are copied once here (they change only with the setup)
+  if (g_ns && (f->r || f->densityBG)) {
+    anel_fields d{};
+    d.r = f->r;
+    d.densityBG = f->densityBG;
+    return g_ns->set_fields(&d, ANEL_MEM_HOST, nullptr);
+  }
+  return ANEL_OK;
+}
+
+void anel_rk_substep(const double* a1, const double* a2, const double* a3, const double* ec,
+                     const double* dt_rk, const double* dt, const int32_t* psolve, int32_t* stat) {
+  (void)ec;
+  (void)psolve;  // rk_ss always solves for the pressure (NSsolver.F90:520-523)
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (!g_ns || !g_bound_ok || !a1 || !a2 || !a3 || !dt_rk || !dt) {
+    anel::set_error("anel_rk_substep before anel_ns_init/anel_bind_fields or null argument");
+    if (stat) *stat = ANEL_ERR_ARG;
+    return;
+  }
+  anel_fields io = g_bound;
+  io.r = nullptr;
+  io.densityBG = nullptr;
+  int st = g_ns->set_fields(&io, ANEL_MEM_HOST, nullptr);
+  if (st == ANEL_OK) st = g_ns->substep(*a1, *a2, *a3, *dt_rk, *dt, nullptr, nullptr, nullptr);
+  if (st == ANEL_OK) st = g_ns->get_fields(&io, ANEL_MEM_HOST, nullptr);
+  if (stat) *stat = st;
+}
+
+int anel_ns_finalize(void) {
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  delete g_ns;
+  g_ns = nullptr;
+  g_bound_ok = false;
+  return ANEL_OK;
 }
 
 }  // extern "C"

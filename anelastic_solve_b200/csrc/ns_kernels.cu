@@ -1,0 +1,583 @@
+// ns_kernels.cu -- sm_100a kernels of the RK3 sub-step.  Compiled with
+// -fmad=false: every sum/product is rounded as the reference's Fortran
+// expressions evaluated left to right (citations per kernel).
+#include "ns_launch.h"
+
+namespace anel {
+
+static constexpr double R12 = 1.0 / 2.0;  // ratios::r_1_2 (modules.F90:203)
+
+// --------------------------------------------------------------- RHS
+// u1_rhs (NSsolver.F90:646-804): returns Utemp(i,j,k) before ghosting.
+__device__ __forceinline__ double rhs_u(const NSDev& D, int i, int j, int k) {
+  const double* un = D.u;
+  const double* vn = D.v;
+  const double* wn = D.w;
+  const double rRe = D.rRe;
+  const double rk = D.rz[k - 1];
+  double acc = 0.0;
+  acc = acc +
+        rRe * ((FA(un, i + 1, j, k) - FA(un, i, j, k)) * MT(D.rdxc, i + 1) -
+               (FA(un, i, j, k) - FA(un, i - 1, j, k)) * MT(D.rdxc, i)) *
+            MT(D.rdxe, i);
+  acc = acc +
+        rRe * ((FA(un, i, j + 1, k) - FA(un, i, j, k)) * MT(D.rdye, j) -
+               (FA(un, i, j, k) - FA(un, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+            MT(D.rdyc, j);
+  double ua2 = R12 * (FA(un, i + 1, j, k) + FA(un, i, j, k));
+  double ua1 = R12 * (FA(un, i, j, k) + FA(un, i - 1, j, k));
+  acc = acc + (ua1 * ua1 - ua2 * ua2) * MT(D.rdxe, i);
+  ua2 = R12 * (FA(un, i, j, k + 1) + FA(un, i, j, k));
+  ua1 = R12 * (FA(un, i, j, k) + FA(un, i, j, k - 1));
+  const double ra2 = R12 * (D.rz[k] + rk);
+  const double ra1 = R12 * (rk + D.rz[k - 2]);
+  const double wa2 = R12 * (FA(wn, i + 1, j, k) + FA(wn, i, j, k));
+  const double wa1 = R12 * (FA(wn, i + 1, j, k - 1) + FA(wn, i, j, k - 1));
+  acc = acc + (ra1 * ua1 * wa1 - ra2 * ua2 * wa2) * MT(D.rdzc, k) / rk;
+  ua2 = R12 * (FA(un, i, j + 1, k) + FA(un, i, j, k));
+  ua1 = R12 * (FA(un, i, j, k) + FA(un, i, j - 1, k));
+  const double va2 = R12 * (FA(vn, i + 1, j, k) + FA(vn, i, j, k));
+  const double va1 = R12 * (FA(vn, i + 1, j - 1, k) + FA(vn, i, j - 1, k));
+  acc = acc + (ua1 * va1 - ua2 * va2) * MT(D.rdyc, j);
+  if (D.vles) {  // NSsolver.F90:761-804
+    const double* nuT = D.nuT;
+    acc = acc - 2.0 *
+                    (FA(nuT, i + 1, j, k) * (FA(un, i + 1, j, k) - FA(un, i, j, k)) * MT(D.rdxc, i + 1) -
+                     FA(nuT, i, j, k) * (FA(un, i, j, k) - FA(un, i - 1, j, k)) * MT(D.rdxc, i)) *
+                    MT(D.rdxe, i);
+    double n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j - 1, k) +
+                        FA(nuT, i + 1, j - 1, k));
+    double n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j + 1, k) +
+                        FA(nuT, i + 1, j + 1, k));
+    acc = acc - 1.0 *
+                    (n2 * (FA(un, i, j + 1, k) - FA(un, i, j, k)) * MT(D.rdye, j) -
+                     n1 * (FA(un, i, j, k) - FA(un, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+                    MT(D.rdyc, j);
+    acc = acc - 1.0 *
+                    (n2 * (FA(vn, i + 1, j + 1, k) - FA(vn, i, j + 1, k)) * MT(D.rdxe, i) -
+                     n1 * (FA(vn, i + 1, j, k) - FA(vn, i, j, k)) * MT(D.rdxe, i)) *
+                    MT(D.rdyc, j);
+    n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j, k - 1) + FA(nuT, i + 1, j, k - 1));
+    n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j, k + 1) + FA(nuT, i + 1, j, k + 1));
+    acc = acc - 1.0 *
+                    (ra2 * n2 * (FA(wn, i + 1, j, k) - FA(wn, i, j, k)) * MT(D.rdxe, i) -
+                     ra1 * n1 * (FA(wn, i + 1, j, k - 1) - FA(wn, i, j, k - 1)) * MT(D.rdxe, i)) *
+                    MT(D.rdzc, k) / rk;
+  }
+  return acc;
+}
+
+// u2_rhs (NSsolver.F90:912-1081)
+__device__ __forceinline__ double rhs_v(const NSDev& D, int i, int j, int k) {
+  const double* un = D.u;
+  const double* vn = D.v;
+  const double* wn = D.w;
+  const double rRe = D.rRe;
+  const double rk = D.rz[k - 1];
+  double acc = 0.0;
+  acc = acc +
+        rRe * ((FA(vn, i + 1, j, k) - FA(vn, i, j, k)) * MT(D.rdxe, i) -
+               (FA(vn, i, j, k) - FA(vn, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+            MT(D.rdxc, i);
+  acc = acc +
+        rRe * ((FA(vn, i, j + 1, k) - FA(vn, i, j, k)) * MT(D.rdyc, j + 1) -
+               (FA(vn, i, j, k) - FA(vn, i, j - 1, k)) * MT(D.rdyc, j)) *
+            MT(D.rdye, j);
+  double va1 = 0.5 * (FA(vn, i, j + 1, k) + FA(vn, i, j, k));
+  double va2 = 0.5 * (FA(vn, i, j, k) + FA(vn, i, j - 1, k));
+  acc = acc - (va1 * va1 - va2 * va2) * MT(D.rdye, j);
+  va1 = 0.5 * (FA(vn, i + 1, j, k) + FA(vn, i, j, k));
+  va2 = 0.5 * (FA(vn, i, j, k) + FA(vn, i - 1, j, k));
+  const double ua1 = 0.5 * (FA(un, i, j + 1, k) + FA(un, i, j, k));
+  const double ua2 = 0.5 * (FA(un, i - 1, j + 1, k) + FA(un, i - 1, j, k));
+  acc = acc - (ua1 * va1 - ua2 * va2) * MT(D.rdxc, i);
+  va1 = 0.5 * (FA(vn, i, j, k + 1) + FA(vn, i, j, k));
+  va2 = 0.5 * (FA(vn, i, j, k) + FA(vn, i, j, k - 1));
+  const double ra1 = 0.5 * (D.rz[k] + rk);
+  const double ra2 = 0.5 * (rk + D.rz[k - 2]);
+  const double wa1 = 0.5 * (FA(wn, i, j + 1, k) + FA(wn, i, j, k));
+  const double wa2 = 0.5 * (FA(wn, i, j + 1, k - 1) + FA(wn, i, j, k - 1));
+  acc = acc - (ra1 * wa1 * va1 - ra2 * wa2 * va2) * MT(D.rdzc, k) / rk;
+  if (D.vles) {  // NSsolver.F90:1038-1081
+    const double* nuT = D.nuT;
+    double n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i - 1, j, k) + FA(nuT, i, j + 1, k) +
+                        FA(nuT, i - 1, j + 1, k));
+    double n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j + 1, k) +
+                        FA(nuT, i + 1, j + 1, k));
+    acc = acc - 1.0 *
+                    (n2 * (FA(vn, i + 1, j, k) - FA(vn, i, j, k)) * MT(D.rdxe, i) -
+                     n1 * (FA(vn, i, j, k) - FA(vn, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+                    MT(D.rdxc, i);
+    acc = acc - 1.0 *
+                    (n2 * (FA(un, i + 1, j + 1, k) - FA(un, i + 1, j, k)) * MT(D.rdye, j) -
+                     n1 * (FA(un, i, j + 1, k) - FA(un, i, j, k)) * MT(D.rdye, j)) *
+                    MT(D.rdxc, i);
+    acc = acc - 2.0 *
+                    (FA(nuT, i, j + 1, k) * (FA(vn, i, j + 1, k) - FA(vn, i, j, k)) * MT(D.rdyc, j + 1) -
+                     FA(nuT, i, j, k) * (FA(vn, i, j, k) - FA(vn, i, j - 1, k)) * MT(D.rdyc, j)) *
+                    MT(D.rdye, j);
+    n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i, j + 1, k) + FA(nuT, i, j, k - 1) + FA(nuT, i, j + 1, k - 1));
+    n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i, j + 1, k) + FA(nuT, i, j, k + 1) + FA(nuT, i, j + 1, k + 1));
+    // the reference pairs raver2 (lower face) with nuTaver2 (upper face)
+    acc = acc - 1.0 *
+                    (ra2 * n2 * (FA(wn, i, j + 1, k) - FA(wn, i, j, k)) * MT(D.rdye, j) -
+                     ra1 * n1 * (FA(wn, i, j + 1, k - 1) - FA(wn, i, j, k - 1)) * MT(D.rdye, j)) *
+                    MT(D.rdzc, k) / rk;
+  }
+  return acc;
+}
+
+// u3_rhs (NSsolver.F90:1195-1377); rows above nz+1-EW carry no terms.
+__device__ __forceinline__ double rhs_w(const NSDev& D, int i, int j, int k) {
+  if (k > D.nz + 1 - D.ew) return 0.0;
+  const double* un = D.u;
+  const double* vn = D.v;
+  const double* wn = D.w;
+  const double rRe = D.rRe;
+  const double rk = D.rz[k - 1], rkp = D.rz[k];
+  double acc = 0.0;
+  acc = acc + R12 * D.g * ((FA(D.rho, i, j, k + 1) - D.bgz[k]) + (FA(D.rho, i, j, k) - D.bgz[k - 1])) /
+                  (R12 * (D.bgz[k] + D.bgz[k - 1]));
+  acc = acc +
+        rRe * ((FA(wn, i + 1, j, k) - FA(wn, i, j, k)) * MT(D.rdxe, i) -
+               (FA(wn, i, j, k) - FA(wn, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+            MT(D.rdxc, i);
+  acc = acc +
+        rRe * ((FA(wn, i, j + 1, k) - FA(wn, i, j, k)) * MT(D.rdye, j) -
+               (FA(wn, i, j, k) - FA(wn, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+            MT(D.rdyc, j);
+  double wa1 = 0.5 * (FA(wn, i, j, k + 1) + FA(wn, i, j, k));
+  double wa2 = 0.5 * (FA(wn, i, j, k) + FA(wn, i, j, k - 1));
+  acc = acc - (rk * wa1 * wa1 - rkp * wa2 * wa2) * MT(D.rdze, k) / (0.5 * (rk + rkp));
+  wa1 = 0.5 * (FA(wn, i + 1, j, k) + FA(wn, i, j, k));
+  wa2 = 0.5 * (FA(wn, i, j, k) + FA(wn, i - 1, j, k));
+  const double ua1 = 0.5 * (FA(un, i, j, k + 1) + FA(un, i, j, k));
+  const double ua2 = 0.5 * (FA(un, i - 1, j, k + 1) + FA(un, i - 1, j, k));
+  acc = acc - (ua1 * wa1 - ua2 * wa2) * MT(D.rdxc, i);
+  wa1 = 0.5 * (FA(wn, i, j + 1, k) + FA(wn, i, j, k));
+  wa2 = 0.5 * (FA(wn, i, j, k) + FA(wn, i, j - 1, k));
+  const double va1 = 0.5 * (FA(vn, i, j, k + 1) + FA(vn, i, j, k));
+  const double va2 = 0.5 * (FA(vn, i, j - 1, k + 1) + FA(vn, i, j - 1, k));
+  acc = acc - (va1 * wa1 - va2 * wa2) * MT(D.rdyc, j);
+  if (D.vles) {  // NSsolver.F90:1339-1377
+    const double* nuT = D.nuT;
+    double n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i - 1, j, k) + FA(nuT, i, j, k + 1) +
+                        FA(nuT, i - 1, j, k + 1));
+    double n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j, k + 1) +
+                        FA(nuT, i + 1, j, k + 1));
+    acc = acc - 1.0 *
+                    (n2 * (FA(wn, i + 1, j, k) - FA(wn, i, j, k)) * MT(D.rdxe, i) -
+                     n1 * (FA(wn, i, j, k) - FA(wn, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+                    MT(D.rdxc, i);
+    acc = acc - 1.0 *
+                    (n2 * (FA(un, i + 1, j, k + 1) - FA(un, i + 1, j, k)) * MT(D.rdze, k) -
+                     n1 * (FA(un, i, j, k + 1) - FA(un, i, j, k)) * MT(D.rdze, k)) *
+                    MT(D.rdxc, i);
+    n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i, j - 1, k) + FA(nuT, i, j, k + 1) + FA(nuT, i, j - 1, k + 1));
+    n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i, j + 1, k) + FA(nuT, i, j, k + 1) + FA(nuT, i, j + 1, k + 1));
+    acc = acc - 1.0 *
+                    (n2 * (FA(wn, i, j + 1, k) - FA(wn, i, j, k)) * MT(D.rdye, j) -
+                     n1 * (FA(wn, i, j, k) - FA(wn, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+                    MT(D.rdyc, j);
+    acc = acc - 1.0 *
+                    (n2 * (FA(vn, i, j + 1, k + 1) - FA(vn, i, j + 1, k)) * MT(D.rdze, k) -
+                     n1 * (FA(vn, i, j, k + 1) - FA(vn, i, j, k)) * MT(D.rdze, k)) *
+                    MT(D.rdyc, j);
+  }
+  return acc;
+}
+
+// rho_rhs (NSsolver.F90:1720-1815) and scal1_rhs (:1890-1985)
+template <bool kRho>
+__device__ __forceinline__ double rhs_scalar(const NSDev& D, int i, int j, int k) {
+  const double* un = D.u;
+  const double* vn = D.v;
+  const double* wn = D.w;
+  const double* c = kRho ? D.rho : D.s;
+  const double Dk = kRho ? D.rRe * D.rPr : D.rRe * D.rSc;
+  double acc = 0.0;
+  acc = acc +
+        Dk * ((FA(c, i + 1, j, k) - FA(c, i, j, k)) * MT(D.rdxe, i) -
+              (FA(c, i, j, k) - FA(c, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+            MT(D.rdxc, i);
+  acc = acc +
+        Dk * ((FA(c, i, j + 1, k) - FA(c, i, j, k)) * MT(D.rdye, j) -
+              (FA(c, i, j, k) - FA(c, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+            MT(D.rdyc, j);
+  double c2 = 0.5 * (FA(c, i + 1, j, k) + FA(c, i, j, k));
+  double c1 = 0.5 * (FA(c, i, j, k) + FA(c, i - 1, j, k));
+  acc = acc + (FA(un, i - 1, j, k) * c1 - FA(un, i, j, k) * c2) * MT(D.rdxc, i);
+  c2 = 0.5 * (FA(c, i, j + 1, k) + FA(c, i, j, k));
+  c1 = 0.5 * (FA(c, i, j, k) + FA(c, i, j - 1, k));
+  acc = acc + (FA(vn, i, j - 1, k) * c1 - FA(vn, i, j, k) * c2) * MT(D.rdyc, j);
+  c2 = 0.5 * (FA(c, i, j, k + 1) + FA(c, i, j, k));
+  c1 = 0.5 * (FA(c, i, j, k) + FA(c, i, j, k - 1));
+  if (kRho) {
+    const double rk = D.rz[k - 1];
+    const double ra2 = 0.5 * (D.rz[k] + rk);
+    const double ra1 = 0.5 * (rk + D.rz[k - 2]);
+    acc = acc + (ra1 * FA(wn, i, j, k - 1) * c1 - ra2 * FA(wn, i, j, k) * c2) * MT(D.rdzc, k) / rk;
+  } else {
+    acc = acc + (FA(wn, i, j, k - 1) * c1 - FA(wn, i, j, k) * c2) * MT(D.rdzc, k);
+  }
+  if (kRho ? D.rles : D.sles) {
+    const double* kT = kRho ? D.kT : D.nT;
+    double k2 = 0.5 * (FA(kT, i + 1, j, k) + FA(kT, i, j, k));
+    // scal1_rhs keeps the reference's sign slip in the lower average
+    double k1 = kRho ? 0.5 * (FA(kT, i, j, k) + FA(kT, i - 1, j, k))
+                     : 0.5 * (FA(kT, i, j, k) - FA(kT, i - 1, j, k));
+    acc = acc - 1.0 *
+                    (k2 * (FA(c, i + 1, j, k) - FA(c, i, j, k)) * MT(D.rdxe, i) -
+                     k1 * (FA(c, i, j, k) - FA(c, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+                    MT(D.rdxc, i);
+    k2 = 0.5 * (FA(kT, i, j + 1, k) + FA(kT, i, j, k));
+    k1 = kRho ? 0.5 * (FA(kT, i, j, k) + FA(kT, i, j - 1, k))
+              : 0.5 * (FA(kT, i, j, k) - FA(kT, i, j - 1, k));
+    acc = acc - 1.0 *
+                    (k2 * (FA(c, i, j + 1, k) - FA(c, i, j, k)) * MT(D.rdye, j) -
+                     k1 * (FA(c, i, j, k) - FA(c, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+                    MT(D.rdyc, j);
+  }
+  return acc;
+}
+
+// K1: all right-hand sides and the low-storage accumulation
+// q = a1*q + a2*F*dt (var_advance, NSsolver.F90:2225-2264) in one pass.
+// first = substep with a1 = 0 after zero_temps: q is known to be zero,
+// so it is not read (0*0 + x == 0 + x).
+template <bool kFirst>
+__global__ void k_rhs_accum(NSDev D, double a1, double a2, double dt) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > D.nx + 1) return;
+  const int64_t c = NS_IX(i, j, k);
+  const double fu = rhs_u(D, i, j, k);
+  const double fv = rhs_v(D, i, j, k);
+  const double fw = rhs_w(D, i, j, k);
+  const double fr = rhs_scalar<true>(D, i, j, k);
+  const double q0u = kFirst ? 0.0 : D.qu[c];
+  const double q0v = kFirst ? 0.0 : D.qv[c];
+  const double q0w = kFirst ? 0.0 : D.qw[c];
+  const double q0r = kFirst ? 0.0 : D.qr[c];
+  D.qu[c] = a1 * q0u + a2 * fu * dt;
+  D.qv[c] = a1 * q0v + a2 * fv * dt;
+  D.qw[c] = a1 * q0w + a2 * fw * dt;
+  D.qr[c] = a1 * q0r + a2 * fr * dt;
+  if (D.scal1_on) {
+    const double fs = rhs_scalar<false>(D, i, j, k);
+    const double q0s = kFirst ? 0.0 : D.qs[c];
+    D.qs[c] = a1 * q0s + a2 * fs * dt;
+  }
+}
+
+// ---------------------------------------------------------- ghosting
+// bound_update of the two z faces of one column (BC.F90:471-529) after
+// the periodic wrap; col(k) = a[base + (k-1)*XY].
+__device__ __forceinline__ void zghost_column(const NSDev& D, const ZRule& R, double* a, int64_t base) {
+  const int sz = 2, ez = D.nz + 1, iW = R.iw;
+  const int64_t XY = D.XY;
+#define COL(k) a[base + (int64_t)((k) - 1) * XY]
+  auto dzt = [&](int k) { return R.dzt_is_zc ? D.dzc[k - 1] : D.dze[k - 1]; };
+  // the serial ghost() first wraps z periodically (BC.F90:64-66)
+  COL(sz - 1) = COL(ez);
+  COL(ez + 1) = COL(sz);
+  for (int face = 1; face <= 2; ++face) {
+    const int bt = R.type[face - 1];
+    if (R.type[0] == 3 && face == 2) break;  // periodic: bound_update called once
+    const double value = R.val[face - 1];
+    if (bt == 1) {
+      if (face == 1) COL(sz - 1) = value;
+      else COL(ez + 1 - iW) = value;
+    } else if (bt == 2) {
+      if (face == 1) {
+        if (R.rt == 1) COL(sz) = COL(sz + 1) - value * dzt(sz + 1 + R.of1);
+        COL(sz - 1) = COL(sz) - value * dzt(sz + R.of1);
+      } else {
+        if (R.rt == 1) COL(ez - iW) = COL(ez - 1 - iW) + value * dzt(ez - 1 + R.of2 - iW);
+        COL(ez + 1 - iW) = COL(ez - iW) + value * dzt(ez + R.of2 - iW);
+      }
+    } else if (bt == 3) {
+      COL(sz - 1) = COL(ez - iW);
+      COL(ez + 1 - iW) = COL(sz);
+    } else if (bt == 4) {
+      if (face == 1) COL(sz - 1) = COL(sz) - value * dzt(sz + R.of1);
+      else COL(ez + 1 - iW) = COL(ez - iW) + value * dzt(ez + R.of2 - iW);
+    } else if (bt == 6) {
+      if (face == 1) COL(sz - 1) = 2.0 * value - 1.0 * COL(sz);
+      else COL(ez + 1 - iW) = 2.0 * value - 1.0 * COL(ez - iW);
+    } else if (bt == 7) {
+      if (face == 1) {
+        COL(sz) = 0.0;
+        COL(sz - 1) = -1.0 * COL(sz + 1);
+      } else {
+        COL(ez) = 0.0;
+        COL(ez + 1 - iW) = -1.0 * COL(ez - iW - 1);
+      }
+    }
+    if (face == 2 && iW == 1) COL(ez + 1) = 0.0;
+  }
+#undef COL
+}
+
+// Copy the finished column (i,j) into its periodic images in x and y
+// (the ghost columns, BC.F90:55-63 with TB = 3 in x and y).
+__device__ __forceinline__ void copy_images(const NSDev& D, double* a, int i, int j) {
+  int is[2], js[2];
+  int ni = 1, nj = 1;
+  is[0] = i;
+  js[0] = j;
+  if (i == 2) is[ni++] = D.nx + 2;
+  else if (i == D.nx + 1) is[ni++] = 1;
+  if (i == 2 && i == D.nx + 1) is[ni++] = 1;  // nx == 1
+  if (j == 2) js[nj++] = D.ny + 2;
+  else if (j == D.ny + 1) js[nj++] = 1;
+  if (j == 2 && j == D.ny + 1) js[nj++] = 1;
+  if (ni == 1 && nj == 1) return;
+  const int64_t src = NS_IX(i, j, 1);
+  for (int a_ = 0; a_ < ni; ++a_)
+    for (int b_ = 0; b_ < nj; ++b_) {
+      if (a_ == 0 && b_ == 0) continue;
+      const int64_t dst = NS_IX(is[a_], js[b_], 1);
+      for (int k = 1; k <= D.Z; ++k) a[dst + (int64_t)(k - 1) * D.XY] = a[src + (int64_t)(k - 1) * D.XY];
+    }
+}
+
+// Generic ghost pass of one field: one thread per interior column.
+__global__ void k_ghost_field(NSDev D, double* a, ZRule R) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  if (i > D.nx + 1) return;
+  zghost_column(D, R, a, NS_IX(i, j, 1));
+  copy_images(D, a, i, j);
+}
+
+// ------------------------------------------------------- CN (z implicit)
+// var_advance_CN_PL (NSsolver.F90:3054-3465) for one interior column with
+// column-independent tridiagonal factors (DNS; r = r(z)).  fac holds, per
+// row k = 1..n (n = nz+2): ap (eliminated sub-diagonal), bp (eliminated
+// diagonal), c (super-diagonal), t1, t2 (explicit-term weights), rb
+// (right-hand side of a wall row) and isbc (1 for wall rows).
+struct CNFac {
+  const double *ap, *bp, *c, *t1, *t2, *rb, *isbc;
+};
+
+template <int kVar>
+__global__ void k_cn_column(NSDev D, double* __restrict__ fld, const double* __restrict__ q,
+                            CNFac F, double a3, double rkdt, ZRule R) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  if (i > D.nx + 1) return;
+  const int n = D.nz + 2;
+  const int64_t base = NS_IX(i, j, 1);
+  const int64_t XY = D.XY;
+  // forward sweep: G(k) = rhs(k) + ap(k) G(k-1); G is stored in place
+  double um = fld[base];            // u_old(k-1)
+  double uk = fld[base + XY];       // u_old(k)
+  double g = F.rb[0];               // row 1 is a wall row
+  fld[base] = g;
+  for (int k = 2; k <= n; ++k) {
+    const int64_t o = base + (int64_t)(k - 1) * XY;
+    const double up = (k < n) ? fld[o + XY] : 0.0;  // u_old(k+1)
+    double rhs;
+    if (F.isbc[k - 1] != 0.0) {
+      rhs = F.rb[k - 1];
+    } else {
+      rhs = 1.0 * uk + a3 * q[o] * 1.0;
+      if (kVar != 3)
+        rhs = rhs + rkdt * 0.5 *
+                        (F.t2[k - 1] * (up - uk) * MT(D.rdze, k) -
+                         F.t1[k - 1] * (uk - um) * MT(D.rdze, k - 1)) *
+                        MT(D.rdzc, k);
+      else
+        rhs = rhs + rkdt * 0.5 *
+                        (F.t2[k - 1] * (up - uk) * MT(D.rdzc, k + 1) -
+                         F.t1[k - 1] * (uk - um) * MT(D.rdzc, k)) *
+                        MT(D.rdze, k);
+    }
+    g = rhs + F.ap[k - 1] * g;
+    fld[o] = g;
+    um = uk;
+    uk = up;
+  }
+  // back substitution: G(n) = G(n)/bp(n); G(k) = (G(k) - c(k) G(k+1))/bp(k)
+  double gn = fld[base + (int64_t)(n - 1) * XY] / F.bp[n - 1];
+  fld[base + (int64_t)(n - 1) * XY] = gn;
+  for (int k = n - 1; k >= 1; --k) {
+    const int64_t o = base + (int64_t)(k - 1) * XY;
+    gn = (fld[o] - F.c[k - 1] * gn) / F.bp[k - 1];
+    fld[o] = gn;
+  }
+  zghost_column(D, R, fld, base);
+  copy_images(D, fld, i, j);
+}
+
+// ------------------------------------------------------------ Psource
+// NSsolver.F90:2167-2223 (its ghost pass is not needed: the multigrid
+// reads the interior of the right-hand side only).
+__global__ void k_psource(NSDev D, double rdt) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > D.nx + 1) return;
+  const double rk = D.rz[k - 1];
+  const double H = 0.5;
+  const double v = ((rk * FA(D.u, i, j, k) - rk * FA(D.u, i - 1, j, k)) * MT(D.rdxc, i) +
+                    (rk * FA(D.v, i, j, k) - rk * FA(D.v, i, j - 1, k)) * MT(D.rdyc, j) +
+                    (H * (D.rz[k] + rk) * FA(D.w, i, j, k) - H * (rk + D.rz[k - 2]) * FA(D.w, i, j, k - 1)) *
+                        MT(D.rdzc, k)) *
+                   rdt;
+  FA(D.psrc, i, j, k) = 0.0 + v;
+}
+
+// ------------------------------------------------------ Pgrad + ghosts
+// Pgrad (NSsolver.F90:2023-2085) on one column, then ghost(u,'u'),
+// ghost(v,'v'), ghost(w,'w') (NSsolver.F90:572-574).
+__global__ void k_pgrad_column(NSDev D, double dt, ZRule Ru, ZRule Rv, ZRule Rw) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  if (i > D.nx + 1) return;
+  const int kend_w = D.nz + 1 - D.ew;
+  for (int k = 2; k <= D.nz + 1; ++k) {
+    const double rk = D.rz[k - 1];
+    const double pk = FA(D.p, i, j, k);
+    FA(D.u, i, j, k) = FA(D.u, i, j, k) - (FA(D.p, i + 1, j, k) / rk - pk / rk) * MT(D.rdxe, i) * dt;
+    FA(D.v, i, j, k) = FA(D.v, i, j, k) - (FA(D.p, i, j + 1, k) / rk - pk / rk) * MT(D.rdye, j) * dt;
+    if (k <= kend_w)
+      FA(D.w, i, j, k) =
+          FA(D.w, i, j, k) - (FA(D.p, i, j, k + 1) / D.rz[k] - pk / rk) * MT(D.rdze, k) * dt;
+  }
+  const int64_t base = NS_IX(i, j, 1);
+  zghost_column(D, Ru, D.u, base);
+  zghost_column(D, Rv, D.v, base);
+  zghost_column(D, Rw, D.w, base);
+  copy_images(D, D.u, i, j);
+  copy_images(D, D.v, i, j);
+  copy_images(D, D.w, i, j);
+}
+
+// -------------------------------------------------------------- calcdt
+// Routines.F90:221-233: max over the interior of the advective CFL rate
+// (order x, z, y as in the reference), exact integer max of the bits.
+__global__ void k_cfl_max(NSDev D, unsigned long long* out) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
+  unsigned long long m = 0;
+  if (i <= D.nx + 1) {
+    const double adv = MT(D.rdxc, i) * fabs(0.5 * (FA(D.u, i, j, k) + FA(D.u, i - 1, j, k))) +
+                       MT(D.rdzc, k) * fabs(0.5 * (FA(D.w, i, j, k) + FA(D.w, i, j, k - 1))) +
+                       MT(D.rdyc, j) * fabs(0.5 * (FA(D.v, i, j, k) + FA(D.v, i, j - 1, k)));
+    m = __double_as_longlong(adv);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long w = __shfl_xor_sync(0xffffffffu, m, o);
+    m = w > m ? w : m;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// divergence (Routines.F90:121-146): max |div| (exact) and the
+// volume-weighted sums of |div| and volume (block partials, fixed order)
+__global__ void k_divergence(NSDev D, unsigned long long* mx, double* part) {
+  __shared__ double sh[2][8];
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
+  double s1 = 0.0, s2 = 0.0;
+  unsigned long long m = 0;
+  if (i <= D.nx + 1) {
+    const double d = (FA(D.u, i, j, k) - FA(D.u, i - 1, j, k)) * MT(D.rdxc, i) +
+                     (FA(D.v, i, j, k) - FA(D.v, i, j - 1, k)) * MT(D.rdyc, j) +
+                     (FA(D.w, i, j, k) - FA(D.w, i, j, k - 1)) * MT(D.rdzc, k);
+    const double vol = 1.0 / (MT(D.rdxc, i) * MT(D.rdyc, j) * MT(D.rdzc, k));
+    s1 = fabs(d) * vol;
+    s2 = vol;
+    m = __double_as_longlong(fabs(d));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    const unsigned long long w = __shfl_xor_sync(0xffffffffu, m, o);
+    m = w > m ? w : m;
+  }
+  const int wid = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][wid] = s1;
+    sh[1][wid] = s2;
+    atomicMax(mx, m);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+      a += sh[0][q];
+      b += sh[1][q];
+    }
+    const int64_t bid = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
+    part[2 * bid] = a;
+    part[2 * bid + 1] = b;
+  }
+}
+
+// ------------------------------------------------------------ launchers
+static dim3 cell_grid(const NSDev& D, int tx) {
+  return dim3((unsigned)((D.nx + tx - 1) / tx), (unsigned)D.ny, (unsigned)D.nz);
+}
+static dim3 col_grid(const NSDev& D, int tx) {
+  return dim3((unsigned)((D.nx + tx - 1) / tx), (unsigned)D.ny, 1u);
+}
+
+void launch_rhs_accum(const NSDev& D, double a1, double a2, double dt, bool first, cudaStream_t s) {
+  const int tx = 128;
+  if (first) k_rhs_accum<true><<<cell_grid(D, tx), tx, 0, s>>>(D, a1, a2, dt);
+  else k_rhs_accum<false><<<cell_grid(D, tx), tx, 0, s>>>(D, a1, a2, dt);
+  count_launch();
+}
+
+void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
+               double rkdt, const ZRule& R, cudaStream_t s) {
+  const int tx = 64;
+  CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc};
+  if (var == 3) k_cn_column<3><<<col_grid(D, tx), tx, 0, s>>>(D, fld, q, f, a3, rkdt, R);
+  else k_cn_column<1><<<col_grid(D, tx), tx, 0, s>>>(D, fld, q, f, a3, rkdt, R);
+  count_launch();
+}
+
+void launch_psource(const NSDev& D, double dt, cudaStream_t s) {
+  const int tx = 128;
+  k_psource<<<cell_grid(D, tx), tx, 0, s>>>(D, 1.0 / dt);
+  count_launch();
+}
+
+void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, const ZRule& Rw,
+                  cudaStream_t s) {
+  const int tx = 64;
+  k_pgrad_column<<<col_grid(D, tx), tx, 0, s>>>(D, dt, Ru, Rv, Rw);
+  count_launch();
+}
+
+void launch_ghost_field(const NSDev& D, double* a, const ZRule& R, cudaStream_t s) {
+  const int tx = 64;
+  k_ghost_field<<<col_grid(D, tx), tx, 0, s>>>(D, a, R);
+  count_launch();
+}
+
+void launch_cfl_max(const NSDev& D, unsigned long long* out, cudaStream_t s) {
+  const int tx = 128;
+  k_cfl_max<<<cell_grid(D, tx), tx, 0, s>>>(D, out);
+  count_launch();
+}
+
+int64_t divergence_blocks(const NSDev& D) {
+  const int tx = 128;
+  return (int64_t)((D.nx + tx - 1) / tx) * D.ny * D.nz;
+}
+
+void launch_divergence(const NSDev& D, unsigned long long* mx, double* part, cudaStream_t s) {
+  const int tx = 128;
+  k_divergence<<<cell_grid(D, tx), tx, 0, s>>>(D, mx, part);
+  count_launch();
+}
+
+}  // namespace anel

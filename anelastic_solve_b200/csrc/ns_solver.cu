@@ -1,0 +1,499 @@
+// ns_solver.cu -- host side of the B200 RK3 time stepper: field storage,
+// boundary rules, the column-independent Crank-Nicolson factors and the
+// sub-step / step schedule of rk_ss and NSsolver (NSsolver.F90:63-583).
+// Host code is compiled with -ffp-contract=off so the factors round as
+// the reference's expressions.
+#include "ns_solver.h"
+
+#include <cmath>
+#include <cstring>
+
+namespace anel {
+
+static const int kVarCode[5] = {1, 2, 3, 5, 8};  // u v w rho scal1 (boundC index)
+
+NSSolver* NSSolver::create(const anel_grid_desc* g, const anel_mg_params* mg,
+                           const anel_ns_params* ns, int device, int* status) {
+  NSSolver* s = new NSSolver();
+  const int st = s->init(g, mg, ns, device);
+  if (status) *status = st;
+  if (st != ANEL_OK) {
+    delete s;
+    return nullptr;
+  }
+  return s;
+}
+
+NSSolver::~NSSolver() {
+  cudaSetDevice(device_);
+  delete mg_;
+  for (double* p : d_fields_) cudaFree(p);
+  cudaFree(d_metric_);
+  cudaFree(d_prof_);
+  cudaFree(d_cn_);
+  cudaFree(d_red_);
+  cudaFree(d_part_);
+  if (h_cn_) cudaFreeHost(h_cn_);
+  if (h_red_) cudaFreeHost(h_red_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const anel_ns_params* ns,
+                   int device) {
+  if (!g || !mgp || !ns) {
+    set_error("null grid, mg or ns parameters");
+    return ANEL_ERR_ARG;
+  }
+  prm_ = *ns;
+  device_ = device;
+  nx_ = g->nx;
+  ny_ = g->ny;
+  nz_ = g->nz;
+  // this implementation: x and y periodic for every field
+  for (int d = 0; d < 2; ++d)
+    for (int f = 0; f < 2; ++f)
+      for (int v = 0; v < 8; ++v)
+        if (ns->tb[d][f][v] != 3) {
+          set_error("the GPU stepper needs x and y periodic for every field (TB(%d,%d,%d)=%d)", d + 1,
+                    f + 1, v + 1, ns->tb[d][f][v]);
+          return ANEL_ERR_UNSUPPORTED;
+        }
+  // z wall types the CN rows of var_advance_CN_PL accept (NSsolver.F90:3297-3429)
+  for (int vi = 0; vi < 5; ++vi) {
+    const int v = kVarCode[vi] - 1;
+    const int t0 = ns->tb[2][0][v], t1 = ns->tb[2][1][v];
+    if (!(t0 == 1 || t0 == 2 || t0 == 6) || !(t1 == 1 || t1 == 2 || t1 == 6 || t1 == 7)) {
+      set_error("z boundary types %d/%d of variable %d have no Crank-Nicolson row in the reference",
+                t0, t1, v + 1);
+      return ANEL_ERR_BC;
+    }
+  }
+  if (ns->vmodel != ANEL_MODEL_DNS || ns->rmodel != ANEL_MODEL_DNS || ns->smodel != ANEL_MODEL_DNS) {
+    set_error("the LES (SSM) stepper is not available in this build");
+    return ANEL_ERR_UNSUPPORTED;
+  }
+  if (ns->ew != 0 && ns->ew != 1) {
+    set_error("ew must be 0 or 1");
+    return ANEL_ERR_ARG;
+  }
+  const int n[3] = {nx_, ny_, nz_};
+  const double* src[3][6] = {{g->xe, g->xc, g->dxe, g->dxc, g->rdxe, g->rdxc},
+                             {g->ye, g->yc, g->dye, g->dyc, g->rdye, g->rdyc},
+                             {g->ze, g->zc, g->dze, g->dzc, g->rdze, g->rdzc}};
+  for (int d = 0; d < 3; ++d)
+    for (int a = 0; a < 6; ++a) m_[d][a].assign(src[d][a], src[d][a] + n[d] + 2);
+  rRe_ = 1.0 / ns->Re;
+  rPr_ = 1.0 / ns->Pr;
+  rSc_ = 1.0 / ns->Sc;
+  g_orig_ = ns->g_final;
+  gnow_ = ns->g_init;
+  int st = ANEL_OK;
+  mg_ = MGSolver::create(g, mgp, device, &st);
+  if (!mg_) return st;
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  ANEL_CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  ANEL_CUDA_TRY(cudaEventCreate(&ev0_));
+  ANEL_CUDA_TRY(cudaEventCreate(&ev1_));
+  const int X = nx_ + 2, Y = ny_ + 2, Z = nz_ + 2;
+  G_ = (int64_t)X * Y * Z;
+  for (int q = 0; q < 14; ++q) {
+    if (q == 6 || q == 7) continue;  // r, densityBG: allocated below
+    ANEL_CUDA_TRY(cudaMalloc(&d_fields_[q], G_ * sizeof(double)));
+    ANEL_CUDA_TRY(cudaMemset(d_fields_[q], 0, G_ * sizeof(double)));
+  }
+  // metrics
+  std::vector<double> met;
+  for (int a : {4, 5}) met.insert(met.end(), m_[0][a].begin(), m_[0][a].end());
+  for (int a : {4, 5}) met.insert(met.end(), m_[1][a].begin(), m_[1][a].end());
+  for (int a : {4, 5}) met.insert(met.end(), m_[2][a].begin(), m_[2][a].end());
+  met.insert(met.end(), m_[2][2].begin(), m_[2][2].end());  // dze
+  met.insert(met.end(), m_[2][3].begin(), m_[2][3].end());  // dzc
+  ANEL_CUDA_TRY(cudaMalloc(&d_metric_, met.size() * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMemcpy(d_metric_, met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice));
+  ANEL_CUDA_TRY(cudaMalloc(&d_prof_, 2 * (size_t)Z * sizeof(double)));
+  const size_t ncn = 3 * 5 * 7 * (size_t)Z;
+  ANEL_CUDA_TRY(cudaMalloc(&d_cn_, ncn * sizeof(double)));
+  ANEL_CUDA_TRY(cudaHostAlloc(&h_cn_, ncn * sizeof(double), cudaHostAllocDefault));
+  ANEL_CUDA_TRY(cudaMalloc(&d_red_, 4 * sizeof(unsigned long long)));
+  ANEL_CUDA_TRY(cudaHostAlloc(&h_red_, 4 * sizeof(double), cudaHostAllocDefault));
+  // device view
+  D_.nx = nx_;
+  D_.ny = ny_;
+  D_.nz = nz_;
+  D_.X = X;
+  D_.Y = Y;
+  D_.Z = Z;
+  D_.XY = (int64_t)X * Y;
+  D_.G = G_;
+  const double* mp = d_metric_;
+  D_.rdxe = mp;
+  D_.rdxc = mp + X;
+  D_.rdye = mp + 2 * X;
+  D_.rdyc = mp + 2 * X + Y;
+  D_.rdze = mp + 2 * X + 2 * Y;
+  D_.rdzc = mp + 2 * X + 2 * Y + Z;
+  D_.dze = mp + 2 * X + 2 * Y + 2 * Z;
+  D_.dzc = mp + 2 * X + 2 * Y + 3 * Z;
+  D_.rz = d_prof_;
+  D_.bgz = d_prof_ + Z;
+  D_.u = d_fields_[0];
+  D_.v = d_fields_[1];
+  D_.w = d_fields_[2];
+  D_.p = d_fields_[3];
+  D_.rho = d_fields_[4];
+  D_.s = d_fields_[5];
+  D_.qu = d_fields_[8];
+  D_.qv = d_fields_[9];
+  D_.qw = d_fields_[10];
+  D_.qr = d_fields_[11];
+  D_.qs = d_fields_[12];
+  D_.psrc = d_fields_[13];
+  D_.rRe = rRe_;
+  D_.rPr = rPr_;
+  D_.rSc = rSc_;
+  D_.g = gnow_;
+  D_.vles = D_.rles = D_.sles = 0;
+  D_.ew = ns->ew;
+  D_.scal1_on = ns->scal1_on;
+  // r = densityBG = 1 until set
+  rz_.assign(Z, 1.0);
+  bgz_.assign(Z, 1.0);
+  // full r / densityBG arrays kept for get_fields
+  for (int q : {6, 7}) {
+    ANEL_CUDA_TRY(cudaMalloc(&d_fields_[q], G_ * sizeof(double)));
+    std::vector<double> one(G_, 1.0);
+    ANEL_CUDA_TRY(cudaMemcpy(d_fields_[q], one.data(), G_ * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  return upload_profiles();
+}
+
+int NSSolver::upload_profiles() {
+  std::vector<double> pr(rz_);
+  pr.insert(pr.end(), bgz_.begin(), bgz_.end());
+  ANEL_CUDA_TRY(cudaMemcpy(d_prof_, pr.data(), pr.size() * sizeof(double), cudaMemcpyHostToDevice));
+  for (double& v : cn_rkdt_) v = -1.0;  // factors depend on r
+  return ANEL_OK;
+}
+
+// vtype -> z rule (ghost/bound_update, BC.F90:67-95 and 334-420)
+ZRule NSSolver::zrule(int vt) const {
+  ZRule R{};
+  int l = 7, stag = 0;
+  switch (vt) {
+    case NV_U: l = 1; stag = 1; break;
+    case NV_V: l = 2; stag = 2; break;
+    case NV_W: l = 3; stag = 3; break;
+    case NV_P: l = 4; break;
+    case NV_RHO: l = 5; R.rt = 1; break;
+    case NV_CFLUC: l = 6; break;
+    case NV_SCAL1: l = 8; R.rt = 1; break;
+    case NV_SCAL1TEMP: l = 8; break;
+    default: l = 7; stag = (vt == NV_UTEMP) ? 1 : (vt == NV_VTEMP) ? 2 : (vt == NV_WTEMP) ? 3 : 0;
+  }
+  for (int f = 0; f < 2; ++f) {
+    R.type[f] = prm_.tb[2][f][l - 1];
+    R.val[f] = prm_.vb[2][f][l - 1];
+  }
+  if (stag == 0) {
+    R.of1 = -1;
+    R.of2 = 0;
+    R.dzt_is_zc = 0;
+  } else {
+    R.of1 = 0;
+    R.of2 = 1;
+    R.dzt_is_zc = (stag == 3) ? 1 : 0;
+  }
+  R.iw = (stag == 3) ? prm_.ew : 0;
+  return R;
+}
+
+// Column-independent factors of the CN system of each variable for one
+// rkdt (var_advance_CN_PL, NSsolver.F90:3102-3296), then the elimination
+// of the Thomas routine (mg_relax.F90:563-568) applied to them.
+int NSSolver::cn_factors(int slot, double rkdt, cudaStream_t s) {
+  if (cn_rkdt_[slot] == rkdt) return ANEL_OK;
+  // the pinned staging slot may still feed an earlier asynchronous copy
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  const int Z = nz_ + 2, n = Z, sz = 2, ez = nz_ + 1;
+  const double H = 0.5;
+  auto R = [&](int k) { return rz_[k - 1]; };
+  auto rdze = [&](int k) { return m_[2][4][k - 1]; };
+  auto rdzc = [&](int k) { return m_[2][5][k - 1]; };
+  auto dze = [&](int k) { return m_[2][2][k - 1]; };
+  auto dzc = [&](int k) { return m_[2][3][k - 1]; };
+  for (int vi = 0; vi < 5; ++vi) {
+    const int var = kVarCode[vi];
+    double* base = h_cn_ + ((size_t)(slot * 5 + vi) * 7) * Z;
+    double *ap = base, *bp = base + Z, *c = base + 2 * Z, *t1a = base + 3 * Z, *t2a = base + 4 * Z,
+           *rb = base + 5 * Z, *isbc = base + 6 * Z;
+    std::vector<double> sub(n, 0.0), diag(n, 0.0), sup(n, 0.0);
+    for (int q = 0; q < n; ++q) {
+      t1a[q] = t2a[q] = rb[q] = isbc[q] = 0.0;
+    }
+    for (int k = sz; k <= ez; ++k) {
+      double t1, t2;
+      if (var != 3) {
+        const double ra1 = H * (R(k + 1) + R(k));
+        const double ra2 = H * (R(k) + R(k - 1));
+        if (var == 1 || var == 2) {
+          t1 = (rRe_ + 0.0) * ra1 / R(k);
+          t2 = (rRe_ + 0.0) * ra2 / R(k);
+        } else if (var == 5) {
+          t1 = (rRe_ * rPr_ + 0.0) * ra1 / R(k);
+          t2 = (rRe_ * rPr_ + 0.0) * ra2 / R(k);
+        } else {
+          t1 = rRe_ * rSc_ + 0.0;
+          t2 = rRe_ * rSc_ + 0.0;
+        }
+        sub[k - 1] = -0.5 * rkdt * t1 * rdze(k - 1) * rdzc(k);
+        sup[k - 1] = -0.5 * rkdt * t2 * rdze(k) * rdzc(k);
+        diag[k - 1] = 1.0 + 0.5 * rkdt * (t1 * rdze(k - 1) + t2 * rdze(k)) * rdzc(k);
+      } else {
+        t1 = (rRe_ + 0.0) * R(k) / (H * (R(k + 1) + R(k)));
+        t2 = (rRe_ + 0.0) * R(k + 1) / (H * (R(k + 1) + R(k)));
+        sub[k - 1] = -0.5 * rkdt * t1 * rdze(k) * rdzc(k);
+        sup[k - 1] = -0.5 * rkdt * t2 * rdze(k) * rdzc(k + 1);
+        diag[k - 1] = 1.0 + 0.5 * rkdt * (t1 * rdzc(k) + t2 * rdzc(k + 1)) * rdze(k);
+      }
+      t1a[k - 1] = t1;
+      t2a[k - 1] = t2;
+    }
+    // wall rows (NSsolver.F90:3297-3429)
+    const int tbmin = prm_.tb[2][0][var - 1], tbmax = prm_.tb[2][1][var - 1];
+    const double vbmin = prm_.vb[2][0][var - 1], vbmax = prm_.vb[2][1][var - 1];
+    auto set = [&](int k, double a, double b, double cc, double d) {
+      sub[k - 1] = a;
+      diag[k - 1] = b;
+      sup[k - 1] = cc;
+      rb[k - 1] = d;
+      isbc[k - 1] = 1.0;
+    };
+    if (tbmin == 1) set(sz - 1, 0.0, 1.0, 0.0, vbmin);
+    else if (tbmin == 2) {
+      if (var == 3) set(sz - 1, 0.0, -1.0, 1.0, dzc(sz - 1) * vbmin);
+      else if (var == 5 || var == 8) {
+        set(sz - 1, 0.0, -1.0, 1.0, dze(sz - 1) * vbmin);
+        set(sz, 0.0, -1.0, 1.0, dze(sz) * vbmin);
+      } else set(sz - 1, 0.0, -1.0, 1.0, dze(sz - 1) * vbmin);
+    } else if (tbmin == 6) set(sz - 1, 0.0, 1.0, 1.0, 2.0 * vbmin);
+    if (tbmax == 1) set(ez + 1, 0.0, 1.0, 0.0, vbmax);
+    else if (tbmax == 2) {
+      if (var == 3) set(ez + 1, -1.0, 1.0, 0.0, dzc(ez + 1) * vbmax);
+      else if (var == 5 || var == 8) {
+        set(ez + 1, -1.0, 1.0, 0.0, dze(ez + 1) * vbmax);
+        set(ez, -1.0, 1.0, 0.0, dze(ez) * vbmax);
+      } else set(ez + 1, -1.0, 1.0, 0.0, dze(ez + 1) * vbmax);
+    } else if (tbmax == 6) set(ez + 1, 1.0, 1.0, 0.0, 2.0 * vbmax);
+    else if (tbmax == 7) {
+      set(ez + 1, 0.0, 1.0, 0.0, 0.0);
+      set(ez, 0.0, 1.0, 0.0, 0.0);
+    }
+    // elimination (a, b overwritten, c untouched)
+    std::vector<double> a(sub), b(diag);
+    for (int j = 1; j <= n - 1; ++j) {
+      a[j] = -a[j] / b[j - 1];
+      b[j] = b[j] + a[j] * sup[j - 1];
+    }
+    for (int q = 0; q < n; ++q) {
+      ap[q] = (q == 0) ? 0.0 : a[q];
+      bp[q] = b[q];
+      c[q] = sup[q];
+    }
+  }
+  double* dst = d_cn_ + (size_t)slot * 5 * 7 * Z;
+  ANEL_CUDA_TRY(cudaMemcpyAsync(dst, h_cn_ + (size_t)slot * 5 * 7 * Z, 5 * 7 * (size_t)Z * sizeof(double),
+                                cudaMemcpyHostToDevice, s));
+  cn_rkdt_[slot] = rkdt;
+  return ANEL_OK;
+}
+
+CNFacHost NSSolver::fac(int slot, int vi) const {
+  const int Z = nz_ + 2;
+  const double* base = d_cn_ + ((size_t)(slot * 5 + vi) * 7) * Z;
+  return CNFacHost{base, base + Z, base + 2 * Z, base + 3 * Z, base + 4 * Z, base + 5 * Z, base + 6 * Z};
+}
+
+// --------------------------------------------------------------- fields
+int NSSolver::set_fields(const anel_fields* f, int mem, cudaStream_t s) {
+  if (!f) return ANEL_ERR_ARG;
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  double* const* src = reinterpret_cast<double* const*>(f);
+  const cudaMemcpyKind kind = mem == ANEL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  bool density = false;
+  for (int q = 0; q < 14; ++q) {
+    if (!src[q]) continue;
+    ANEL_CUDA_TRY(cudaMemcpyAsync(d_fields_[q], src[q], G_ * sizeof(double), kind, s));
+    if (q == 6 || q == 7) density = true;
+  }
+  if (density) {
+    // profiles of r and densityBG: both must be functions of z only
+    std::vector<double> h(G_);
+    const int64_t XY = (int64_t)(nx_ + 2) * (ny_ + 2);
+    for (int q : {6, 7}) {
+      if (!src[q]) continue;
+      ANEL_CUDA_TRY(cudaMemcpyAsync(h.data(), d_fields_[q], G_ * sizeof(double), cudaMemcpyDeviceToHost, s));
+      ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+      std::vector<double>& prof = (q == 6) ? rz_ : bgz_;
+      for (int k = 0; k < nz_ + 2; ++k) {
+        const double v = h[(int64_t)k * XY];
+        for (int64_t o = 1; o < XY; ++o)
+          if (!(h[(int64_t)k * XY + o] == v)) {
+            set_error("%s must be horizontally uniform (a function of z); plane k=%d differs",
+                      q == 6 ? "r" : "densityBG", k + 1);
+            return ANEL_ERR_UNSUPPORTED;
+          }
+        prof[k] = v;
+      }
+      if (q == 6) {
+        const int st = mg_->set_density_host(h.data());
+        if (st != ANEL_OK) return st;
+      }
+    }
+    const int st = upload_profiles();
+    if (st != ANEL_OK) return st;
+  }
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  return ANEL_OK;
+}
+
+int NSSolver::get_fields(const anel_fields* f, int mem, cudaStream_t s) {
+  if (!f) return ANEL_ERR_ARG;
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  double* const* dst = reinterpret_cast<double* const*>(f);
+  const cudaMemcpyKind kind = mem == ANEL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  for (int q = 0; q < 14; ++q)
+    if (dst[q]) ANEL_CUDA_TRY(cudaMemcpyAsync(dst[q], d_fields_[q], G_ * sizeof(double), kind, s));
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  return ANEL_OK;
+}
+
+// --------------------------------------------------------------- rk_ss
+int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, cudaStream_t s,
+                      int* iters, double* relmax, bool q_zero) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  // slot of the factor cache (three rkdt values per step)
+  int slot = -1;
+  for (int q = 0; q < 3; ++q)
+    if (cn_rkdt_[q] == dt_rk) slot = q;
+  if (slot < 0) {
+    slot = cn_next_;
+    cn_next_ = (cn_next_ + 1) % 3;
+    const int st = cn_factors(slot, dt_rk, s);
+    if (st != ANEL_OK) return st;
+  }
+  D_.g = gnow_;
+  launch_rhs_accum(D_, a1, a2, dt, q_zero && a1 == 0.0, s);
+  const ZRule ru = zrule(NV_U), rv = zrule(NV_V), rw = zrule(NV_W);
+  launch_cn(D_, 1, D_.u, D_.qu, fac(slot, 0), a3, dt_rk, ru, s);
+  launch_cn(D_, 2, D_.v, D_.qv, fac(slot, 1), a3, dt_rk, rv, s);
+  launch_cn(D_, 3, D_.w, D_.qw, fac(slot, 2), a3, dt_rk, rw, s);
+  launch_psource(D_, dt_rk, s);
+  launch_cn(D_, 5, D_.rho, D_.qr, fac(slot, 3), a3, dt_rk, zrule(NV_RHO), s);
+  if (prm_.scal1_on) launch_cn(D_, 8, D_.s, D_.qs, fac(slot, 4), a3, dt_rk, zrule(NV_SCAL1), s);
+  anel_mg_report rep{};
+  const int st = mg_->solve_device(D_.p, D_.psrc, s, &rep);
+  if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
+  launch_pgrad(D_, dt_rk, ru, rv, rw, s);
+  if (iters) *iters = rep.iter;
+  if (relmax) *relmax = rep.relmax;
+  return check_launch("rk substep");
+}
+
+double NSSolver::calcdt(cudaStream_t s, int* st) {
+  cudaMemsetAsync(d_red_, 0, sizeof(unsigned long long), s);
+  launch_cfl_max(D_, d_red_, s);
+  cudaMemcpyAsync(h_red_, d_red_, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    *st = ANEL_ERR_CUDA;
+    return 0.0;
+  }
+  double dt = prm_.cfl / h_red_[0];
+  if (dt >= prm_.dtmax) dt = prm_.dtmax;
+  *st = ANEL_OK;
+  return dt;
+}
+
+int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  static const double A1[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+  static const double A3[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+  anel_step_report r{};
+  ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
+  for (int n = 0; n < nsteps; ++n) {
+    // zero_temps (memManage.F90:844-853)
+    for (int q : {8, 9, 10, 11, 12, 13})
+      ANEL_CUDA_TRY(cudaMemsetAsync(d_fields_[q], 0, G_ * sizeof(double), s));
+    int st = ANEL_OK;
+    const double delt = calcdt(s, &st);
+    if (st != ANEL_OK) return st;
+    // gravity (Routines.F90:27-52)
+    if (time_ < prm_.gt1) gnow_ = 0.0;
+    else if (time_ > prm_.gt1 && time_ < prm_.gt2) gnow_ = g_orig_ * (time_ - prm_.gt1) / (prm_.gt2 - prm_.gt1);
+    else if (time_ >= prm_.gt2) gnow_ = g_orig_;
+    const double DTR[3] = {1.0 / 3.0 * delt, 5.0 / 12.0 * delt, 1.0 / 4.0 * delt};
+    for (int q = 0; q < 3; ++q) {
+      st = substep(A1[q], 1.0, A3[q], DTR[q], delt, s, &r.mg_iter[q], &r.mg_relmax[q], true);
+      if (st != ANEL_OK) return st;
+    }
+    time_ = time_ + delt;
+    r.nstep = nstep_;
+    r.dt = delt;
+    r.time = time_;
+    nstep_ += 1;
+  }
+  ANEL_CUDA_TRY(cudaEventRecord(ev1_, s));
+  ANEL_CUDA_TRY(cudaEventSynchronize(ev1_));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev0_, ev1_);
+  r.ms = ms;
+  double dv[2];
+  const int st = divergence(s, dv);
+  if (st != ANEL_OK) return st;
+  r.avg_div = dv[0];
+  r.max_div = dv[1];
+  if (rep) *rep = r;
+  return ANEL_OK;
+}
+
+int NSSolver::project(cudaStream_t s, int* iters, double* relmax) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  launch_psource(D_, 1.0, s);
+  anel_mg_report rep{};
+  const int st = mg_->solve_device(D_.p, D_.psrc, s, &rep);
+  if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
+  launch_pgrad(D_, 1.0, zrule(NV_U), zrule(NV_V), zrule(NV_W), s);
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  if (iters) *iters = rep.iter;
+  if (relmax) *relmax = rep.relmax;
+  return check_launch("project");
+}
+
+int NSSolver::divergence(cudaStream_t s, double* out) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  const int64_t nb = divergence_blocks(D_);
+  if (!d_part_) ANEL_CUDA_TRY(cudaMalloc(&d_part_, 2 * nb * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMemsetAsync(d_red_ + 1, 0, sizeof(unsigned long long), s));
+  launch_divergence(D_, d_red_ + 1, d_part_, s);
+  std::vector<double> part(2 * nb);
+  ANEL_CUDA_TRY(cudaMemcpyAsync(part.data(), d_part_, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+  ANEL_CUDA_TRY(cudaMemcpyAsync(h_red_ + 1, d_red_ + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  double a = 0.0, b = 0.0;
+  for (int64_t q = 0; q < nb; ++q) {
+    a += part[2 * q];
+    b += part[2 * q + 1];
+  }
+  out[0] = a / b;
+  out[1] = h_red_[1];
+  return check_launch("divergence");
+}
+
+}  // namespace anel

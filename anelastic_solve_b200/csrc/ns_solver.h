@@ -1,0 +1,69 @@
+// ns_solver.h -- host side of the B200 RK3 time stepper.
+#pragma once
+
+#include <vector>
+
+#include "mg_solver.h"
+#include "ns_launch.h"
+
+namespace anel {
+
+// One shear-layer member: device-resident fields, its multigrid context
+// and the sub-step schedule of NSsolver/rk_ss (NSsolver.F90:63-583).
+class NSSolver {
+ public:
+  static NSSolver* create(const anel_grid_desc* g, const anel_mg_params* mg, const anel_ns_params* ns,
+                          int device, int* status);
+  ~NSSolver();
+
+  int set_fields(const anel_fields* f, int mem, cudaStream_t s);
+  int get_fields(const anel_fields* f, int mem, cudaStream_t s);
+  int substep(double a1, double a2, double a3, double dt_rk, double dt, cudaStream_t s, int* iters,
+              double* relmax, bool q_zero = false);
+  int step(int nsteps, cudaStream_t s, anel_step_report* rep);
+  int project(cudaStream_t s, int* iters, double* relmax);
+  int divergence(cudaStream_t s, double* out);
+  void set_clock(double time, int nstep) {
+    time_ = time;
+    nstep_ = nstep;
+  }
+  MGSolver* mg() { return mg_; }
+  cudaStream_t stream() const { return stream_; }
+  int64_t cells() const { return (int64_t)nx_ * ny_ * nz_; }
+
+ private:
+  NSSolver() = default;
+  int init(const anel_grid_desc* g, const anel_mg_params* mg, const anel_ns_params* ns, int device);
+  int upload_profiles();
+  int cn_factors(int slot, double rkdt, cudaStream_t s);
+  ZRule zrule(int vtype) const;
+  double calcdt(cudaStream_t s, int* st);
+
+  anel_ns_params prm_{};
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr;
+  int nx_ = 0, ny_ = 0, nz_ = 0;
+  int64_t G_ = 0;
+  std::vector<double> m_[3][6];  // fine metrics (xe xc dxe dxc rdxe rdxc)
+  std::vector<double> rz_, bgz_;
+  double rRe_ = 0, rPr_ = 0, rSc_ = 0, g_orig_ = 0, gnow_ = 0;
+  double time_ = 0.0;
+  int nstep_ = 1;
+  MGSolver* mg_ = nullptr;
+  NSDev D_{};
+  // device allocations
+  double* d_fields_[17] = {nullptr};
+  double* d_metric_ = nullptr;      // rdxe rdxc rdye rdyc rdze rdzc dze dzc
+  double* d_prof_ = nullptr;        // rz bgz
+  double* d_cn_ = nullptr;          // CN factors: 3 slots x 5 vars x 7 arrays x (nz+2)
+  double* h_cn_ = nullptr;          // pinned staging of the same
+  double cn_rkdt_[3] = {-1, -1, -1};
+  int cn_next_ = 0;
+  unsigned long long* d_red_ = nullptr;
+  double* d_part_ = nullptr;
+  double* h_red_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  CNFacHost fac(int slot, int vi) const;
+};
+
+}  // namespace anel

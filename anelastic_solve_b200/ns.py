@@ -1,0 +1,97 @@
+"""Python mirror of the reference time stepper (NSsolver / rk_ss).
+
+The reference advances its module fields with ``rk_ss(a1, a2, a3, ec,
+dt_rk, dt, psolve, stat)`` three times per ``NSsolver`` step
+(ANELASTIC_SL/dns/NSsolver.F90:63-583).  :class:`NSSolver` keeps the fields
+on one GPU and exposes the same sub-step and step, running the sm_100a
+kernels of libanel.so (no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._lib import AnelError, check, lib
+from .mg import _ptr
+
+__all__ = ["NSSolver", "RK3"]
+
+# Williamson low-storage RK3 coefficients (a1, a2, a3, ec, dt_rk/dt),
+# NSsolver.F90:198-261
+RK3 = ((0.0, 1.0, 1.0 / 3.0, -1.0 / 6.0, 1.0 / 3.0),
+       (-5.0 / 9.0, 1.0, 15.0 / 16.0, -10.0 / 3.0, 5.0 / 12.0),
+       (-153.0 / 128.0, 1.0, 8.0 / 15.0, 15.0 / 8.0, 1.0 / 4.0))
+
+
+class NSSolver:
+    def __init__(self, grid, mgp: abi.MGParams, nsp: abi.NSParams, device: int = 0):
+        self._desc, self._keep = abi.make_grid_desc(grid)
+        self.grid, self.mgp, self.nsp = grid, mgp, nsp
+        st = C.c_int32(0)
+        self._h = lib().anel_ns_create(C.byref(self._desc), C.byref(mgp), C.byref(nsp), int(device),
+                                       C.byref(st))
+        if not self._h:
+            raise AnelError(st.value, lib().anel_last_error().decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().anel_ns_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def _fields(self, d: dict):
+        fs = abi.Fields()
+        mem = None
+        for name, a in d.items():
+            if a is None:
+                continue
+            p, m = _ptr(a)
+            if mem is not None and m != mem:
+                raise TypeError("all fields of one call must live in the same memory space")
+            mem = m
+            setattr(fs, name, p)
+        return fs, (abi.MEM_HOST if mem is None else mem)
+
+    def set_fields(self, d: dict):
+        fs, mem = self._fields(d)
+        check(lib().anel_ns_set_fields(self._h, C.byref(fs), mem))
+
+    def get_fields(self, names=("u", "v", "w", "p", "rho", "scal1")) -> dict:
+        out = {n: np.zeros(self.grid.ghosted, order="F") for n in names}
+        fs, mem = self._fields(out)
+        check(lib().anel_ns_get_fields(self._h, C.byref(fs), mem))
+        return out
+
+    def get_into(self, d: dict):
+        fs, mem = self._fields(d)
+        check(lib().anel_ns_get_fields(self._h, C.byref(fs), mem))
+
+    def substep(self, a1, a2, a3, dt_rk, dt, stream=None):
+        it = C.c_int32(0)
+        rm = C.c_double(0)
+        s = C.c_void_p(int(stream)) if stream is not None else None
+        check(lib().anel_ns_ctx_substep(self._h, a1, a2, a3, dt_rk, dt, s, C.byref(it), C.byref(rm)))
+        return it.value, rm.value
+
+    def step(self, n: int = 1, stream=None) -> abi.StepReport:
+        rep = abi.StepReport()
+        s = C.c_void_p(int(stream)) if stream is not None else None
+        check(lib().anel_ns_ctx_step(self._h, int(n), s, C.byref(rep)))
+        return rep
+
+    def set_clock(self, time: float, nstep: int):
+        check(lib().anel_ns_ctx_set_clock(self._h, float(time), int(nstep)))
+
+    def project(self):
+        it = C.c_int32(0)
+        rm = C.c_double(0)
+        check(lib().anel_ns_ctx_project(self._h, C.byref(it), C.byref(rm)))
+        return it.value, rm.value
+
+    def divergence(self):
+        out = (C.c_double * 2)()
+        check(lib().anel_ns_ctx_divergence(self._h, out))
+        return out[0], out[1]

@@ -177,6 +177,113 @@ int anel_mg_ctx_levels(const anel_mg_ctx* ctx, int32_t* out, int32_t cap);
 int anel_mg_ctx_debug_pass(anel_mg_ctx* ctx, int32_t which, double* d_phi,
                            const double* d_src, void* stream);
 
+/* ======================================================================
+ * RK3 time stepper (rk_ss / NSsolver, ANELASTIC_SL/dns/NSsolver.F90)
+ * ==================================================================== */
+
+/* velocity / scalar models (the Vmodel/Rmodel/Smodel ini keys,
+ * ANELASTIC_SL/dns/input.F90): DNS, or the constant-coefficient
+ * Smagorinsky model (SSM, SSMrho, SSMscal1). */
+enum { ANEL_MODEL_DNS = 0, ANEL_MODEL_SSM = 1 };
+/* LES filter width (les_grid_size, straincal.F90:126-134) */
+enum { ANEL_DELTA_3ROOT = 0, ANEL_DELTA_2ROOT = 1 };
+/* LES wall damping: LITERAL = Mason damping of SSM.F90:27,60 with its
+ * REAL(4) literals; NONE = f_damp == 1, i.e. Csgs = SSM_const. */
+enum { ANEL_DAMP_LITERAL = 0, ANEL_DAMP_NONE = 1 };
+
+/* Field variables of the boundC tables TB(3,2,8)/VB(3,2,8)
+ * (ANELASTIC_SL/include/modules.F90:80-86): index l-1 of
+ * 1=U1 2=U2 3=U3 4=P 5=RHO 6=FLUC 7=temporaries/psource 8=SCAL1.
+ * Types: 1 Dirichlet, 2 Neumann, 3 periodic, 4 one-point Neumann,
+ * 6 wall6, 7 wall7, 8 linear extrapolation (ANELASTIC_SL/dns/BC.F90:334-585). */
+typedef struct {
+  double Re, Pr, Sc;                  /* rRe = 1/Re, rPr = 1/Pr, rSc = 1/Sc */
+  double cfl, dtmax;                  /* calcdt (Routines.F90:186-258), DeltaT_max */
+  double g_init, g_final, gt1, gt2;   /* gravity ramp (Routines.F90:2-52) */
+  int32_t vmodel, rmodel, smodel;     /* ANEL_MODEL_* */
+  int32_t les_delta;                  /* ANEL_DELTA_* */
+  int32_t les_damp;                   /* ANEL_DAMP_* */
+  double ssm_const, pr_sgs;           /* SSM_const, Pr_eddy (Pr_sgs) */
+  int32_t les_start, les_freq;        /* les_start_step, les_call_freq */
+  int32_t tb[3][2][8];                /* TB(dir,face,var) */
+  double vb[3][2][8];                 /* VB(dir,face,var) */
+  /* EW edge-node flag of the w field (Domain module).  0: as Sturb.F90:
+   * 110-112 forces it -- w at the top wall face (k = nz+1) is advanced as
+   * an unknown, which leaves the Neumann pressure problem incompatible.
+   * 1: the edge-node mode the code is written for -- u3_rhs and Pgrad stop
+   * at nz, and the w ghost sets w(nz+1) to the wall value and w(nz+2) to 0
+   * (BC.F90:471-527). */
+  int32_t ew;
+  /* 1: advance scal1 as rk_ss always does.  0: hold scal1 (and its
+   * accumulator) at zero, valid when scal1 starts at zero with zero wall
+   * values -- it then stays zero in the reference as well. */
+  int32_t scal1_on;
+} anel_ns_params;
+
+/* Host (or device) pointers to the ghosted FP64 fields of the Flow and
+ * LESmod modules.  u at (xe,yc,zc), v at (xc,ye,zc), w at (xc,yc,ze),
+ * the others at cell centres.  q_* are the RK3 accumulators u1_tmp2,
+ * u2_tmp2, u3_tmp2, r_tmp2, scal1_tmp2; psrc is r_tmp1 (the Poisson right-
+ * hand side scratch).  nuT/kappaT/nappaT may be NULL for DNS. */
+typedef struct {
+  double *u, *v, *w, *p, *rho, *scal1;
+  double *r, *densityBG;
+  double *q_u, *q_v, *q_w, *q_rho, *q_s;
+  double *psrc;
+  double *nuT, *kappaT, *nappaT;
+} anel_fields;
+
+/* Per-step report */
+typedef struct {
+  int32_t nstep;        /* step number just completed */
+  int32_t mg_iter[3];   /* MG cycles of the three sub-steps */
+  double dt;            /* delt used */
+  double time;          /* time after the step */
+  double mg_relmax[3];  /* MG stop metric of each sub-step */
+  double max_div;       /* max |div u| after the step (divergence()) */
+  double avg_div;       /* volume-weighted mean |div u| */
+  double ms;            /* device time of the step */
+} anel_step_report;
+
+typedef struct anel_ns_ctx anel_ns_ctx;
+
+/* Context calls: fields live on the device inside the context. */
+anel_ns_ctx* anel_ns_create(const anel_grid_desc* grid, const anel_mg_params* mg,
+                            const anel_ns_params* ns, int32_t device, int32_t* status);
+void anel_ns_destroy(anel_ns_ctx* ctx);
+/* Copy fields in/out (mem = ANEL_MEM_HOST or ANEL_MEM_DEVICE pointers).
+ * Null members are skipped.  r and densityBG must be horizontally
+ * uniform (functions of z only). */
+int anel_ns_set_fields(anel_ns_ctx* ctx, const anel_fields* f, int32_t mem);
+int anel_ns_get_fields(anel_ns_ctx* ctx, const anel_fields* f, int32_t mem);
+/* One RK sub-step, rk_ss(a1,a2,a3,ec,dt_rk,dt,psolve,stat)
+ * (NSsolver.F90:418-583), on the context's fields. */
+int anel_ns_ctx_substep(anel_ns_ctx* ctx, double a1, double a2, double a3, double dt_rk,
+                        double dt, void* stream, int32_t* mg_iter, double* mg_relmax);
+/* nsteps full time steps of NSsolver (NSsolver.F90:63-283 without the
+ * output/statistics diagnostics): calcdt, gravity, LES update, three
+ * sub-steps.  report (may be NULL) describes the last step. */
+int anel_ns_ctx_step(anel_ns_ctx* ctx, int32_t nsteps, void* stream, anel_step_report* report);
+/* time and step counter (time, nstep of the Parameters module) */
+int anel_ns_ctx_set_clock(anel_ns_ctx* ctx, double time, int32_t nstep);
+/* Projection of the current velocity onto divergence-free fields (used to
+ * prepare initial conditions): Psource with dt = 1, one MG solve starting
+ * from p, Pgrad with dt = 1 and the velocity ghost passes. */
+int anel_ns_ctx_project(anel_ns_ctx* ctx, int32_t* mg_iter, double* mg_relmax);
+/* divergence() (Routines.F90:54-183) of the current velocity:
+ * out[0] = volume-weighted mean |div|, out[1] = max |div|. */
+int anel_ns_ctx_divergence(anel_ns_ctx* ctx, double* out);
+
+/* Drop-in form for the Fortran driver: bind the module arrays (host)
+ * once, then call anel_rk_substep with the reference's rk_ss arguments;
+ * every call copies the bound fields to the device and back. */
+int anel_ns_init(const anel_grid_desc* grid, const anel_mg_params* mg, const anel_ns_params* ns);
+int anel_bind_fields(const anel_fields* f);
+void anel_rk_substep(const double* a1, const double* a2, const double* a3, const double* ec,
+                     const double* dt_rk, const double* dt, const int32_t* psolve,
+                     int32_t* stat);
+int anel_ns_finalize(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -52,7 +52,7 @@ struct orc_mg {
   double vbc[6];
   int maxcy;
   double tolmax;
-  int smoother, mode;
+  int smoother, mode, stop;
   int pre[ML], post[ML];
   double* r;              /* Flow::r, fine ghosted */
   /* fine grid metrics, n+2 each, [0] = Fortran index 1 */
@@ -291,6 +291,7 @@ orc_mg* orc_mg_create(const anel_grid_desc* g, const anel_mg_params* p, int* sta
   m->tolmax = p->tolmax;
   m->smoother = p->smoother;
   m->mode = p->mode;
+  m->stop = p->stop;
   for (int f = 0; f < 6; ++f) {
     m->tbc[f] = p->tbc[f];
     m->vbc[f] = p->vbc[f];
@@ -1152,6 +1153,28 @@ static double residual(orc_mg* m, double* phio, const double* phin) {
   return relmax;
 }
 
+/* ||f - A phi|| / ||f|| on the finest level with the built coefficients */
+static double fine_resid_norm(orc_mg* m, const double* phi, const double* f) {
+  const int l = m->ngrid;
+  LVLDIMS(m, l);
+  double* c[7];
+  for (int q = 0; q < 7; ++q) c[q] = lvl_ptr(m->workc[q], m, l);
+  double rr = 0.0, ff = 0.0;
+  for (int k = m->sk[l][2]; k <= m->ek[l][2]; ++k)
+    for (int j = m->sk[l][1]; j <= m->ek[l][1]; ++j)
+      for (int i = m->sk[l][0]; i <= m->ek[l][0]; ++i) {
+        const double ax =
+            AT(c[0], i, j, k) * AT(phi, i - 1, j, k) + AT(c[1], i, j, k) * AT(phi, i + 1, j, k) +
+            AT(c[2], i, j, k) * AT(phi, i, j - 1, k) + AT(c[3], i, j, k) * AT(phi, i, j + 1, k) +
+            AT(c[4], i, j, k) * AT(phi, i, j, k - 1) + AT(c[5], i, j, k) * AT(phi, i, j, k + 1) +
+            AT(c[6], i, j, k) * AT(phi, i, j, k);
+        const double rv = AT(f, i, j, k) - ax;
+        rr += rv * rv;
+        ff += AT(f, i, j, k) * AT(f, i, j, k);
+      }
+  return ff > 0.0 ? sqrt(rr / ff) : sqrt(rr);
+}
+
 /* -------------------------------------------------------------- mg_solver
  * mg_solver.F90:71-140 */
 void orc_mg_solve(orc_mg* m, double* phif, double* rhsf, int* iter, double* relmax) {
@@ -1163,10 +1186,26 @@ void orc_mg_solve(orc_mg* m, double* phif, double* rhsf, int* iter, double* relm
   memcpy(lvl_ptr(m->work2, m, ng), rhsf, sizeof(double) * G);
   double rm = 0.0;
   int it;
-  for (it = 1; it <= m->maxcy; ++it) {
-    cycle(m, rhsf);
-    rm = residual(m, phif, lvl_ptr(m->work1, m, ng));
-    if (rm <= m->tolmax) break;
+  if (m->stop == ANEL_STOP_RESID) {
+    /* extension: stop on ||f - A phi||_2 / ||f||_2 of the fine operator;
+     * the caller's rhsf is kept for the norms (work2 holds the copy the
+     * cycles use) */
+    const double* f = lvl_ptr(m->work2, m, ng);
+    double* fsave = (double*)malloc(sizeof(double) * G);
+    memcpy(fsave, f, sizeof(double) * G);
+    for (it = 1; it <= m->maxcy; ++it) {
+      cycle(m, rhsf);
+      rm = fine_resid_norm(m, lvl_ptr(m->work1, m, ng), fsave);
+      if (rm <= m->tolmax) break;
+    }
+    free(fsave);
+    memcpy(phif, lvl_ptr(m->work1, m, ng), sizeof(double) * G);
+  } else {
+    for (it = 1; it <= m->maxcy; ++it) {
+      cycle(m, rhsf);
+      rm = residual(m, phif, lvl_ptr(m->work1, m, ng));
+      if (rm <= m->tolmax) break;
+    }
   }
   /* A DO loop that runs to completion leaves iter = maxcy+1 (Fortran
    * semantics), which is what the reference returns when it did not

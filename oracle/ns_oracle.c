@@ -1,3 +1,1137 @@
-/* ns_oracle.c -- CPU restatement of the RK3 sub-step (filled in with the
- * stepper oracle).  TEST INFRASTRUCTURE ONLY. */
+/*
+ * ns_oracle.c -- CPU FP64 restatement of the reference RK3 time step
+ * (ANELASTIC_SL/dns/NSsolver.F90, BC.F90, Routines.F90, les/SSM.F90,
+ * les/straincal.F90).  TEST INFRASTRUCTURE ONLY: used by the parity tests,
+ * the smoke check and the CPU-baseline leg of bench.py; the product never
+ * links or calls it.
+ *
+ * Serial semantics (one MPI rank, EU = EV = EW = 0, RK3CN = .true.,
+ * RK3 = pcorrect = .false., LESflag = 1: Sturb.F90:110-120).  Every
+ * expression follows the Fortran source left to right; compiled with
+ * -ffp-contract=off.  Fortran REAL(4) literals (0.5, 0.41, 0.3) are
+ * written as (double)(float) where they are not exact.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
 #include "oracle.h"
+
+typedef struct {
+  int nx, ny, nz;
+  long X, Y, Z, G;
+  /* metrics, [0] = Fortran index 1 */
+  const double *xe, *xc, *dxe, *dxc, *rdxe, *rdxc;
+  const double *ye, *yc, *dye, *dyc, *rdye, *rdyc;
+  const double *ze, *zc, *dze, *dzc, *rdze, *rdzc;
+} orc_dom;
+
+struct orc_ns {
+  orc_dom d;
+  anel_grid_desc g;
+  anel_ns_params p;
+  orc_mg* mg;
+  double rRe, rPr, rSc, g_orig, gnow, time;
+  int nstep;
+  anel_fields f;  /* caller-owned host arrays */
+  double* Ftemp;  /* RHS scratch */
+  double *Csgs, *CTsgs, *CSsgs, *delg, *modS;
+  double* work[4];
+};
+
+#define IX(i, j, k) (((long)(i) - 1) + D->X * (((long)(j) - 1) + D->Y * ((long)(k) - 1)))
+#define A_(a, i, j, k) (a)[IX(i, j, k)]
+#define M(a, i) (a)[(i) - 1]
+
+static const double R12 = 1.0 / 2.0; /* ratios::r_1_2 (modules.F90:203) */
+
+/* ---------------------------------------------------------------- ghost
+ * ghost() + bound_update() serial semantics (BC.F90:1-187, 334-585). */
+enum { VT_U, VT_V, VT_W, VT_P, VT_RHO, VT_CFLUC, VT_PSOURCE, VT_UTEMP, VT_VTEMP, VT_WTEMP,
+       VT_RTEMP, VT_S1TEMP, VT_SCAL1, VT_SCAL1TEMP };
+
+static void vtype_info(int vt, int* l, int* rt, int* stag) {
+  /* stag: 1 = u-staggered, 2 = v, 3 = w, 0 = cell centred */
+  *rt = 0;
+  *stag = 0;
+  switch (vt) {
+    case VT_U: *l = 1; *stag = 1; break;
+    case VT_V: *l = 2; *stag = 2; break;
+    case VT_W: *l = 3; *stag = 3; break;
+    case VT_P: *l = 4; break;
+    case VT_RHO: *l = 5; *rt = 1; break;
+    case VT_CFLUC: *l = 6; break;
+    case VT_PSOURCE: *l = 7; break;
+    case VT_UTEMP: *l = 7; *stag = 1; break;
+    case VT_VTEMP: *l = 7; *stag = 2; break;
+    case VT_WTEMP: *l = 7; *stag = 3; break;
+    case VT_RTEMP: *l = 7; break;
+    case VT_S1TEMP: *l = 7; break;
+    case VT_SCAL1: *l = 8; *rt = 1; break;
+    default: *l = 8; break; /* VT_SCAL1TEMP */
+  }
+}
+
+/* bound_update for one (dir, face) */
+static void bound_update(const orc_dom* D, double* var, int btype, int face, int dir, double value,
+                         int stag, int rt, int ew) {
+  const int sx = 2, ex = D->nx + 1, sy = 2, ey = D->ny + 1, sz = 2, ez = D->nz + 1;
+  int of1 = 0, of2 = 0;
+  const double *dxt, *dyt, *dzt;
+  if (stag == 1) {
+    dxt = D->dxc; dyt = D->dye; dzt = D->dze; of2 = 1;
+  } else if (stag == 2) {
+    dxt = D->dxe; dyt = D->dyc; dzt = D->dze; of2 = 1;
+  } else if (stag == 3) {
+    dxt = D->dxe; dyt = D->dye; dzt = D->dzc; of2 = 1;
+  } else {
+    dxt = D->dxe; dyt = D->dye; dzt = D->dze; of1 = -1;
+  }
+  const long X = D->X, Y = D->Y, Z = D->Z;
+  if (dir == 1) {
+    for (long k = 1; k <= Z; ++k)
+      for (long j = 1; j <= Y; ++j) {
+        double* L = &A_(var, 1, j, k);
+        /* L[i-1] = var(i,j,k) */
+        if (btype == 1) {
+          if (face == 1) L[sx - 2] = value;
+          else L[ex] = value;
+        } else if (btype == 2) {
+          if (face == 1) {
+            if (rt == 1) L[sx - 1] = L[sx] - value * M(dxt, sx + 1 + of1);
+            L[sx - 2] = L[sx - 1] - value * M(dxt, sx + of1);
+          } else {
+            if (rt == 1) L[ex - 1] = L[ex - 2] + value * M(dxt, ex - 1 + of2);
+            L[ex] = L[ex - 1] + value * M(dxt, ex + of2);
+          }
+        } else if (btype == 3) {
+          L[sx - 2] = L[ex - 1];
+          L[ex] = L[sx - 1];
+        } else if (btype == 4) {
+          if (face == 1) L[sx - 2] = L[sx - 1] - value * M(dxt, sx + of1);
+          else L[ex] = L[ex - 1] + value * M(dxt, ex + of2);
+        } else if (btype == 8) {
+          if (face == 1) L[sx - 2] = 2.0 * L[sx - 1] - L[sx];
+          else L[ex] = 2.0 * L[ex - 1] - L[ex - 2];
+        }
+      }
+  } else if (dir == 2) {
+    for (long k = 1; k <= Z; ++k)
+      for (long i = 1; i <= X; ++i) {
+#define V2(j) A_(var, i, j, k)
+        if (btype == 1) {
+          if (face == 1) V2(sy - 1) = value;
+          else V2(ey + 1) = value;
+        } else if (btype == 2) {
+          if (face == 1) {
+            if (rt == 1) V2(sy) = V2(sy + 1) - value * M(dyt, sy + 1 + of1);
+            V2(sy - 1) = V2(sy) - value * M(dyt, sy + of1);
+          } else {
+            if (rt == 1) V2(ey) = V2(ey - 1) + value * M(dyt, ey - 1 + of2);
+            V2(ey + 1) = V2(ey) + value * M(dyt, ey + of2);
+          }
+        } else if (btype == 3) {
+          V2(sy - 1) = V2(ey);
+          V2(ey + 1) = V2(sy);
+        } else if (btype == 4) {
+          if (face == 1) V2(sy - 1) = V2(sy) - value * M(dyt, sy + of1);
+          else V2(ey + 1) = V2(ey) + value * M(dyt, ey + of2);
+        }
+#undef V2
+      }
+  } else {
+    const int iW = (stag == 3) ? ew : 0;
+    for (long j = 1; j <= Y; ++j)
+      for (long i = 1; i <= X; ++i) {
+#define V3(k) A_(var, i, j, k)
+        if (btype == 1) {
+          if (face == 1) V3(sz - 1) = value;
+          else V3(ez + 1 - iW) = value;
+        } else if (btype == 2) {
+          if (face == 1) {
+            if (rt == 1) V3(sz) = V3(sz + 1) - value * M(dzt, sz + 1 + of1);
+            V3(sz - 1) = V3(sz) - value * M(dzt, sz + of1);
+          } else {
+            if (rt == 1) V3(ez - iW) = V3(ez - 1 - iW) + value * M(dzt, ez - 1 + of2 - iW);
+            V3(ez + 1 - iW) = V3(ez - iW) + value * M(dzt, ez + of2 - iW);
+          }
+        } else if (btype == 3) {
+          V3(sz - 1) = V3(ez - iW);
+          V3(ez + 1 - iW) = V3(sz);
+        } else if (btype == 4) {
+          if (face == 1) V3(sz - 1) = V3(sz) - value * M(dzt, sz + of1);
+          else V3(ez + 1 - iW) = V3(ez - iW) + value * M(dzt, ez + of2 - iW);
+        } else if (btype == 6) {
+          if (face == 1) V3(sz - 1) = 2.0 * value - 1.0 * V3(sz);
+          else V3(ez + 1 - iW) = 2.0 * value - 1.0 * V3(ez - iW);
+        } else if (btype == 7) {
+          if (face == 1) {
+            V3(sz) = 0.0;
+            V3(sz - 1) = -1.0 * V3(sz + 1);
+          } else {
+            V3(ez) = 0.0;
+            V3(ez + 1 - iW) = -1.0 * V3(ez - iW - 1);
+          }
+        }
+        /* SET EXTRA POINT TO ZERO (BC.F90:526-527) */
+        if (face == 2 && iW == 1) V3(ez + 1) = 0.0;
+#undef V3
+      }
+  }
+}
+
+static void ghost(const orc_ns* s, double* var, int vt) {
+  const orc_dom* D = &s->d;
+  const long X = D->X, Y = D->Y, Z = D->Z;
+  const int sx = 2, ex = D->nx + 1, sy = 2, ey = D->ny + 1, sz = 2, ez = D->nz + 1;
+  /* full periodic wrap (BC.F90:55-66) */
+  for (long k = 1; k <= Z; ++k)
+    for (long j = 1; j <= Y; ++j) {
+      A_(var, sx - 1, j, k) = A_(var, ex, j, k);
+      A_(var, ex + 1, j, k) = A_(var, sx, j, k);
+    }
+  for (long k = 1; k <= Z; ++k)
+    for (long i = 1; i <= X; ++i) {
+      A_(var, i, sy - 1, k) = A_(var, i, ey, k);
+      A_(var, i, ey + 1, k) = A_(var, i, sy, k);
+    }
+  for (long j = 1; j <= Y; ++j)
+    for (long i = 1; i <= X; ++i) {
+      A_(var, i, j, sz - 1) = A_(var, i, j, ez);
+      A_(var, i, j, ez + 1) = A_(var, i, j, sz);
+    }
+  int l, rt, stag;
+  vtype_info(vt, &l, &rt, &stag);
+  for (int n = 1; n <= 3; ++n)
+    for (int m = 1; m <= 2; ++m) {
+      const int tb = s->p.tb[n - 1][m - 1][l - 1];
+      const int tb1 = s->p.tb[n - 1][0][l - 1];
+      if (tb1 != 3 || m == 1)
+        bound_update(D, var, tb, m, n, s->p.vb[n - 1][m - 1][l - 1], stag, rt, s->p.ew);
+    }
+}
+
+/* ------------------------------------------------------------ create */
+orc_ns* orc_ns_create(const anel_grid_desc* g, const anel_mg_params* mgp, const anel_ns_params* np,
+                      int* stat) {
+  orc_ns* s = (orc_ns*)calloc(1, sizeof(orc_ns));
+  s->g = *g;
+  s->p = *np;
+  orc_dom* D = &s->d;
+  D->nx = g->nx;
+  D->ny = g->ny;
+  D->nz = g->nz;
+  D->X = g->nx + 2;
+  D->Y = g->ny + 2;
+  D->Z = g->nz + 2;
+  D->G = D->X * D->Y * D->Z;
+  D->xe = g->xe; D->xc = g->xc; D->dxe = g->dxe; D->dxc = g->dxc; D->rdxe = g->rdxe; D->rdxc = g->rdxc;
+  D->ye = g->ye; D->yc = g->yc; D->dye = g->dye; D->dyc = g->dyc; D->rdye = g->rdye; D->rdyc = g->rdyc;
+  D->ze = g->ze; D->zc = g->zc; D->dze = g->dze; D->dzc = g->dzc; D->rdze = g->rdze; D->rdzc = g->rdzc;
+  s->rRe = 1.0 / np->Re;
+  s->rPr = 1.0 / np->Pr;
+  s->rSc = 1.0 / np->Sc;
+  s->g_orig = np->g_final;
+  s->gnow = np->g_init;
+  s->mg = orc_mg_create(g, mgp, stat);
+  if (*stat != 0) return s;
+  s->Ftemp = (double*)calloc(D->G, sizeof(double));
+  s->Csgs = (double*)calloc(D->G, sizeof(double));
+  s->CTsgs = (double*)calloc(D->G, sizeof(double));
+  s->CSsgs = (double*)calloc(D->G, sizeof(double));
+  s->delg = (double*)calloc(D->G, sizeof(double));
+  s->modS = (double*)calloc(D->G, sizeof(double));
+  for (int q = 0; q < 4; ++q) s->work[q] = (double*)calloc(D->G, sizeof(double));
+  s->nstep = 1;
+  return s;
+}
+
+void orc_ns_destroy(orc_ns* s) {
+  if (!s) return;
+  orc_mg_destroy(s->mg);
+  free(s->Ftemp);
+  free(s->Csgs);
+  free(s->CTsgs);
+  free(s->CSsgs);
+  free(s->delg);
+  free(s->modS);
+  for (int q = 0; q < 4; ++q) free(s->work[q]);
+  free(s);
+}
+
+void orc_ns_bind(orc_ns* s, const anel_fields* f) { s->f = *f; }
+void orc_ns_set_clock(orc_ns* s, double time, int nstep) {
+  s->time = time;
+  s->nstep = nstep;
+}
+
+static int les_on(const orc_ns* s) {
+  return s->p.vmodel == ANEL_MODEL_SSM;
+}
+
+/* ---------------------------------------------------------------- u1_rhs
+ * NSsolver.F90:585-860 (DNS linear + non-linear, SSM LES terms). */
+static void u1_rhs(orc_ns* s, double* Ut) {
+  const orc_dom* D = &s->d;
+  const double *un = s->f.u, *vn = s->f.v, *wn = s->f.w, *r = s->f.r, *nuT = s->f.nuT;
+  const double rRe = s->rRe;
+  memset(Ut, 0, sizeof(double) * D->G);
+  const int sx = 2, ex = D->nx + 1, sy = 2, ey = D->ny + 1, sz = 2, ez = D->nz + 1;
+  for (int k = sz; k <= ez; ++k)
+    for (int j = sy; j <= ey; ++j)
+      for (int i = sx; i <= ex; ++i)
+        A_(Ut, i, j, k) = A_(Ut, i, j, k) +
+                          rRe * ((A_(un, i + 1, j, k) - A_(un, i, j, k)) * M(D->rdxc, i + 1) -
+                                 (A_(un, i, j, k) - A_(un, i - 1, j, k)) * M(D->rdxc, i)) *
+                              M(D->rdxe, i) +
+                          rRe * ((A_(un, i, j + 1, k) - A_(un, i, j, k)) * M(D->rdye, j) -
+                                 (A_(un, i, j, k) - A_(un, i, j - 1, k)) * M(D->rdye, j - 1)) *
+                              M(D->rdyc, j);
+  for (int k = sz; k <= ez; ++k)
+    for (int j = sy; j <= ey; ++j)
+      for (int i = sx; i <= ex; ++i) {
+        double ua2 = R12 * (A_(un, i + 1, j, k) + A_(un, i, j, k));
+        double ua1 = R12 * (A_(un, i, j, k) + A_(un, i - 1, j, k));
+        A_(Ut, i, j, k) = A_(Ut, i, j, k) + (ua1 * ua1 - ua2 * ua2) * M(D->rdxe, i);
+        ua2 = R12 * (A_(un, i, j, k + 1) + A_(un, i, j, k));
+        ua1 = R12 * (A_(un, i, j, k) + A_(un, i, j, k - 1));
+        const double ra2 = R12 * (A_(r, i, j, k + 1) + A_(r, i, j, k));
+        const double ra1 = R12 * (A_(r, i, j, k) + A_(r, i, j, k - 1));
+        const double wa2 = R12 * (A_(wn, i + 1, j, k) + A_(wn, i, j, k));
+        const double wa1 = R12 * (A_(wn, i + 1, j, k - 1) + A_(wn, i, j, k - 1));
+        A_(Ut, i, j, k) =
+            A_(Ut, i, j, k) + (ra1 * ua1 * wa1 - ra2 * ua2 * wa2) * M(D->rdzc, k) / A_(r, i, j, k);
+        ua2 = R12 * (A_(un, i, j + 1, k) + A_(un, i, j, k));
+        ua1 = R12 * (A_(un, i, j, k) + A_(un, i, j - 1, k));
+        const double va2 = R12 * (A_(vn, i + 1, j, k) + A_(vn, i, j, k));
+        const double va1 = R12 * (A_(vn, i + 1, j - 1, k) + A_(vn, i, j - 1, k));
+        A_(Ut, i, j, k) = A_(Ut, i, j, k) + (ua1 * va1 - ua2 * va2) * M(D->rdyc, j);
+      }
+  if (les_on(s)) {
+    for (int k = sz; k <= ez; ++k)
+      for (int j = sy; j <= ey; ++j)
+        for (int i = sx; i <= ex; ++i) {
+          A_(Ut, i, j, k) =
+              A_(Ut, i, j, k) -
+              1 * 2.0 *
+                  (A_(nuT, i + 1, j, k) * (A_(un, i + 1, j, k) - A_(un, i, j, k)) * M(D->rdxc, i + 1) -
+                   A_(nuT, i, j, k) * (A_(un, i, j, k) - A_(un, i - 1, j, k)) * M(D->rdxc, i)) *
+                  M(D->rdxe, i);
+          double n1 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i + 1, j, k) + A_(nuT, i, j - 1, k) +
+                              A_(nuT, i + 1, j - 1, k));
+          double n2 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i + 1, j, k) + A_(nuT, i, j + 1, k) +
+                              A_(nuT, i + 1, j + 1, k));
+          A_(Ut, i, j, k) = A_(Ut, i, j, k) -
+                            1 * 1.0 *
+                                (n2 * (A_(un, i, j + 1, k) - A_(un, i, j, k)) * M(D->rdye, j) -
+                                 n1 * (A_(un, i, j, k) - A_(un, i, j - 1, k)) * M(D->rdye, j - 1)) *
+                                M(D->rdyc, j);
+          A_(Ut, i, j, k) = A_(Ut, i, j, k) -
+                            1 * 1.0 *
+                                (n2 * (A_(vn, i + 1, j + 1, k) - A_(vn, i, j + 1, k)) * M(D->rdxe, i) -
+                                 n1 * (A_(vn, i + 1, j, k) - A_(vn, i, j, k)) * M(D->rdxe, i)) *
+                                M(D->rdyc, j);
+          n1 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i + 1, j, k) + A_(nuT, i, j, k - 1) +
+                       A_(nuT, i + 1, j, k - 1));
+          n2 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i + 1, j, k) + A_(nuT, i, j, k + 1) +
+                       A_(nuT, i + 1, j, k + 1));
+          const double ra2 = R12 * (A_(r, i, j, k + 1) + A_(r, i, j, k));
+          const double ra1 = R12 * (A_(r, i, j, k) + A_(r, i, j, k - 1));
+          A_(Ut, i, j, k) =
+              A_(Ut, i, j, k) -
+              1 * 1.0 *
+                  (ra2 * n2 * (A_(wn, i + 1, j, k) - A_(wn, i, j, k)) * M(D->rdxe, i) -
+                   ra1 * n1 * (A_(wn, i + 1, j, k - 1) - A_(wn, i, j, k - 1)) * M(D->rdxe, i)) *
+                  M(D->rdzc, k) / A_(r, i, j, k);
+        }
+  }
+  ghost(s, Ut, VT_UTEMP);
+}
+
+/* ---------------------------------------------------------------- u2_rhs
+ * NSsolver.F90:863-1136 */
+static void u2_rhs(orc_ns* s, double* Vt) {
+  const orc_dom* D = &s->d;
+  const double *un = s->f.u, *vn = s->f.v, *wn = s->f.w, *r = s->f.r, *nuT = s->f.nuT;
+  const double rRe = s->rRe;
+  memset(Vt, 0, sizeof(double) * D->G);
+  const int sx = 2, ex = D->nx + 1, sy = 2, ey = D->ny + 1, sz = 2, ez = D->nz + 1;
+  for (int k = sz; k <= ez; ++k)
+    for (int j = sy; j <= ey; ++j)
+      for (int i = sx; i <= ex; ++i)
+        A_(Vt, i, j, k) = A_(Vt, i, j, k) +
+                          rRe * ((A_(vn, i + 1, j, k) - A_(vn, i, j, k)) * M(D->rdxe, i) -
+                                 (A_(vn, i, j, k) - A_(vn, i - 1, j, k)) * M(D->rdxe, i - 1)) *
+                              M(D->rdxc, i) +
+                          rRe * ((A_(vn, i, j + 1, k) - A_(vn, i, j, k)) * M(D->rdyc, j + 1) -
+                                 (A_(vn, i, j, k) - A_(vn, i, j - 1, k)) * M(D->rdyc, j)) *
+                              M(D->rdye, j);
+  for (int k = sz; k <= ez; ++k)
+    for (int j = sy; j <= ey; ++j)
+      for (int i = sx; i <= ex; ++i) {
+        double va1 = 0.5 * (A_(vn, i, j + 1, k) + A_(vn, i, j, k));
+        double va2 = 0.5 * (A_(vn, i, j, k) + A_(vn, i, j - 1, k));
+        A_(Vt, i, j, k) = A_(Vt, i, j, k) - (va1 * va1 - va2 * va2) * M(D->rdye, j);
+        va1 = 0.5 * (A_(vn, i + 1, j, k) + A_(vn, i, j, k));
+        va2 = 0.5 * (A_(vn, i, j, k) + A_(vn, i - 1, j, k));
+        const double ua1 = 0.5 * (A_(un, i, j + 1, k) + A_(un, i, j, k));
+        const double ua2 = 0.5 * (A_(un, i - 1, j + 1, k) + A_(un, i - 1, j, k));
+        A_(Vt, i, j, k) = A_(Vt, i, j, k) - (ua1 * va1 - ua2 * va2) * M(D->rdxc, i);
+        va1 = 0.5 * (A_(vn, i, j, k + 1) + A_(vn, i, j, k));
+        va2 = 0.5 * (A_(vn, i, j, k) + A_(vn, i, j, k - 1));
+        const double ra1 = 0.5 * (A_(r, i, j, k + 1) + A_(r, i, j, k));
+        const double ra2 = 0.5 * (A_(r, i, j, k) + A_(r, i, j, k - 1));
+        const double wa1 = 0.5 * (A_(wn, i, j + 1, k) + A_(wn, i, j, k));
+        const double wa2 = 0.5 * (A_(wn, i, j + 1, k - 1) + A_(wn, i, j, k - 1));
+        A_(Vt, i, j, k) =
+            A_(Vt, i, j, k) - (ra1 * wa1 * va1 - ra2 * wa2 * va2) * M(D->rdzc, k) / A_(r, i, j, k);
+      }
+  if (les_on(s)) {
+    for (int k = sz; k <= ez; ++k)
+      for (int j = sy; j <= ey; ++j)
+        for (int i = sx; i <= ex; ++i) {
+          double n1 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i - 1, j, k) + A_(nuT, i, j + 1, k) +
+                              A_(nuT, i - 1, j + 1, k));
+          double n2 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i + 1, j, k) + A_(nuT, i, j + 1, k) +
+                              A_(nuT, i + 1, j + 1, k));
+          A_(Vt, i, j, k) = A_(Vt, i, j, k) -
+                            1 * 1.0 *
+                                (n2 * (A_(vn, i + 1, j, k) - A_(vn, i, j, k)) * M(D->rdxe, i) -
+                                 n1 * (A_(vn, i, j, k) - A_(vn, i - 1, j, k)) * M(D->rdxe, i - 1)) *
+                                M(D->rdxc, i);
+          A_(Vt, i, j, k) = A_(Vt, i, j, k) -
+                            1 * 1.0 *
+                                (n2 * (A_(un, i + 1, j + 1, k) - A_(un, i + 1, j, k)) * M(D->rdye, j) -
+                                 n1 * (A_(un, i, j + 1, k) - A_(un, i, j, k)) * M(D->rdye, j)) *
+                                M(D->rdxc, i);
+          A_(Vt, i, j, k) =
+              A_(Vt, i, j, k) -
+              1 * 2.0 *
+                  (A_(nuT, i, j + 1, k) * (A_(vn, i, j + 1, k) - A_(vn, i, j, k)) * M(D->rdyc, j + 1) -
+                   A_(nuT, i, j, k) * (A_(vn, i, j, k) - A_(vn, i, j - 1, k)) * M(D->rdyc, j)) *
+                  M(D->rdye, j);
+          n1 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i, j + 1, k) + A_(nuT, i, j, k - 1) +
+                       A_(nuT, i, j + 1, k - 1));
+          n2 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i, j + 1, k) + A_(nuT, i, j, k + 1) +
+                       A_(nuT, i, j + 1, k + 1));
+          const double ra1 = 0.5 * (A_(r, i, j, k + 1) + A_(r, i, j, k));
+          const double ra2 = 0.5 * (A_(r, i, j, k) + A_(r, i, j, k - 1));
+          /* the reference pairs raver2 (lower face) with nuTaver2 (upper) */
+          A_(Vt, i, j, k) =
+              A_(Vt, i, j, k) -
+              1 * 1.0 *
+                  (ra2 * n2 * (A_(wn, i, j + 1, k) - A_(wn, i, j, k)) * M(D->rdye, j) -
+                   ra1 * n1 * (A_(wn, i, j + 1, k - 1) - A_(wn, i, j, k - 1)) * M(D->rdye, j)) *
+                  M(D->rdzc, k) / A_(r, i, j, k);
+        }
+  }
+  ghost(s, Vt, VT_VTEMP);
+}
+
+/* ---------------------------------------------------------------- u3_rhs
+ * NSsolver.F90:1138-1432 (density_mean at :1201 is dead: its result is
+ * not used). */
+static void u3_rhs(orc_ns* s, double* Wt) {
+  const orc_dom* D = &s->d;
+  const double *un = s->f.u, *vn = s->f.v, *wn = s->f.w, *r = s->f.r, *nuT = s->f.nuT;
+  const double *rhon = s->f.rho, *bg = s->f.densityBG;
+  const double rRe = s->rRe, g = s->gnow;
+  memset(Wt, 0, sizeof(double) * D->G);
+  const int sx = 2, ex = D->nx + 1, sy = 2, ey = D->ny + 1, sz = 2, ez = D->nz + 1;
+  const int kend = ez - s->p.ew; /* k = sz..ez-EW */
+  for (int k = sz; k <= kend; ++k)
+    for (int j = sy; j <= ey; ++j)
+      for (int i = sx; i <= ex; ++i)
+        A_(Wt, i, j, k) = A_(Wt, i, j, k) +
+                          R12 * g *
+                              ((A_(rhon, i, j, k + 1) - A_(bg, i, j, k + 1)) +
+                               (A_(rhon, i, j, k) - A_(bg, i, j, k))) /
+                              (R12 * (A_(bg, i, j, k + 1) + A_(bg, i, j, k)));
+  for (int k = sz; k <= kend; ++k)
+    for (int j = sy; j <= ey; ++j)
+      for (int i = sx; i <= ex; ++i)
+        A_(Wt, i, j, k) = A_(Wt, i, j, k) +
+                          rRe * ((A_(wn, i + 1, j, k) - A_(wn, i, j, k)) * M(D->rdxe, i) -
+                                 (A_(wn, i, j, k) - A_(wn, i - 1, j, k)) * M(D->rdxe, i - 1)) *
+                              M(D->rdxc, i) +
+                          rRe * ((A_(wn, i, j + 1, k) - A_(wn, i, j, k)) * M(D->rdye, j) -
+                                 (A_(wn, i, j, k) - A_(wn, i, j - 1, k)) * M(D->rdye, j - 1)) *
+                              M(D->rdyc, j);
+  for (int k = sz; k <= kend; ++k)
+    for (int j = sy; j <= ey; ++j)
+      for (int i = sx; i <= ex; ++i) {
+        double wa1 = 0.5 * (A_(wn, i, j, k + 1) + A_(wn, i, j, k));
+        double wa2 = 0.5 * (A_(wn, i, j, k) + A_(wn, i, j, k - 1));
+        A_(Wt, i, j, k) = A_(Wt, i, j, k) -
+                          (A_(r, i, j, k) * wa1 * wa1 - A_(r, i, j, k + 1) * wa2 * wa2) * M(D->rdze, k) /
+                              (0.5 * (A_(r, i, j, k) + A_(r, i, j, k + 1)));
+        wa1 = 0.5 * (A_(wn, i + 1, j, k) + A_(wn, i, j, k));
+        wa2 = 0.5 * (A_(wn, i, j, k) + A_(wn, i - 1, j, k));
+        const double ua1 = 0.5 * (A_(un, i, j, k + 1) + A_(un, i, j, k));
+        const double ua2 = 0.5 * (A_(un, i - 1, j, k + 1) + A_(un, i - 1, j, k));
+        A_(Wt, i, j, k) = A_(Wt, i, j, k) - (ua1 * wa1 - ua2 * wa2) * M(D->rdxc, i);
+        wa1 = 0.5 * (A_(wn, i, j + 1, k) + A_(wn, i, j, k));
+        wa2 = 0.5 * (A_(wn, i, j, k) + A_(wn, i, j - 1, k));
+        const double va1 = 0.5 * (A_(vn, i, j, k + 1) + A_(vn, i, j, k));
+        const double va2 = 0.5 * (A_(vn, i, j - 1, k + 1) + A_(vn, i, j - 1, k));
+        A_(Wt, i, j, k) = A_(Wt, i, j, k) - (va1 * wa1 - va2 * wa2) * M(D->rdyc, j);
+      }
+  if (les_on(s)) {
+    for (int k = sz; k <= kend; ++k)
+      for (int j = sy; j <= ey; ++j)
+        for (int i = sx; i <= ex; ++i) {
+          double n1 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i - 1, j, k) + A_(nuT, i, j, k + 1) +
+                              A_(nuT, i - 1, j, k + 1));
+          double n2 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i + 1, j, k) + A_(nuT, i, j, k + 1) +
+                              A_(nuT, i + 1, j, k + 1));
+          A_(Wt, i, j, k) = A_(Wt, i, j, k) -
+                            1 * 1.0 *
+                                (n2 * (A_(wn, i + 1, j, k) - A_(wn, i, j, k)) * M(D->rdxe, i) -
+                                 n1 * (A_(wn, i, j, k) - A_(wn, i - 1, j, k)) * M(D->rdxe, i - 1)) *
+                                M(D->rdxc, i);
+          A_(Wt, i, j, k) = A_(Wt, i, j, k) -
+                            1 * 1.0 *
+                                (n2 * (A_(un, i + 1, j, k + 1) - A_(un, i + 1, j, k)) * M(D->rdze, k) -
+                                 n1 * (A_(un, i, j, k + 1) - A_(un, i, j, k)) * M(D->rdze, k)) *
+                                M(D->rdxc, i);
+          n1 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i, j - 1, k) + A_(nuT, i, j, k + 1) +
+                       A_(nuT, i, j - 1, k + 1));
+          n2 = 0.25 * (A_(nuT, i, j, k) + A_(nuT, i, j + 1, k) + A_(nuT, i, j, k + 1) +
+                       A_(nuT, i, j + 1, k + 1));
+          A_(Wt, i, j, k) = A_(Wt, i, j, k) -
+                            1 * 1.0 *
+                                (n2 * (A_(wn, i, j + 1, k) - A_(wn, i, j, k)) * M(D->rdye, j) -
+                                 n1 * (A_(wn, i, j, k) - A_(wn, i, j - 1, k)) * M(D->rdye, j - 1)) *
+                                M(D->rdyc, j);
+          A_(Wt, i, j, k) = A_(Wt, i, j, k) -
+                            1 * 1.0 *
+                                (n2 * (A_(vn, i, j + 1, k + 1) - A_(vn, i, j + 1, k)) * M(D->rdze, k) -
+                                 n1 * (A_(vn, i, j, k + 1) - A_(vn, i, j, k)) * M(D->rdze, k)) *
+                                M(D->rdyc, j);
+        }
+  }
+  ghost(s, Wt, VT_WTEMP);
+}
+
+/* ------------------------------------------------ rho_rhs / scal1_rhs
+ * NSsolver.F90:1667-1838 and 1841-2020.  The scalar LES term keeps the
+ * reference's sign slip nappaT(i)-nappaT(i-1) in the lower-face average
+ * (:1970,1975). */
+static void scalar_rhs(orc_ns* s, double* St, int is_rho) {
+  const orc_dom* D = &s->d;
+  const double *un = s->f.u, *vn = s->f.v, *wn = s->f.w, *r = s->f.r;
+  const double* c = is_rho ? s->f.rho : s->f.scal1;
+  const double* kT = is_rho ? s->f.kappaT : s->f.nappaT;
+  const double Dk = is_rho ? s->rRe * s->rPr : s->rRe * s->rSc;
+  const int model = is_rho ? s->p.rmodel : s->p.smodel;
+  memset(St, 0, sizeof(double) * D->G);
+  const int sx = 2, ex = D->nx + 1, sy = 2, ey = D->ny + 1, sz = 2, ez = D->nz + 1;
+  for (int k = sz; k <= ez; ++k)
+    for (int j = sy; j <= ey; ++j)
+      for (int i = sx; i <= ex; ++i)
+        A_(St, i, j, k) = A_(St, i, j, k) +
+                          Dk * ((A_(c, i + 1, j, k) - A_(c, i, j, k)) * M(D->rdxe, i) -
+                                (A_(c, i, j, k) - A_(c, i - 1, j, k)) * M(D->rdxe, i - 1)) *
+                              M(D->rdxc, i) +
+                          Dk * ((A_(c, i, j + 1, k) - A_(c, i, j, k)) * M(D->rdye, j) -
+                                (A_(c, i, j, k) - A_(c, i, j - 1, k)) * M(D->rdye, j - 1)) *
+                              M(D->rdyc, j);
+  for (int k = sz; k <= ez; ++k)
+    for (int j = sy; j <= ey; ++j)
+      for (int i = sx; i <= ex; ++i) {
+        double c2 = 0.5 * (A_(c, i + 1, j, k) + A_(c, i, j, k));
+        double c1 = 0.5 * (A_(c, i, j, k) + A_(c, i - 1, j, k));
+        A_(St, i, j, k) =
+            A_(St, i, j, k) + (A_(un, i - 1, j, k) * c1 - A_(un, i, j, k) * c2) * M(D->rdxc, i);
+        c2 = 0.5 * (A_(c, i, j + 1, k) + A_(c, i, j, k));
+        c1 = 0.5 * (A_(c, i, j, k) + A_(c, i, j - 1, k));
+        A_(St, i, j, k) =
+            A_(St, i, j, k) + (A_(vn, i, j - 1, k) * c1 - A_(vn, i, j, k) * c2) * M(D->rdyc, j);
+        c2 = 0.5 * (A_(c, i, j, k + 1) + A_(c, i, j, k));
+        c1 = 0.5 * (A_(c, i, j, k) + A_(c, i, j, k - 1));
+        if (is_rho) {
+          const double ra2 = 0.5 * (A_(r, i, j, k + 1) + A_(r, i, j, k));
+          const double ra1 = 0.5 * (A_(r, i, j, k) + A_(r, i, j, k - 1));
+          A_(St, i, j, k) = A_(St, i, j, k) + (ra1 * A_(wn, i, j, k - 1) * c1 -
+                                               ra2 * A_(wn, i, j, k) * c2) *
+                                                  M(D->rdzc, k) / A_(r, i, j, k);
+        } else {
+          A_(St, i, j, k) =
+              A_(St, i, j, k) + (A_(wn, i, j, k - 1) * c1 - A_(wn, i, j, k) * c2) * M(D->rdzc, k);
+        }
+      }
+  if (model == ANEL_MODEL_SSM) {
+    for (int k = sz; k <= ez; ++k)
+      for (int j = sy; j <= ey; ++j)
+        for (int i = sx; i <= ex; ++i) {
+          double k2 = 0.5 * (A_(kT, i + 1, j, k) + A_(kT, i, j, k));
+          double k1 = is_rho ? 0.5 * (A_(kT, i, j, k) + A_(kT, i - 1, j, k))
+                             : 0.5 * (A_(kT, i, j, k) - A_(kT, i - 1, j, k));
+          A_(St, i, j, k) = A_(St, i, j, k) -
+                            1 * 1.0 *
+                                (k2 * (A_(c, i + 1, j, k) - A_(c, i, j, k)) * M(D->rdxe, i) -
+                                 k1 * (A_(c, i, j, k) - A_(c, i - 1, j, k)) * M(D->rdxe, i - 1)) *
+                                M(D->rdxc, i);
+          k2 = 0.5 * (A_(kT, i, j + 1, k) + A_(kT, i, j, k));
+          k1 = is_rho ? 0.5 * (A_(kT, i, j, k) + A_(kT, i, j - 1, k))
+                      : 0.5 * (A_(kT, i, j, k) - A_(kT, i, j - 1, k));
+          A_(St, i, j, k) = A_(St, i, j, k) -
+                            1 * 1.0 *
+                                (k2 * (A_(c, i, j + 1, k) - A_(c, i, j, k)) * M(D->rdye, j) -
+                                 k1 * (A_(c, i, j, k) - A_(c, i, j - 1, k)) * M(D->rdye, j - 1)) *
+                                M(D->rdyc, j);
+        }
+  }
+  ghost(s, St, is_rho ? VT_RTEMP : VT_SCAL1TEMP);
+}
+
+/* var_advance (NSsolver.F90:2225-2264), interior only */
+static void var_advance(const orc_ns* s, const double* v1, double* v2, double f1, double f2, double f3) {
+  const orc_dom* D = &s->d;
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i)
+        A_(v2, i, j, k) = f1 * A_(v2, i, j, k) + f2 * A_(v1, i, j, k) * f3;
+}
+
+/* Thomas of mg_relax.F90:541-595 (a, b overwritten, c untouched) */
+static void thomas_ns(double* a, double* b, const double* c, double* G, int n) {
+  for (int j = 1; j <= n - 1; ++j) {
+    a[j] = -a[j] / b[j - 1];
+    b[j] = b[j] + a[j] * c[j - 1];
+    G[j] = G[j] + a[j] * G[j - 1];
+  }
+  G[n - 1] = G[n - 1] / b[n - 1];
+  for (int j = n - 1; j >= 1; --j) G[j - 1] = (G[j - 1] - c[j - 1] * G[j]) / b[j - 1];
+}
+
+/* -------------------------------------------------- var_advance_CN_PL
+ * NSsolver.F90:3054-3465 with f1 = 1, f3 = 1 (as rk_ss calls it),
+ * Deddy = 0 (:3116), pcorrect = .false..  var: 1 u, 2 v, 3 w, 5 rho,
+ * 8 scal1.  The sub/sup/diag/rhs arrays are built over the ghosted (i,j)
+ * range, ghosted as 'cfluc', given the wall rows, then solved by Thomas
+ * over k = 1..nz+2 per interior column. */
+static void cn_pl(orc_ns* s, const double* q, double* u, double a3, double rkdt, int var) {
+  const orc_dom* D = &s->d;
+  const double* r = s->f.r;
+  const double rRe = s->rRe;
+  double *sub = s->work[0], *diag = s->work[1], *sup = s->work[2], *rhs = s->work[3];
+  const long G = D->G;
+  memset(sub, 0, sizeof(double) * G);
+  memset(sup, 0, sizeof(double) * G);
+  memset(diag, 0, sizeof(double) * G);
+  memset(rhs, 0, sizeof(double) * G);
+  const int sz = 2, ez = D->nz + 1;
+  const double H = (double)(float)0.5; /* REAL(4) literal 0.5 (exact) */
+  const int les = les_on(s);
+  const double* kT = (var == 5) ? s->f.kappaT : (var == 8) ? s->f.nappaT : s->f.nuT;
+  /* the LES block of var_advance_CN_PL is gated on Vmodel for every
+   * variable, scalars included (NSsolver.F90:3160-3190) */
+  const int les_var = les;
+  for (long j = 1; j <= D->Y; ++j)
+    for (long i = 1; i <= D->X; ++i) {
+      if (var != 3) {
+        for (int k = sz; k <= ez; ++k) {
+          double t1, t2;
+          const double ra1 = H * (A_(r, i, j, k + 1) + A_(r, i, j, k));
+          const double ra2 = H * (A_(r, i, j, k) + A_(r, i, j, k - 1));
+          if (var == 1 || var == 2) {
+            t1 = (rRe + 0.0) * ra1 / A_(r, i, j, k);
+            t2 = (rRe + 0.0) * ra2 / A_(r, i, j, k);
+          } else if (var == 5) {
+            t1 = (rRe * s->rPr + 0.0) * ra1 / A_(r, i, j, k);
+            t2 = (rRe * s->rPr + 0.0) * ra2 / A_(r, i, j, k);
+          } else {
+            t1 = rRe * s->rSc + 0.0;
+            t2 = rRe * s->rSc + 0.0;
+          }
+          A_(sub, i, j, k) = -0.5 * rkdt * t1 * M(D->rdze, k - 1) * M(D->rdzc, k);
+          A_(sup, i, j, k) = -0.5 * rkdt * t2 * M(D->rdze, k) * M(D->rdzc, k);
+          A_(diag, i, j, k) =
+              1.0 + 0.5 * rkdt * (t1 * M(D->rdze, k - 1) + t2 * M(D->rdze, k)) * M(D->rdzc, k);
+        }
+        if (les_var && i >= 1 && j >= 1) {
+          for (int k = sz; k <= ez; ++k) {
+            const double ra1 = H * (A_(r, i, j, k + 1) + A_(r, i, j, k));
+            const double ra2 = H * (A_(r, i, j, k) + A_(r, i, j, k - 1));
+            double t1, t2;
+            if (var == 1) {
+              t1 = -0.25 * (A_(kT, i, j, k) + A_(kT, i + 1 <= D->X ? i + 1 : i, j, k) +
+                            A_(kT, i, j, k - 1) + A_(kT, i + 1 <= D->X ? i + 1 : i, j, k - 1)) *
+                   ra1 / A_(r, i, j, k);
+              t2 = -0.25 * (A_(kT, i, j, k) + A_(kT, i + 1 <= D->X ? i + 1 : i, j, k) +
+                            A_(kT, i, j, k + 1) + A_(kT, i + 1 <= D->X ? i + 1 : i, j, k + 1)) *
+                   ra2 / A_(r, i, j, k);
+            } else if (var == 2) {
+              t1 = -0.25 * (A_(kT, i, j, k) + A_(kT, i, j + 1 <= D->Y ? j + 1 : j, k) +
+                            A_(kT, i, j, k - 1) + A_(kT, i, j + 1 <= D->Y ? j + 1 : j, k - 1)) *
+                   ra1 / A_(r, i, j, k);
+              t2 = -0.25 * (A_(kT, i, j, k) + A_(kT, i, j + 1 <= D->Y ? j + 1 : j, k) +
+                            A_(kT, i, j, k + 1) + A_(kT, i, j + 1 <= D->Y ? j + 1 : j, k + 1)) *
+                   ra2 / A_(r, i, j, k);
+            } else if (var == 5) {
+              t1 = -0.5 * (A_(kT, i, j, k) + A_(kT, i, j, k - 1)) * ra1 / A_(r, i, j, k);
+              t2 = -0.5 * (A_(kT, i, j, k) + A_(kT, i, j, k + 1)) * ra2 / A_(r, i, j, k);
+            } else {
+              t1 = -0.5 * (A_(kT, i, j, k) + A_(kT, i, j, k - 1));
+              t2 = -0.5 * (A_(kT, i, j, k) + A_(kT, i, j, k + 1));
+            }
+            A_(sub, i, j, k) = A_(sub, i, j, k) - 1 * 0.5 * rkdt * t1 * M(D->rdze, k - 1) * M(D->rdzc, k);
+            A_(sup, i, j, k) = A_(sup, i, j, k) - 1 * 0.5 * rkdt * t2 * M(D->rdze, k) * M(D->rdzc, k);
+            A_(diag, i, j, k) = A_(diag, i, j, k) + 1 * 0.5 * rkdt *
+                                                        (t1 * M(D->rdze, k - 1) + t2 * M(D->rdze, k)) *
+                                                        M(D->rdzc, k);
+          }
+        }
+      } else {
+        for (int k = sz; k <= ez; ++k) {
+          const double t1 = (rRe + 0.0) * A_(r, i, j, k) / (H * (A_(r, i, j, k + 1) + A_(r, i, j, k)));
+          const double t2 =
+              (rRe + 0.0) * A_(r, i, j, k + 1) / (H * (A_(r, i, j, k + 1) + A_(r, i, j, k)));
+          A_(sub, i, j, k) = -0.5 * rkdt * t1 * M(D->rdze, k) * M(D->rdzc, k);
+          A_(sup, i, j, k) = -0.5 * rkdt * t2 * M(D->rdze, k) * M(D->rdzc, k + 1);
+          A_(diag, i, j, k) =
+              1.0 + 0.5 * rkdt * (t1 * M(D->rdzc, k) + t2 * M(D->rdzc, k + 1)) * M(D->rdze, k);
+        }
+        if (les) {
+          for (int k = sz; k <= ez; ++k) {
+            const double t1 =
+                -A_(kT, i, j, k) * A_(r, i, j, k) / (H * (A_(r, i, j, k + 1) + A_(r, i, j, k)));
+            const double t2 =
+                -A_(kT, i, j, k + 1) * A_(r, i, j, k + 1) / (H * (A_(r, i, j, k + 1) + A_(r, i, j, k)));
+            A_(sub, i, j, k) = A_(sub, i, j, k) - 1 * 1.0 * rkdt * t1 * M(D->rdze, k) * M(D->rdzc, k);
+            A_(sup, i, j, k) =
+                A_(sup, i, j, k) - 1 * 1.0 * rkdt * t2 * M(D->rdze, k) * M(D->rdzc, k + 1);
+            A_(diag, i, j, k) = A_(diag, i, j, k) + 1 * 1.0 * rkdt *
+                                                        (t1 * M(D->rdzc, k) + t2 * M(D->rdzc, k + 1)) *
+                                                        M(D->rdze, k);
+          }
+        }
+      }
+    }
+  /* right-hand side (:3185-3296) */
+  for (long j = 1; j <= D->Y; ++j)
+    for (long i = 1; i <= D->X; ++i)
+      for (int k = sz; k <= ez; ++k) {
+        A_(rhs, i, j, k) = 1.0 * A_(u, i, j, k) + a3 * A_(q, i, j, k) * 1.0;
+        if (var != 3) {
+          const double ra1 = H * (A_(r, i, j, k + 1) + A_(r, i, j, k));
+          const double ra2 = H * (A_(r, i, j, k) + A_(r, i, j, k - 1));
+          double t1, t2;
+          if (var == 1 || var == 2) {
+            t1 = (rRe + 0.0) * ra1 / A_(r, i, j, k);
+            t2 = (rRe + 0.0) * ra2 / A_(r, i, j, k);
+          } else if (var == 5) {
+            t1 = (rRe * s->rPr + 0.0) * ra1 / A_(r, i, j, k);
+            t2 = (rRe * s->rPr + 0.0) * ra2 / A_(r, i, j, k);
+          } else {
+            t1 = rRe * s->rSc + 0.0;
+            t2 = rRe * s->rSc + 0.0;
+          }
+          A_(rhs, i, j, k) =
+              A_(rhs, i, j, k) +
+              rkdt * 0.5 *
+                  (t2 * (A_(u, i, j, k + 1) - A_(u, i, j, k)) * M(D->rdze, k) -
+                   t1 * (A_(u, i, j, k) - A_(u, i, j, k - 1)) * M(D->rdze, k - 1)) *
+                  M(D->rdzc, k);
+          if (les_var) {
+            if (var == 1) {
+              const long ip = i + 1 <= D->X ? i + 1 : i;
+              t1 = -0.25 * (A_(kT, i, j, k) + A_(kT, ip, j, k) + A_(kT, i, j, k - 1) + A_(kT, ip, j, k - 1)) *
+                   ra1 / A_(r, i, j, k);
+              t2 = -0.25 * (A_(kT, i, j, k) + A_(kT, ip, j, k) + A_(kT, i, j, k + 1) + A_(kT, ip, j, k + 1)) *
+                   ra2 / A_(r, i, j, k);
+            } else if (var == 2) {
+              const long jp = j + 1 <= D->Y ? j + 1 : j;
+              t1 = -0.25 * (A_(kT, i, j, k) + A_(kT, i, jp, k) + A_(kT, i, j, k - 1) + A_(kT, i, jp, k - 1)) *
+                   ra1 / A_(r, i, j, k);
+              t2 = -0.25 * (A_(kT, i, j, k) + A_(kT, i, jp, k) + A_(kT, i, j, k + 1) + A_(kT, i, jp, k + 1)) *
+                   ra2 / A_(r, i, j, k);
+            } else if (var == 5) {
+              t1 = -0.5 * (A_(kT, i, j, k) + A_(kT, i, j, k - 1)) * ra1 / A_(r, i, j, k);
+              t2 = -0.5 * (A_(kT, i, j, k) + A_(kT, i, j, k + 1)) * ra2 / A_(r, i, j, k);
+            } else {
+              t1 = -0.5 * (A_(kT, i, j, k) + A_(kT, i, j, k - 1));
+              t2 = -0.5 * (A_(kT, i, j, k) + A_(kT, i, j, k + 1));
+            }
+            A_(rhs, i, j, k) =
+                A_(rhs, i, j, k) +
+                1 * rkdt * 0.5 *
+                    (t2 * (A_(u, i, j, k + 1) - A_(u, i, j, k)) * M(D->rdze, k) -
+                     t1 * (A_(u, i, j, k) - A_(u, i, j, k - 1)) * M(D->rdze, k - 1)) *
+                    M(D->rdzc, k);
+          }
+        } else {
+          const double t1 = (rRe + 0.0) * A_(r, i, j, k) / (H * (A_(r, i, j, k + 1) + A_(r, i, j, k)));
+          const double t2 =
+              (rRe + 0.0) * A_(r, i, j, k + 1) / (H * (A_(r, i, j, k + 1) + A_(r, i, j, k)));
+          A_(rhs, i, j, k) =
+              A_(rhs, i, j, k) +
+              rkdt * 0.5 *
+                  (t2 * (A_(u, i, j, k + 1) - A_(u, i, j, k)) * M(D->rdzc, k + 1) -
+                   t1 * (A_(u, i, j, k) - A_(u, i, j, k - 1)) * M(D->rdzc, k)) *
+                  M(D->rdze, k);
+          if (les) {
+            const double u1 = -A_(kT, i, j, k) * A_(r, i, j, k) / (H * (A_(r, i, j, k + 1) + A_(r, i, j, k)));
+            const double u2 =
+                -A_(kT, i, j, k + 1) * A_(r, i, j, k + 1) / (H * (A_(r, i, j, k + 1) + A_(r, i, j, k)));
+            A_(rhs, i, j, k) =
+                A_(rhs, i, j, k) +
+                1 * rkdt * 1.0 *
+                    (u2 * (A_(u, i, j, k + 1) - A_(u, i, j, k)) * M(D->rdzc, k + 1) -
+                     u1 * (A_(u, i, j, k) - A_(u, i, j, k - 1)) * M(D->rdzc, k)) *
+                    M(D->rdze, k);
+          }
+        }
+      }
+  ghost(s, sub, VT_CFLUC);
+  ghost(s, diag, VT_CFLUC);
+  ghost(s, sup, VT_CFLUC);
+  ghost(s, rhs, VT_CFLUC);
+  /* wall rows (:3297-3429) */
+  const int tbmin = s->p.tb[2][0][var - 1], tbmax = s->p.tb[2][1][var - 1];
+  const double vbmin = s->p.vb[2][0][var - 1], vbmax = s->p.vb[2][1][var - 1];
+  for (long j = 1; j <= D->Y; ++j)
+    for (long i = 1; i <= D->X; ++i) {
+#define SET(k, a, b, c, d) \
+  do {                     \
+    A_(sub, i, j, k) = a;  \
+    A_(diag, i, j, k) = b; \
+    A_(sup, i, j, k) = c;  \
+    A_(rhs, i, j, k) = d;  \
+  } while (0)
+      if (tbmin == 1) SET(sz - 1, 0.0, 1.0, 0.0, vbmin);
+      else if (tbmin == 2) {
+        if (var == 3) SET(sz - 1, 0.0, -1.0, 1.0, M(D->dzc, sz - 1) * vbmin);
+        else if (var == 5 || var == 8) {
+          SET(sz - 1, 0.0, -1.0, 1.0, M(D->dze, sz - 1) * vbmin);
+          SET(sz, 0.0, -1.0, 1.0, M(D->dze, sz) * vbmin);
+        } else SET(sz - 1, 0.0, -1.0, 1.0, M(D->dze, sz - 1) * vbmin);
+      } else if (tbmin == 6) SET(sz - 1, 0.0, 1.0, 1.0, 2.0 * vbmin);
+      if (tbmax == 1) SET(ez + 1, 0.0, 1.0, 0.0, vbmax);
+      else if (tbmax == 2) {
+        if (var == 3) SET(ez + 1, -1.0, 1.0, 0.0, M(D->dzc, ez + 1) * vbmax);
+        else if (var == 5 || var == 8) {
+          SET(ez + 1, -1.0, 1.0, 0.0, M(D->dze, ez + 1) * vbmax);
+          SET(ez, -1.0, 1.0, 0.0, M(D->dze, ez) * vbmax);
+        } else SET(ez + 1, -1.0, 1.0, 0.0, M(D->dze, ez + 1) * vbmax);
+      } else if (tbmax == 6) SET(ez + 1, 1.0, 1.0, 0.0, 2.0 * vbmax);
+      else if (tbmax == 7) {
+        SET(ez + 1, 0.0, 1.0, 0.0, 0.0);
+        SET(ez, 0.0, 1.0, 0.0, 0.0);
+      }
+#undef SET
+    }
+  /* Thomas per interior column over k = 1..nz+2 (:3431-3436) */
+  const int n = D->nz + 2;
+  double* a = (double*)malloc(sizeof(double) * 4 * n);
+  double *b = a + n, *cc = b + n, *gg = cc + n;
+  for (int j = 2; j <= D->ny + 1; ++j)
+    for (int i = 2; i <= D->nx + 1; ++i) {
+      for (int k = 1; k <= n; ++k) {
+        a[k - 1] = A_(sub, i, j, k);
+        b[k - 1] = A_(diag, i, j, k);
+        cc[k - 1] = A_(sup, i, j, k);
+        gg[k - 1] = A_(rhs, i, j, k);
+      }
+      thomas_ns(a, b, cc, gg, n);
+      for (int k = 1; k <= n; ++k) A_(rhs, i, j, k) = gg[k - 1];
+    }
+  free(a);
+  ghost(s, rhs, var == 1 ? VT_U : var == 2 ? VT_V : var == 3 ? VT_W : var == 5 ? VT_RHO : VT_SCAL1);
+  memcpy(u, rhs, sizeof(double) * G);
+}
+
+/* ---------------------------------------------------------------- Psource
+ * NSsolver.F90:2167-2223 */
+static void psource(orc_ns* s, double* SRC, double dt) {
+  const orc_dom* D = &s->d;
+  const double *U = s->f.u, *V = s->f.v, *W = s->f.w, *r = s->f.r;
+  const double H = (double)(float)0.5;
+  memset(SRC, 0, sizeof(double) * D->G);
+  const double rdt = 1.0 / dt;
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i)
+        A_(SRC, i, j, k) =
+            A_(SRC, i, j, k) +
+            ((A_(r, i, j, k) * A_(U, i, j, k) - A_(r, i, j, k) * A_(U, i - 1, j, k)) * M(D->rdxc, i) +
+             (A_(r, i, j, k) * A_(V, i, j, k) - A_(r, i, j, k) * A_(V, i, j - 1, k)) * M(D->rdyc, j) +
+             (H * (A_(r, i, j, k + 1) + A_(r, i, j, k)) * A_(W, i, j, k) -
+              H * (A_(r, i, j, k) + A_(r, i, j, k - 1)) * A_(W, i, j, k - 1)) *
+                 M(D->rdzc, k)) *
+                rdt;
+  ghost(s, SRC, VT_PSOURCE);
+}
+
+/* ---------------------------------------------------------------- Pgrad
+ * NSsolver.F90:2023-2085 */
+static void pgrad(orc_ns* s, double dt) {
+  const orc_dom* D = &s->d;
+  const double *pn = s->f.p, *r = s->f.r;
+  double *U = s->f.u, *V = s->f.v, *W = s->f.w;
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i)
+        A_(U, i, j, k) = A_(U, i, j, k) - (A_(pn, i + 1, j, k) / A_(r, i, j, k) -
+                                           A_(pn, i, j, k) / A_(r, i, j, k)) *
+                                              M(D->rdxe, i) * dt;
+  ghost(s, U, VT_UTEMP);
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i)
+        A_(V, i, j, k) = A_(V, i, j, k) - (A_(pn, i, j + 1, k) / A_(r, i, j, k) -
+                                           A_(pn, i, j, k) / A_(r, i, j, k)) *
+                                              M(D->rdye, j) * dt;
+  ghost(s, V, VT_VTEMP);
+  for (int k = 2; k <= D->nz + 1 - s->p.ew; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i)
+        A_(W, i, j, k) = A_(W, i, j, k) - (A_(pn, i, j, k + 1) / A_(r, i, j, k + 1) -
+                                           A_(pn, i, j, k) / A_(r, i, j, k)) *
+                                              M(D->rdze, k) * dt;
+  ghost(s, W, VT_WTEMP);
+}
+
+/* ---------------------------------------------------------------- rk_ss
+ * NSsolver.F90:418-583 (RK3CN branch). */
+int orc_ns_substep(orc_ns* s, double a1, double a2, double a3, double dt_rk, double dt, int* iters,
+                   double* relmax) {
+  const orc_dom* D = &s->d;
+  anel_fields* f = &s->f;
+  memset(f->psrc, 0, sizeof(double) * D->G);
+  u1_rhs(s, s->Ftemp);
+  var_advance(s, s->Ftemp, f->q_u, a1, a2, dt);
+  u2_rhs(s, s->Ftemp);
+  var_advance(s, s->Ftemp, f->q_v, a1, a2, dt);
+  u3_rhs(s, s->Ftemp);
+  var_advance(s, s->Ftemp, f->q_w, a1, a2, dt);
+  scalar_rhs(s, s->Ftemp, 1);
+  var_advance(s, s->Ftemp, f->q_rho, a1, a2, dt);
+  scalar_rhs(s, s->Ftemp, 0);
+  var_advance(s, s->Ftemp, f->q_s, a1, a2, dt);
+  ghost(s, f->q_u, VT_UTEMP);
+  ghost(s, f->q_v, VT_VTEMP);
+  ghost(s, f->q_w, VT_WTEMP);
+  ghost(s, f->q_rho, VT_RTEMP);
+  ghost(s, f->q_s, VT_S1TEMP);
+  cn_pl(s, f->q_u, f->u, a3, dt_rk, 1);
+  cn_pl(s, f->q_v, f->v, a3, dt_rk, 2);
+  cn_pl(s, f->q_w, f->w, a3, dt_rk, 3);
+  memset(f->psrc, 0, sizeof(double) * D->G);
+  psource(s, f->psrc, dt_rk);
+  cn_pl(s, f->q_rho, f->rho, a3, dt_rk, 5);
+  cn_pl(s, f->q_s, f->scal1, a3, dt_rk, 8);
+  /* Ftemp = p ; mg_solver(Ftemp, r_tmp1, niters, resmax) ; p = Ftemp */
+  memcpy(s->Ftemp, f->p, sizeof(double) * D->G);
+  orc_mg_set_density(s->mg, f->r);
+  orc_mg_solve(s->mg, s->Ftemp, f->psrc, iters, relmax);
+  memcpy(f->p, s->Ftemp, sizeof(double) * D->G);
+  pgrad(s, dt_rk);
+  ghost(s, f->q_u, VT_UTEMP);
+  ghost(s, f->q_v, VT_VTEMP);
+  ghost(s, f->q_w, VT_WTEMP);
+  ghost(s, f->u, VT_U);
+  ghost(s, f->v, VT_V);
+  ghost(s, f->w, VT_W);
+  ghost(s, f->rho, VT_RHO);
+  ghost(s, f->scal1, VT_SCAL1);
+  return 0;
+}
+
+/* ---------------------------------------------------------------- calcdt
+ * Routines.F90:186-258 and NSsolver.F90:72-73 */
+static double calcdt(const orc_ns* s) {
+  const orc_dom* D = &s->d;
+  const double *u = s->f.u, *v = s->f.v, *w = s->f.w;
+  double mx = 0.0;
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i) {
+        const double adv = M(D->rdxc, i) * fabs(0.5 * (A_(u, i, j, k) + A_(u, i - 1, j, k))) +
+                           M(D->rdzc, k) * fabs(0.5 * (A_(w, i, j, k) + A_(w, i, j, k - 1))) +
+                           M(D->rdyc, j) * fabs(0.5 * (A_(v, i, j, k) + A_(v, i, j - 1, k)));
+        mx = mx > adv ? mx : adv;
+      }
+  double dt = s->p.cfl / mx;
+  if (dt >= s->p.dtmax) dt = s->p.dtmax;
+  return dt;
+}
+
+/* gravity ramp, Routines.F90:27-52 */
+static void gravity(orc_ns* s) {
+  const double t = s->time, t1 = s->p.gt1, t2 = s->p.gt2;
+  if (t < t1) s->gnow = 0.0;
+  else if (t > t1 && t < t2) s->gnow = s->g_orig * (t - t1) / (t2 - t1);
+  else if (t >= t2) s->gnow = s->g_orig;
+}
+
+/* straincal modS (straincal.F90:48-73) and delg (:126-134) */
+static void straincal(orc_ns* s) {
+  const orc_dom* D = &s->d;
+  const double *l1 = s->f.u, *l2 = s->f.v, *l3 = s->f.w;
+  double* modS = s->modS;
+  memset(modS, 0, sizeof(double) * D->G);
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i) {
+        const double TS11 = (A_(l1, i + 1, j, k) - A_(l1, i, j, k)) * M(D->rdxc, i);
+        const double TS22 = (A_(l2, i, j + 1, k) - A_(l2, i, j, k)) * M(D->rdyc, j);
+        const double TS33 = (A_(l3, i, j, k + 1) - A_(l3, i, j, k)) * M(D->rdzc, k);
+        double t1 = 0.25 * (A_(l1, i, j, k) + A_(l1, i + 1, j, k) + A_(l1, i, j + 1, k) + A_(l1, i + 1, j + 1, k));
+        double t2 = 0.25 * (A_(l1, i, j, k) + A_(l1, i + 1, j, k) + A_(l1, i, j - 1, k) + A_(l1, i + 1, j - 1, k));
+        double t3 = 0.25 * (A_(l2, i, j, k) + A_(l2, i, j + 1, k) + A_(l2, i + 1, j, k) + A_(l2, i + 1, j + 1, k));
+        double t4 = 0.25 * (A_(l2, i, j, k) + A_(l2, i, j + 1, k) + A_(l2, i - 1, j, k) + A_(l2, i - 1, j + 1, k));
+        const double TS12 = 0.5 * ((t1 - t2) * M(D->rdyc, j) + (t3 - t4) * M(D->rdxc, i));
+        t1 = 0.25 * (A_(l1, i, j, k) + A_(l1, i + 1, j, k) + A_(l1, i, j, k + 1) + A_(l1, i + 1, j, k + 1));
+        t2 = 0.25 * (A_(l1, i, j, k) + A_(l1, i + 1, j, k) + A_(l1, i, j, k - 1) + A_(l1, i + 1, j, k - 1));
+        t3 = 0.25 * (A_(l3, i, j, k) + A_(l3, i, j, k + 1) + A_(l3, i + 1, j, k) + A_(l3, i + 1, j, k + 1));
+        t4 = 0.25 * (A_(l3, i, j, k) + A_(l3, i, j, k + 1) + A_(l3, i - 1, j, k) + A_(l3, i - 1, j, k + 1));
+        const double TS13 = 0.5 * ((t1 - t2) * M(D->rdzc, k) + (t3 - t4) * M(D->rdxc, i));
+        t1 = 0.25 * (A_(l2, i, j, k) + A_(l2, i, j + 1, k) + A_(l2, i, j, k + 1) + A_(l2, i, j + 1, k + 1));
+        t2 = 0.25 * (A_(l2, i, j, k) + A_(l2, i, j + 1, k) + A_(l2, i, j, k - 1) + A_(l2, i, j + 1, k - 1));
+        t3 = 0.25 * (A_(l3, i, j, k) + A_(l3, i, j, k + 1) + A_(l3, i, j + 1, k) + A_(l3, i, j + 1, k + 1));
+        t4 = 0.25 * (A_(l3, i, j, k) + A_(l3, i, j, k + 1) + A_(l3, i, j - 1, k) + A_(l3, i, j - 1, k + 1));
+        const double TS23 = 0.5 * ((t1 - t2) * M(D->rdzc, k) + (t3 - t4) * M(D->rdyc, j));
+        /* x**2.d0 is evaluated as x*x */
+        A_(modS, i, j, k) = sqrt(2.0) * sqrt(TS11 * TS11 + TS22 * TS22 + TS33 * TS33 + 2.0 * (TS12 * TS12) +
+                                             2.0 * (TS13 * TS13) + 2.0 * (TS23 * TS23));
+      }
+  ghost(s, modS, VT_CFLUC);
+}
+
+/* grid-only LES quantities: delg (straincal.F90:126-134) and the model
+ * coefficients Csgs/CTsgs/CSsgs (SSM.F90:27,60,97) */
+static void les_coeffs(orc_ns* s) {
+  const orc_dom* D = &s->d;
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i) {
+        double dg;
+        if (s->p.les_delta == ANEL_DELTA_3ROOT)
+          dg = pow(M(D->dxc, i) * M(D->dyc, j) * M(D->dzc, k), 1.0 / 3.0);
+        else
+          dg = pow(M(D->dxc, i) * M(D->dxc, i) + M(D->dyc, j) * M(D->dyc, j) + M(D->dzc, k) * M(D->dzc, k),
+                   1.0 / 2.0);
+        A_(s->delg, i, j, k) = dg;
+        const double c = s->p.ssm_const;
+        double damp_u, damp_t;
+        if (s->p.les_damp == ANEL_DAMP_LITERAL) {
+          const double k41 = (double)(float)0.41;
+          const double zo_u = 0.3, zo_t = (double)(float)0.3; /* 0.3d0 in SSM, 0.3 in SSMrho */
+          const double a = k41 * (M(D->zc, k) + zo_u);
+          damp_u = (a * a) / ((a * a) + c * (dg * dg));
+          const double b = k41 * (M(D->zc, k) + zo_t);
+          damp_t = (b * b) / ((b * b) + c * (dg * dg));
+        } else {
+          damp_u = 1.0;
+          damp_t = 1.0;
+        }
+        A_(s->Csgs, i, j, k) = c * damp_u;
+        A_(s->CTsgs, i, j, k) = A_(s->Csgs, i, j, k) / s->p.pr_sgs * damp_t;
+        A_(s->CSsgs, i, j, k) = A_(s->Csgs, i, j, k) / s->p.pr_sgs * damp_u;
+      }
+  ghost(s, s->delg, VT_CFLUC);
+  ghost(s, s->Csgs, VT_CFLUC);
+  ghost(s, s->CTsgs, VT_CFLUC);
+  ghost(s, s->CSsgs, VT_CFLUC);
+}
+
+/* SGSdiff (straincal.F90:339-414): nuT, kappaT, nappaT */
+static void sgsdiff(orc_ns* s) {
+  const orc_dom* D = &s->d;
+  straincal(s);
+  double* outs[3] = {s->f.nuT, s->f.kappaT, s->f.nappaT};
+  const double* C[3] = {s->Csgs, s->CTsgs, s->CSsgs};
+  for (int q = 0; q < 3; ++q) {
+    double* o = outs[q];
+    memset(o, 0, sizeof(double) * D->G);
+    for (int k = 2; k <= D->nz + 1; ++k)
+      for (int j = 2; j <= D->ny + 1; ++j)
+        for (int i = 2; i <= D->nx + 1; ++i)
+          A_(o, i, j, k) = -(A_(C[q], i, j, k) + 0.0) * (A_(s->delg, i, j, k) * A_(s->delg, i, j, k)) *
+                               A_(s->modS, i, j, k) +
+                           0.0;
+    ghost(s, o, VT_CFLUC);
+  }
+}
+
+/* One NSsolver time step (NSsolver.F90:63-283 minus output/statistics). */
+int orc_ns_step(orc_ns* s, anel_step_report* rep) {
+  const orc_dom* D = &s->d;
+  anel_fields* f = &s->f;
+  const long G = D->G;
+  memset(f->q_u, 0, sizeof(double) * G);
+  memset(f->q_v, 0, sizeof(double) * G);
+  memset(f->q_w, 0, sizeof(double) * G);
+  memset(f->psrc, 0, sizeof(double) * G);
+  memset(f->q_rho, 0, sizeof(double) * G);
+  memset(f->q_s, 0, sizeof(double) * G);
+  const double delt = calcdt(s);
+  gravity(s);
+  const int les = s->p.vmodel == ANEL_MODEL_SSM;
+  if (les && s->nstep >= s->p.les_start && s->nstep % s->p.les_freq == 0) les_coeffs(s);
+  static const double A1[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+  static const double A3[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+  const double DTR[3] = {1.0 / 3.0 * delt, 5.0 / 12.0 * delt, 1.0 / 4.0 * delt};
+  int it[3];
+  double rm[3];
+  for (int q = 0; q < 3; ++q) {
+    if (les && s->nstep > s->p.les_start) sgsdiff(s);
+    orc_ns_substep(s, A1[q], 1.0, A3[q], DTR[q], delt, &it[q], &rm[q]);
+  }
+  s->time = s->time + delt;
+  if (rep) {
+    rep->nstep = s->nstep;
+    rep->dt = delt;
+    rep->time = s->time;
+    for (int q = 0; q < 3; ++q) {
+      rep->mg_iter[q] = it[q];
+      rep->mg_relmax[q] = rm[q];
+    }
+  }
+  s->nstep += 1;
+  return 0;
+}
+
+/* Projection of the initial field (not a reference routine: the
+ * shear-layer benchmark starts from a divergence-free field): Psource
+ * with dt = 1, one MG solve from p, Pgrad with dt = 1, velocity ghosts. */
+int orc_ns_project(orc_ns* s, int* iters, double* relmax) {
+  const orc_dom* D = &s->d;
+  anel_fields* f = &s->f;
+  memset(f->psrc, 0, sizeof(double) * D->G);
+  psource(s, f->psrc, 1.0);
+  memcpy(s->Ftemp, f->p, sizeof(double) * D->G);
+  orc_mg_set_density(s->mg, f->r);
+  orc_mg_solve(s->mg, s->Ftemp, f->psrc, iters, relmax);
+  memcpy(f->p, s->Ftemp, sizeof(double) * D->G);
+  pgrad(s, 1.0);
+  ghost(s, f->u, VT_U);
+  ghost(s, f->v, VT_V);
+  ghost(s, f->w, VT_W);
+  return 0;
+}
+
+/* ghost() of one field by type name index (tests) */
+void orc_ns_ghost(orc_ns* s, double* var, int vt) { ghost(s, var, vt); }
+
+/* divergence (Routines.F90:54-183): out[0] avg, out[1] max |div| */
+void orc_ns_divergence(orc_ns* s, double* out) {
+  const orc_dom* D = &s->d;
+  const double *u = s->f.u, *v = s->f.v, *w = s->f.w;
+  double sum = 0.0, vol = 0.0, mx = 0.0;
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i) {
+        const double d = (A_(u, i, j, k) - A_(u, i - 1, j, k)) * M(D->rdxc, i) +
+                         (A_(v, i, j, k) - A_(v, i, j - 1, k)) * M(D->rdyc, j) +
+                         (A_(w, i, j, k) - A_(w, i, j, k - 1)) * M(D->rdzc, k);
+        if (fabs(d) > mx) mx = fabs(d);
+        sum = sum + fabs(d) / (M(D->rdxc, i) * M(D->rdyc, j) * M(D->rdzc, k));
+        vol = vol + 1.0 / (M(D->rdxc, i) * M(D->rdyc, j) * M(D->rdzc, k));
+      }
+  out[0] = sum / vol;
+  out[1] = mx;
+}

@@ -51,6 +51,23 @@ double orc_mg_true_resid(orc_mg* m, const double* phi, const double* f);
 /* Apply the fine operator: out(interior) = A phi (phi ghosts must be set). */
 void orc_mg_apply(orc_mg* m, const double* phi, double* out);
 
+/* ---- RK3 stepper (ns_oracle.c) ---- */
+typedef struct orc_ns orc_ns;
+orc_ns* orc_ns_create(const anel_grid_desc* g, const anel_mg_params* mgp, const anel_ns_params* np,
+                      int* stat);
+void orc_ns_destroy(orc_ns* s);
+/* the oracle works in place on the caller's host arrays */
+void orc_ns_bind(orc_ns* s, const anel_fields* f);
+void orc_ns_set_clock(orc_ns* s, double time, int nstep);
+int orc_ns_substep(orc_ns* s, double a1, double a2, double a3, double dt_rk, double dt, int* iters,
+                   double* relmax);
+int orc_ns_step(orc_ns* s, anel_step_report* rep);
+int orc_ns_project(orc_ns* s, int* iters, double* relmax);
+void orc_ns_divergence(orc_ns* s, double* out);
+/* vt: 0 u 1 v 2 w 3 p 4 rho 5 cfluc 6 psource 7 utemp 8 vtemp 9 wtemp
+ *     10 rtemp 11 s1temp 12 scal1 13 scal1temp */
+void orc_ns_ghost(orc_ns* s, double* var, int vt);
+
 #ifdef __cplusplus
 }
 #endif

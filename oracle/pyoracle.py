@@ -101,3 +101,76 @@ class OracleMG:
         out = np.zeros_like(phi, order="F")
         lib().orc_mg_apply(self._h, abi.dptr(_f(phi)), abi.dptr(out))
         return out
+
+
+def _ns_lib():
+    L = lib()
+    if not hasattr(L, "_ns_ready"):
+        L.orc_ns_create.restype = C.c_void_p
+        L.orc_ns_create.argtypes = [C.POINTER(abi.GridDesc), C.POINTER(abi.MGParams),
+                                    C.POINTER(abi.NSParams), C.POINTER(C.c_int)]
+        L.orc_ns_destroy.argtypes = [C.c_void_p]
+        L.orc_ns_bind.argtypes = [C.c_void_p, C.POINTER(abi.Fields)]
+        L.orc_ns_set_clock.argtypes = [C.c_void_p, C.c_double, C.c_int]
+        L.orc_ns_substep.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double,
+                                     C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.orc_ns_step.argtypes = [C.c_void_p, C.POINTER(abi.StepReport)]
+        L.orc_ns_project.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.orc_ns_divergence.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+        L.orc_ns_ghost.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
+        L._ns_ready = True
+    return L
+
+
+class OracleNS:
+    """rk_ss / NSsolver of the reference on the CPU, in place on a dict of
+    Fortran-ordered host fields (names of abi.FIELD_NAMES)."""
+
+    def __init__(self, grid, mgp: abi.MGParams, nsp: abi.NSParams, fields: dict):
+        L = _ns_lib()
+        self._desc, self._keep = abi.make_grid_desc(grid)
+        st = C.c_int(0)
+        self._h = L.orc_ns_create(C.byref(self._desc), C.byref(mgp), C.byref(nsp), C.byref(st))
+        if st.value != 0:
+            raise ValueError(f"oracle NS init failed, stat={st.value}")
+        self.fields = fields
+        fs = abi.Fields()
+        for n in abi.FIELD_NAMES:
+            a = fields.get(n)
+            if a is not None:
+                setattr(fs, n, abi.dptr(_f(a)))
+        self._fs = fs
+        L.orc_ns_bind(self._h, C.byref(fs))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _ns_lib().orc_ns_destroy(self._h)
+            self._h = None
+
+    def set_clock(self, time: float, nstep: int):
+        _ns_lib().orc_ns_set_clock(self._h, time, nstep)
+
+    def substep(self, a1, a2, a3, dt_rk, dt):
+        it = C.c_int(0)
+        rm = C.c_double(0)
+        _ns_lib().orc_ns_substep(self._h, a1, a2, a3, dt_rk, dt, C.byref(it), C.byref(rm))
+        return it.value, rm.value
+
+    def step(self) -> abi.StepReport:
+        rep = abi.StepReport()
+        _ns_lib().orc_ns_step(self._h, C.byref(rep))
+        return rep
+
+    def project(self):
+        it = C.c_int(0)
+        rm = C.c_double(0)
+        _ns_lib().orc_ns_project(self._h, C.byref(it), C.byref(rm))
+        return it.value, rm.value
+
+    def divergence(self):
+        out = (C.c_double * 2)()
+        _ns_lib().orc_ns_divergence(self._h, out)
+        return out[0], out[1]
+
+    def ghost(self, a, vt: int):
+        _ns_lib().orc_ns_ghost(self._h, abi.dptr(_f(a)), vt)

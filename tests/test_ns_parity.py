@@ -1,0 +1,150 @@
+"""GPU RK3 stepper vs the CPU oracle (rk_ss / NSsolver restatement).
+
+FP64 with the FP64 multigrid: bit-identical fields after sub-steps and
+full steps, for both settings of the w edge-node flag.  Mixed-precision
+multigrid: velocity and density within 1e-8 relative L2 of the FP64
+oracle after the step count, pressure within 1e-9 after removing the mean.
+"""
+import numpy as np
+import pytest
+
+from anelastic_solve_b200 import abi, shear
+from anelastic_solve_b200 import grid as G
+from anelastic_solve_b200.ns import RK3, NSSolver
+from oracle.pyoracle import OracleNS
+
+from .helpers import levels_for, rel_l2, remove_mean
+
+pytestmark = pytest.mark.gpu
+
+CMP = ("u", "v", "w", "p", "rho", "scal1")
+
+
+def setup_case(n=(32, 16, 32), ew=1, precision=abi.PREC_FP64, tol=1e-10, mode=abi.MODE_METRIC,
+               scal1_on=1, Re=1000.0, g=-0.12):
+    g_ = G.shear_layer_grid(*n, stretched=True)
+    mgp = abi.make_mg_params(levels_for(g_), maxcy=200, tolmax=tol, pre=2, post=2,
+                             tbc=(0, 1, 0, 1, 0, 0), mode=mode, stop=abi.STOP_RESID,
+                             precision=abi.PREC_FP64)
+    nsp = abi.make_ns_params(Re=Re, Pr=1.0, g=g, dtmax=0.01, ew=ew, scal1_on=scal1_on)
+    f = shear.shear_layer_fields(g_)
+    o = OracleNS(g_, mgp, nsp, f)
+    for name, vt in (("u", 0), ("v", 1), ("w", 2), ("rho", 4), ("scal1", 12)):
+        o.ghost(f[name], vt)
+    o.project()
+    start = {k: v.copy(order="F") for k, v in f.items()}
+    mgp_gpu = abi.make_mg_params(levels_for(g_), maxcy=200, tolmax=tol, pre=2, post=2,
+                                 tbc=(0, 1, 0, 1, 0, 0), mode=mode, stop=abi.STOP_RESID,
+                                 precision=precision)
+    s = NSSolver(g_, mgp_gpu, nsp)
+    s.set_fields({k: start[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
+    return g_, o, s, f, start
+
+
+@pytest.mark.parametrize("ew", [1, 0])
+def test_substeps_bitwise(ew):
+    g_, o, s, f, start = setup_case(ew=ew)
+    dt = 0.01
+    for q, (a1, a2, a3, ec, fr) in enumerate(RK3):
+        it_o, _ = o.substep(a1, a2, a3, fr * dt, dt)
+        it_g, _ = s.substep(a1, a2, a3, fr * dt, dt)
+        got = s.get_fields(CMP + ("q_u", "q_v", "q_w", "q_rho"))
+        for name in CMP:
+            np.testing.assert_array_equal(got[name], f[name], err_msg=f"{name} after sub-step {q}")
+        for name in ("q_u", "q_v", "q_w", "q_rho"):
+            np.testing.assert_array_equal(got[name][1:-1, 1:-1, 1:-1], f[name][1:-1, 1:-1, 1:-1],
+                                          err_msg=f"{name} after sub-step {q}")
+        assert it_o == it_g
+
+
+@pytest.mark.parametrize("ew", [1, 0])
+def test_steps_bitwise(ew):
+    g_, o, s, f, start = setup_case(ew=ew)
+    for n in range(3):
+        ro = o.step()
+        rg = s.step(1)
+        assert ro.dt == rg.dt and ro.time == rg.time
+        assert list(ro.mg_iter) == list(rg.mg_iter)
+    got = s.get_fields(CMP)
+    for name in CMP:
+        np.testing.assert_array_equal(got[name], f[name], err_msg=name)
+
+
+def test_divergence_bound_after_steps():
+    """north_star bound: max|div u| <= 1e-10 max|u| / dz_min (ew = 1)."""
+    g_, o, s, f, start = setup_case(ew=1)
+    rep = s.step(3)
+    got = s.get_fields(("u", "v", "w"))
+    umax = max(np.abs(got[k][1:-1, 1:-1, 1:-1]).max() for k in ("u", "v", "w"))
+    dzmin = g_.z.dxc[1:-1].min()
+    assert rep.max_div <= 1e-10 * umax / dzmin, (rep.max_div, umax, dzmin)
+    avg, mx = s.divergence()
+    assert mx == rep.max_div
+
+
+def test_scal1_off_matches_reference_zero_scalar():
+    g_, o, s, f, start = setup_case(scal1_on=0)
+    for n in range(2):
+        o.step()
+        s.step(1)
+    got = s.get_fields(CMP)
+    for name in ("u", "v", "w", "p", "rho"):
+        np.testing.assert_array_equal(got[name], f[name], err_msg=name)
+    assert not np.any(got["scal1"]) and not np.any(f["scal1"])
+
+
+def test_dropin_rk_substep_equals_context():
+    """anel_ns_init / anel_bind_fields / anel_rk_substep (host arrays, the
+    reference's rk_ss argument list) give the same fields."""
+    import ctypes as C
+
+    from anelastic_solve_b200 import _lib
+
+    g_, o, s, f, start = setup_case()
+    L = _lib.lib()
+    desc, keep = abi.make_grid_desc(g_)
+    _lib.check(L.anel_ns_init(C.byref(desc), C.byref(s.mgp), C.byref(s.nsp)))
+    host = {k: v.copy(order="F") for k, v in start.items()}
+    fs = abi.Fields()
+    for n in abi.FIELD_NAMES:
+        if n in host and n not in ("nuT", "kappaT", "nappaT"):
+            setattr(fs, n, abi.dptr(host[n]))
+    _lib.check(L.anel_bind_fields(C.byref(fs)))
+    dt = 0.01
+    for (a1, a2, a3, ec, fr) in RK3:
+        args = [C.c_double(x) for x in (a1, a2, a3, ec, fr * dt, dt)]
+        ps = C.c_int32(1)
+        st = C.c_int32(-99)
+        L.anel_rk_substep(*[C.byref(a) for a in args], C.byref(ps), C.byref(st))
+        assert st.value == 0, _lib.last_error()
+        s.substep(a1, a2, a3, fr * dt, dt)
+    got = s.get_fields(CMP)
+    for name in CMP:
+        np.testing.assert_array_equal(host[name], got[name], err_msg=name)
+    L.anel_ns_finalize()
+
+
+def test_shear_layer_config0_20_steps():
+    """64x32x64 shear layer, Re=1000, Pr=1, Ri=0.12, 20 steps at dt=0.01, MG
+    to relative residual 1e-10 each sub-step: FP64 GPU == oracle bitwise."""
+    g_, o, s, f, start = setup_case(n=(64, 32, 64))
+    for n in range(20):
+        o.step()
+    s.step(20)
+    got = s.get_fields(CMP)
+    for name in CMP:
+        np.testing.assert_array_equal(got[name], f[name], err_msg=name)
+
+
+def test_mixed_precision_stepper_within_tolerance():
+    """Mixed-precision MG inside the projection (config 2/3 form): fields
+    within 1e-8 rel L2 of the FP64 oracle after 5 steps; MG solved to
+    1e-12 so the projection error stays below the tolerance."""
+    g_, o, s, f, start = setup_case(precision=abi.PREC_MIXED, tol=1e-12)
+    for n in range(5):
+        o.step()
+    s.step(5)
+    got = s.get_fields(CMP)
+    for name in ("u", "v", "w", "rho"):
+        assert rel_l2(got[name], f[name]) < 1e-8, name
+    assert rel_l2(remove_mean(got["p"]), remove_mean(f["p"])) < 1e-9
