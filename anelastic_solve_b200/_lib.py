@@ -43,6 +43,7 @@ SIGNATURES = {
                                       C.c_double, _P, _IP, _DP]),
     "anel_ns_ctx_step": (C.c_int, [_P, C.c_int32, _P, C.POINTER(abi.StepReport)]),
     "anel_ns_ctx_set_clock": (C.c_int, [_P, C.c_double, C.c_int32]),
+    "anel_ns_ctx_set_profiling": (C.c_int, [_P, C.c_int32]),
     "anel_ns_ctx_project": (C.c_int, [_P, _IP, _DP]),
     "anel_ns_ctx_divergence": (C.c_int, [_P, _DP]),
     "anel_ns_init": (C.c_int, [C.POINTER(abi.GridDesc), C.POINTER(abi.MGParams),

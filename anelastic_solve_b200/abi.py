@@ -143,7 +143,9 @@ FIELD_NAMES = [n for n, _ in Fields._fields_]
 class StepReport(C.Structure):
     _fields_ = [("nstep", C.c_int32), ("mg_iter", C.c_int32 * 3), ("dt", C.c_double),
                 ("time", C.c_double), ("mg_relmax", C.c_double * 3), ("max_div", C.c_double),
-                ("avg_div", C.c_double), ("ms", C.c_double)]
+                ("avg_div", C.c_double), ("ms", C.c_double), ("mg_ms", C.c_double),
+                ("launches", C.c_int64), ("fine_sweeps", C.c_int32), ("reserved", C.c_int32),
+                ("fine_sweep_ms", C.c_double)]
 
 
 def free_slip_bcs(p: NSParams, rho_value=(0.0, 0.0)):

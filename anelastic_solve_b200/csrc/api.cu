@@ -190,6 +190,11 @@ int anel_ns_ctx_step(anel_ns_ctx* ctx, int32_t nsteps, void* stream, anel_step_r
   return ctx->s->step(nsteps, static_cast<cudaStream_t>(stream), report);
 }
 
+int anel_ns_ctx_set_profiling(anel_ns_ctx* ctx, int32_t on) {
+  if (!ctx) return ANEL_ERR_ARG;
+  return ctx->s->mg()->set_profiling(on != 0);
+}
+
 int anel_ns_ctx_set_clock(anel_ns_ctx* ctx, double time, int32_t nstep) {
   if (!ctx) return ANEL_ERR_ARG;
   ctx->s->set_clock(time, nstep);

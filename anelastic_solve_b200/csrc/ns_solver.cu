@@ -398,6 +398,9 @@ int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, 
   anel_mg_report rep{};
   const int st = mg_->solve_device(D_.p, D_.psrc, s, &rep);
   if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
+  acc_mg_ms_ += rep.ms;
+  acc_sweep_ms_ += rep.fine_sweep_ms;
+  acc_sweeps_ += rep.fine_sweeps;
   launch_pgrad(D_, dt_rk, ru, rv, rw, s);
   if (iters) *iters = rep.iter;
   if (relmax) *relmax = rep.relmax;
@@ -424,6 +427,9 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   static const double A1[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
   static const double A3[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
   anel_step_report r{};
+  acc_mg_ms_ = acc_sweep_ms_ = 0.0;
+  acc_sweeps_ = 0;
+  const int64_t launches0 = g_launches.load();
   ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
   for (int n = 0; n < nsteps; ++n) {
     // zero_temps (memManage.F90:844-853)
@@ -452,6 +458,10 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ev0_, ev1_);
   r.ms = ms;
+  r.mg_ms = acc_mg_ms_;
+  r.fine_sweep_ms = acc_sweep_ms_;
+  r.fine_sweeps = acc_sweeps_;
+  r.launches = g_launches.load() - launches0;
   double dv[2];
   const int st = divergence(s, dv);
   if (st != ANEL_OK) return st;

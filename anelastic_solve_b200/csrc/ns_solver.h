@@ -64,6 +64,9 @@ class NSSolver {
   double* h_red_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   CNFacHost fac(int slot, int vi) const;
+  // multigrid totals of the current step() call
+  double acc_mg_ms_ = 0.0, acc_sweep_ms_ = 0.0;
+  int acc_sweeps_ = 0;
 };
 
 }  // namespace anel

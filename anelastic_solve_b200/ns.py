@@ -82,6 +82,9 @@ class NSSolver:
         check(lib().anel_ns_ctx_step(self._h, int(n), s, C.byref(rep)))
         return rep
 
+    def set_profiling(self, on: bool):
+        check(lib().anel_ns_ctx_set_profiling(self._h, 1 if on else 0))
+
     def set_clock(self, time: float, nstep: int):
         check(lib().anel_ns_ctx_set_clock(self._h, float(time), int(nstep)))
 

@@ -18,36 +18,32 @@ _A = 16807
 
 
 def park_miller(seed: int, n: int) -> np.ndarray:
-    """n uniform numbers in (0,1) from the minimal standard generator."""
+    """n uniform numbers in (0,1) from the minimal standard generator,
+    computed in blocks: x_{b+t} = x_b * a^t mod m."""
     out = np.empty(n, dtype=np.float64)
     x = int(seed) % _M or 1
-    # vectorised by jumping: a^k mod m for a block of k values
-    blk = 4096
-    powers = np.empty(blk, dtype=np.int64)
+    blk = 1 << 16
+    pw = np.empty(blk, dtype=np.int64)
     p = 1
-    for q in range(blk):
+    for t in range(blk):
         p = (p * _A) % _M
-        powers[q] = p
-    a_blk = int(powers[-1])
-    pw = powers.astype(object)
+        pw[t] = p  # a^(t+1)
     q = 0
     while q < n:
         m = min(blk, n - q)
-        vals = (np.array([(x * int(pw[t])) % _M for t in range(m)], dtype=np.float64)
-                if m < 64 else _block(x, powers[:m]))
+        vals = _mulmod(x, pw[:m])
         out[q:q + m] = vals / _M
-        x = (x * (a_blk if m == blk else int(powers[m - 1]))) % _M
+        x = int(vals[-1])
         q += m
     return out
 
 
-def _block(x: int, powers: np.ndarray) -> np.ndarray:
-    # (x * p) mod m without overflow: split x into 16-bit halves
+def _mulmod(x: int, powers: np.ndarray) -> np.ndarray:
+    """(x * p) mod (2^31-1) for an int64 array p, without overflow."""
     x_hi, x_lo = x >> 16, x & 0xFFFF
-    hi = (powers * x_hi) % _M
-    hi = (hi * 65536) % _M
+    hi = ((powers * x_hi) % _M) * 65536 % _M
     lo = (powers * x_lo) % _M
-    return ((hi + lo) % _M).astype(np.float64)
+    return (hi + lo) % _M
 
 
 def shear_layer_fields(grid, amp: float = 1e-3, seed: int = 12345, zmax: float = 2.0):

@@ -1,22 +1,28 @@
 #!/usr/bin/env python
 """Benchmark of the B200 hot path (one JSON line on rank 0).
 
-Workload "poisson" (default): standalone pressure-Poisson solves on the
-512x256x512 staggered shear-layer grid (domain 4pi x 2pi x 20, periodic
-x/y, Neumann z walls, z tanh-stretched), right-hand side = divergence-like
-seeded N(0,1) field with the volume mean removed, phi0 = 0, solved to a
-true relative residual ||f - A phi||/||f|| <= 1e-10.  One step = one solve.
+Workload "dns" (default): the DNS shear layer on the 512x256x512
+staggered grid (domain 4pi x 2pi x 20, periodic x/y, free-slip z walls, z
+tanh-stretched), Re=4000, Pr=1, Ri=0.08, seeded perturbation 1e-3, time
+step from CFL 0.5 (calcdt); every sub-step projects with the mixed-precision
+multigrid (FP32 V-cycles inside FP64 defect correction) to a true relative
+residual of 1e-10.  One step = one full RK3 time step (three sub-steps,
+three projections).  Fields are FP64.
 
-  value  -- cell-solves/s: interior cells x solves / device time, inputs
-            resident in HBM (CUDA events on the solve stream, max over ranks)
-  e2e    -- the same through the C-ABI with host (pinned) buffers: the
-            host->device copy of phi0 and f and the device->host copy of
-            phi are inside the timed region
-  roofline -- the dominant kernel (finest-level red-black smoother):
-            algorithmic bytes per launch / mean launch time (CUDA events)
+  value    -- cell-updates/s: interior cells x steps / device time, state
+              resident in HBM (CUDA events on the step stream, max over ranks)
+  e2e      -- the same through the C-ABI with the state in pinned host
+              memory: every step copies u, v, w, p, rho host->device, runs
+              the step and copies them back
+  roofline -- the dominant kernel (finest-level red-black smoother of the
+              pressure solves): algorithmic bytes per launch / mean launch
+              time (CUDA events on its stream)
+
+Workload "poisson": standalone pressure solves of the same grid (one step
+= one solve to 1e-10 from phi0 = 0).
 
 --impl reference times the CPU restatement of the same algorithm (the
-reference cannot be built here) on the host cores instead.
+Fortran reference cannot be built here) on the host cores instead.
 N > 1 GPUs (torchrun): independent replicas, no collective on the data path.
 """
 from __future__ import annotations
@@ -38,10 +44,13 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOADS = {
-    # name: (nx, ny, nz, levels)
-    "poisson": (512, 256, 512, (9, 8, 9)),
-    "poisson256": (256, 256, 256, (8, 8, 8)),
-    "poisson_small": (64, 32, 64, (6, 5, 6)),
+    # name: kind, (nx, ny, nz), MG levels, physics
+    "dns": ("dns", (512, 256, 512), (9, 8, 9), dict(Re=4000.0, g=-0.08, amp=1e-3, cfl=0.5)),
+    "dns256": ("dns", (256, 256, 256), (8, 8, 8), dict(Re=4000.0, g=-0.08, amp=1e-3, cfl=0.5)),
+    "dns_small": ("dns", (64, 32, 64), (6, 5, 6), dict(Re=1000.0, g=-0.12, amp=1e-3, cfl=0.5)),
+    "poisson": ("poisson", (512, 256, 512), (9, 8, 9), {}),
+    "poisson256": ("poisson", (256, 256, 256), (8, 8, 8), {}),
+    "poisson_small": ("poisson", (64, 32, 64), (6, 5, 6), {}),
 }
 TOL = 1e-10
 
@@ -113,43 +122,63 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_problem(workload):
-    from anelastic_solve_b200 import grid as G
+def mg_params(lv, precision, mode=None):
+    from anelastic_solve_b200 import abi
 
-    nx, ny, nz, lv = WORKLOADS[workload]
-    g = G.shear_layer_grid(nx, ny, nz, stretched=True)
+    return abi.make_mg_params(lv, maxcy=400, tolmax=TOL, pre=2, post=2, tbc=(0, 1, 0, 1, 0, 0),
+                              precision=precision,
+                              mode=abi.MODE_METRIC if mode is None else mode, stop=abi.STOP_RESID)
+
+
+def ns_params(phys):
+    from anelastic_solve_b200 import abi
+
+    # DeltaT_max large: the CFL condition sets the step (calcdt)
+    return abi.make_ns_params(Re=phys["Re"], Pr=1.0, g=phys["g"], cfl=phys["cfl"], dtmax=1e9,
+                              ew=1, scal1_on=0)
+
+
+def poisson_rhs(g):
+    """Seeded N(0,1) right-hand side with the volume mean removed (the
+    compatibility condition of the Neumann/periodic problem)."""
     rng = np.random.default_rng(1)
     f = rng.standard_normal(g.ghosted[::-1])  # (Z,Y,X) C-order == Fortran (X,Y,Z)
     vol = (g.z.dxc[1:-1, None, None] * g.y.dxc[None, 1:-1, None] * g.x.dxc[None, None, 1:-1])
     inner = f[1:-1, 1:-1, 1:-1]
     inner -= (inner * vol).sum() / vol.sum()
-    return g, lv, f
+    return f
 
 
-def mg_params(lv, precision, mode):
-    from anelastic_solve_b200 import abi
+def initial_state(g, phys):
+    from anelastic_solve_b200 import shear
 
-    return abi.make_mg_params(lv, maxcy=400, tolmax=TOL, pre=2, post=2, tbc=(0, 1, 0, 1, 0, 0),
-                              precision=precision, mode=mode, stop=abi.STOP_RESID)
+    return shear.shear_layer_fields(g, amp=phys["amp"], seed=12345)
 
 
-# ----------------------------------------------------------------- ours
-def run_ours(args, rank, world, local_rank):
+STATE = ("u", "v", "w", "p", "rho")
+
+
+# ---------------------------------------------------------------- ours: dns
+def run_dns(args, rank, world, local_rank):
     import torch
 
     from anelastic_solve_b200 import _lib, abi
+    from anelastic_solve_b200 import grid as G
     from anelastic_solve_b200.mg import MGSolver
+    from anelastic_solve_b200.ns import NSSolver
 
+    kind, n, lv, phys = WORKLOADS[args.workload]
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    g, lv, f = make_problem(args.workload)
+    g = G.shear_layer_grid(*n, stretched=True)
     N = g.x.n * g.y.n * g.z.n
     prec = abi.PREC_MIXED if args.prec == "mixed" else abi.PREC_FP64
-    mode = abi.MODE_METRIC if args.mode == "metric" else abi.MODE_LITERAL
-    s = MGSolver(g, mg_params(lv, prec, mode), device=local_rank)
+    s = NSSolver(g, mg_params(lv, prec), ns_params(phys), device=local_rank)
+    f = initial_state(g, phys)
+    s.set_fields({k: f[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
+    s.project()
     st = torch.cuda.Stream(device=dev)
-    dsrc = torch.from_numpy(f).to(dev)
-    dphi = torch.zeros_like(dsrc)
+    h = st.cuda_stream
 
     def barrier():
         if world > 1:
@@ -157,101 +186,192 @@ def run_ours(args, rank, world, local_rank):
 
             dist.barrier()
 
-    # warm-up
-    with torch.cuda.stream(st):
-        for _ in range(args.warmup):
-            dphi.zero_()
-            s.solve(dphi, dsrc, stream=st.cuda_stream)
-    st.synchronize()
-    # timed region (device-resident inputs)
+    for _ in range(args.warmup):
+        s.step(1, stream=h)
+    torch.cuda.synchronize()
     s.set_profiling(True)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    iters, resids, sweep_ms, sweeps = [], [], 0.0, 0
-    launches0 = _lib.launch_count()
+    reps = []
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local_rank) as clk:
-        with torch.cuda.stream(st):
-            ev0.record(st)
-            for _ in range(args.steps):
-                dphi.zero_()
-                s.solve(dphi, dsrc, stream=st.cuda_stream)
-                r = s.last_report
-                iters.append(r.iter)
-                resids.append(r.resid)
-                sweep_ms += r.fine_sweep_ms
-                sweeps += r.fine_sweeps
-            ev1.record(st)
+        torch.cuda.nvtx.range_push("timed")
+        ev0.record(st)
+        for _ in range(args.steps):
+            reps.append(s.step(1, stream=h))
+        ev1.record(st)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
     barrier()
-    launches = _lib.launch_count() - launches0
     s.set_profiling(False)
-    ms = ev0.elapsed_time(ev1)
-    # e2e: reference-facing call with host buffers (pinned), copies inside
-    if args.no_e2e:
-        return {"ms_step": ms / args.steps, "e2e_ms": float("nan"), "N": N, "iters": iters,
-                "resids": resids, "sweep_ms": sweep_ms, "sweeps": sweeps, "launches": launches,
-                "clocks": clk.summary(), "bytes_io": (2 * dsrc.numel() * 8, dsrc.numel() * 8)}
-    ph = torch.zeros(dsrc.shape, dtype=torch.float64).pin_memory()
-    fh = torch.from_numpy(f).pin_memory()
-    phn = np.asfortranarray(ph.numpy().T)
-    fhn = np.asfortranarray(fh.numpy().T)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(st):
-        s.solve(phn, fhn, stream=st.cuda_stream)  # warm
-        st.synchronize()
+    ms_step = ev0.elapsed_time(ev1) / args.steps
+    out = {"N": N, "ms_step": ms_step, "clocks": clk.summary(),
+           "launches": int(sum(r.launches for r in reps)),
+           "sweeps": int(sum(r.fine_sweeps for r in reps)),
+           "sweep_ms": float(sum(r.fine_sweep_ms for r in reps)),
+           "mg_ms_step": float(np.mean([r.mg_ms for r in reps])),
+           "mg_iters": [list(r.mg_iter) for r in reps],
+           "dt": reps[-1].dt, "max_div": reps[-1].max_div,
+           "umax": None}
+    # e2e: the state lives in pinned host memory; every step copies it in,
+    # runs through the C-ABI and copies it back
+    if not args.no_e2e:
+        host = {k: np.asfortranarray(torch.zeros(g.ghosted[::-1], dtype=torch.float64)
+                                     .pin_memory().numpy().T) for k in STATE}
+        s.get_into(host)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ne = max(1, args.steps // 2)
+        torch.cuda.synchronize()
         e0.record(st)
-        for _ in range(max(1, args.steps // 2)):
-            phn[...] = 0.0
-            s.solve(phn, fhn, stream=st.cuda_stream)
+        for _ in range(ne):
+            s.set_fields(host)
+            s.step(1, stream=h)
+            s.get_into(host)
         e1.record(st)
-    torch.cuda.synchronize()
-    e2e_steps = max(1, args.steps // 2)
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    ms_step = ms / args.steps
-    # max over ranks
+        torch.cuda.synchronize()
+        out["e2e_ms"] = e0.elapsed_time(e1) / ne
+        nb = len(STATE) * int(np.prod(g.ghosted)) * 8
+        out["bytes_io"] = (nb, nb)
+    # mixed vs FP64 multigrid on this workload's pressure equation: cold
+    # solves (phi0 = 0) of the last sub-step's right-hand side
+    if rank == 0 and not args.no_fp64:
+        fld = s.get_fields(("psrc",))
+        rhs = torch.from_numpy(np.ascontiguousarray(fld["psrc"].T)).to(dev)
+        mg = {}
+        for name, pr in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
+            m = MGSolver(g, mg_params(lv, pr), device=local_rank)
+            phi = torch.zeros_like(rhs)
+            m.solve(phi, rhs, stream=h)
+            phi.zero_()
+            m.solve(phi, rhs, stream=h)
+            r = m.last_report
+            mg[name] = {"ms": round(r.ms, 3), "iter": r.iter, "resid": r.resid}
+            m.close()
+        out["mg_cold"] = mg
+    fu = s.get_fields(("u", "v", "w"))
+    out["umax"] = float(max(np.abs(fu[k][1:-1, 1:-1, 1:-1]).max() for k in ("u", "v", "w")))
+    out["dzmin"] = float(g.z.dxc[1:-1].min())
+    s.close()
     if world > 1:
         import torch.distributed as dist
 
-        t = torch.tensor([ms_step, e2e_ms], device=dev, dtype=torch.float64)
+        t = torch.tensor([out["ms_step"], out.get("e2e_ms", 0.0)], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step, e2e_ms = float(t[0]), float(t[1])
-    out = {
-        "ms_step": ms_step, "e2e_ms": e2e_ms, "N": N, "iters": iters, "resids": resids,
-        "sweep_ms": sweep_ms, "sweeps": sweeps, "launches": launches,
-        "clocks": clk.summary(), "bytes_io": (2 * dsrc.numel() * 8, dsrc.numel() * 8),
-    }
-    # FP64 companion solve (mixed vs FP64 pair of the metric), rank 0 only
-    if rank == 0 and prec == abi.PREC_MIXED and not args.no_fp64:
-        s64 = MGSolver(g, mg_params(lv, abi.PREC_FP64, mode), device=local_rank)
+        out["ms_step"], out["e2e_ms"] = float(t[0]), float(t[1])
+    return out
+
+
+# ------------------------------------------------------------ ours: poisson
+def run_poisson(args, rank, world, local_rank):
+    import torch
+
+    from anelastic_solve_b200 import _lib, abi
+    from anelastic_solve_b200 import grid as G
+    from anelastic_solve_b200.mg import MGSolver
+
+    kind, n, lv, phys = WORKLOADS[args.workload]
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    g = G.shear_layer_grid(*n, stretched=True)
+    N = g.x.n * g.y.n * g.z.n
+    prec = abi.PREC_MIXED if args.prec == "mixed" else abi.PREC_FP64
+    s = MGSolver(g, mg_params(lv, prec), device=local_rank)
+    st = torch.cuda.Stream(device=dev)
+    f = poisson_rhs(g)
+    dsrc = torch.from_numpy(f).to(dev)
+    dphi = torch.zeros_like(dsrc)
+    for _ in range(args.warmup):
         with torch.cuda.stream(st):
             dphi.zero_()
-            s64.solve(dphi, dsrc, stream=st.cuda_stream)
-            dphi.zero_()
-            s64.solve(dphi, dsrc, stream=st.cuda_stream)
+        s.solve(dphi, dsrc, stream=st.cuda_stream)
+    st.synchronize()
+    s.set_profiling(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    iters, sweep_ms, sweeps = [], 0.0, 0
+    launches0 = _lib.launch_count()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.nvtx.range_push("timed")
+        ev0.record(st)
+        for _ in range(args.steps):
+            with torch.cuda.stream(st):
+                dphi.zero_()
+            s.solve(dphi, dsrc, stream=st.cuda_stream)
+            iters.append(s.last_report.iter)
+            sweep_ms += s.last_report.fine_sweep_ms
+            sweeps += s.last_report.fine_sweeps
+        ev1.record(st)
         torch.cuda.synchronize()
-        out["fp64"] = {"ms": s64.last_report.ms, "iter": s64.last_report.iter,
-                       "resid": s64.last_report.resid}
-        s64.close()
+        torch.cuda.nvtx.range_pop()
+    s.set_profiling(False)
+    out = {"N": N, "ms_step": ev0.elapsed_time(ev1) / args.steps, "clocks": clk.summary(),
+           "launches": _lib.launch_count() - launches0, "sweeps": sweeps, "sweep_ms": sweep_ms,
+           "iters": iters, "resid": s.last_report.resid}
+    if not args.no_e2e:
+        ph = np.asfortranarray(torch.zeros(dsrc.shape, dtype=torch.float64).pin_memory().numpy().T)
+        fh = np.asfortranarray(torch.from_numpy(f).pin_memory().numpy().T)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ne = max(1, args.steps // 2)
+        e0.record(st)
+        for _ in range(ne):
+            ph[...] = 0.0
+            s.solve(ph, fh, stream=st.cuda_stream)
+        e1.record(st)
+        torch.cuda.synchronize()
+        out["e2e_ms"] = e0.elapsed_time(e1) / ne
+        out["bytes_io"] = (2 * dsrc.numel() * 8, dsrc.numel() * 8)
     s.close()
     return out
 
 
-def cpu_sample(workload, mode, threads):
-    """One FP64 V-cycle of the oracle restatement on the host cores, at the
-    full workload size; returns seconds per V-cycle."""
+# ------------------------------------------------------------ CPU samples
+def cpu_sample_dns(workload, threads):
+    """One FP64 RK3 sub-step of the oracle restatement on the host cores at
+    the full workload size, from the projected initial state (the first
+    sub-step of step 1).  Returns (seconds, MG cycles, cells)."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from anelastic_solve_b200 import abi
+    from anelastic_solve_b200 import grid as G
+    from oracle.pyoracle import OracleNS
+
+    kind, n, lv, phys = WORKLOADS[workload]
+    g = G.shear_layer_grid(*n, stretched=True)
+    f = initial_state(g, phys)
+    o = OracleNS(g, mg_params(lv, abi.PREC_FP64), ns_params(phys), f)
+    for name, vt in (("u", 0), ("v", 1), ("w", 2), ("rho", 4), ("scal1", 12)):
+        o.ghost(f[name], vt)
+    o.project()
+    dt = cfl_dt(g, f, phys["cfl"])
+    t = time.perf_counter()
+    it, _ = o.substep(0.0, 1.0, 1.0 / 3.0, 1.0 / 3.0 * dt, dt)
+    return time.perf_counter() - t, it, g.x.n * g.y.n * g.z.n
+
+
+def cfl_dt(g, f, cfl):
+    """calcdt (Routines.F90:221-240) on host arrays."""
+    u, v, w = (f[k] for k in ("u", "v", "w"))
+    au = np.abs(0.5 * (u[1:-1, 1:-1, 1:-1] + u[:-2, 1:-1, 1:-1])) * g.x.rdxc[1:-1, None, None]
+    aw = np.abs(0.5 * (w[1:-1, 1:-1, 1:-1] + w[1:-1, 1:-1, :-2])) * g.z.rdxc[None, None, 1:-1]
+    av = np.abs(0.5 * (v[1:-1, 1:-1, 1:-1] + v[1:-1, :-2, 1:-1])) * g.y.rdxc[None, 1:-1, None]
+    return cfl / float((au + aw + av).max())
+
+
+def cpu_sample_poisson(workload, threads):
+    """One FP64 V-cycle of the oracle restatement at full size."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from anelastic_solve_b200 import abi
+    from anelastic_solve_b200 import grid as G
     from oracle.pyoracle import OracleMG
 
-    g, lv, f = make_problem(workload)
-    fF = np.asfortranarray(f.T)
-    p = mg_params(lv, abi.PREC_FP64, abi.MODE_METRIC if mode == "metric" else abi.MODE_LITERAL)
+    kind, n, lv, phys = WORKLOADS[workload]
+    g = G.shear_layer_grid(*n, stretched=True)
+    fF = np.asfortranarray(poisson_rhs(g).T)
+    p = mg_params(lv, abi.PREC_FP64)
     p.maxcy = 1
     p.tolmax = 0.0
     o = OracleMG(g, p)
     phi = np.zeros(g.ghosted, order="F")
-    o.solve(phi, fF.copy(order="F"))  # warm (first touch)
+    o.solve(phi, fF.copy(order="F"))
     t = time.perf_counter()
     o.solve(phi, fF.copy(order="F"))
     return time.perf_counter() - t, g.x.n * g.y.n * g.z.n
@@ -263,49 +383,62 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="poisson", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="dns", choices=sorted(WORKLOADS))
     ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--mode", default="metric", choices=["metric", "literal"])
-    ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 multigrid companion")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
-    nx, ny, nz, lv = WORKLOADS[args.workload]
-    config = {"workload": f"pressure-Poisson solve {nx}x{ny}x{nz}, tanh-stretched z, periodic x/y, "
-                          f"Neumann z, to ||f-A phi||/||f|| <= {TOL:g}",
-              "grid": [nx, ny, nz], "mg_levels": list(lv), "smoother": "RBPGS V(2,2)",
-              "mode": args.mode, "precision": args.prec,
-              "parallelism": f"replicas x{args.gpus}",
-              "l2": "inputs larger than L2 (545 MB per FP64 field)" if args.workload == "poisson"
-              else "small workload"}
-    metric = "MG solve throughput to 1e-10 relative residual (cell-solves/s)"
+    kind, n, lv, phys = WORKLOADS[args.workload]
+    nx, ny, nz = n
+    if kind == "dns":
+        metric = "cell-updates/s (RK3 step incl. 3 projections)"
+        unit = "cell-updates/s"
+        config = {"workload": f"DNS shear layer {nx}x{ny}x{nz}: Re={phys['Re']:g}, Pr=1, "
+                              f"Ri={-phys['g']:g}, amp {phys['amp']:g}, CFL {phys['cfl']:g}, "
+                              f"MG to ||f-A p||/||f|| <= {TOL:g} each sub-step",
+                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"RBPGS V(2,2), metric, {args.prec}",
+                  "ew": 1, "scal1": "off (zero)", "parallelism": f"replicas x{args.gpus}",
+                  "l2": "inputs larger than L2 (545 MB per FP64 field)" if nx >= 256 else "small"}
+    else:
+        metric = "MG solve throughput to 1e-10 relative residual (cell-solves/s)"
+        unit = "cell-solves/s"
+        config = {"workload": f"pressure-Poisson solve {nx}x{ny}x{nz}, tanh-stretched z, periodic "
+                              f"x/y, Neumann z, to ||f-A phi||/||f|| <= {TOL:g} from phi0 = 0",
+                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"RBPGS V(2,2), metric, {args.prec}",
+                  "parallelism": f"replicas x{args.gpus}",
+                  "l2": "inputs larger than L2 (545 MB per FP64 field)" if nx >= 256 else "small"}
+    threads = os.cpu_count() or 1
     if args.impl == "reference":
         if rank != 0:
             return
-        threads = os.cpu_count() or 1
-        sec_cyc, N = cpu_sample(args.workload, args.mode, threads)
-        cyc = FP64_CYCLES.get((args.workload, args.mode))
-        steps = []
-        for _ in range(args.warmup + args.steps):
-            t, _ = cpu_sample(args.workload, args.mode, threads)
-            steps.append(t)
-        sec_cyc = float(np.mean(steps[args.warmup:]))
-        value = N / (sec_cyc * cyc) if cyc else None
-        line = {"impl": "reference", "metric": metric, "value": value, "unit": "cell-solves/s",
-                "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": sec_cyc * cyc * 1e3 if cyc else None, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": config,
-                "cpu_baseline": {"value": value, "unit": "cell-solves/s", "cores": threads,
-                                 "kind": "port",
-                                 "sample": f"1 FP64 V-cycle of the oracle restatement per step at "
-                                           f"full size, x {cyc} V-cycles (the FP64 cycle count of "
-                                           f"this workload)"},
-                "e2e": {"value": value, "unit": "cell-solves/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
+        samples = []
+        for _ in range(max(1, args.warmup + args.steps) if kind == "poisson" else 1):
+            samples.append(cpu_sample_dns(args.workload, threads) if kind == "dns"
+                           else cpu_sample_poisson(args.workload, threads))
+        if kind == "dns":
+            t, it, N = samples[-1]
+            value = N / (3.0 * t)
+            sample = (f"first FP64 RK3 sub-step after the initial projection, oracle restatement "
+                      f"at full size ({t:.1f} s, {it} MG V-cycles), x3 per step")
+            ms = 3 * t * 1e3
+        else:
+            t = float(np.mean([x[0] for x in samples[args.warmup:]] or [samples[-1][0]]))
+            N = samples[-1][1]
+            cyc = 48
+            value = N / (t * cyc)
+            sample = f"1 FP64 V-cycle of the oracle restatement at full size ({t:.2f} s) x {cyc}"
+            ms = t * cyc * 1e3
+        line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": 0,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
     if world > 1:
@@ -313,9 +446,9 @@ def main():
         import torch.distributed as dist
         from datetime import timedelta
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    r = run_ours(args, rank, world, local_rank)
+    r = run_dns(args, rank, world, local_rank) if kind == "dns" else run_poisson(args, rank, world, local_rank)
     if world > 1:
         import torch.distributed as dist
 
@@ -325,52 +458,54 @@ def main():
     peak, peak_kind = load_peaks()
     N = r["N"]
     value = world * N / (r["ms_step"] / 1e3)
-    e2e_value = world * N / (r["e2e_ms"] / 1e3)
-    # roofline of the finest-level smoother: one colour per launch reads phi
-    # (8 or 4 B: the neighbours), f (half the cells) and writes half the
-    # cells -> 12 B/cell FP64, 6 B/cell FP32, per launch
     bpc = 6.0 if args.prec == "mixed" else 12.0
     kernel = "k_rb_sweep<float>" if args.prec == "mixed" else "k_rb_sweep<double>"
     roof = None
     if r["sweeps"]:
         t_launch = r["sweep_ms"] / r["sweeps"] / 1e3
         achieved = bpc * N / t_launch / 1e9
-        traffic = load_traffic(f"{args.workload}:{kernel}")
         roof = {"bound": "hbm", "kernel": kernel, "achieved": round(achieved, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                "peak_kind": f"{peak_kind} (hbm_gbs)", "algorithmic_bytes_per_launch": bpc * N,
-                "mean_launch_ms": round(t_launch * 1e3, 4)}
+                "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": load_traffic(f"{args.workload}:{kernel}"),
+                "peak_kind": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": bpc * N,
+                "mean_launch_ms": round(t_launch * 1e3, 4),
+                "share_note": "finest-level smoother launches only; share of step time in profiles/"}
     cpu = None
     if not args.no_cpu:
-        threads = os.cpu_count() or 1
-        sec_cyc, _ = cpu_sample(args.workload, args.mode, threads)
-        cyc = FP64_CYCLES.get((args.workload, args.mode)) or (r.get("fp64") or {}).get("iter")
-        if cyc:
-            cpu = {"value": N / (sec_cyc * cyc), "unit": "cell-solves/s", "cores": threads,
-                   "kind": "port",
-                   "sample": f"1 FP64 V-cycle of the oracle restatement at full size "
-                             f"({sec_cyc:.2f} s) x {cyc} V-cycles"}
-    line = {
-        "metric": metric, "value": value, "unit": "cell-solves/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_step"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32-in-f64" if args.prec == "mixed" else "f64", "data": "synthetic",
-        "config": config,
-        "mg_solve_ms": {args.prec: r["ms_step"], **({"fp64": r["fp64"]["ms"]} if "fp64" in r else {})},
-        "mg_iters": {args.prec: r["iters"][-1], **({"fp64": r["fp64"]["iter"]} if "fp64" in r else {})},
-        "resid": max(r["resids"]),
-        "e2e": {"value": e2e_value, "unit": "cell-solves/s",
-                "h2d_bytes_per_step": r["bytes_io"][0], "d2h_bytes_per_step": r["bytes_io"][1],
-                "ms_per_step": r["e2e_ms"]},
-        "roofline": roof, "cpu_baseline": cpu, "clocks": r["clocks"],
-        "gpu_launches": r["launches"],
-    }
+        if kind == "dns":
+            t, it, _ = cpu_sample_dns(args.workload, threads)
+            cpu = {"value": N / (3.0 * t), "unit": unit, "cores": threads, "kind": "port",
+                   "sample": f"first FP64 RK3 sub-step after the initial projection, oracle "
+                             f"restatement at full size ({t:.1f} s, {it} MG V-cycles), x3 per step"}
+        else:
+            t, _ = cpu_sample_poisson(args.workload, threads)
+            cyc = r["iters"][-1] if args.prec == "fp64" else 48
+            cpu = {"value": N / (t * cyc), "unit": unit, "cores": threads, "kind": "port",
+                   "sample": f"1 FP64 V-cycle of the oracle restatement at full size ({t:.2f} s) x {cyc}"}
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (MG f32-in-f64)" if args.prec == "mixed" else "f64", "data": "synthetic",
+            "config": config}
+    if kind == "dns":
+        line["mg_ms_per_step"] = round(r["mg_ms_step"], 3)
+        line["mg_iters_last_step"] = r["mg_iters"][-1]
+        line["dt"] = r["dt"]
+        line["max_div"] = r["max_div"]
+        line["div_bound"] = 1e-10 * r["umax"] / r["dzmin"]
+        if "mg_cold" in r:
+            line["mg_solve_ms"] = r["mg_cold"]
+    else:
+        line["mg_iters"] = r["iters"][-1]
+        line["resid"] = r["resid"]
+    if "e2e_ms" in r:
+        line["e2e"] = {"value": world * N / (r["e2e_ms"] / 1e3), "unit": unit,
+                       "h2d_bytes_per_step": r["bytes_io"][0], "d2h_bytes_per_step": r["bytes_io"][1],
+                       "ms_per_step": r["e2e_ms"]}
+    line.update({"roofline": roof, "cpu_baseline": cpu, "clocks": r["clocks"],
+                 "gpu_launches": r["launches"]})
     print(json.dumps(line))
 
-
-# FP64 V-cycles of the oracle/GPU FP64 algorithm (bit-identical) to reach
-# the 1e-10 true residual on each workload; measured on the GPU path.
-FP64_CYCLES = {}
 
 if __name__ == "__main__":
     main()

@@ -242,7 +242,12 @@ typedef struct {
   double mg_relmax[3];  /* MG stop metric of each sub-step */
   double max_div;       /* max |div u| after the step (divergence()) */
   double avg_div;       /* volume-weighted mean |div u| */
-  double ms;            /* device time of the step */
+  double ms;            /* device time of the steps of the call */
+  double mg_ms;         /* part of it spent in the multigrid solves */
+  int64_t launches;     /* kernels of this library launched by the call */
+  int32_t fine_sweeps;  /* finest-level smoother launches timed (profiling on) */
+  int32_t reserved;
+  double fine_sweep_ms; /* their summed device time (profiling on) */
 } anel_step_report;
 
 typedef struct anel_ns_ctx anel_ns_ctx;
@@ -264,6 +269,9 @@ int anel_ns_ctx_substep(anel_ns_ctx* ctx, double a1, double a2, double a3, doubl
  * output/statistics diagnostics): calcdt, gravity, LES update, three
  * sub-steps.  report (may be NULL) describes the last step. */
 int anel_ns_ctx_step(anel_ns_ctx* ctx, int32_t nsteps, void* stream, anel_step_report* report);
+/* Profiling of the multigrid inside the steps (see
+ * anel_mg_ctx_set_profiling); totals land in the step report. */
+int anel_ns_ctx_set_profiling(anel_ns_ctx* ctx, int32_t on);
 /* time and step counter (time, nstep of the Parameters module) */
 int anel_ns_ctx_set_clock(anel_ns_ctx* ctx, double time, int32_t nstep);
 /* Projection of the current velocity onto divergence-free fields (used to

@@ -278,6 +278,7 @@ static void u1_rhs(orc_ns* s, double* Ut) {
   const double rRe = s->rRe;
   memset(Ut, 0, sizeof(double) * D->G);
   const int sx = 2, ex = D->nx + 1, sy = 2, ey = D->ny + 1, sz = 2, ez = D->nz + 1;
+  #pragma omp parallel for schedule(static)
   for (int k = sz; k <= ez; ++k)
     for (int j = sy; j <= ey; ++j)
       for (int i = sx; i <= ex; ++i)
@@ -288,6 +289,7 @@ static void u1_rhs(orc_ns* s, double* Ut) {
                           rRe * ((A_(un, i, j + 1, k) - A_(un, i, j, k)) * M(D->rdye, j) -
                                  (A_(un, i, j, k) - A_(un, i, j - 1, k)) * M(D->rdye, j - 1)) *
                               M(D->rdyc, j);
+  #pragma omp parallel for schedule(static)
   for (int k = sz; k <= ez; ++k)
     for (int j = sy; j <= ey; ++j)
       for (int i = sx; i <= ex; ++i) {
@@ -309,6 +311,7 @@ static void u1_rhs(orc_ns* s, double* Ut) {
         A_(Ut, i, j, k) = A_(Ut, i, j, k) + (ua1 * va1 - ua2 * va2) * M(D->rdyc, j);
       }
   if (les_on(s)) {
+    #pragma omp parallel for schedule(static)
     for (int k = sz; k <= ez; ++k)
       for (int j = sy; j <= ey; ++j)
         for (int i = sx; i <= ex; ++i) {
@@ -357,6 +360,7 @@ static void u2_rhs(orc_ns* s, double* Vt) {
   const double rRe = s->rRe;
   memset(Vt, 0, sizeof(double) * D->G);
   const int sx = 2, ex = D->nx + 1, sy = 2, ey = D->ny + 1, sz = 2, ez = D->nz + 1;
+  #pragma omp parallel for schedule(static)
   for (int k = sz; k <= ez; ++k)
     for (int j = sy; j <= ey; ++j)
       for (int i = sx; i <= ex; ++i)
@@ -367,6 +371,7 @@ static void u2_rhs(orc_ns* s, double* Vt) {
                           rRe * ((A_(vn, i, j + 1, k) - A_(vn, i, j, k)) * M(D->rdyc, j + 1) -
                                  (A_(vn, i, j, k) - A_(vn, i, j - 1, k)) * M(D->rdyc, j)) *
                               M(D->rdye, j);
+  #pragma omp parallel for schedule(static)
   for (int k = sz; k <= ez; ++k)
     for (int j = sy; j <= ey; ++j)
       for (int i = sx; i <= ex; ++i) {
@@ -388,6 +393,7 @@ static void u2_rhs(orc_ns* s, double* Vt) {
             A_(Vt, i, j, k) - (ra1 * wa1 * va1 - ra2 * wa2 * va2) * M(D->rdzc, k) / A_(r, i, j, k);
       }
   if (les_on(s)) {
+    #pragma omp parallel for schedule(static)
     for (int k = sz; k <= ez; ++k)
       for (int j = sy; j <= ey; ++j)
         for (int i = sx; i <= ex; ++i) {
@@ -440,6 +446,7 @@ static void u3_rhs(orc_ns* s, double* Wt) {
   memset(Wt, 0, sizeof(double) * D->G);
   const int sx = 2, ex = D->nx + 1, sy = 2, ey = D->ny + 1, sz = 2, ez = D->nz + 1;
   const int kend = ez - s->p.ew; /* k = sz..ez-EW */
+  #pragma omp parallel for schedule(static)
   for (int k = sz; k <= kend; ++k)
     for (int j = sy; j <= ey; ++j)
       for (int i = sx; i <= ex; ++i)
@@ -448,6 +455,7 @@ static void u3_rhs(orc_ns* s, double* Wt) {
                               ((A_(rhon, i, j, k + 1) - A_(bg, i, j, k + 1)) +
                                (A_(rhon, i, j, k) - A_(bg, i, j, k))) /
                               (R12 * (A_(bg, i, j, k + 1) + A_(bg, i, j, k)));
+  #pragma omp parallel for schedule(static)
   for (int k = sz; k <= kend; ++k)
     for (int j = sy; j <= ey; ++j)
       for (int i = sx; i <= ex; ++i)
@@ -458,6 +466,7 @@ static void u3_rhs(orc_ns* s, double* Wt) {
                           rRe * ((A_(wn, i, j + 1, k) - A_(wn, i, j, k)) * M(D->rdye, j) -
                                  (A_(wn, i, j, k) - A_(wn, i, j - 1, k)) * M(D->rdye, j - 1)) *
                               M(D->rdyc, j);
+  #pragma omp parallel for schedule(static)
   for (int k = sz; k <= kend; ++k)
     for (int j = sy; j <= ey; ++j)
       for (int i = sx; i <= ex; ++i) {
@@ -478,6 +487,7 @@ static void u3_rhs(orc_ns* s, double* Wt) {
         A_(Wt, i, j, k) = A_(Wt, i, j, k) - (va1 * wa1 - va2 * wa2) * M(D->rdyc, j);
       }
   if (les_on(s)) {
+    #pragma omp parallel for schedule(static)
     for (int k = sz; k <= kend; ++k)
       for (int j = sy; j <= ey; ++j)
         for (int i = sx; i <= ex; ++i) {
@@ -527,6 +537,7 @@ static void scalar_rhs(orc_ns* s, double* St, int is_rho) {
   const int model = is_rho ? s->p.rmodel : s->p.smodel;
   memset(St, 0, sizeof(double) * D->G);
   const int sx = 2, ex = D->nx + 1, sy = 2, ey = D->ny + 1, sz = 2, ez = D->nz + 1;
+  #pragma omp parallel for schedule(static)
   for (int k = sz; k <= ez; ++k)
     for (int j = sy; j <= ey; ++j)
       for (int i = sx; i <= ex; ++i)
@@ -537,6 +548,7 @@ static void scalar_rhs(orc_ns* s, double* St, int is_rho) {
                           Dk * ((A_(c, i, j + 1, k) - A_(c, i, j, k)) * M(D->rdye, j) -
                                 (A_(c, i, j, k) - A_(c, i, j - 1, k)) * M(D->rdye, j - 1)) *
                               M(D->rdyc, j);
+  #pragma omp parallel for schedule(static)
   for (int k = sz; k <= ez; ++k)
     for (int j = sy; j <= ey; ++j)
       for (int i = sx; i <= ex; ++i) {
@@ -562,6 +574,7 @@ static void scalar_rhs(orc_ns* s, double* St, int is_rho) {
         }
       }
   if (model == ANEL_MODEL_SSM) {
+    #pragma omp parallel for schedule(static)
     for (int k = sz; k <= ez; ++k)
       for (int j = sy; j <= ey; ++j)
         for (int i = sx; i <= ex; ++i) {
@@ -589,6 +602,7 @@ static void scalar_rhs(orc_ns* s, double* St, int is_rho) {
 /* var_advance (NSsolver.F90:2225-2264), interior only */
 static void var_advance(const orc_ns* s, const double* v1, double* v2, double f1, double f2, double f3) {
   const orc_dom* D = &s->d;
+  #pragma omp parallel for schedule(static)
   for (int k = 2; k <= D->nz + 1; ++k)
     for (int j = 2; j <= D->ny + 1; ++j)
       for (int i = 2; i <= D->nx + 1; ++i)
@@ -629,6 +643,7 @@ static void cn_pl(orc_ns* s, const double* q, double* u, double a3, double rkdt,
   /* the LES block of var_advance_CN_PL is gated on Vmodel for every
    * variable, scalars included (NSsolver.F90:3160-3190) */
   const int les_var = les;
+#pragma omp parallel for schedule(static)
   for (long j = 1; j <= D->Y; ++j)
     for (long i = 1; i <= D->X; ++i) {
       if (var != 3) {
@@ -711,6 +726,7 @@ static void cn_pl(orc_ns* s, const double* q, double* u, double a3, double rkdt,
       }
     }
   /* right-hand side (:3185-3296) */
+#pragma omp parallel for schedule(static)
   for (long j = 1; j <= D->Y; ++j)
     for (long i = 1; i <= D->X; ++i)
       for (int k = sz; k <= ez; ++k) {
@@ -825,9 +841,10 @@ static void cn_pl(orc_ns* s, const double* q, double* u, double a3, double rkdt,
     }
   /* Thomas per interior column over k = 1..nz+2 (:3431-3436) */
   const int n = D->nz + 2;
-  double* a = (double*)malloc(sizeof(double) * 4 * n);
-  double *b = a + n, *cc = b + n, *gg = cc + n;
-  for (int j = 2; j <= D->ny + 1; ++j)
+#pragma omp parallel for schedule(static)
+  for (int j = 2; j <= D->ny + 1; ++j) {
+    double* a = (double*)malloc(sizeof(double) * 4 * n);
+    double *b = a + n, *cc = b + n, *gg = cc + n;
     for (int i = 2; i <= D->nx + 1; ++i) {
       for (int k = 1; k <= n; ++k) {
         a[k - 1] = A_(sub, i, j, k);
@@ -838,7 +855,8 @@ static void cn_pl(orc_ns* s, const double* q, double* u, double a3, double rkdt,
       thomas_ns(a, b, cc, gg, n);
       for (int k = 1; k <= n; ++k) A_(rhs, i, j, k) = gg[k - 1];
     }
-  free(a);
+    free(a);
+  }
   ghost(s, rhs, var == 1 ? VT_U : var == 2 ? VT_V : var == 3 ? VT_W : var == 5 ? VT_RHO : VT_SCAL1);
   memcpy(u, rhs, sizeof(double) * G);
 }
@@ -851,6 +869,7 @@ static void psource(orc_ns* s, double* SRC, double dt) {
   const double H = (double)(float)0.5;
   memset(SRC, 0, sizeof(double) * D->G);
   const double rdt = 1.0 / dt;
+  #pragma omp parallel for schedule(static)
   for (int k = 2; k <= D->nz + 1; ++k)
     for (int j = 2; j <= D->ny + 1; ++j)
       for (int i = 2; i <= D->nx + 1; ++i)
@@ -871,6 +890,7 @@ static void pgrad(orc_ns* s, double dt) {
   const orc_dom* D = &s->d;
   const double *pn = s->f.p, *r = s->f.r;
   double *U = s->f.u, *V = s->f.v, *W = s->f.w;
+  #pragma omp parallel for schedule(static)
   for (int k = 2; k <= D->nz + 1; ++k)
     for (int j = 2; j <= D->ny + 1; ++j)
       for (int i = 2; i <= D->nx + 1; ++i)
@@ -878,6 +898,7 @@ static void pgrad(orc_ns* s, double dt) {
                                            A_(pn, i, j, k) / A_(r, i, j, k)) *
                                               M(D->rdxe, i) * dt;
   ghost(s, U, VT_UTEMP);
+  #pragma omp parallel for schedule(static)
   for (int k = 2; k <= D->nz + 1; ++k)
     for (int j = 2; j <= D->ny + 1; ++j)
       for (int i = 2; i <= D->nx + 1; ++i)
@@ -885,6 +906,7 @@ static void pgrad(orc_ns* s, double dt) {
                                            A_(pn, i, j, k) / A_(r, i, j, k)) *
                                               M(D->rdye, j) * dt;
   ghost(s, V, VT_VTEMP);
+  #pragma omp parallel for schedule(static)
   for (int k = 2; k <= D->nz + 1 - s->p.ew; ++k)
     for (int j = 2; j <= D->ny + 1; ++j)
       for (int i = 2; i <= D->nx + 1; ++i)
