@@ -197,6 +197,308 @@ __global__ void k_rb_sweep(DevLevel<T> L, int color) {
   }
 }
 
+// -------------------------------------------------------- z-line sweep
+// ZLINE smoother: one (i+j) colour of red-black z-line Gauss-Seidel
+// (colour 0 = (i+j) even, the reference's first pass of mg_relaxLz,
+// mg_relax.F90:487-535) with the level's own 7-point operator.  Each line
+// is the tridiagonal (a = c5, b = c7, c = c6) solved by the Thomas routine
+// of mg_relax.F90:541-595; for x/y-uniform coefficients its elimination is
+// the same on every column, so only the substitution runs here:
+//   G(1) = r(1), G(k) = r(k) + ap(k) G(k-1), phi(n) = G(n)/bp(n),
+//   phi(k) = (G(k) - c(k) phi(k+1)) / bp(k).
+// G is kept in the line's own cells (no other thread reads them in this
+// colour).  One thread per pair of adjacent columns (i0, i0+1), which holds
+// one column of each colour.
+template <typename T>
+struct ZFac {
+  const T* ap;  // eliminated sub-diagonal, per k (index k-1; k = 2..nz+1 used)
+  const T* bp;  // eliminated diagonal
+};
+
+template <typename T>
+__global__ void k_zline(DevLevel<T> L, int color, ZFac<T> F) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;  // pair index
+  const int j = 2 + blockIdx.y;
+  const int i0 = 2 + 2 * p;
+  if (i0 > L.nx + 1) return;
+  const int i = i0 + ((color + i0 + j) & 1);
+  if (i > L.nx + 1) return;
+  const T a1 = cx1p(L)[i - 1], a2 = cx2p(L)[i - 1];
+  const T a3 = cy3p(L)[j - 1], a4 = cy4p(L)[j - 1];
+  const T* __restrict__ cz5 = cz5p(L);
+  const T* __restrict__ cz6 = cz6p(L);
+  T* phi = L.phi;
+  const T* __restrict__ src = L.src;
+  const int nz = L.nz;
+  const int64_t X = L.X, XY = L.XY;
+  const int64_t c0 = cidx(i, j, 1, L.X, L.XY);
+  // forward substitution, k = 2 .. nz+1, in blocks of U rows whose loads
+  // are all issued before the dependent recurrence (software pipelining)
+  constexpr int U = 8;
+  T g = T(0);
+  for (int kb = 2; kb <= nz + 1; kb += U) {
+    T r[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = kb + u;
+      if (k <= nz + 1) {
+        const int64_t c = c0 + (int64_t)(k - 1) * XY;
+        r[u] = src[c] - (a1 * phi[c - 1] + a2 * phi[c + 1] + a3 * phi[c - X] + a4 * phi[c + X]);
+        if (k == 2) r[u] = r[u] - cz5[1] * phi[c - XY];
+        if (k == nz + 1) r[u] = r[u] - cz6[nz] * phi[c + XY];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = kb + u;
+      if (k <= nz + 1) {
+        g = (k == 2) ? r[u] : r[u] + F.ap[k - 1] * g;
+        phi[c0 + (int64_t)(k - 1) * XY] = g;
+      }
+    }
+  }
+  // back substitution in blocks of U rows (loads of G first)
+  T x = g / F.bp[nz];
+  phi[c0 + (int64_t)nz * XY] = x;
+  for (int kb = nz; kb >= 2; kb -= U) {
+    T gv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = kb - u;
+      if (k >= 2) gv[u] = phi[c0 + (int64_t)(k - 1) * XY];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = kb - u;
+      if (k >= 2) {
+        x = (gv[u] - cz6[k - 1] * x) / F.bp[k - 1];
+        phi[c0 + (int64_t)(k - 1) * XY] = x;
+      }
+    }
+  }
+}
+
+// Warp-per-line z-line smoother for levels with few columns (FP32 path):
+// the line's tridiagonal system is solved by parallel cyclic reduction in
+// shared memory (log2(nz) steps, each row updated from its neighbours at
+// distance 2^s), so the latency is that of a few loads instead of a
+// 2*nz-long dependent chain.  Not bit-matched to the Thomas order; used
+// only inside the FP32 V-cycle of the mixed-precision solver.
+template <typename T, int NMAX>
+__global__ void k_zline_pcr(DevLevel<T> L, int color) {
+  extern __shared__ unsigned char zl_smem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int nz = L.nz;
+  T* sm = reinterpret_cast<T*>(zl_smem) + (size_t)wib * 4 * NMAX;
+  T* A = sm;
+  T* B = sm + NMAX;
+  T* C = sm + 2 * NMAX;
+  T* D = sm + 3 * NMAX;
+  const int pairs = (L.nx + 1) >> 1;
+  const int t = blockIdx.x * (blockDim.x >> 5) + wib;  // column of this colour
+  if (t >= pairs * L.ny) return;
+  const int j = 2 + t / pairs;
+  const int i0 = 2 + 2 * (t % pairs);
+  const int i = i0 + ((color + i0 + j) & 1);
+  if (i > L.nx + 1) return;
+  const T a1 = cx1p(L)[i - 1], a2 = cx2p(L)[i - 1];
+  const T a3 = cy3p(L)[j - 1], a4 = cy4p(L)[j - 1];
+  const T* cz5 = cz5p(L);
+  const T* cz6 = cz6p(L);
+  const T* d5 = dz5p(L);
+  const T* d6 = dz6p(L);
+  const int64_t X = L.X, XY = L.XY;
+  const int64_t c0 = cidx(i, j, 1, L.X, L.XY);
+  const T* phi = L.phi;
+  for (int q = lane; q < nz; q += 32) {
+    const int k = q + 2;
+    const int64_t c = c0 + (int64_t)(k - 1) * XY;
+    T d = L.src[c] - (a1 * phi[c - 1] + a2 * phi[c + 1] + a3 * phi[c - X] + a4 * phi[c + X]);
+    T a = cz5[k - 1], cc = cz6[k - 1];
+    if (q == 0) {
+      d -= a * phi[c - XY];
+      a = T(0);
+    }
+    if (q == nz - 1) {
+      d -= cc * phi[c + XY];
+      cc = T(0);
+    }
+    A[q] = a;
+    C[q] = cc;
+    B[q] = -(a1 + a2 + a3 + a4 + d5[k - 1] + d6[k - 1]);
+    D[q] = d;
+  }
+  __syncwarp();
+  constexpr int R = NMAX / 32;
+  for (int st = 1; st < nz; st <<= 1) {
+    T na[R], nb[R], nc[R], nd[R];
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      const int q = lane + 32 * u;
+      if (q < nz) {
+        T a = A[q], b = B[q], cc = C[q], d = D[q];
+        if (q - st >= 0) {
+          const T al = -a / B[q - st];
+          b += al * C[q - st];
+          d += al * D[q - st];
+          a = al * A[q - st];
+        } else {
+          a = T(0);
+        }
+        if (q + st < nz) {
+          const T be = -cc / B[q + st];
+          b += be * A[q + st];
+          d += be * D[q + st];
+          cc = be * C[q + st];
+        } else {
+          cc = T(0);
+        }
+        na[u] = a;
+        nb[u] = b;
+        nc[u] = cc;
+        nd[u] = d;
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      const int q = lane + 32 * u;
+      if (q < nz) {
+        A[q] = na[u];
+        B[q] = nb[u];
+        C[q] = nc[u];
+        D[q] = nd[u];
+      }
+    }
+    __syncwarp();
+  }
+  for (int q = lane; q < nz; q += 32) L.phi[c0 + (int64_t)(q + 1) * XY] = D[q] / B[q];
+}
+
+// Partitioned z-line smoother for the FP32 cycle.  Every line of a level
+// has the same tridiagonal matrix (x/y-uniform coefficients), so the line
+// is cut into P segments whose factors are precomputed on the host:
+//   phase 1  each segment solves its own rows with the eliminated factors
+//            (ap, bp) ignoring its neighbours -> y;
+//   phase 2  the 2P interface values (first and last row of every segment)
+//            follow from y by the precomputed inverse of the interface
+//            system, z = Minv * yb;
+//   phase 3  x = y + u * L(s-1) + v * F(s+1) with the precomputed influence
+//            vectors u (response to the row before the segment) and v.
+// A CTA holds 32 lines (lanes) x P segments (warps); the dependent chain
+// is 2 n/P rows instead of 2 n.  Not bit-matched to the Thomas order (the
+// FP64 path keeps it).
+template <typename T>
+struct SegFac {
+  const T* ap;    // segment-local eliminated sub-diagonal, per row (index k-1)
+  const T* bp;    // segment-local eliminated diagonal
+  const T* u;     // influence of the row before the segment
+  const T* v;     // influence of the row after the segment
+  const T* minv;  // (2P x 2P) inverse of the interface system, row major
+};
+
+template <typename T, int P>
+__global__ void __launch_bounds__(32 * P) k_zline_seg(DevLevel<T> L, int color, SegFac<T> F) {
+  __shared__ T yb[32][2 * P + 1];
+  __shared__ T zz[32][2 * P + 1];
+  const int lane = threadIdx.x;  // line within the CTA
+  const int s = threadIdx.y;     // segment
+  const int pairs = (L.nx + 1) >> 1;
+  const int64_t t = (int64_t)blockIdx.x * 32 + lane;
+  bool active = t < (int64_t)pairs * L.ny;
+  int i = 0, j = 0;
+  if (active) {
+    j = 2 + (int)(t / pairs);
+    const int i0 = 2 + 2 * (int)(t % pairs);
+    i = i0 + ((color + i0 + j) & 1);
+    active = i <= L.nx + 1;
+  }
+  const int n = L.nz;
+  const int m = n / P;
+  const int lo = s * m, hi = lo + m;  // rows [lo, hi) of the line (row q <-> k = q+2)
+  T y_first = T(0), y_last = T(0);
+  int64_t c0 = 0;
+  const int64_t X = L.X, XY = L.XY;
+  if (active) {
+    const T a1 = cx1p(L)[i - 1], a2 = cx2p(L)[i - 1];
+    const T a3 = cy3p(L)[j - 1], a4 = cy4p(L)[j - 1];
+    const T* __restrict__ cz5 = cz5p(L);
+    const T* __restrict__ cz6 = cz6p(L);
+    T* phi = L.phi;
+    const T* __restrict__ src = L.src;
+    c0 = cidx(i, j, 2, L.X, L.XY);  // row 0
+    constexpr int U = 8;
+    T g = T(0);
+    for (int qb = lo; qb < hi; qb += U) {
+      T r[U];
+#pragma unroll
+      for (int w = 0; w < U; ++w) {
+        const int q = qb + w;
+        if (q < hi) {
+          const int64_t c = c0 + (int64_t)q * XY;
+          r[w] = src[c] - (a1 * phi[c - 1] + a2 * phi[c + 1] + a3 * phi[c - X] + a4 * phi[c + X]);
+          if (q == 0) r[w] = r[w] - cz5[1] * phi[c - XY];
+          if (q == n - 1) r[w] = r[w] - cz6[n] * phi[c + XY];
+        }
+      }
+#pragma unroll
+      for (int w = 0; w < U; ++w) {
+        const int q = qb + w;
+        if (q < hi) {
+          g = (q == lo) ? r[w] : r[w] + F.ap[q + 1] * g;
+          phi[c0 + (int64_t)q * XY] = g;
+        }
+      }
+    }
+    T x = g / F.bp[hi];
+    phi[c0 + (int64_t)(hi - 1) * XY] = x;
+    y_last = x;
+    for (int qb = hi - 2; qb >= lo; qb -= U) {
+      T gv[U];
+#pragma unroll
+      for (int w = 0; w < U; ++w) {
+        const int q = qb - w;
+        if (q >= lo) gv[w] = phi[c0 + (int64_t)q * XY];
+      }
+#pragma unroll
+      for (int w = 0; w < U; ++w) {
+        const int q = qb - w;
+        if (q >= lo) {
+          x = (gv[w] - cz6[q + 1] * x) / F.bp[q + 1];
+          phi[c0 + (int64_t)q * XY] = x;
+        }
+      }
+    }
+    y_first = x;
+  }
+  yb[lane][2 * s] = y_first;
+  yb[lane][2 * s + 1] = y_last;
+  __syncthreads();
+  {
+    T z0 = T(0), z1 = T(0);
+    const T* m0 = F.minv + (size_t)(2 * s) * (2 * P);
+    const T* m1 = m0 + 2 * P;
+#pragma unroll 8
+    for (int p = 0; p < 2 * P; ++p) {
+      const T yv = yb[lane][p];
+      z0 += m0[p] * yv;
+      z1 += m1[p] * yv;
+    }
+    zz[lane][2 * s] = z0;
+    zz[lane][2 * s + 1] = z1;
+  }
+  __syncthreads();
+  if (!active) return;
+  const T Lprev = (s > 0) ? zz[lane][2 * s - 1] : T(0);
+  const T Fnext = (s < P - 1) ? zz[lane][2 * s + 2] : T(0);
+  T* phi = L.phi;
+  for (int q = lo; q < hi; ++q) {
+    const int64_t c = c0 + (int64_t)q * XY;
+    phi[c] = phi[c] + F.u[q + 1] * Lprev + F.v[q + 1] * Fnext;
+  }
+}
+
 // ----------------------------------------------------- residual + restrict
 // mg_restr.F90:114-241.  One thread per coarse cell (ghosts included):
 // coarse phi <- 0 everywhere, coarse f <- 0 on ghosts and, on the interior,

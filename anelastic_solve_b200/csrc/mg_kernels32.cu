@@ -8,6 +8,8 @@ namespace anel {
 
 template void launch_bdry<float>(const DevLevel<float>&, float*, cudaStream_t);
 template void launch_rb_sweep<float>(const DevLevel<float>&, int, cudaStream_t);
+template void launch_zline<float>(const DevLevel<float>&, int, const float*, const float*, cudaStream_t);
+template void launch_zline_seg<float>(const DevLevel<float>&, int, const SegFac<float>&, cudaStream_t);
 template void launch_restrict<float>(const DevLevel<float>&, const DevLevel<float>&, int,
                                      cudaStream_t);
 template void launch_prolong<float>(const DevLevel<float>&, const DevLevel<float>&, int,

@@ -20,6 +20,12 @@ void launch_bdry(const DevLevel<T>& L, T* phi, cudaStream_t s);
 template <typename T>
 void launch_rb_sweep(const DevLevel<T>& L, int color, cudaStream_t s);
 template <typename T>
+void launch_zline(const DevLevel<T>& L, int color, const T* ap, const T* bp, cudaStream_t s);
+// segments of the partitioned FP32 z-line solver (lines must be a multiple)
+constexpr int kZSeg = 16;
+template <typename T>
+void launch_zline_seg(const DevLevel<T>& L, int color, const SegFac<T>& F, cudaStream_t s);
+template <typename T>
 void launch_restrict(const DevLevel<T>& F, const DevLevel<T>& C, int cdir, cudaStream_t s);
 template <typename T>
 void launch_prolong(const DevLevel<T>& F, const DevLevel<T>& C, int cdir, cudaStream_t s);

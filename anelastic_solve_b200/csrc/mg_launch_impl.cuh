@@ -19,6 +19,37 @@ void launch_rb_sweep(const DevLevel<T>& L, int color, cudaStream_t s) {
   count_launch();
 }
 template <typename T>
+void launch_zline(const DevLevel<T>& L, int color, const T* ap, const T* bp, cudaStream_t s) {
+  const int pairs = (L.nx + 1) / 2;
+  const int64_t cols = (int64_t)pairs * L.ny;
+  // few long lines (coarse levels of the FP32 cycle): one warp per line
+  if (sizeof(T) == 4 && cols < 16384 && L.nz <= 512 && L.nz >= 2) {
+    constexpr int NMAX = 512;
+    const int warps = 4;
+    const size_t sm = (size_t)warps * 4 * NMAX * sizeof(T);
+    const unsigned blocks = (unsigned)((cols + warps - 1) / warps);
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_zline_pcr<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      attr = true;
+    }
+    k_zline_pcr<T, NMAX><<<blocks, 32 * warps, sm, s>>>(L, color);
+    count_launch();
+    return;
+  }
+  const int tx = 64;
+  dim3 grid((unsigned)((pairs + tx - 1) / tx), (unsigned)L.ny, 1u);
+  k_zline<T><<<grid, tx, 0, s>>>(L, color, ZFac<T>{ap, bp});
+  count_launch();
+}
+template <typename T>
+void launch_zline_seg(const DevLevel<T>& L, int color, const SegFac<T>& F, cudaStream_t s) {
+  const int64_t cols = (int64_t)((L.nx + 1) / 2) * L.ny;
+  dim3 block(32, kZSeg, 1);
+  k_zline_seg<T, kZSeg><<<(unsigned)((cols + 31) / 32), block, 0, s>>>(L, color, F);
+  count_launch();
+}
+template <typename T>
 void launch_restrict(const DevLevel<T>& F, const DevLevel<T>& C, int cdir, cudaStream_t s) {
   k_restrict<T><<<gs_blocks(C.G), 256, 0, s>>>(F, C, cdir);
   count_launch();

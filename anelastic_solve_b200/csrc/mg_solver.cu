@@ -50,8 +50,8 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
     set_error("unknown smoother %d", p->smoother);
     return ANEL_ERR_ARG;
   }
-  if (p->smoother != ANEL_SMOOTHER_RBPGS) {
-    set_error("the z-line smoothers (LJ, ZLINE) are not available in this build");
+  if (p->smoother == ANEL_SMOOTHER_LJ) {
+    set_error("the reference's LJ z-line smoother is not available in this build (use ZLINE)");
     return ANEL_ERR_UNSUPPORTED;
   }
   if (p->mode != ANEL_MODE_LITERAL && p->mode != ANEL_MODE_METRIC) {
@@ -86,7 +86,8 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
   }
   for (int d = 0; d < 3; ++d) {
     const int Ld = p->levels[d];
-    if (Ld < 2) {
+    // ZLINE may keep z unrefined (horizontal semi-coarsening, an extension)
+    if (Ld < 2 && !(d == 2 && p->smoother == ANEL_SMOOTHER_ZLINE)) {
       set_error("no coarsening in direction %d at the finest level (mg_check_size codes 10-12)",
                 d + 1);
       return ANEL_ERR_SIZE;
@@ -184,6 +185,10 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
       ANEL_CUDA_TRY(cudaMemset(d_src64_[l], 0, G * sizeof(double)));
     }
     ANEL_CUDA_TRY(cudaMalloc(&d_coef64_[l], ncoef * sizeof(double)));
+    if (p->smoother == ANEL_SMOOTHER_ZLINE) {
+      ANEL_CUDA_TRY(cudaMalloc(&d_zf64_[l], 2 * (size_t)geo_[l].Z * sizeof(double)));
+      ANEL_CUDA_TRY(cudaMalloc(&d_zf32_[l], 2 * (size_t)geo_[l].Z * sizeof(float)));
+    }
     if (mixed) {
       ANEL_CUDA_TRY(cudaMalloc(&d_phi32_[l], G * sizeof(float)));
       ANEL_CUDA_TRY(cudaMalloc(&d_src32_[l], G * sizeof(float)));
@@ -212,6 +217,8 @@ MGSolver::~MGSolver() {
     cudaFree(d_phi32_[l]);
     cudaFree(d_src32_[l]);
     cudaFree(d_coef32_[l]);
+    cudaFree(d_zf64_[l]);
+    cudaFree(d_zf32_[l]);
   }
   cudaFree(d_max_);
   cudaFree(d_part_);
@@ -357,6 +364,15 @@ void MGSolver::build_agglomerated() {
       C[n + 1] = E[n] + 0.5 * DC[n + 1];
       for (int q = 1; q <= n + 1; ++q) DE[q - 1] = C[q] - C[q - 1];
       DE[n + 1] = DE[n];
+      // a direction whose finer spacings are one value is coarsened
+      // exactly: every coarse spacing is twice it
+      const std::vector<double>& DCf = ag_[l + 1][d][2];
+      const std::vector<double>& DEf = ag_[l + 1][d][3];
+      bool uni = true;
+      for (size_t q = 0; q < DCf.size(); ++q)
+        if (!(DCf[q] == DCf[0] && DEf[q] == DCf[0])) uni = false;
+      if (uni)
+        for (int q = 0; q < n + 2; ++q) DC[q] = DE[q] = 2.0 * DCf[0];
       ag_[l][d][0] = E;
       ag_[l][d][1] = C;
       ag_[l][d][2] = DC;
@@ -470,8 +486,57 @@ int MGSolver::build_coefficients(const std::vector<double>& rz) {
   return ANEL_OK;
 }
 
+// ZLINE: the line system of column (i,j) is (a, b, c) = (c5, c7, c6)
+// with c7 = -(c1+c2+c3+c4+d5+d6).  With x/y-uniform coefficients every
+// column has the same system, so the Thomas elimination (mg_relax.F90:
+// 563-566) is done once per level here; the kernel runs the substitution.
+int MGSolver::build_zline_factors() {
+  for (int l = 1; l <= ngrid_; ++l) {
+    const LevelGeom& G = geo_[l];
+    const LevelCoef& c = coef_[l];
+    for (int i = G.s[0]; i <= G.e[0]; ++i)
+      if (!(c.cx1[i - 1] == c.cx1[G.s[0] - 1] && c.cx2[i - 1] == c.cx2[G.s[0] - 1])) {
+        set_error("ZLINE needs x-uniform level coefficients (level %d)", l);
+        return ANEL_ERR_UNSUPPORTED;
+      }
+    for (int j = G.s[1]; j <= G.e[1]; ++j)
+      if (!(c.cy3[j - 1] == c.cy3[G.s[1] - 1] && c.cy4[j - 1] == c.cy4[G.s[1] - 1])) {
+        set_error("ZLINE needs y-uniform level coefficients (level %d)", l);
+        return ANEL_ERR_UNSUPPORTED;
+      }
+    const double a1 = c.cx1[G.s[0] - 1], a2 = c.cx2[G.s[0] - 1];
+    const double a3 = c.cy3[G.s[1] - 1], a4 = c.cy4[G.s[1] - 1];
+    const int n = G.n[2];
+    std::vector<double> ap(G.Z, 0.0), bp(G.Z, 0.0);
+    // rows r = 0..n-1 <-> k = r+2; stored at index k-1
+    double bprev = 0.0;
+    for (int r = 0; r < n; ++r) {
+      const int k = r + 2;
+      const double b = -(a1 + a2 + a3 + a4 + c.dz5[k - 1] + c.dz6[k - 1]);
+      if (r == 0) {
+        bp[k - 1] = b;
+      } else {
+        const double a = -c.cz5[k - 1] / bprev;
+        ap[k - 1] = a;
+        bp[k - 1] = b + a * c.cz6[k - 2];
+      }
+      bprev = bp[k - 1];
+    }
+    std::vector<double> both(ap);
+    both.insert(both.end(), bp.begin(), bp.end());
+    ANEL_CUDA_TRY(cudaMemcpy(d_zf64_[l], both.data(), both.size() * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<float> b32(both.begin(), both.end());
+    ANEL_CUDA_TRY(cudaMemcpy(d_zf32_[l], b32.data(), b32.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return ANEL_OK;
+}
+
 int MGSolver::upload_coefficients() {
   ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (prm_.smoother == ANEL_SMOOTHER_ZLINE) {
+    const int st = build_zline_factors();
+    if (st != ANEL_OK) return st;
+  }
   for (int l = 1; l <= ngrid_; ++l) {
     const LevelCoef& c = coef_[l];
     std::vector<double> packed;
@@ -585,10 +650,13 @@ int MGSolver::coarsen_dirs(int lC) const {
 void MGSolver::relax64(int l, int iters, cudaStream_t s) {
   const DevLevel<double> L = L64(l);
   const bool prof = prof_ && l == ngrid_;
+  const bool zl = prm_.smoother == ANEL_SMOOTHER_ZLINE;
+  const double* zf = d_zf64_[l];
   for (int it = 0; it < iters; ++it) {
     for (int color = 0; color < 2; ++color) {
       if (prof) prof_begin(s);
-      launch_rb_sweep(L, color, s);
+      if (zl) launch_zline(L, color, zf, zf + geo_[l].Z, s);
+      else launch_rb_sweep(L, color, s);
       if (prof) prof_end(s);
       launch_bdry(L, L.phi, s);
     }
@@ -620,10 +688,13 @@ void MGSolver::cycle64(cudaStream_t s) {
 void MGSolver::relax32(int l, int iters, cudaStream_t s) {
   const DevLevel<float> L = L32(l, true);
   const bool prof = prof_ && l == ngrid_;
+  const bool zl = prm_.smoother == ANEL_SMOOTHER_ZLINE;
+  const float* zf = d_zf32_[l];
   for (int it = 0; it < iters; ++it) {
     for (int color = 0; color < 2; ++color) {
       if (prof) prof_begin(s);
-      launch_rb_sweep(L, color, s);
+      if (zl) launch_zline(L, color, zf, zf + geo_[l].Z, s);
+      else launch_rb_sweep(L, color, s);
       if (prof) prof_end(s);
       launch_bdry(L, L.phi, s);
     }
@@ -808,16 +879,14 @@ int MGSolver::debug_pass(int which, double* d_phi, const double* d_src, cudaStre
   if (!s) s = stream_;
   const int ng = ngrid_;
   const DevLevel<double> W = L64(ng);
-  if (which == 0 || which == 1) {
+  if (which == 1) {
     DevLevel<double> F = fine_view(d_phi, d_src);
-    if (which == 0) {
-      launch_rb_sweep(F, 0, s);
-      launch_bdry(F, d_phi, s);
-      launch_rb_sweep(F, 1, s);
-      launch_bdry(F, d_phi, s);
-    } else {
-      launch_bdry(F, d_phi, s);
-    }
+    launch_bdry(F, d_phi, s);
+  } else if (which == 0) {
+    ANEL_CUDA_TRY(cudaMemcpyAsync(W.phi, d_phi, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    ANEL_CUDA_TRY(cudaMemcpyAsync(W.src, d_src, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    relax64(ng, 1, s);
+    ANEL_CUDA_TRY(cudaMemcpyAsync(d_phi, W.phi, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
   } else if (which == 2) {
     ANEL_CUDA_TRY(cudaMemcpyAsync(W.phi, d_phi, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
     ANEL_CUDA_TRY(cudaMemcpyAsync(W.src, d_src, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));

@@ -81,6 +81,10 @@ class MGSolver {
   float* d_phi32_[ANEL_MAX_LEVELS + 1] = {nullptr};
   float* d_src32_[ANEL_MAX_LEVELS + 1] = {nullptr};
   float* d_coef32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  // ZLINE: per level eliminated tridiagonal factors ap[Z], bp[Z]
+  double* d_zf64_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  float* d_zf32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  int build_zline_factors();
   unsigned long long* d_max_ = nullptr;   // 2 words
   double* d_part_ = nullptr;              // norm partials
   double* d_norm_ = nullptr;              // 2 doubles

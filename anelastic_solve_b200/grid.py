@@ -100,13 +100,22 @@ def _axis_from_edges(edges: np.ndarray, gridtype: str) -> Axis:
 
 
 def uniform_axis(n: int, L: float, start: float = 0.0) -> Axis:
-    """Uniform spacing L/n starting at ``start``."""
-    edges = start + L * np.arange(n + 1, dtype=np.float64) / n
-    return _axis_from_edges(edges, "uniform")
+    """Uniform spacing h = L/n starting at ``start``.  dxc, dxe and their
+    reciprocals hold the single value h (1/h) at every index, as the
+    reference's uniform grid files do (ANELASTIC_SL/run_dir/x?_grid.in), so
+    the metric coefficients are bitwise identical along the axis."""
+    h = L / n
+    k = np.arange(n + 2, dtype=np.float64)
+    xe = start + h * k          # xe(1) = start, xe(n+1) = start + L
+    xc = start + h * (k - 0.5)
+    d = np.full(n + 2, h)
+    r = np.full(n + 2, 1.0 / h)
+    return Axis(n=n, L=float(L), xe=xe, xc=xc, dxe=d.copy(), dxc=d.copy(), rdxe=r.copy(),
+                rdxc=r.copy(), x0=float(xc[0]), gridtype="uniform")
 
 
 def tanh_axis(n: int, half: float = 10.0, factor: float = 2.0) -> Axis:
-    """tanh-stretched axis on [-half, half], clustered about 0:
+    """tanh-stretched axis on [-half, half] (cells narrowest at the walls):
     ze_k = half * tanh(factor*s_k)/tanh(factor), s_k = -1 + 2(k-1)/n, k = 1..n+1."""
     s = -1.0 + 2.0 * np.arange(n + 1, dtype=np.float64) / n
     edges = half * np.tanh(factor * s) / math.tanh(factor)

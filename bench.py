@@ -122,11 +122,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+SMOOTHER = {"smoother": "rbpgs"}
+
+
 def mg_params(lv, precision, mode=None):
+    """V(2,2) cycles, metric operator, true-residual stop.  With the ZLINE
+    smoother the z direction is not coarsened (horizontal semi-coarsening)."""
     from anelastic_solve_b200 import abi
 
-    return abi.make_mg_params(lv, maxcy=400, tolmax=TOL, pre=2, post=2, tbc=(0, 1, 0, 1, 0, 0),
+    zl = SMOOTHER["smoother"] == "zline"
+    levels = (lv[0], lv[1], 1) if zl else lv
+    return abi.make_mg_params(levels, maxcy=400, tolmax=TOL, pre=2, post=2, tbc=(0, 1, 0, 1, 0, 0),
                               precision=precision,
+                              smoother=abi.SMOOTHER_ZLINE if zl else abi.SMOOTHER_RBPGS,
                               mode=abi.MODE_METRIC if mode is None else mode, stop=abi.STOP_RESID)
 
 
@@ -385,10 +393,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dns", choices=sorted(WORKLOADS))
     ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--smoother", default="rbpgs", choices=["rbpgs", "zline"],
+                    help="rbpgs: red-black point GS, full coarsening; zline: z-line GS, x/y coarsening")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 multigrid companion")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     args = ap.parse_args()
+    SMOOTHER["smoother"] = args.smoother
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
@@ -400,7 +411,7 @@ def main():
         config = {"workload": f"DNS shear layer {nx}x{ny}x{nz}: Re={phys['Re']:g}, Pr=1, "
                               f"Ri={-phys['g']:g}, amp {phys['amp']:g}, CFL {phys['cfl']:g}, "
                               f"MG to ||f-A p||/||f|| <= {TOL:g} each sub-step",
-                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"RBPGS V(2,2), metric, {args.prec}",
+                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V(2,2), metric, {args.prec}",
                   "ew": 1, "scal1": "off (zero)", "parallelism": f"replicas x{args.gpus}",
                   "l2": "inputs larger than L2 (545 MB per FP64 field)" if nx >= 256 else "small"}
     else:
@@ -408,7 +419,7 @@ def main():
         unit = "cell-solves/s"
         config = {"workload": f"pressure-Poisson solve {nx}x{ny}x{nz}, tanh-stretched z, periodic "
                               f"x/y, Neumann z, to ||f-A phi||/||f|| <= {TOL:g} from phi0 = 0",
-                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"RBPGS V(2,2), metric, {args.prec}",
+                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V(2,2), metric, {args.prec}",
                   "parallelism": f"replicas x{args.gpus}",
                   "l2": "inputs larger than L2 (545 MB per FP64 field)" if nx >= 256 else "small"}
     threads = os.cpu_count() or 1
@@ -458,8 +469,14 @@ def main():
     peak, peak_kind = load_peaks()
     N = r["N"]
     value = world * N / (r["ms_step"] / 1e3)
-    bpc = 6.0 if args.prec == "mixed" else 12.0
-    kernel = "k_rb_sweep<float>" if args.prec == "mixed" else "k_rb_sweep<double>"
+    # smoother bytes per cell and launch (one colour): RB reads phi (all
+    # cells, neighbours), f and writes phi for half the cells -> 12 B FP64;
+    # a z-line colour additionally writes and re-reads the line's
+    # elimination values in place -> 16 B FP64 (halved for FP32)
+    zl = args.smoother == "zline"
+    bpc = (8.0 if zl else 6.0) if args.prec == "mixed" else (16.0 if zl else 12.0)
+    kname = "k_zline" if zl else "k_rb_sweep"
+    kernel = f"{kname}<float>" if args.prec == "mixed" else f"{kname}<double>"
     roof = None
     if r["sweeps"]:
         t_launch = r["sweep_ms"] / r["sweeps"] / 1e3

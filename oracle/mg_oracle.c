@@ -267,6 +267,16 @@ static void agglomerate(orc_mg* m) {
       C[n + 1] = E[n] + 0.5 * DC[n + 1];
       for (int q = 1; q <= n + 1; ++q) DE[q - 1] = C[q] - C[q - 1];
       DE[n + 1] = DE[n];
+      /* a direction whose finer spacings are one value is coarsened
+       * exactly: every coarse spacing is twice it */
+      const int nf2 = m->nk[l + 1][d] + 1;
+      const double* DCf = m->ag[l + 1][d][2];
+      const double* DEf = m->ag[l + 1][d][3];
+      int uni = 1;
+      for (int q = 1; q < nf2; ++q)
+        if (!(DCf[q] == DCf[0] && DEf[q] == DCf[0])) uni = 0;
+      if (uni && DEf[0] == DCf[0])
+        for (int q = 0; q < n + 2; ++q) DC[q] = DE[q] = 2.0 * DCf[0];
     }
   }
 }

@@ -158,3 +158,69 @@ def test_mixed_precision_reaches_fp64_solution(mode):
     got = to_host(dphi)
     assert s2.last_report.status == abi.OK
     assert rel_l2(remove_mean(got), remove_mean(ref)) < 1e-9
+
+
+# ----------------------------------------------------------------- ZLINE
+ZCASES = {
+    # horizontal semi-coarsening (no z levels) and full coarsening
+    "zline_semi": (lambda: G.shear_layer_grid(32, 16, 32, stretched=True), (5, 4, 1)),
+    "zline_full": (lambda: G.shear_layer_grid(32, 16, 32, stretched=True), (5, 4, 5)),
+    "zline_odd": (lambda: G.Grid(G.uniform_axis(12, 1.0), G.uniform_axis(6, 0.5),
+                                 G.tanh_axis(24)), (3, 2, 1)),
+}
+
+
+def _zpair(name, **kw):
+    mk, lv = ZCASES[name]
+    g = mk()
+    p = mg_params(g, levels=lv, tbc=(0, 1, 0, 1, 0, 0), mode=abi.MODE_METRIC,
+                  smoother=abi.SMOOTHER_ZLINE, **kw)
+    return g, p, OracleMG(g, p), MGSolver(g, p)
+
+
+@pytest.mark.parametrize("name", list(ZCASES))
+@pytest.mark.parametrize("which", [0, 2])
+def test_zline_pass_bitwise(name, which):
+    g, p, o, s = _zpair(name)
+    rng = np.random.default_rng(31 + which)
+    phi = field(g, rng)
+    src = field(g, rng)
+    ref = phi.copy(order="F")
+    o.debug_pass(which, ref, src.copy(order="F"))
+    dphi = to_dev(phi)
+    s.debug_pass(which, dphi, to_dev(src))
+    np.testing.assert_array_equal(to_host(dphi), ref)
+
+
+@pytest.mark.parametrize("name", list(ZCASES))
+@pytest.mark.parametrize("stop", [abi.STOP_RELMAX, abi.STOP_RESID])
+def test_zline_solve_bitwise(name, stop):
+    g, p, o, s = _zpair(name, maxcy=40, tolmax=1e-10, stop=stop)
+    rng = np.random.default_rng(8)
+    src = compatible(field(g, rng), g, abi.MODE_METRIC)
+    ref = zeros(g)
+    it_o, rm_o = o.solve(ref, src.copy(order="F"))
+    dphi = to_dev(zeros(g))
+    it_g, rm_g = s.solve(dphi, to_dev(src))
+    assert it_o == it_g
+    if stop == abi.STOP_RELMAX:
+        assert rm_o == rm_g
+    np.testing.assert_array_equal(to_host(dphi), ref)
+
+
+def test_zline_mixed_precision():
+    g = G.shear_layer_grid(32, 16, 32, stretched=True)
+    rng = np.random.default_rng(22)
+    src = compatible(field(g, rng), g, abi.MODE_METRIC)
+    po = mg_params(g, levels=(5, 4, 1), mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE,
+                   maxcy=100, tolmax=1e-13, stop=abi.STOP_RESID)
+    ref = zeros(g)
+    OracleMG(g, po).solve(ref, src.copy(order="F"))
+    pm = mg_params(g, levels=(5, 4, 1), mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE,
+                   maxcy=60, tolmax=1e-12, stop=abi.STOP_RESID, precision=abi.PREC_MIXED)
+    s = MGSolver(g, pm)
+    dphi = to_dev(zeros(g))
+    s.solve(dphi, to_dev(src))
+    assert s.last_report.status == abi.OK and s.last_report.resid <= 1e-12
+    assert s.last_report.iter <= 24
+    assert rel_l2(remove_mean(to_host(dphi)), remove_mean(ref)) < 1e-9
