@@ -378,32 +378,52 @@ __global__ void k_zline_pcr(DevLevel<T> L, int color) {
 
 // Partitioned z-line smoother for the FP32 cycle.  Every line of a level
 // has the same tridiagonal matrix (x/y-uniform coefficients), so the line
-// is cut into P segments whose factors are precomputed on the host:
+// is cut into P segments of m <= MR rows whose factors are precomputed on
+// the host:
 //   phase 1  each segment solves its own rows with the eliminated factors
-//            (ap, bp) ignoring its neighbours -> y;
+//            (ap, 1/bp) ignoring its neighbours -> y, held in registers;
 //   phase 2  the 2P interface values (first and last row of every segment)
 //            follow from y by the precomputed inverse of the interface
 //            system, z = Minv * yb;
 //   phase 3  x = y + u * L(s-1) + v * F(s+1) with the precomputed influence
-//            vectors u (response to the row before the segment) and v.
-// A CTA holds 32 lines (lanes) x P segments (warps); the dependent chain
-// is 2 n/P rows instead of 2 n.  Not bit-matched to the Thomas order (the
-// FP64 path keeps it).
+//            vectors u (response to the row before the segment) and v,
+//            written once.
+// A CTA holds 32 lines (lanes) x P segments (warps); each row is read
+// (source and the four horizontal neighbours) and written exactly once and
+// the dependent chain is 2m rows instead of 2n.  Not bit-matched to the
+// Thomas order (the FP64 path keeps that).
 template <typename T>
 struct SegFac {
   const T* ap;    // segment-local eliminated sub-diagonal, per row (index k-1)
-  const T* bp;    // segment-local eliminated diagonal
+  const T* rbp;   // reciprocal of the segment-local eliminated diagonal
   const T* u;     // influence of the row before the segment
   const T* v;     // influence of the row after the segment
   const T* minv;  // (2P x 2P) inverse of the interface system, row major
 };
 
-template <typename T, int P>
-__global__ void __launch_bounds__(32 * P) k_zline_seg(DevLevel<T> L, int color, SegFac<T> F) {
+template <typename T, int P, int MR>
+__global__ void __launch_bounds__(32 * P, 2) k_zline_seg(DevLevel<T> L, int color, SegFac<T> F) {
+  // y of every row held in shared memory as [row][segment][lane] (each
+  // warp touches 32 consecutive words: no bank conflicts); sized
+  // MR * P * 32 elements by the launcher
+  extern __shared__ unsigned char zs_smem[];
+  T* ys = reinterpret_cast<T*>(zs_smem);
+  constexpr int NMAX = P * MR;
+  // the line factors of the level, staged once per CTA (uniform across the
+  // lanes: shared-memory broadcasts instead of dependent global loads)
+  __shared__ T f_ap[NMAX], f_rbp[NMAX], f_c6[NMAX], f_u[NMAX], f_v[NMAX];
   __shared__ T yb[32][2 * P + 1];
-  __shared__ T zz[32][2 * P + 1];
   const int lane = threadIdx.x;  // line within the CTA
   const int s = threadIdx.y;     // segment
+  const int n = L.nz;
+  const T* __restrict__ cz6 = cz6p(L);
+  for (int q = threadIdx.y * 32 + lane; q < n; q += 32 * P) {
+    f_ap[q] = F.ap[q + 1];
+    f_rbp[q] = F.rbp[q + 1];
+    f_c6[q] = cz6[q + 1];
+    f_u[q] = F.u[q + 1];
+    f_v[q] = F.v[q + 1];
+  }
   const int pairs = (L.nx + 1) >> 1;
   const int64_t t = (int64_t)blockIdx.x * 32 + lane;
   bool active = t < (int64_t)pairs * L.ny;
@@ -414,89 +434,64 @@ __global__ void __launch_bounds__(32 * P) k_zline_seg(DevLevel<T> L, int color, 
     i = i0 + ((color + i0 + j) & 1);
     active = i <= L.nx + 1;
   }
-  const int n = L.nz;
   const int m = n / P;
-  const int lo = s * m, hi = lo + m;  // rows [lo, hi) of the line (row q <-> k = q+2)
-  T y_first = T(0), y_last = T(0);
-  int64_t c0 = 0;
+  const int lo = s * m;  // rows [lo, lo+m) of the line (row q <-> k = q+2)
   const int64_t X = L.X, XY = L.XY;
+  const int64_t c0 = active ? cidx(i, j, 2, L.X, L.XY) + (int64_t)lo * XY : 0;
+  T* yrow = ys + s * 32 + lane;  // row w at yrow[w * P * 32]
+  constexpr int YS = P * 32;
+  // residual rows of the segment (loads only; the factors are not needed)
   if (active) {
     const T a1 = cx1p(L)[i - 1], a2 = cx2p(L)[i - 1];
     const T a3 = cy3p(L)[j - 1], a4 = cy4p(L)[j - 1];
-    const T* __restrict__ cz5 = cz5p(L);
-    const T* __restrict__ cz6 = cz6p(L);
-    T* phi = L.phi;
-    const T* __restrict__ src = L.src;
-    c0 = cidx(i, j, 2, L.X, L.XY);  // row 0
-    constexpr int U = 8;
-    T g = T(0);
-    for (int qb = lo; qb < hi; qb += U) {
-      T r[U];
-#pragma unroll
-      for (int w = 0; w < U; ++w) {
-        const int q = qb + w;
-        if (q < hi) {
-          const int64_t c = c0 + (int64_t)q * XY;
-          r[w] = src[c] - (a1 * phi[c - 1] + a2 * phi[c + 1] + a3 * phi[c - X] + a4 * phi[c + X]);
-          if (q == 0) r[w] = r[w] - cz5[1] * phi[c - XY];
-          if (q == n - 1) r[w] = r[w] - cz6[n] * phi[c + XY];
-        }
-      }
-#pragma unroll
-      for (int w = 0; w < U; ++w) {
-        const int q = qb + w;
-        if (q < hi) {
-          g = (q == lo) ? r[w] : r[w] + F.ap[q + 1] * g;
-          phi[c0 + (int64_t)q * XY] = g;
-        }
-      }
-    }
-    T x = g / F.bp[hi];
-    phi[c0 + (int64_t)(hi - 1) * XY] = x;
-    y_last = x;
-    for (int qb = hi - 2; qb >= lo; qb -= U) {
-      T gv[U];
-#pragma unroll
-      for (int w = 0; w < U; ++w) {
-        const int q = qb - w;
-        if (q >= lo) gv[w] = phi[c0 + (int64_t)q * XY];
-      }
-#pragma unroll
-      for (int w = 0; w < U; ++w) {
-        const int q = qb - w;
-        if (q >= lo) {
-          x = (gv[w] - cz6[q + 1] * x) / F.bp[q + 1];
-          phi[c0 + (int64_t)q * XY] = x;
-        }
-      }
-    }
-    y_first = x;
-  }
-  yb[lane][2 * s] = y_first;
-  yb[lane][2 * s + 1] = y_last;
-  __syncthreads();
-  {
-    T z0 = T(0), z1 = T(0);
-    const T* m0 = F.minv + (size_t)(2 * s) * (2 * P);
-    const T* m1 = m0 + 2 * P;
+    const T* __restrict__ phi = L.phi + c0;
+    const T* __restrict__ src = L.src + c0;
 #pragma unroll 8
-    for (int p = 0; p < 2 * P; ++p) {
-      const T yv = yb[lane][p];
-      z0 += m0[p] * yv;
-      z1 += m1[p] * yv;
+    for (int w = 0; w < m; ++w) {
+      const int c = w * (int)XY;  // < 2^31: m * XY is checked by the launcher
+      yrow[w * YS] = src[c] - (a1 * phi[c - 1] + a2 * phi[c + 1] + a3 * phi[c - X] + a4 * phi[c + X]);
     }
-    zz[lane][2 * s] = z0;
-    zz[lane][2 * s + 1] = z1;
+    if (lo == 0) yrow[0] -= cz5p(L)[1] * phi[-XY];
+    if (lo + m == n) yrow[(m - 1) * YS] -= cz6[n] * phi[(int64_t)(m - 1) * XY + XY];
   }
+  __syncthreads();  // factors staged
+  T yfirst = T(0), ylast = T(0);
+  if (active) {
+    T g = yrow[0];
+    for (int w = 1; w < m; ++w) {
+      g = yrow[w * YS] + f_ap[lo + w] * g;
+      yrow[w * YS] = g;
+    }
+    T x = g * f_rbp[lo + m - 1];
+    yrow[(m - 1) * YS] = x;
+    ylast = x;
+    for (int w = m - 2; w >= 0; --w) {
+      x = (yrow[w * YS] - f_c6[lo + w] * x) * f_rbp[lo + w];
+      yrow[w * YS] = x;
+    }
+    yfirst = x;
+  }
+  yb[lane][2 * s] = yfirst;
+  yb[lane][2 * s + 1] = ylast;
   __syncthreads();
   if (!active) return;
-  const T Lprev = (s > 0) ? zz[lane][2 * s - 1] : T(0);
-  const T Fnext = (s < P - 1) ? zz[lane][2 * s + 2] : T(0);
-  T* phi = L.phi;
-  for (int q = lo; q < hi; ++q) {
-    const int64_t c = c0 + (int64_t)q * XY;
-    phi[c] = phi[c] + F.u[q + 1] * Lprev + F.v[q + 1] * Fnext;
+  // the two interface values this segment needs: L(s-1) = z[2s-1] and
+  // F(s+1) = z[2s+2], z = Minv * yb
+  T Lprev = T(0), Fnext = T(0);
+  if (s > 0) {
+    const T* mr = F.minv + (size_t)(2 * s - 1) * (2 * P);
+#pragma unroll
+    for (int p = 0; p < 2 * P; ++p) Lprev += mr[p] * yb[lane][p];
   }
+  if (s < P - 1) {
+    const T* mr = F.minv + (size_t)(2 * s + 2) * (2 * P);
+#pragma unroll
+    for (int p = 0; p < 2 * P; ++p) Fnext += mr[p] * yb[lane][p];
+  }
+  T* phi = L.phi;
+#pragma unroll 8
+  for (int w = 0; w < m; ++w)
+    phi[c0 + (int64_t)w * XY] = yrow[w * YS] + f_u[lo + w] * Lprev + f_v[lo + w] * Fnext;
 }
 
 // ----------------------------------------------------- residual + restrict

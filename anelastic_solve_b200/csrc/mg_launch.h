@@ -21,8 +21,10 @@ template <typename T>
 void launch_rb_sweep(const DevLevel<T>& L, int color, cudaStream_t s);
 template <typename T>
 void launch_zline(const DevLevel<T>& L, int color, const T* ap, const T* bp, cudaStream_t s);
-// segments of the partitioned FP32 z-line solver (lines must be a multiple)
+// partitioned FP32 z-line solver: kZSeg segments per line, each of
+// 2..kZSegRows rows (lines of nz = kZSeg * m rows)
 constexpr int kZSeg = 16;
+constexpr int kZSegRows = 32;
 template <typename T>
 void launch_zline_seg(const DevLevel<T>& L, int color, const SegFac<T>& F, cudaStream_t s);
 template <typename T>

@@ -45,8 +45,15 @@ void launch_zline(const DevLevel<T>& L, int color, const T* ap, const T* bp, cud
 template <typename T>
 void launch_zline_seg(const DevLevel<T>& L, int color, const SegFac<T>& F, cudaStream_t s) {
   const int64_t cols = (int64_t)((L.nx + 1) / 2) * L.ny;
+  const size_t sm = (size_t)kZSegRows * kZSeg * 32 * sizeof(T);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_zline_seg<T, kZSeg, kZSegRows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sm);
+    attr = true;
+  }
   dim3 block(32, kZSeg, 1);
-  k_zline_seg<T, kZSeg><<<(unsigned)((cols + 31) / 32), block, 0, s>>>(L, color, F);
+  k_zline_seg<T, kZSeg, kZSegRows><<<(unsigned)((cols + 31) / 32), block, sm, s>>>(L, color, F);
   count_launch();
 }
 template <typename T>

@@ -13,6 +13,8 @@
 namespace anel {
 
 static inline int imax(int a, int b) { return a > b ? a : b; }
+int zline_segment_factors(int n, int P, const std::vector<double>& sub, const std::vector<double>& dia,
+                          const std::vector<double>& sup, std::vector<double>& out);
 
 // ------------------------------------------------------------------ init
 MGSolver* MGSolver::create(const anel_grid_desc* g, const anel_mg_params* p, int device,
@@ -188,6 +190,12 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
     if (p->smoother == ANEL_SMOOTHER_ZLINE) {
       ANEL_CUDA_TRY(cudaMalloc(&d_zf64_[l], 2 * (size_t)geo_[l].Z * sizeof(double)));
       ANEL_CUDA_TRY(cudaMalloc(&d_zf32_[l], 2 * (size_t)geo_[l].Z * sizeof(float)));
+      const int nz = geo_[l].n[2];
+      // (the kernel indexes a segment's rows with 32-bit offsets m * X * Y)
+      if (mixed && nz % kZSeg == 0 && nz >= 2 * kZSeg && nz <= kZSeg * kZSegRows &&
+          (int64_t)(nz / kZSeg + 1) * geo_[l].X * geo_[l].Y < (int64_t)1 << 31)
+        ANEL_CUDA_TRY(cudaMalloc(&d_zseg32_[l], (4 * (size_t)geo_[l].Z + 4 * kZSeg * kZSeg) *
+                                                    sizeof(float)));
     }
     if (mixed) {
       ANEL_CUDA_TRY(cudaMalloc(&d_phi32_[l], G * sizeof(float)));
@@ -219,6 +227,7 @@ MGSolver::~MGSolver() {
     cudaFree(d_coef32_[l]);
     cudaFree(d_zf64_[l]);
     cudaFree(d_zf32_[l]);
+    cudaFree(d_zseg32_[l]);
   }
   cudaFree(d_max_);
   cudaFree(d_part_);
@@ -527,6 +536,131 @@ int MGSolver::build_zline_factors() {
     ANEL_CUDA_TRY(cudaMemcpy(d_zf64_[l], both.data(), both.size() * sizeof(double), cudaMemcpyHostToDevice));
     std::vector<float> b32(both.begin(), both.end());
     ANEL_CUDA_TRY(cudaMemcpy(d_zf32_[l], b32.data(), b32.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (d_zseg32_[l]) {
+      std::vector<double> sub(n), dia(n), sup(n);
+      for (int r = 0; r < n; ++r) {
+        const int k = r + 2;
+        sub[r] = c.cz5[k - 1];
+        sup[r] = c.cz6[k - 1];
+        dia[r] = -(a1 + a2 + a3 + a4 + c.dz5[k - 1] + c.dz6[k - 1]);
+      }
+      std::vector<double> seg;
+      const int st = zline_segment_factors(n, kZSeg, sub, dia, sup, seg);
+      if (st != ANEL_OK) return st;
+      // rows r <-> index r+1 (the layout of the Thomas factors above)
+      std::vector<float> f32(4 * (size_t)G.Z + 4 * kZSeg * kZSeg, 0.0f);
+      for (int a = 0; a < 4; ++a)
+        for (int r = 0; r < n; ++r) {
+          const double f = seg[(size_t)a * n + r];
+          f32[(size_t)a * G.Z + r + 1] = (float)(a == 1 ? 1.0 / f : f);  // bp -> 1/bp
+        }
+      for (int q = 0; q < 4 * kZSeg * kZSeg; ++q) f32[4 * (size_t)G.Z + q] = (float)seg[4 * (size_t)n + q];
+      ANEL_CUDA_TRY(cudaMemcpy(d_zseg32_[l], f32.data(), f32.size() * sizeof(float),
+                               cudaMemcpyHostToDevice));
+    }
+  }
+  return ANEL_OK;
+}
+
+// Factors of the partitioned line solver: the n rows of the tridiagonal
+// system (sub, dia, sup) are cut into P segments of m = n/P rows.  Output,
+// each array of n values followed by the (2P)^2 interface inverse:
+//   ap, bp  Thomas factors of every segment taken alone (first row of a
+//           segment: bp = dia, ap unused);
+//   u, v    the segment's solution for a unit value in the row before it
+//           (u, coupling -sub[lo]) and in the row after it (v, -sup[hi-1]);
+//   minv    inverse of I - K, K coupling the interface unknowns
+//           (F_0, L_0, F_1, L_1, ...) = first/last row of each segment.
+int zline_segment_factors(int n, int P, const std::vector<double>& sub, const std::vector<double>& dia,
+                          const std::vector<double>& sup, std::vector<double>& out) {
+  const int m = n / P;
+  const int P2 = 2 * P;
+  out.assign(4 * (size_t)n + (size_t)P2 * P2, 0.0);
+  double* ap = out.data();
+  double* bp = ap + n;
+  double* u = bp + n;
+  double* v = u + n;
+  double* minv = v + n;
+  auto solve_seg = [&](int lo, int hi, std::vector<double>& rhs) {
+    double g = rhs[lo];
+    std::vector<double> gs(hi - lo);
+    gs[0] = g;
+    for (int q = lo + 1; q < hi; ++q) {
+      g = rhs[q] + ap[q] * g;
+      gs[q - lo] = g;
+    }
+    double x = g / bp[hi - 1];
+    rhs[hi - 1] = x;
+    for (int q = hi - 2; q >= lo; --q) {
+      x = (gs[q - lo] - sup[q] * x) / bp[q];
+      rhs[q] = x;
+    }
+  };
+  std::vector<double> M((size_t)P2 * P2, 0.0);
+  for (int s = 0; s < P; ++s) {
+    const int lo = s * m, hi = lo + m;
+    bp[lo] = dia[lo];
+    for (int q = lo + 1; q < hi; ++q) {
+      ap[q] = -sub[q] / bp[q - 1];
+      bp[q] = dia[q] + ap[q] * sup[q - 1];
+    }
+    for (int q = lo; q < hi; ++q)
+      if (!(std::isfinite(bp[q]) && bp[q] != 0.0)) {
+        set_error("z-line segment %d is singular at row %d", s, q);
+        return ANEL_ERR_NONFINITE;
+      }
+    std::vector<double> w(n, 0.0);
+    if (s > 0) {
+      w[lo] = -sub[lo];
+      solve_seg(lo, hi, w);
+      for (int q = lo; q < hi; ++q) u[q] = w[q];
+    }
+    if (s < P - 1) {
+      std::fill(w.begin(), w.end(), 0.0);
+      w[hi - 1] = -sup[hi - 1];
+      solve_seg(lo, hi, w);
+      for (int q = lo; q < hi; ++q) v[q] = w[q];
+    }
+    M[(size_t)(2 * s) * P2 + 2 * s] = 1.0;
+    M[(size_t)(2 * s + 1) * P2 + 2 * s + 1] = 1.0;
+    if (s > 0) {
+      M[(size_t)(2 * s) * P2 + 2 * s - 1] -= u[lo];
+      M[(size_t)(2 * s + 1) * P2 + 2 * s - 1] -= u[hi - 1];
+    }
+    if (s < P - 1) {
+      M[(size_t)(2 * s) * P2 + 2 * s + 2] -= v[lo];
+      M[(size_t)(2 * s + 1) * P2 + 2 * s + 2] -= v[hi - 1];
+    }
+  }
+  // Gauss-Jordan with partial pivoting
+  for (int r = 0; r < P2; ++r) minv[(size_t)r * P2 + r] = 1.0;
+  for (int c = 0; c < P2; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < P2; ++r)
+      if (std::fabs(M[(size_t)r * P2 + c]) > std::fabs(M[(size_t)piv * P2 + c])) piv = r;
+    if (!(std::fabs(M[(size_t)piv * P2 + c]) > 0.0)) {
+      set_error("z-line interface system is singular");
+      return ANEL_ERR_NONFINITE;
+    }
+    if (piv != c)
+      for (int q = 0; q < P2; ++q) {
+        std::swap(M[(size_t)c * P2 + q], M[(size_t)piv * P2 + q]);
+        std::swap(minv[(size_t)c * P2 + q], minv[(size_t)piv * P2 + q]);
+      }
+    const double d = M[(size_t)c * P2 + c];
+    for (int q = 0; q < P2; ++q) {
+      M[(size_t)c * P2 + q] /= d;
+      minv[(size_t)c * P2 + q] /= d;
+    }
+    for (int r = 0; r < P2; ++r) {
+      if (r == c) continue;
+      const double f = M[(size_t)r * P2 + c];
+      if (f == 0.0) continue;
+      for (int q = 0; q < P2; ++q) {
+        M[(size_t)r * P2 + q] -= f * M[(size_t)c * P2 + q];
+        minv[(size_t)r * P2 + q] -= f * minv[(size_t)c * P2 + q];
+      }
+    }
   }
   return ANEL_OK;
 }
@@ -690,10 +824,14 @@ void MGSolver::relax32(int l, int iters, cudaStream_t s) {
   const bool prof = prof_ && l == ngrid_;
   const bool zl = prm_.smoother == ANEL_SMOOTHER_ZLINE;
   const float* zf = d_zf32_[l];
+  const float* zs = d_zseg32_[l];
+  const int Z = geo_[l].Z;
+  const SegFac<float> sf{zs, zs + Z, zs + 2 * Z, zs + 3 * Z, zs + 4 * Z};
   for (int it = 0; it < iters; ++it) {
     for (int color = 0; color < 2; ++color) {
       if (prof) prof_begin(s);
-      if (zl) launch_zline(L, color, zf, zf + geo_[l].Z, s);
+      if (zl && zs) launch_zline_seg(L, color, sf, s);
+      else if (zl) launch_zline(L, color, zf, zf + geo_[l].Z, s);
       else launch_rb_sweep(L, color, s);
       if (prof) prof_end(s);
       launch_bdry(L, L.phi, s);

@@ -84,6 +84,10 @@ class MGSolver {
   // ZLINE: per level eliminated tridiagonal factors ap[Z], bp[Z]
   double* d_zf64_[ANEL_MAX_LEVELS + 1] = {nullptr};
   float* d_zf32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  // partitioned z-line factors of the FP32 cycle (ap, 1/bp, u, v: Z each;
+  // then the 2P x 2P interface inverse), null where the level's nz does
+  // not split into kZSeg segments of at least two rows
+  float* d_zseg32_[ANEL_MAX_LEVELS + 1] = {nullptr};
   int build_zline_factors();
   unsigned long long* d_max_ = nullptr;   // 2 words
   double* d_part_ = nullptr;              // norm partials

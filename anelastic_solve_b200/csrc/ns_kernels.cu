@@ -459,22 +459,35 @@ __global__ void k_pgrad_column(NSDev D, double dt, ZRule Ru, ZRule Rv, ZRule Rw)
 // -------------------------------------------------------------- calcdt
 // Routines.F90:221-233: max over the interior of the advective CFL rate
 // (order x, z, y as in the reference), exact integer max of the bits.
-__global__ void k_cfl_max(NSDev D, unsigned long long* out) {
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = 2 + blockIdx.y;
-  const int k = 2 + blockIdx.z;
+__global__ void __launch_bounds__(256) k_cfl_max(NSDev D, unsigned long long* out) {
+  // grid-stride over the interior; the maximum of non-negative doubles is
+  // taken on their bit patterns, so the result is exact in any order
+  __shared__ unsigned long long sh[8];
+  const int64_t nx = D.nx, nxy = (int64_t)D.nx * D.ny;
+  const int64_t n = nxy * D.nz;
   unsigned long long m = 0;
-  if (i <= D.nx + 1) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int k = 2 + (int)(q / nxy);
+    const int64_t r = q - (int64_t)(k - 2) * nxy;
+    const int j = 2 + (int)(r / nx);
+    const int i = 2 + (int)(r - (int64_t)(j - 2) * nx);
     const double adv = MT(D.rdxc, i) * fabs(0.5 * (FA(D.u, i, j, k) + FA(D.u, i - 1, j, k))) +
                        MT(D.rdzc, k) * fabs(0.5 * (FA(D.w, i, j, k) + FA(D.w, i, j, k - 1))) +
                        MT(D.rdyc, j) * fabs(0.5 * (FA(D.v, i, j, k) + FA(D.v, i, j - 1, k)));
-    m = __double_as_longlong(adv);
+    const unsigned long long b = __double_as_longlong(adv);
+    m = b > m ? b : m;
   }
   for (int o = 16; o > 0; o >>= 1) {
     const unsigned long long w = __shfl_xor_sync(0xffffffffu, m, o);
     m = w > m ? w : m;
   }
-  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) m = sh[q] > m ? sh[q] : m;
+    atomicMax(out, m);
+  }
 }
 
 // divergence (Routines.F90:121-146): max |div| (exact) and the
@@ -564,8 +577,10 @@ void launch_ghost_field(const NSDev& D, double* a, const ZRule& R, cudaStream_t 
 }
 
 void launch_cfl_max(const NSDev& D, unsigned long long* out, cudaStream_t s) {
-  const int tx = 128;
-  k_cfl_max<<<cell_grid(D, tx), tx, 0, s>>>(D, out);
+  const int64_t cells = (int64_t)D.nx * D.ny * D.nz;
+  int64_t blocks = (cells + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_cfl_max<<<(unsigned)blocks, 256, 0, s>>>(D, out);
   count_launch();
 }
 

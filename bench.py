@@ -51,6 +51,8 @@ WORKLOADS = {
     "poisson": ("poisson", (512, 256, 512), (9, 8, 9), {}),
     "poisson256": ("poisson", (256, 256, 256), (8, 8, 8), {}),
     "poisson_small": ("poisson", (64, 32, 64), (6, 5, 6), {}),
+    # profiling case: 134 MB per FP32 field (above L2), ~1.5 GB on the device
+    "poisson_prof": ("poisson", (512, 128, 512), (9, 7, 9), {}),
 }
 TOL = 1e-10
 
