@@ -71,27 +71,33 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return s;
 }
 
+// The interior is walked as x-rows (j, k): a CTA takes rows blockIdx.x,
+// blockIdx.x + gridDim.x, ... and its threads run along i, so the index
+// math is one 32-bit division per row.  The per-thread accumulation order
+// is fixed by the launch shape, so the sums are deterministic.
 template <bool kStore>
-__global__ void k_resid_norm(DevLevel<double> L, const double* __restrict__ phi,
-                             const double* __restrict__ f, float* __restrict__ r32,
-                             double* __restrict__ part) {
+__global__ void __launch_bounds__(kNormThreads) k_resid_norm(DevLevel<double> L,
+                                                            const double* __restrict__ phi,
+                                                            const double* __restrict__ f,
+                                                            float* __restrict__ r32,
+                                                            double* __restrict__ part) {
   __shared__ double sh[kNormThreads / 32];
   double rr = 0.0, ff = 0.0;
-  const int64_t N = (int64_t)L.nx * L.ny * L.nz;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int i = 2 + (int)(t % L.nx);
-    const int64_t r = t / L.nx;
-    const int j = 2 + (int)(r % L.ny);
-    const int k = 2 + (int)(r / L.ny);
-    const int64_t c = cidx(i, j, k, L.X, L.XY);
-    DevLevel<double> Lp = L;
-    Lp.phi = const_cast<double*>(phi);
-    Lp.src = const_cast<double*>(f);
-    const double res = fine_resid(Lp, i, j, k);
-    if (kStore) r32[c] = (float)res;
-    rr += res * res;
-    ff += f[c] * f[c];
+  DevLevel<double> Lp = L;
+  Lp.phi = const_cast<double*>(phi);
+  Lp.src = const_cast<double*>(f);
+  const int nrow = L.ny * L.nz;
+  for (int row = blockIdx.x; row < nrow; row += gridDim.x) {
+    const int j = 2 + row % L.ny;
+    const int k = 2 + row / L.ny;
+    const int64_t base = cidx(0, j, k, L.X, L.XY);
+    for (int i = 2 + threadIdx.x; i <= L.nx + 1; i += blockDim.x) {
+      const int64_t c = base + i;
+      const double res = fine_resid(Lp, i, j, k);
+      if (kStore) r32[c] = (float)res;
+      rr += res * res;
+      ff += f[c] * f[c];
+    }
   }
   const double s1 = block_sum(rr, sh);
   const double s2 = block_sum(ff, sh);
@@ -117,7 +123,8 @@ __global__ void k_fold(const double* __restrict__ part, int nb, double* out) {
 }
 
 int resid_norm_blocks(const DevLevel<double>& L) {
-  return gs_blocks((int64_t)L.nx * L.ny * L.nz, kNormThreads);
+  const int64_t rows = (int64_t)L.ny * L.nz;
+  return (int)(rows < 148 * 8 ? rows : 148 * 8);
 }
 
 void launch_resid_norm(const DevLevel<double>& L, const double* phi, const double* f, double* part,
@@ -136,22 +143,20 @@ void launch_resid_store(const DevLevel<double>& L, const double* phi, const doub
   count_launch(2);
 }
 
-__global__ void k_add_correction(DevLevel<double> L, double* __restrict__ phi,
-                                 const float* __restrict__ e) {
-  const int64_t N = (int64_t)L.nx * L.ny * L.nz;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < N;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int i = 2 + (int)(t % L.nx);
-    const int64_t r = t / L.nx;
-    const int j = 2 + (int)(r % L.ny);
-    const int k = 2 + (int)(r / L.ny);
-    const int64_t c = cidx(i, j, k, L.X, L.XY);
-    phi[c] = phi[c] + (double)e[c];
+__global__ void __launch_bounds__(256) k_add_correction(DevLevel<double> L, double* __restrict__ phi,
+                                                       const float* __restrict__ e) {
+  const int nrow = L.ny * L.nz;
+  for (int row = blockIdx.x; row < nrow; row += gridDim.x) {
+    const int j = 2 + row % L.ny;
+    const int k = 2 + row / L.ny;
+    const int64_t base = cidx(0, j, k, L.X, L.XY);
+    for (int i = 2 + threadIdx.x; i <= L.nx + 1; i += blockDim.x) phi[base + i] = phi[base + i] + (double)e[base + i];
   }
 }
 
 void launch_add_correction(const DevLevel<double>& L, double* phi, const float* e, cudaStream_t s) {
-  k_add_correction<<<gs_blocks((int64_t)L.nx * L.ny * L.nz), 256, 0, s>>>(L, phi, e);
+  const int64_t rows = (int64_t)L.ny * L.nz;
+  k_add_correction<<<(unsigned)(rows < 148 * 8 ? rows : 148 * 8), 256, 0, s>>>(L, phi, e);
   count_launch();
 }
 

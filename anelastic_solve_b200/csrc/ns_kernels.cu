@@ -246,7 +246,7 @@ __device__ __forceinline__ double rhs_scalar(const NSDev& D, int i, int j, int k
 // first = substep with a1 = 0 after zero_temps: q is known to be zero,
 // so it is not read (0*0 + x == 0 + x).
 template <bool kFirst>
-__global__ void k_rhs_accum(NSDev D, double a1, double a2, double dt) {
+__global__ void __launch_bounds__(128, 8) k_rhs_accum(NSDev D, double a1, double a2, double dt) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
   const int k = 2 + blockIdx.z;
@@ -362,51 +362,108 @@ struct CNFac {
   const double *ap, *bp, *c, *t1, *t2, *rb, *isbc;
 };
 
+// The per-row factors and z metrics are staged in shared memory (stride
+// n+1 doubles each: ap, bp, c, t1, t2, rb, isbc, rdze, rdzc) and both
+// sweeps run in batches of kCNU rows whose global loads are issued before
+// any of the batch's stores, so a column costs n/kCNU memory latencies
+// instead of n.  The arithmetic and its order are those of the
+// row-by-row Thomas algorithm.
+constexpr int kCNU = 8;
+constexpr int kCNThreads = 256;
+
 template <int kVar>
-__global__ void k_cn_column(NSDev D, double* __restrict__ fld, const double* __restrict__ q,
-                            CNFac F, double a3, double rkdt, ZRule R) {
+__global__ void __launch_bounds__(kCNThreads) k_cn_column(NSDev D, double* __restrict__ fld,
+                                                          const double* __restrict__ q, CNFac F,
+                                                          double a3, double rkdt, ZRule R) {
+  extern __shared__ double cn_sm[];
+  const int n = D.nz + 2;
+  const int S = n + 1;
+  double* s_ap = cn_sm;
+  double* s_bp = s_ap + S;
+  double* s_c = s_bp + S;
+  double* s_t1 = s_c + S;
+  double* s_t2 = s_t1 + S;
+  double* s_rb = s_t2 + S;
+  double* s_bc = s_rb + S;
+  double* s_re = s_bc + S;  // rdze
+  double* s_rc = s_re + S;  // rdzc
+  for (int r = threadIdx.x; r < S; r += blockDim.x) {
+    const bool in = r < n;
+    s_ap[r] = in ? F.ap[r] : 0.0;
+    s_bp[r] = in ? F.bp[r] : 1.0;
+    s_c[r] = in ? F.c[r] : 0.0;
+    s_t1[r] = in ? F.t1[r] : 0.0;
+    s_t2[r] = in ? F.t2[r] : 0.0;
+    s_rb[r] = in ? F.rb[r] : 0.0;
+    s_bc[r] = in ? F.isbc[r] : 1.0;
+    s_re[r] = in ? D.rdze[r] : 0.0;
+    s_rc[r] = in ? D.rdzc[r] : 0.0;
+  }
+  __syncthreads();
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
   if (i > D.nx + 1) return;
-  const int n = D.nz + 2;
   const int64_t base = NS_IX(i, j, 1);
   const int64_t XY = D.XY;
   // forward sweep: G(k) = rhs(k) + ap(k) G(k-1); G is stored in place
-  double um = fld[base];            // u_old(k-1)
-  double uk = fld[base + XY];       // u_old(k)
-  double g = F.rb[0];               // row 1 is a wall row
+  double um = fld[base];       // u_old(k-1)
+  double uk = fld[base + XY];  // u_old(k)
+  double g = s_rb[0];          // row 1 is a wall row
   fld[base] = g;
-  for (int k = 2; k <= n; ++k) {
-    const int64_t o = base + (int64_t)(k - 1) * XY;
-    const double up = (k < n) ? fld[o + XY] : 0.0;  // u_old(k+1)
-    double rhs;
-    if (F.isbc[k - 1] != 0.0) {
-      rhs = F.rb[k - 1];
-    } else {
-      rhs = 1.0 * uk + a3 * q[o] * 1.0;
-      if (kVar != 3)
-        rhs = rhs + rkdt * 0.5 *
-                        (F.t2[k - 1] * (up - uk) * MT(D.rdze, k) -
-                         F.t1[k - 1] * (uk - um) * MT(D.rdze, k - 1)) *
-                        MT(D.rdzc, k);
-      else
-        rhs = rhs + rkdt * 0.5 *
-                        (F.t2[k - 1] * (up - uk) * MT(D.rdzc, k + 1) -
-                         F.t1[k - 1] * (uk - um) * MT(D.rdzc, k)) *
-                        MT(D.rdze, k);
+  for (int kb = 2; kb <= n; kb += kCNU) {
+    double up[kCNU], qv[kCNU];
+#pragma unroll
+    for (int u = 0; u < kCNU; ++u) {
+      const int k = kb + u;
+      const int64_t o = base + (int64_t)(k - 1) * XY;
+      up[u] = (k < n) ? fld[o + XY] : 0.0;  // u_old(k+1)
+      qv[u] = (k <= n) ? q[o] : 0.0;
     }
-    g = rhs + F.ap[k - 1] * g;
-    fld[o] = g;
-    um = uk;
-    uk = up;
+#pragma unroll
+    for (int u = 0; u < kCNU; ++u) {
+      const int k = kb + u;
+      if (k <= n) {
+        double rhs;
+        if (s_bc[k - 1] != 0.0) {
+          rhs = s_rb[k - 1];
+        } else {
+          rhs = 1.0 * uk + a3 * qv[u] * 1.0;
+          if (kVar != 3)
+            rhs = rhs + rkdt * 0.5 *
+                            (s_t2[k - 1] * (up[u] - uk) * s_re[k - 1] -
+                             s_t1[k - 1] * (uk - um) * s_re[k - 2]) *
+                            s_rc[k - 1];
+          else
+            rhs = rhs + rkdt * 0.5 *
+                            (s_t2[k - 1] * (up[u] - uk) * s_rc[k] -
+                             s_t1[k - 1] * (uk - um) * s_rc[k - 1]) *
+                            s_re[k - 1];
+        }
+        g = rhs + s_ap[k - 1] * g;
+        fld[base + (int64_t)(k - 1) * XY] = g;
+        um = uk;
+        uk = up[u];
+      }
+    }
   }
   // back substitution: G(n) = G(n)/bp(n); G(k) = (G(k) - c(k) G(k+1))/bp(k)
-  double gn = fld[base + (int64_t)(n - 1) * XY] / F.bp[n - 1];
+  double gn = g / s_bp[n - 1];
   fld[base + (int64_t)(n - 1) * XY] = gn;
-  for (int k = n - 1; k >= 1; --k) {
-    const int64_t o = base + (int64_t)(k - 1) * XY;
-    gn = (fld[o] - F.c[k - 1] * gn) / F.bp[k - 1];
-    fld[o] = gn;
+  for (int kb = n - 1; kb >= 1; kb -= kCNU) {
+    double gv[kCNU];
+#pragma unroll
+    for (int u = 0; u < kCNU; ++u) {
+      const int k = kb - u;
+      gv[u] = (k >= 1) ? fld[base + (int64_t)(k - 1) * XY] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kCNU; ++u) {
+      const int k = kb - u;
+      if (k >= 1) {
+        gn = (gv[u] - s_c[k - 1] * gn) / s_bp[k - 1];
+        fld[base + (int64_t)(k - 1) * XY] = gn;
+      }
+    }
   }
   zghost_column(D, R, fld, base);
   copy_images(D, fld, i, j);
@@ -431,22 +488,28 @@ __global__ void k_psource(NSDev D, double rdt) {
 }
 
 // ------------------------------------------------------ Pgrad + ghosts
-// Pgrad (NSsolver.F90:2023-2085) on one column, then ghost(u,'u'),
-// ghost(v,'v'), ghost(w,'w') (NSsolver.F90:572-574).
-__global__ void k_pgrad_column(NSDev D, double dt, ZRule Ru, ZRule Rv, ZRule Rw) {
+// Pgrad (NSsolver.F90:2023-2085): one thread per interior cell (the update
+// of a cell reads p only), then ghost(u,'u'), ghost(v,'v'), ghost(w,'w')
+// (NSsolver.F90:572-574) by columns.
+__global__ void __launch_bounds__(128) k_pgrad(NSDev D, double dt) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > D.nx + 1) return;
+  const int kend_w = D.nz + 1 - D.ew;
+  const double* __restrict__ p = D.p;
+  const double rk = D.rz[k - 1];
+  const double pk = FA(p, i, j, k);
+  FA(D.u, i, j, k) = FA(D.u, i, j, k) - (FA(p, i + 1, j, k) / rk - pk / rk) * MT(D.rdxe, i) * dt;
+  FA(D.v, i, j, k) = FA(D.v, i, j, k) - (FA(p, i, j + 1, k) / rk - pk / rk) * MT(D.rdye, j) * dt;
+  if (k <= kend_w)
+    FA(D.w, i, j, k) = FA(D.w, i, j, k) - (FA(p, i, j, k + 1) / D.rz[k] - pk / rk) * MT(D.rdze, k) * dt;
+}
+
+__global__ void k_pgrad_ghost(NSDev D, ZRule Ru, ZRule Rv, ZRule Rw) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
   if (i > D.nx + 1) return;
-  const int kend_w = D.nz + 1 - D.ew;
-  for (int k = 2; k <= D.nz + 1; ++k) {
-    const double rk = D.rz[k - 1];
-    const double pk = FA(D.p, i, j, k);
-    FA(D.u, i, j, k) = FA(D.u, i, j, k) - (FA(D.p, i + 1, j, k) / rk - pk / rk) * MT(D.rdxe, i) * dt;
-    FA(D.v, i, j, k) = FA(D.v, i, j, k) - (FA(D.p, i, j + 1, k) / rk - pk / rk) * MT(D.rdye, j) * dt;
-    if (k <= kend_w)
-      FA(D.w, i, j, k) =
-          FA(D.w, i, j, k) - (FA(D.p, i, j, k + 1) / D.rz[k] - pk / rk) * MT(D.rdze, k) * dt;
-  }
   const int64_t base = NS_IX(i, j, 1);
   zghost_column(D, Ru, D.u, base);
   zghost_column(D, Rv, D.v, base);
@@ -550,10 +613,17 @@ void launch_rhs_accum(const NSDev& D, double a1, double a2, double dt, bool firs
 
 void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
                double rkdt, const ZRule& R, cudaStream_t s) {
-  const int tx = 64;
+  const int tx = kCNThreads;
   CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc};
-  if (var == 3) k_cn_column<3><<<col_grid(D, tx), tx, 0, s>>>(D, fld, q, f, a3, rkdt, R);
-  else k_cn_column<1><<<col_grid(D, tx), tx, 0, s>>>(D, fld, q, f, a3, rkdt, R);
+  const size_t sm = 9 * (size_t)(D.nz + 3) * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_cn_column<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_cn_column<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  if (var == 3) k_cn_column<3><<<col_grid(D, tx), tx, sm, s>>>(D, fld, q, f, a3, rkdt, R);
+  else k_cn_column<1><<<col_grid(D, tx), tx, sm, s>>>(D, fld, q, f, a3, rkdt, R);
   count_launch();
 }
 
@@ -565,9 +635,9 @@ void launch_psource(const NSDev& D, double dt, cudaStream_t s) {
 
 void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, const ZRule& Rw,
                   cudaStream_t s) {
-  const int tx = 64;
-  k_pgrad_column<<<col_grid(D, tx), tx, 0, s>>>(D, dt, Ru, Rv, Rw);
-  count_launch();
+  k_pgrad<<<cell_grid(D, 128), 128, 0, s>>>(D, dt);
+  k_pgrad_ghost<<<col_grid(D, 64), 64, 0, s>>>(D, Ru, Rv, Rw);
+  count_launch(2);
 }
 
 void launch_ghost_field(const NSDev& D, double* a, const ZRule& R, cudaStream_t s) {

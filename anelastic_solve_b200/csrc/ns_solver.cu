@@ -78,6 +78,12 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
     set_error("ew must be 0 or 1");
     return ANEL_ERR_ARG;
   }
+  // the Crank-Nicolson kernel stages 9 column profiles of nz+3 doubles in
+  // shared memory (200 KB at most)
+  if (9 * (int64_t)(nz_ + 3) * 8 > 200 * 1024) {
+    set_error("nz = %d exceeds the column solver's limit of 2841", nz_);
+    return ANEL_ERR_UNSUPPORTED;
+  }
   const int n[3] = {nx_, ny_, nz_};
   const double* src[3][6] = {{g->xe, g->xc, g->dxe, g->dxc, g->rdxe, g->rdxc},
                              {g->ye, g->yc, g->dye, g->dyc, g->rdye, g->rdyc},
