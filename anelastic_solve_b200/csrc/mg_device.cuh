@@ -25,6 +25,10 @@ struct DevLevel {
   T* src;
   const T* coef;   // cx1[X] cx2[X] cy3[Y] cy4[Y] cz5[Z] cz6[Z] dz5[Z] dz6[Z]
   BdryRule rule;
+  // optional ghost table of a homogeneous rule (all boundary values 0):
+  // gtab[g] = {ghost cell, interior cell it copies or -1 for 0}; null = the
+  // rule is evaluated by ghost_value
+  const int2* gtab;
 };
 
 template <typename T>
@@ -149,15 +153,83 @@ __device__ __forceinline__ void ghost_cell(int64_t g, int X, int Y, int Z, int& 
   k = 2 + (int)(r / ny);
 }
 
+// Source of ghost cell (i,j,k) under a homogeneous rule: the walk of
+// ghost_value without its arithmetic.  With every boundary value 0 the
+// Neumann additions vanish, so the ghost is a copy of the interior cell the
+// walk ends on, or 0 when it ends on a Dirichlet face.
 template <typename T>
-__global__ void k_bdry(DevLevel<T> L, T* __restrict__ phi) {
+__device__ __forceinline__ int64_t ghost_source(const DevLevel<T>& L, int i, int j, int k) {
+  const BdryRule& R = L.rule;
+  int t = 9;
+  const int X = L.X, Y = L.Y, Z = L.Z;
+  for (;;) {
+    int p = 0;
+    if (t >= 9 && R.type[5] && i == X) p = 9;
+    else if (t >= 8 && R.type[4] && i == 1) p = 8;
+    else if (t >= 7 && R.type[3] && k == Z) p = 7;
+    else if (t >= 6 && R.type[2] && j == 1) p = 6;
+    else if (t >= 5 && R.type[1] && k == 1) p = 5;
+    else if (t >= 4 && R.type[0] && j == Y) p = 4;
+    else if (t >= 3 && (k == 1 || k == Z)) p = 3;
+    else if (t >= 2 && (j == 1 || j == Y)) p = 2;
+    else if (t >= 1 && (i == 1 || i == X)) p = 1;
+    if (p == 0) return cidx(i, j, k, X, L.XY);
+    if (p >= 4) {
+      const int face = p - 4;
+      if (R.type[face] == 2) return -1;
+      switch (face) {
+        case 0: j = Y - 1; break;
+        case 1: k = 2; break;
+        case 2: j = 2; break;
+        case 3: k = Z - 1; break;
+        case 4: i = 2; break;
+        default: i = X - 1; break;
+      }
+    } else if (p == 3) {
+      k = (k == 1) ? Z - 1 : 2;
+    } else if (p == 2) {
+      j = (j == 1) ? Y - 1 : 2;
+    } else {
+      i = (i == 1) ? X - 1 : 2;
+    }
+    t = p - 1;
+  }
+}
+
+// Fill the ghost table of a level with a homogeneous rule (G < 2^31).
+template <typename T>
+__global__ void k_ghost_table(DevLevel<T> L, int2* __restrict__ tab) {
   const int64_t nghost = L.G - (int64_t)L.nx * L.ny * L.nz;
   for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < nghost;
        g += (int64_t)gridDim.x * blockDim.x) {
     int i, j, k;
     ghost_cell(g, L.X, L.Y, L.Z, i, j, k);
+    tab[g] = make_int2((int)cidx(i, j, k, L.X, L.XY), (int)ghost_source(L, i, j, k));
+  }
+}
+
+// Ghost cells t0, t0+stride, ... of level L (the body of k_bdry).
+template <typename T>
+__device__ __forceinline__ void bdry_range(const DevLevel<T>& L, T* __restrict__ phi, int64_t t0,
+                                           int64_t stride) {
+  const int64_t nghost = L.G - (int64_t)L.nx * L.ny * L.nz;
+  if (L.gtab) {
+    for (int64_t g = t0; g < nghost; g += stride) {
+      const int2 e = L.gtab[g];
+      phi[e.x] = e.y >= 0 ? phi[e.y] : T(0);
+    }
+    return;
+  }
+  for (int64_t g = t0; g < nghost; g += stride) {
+    int i, j, k;
+    ghost_cell(g, L.X, L.Y, L.Z, i, j, k);
     phi[cidx(i, j, k, L.X, L.XY)] = ghost_value(L, phi, i, j, k);
   }
+}
+
+template <typename T>
+__global__ void k_bdry(DevLevel<T> L, T* __restrict__ phi) {
+  bdry_range(L, phi, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
 }
 
 // ------------------------------------------------------------- RB sweep
@@ -399,33 +471,51 @@ struct SegFac {
   const T* u;     // influence of the row before the segment
   const T* v;     // influence of the row after the segment
   const T* minv;  // (2P x 2P) inverse of the interface system, row major
+  // ghost copies written by the sweep itself (homogeneous rule), or null:
+  // img[3*((i-2) + nx*(j-2)) + e] = offset of the e-th ghost column that
+  // copies line (i,j) (kNoImage: none); z1/zZ = source of the k=1 / k=Z
+  // ghost of every column (0: zero, 1: row k=2, 2: row k=nz+1)
+  const int* img;
+  int z1, zZ;
+};
+constexpr int kNoImage = -2147483647 - 1;
+
+// Shared state of the partitioned solver: the line factors of the level,
+// staged once per CTA (uniform across the lanes: shared-memory broadcasts
+// instead of dependent global loads) and the interface values.
+template <typename T, int P, int MR>
+struct ZSegShared {
+  T ap[P * MR], rbp[P * MR], c6[P * MR], u[P * MR], v[P * MR];
+  T yb[32][2 * P + 1];
 };
 
 template <typename T, int P, int MR>
-__global__ void __launch_bounds__(32 * P, 2) k_zline_seg(DevLevel<T> L, int color, SegFac<T> F) {
-  // y of every row held in shared memory as [row][segment][lane] (each
-  // warp touches 32 consecutive words: no bank conflicts); sized
-  // MR * P * 32 elements by the launcher
-  extern __shared__ unsigned char zs_smem[];
-  T* ys = reinterpret_cast<T*>(zs_smem);
-  constexpr int NMAX = P * MR;
-  // the line factors of the level, staged once per CTA (uniform across the
-  // lanes: shared-memory broadcasts instead of dependent global loads)
-  __shared__ T f_ap[NMAX], f_rbp[NMAX], f_c6[NMAX], f_u[NMAX], f_v[NMAX];
-  __shared__ T yb[32][2 * P + 1];
-  const int lane = threadIdx.x;  // line within the CTA
+__device__ __forceinline__ void zseg_stage(const DevLevel<T>& L, const SegFac<T>& F,
+                                           ZSegShared<T, P, MR>& S) {
+  const T* __restrict__ cz6 = cz6p(L);
+  for (int q = threadIdx.y * 32 + threadIdx.x; q < L.nz; q += 32 * P) {
+    S.ap[q] = F.ap[q + 1];
+    S.rbp[q] = F.rbp[q + 1];
+    S.c6[q] = cz6[q + 1];
+    S.u[q] = F.u[q + 1];
+    S.v[q] = F.v[q + 1];
+  }
+}
+
+// Lines t0 .. t0+31 of one colour (lane = line, threadIdx.y = segment),
+// after zseg_stage by every thread of the CTA; ys holds MR * P * 32
+// elements laid out [row][segment][lane] (each warp touches 32 consecutive
+// words: no bank conflicts).  Contains two __syncthreads, so the whole CTA
+// calls it together; the first one also publishes the staged factors and
+// ends every thread's use of S from a previous call.
+template <typename T, int P, int MR>
+__device__ __forceinline__ void zseg_chunk(const DevLevel<T>& L, int color, const SegFac<T>& F,
+                                           ZSegShared<T, P, MR>& S, T* ys, int64_t t0) {
+  const int lane = threadIdx.x;  // line within the chunk
   const int s = threadIdx.y;     // segment
   const int n = L.nz;
-  const T* __restrict__ cz6 = cz6p(L);
-  for (int q = threadIdx.y * 32 + lane; q < n; q += 32 * P) {
-    f_ap[q] = F.ap[q + 1];
-    f_rbp[q] = F.rbp[q + 1];
-    f_c6[q] = cz6[q + 1];
-    f_u[q] = F.u[q + 1];
-    f_v[q] = F.v[q + 1];
-  }
   const int pairs = (L.nx + 1) >> 1;
-  const int64_t t = (int64_t)blockIdx.x * 32 + lane;
+  const int64_t t = t0 + lane;
   bool active = t < (int64_t)pairs * L.ny;
   int i = 0, j = 0;
   if (active) {
@@ -448,50 +538,102 @@ __global__ void __launch_bounds__(32 * P, 2) k_zline_seg(DevLevel<T> L, int colo
     const T* __restrict__ src = L.src + c0;
 #pragma unroll 8
     for (int w = 0; w < m; ++w) {
-      const int c = w * (int)XY;  // < 2^31: m * XY is checked by the launcher
+      const int c = w * (int)XY;  // < 2^31: m * XY is checked by the host
       yrow[w * YS] = src[c] - (a1 * phi[c - 1] + a2 * phi[c + 1] + a3 * phi[c - X] + a4 * phi[c + X]);
     }
     if (lo == 0) yrow[0] -= cz5p(L)[1] * phi[-XY];
-    if (lo + m == n) yrow[(m - 1) * YS] -= cz6[n] * phi[(int64_t)(m - 1) * XY + XY];
+    if (lo + m == n) yrow[(m - 1) * YS] -= cz6p(L)[n] * phi[(int64_t)(m - 1) * XY + XY];
   }
-  __syncthreads();  // factors staged
+  __syncthreads();
   T yfirst = T(0), ylast = T(0);
   if (active) {
     T g = yrow[0];
     for (int w = 1; w < m; ++w) {
-      g = yrow[w * YS] + f_ap[lo + w] * g;
+      g = yrow[w * YS] + S.ap[lo + w] * g;
       yrow[w * YS] = g;
     }
-    T x = g * f_rbp[lo + m - 1];
+    T x = g * S.rbp[lo + m - 1];
     yrow[(m - 1) * YS] = x;
     ylast = x;
     for (int w = m - 2; w >= 0; --w) {
-      x = (yrow[w * YS] - f_c6[lo + w] * x) * f_rbp[lo + w];
+      x = (yrow[w * YS] - S.c6[lo + w] * x) * S.rbp[lo + w];
       yrow[w * YS] = x;
     }
     yfirst = x;
   }
-  yb[lane][2 * s] = yfirst;
-  yb[lane][2 * s + 1] = ylast;
+  S.yb[lane][2 * s] = yfirst;
+  S.yb[lane][2 * s + 1] = ylast;
   __syncthreads();
-  if (!active) return;
-  // the two interface values this segment needs: L(s-1) = z[2s-1] and
-  // F(s+1) = z[2s+2], z = Minv * yb
-  T Lprev = T(0), Fnext = T(0);
-  if (s > 0) {
-    const T* mr = F.minv + (size_t)(2 * s - 1) * (2 * P);
+  if (active) {
+    // the two interface values this segment needs: L(s-1) = z[2s-1] and
+    // F(s+1) = z[2s+2], z = Minv * yb
+    T Lprev = T(0), Fnext = T(0);
+    if (s > 0) {
+      const T* mr = F.minv + (size_t)(2 * s - 1) * (2 * P);
 #pragma unroll
-    for (int p = 0; p < 2 * P; ++p) Lprev += mr[p] * yb[lane][p];
-  }
-  if (s < P - 1) {
-    const T* mr = F.minv + (size_t)(2 * s + 2) * (2 * P);
+      for (int p = 0; p < 2 * P; ++p) Lprev += mr[p] * S.yb[lane][p];
+    }
+    if (s < P - 1) {
+      const T* mr = F.minv + (size_t)(2 * s + 2) * (2 * P);
 #pragma unroll
-    for (int p = 0; p < 2 * P; ++p) Fnext += mr[p] * yb[lane][p];
-  }
-  T* phi = L.phi;
+      for (int p = 0; p < 2 * P; ++p) Fnext += mr[p] * S.yb[lane][p];
+    }
+    T* phi = L.phi;
+    if (!F.img) {
 #pragma unroll 8
-  for (int w = 0; w < m; ++w)
-    phi[c0 + (int64_t)w * XY] = yrow[w * YS] + f_u[lo + w] * Lprev + f_v[lo + w] * Fnext;
+      for (int w = 0; w < m; ++w)
+        phi[c0 + (int64_t)w * XY] = yrow[w * YS] + S.u[lo + w] * Lprev + S.v[lo + w] * Fnext;
+    } else {
+      const int* im = F.img + 3 * ((i - 2) + (int64_t)L.nx * (j - 2));
+      const int d0 = im[0], d1 = im[1], d2 = im[2];
+      T xfirst = T(0), xlast = T(0);
+#pragma unroll 4
+      for (int w = 0; w < m; ++w) {
+        const T x = yrow[w * YS] + S.u[lo + w] * Lprev + S.v[lo + w] * Fnext;
+        const int64_t c = c0 + (int64_t)w * XY;
+        phi[c] = x;
+        if (d0 != kNoImage) phi[c + d0] = x;
+        if (d1 != kNoImage) phi[c + d1] = x;
+        if (d2 != kNoImage) phi[c + d2] = x;
+        if (w == 0) xfirst = x;
+        if (w == m - 1) xlast = x;
+      }
+      // z ghosts of the column and of its images (rows k=1 and k=Z)
+      auto zrow = [&](int code, bool own_first) -> T {
+        if (code == 0) return T(0);
+        if ((code == 1) == own_first) return own_first ? xfirst : xlast;
+        // the other end of the line: interface value z[0] or z[2P-1]
+        const T* mr = F.minv + (size_t)(code == 1 ? 0 : 2 * P - 1) * (2 * P);
+        T acc = T(0);
+        for (int p = 0; p < 2 * P; ++p) acc += mr[p] * S.yb[lane][p];
+        return acc;
+      };
+      if (lo == 0) {
+        const T g = zrow(F.z1, true);
+        const int64_t c = c0 - XY;
+        phi[c] = g;
+        if (d0 != kNoImage) phi[c + d0] = g;
+        if (d1 != kNoImage) phi[c + d1] = g;
+        if (d2 != kNoImage) phi[c + d2] = g;
+      }
+      if (lo + m == n) {
+        const T g = zrow(F.zZ, false);
+        const int64_t c = c0 + (int64_t)m * XY;
+        phi[c] = g;
+        if (d0 != kNoImage) phi[c + d0] = g;
+        if (d1 != kNoImage) phi[c + d1] = g;
+        if (d2 != kNoImage) phi[c + d2] = g;
+      }
+    }
+  }
+}
+
+template <typename T, int P, int MR>
+__global__ void __launch_bounds__(32 * P, 2) k_zline_seg(DevLevel<T> L, int color, SegFac<T> F) {
+  extern __shared__ unsigned char zs_smem[];
+  __shared__ ZSegShared<T, P, MR> S;
+  zseg_stage(L, F, S);
+  zseg_chunk(L, color, F, S, reinterpret_cast<T*>(zs_smem), (int64_t)blockIdx.x * 32);
 }
 
 // ----------------------------------------------------- residual + restrict
@@ -519,9 +661,9 @@ __device__ __forceinline__ T fine_resid(const DevLevel<T>& F, int i, int j, int 
 }
 
 template <typename T>
-__global__ void k_restrict(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < Cl.G;
-       t += (int64_t)gridDim.x * blockDim.x) {
+__device__ __forceinline__ void restrict_range(const DevLevel<T>& F, const DevLevel<T>& Cl, int cdir,
+                                               int64_t t0, int64_t stride) {
+  for (int64_t t = t0; t < Cl.G; t += stride) {
     const int ic = 1 + (int)(t % Cl.X);
     const int64_t r = t / Cl.X;
     const int jc = 1 + (int)(r % Cl.Y);
@@ -577,16 +719,22 @@ __global__ void k_restrict(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
   }
 }
 
+template <typename T>
+__global__ void k_restrict(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
+  restrict_range(F, Cl, cdir, blockIdx.x * (int64_t)blockDim.x + threadIdx.x,
+                 (int64_t)gridDim.x * blockDim.x);
+}
+
 // -------------------------------------------------------------- prolong
 // mg_cor.F90:102-290 for the fine interior (fine ghosts are rebuilt by the
 // boundary pass that follows, as in the reference).  In a coarsened
 // direction fine index f uses coarse ic = (f+1)/2 (f odd, near point ic) or
 // ic = f/2 (f even, near point ic+1); weights 3 (near) and 1 (far).
 template <typename T>
-__global__ void k_prolong(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
+__device__ __forceinline__ void prolong_range(const DevLevel<T>& F, const DevLevel<T>& Cl, int cdir,
+                                              int64_t t0, int64_t stride) {
   const int64_t total = (int64_t)F.nx * F.ny * F.nz;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t t = t0; t < total; t += stride) {
     const int i = 2 + (int)(t % F.nx);
     const int64_t r = t / F.nx;
     const int j = 2 + (int)(r % F.ny);
@@ -642,6 +790,12 @@ __global__ void k_prolong(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
     const int64_t cf = cidx(i, j, k, F.X, F.XY);
     F.phi[cf] = F.phi[cf] + corr;
   }
+}
+
+template <typename T>
+__global__ void k_prolong(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
+  prolong_range(F, Cl, cdir, blockIdx.x * (int64_t)blockDim.x + threadIdx.x,
+                (int64_t)gridDim.x * blockDim.x);
 }
 
 }  // namespace anel

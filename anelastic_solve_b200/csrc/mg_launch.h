@@ -27,6 +27,8 @@ constexpr int kZSeg = 16;
 constexpr int kZSegRows = 32;
 template <typename T>
 void launch_zline_seg(const DevLevel<T>& L, int color, const SegFac<T>& F, cudaStream_t s);
+// ghost table of an FP32 level with a homogeneous rule (L.gtab ignored)
+void launch_ghost_table(const DevLevel<float>& L, int2* tab, cudaStream_t s);
 template <typename T>
 void launch_restrict(const DevLevel<T>& F, const DevLevel<T>& C, int cdir, cudaStream_t s);
 template <typename T>

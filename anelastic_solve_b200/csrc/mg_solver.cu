@@ -203,8 +203,20 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
       ANEL_CUDA_TRY(cudaMemset(d_phi32_[l], 0, G * sizeof(float)));
       ANEL_CUDA_TRY(cudaMemset(d_src32_[l], 0, G * sizeof(float)));
       ANEL_CUDA_TRY(cudaMalloc(&d_coef32_[l], ncoef * sizeof(float)));
+      // ghost table of the FP32 cycle's homogeneous rule (32-bit indices)
+      if (G < ((int64_t)1 << 31)) {
+        const int64_t ngh = G - (int64_t)geo_[l].n[0] * geo_[l].n[1] * geo_[l].n[2];
+        ANEL_CUDA_TRY(cudaMalloc(&d_gtab32_[l], (size_t)ngh * sizeof(int2)));
+        launch_ghost_table(L32(l, true), d_gtab32_[l], stream_);
+      }
     }
   }
+  ANEL_CUDA_TRY(cudaStreamSynchronize(stream_));
+  for (int l = 1; l <= ngrid_; ++l)
+    if (d_zseg32_[l] && d_gtab32_[l]) {
+      const int st = build_self_ghosting(l);
+      if (st != ANEL_OK) return st;
+    }
   ANEL_CUDA_TRY(cudaMalloc(&d_max_, 2 * sizeof(unsigned long long)));
   ANEL_CUDA_TRY(cudaMalloc(&d_part_, 2 * (size_t)gs_blocks(1LL << 40) * sizeof(double)));
   ANEL_CUDA_TRY(cudaMalloc(&d_norm_, 2 * sizeof(double)));
@@ -228,6 +240,8 @@ MGSolver::~MGSolver() {
     cudaFree(d_zf64_[l]);
     cudaFree(d_zf32_[l]);
     cudaFree(d_zseg32_[l]);
+    cudaFree(d_gtab32_[l]);
+    cudaFree(d_img32_[l]);
   }
   cudaFree(d_max_);
   cudaFree(d_part_);
@@ -742,6 +756,7 @@ DevLevel<double> MGSolver::L64(int l) const {
   L.src = d_src64_[l];
   L.coef = d_coef64_[l];
   L.rule = rule_[l];
+  L.gtab = nullptr;
   return L;
 }
 
@@ -760,6 +775,7 @@ DevLevel<float> MGSolver::L32(int l, bool hom) const {
   L.src = d_src32_[l];
   L.coef = d_coef32_[l];
   L.rule = hom ? rule_hom_[l] : rule_[l];
+  L.gtab = hom ? d_gtab32_[l] : nullptr;
   return L;
 }
 
@@ -825,8 +841,7 @@ void MGSolver::relax32(int l, int iters, cudaStream_t s) {
   const bool zl = prm_.smoother == ANEL_SMOOTHER_ZLINE;
   const float* zf = d_zf32_[l];
   const float* zs = d_zseg32_[l];
-  const int Z = geo_[l].Z;
-  const SegFac<float> sf{zs, zs + Z, zs + 2 * Z, zs + 3 * Z, zs + 4 * Z};
+  const SegFac<float> sf = segfac32(l);
   for (int it = 0; it < iters; ++it) {
     for (int color = 0; color < 2; ++color) {
       if (prof) prof_begin(s);
@@ -834,7 +849,7 @@ void MGSolver::relax32(int l, int iters, cudaStream_t s) {
       else if (zl) launch_zline(L, color, zf, zf + geo_[l].Z, s);
       else launch_rb_sweep(L, color, s);
       if (prof) prof_end(s);
-      launch_bdry(L, L.phi, s);
+      if (!(zl && zs && sf.img)) launch_bdry(L, L.phi, s);
     }
   }
   if (iters == 0) launch_bdry(L, L.phi, s);
@@ -859,6 +874,102 @@ void MGSolver::cycle32(cudaStream_t s) {
   }
   relax32(ng, post[ng - 1], s);
 }
+
+SegFac<float> MGSolver::segfac32(int l) const {
+  const float* zs = d_zseg32_[l];
+  SegFac<float> f{};
+  if (!zs) return f;
+  const int Z = geo_[l].Z;
+  f.ap = zs;
+  f.rbp = zs + Z;
+  f.u = zs + 2 * Z;
+  f.v = zs + 3 * Z;
+  f.minv = zs + 4 * Z;
+  f.img = d_img32_[l];
+  f.z1 = zcode_[l][0];
+  f.zZ = zcode_[l][1];
+  return f;
+}
+
+// Derive from the level's ghost table which ghost cells copy which line, so
+// the z-line sweep can write them itself: every ghost column must copy one
+// interior line row by row (or be 0), every line may have at most three
+// such image columns, and the k=1 / k=Z ghosts of all columns must follow
+// one rule (0, row k=2 or row k=nz+1 of the column they image).  A level
+// that does not fit keeps the boundary pass.
+int MGSolver::build_self_ghosting(int l) {
+  const LevelGeom& G = geo_[l];
+  const int X = G.X, Y = G.Y, Z = G.Z, nx = G.n[0], ny = G.n[1], nz = G.n[2];
+  const int64_t XY = (int64_t)X * Y;
+  const int64_t ngh = G.G - (int64_t)nx * ny * nz;
+  std::vector<int2> tab(ngh);
+  ANEL_CUDA_TRY(cudaMemcpy(tab.data(), d_gtab32_[l], ngh * sizeof(int2), cudaMemcpyDeviceToHost));
+  // source column (interior (i,j) as index, -1 zero) of every column of
+  // the ghosted plane for the interior rows, and the z rule per column
+  std::vector<int64_t> colsrc(XY, -2);
+  int zc[2] = {-1, -1};
+  bool ok = true;
+  auto col_of = [&](int64_t c) { return c % XY; };
+  for (int64_t g = 0; g < ngh && ok; ++g) {
+    const int64_t d = tab[g].x, src = tab[g].y;
+    const int64_t dcol = col_of(d);
+    const int dk = 1 + (int)(d / XY);
+    if (dk >= 2 && dk <= nz + 1) {
+      int64_t sc = -1;
+      if (src >= 0) {
+        if (1 + src / XY != dk) ok = false;
+        sc = col_of(src);
+      }
+      if (colsrc[dcol] == -2) colsrc[dcol] = sc;
+      else if (colsrc[dcol] != sc) ok = false;
+    }
+  }
+  for (int64_t c = 0; c < XY && ok; ++c) {
+    const int i = 1 + (int)(c % X), j = 1 + (int)(c / X);
+    const bool interior = i >= 2 && i <= nx + 1 && j >= 2 && j <= ny + 1;
+    if (interior) colsrc[c] = c;
+    else if (colsrc[c] == -2) ok = false;
+  }
+  // z ghosts
+  for (int64_t g = 0; g < ngh && ok; ++g) {
+    const int64_t d = tab[g].x, src = tab[g].y;
+    const int dk = 1 + (int)(d / XY);
+    if (dk != 1 && dk != Z) continue;
+    const int64_t sc = colsrc[col_of(d)];
+    int code;
+    if (src < 0) {
+      code = 0;
+    } else {
+      if (col_of(src) != sc) { ok = false; break; }
+      const int sk = 1 + (int)(src / XY);
+      code = (sk == 2) ? 1 : (sk == nz + 1 ? 2 : -1);
+      if (code < 0) { ok = false; break; }
+    }
+    if (sc < 0 && code != 0) { ok = false; break; }
+    if (sc < 0) continue;  // a zero column: its z ghosts are zero as well
+    int& z = zc[dk == 1 ? 0 : 1];
+    if (z == -1) z = code;
+    else if (z != code) ok = false;
+  }
+  std::vector<int> img(3 * (size_t)nx * ny, kNoImage);
+  for (int64_t c = 0; c < XY && ok; ++c) {
+    const int64_t sc = colsrc[c];
+    if (sc < 0 || sc == c) continue;
+    const int si = 1 + (int)(sc % X), sj = 1 + (int)(sc / X);
+    int* e = &img[3 * ((size_t)(si - 2) + (size_t)nx * (sj - 2))];
+    int q = 0;
+    while (q < 3 && e[q] != kNoImage) ++q;
+    if (q == 3) { ok = false; break; }
+    e[q] = (int)(c - sc);
+  }
+  if (!ok || zc[0] < 0 || zc[1] < 0) return ANEL_OK;  // keep the boundary pass
+  ANEL_CUDA_TRY(cudaMalloc(&d_img32_[l], img.size() * sizeof(int)));
+  ANEL_CUDA_TRY(cudaMemcpy(d_img32_[l], img.data(), img.size() * sizeof(int), cudaMemcpyHostToDevice));
+  zcode_[l][0] = zc[0];
+  zcode_[l][1] = zc[1];
+  return ANEL_OK;
+}
+
 
 // ------------------------------------------------------------ solves
 double MGSolver::true_resid(const double* d_phi, const double* d_rhs, cudaStream_t s,

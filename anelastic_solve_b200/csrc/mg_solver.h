@@ -88,6 +88,14 @@ class MGSolver {
   // then the 2P x 2P interface inverse), null where the level's nz does
   // not split into kZSeg segments of at least two rows
   float* d_zseg32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  // ghost tables of the FP32 levels under the homogeneous rule
+  int2* d_gtab32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  // ghost copies done by the partitioned z-line sweep itself (null: the
+  // level keeps its boundary pass after each colour); see SegFac
+  int* d_img32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  int zcode_[ANEL_MAX_LEVELS + 1][2] = {};
+  int build_self_ghosting(int l);
+  SegFac<float> segfac32(int l) const;
   int build_zline_factors();
   unsigned long long* d_max_ = nullptr;   // 2 words
   double* d_part_ = nullptr;              // norm partials

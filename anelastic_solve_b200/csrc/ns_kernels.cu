@@ -320,36 +320,64 @@ __device__ __forceinline__ void zghost_column(const NSDev& D, const ZRule& R, do
 #undef COL
 }
 
-// Copy the finished column (i,j) into its periodic images in x and y
-// (the ghost columns, BC.F90:55-63 with TB = 3 in x and y).
-__device__ __forceinline__ void copy_images(const NSDev& D, double* a, int i, int j) {
-  int is[2], js[2];
-  int ni = 1, nj = 1;
-  is[0] = i;
-  js[0] = j;
-  if (i == 2) is[ni++] = D.nx + 2;
-  else if (i == D.nx + 1) is[ni++] = 1;
-  if (i == 2 && i == D.nx + 1) is[ni++] = 1;  // nx == 1
-  if (j == 2) js[nj++] = D.ny + 2;
-  else if (j == D.ny + 1) js[nj++] = 1;
-  if (j == 2 && j == D.ny + 1) js[nj++] = 1;
-  if (ni == 1 && nj == 1) return;
-  const int64_t src = NS_IX(i, j, 1);
-  for (int a_ = 0; a_ < ni; ++a_)
-    for (int b_ = 0; b_ < nj; ++b_) {
-      if (a_ == 0 && b_ == 0) continue;
-      const int64_t dst = NS_IX(is[a_], js[b_], 1);
-      for (int k = 1; k <= D.Z; ++k) a[dst + (int64_t)(k - 1) * D.XY] = a[src + (int64_t)(k - 1) * D.XY];
+// Periodic images in x and y (BC.F90:55-63 with TB = 3 in x and y) of up
+// to three fields, after their interior columns are final (z ghosts
+// included): one thread per (ghost column of the ring, k).  Every copy
+// reads an interior column, so the order of the copies does not matter:
+//   (1, j) <- (nx+1, j), (nx+2, j) <- (2, j)      j = 2..ny+1
+//   (i, 1) <- (i, ny+1), (i, ny+2) <- (i, 2)      i = 2..nx+1
+//   corners from the diagonally opposite interior column.
+struct Fields3 {
+  double* a[3];
+  int n;
+};
+
+__global__ void k_images(NSDev D, Fields3 F) {
+  const int nx = D.nx, ny = D.ny;
+  const int ring = 2 * ny + 2 * nx + 4;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ring) return;
+  const int k = 1 + blockIdx.y;
+  int di, dj, si, sj;
+  if (t < 2 * ny) {
+    const int j = 2 + (t % ny);
+    dj = sj = j;
+    if (t < ny) {
+      di = 1;
+      si = nx + 1;
+    } else {
+      di = nx + 2;
+      si = 2;
     }
+  } else if (t < 2 * ny + 2 * nx) {
+    const int u = t - 2 * ny;
+    const int i = 2 + (u % nx);
+    di = si = i;
+    if (u < nx) {
+      dj = 1;
+      sj = ny + 1;
+    } else {
+      dj = ny + 2;
+      sj = 2;
+    }
+  } else {
+    const int c = t - 2 * ny - 2 * nx;
+    di = (c & 1) ? nx + 2 : 1;
+    si = (c & 1) ? 2 : nx + 1;
+    dj = (c & 2) ? ny + 2 : 1;
+    sj = (c & 2) ? 2 : ny + 1;
+  }
+  const int64_t dst = NS_IX(di, dj, k), src = NS_IX(si, sj, k);
+  for (int f = 0; f < F.n; ++f) F.a[f][dst] = F.a[f][src];
 }
 
-// Generic ghost pass of one field: one thread per interior column.
+// Generic z-ghost pass of one field: one thread per interior column (the
+// periodic images follow in k_images).
 __global__ void k_ghost_field(NSDev D, double* a, ZRule R) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
   if (i > D.nx + 1) return;
   zghost_column(D, R, a, NS_IX(i, j, 1));
-  copy_images(D, a, i, j);
 }
 
 // ------------------------------------------------------- CN (z implicit)
@@ -466,7 +494,6 @@ __global__ void __launch_bounds__(kCNThreads) k_cn_column(NSDev D, double* __res
     }
   }
   zghost_column(D, R, fld, base);
-  copy_images(D, fld, i, j);
 }
 
 // ------------------------------------------------------------ Psource
@@ -514,9 +541,6 @@ __global__ void k_pgrad_ghost(NSDev D, ZRule Ru, ZRule Rv, ZRule Rw) {
   zghost_column(D, Ru, D.u, base);
   zghost_column(D, Rv, D.v, base);
   zghost_column(D, Rw, D.w, base);
-  copy_images(D, D.u, i, j);
-  copy_images(D, D.v, i, j);
-  copy_images(D, D.w, i, j);
 }
 
 // -------------------------------------------------------------- calcdt
@@ -597,6 +621,13 @@ __global__ void k_divergence(NSDev D, unsigned long long* mx, double* part) {
 }
 
 // ------------------------------------------------------------ launchers
+static void launch_images(const NSDev& D, double* a0, double* a1, double* a2, cudaStream_t s) {
+  Fields3 F{{a0, a1, a2}, a2 ? 3 : (a1 ? 2 : 1)};
+  const int ring = 2 * D.ny + 2 * D.nx + 4;
+  k_images<<<dim3((unsigned)((ring + 127) / 128), (unsigned)D.Z, 1u), 128, 0, s>>>(D, F);
+  count_launch();
+}
+
 static dim3 cell_grid(const NSDev& D, int tx) {
   return dim3((unsigned)((D.nx + tx - 1) / tx), (unsigned)D.ny, (unsigned)D.nz);
 }
@@ -625,6 +656,7 @@ void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFa
   if (var == 3) k_cn_column<3><<<col_grid(D, tx), tx, sm, s>>>(D, fld, q, f, a3, rkdt, R);
   else k_cn_column<1><<<col_grid(D, tx), tx, sm, s>>>(D, fld, q, f, a3, rkdt, R);
   count_launch();
+  launch_images(D, fld, nullptr, nullptr, s);
 }
 
 void launch_psource(const NSDev& D, double dt, cudaStream_t s) {
@@ -638,12 +670,14 @@ void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, c
   k_pgrad<<<cell_grid(D, 128), 128, 0, s>>>(D, dt);
   k_pgrad_ghost<<<col_grid(D, 64), 64, 0, s>>>(D, Ru, Rv, Rw);
   count_launch(2);
+  launch_images(D, D.u, D.v, D.w, s);
 }
 
 void launch_ghost_field(const NSDev& D, double* a, const ZRule& R, cudaStream_t s) {
   const int tx = 64;
   k_ghost_field<<<col_grid(D, tx), tx, 0, s>>>(D, a, R);
   count_launch();
+  launch_images(D, a, nullptr, nullptr, s);
 }
 
 void launch_cfl_max(const NSDev& D, unsigned long long* out, cudaStream_t s) {
