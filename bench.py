@@ -5,7 +5,8 @@ Workload "dns" (default): the DNS shear layer on the 512x256x512
 staggered grid (domain 4pi x 2pi x 20, periodic x/y, free-slip z walls, z
 tanh-stretched), Re=4000, Pr=1, Ri=0.08, seeded perturbation 1e-3, time
 step from CFL 0.5 (calcdt); every sub-step projects with the mixed-precision
-multigrid (FP32 V-cycles inside FP64 defect correction) to a true relative
+multigrid (FP32 V-cycles inside FP64 defect correction; z-line Gauss-Seidel
+with x/y semi-coarsening unless --smoother rbpgs) to a true relative
 residual of 1e-10.  One step = one full RK3 time step (three sub-steps,
 three projections).  Fields are FP64.
 
@@ -14,15 +15,16 @@ three projections).  Fields are FP64.
   e2e      -- the same through the C-ABI with the state in pinned host
               memory: every step copies u, v, w, p, rho host->device, runs
               the step and copies them back
-  roofline -- the dominant kernel (finest-level red-black smoother of the
-              pressure solves): algorithmic bytes per launch / mean launch
-              time (CUDA events on its stream)
+  roofline -- the dominant kernel (finest-level smoother of the pressure
+              solves): algorithmic bytes per launch / mean launch time
+              (CUDA events on its stream)
 
 Workload "poisson": standalone pressure solves of the same grid (one step
 = one solve to 1e-10 from phi0 = 0).
 
---impl reference times the CPU restatement of the same algorithm (the
-Fortran reference cannot be built here) on the host cores instead.
+--impl reference times the CPU restatement of the reference's algorithm
+(FP64, red-black point Gauss-Seidel; the Fortran reference cannot be built
+here) on the host cores instead.
 N > 1 GPUs (torchrun): independent replicas, no collective on the data path.
 """
 from __future__ import annotations
@@ -395,8 +397,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="dns", choices=sorted(WORKLOADS))
     ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--smoother", default="rbpgs", choices=["rbpgs", "zline"],
-                    help="rbpgs: red-black point GS, full coarsening; zline: z-line GS, x/y coarsening")
+    ap.add_argument("--smoother", default="zline", choices=["rbpgs", "zline"],
+                    help="zline: z-line GS with x/y semi-coarsening (default); rbpgs: the "
+                         "reference's red-black point GS with full coarsening")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 multigrid companion")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
@@ -428,6 +431,8 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        # the reference's own algorithm: red-black point GS, full coarsening
+        SMOOTHER["smoother"] = "rbpgs"
         samples = []
         for _ in range(max(1, args.warmup + args.steps) if kind == "poisson" else 1):
             samples.append(cpu_sample_dns(args.workload, threads) if kind == "dns"
@@ -471,14 +476,18 @@ def main():
     peak, peak_kind = load_peaks()
     N = r["N"]
     value = world * N / (r["ms_step"] / 1e3)
-    # smoother bytes per cell and launch (one colour): RB reads phi (all
-    # cells, neighbours), f and writes phi for half the cells -> 12 B FP64;
-    # a z-line colour additionally writes and re-reads the line's
-    # elimination values in place -> 16 B FP64 (halved for FP32)
+    # smoother bytes per cell and launch (one colour): reads of the other
+    # colour's phi (the neighbours, half the cells), f of this colour and
+    # the write of this colour's phi -> 12 B FP64, 6 B FP32.  The FP64
+    # z-line (Thomas) kernel also writes and re-reads the elimination values
+    # in place (+4 B); the FP32 partitioned z-line kernel keeps them on chip.
     zl = args.smoother == "zline"
-    bpc = (8.0 if zl else 6.0) if args.prec == "mixed" else (16.0 if zl else 12.0)
-    kname = "k_zline" if zl else "k_rb_sweep"
-    kernel = f"{kname}<float>" if args.prec == "mixed" else f"{kname}<double>"
+    bpc = 6.0 if args.prec == "mixed" else (16.0 if zl else 12.0)
+    if zl and args.prec == "mixed" and nz % 16 == 0 and 32 <= nz <= 512:
+        kernel = "k_zline_seg<float,16,32>"
+    else:
+        kname = "k_zline" if zl else "k_rb_sweep"
+        kernel = f"{kname}<float>" if args.prec == "mixed" else f"{kname}<double>"
     roof = None
     if r["sweeps"]:
         t_launch = r["sweep_ms"] / r["sweeps"] / 1e3
@@ -490,6 +499,7 @@ def main():
                 "mean_launch_ms": round(t_launch * 1e3, 4),
                 "share_note": "finest-level smoother launches only; share of step time in profiles/"}
     cpu = None
+    SMOOTHER["smoother"] = "rbpgs"  # the CPU baseline runs the reference's algorithm
     if not args.no_cpu:
         if kind == "dns":
             t, it, _ = cpu_sample_dns(args.workload, threads)
