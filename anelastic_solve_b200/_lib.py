@@ -46,6 +46,8 @@ SIGNATURES = {
     "anel_ns_ctx_set_profiling": (C.c_int, [_P, C.c_int32]),
     "anel_ns_ctx_project": (C.c_int, [_P, _IP, _DP]),
     "anel_ns_ctx_divergence": (C.c_int, [_P, _DP]),
+    "anel_divergence_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _DP, _DP, _DP, _DP, _DP,
+                                          _DP, _DP, _P]),
     "anel_ns_init": (C.c_int, [C.POINTER(abi.GridDesc), C.POINTER(abi.MGParams),
                                C.POINTER(abi.NSParams)]),
     "anel_bind_fields": (C.c_int, [C.POINTER(abi.Fields)]),

@@ -30,6 +30,7 @@ SOURCES = {
     "mg_kernels32.cu": ["-fmad=true"],
     "ns_kernels.cu": ["-fmad=false"],
     "ns_solver.cu": ["-fmad=false"],
+    "noalloc.cu": ["-fmad=false"],
 }
 
 

@@ -282,6 +282,24 @@ int anel_ns_ctx_project(anel_ns_ctx* ctx, int32_t* mg_iter, double* mg_relmax);
  * out[0] = volume-weighted mean |div|, out[1] = max |div|. */
 int anel_ns_ctx_divergence(anel_ns_ctx* ctx, double* out);
 
+/* The same divergence diagnostic for callers that must not have the
+ * library allocate device memory (a driver that pools or pins all of its
+ * device memory up front, or runs under a fully committed memory budget):
+ * it allocates nothing.  This entry point has no counterpart in the
+ * reference.  u, v, w are the caller's ghosted device fields
+ * ((nx+2)(ny+2)(nz+2) doubles, Fortran order), rdxc/rdyc/rdzc its device
+ * metric arrays (n+2 each); out (host, 2 doubles) receives the mean and
+ * max |div| as anel_ns_ctx_divergence does (the mean may differ in the
+ * last bits: its sums run per z-plane).  Partial sums live in a fixed
+ * array inside the library's device image, which limits nz to 4096
+ * (larger: ANEL_ERR_SIZE) and is shared by all calls on a device, so
+ * calls whose GPU work overlaps race; run them on one stream.  The first
+ * call on a device looks up that array's address and keeps it: make it
+ * before any stream capture on the device.  Waits for stream. */
+int anel_divergence_noalloc(int32_t nx, int32_t ny, int32_t nz, const double* u, const double* v,
+                            const double* w, const double* rdxc, const double* rdyc,
+                            const double* rdzc, double* out, void* stream);
+
 /* Drop-in form for the Fortran driver: bind the module arrays (host)
  * once, then call anel_rk_substep with the reference's rk_ss arguments;
  * every call copies the bound fields to the device and back. */
