@@ -433,6 +433,7 @@ def main():
             return
         # the reference's own algorithm: red-black point GS, full coarsening
         SMOOTHER["smoother"] = "rbpgs"
+        config = dict(config, mg=f"RBPGS V(2,2), metric, fp64 (the reference's algorithm on the host)")
         samples = []
         for _ in range(max(1, args.warmup + args.steps) if kind == "poisson" else 1):
             samples.append(cpu_sample_dns(args.workload, threads) if kind == "dns"
