@@ -126,7 +126,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-SMOOTHER = {"smoother": "rbpgs"}
+SMOOTHER = {"smoother": "rbpgs", "pre": 2, "post": 2}
 
 
 def mg_params(lv, precision, mode=None):
@@ -136,7 +136,8 @@ def mg_params(lv, precision, mode=None):
 
     zl = SMOOTHER["smoother"] == "zline"
     levels = (lv[0], lv[1], 1) if zl else lv
-    return abi.make_mg_params(levels, maxcy=400, tolmax=TOL, pre=2, post=2, tbc=(0, 1, 0, 1, 0, 0),
+    return abi.make_mg_params(levels, maxcy=400, tolmax=TOL, pre=SMOOTHER["pre"],
+                              post=SMOOTHER["post"], tbc=(0, 1, 0, 1, 0, 0),
                               precision=precision,
                               smoother=abi.SMOOTHER_ZLINE if zl else abi.SMOOTHER_RBPGS,
                               mode=abi.MODE_METRIC if mode is None else mode, stop=abi.STOP_RESID)
@@ -400,11 +401,13 @@ def main():
     ap.add_argument("--smoother", default="zline", choices=["rbpgs", "zline"],
                     help="zline: z-line GS with x/y semi-coarsening (default); rbpgs: the "
                          "reference's red-black point GS with full coarsening")
+    ap.add_argument("--pre", type=int, default=2, help="pre-smoothing sweeps per level")
+    ap.add_argument("--post", type=int, default=2, help="post-smoothing sweeps per level")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 multigrid companion")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     args = ap.parse_args()
-    SMOOTHER["smoother"] = args.smoother
+    SMOOTHER.update(smoother=args.smoother, pre=args.pre, post=args.post)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
@@ -416,7 +419,7 @@ def main():
         config = {"workload": f"DNS shear layer {nx}x{ny}x{nz}: Re={phys['Re']:g}, Pr=1, "
                               f"Ri={-phys['g']:g}, amp {phys['amp']:g}, CFL {phys['cfl']:g}, "
                               f"MG to ||f-A p||/||f|| <= {TOL:g} each sub-step",
-                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V(2,2), metric, {args.prec}",
+                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V({args.pre},{args.post}), metric, {args.prec}",
                   "ew": 1, "scal1": "off (zero)", "parallelism": f"replicas x{args.gpus}",
                   "l2": "inputs larger than L2 (545 MB per FP64 field)" if nx >= 256 else "small"}
     else:
@@ -424,7 +427,7 @@ def main():
         unit = "cell-solves/s"
         config = {"workload": f"pressure-Poisson solve {nx}x{ny}x{nz}, tanh-stretched z, periodic "
                               f"x/y, Neumann z, to ||f-A phi||/||f|| <= {TOL:g} from phi0 = 0",
-                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V(2,2), metric, {args.prec}",
+                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V({args.pre},{args.post}), metric, {args.prec}",
                   "parallelism": f"replicas x{args.gpus}",
                   "l2": "inputs larger than L2 (545 MB per FP64 field)" if nx >= 256 else "small"}
     threads = os.cpu_count() or 1
@@ -432,7 +435,7 @@ def main():
         if rank != 0:
             return
         # the reference's own algorithm: red-black point GS, full coarsening
-        SMOOTHER["smoother"] = "rbpgs"
+        SMOOTHER.update(smoother="rbpgs", pre=2, post=2)
         config = dict(config, mg=f"RBPGS V(2,2), metric, fp64 (the reference's algorithm on the host)")
         samples = []
         for _ in range(max(1, args.warmup + args.steps) if kind == "poisson" else 1):
@@ -500,7 +503,7 @@ def main():
                 "mean_launch_ms": round(t_launch * 1e3, 4),
                 "share_note": "finest-level smoother launches only; share of step time in profiles/"}
     cpu = None
-    SMOOTHER["smoother"] = "rbpgs"  # the CPU baseline runs the reference's algorithm
+    SMOOTHER.update(smoother="rbpgs", pre=2, post=2)  # the CPU baseline: the reference's algorithm
     if not args.no_cpu:
         if kind == "dns":
             t, it, _ = cpu_sample_dns(args.workload, threads)
