@@ -387,7 +387,7 @@ __global__ void k_ghost_field(NSDev D, double* a, ZRule R) {
 // diagonal), c (super-diagonal), t1, t2 (explicit-term weights), rb
 // (right-hand side of a wall row) and isbc (1 for wall rows).
 struct CNFac {
-  const double *ap, *bp, *c, *t1, *t2, *rb, *isbc;
+  const double *ap, *bp, *c, *t1, *t2, *rb, *isbc, *sub, *diag;
 };
 
 // The per-row factors and z metrics are staged in shared memory (stride
@@ -494,6 +494,208 @@ __global__ void __launch_bounds__(kCNThreads) k_cn_column(NSDev D, double* __res
     }
   }
   zghost_column(D, R, fld, base);
+}
+
+// LES form of var_advance_CN_PL (NSsolver.F90:3054-3465 with Vmodel =
+// SSM): every row adds the eddy terms of the column's kT to the DNS
+// coefficients, so the tridiagonal system differs per column and is
+// eliminated here (Thomas of mg_relax.F90:541-595: a = -sub/b(k-1),
+// b = diag + a c(k-1), G = rhs + a G(k-1)).  G stays in the field, b and
+// c go to per-cell scratch for the back substitution.  Loads of a batch of
+// kCNU rows are issued before its stores.  The arithmetic follows the
+// reference's expressions term by term.
+template <int kVar>
+__global__ void __launch_bounds__(kCNThreads) k_cn_column_les(NSDev D, double* __restrict__ fld,
+                                                              const double* __restrict__ q, CNFac F,
+                                                              double a3, double rkdt, ZRule R,
+                                                              const double* __restrict__ kT,
+                                                              double* __restrict__ bb,
+                                                              double* __restrict__ cc) {
+  extern __shared__ double cn_sm[];
+  const int n = D.nz + 2;
+  const int S = n + 1;
+  double* s_sub = cn_sm;
+  double* s_dia = s_sub + S;
+  double* s_c = s_dia + S;
+  double* s_t1 = s_c + S;
+  double* s_t2 = s_t1 + S;
+  double* s_rb = s_t2 + S;
+  double* s_bc = s_rb + S;
+  double* s_re = s_bc + S;  // rdze
+  double* s_rc = s_re + S;  // rdzc
+  double* s_r = s_rc + S;   // r(z)
+  for (int r = threadIdx.x; r < S; r += blockDim.x) {
+    const bool in = r < n;
+    s_sub[r] = in ? F.sub[r] : 0.0;
+    s_dia[r] = in ? F.diag[r] : 1.0;
+    s_c[r] = in ? F.c[r] : 0.0;
+    s_t1[r] = in ? F.t1[r] : 0.0;
+    s_t2[r] = in ? F.t2[r] : 0.0;
+    s_rb[r] = in ? F.rb[r] : 0.0;
+    s_bc[r] = in ? F.isbc[r] : 1.0;
+    s_re[r] = in ? D.rdze[r] : 0.0;
+    s_rc[r] = in ? D.rdzc[r] : 0.0;
+    s_r[r] = in ? D.rz[r] : 1.0;
+  }
+  __syncthreads();
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  if (i > D.nx + 1) return;
+  const int64_t base = NS_IX(i, j, 1);
+  const int64_t XY = D.XY;
+  // eddy coefficient columns: u pairs (i, i+1), v pairs (j, j+1)
+  const double* kc = kT + base;
+  const double* kn = kT + base + (kVar == 1 ? 1 : (kVar == 2 ? D.X : 0));
+  constexpr double H = 0.5;
+  double um = fld[base];
+  double uk = fld[base + XY];
+  // row 1 is a wall row
+  double g = s_rb[0];
+  double b = s_dia[0];
+  double cprev = s_c[0];
+  fld[base] = g;
+  bb[base] = b;
+  cc[base] = cprev;
+  // kT window: rows k-1 and k of both columns (kn = kc for rho, scal1, w)
+  double kcm = kc[0], kcc = kc[XY], knm = kn[0], knc = kn[XY];
+  for (int kb = 2; kb <= n; kb += kCNU) {
+    double up[kCNU], qv[kCNU], kcp[kCNU], knp[kCNU];
+#pragma unroll
+    for (int u = 0; u < kCNU; ++u) {
+      const int k = kb + u;
+      const int64_t o = (int64_t)(k - 1) * XY;
+      up[u] = (k < n) ? fld[base + o + XY] : 0.0;
+      qv[u] = (k <= n) ? q[base + o] : 0.0;
+      kcp[u] = (k < n) ? kc[o + XY] : 0.0;
+      knp[u] = (k < n) ? kn[o + XY] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kCNU; ++u) {
+      const int k = kb + u;
+      if (k <= n) {
+        double sub, dia, sup, rhs;
+        if (s_bc[k - 1] != 0.0) {
+          sub = s_sub[k - 1];
+          dia = s_dia[k - 1];
+          sup = s_c[k - 1];
+          rhs = s_rb[k - 1];
+        } else {
+          rhs = 1.0 * uk + a3 * qv[u] * 1.0;
+          const double rk = s_r[k - 1];
+          if (kVar != 3) {
+            rhs = rhs + rkdt * 0.5 *
+                            (s_t2[k - 1] * (up[u] - uk) * s_re[k - 1] -
+                             s_t1[k - 1] * (uk - um) * s_re[k - 2]) *
+                            s_rc[k - 1];
+            const double ra1 = H * (s_r[k] + rk);
+            const double ra2 = H * (rk + s_r[k - 2]);
+            double t1, t2;
+            if (kVar == 1 || kVar == 2) {
+              t1 = -0.25 * (kcc + knc + kcm + knm) * ra1 / rk;
+              t2 = -0.25 * (kcc + knc + kcp[u] + knp[u]) * ra2 / rk;
+            } else if (kVar == 5) {
+              t1 = -0.5 * (kcc + kcm) * ra1 / rk;
+              t2 = -0.5 * (kcc + kcp[u]) * ra2 / rk;
+            } else {
+              t1 = -0.5 * (kcc + kcm);
+              t2 = -0.5 * (kcc + kcp[u]);
+            }
+            sub = s_sub[k - 1] - 0.5 * rkdt * t1 * s_re[k - 2] * s_rc[k - 1];
+            sup = s_c[k - 1] - 0.5 * rkdt * t2 * s_re[k - 1] * s_rc[k - 1];
+            dia = s_dia[k - 1] + 0.5 * rkdt * (t1 * s_re[k - 2] + t2 * s_re[k - 1]) * s_rc[k - 1];
+            rhs = rhs + rkdt * 0.5 *
+                            (t2 * (up[u] - uk) * s_re[k - 1] - t1 * (uk - um) * s_re[k - 2]) *
+                            s_rc[k - 1];
+          } else {
+            rhs = rhs + rkdt * 0.5 *
+                            (s_t2[k - 1] * (up[u] - uk) * s_rc[k] -
+                             s_t1[k - 1] * (uk - um) * s_rc[k - 1]) *
+                            s_re[k - 1];
+            const double rkp = s_r[k];
+            const double t1 = -kcc * rk / (H * (rkp + rk));
+            const double t2 = -kcp[u] * rkp / (H * (rkp + rk));
+            sub = s_sub[k - 1] - rkdt * t1 * s_re[k - 1] * s_rc[k - 1];
+            sup = s_c[k - 1] - rkdt * t2 * s_re[k - 1] * s_rc[k];
+            dia = s_dia[k - 1] + rkdt * (t1 * s_rc[k - 1] + t2 * s_rc[k]) * s_re[k - 1];
+            rhs = rhs + rkdt * (t2 * (up[u] - uk) * s_rc[k] - t1 * (uk - um) * s_rc[k - 1]) * s_re[k - 1];
+          }
+        }
+        const double a = -sub / b;
+        b = dia + a * cprev;
+        g = rhs + a * g;
+        const int64_t o = base + (int64_t)(k - 1) * XY;
+        fld[o] = g;
+        bb[o] = b;
+        cc[o] = sup;
+        cprev = sup;
+        um = uk;
+        uk = up[u];
+        kcm = kcc;
+        kcc = kcp[u];
+        knm = knc;
+        knc = knp[u];
+      }
+    }
+  }
+  // back substitution: G(n) = G(n)/b(n); G(k) = (G(k) - c(k) G(k+1))/b(k)
+  double x = g / b;
+  fld[base + (int64_t)(n - 1) * XY] = x;
+  for (int kb = n - 1; kb >= 1; kb -= kCNU) {
+    double gv[kCNU], bv[kCNU], cv[kCNU];
+#pragma unroll
+    for (int u = 0; u < kCNU; ++u) {
+      const int k = kb - u;
+      const int64_t o = base + (int64_t)(k - 1) * XY;
+      gv[u] = (k >= 1) ? fld[o] : 0.0;
+      bv[u] = (k >= 1) ? bb[o] : 1.0;
+      cv[u] = (k >= 1) ? cc[o] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kCNU; ++u) {
+      const int k = kb - u;
+      if (k >= 1) {
+        x = (gv[u] - cv[u] * x) / bv[u];
+        fld[base + (int64_t)(k - 1) * XY] = x;
+      }
+    }
+  }
+  zghost_column(D, R, fld, base);
+}
+
+// ------------------------------------------------------------------ SGS
+// SGSdiff (straincal.F90:339-414) with straincal's strain magnitude
+// (:48-73) on the interior: nuT = -(Csgs + 0) delg^2 |S| + 0 and the same
+// with CTsgs (kappaT) and CSsgs (nappaT); x**2.d0 is x*x.
+__global__ void __launch_bounds__(128) k_sgs(NSDev D) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > D.nx + 1) return;
+  const double *l1 = D.u, *l2 = D.v, *l3 = D.w;
+  const double TS11 = (FA(l1, i + 1, j, k) - FA(l1, i, j, k)) * MT(D.rdxc, i);
+  const double TS22 = (FA(l2, i, j + 1, k) - FA(l2, i, j, k)) * MT(D.rdyc, j);
+  const double TS33 = (FA(l3, i, j, k + 1) - FA(l3, i, j, k)) * MT(D.rdzc, k);
+  double t1 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j + 1, k) + FA(l1, i + 1, j + 1, k));
+  double t2 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j - 1, k) + FA(l1, i + 1, j - 1, k));
+  double t3 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i + 1, j, k) + FA(l2, i + 1, j + 1, k));
+  double t4 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i - 1, j, k) + FA(l2, i - 1, j + 1, k));
+  const double TS12 = 0.5 * ((t1 - t2) * MT(D.rdyc, j) + (t3 - t4) * MT(D.rdxc, i));
+  t1 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j, k + 1) + FA(l1, i + 1, j, k + 1));
+  t2 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j, k - 1) + FA(l1, i + 1, j, k - 1));
+  t3 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i + 1, j, k) + FA(l3, i + 1, j, k + 1));
+  t4 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i - 1, j, k) + FA(l3, i - 1, j, k + 1));
+  const double TS13 = 0.5 * ((t1 - t2) * MT(D.rdzc, k) + (t3 - t4) * MT(D.rdxc, i));
+  t1 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i, j, k + 1) + FA(l2, i, j + 1, k + 1));
+  t2 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i, j, k - 1) + FA(l2, i, j + 1, k - 1));
+  t3 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i, j + 1, k) + FA(l3, i, j + 1, k + 1));
+  t4 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i, j - 1, k) + FA(l3, i, j - 1, k + 1));
+  const double TS23 = 0.5 * ((t1 - t2) * MT(D.rdzc, k) + (t3 - t4) * MT(D.rdyc, j));
+  const double modS = sqrt(2.0) * sqrt(TS11 * TS11 + TS22 * TS22 + TS33 * TS33 + 2.0 * (TS12 * TS12) +
+                                        2.0 * (TS13 * TS13) + 2.0 * (TS23 * TS23));
+  const double dg2 = D.delg2[k - 1];
+  FA(D.nuT, i, j, k) = -(D.Cs[k - 1] + 0.0) * dg2 * modS + 0.0;
+  FA(D.kT, i, j, k) = -(D.CTs[k - 1] + 0.0) * dg2 * modS + 0.0;
+  FA(D.nT, i, j, k) = -(D.CSs[k - 1] + 0.0) * dg2 * modS + 0.0;
 }
 
 // ------------------------------------------------------------ Psource
@@ -645,7 +847,7 @@ void launch_rhs_accum(const NSDev& D, double a1, double a2, double dt, bool firs
 void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
                double rkdt, const ZRule& R, cudaStream_t s) {
   const int tx = kCNThreads;
-  CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc};
+  CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc, F.sub, F.diag};
   const size_t sm = 9 * (size_t)(D.nz + 3) * sizeof(double);
   static bool attr = false;
   if (!attr) {
@@ -657,6 +859,39 @@ void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFa
   else k_cn_column<1><<<col_grid(D, tx), tx, sm, s>>>(D, fld, q, f, a3, rkdt, R);
   count_launch();
   launch_images(D, fld, nullptr, nullptr, s);
+}
+
+void launch_cn_les(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
+                   double rkdt, const ZRule& R, const double* kT, double* b, double* c, cudaStream_t s) {
+  const int tx = kCNThreads;
+  CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc, F.sub, F.diag};
+  const size_t sm = 10 * (size_t)(D.nz + 3) * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_cn_column_les<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_cn_column_les<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_cn_column_les<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_cn_column_les<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_cn_column_les<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  const dim3 g = col_grid(D, tx);
+  switch (var) {
+    case 1: k_cn_column_les<1><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
+    case 2: k_cn_column_les<2><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
+    case 3: k_cn_column_les<3><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
+    case 5: k_cn_column_les<5><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
+    default: k_cn_column_les<8><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
+  }
+  count_launch();
+  launch_images(D, fld, nullptr, nullptr, s);
+}
+
+void launch_sgs(const NSDev& D, const ZRule& cfluc, cudaStream_t s) {
+  k_sgs<<<cell_grid(D, 128), 128, 0, s>>>(D);
+  for (double* a : {D.nuT, D.kT, D.nT}) k_ghost_field<<<col_grid(D, 64), 64, 0, s>>>(D, a, cfluc);
+  count_launch(4);
+  launch_images(D, D.nuT, D.kT, D.nT, s);
 }
 
 void launch_psource(const NSDev& D, double dt, cudaStream_t s) {

@@ -7,13 +7,25 @@
 namespace anel {
 
 // Device pointers of the column-independent CN factors of one variable.
+// Column-independent CN data per row k = 1..nz+2 (index k-1): eliminated
+// sub-diagonal ap and diagonal bp, super-diagonal c, explicit weights t1,
+// t2, wall-row right-hand side rb and flag isbc, and the raw sub-diagonal
+// and diagonal (the LES solve adds its eddy terms to these).
 struct CNFacHost {
-  const double *ap, *bp, *c, *t1, *t2, *rb, *isbc;
+  const double *ap, *bp, *c, *t1, *t2, *rb, *isbc, *sub, *diag;
 };
 
 void launch_rhs_accum(const NSDev& D, double a1, double a2, double dt, bool first, cudaStream_t s);
 void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
                double rkdt, const ZRule& R, cudaStream_t s);
+// var_advance_CN_PL with the eddy terms (Vmodel = SSM): per-column
+// elimination; b, c: G-sized scratch for the eliminated diagonal and the
+// super-diagonal.  kT = nuT (u, v, w), kappaT (rho), nappaT (scal1).
+void launch_cn_les(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
+                   double rkdt, const ZRule& R, const double* kT, double* b, double* c, cudaStream_t s);
+// SGSdiff (straincal.F90:339-414): modS, nuT, kappaT, nappaT on the
+// interior from the model profiles, then their ghosts ('cfluc').
+void launch_sgs(const NSDev& D, const ZRule& cfluc, cudaStream_t s);
 void launch_psource(const NSDev& D, double dt, cudaStream_t s);
 void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, const ZRule& Rw,
                   cudaStream_t s);

@@ -31,6 +31,9 @@ NSSolver::~NSSolver() {
   cudaFree(d_metric_);
   cudaFree(d_prof_);
   cudaFree(d_cn_);
+  cudaFree(d_les_);
+  cudaFree(d_cnb_);
+  cudaFree(d_cnc_);
   cudaFree(d_red_);
   cudaFree(d_part_);
   if (h_cn_) cudaFreeHost(h_cn_);
@@ -70,18 +73,41 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
       return ANEL_ERR_BC;
     }
   }
-  if (ns->vmodel != ANEL_MODEL_DNS || ns->rmodel != ANEL_MODEL_DNS || ns->smodel != ANEL_MODEL_DNS) {
-    set_error("the LES (SSM) stepper is not available in this build");
-    return ANEL_ERR_UNSUPPORTED;
+  for (int m : {ns->vmodel, ns->rmodel, ns->smodel})
+    if (m != ANEL_MODEL_DNS && m != ANEL_MODEL_SSM) {
+      set_error("unknown subgrid model %d", m);
+      return ANEL_ERR_ARG;
+    }
+  les_any_ = ns->vmodel == ANEL_MODEL_SSM || ns->rmodel == ANEL_MODEL_SSM || ns->smodel == ANEL_MODEL_SSM;
+  if (ns->vmodel == ANEL_MODEL_SSM) {
+    if (ns->les_freq < 1) {
+      set_error("les_freq must be >= 1");
+      return ANEL_ERR_ARG;
+    }
+    if (ns->les_delta != ANEL_DELTA_3ROOT && ns->les_delta != ANEL_DELTA_2ROOT) {
+      set_error("unknown les_delta %d", ns->les_delta);
+      return ANEL_ERR_ARG;
+    }
+    // the model coefficients are kept as profiles of k: x and y spacing
+    // must be uniform (the filter width delg then depends on k only)
+    for (int d = 0; d < 2; ++d) {
+      const double* dxc = d == 0 ? g->dxc : g->dyc;
+      const int n = d == 0 ? nx_ : ny_;
+      for (int i = 2; i <= n + 1; ++i)
+        if (!(dxc[i - 1] == dxc[1])) {
+          set_error("the GPU LES model needs uniform %s spacing (dxc(%d) differs)", d == 0 ? "x" : "y", i);
+          return ANEL_ERR_UNSUPPORTED;
+        }
+    }
   }
   if (ns->ew != 0 && ns->ew != 1) {
     set_error("ew must be 0 or 1");
     return ANEL_ERR_ARG;
   }
-  // the Crank-Nicolson kernel stages 9 column profiles of nz+3 doubles in
-  // shared memory (200 KB at most)
-  if (9 * (int64_t)(nz_ + 3) * 8 > 200 * 1024) {
-    set_error("nz = %d exceeds the column solver's limit of 2841", nz_);
+  // the Crank-Nicolson kernels stage up to 10 column profiles of nz+3
+  // doubles in shared memory (200 KB at most)
+  if (10 * (int64_t)(nz_ + 3) * 8 > 200 * 1024) {
+    set_error("nz = %d exceeds the column solver's limit of 2557", nz_);
     return ANEL_ERR_UNSUPPORTED;
   }
   const int n[3] = {nx_, ny_, nz_};
@@ -104,10 +130,22 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
   ANEL_CUDA_TRY(cudaEventCreate(&ev1_));
   const int X = nx_ + 2, Y = ny_ + 2, Z = nz_ + 2;
   G_ = (int64_t)X * Y * Z;
-  for (int q = 0; q < 14; ++q) {
+  for (int q = 0; q < 17; ++q) {
     if (q == 6 || q == 7) continue;  // r, densityBG: allocated below
+    if (q >= 14 && !les_any_) continue;  // nuT, kappaT, nappaT: LES only
     ANEL_CUDA_TRY(cudaMalloc(&d_fields_[q], G_ * sizeof(double)));
     ANEL_CUDA_TRY(cudaMemset(d_fields_[q], 0, G_ * sizeof(double)));
+  }
+  if (les_any_) {
+    // model profiles Csgs, CTsgs, CSsgs, delg^2 (zero until the first
+    // les_coeffs of the step cadence)
+    ANEL_CUDA_TRY(cudaMalloc(&d_les_, 4 * (size_t)Z * sizeof(double)));
+    ANEL_CUDA_TRY(cudaMemset(d_les_, 0, 4 * (size_t)Z * sizeof(double)));
+  }
+  if (ns->vmodel == ANEL_MODEL_SSM) {
+    // per-column eliminated diagonal and super-diagonal of the LES CN solve
+    ANEL_CUDA_TRY(cudaMalloc(&d_cnb_, G_ * sizeof(double)));
+    ANEL_CUDA_TRY(cudaMalloc(&d_cnc_, G_ * sizeof(double)));
   }
   // metrics
   std::vector<double> met;
@@ -119,7 +157,7 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
   ANEL_CUDA_TRY(cudaMalloc(&d_metric_, met.size() * sizeof(double)));
   ANEL_CUDA_TRY(cudaMemcpy(d_metric_, met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice));
   ANEL_CUDA_TRY(cudaMalloc(&d_prof_, 2 * (size_t)Z * sizeof(double)));
-  const size_t ncn = 3 * 5 * 7 * (size_t)Z;
+  const size_t ncn = 3 * 5 * 9 * (size_t)Z;
   ANEL_CUDA_TRY(cudaMalloc(&d_cn_, ncn * sizeof(double)));
   ANEL_CUDA_TRY(cudaHostAlloc(&h_cn_, ncn * sizeof(double), cudaHostAllocDefault));
   ANEL_CUDA_TRY(cudaMalloc(&d_red_, 4 * sizeof(unsigned long long)));
@@ -156,11 +194,20 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
   D_.qr = d_fields_[11];
   D_.qs = d_fields_[12];
   D_.psrc = d_fields_[13];
+  D_.nuT = d_fields_[14];
+  D_.kT = d_fields_[15];
+  D_.nT = d_fields_[16];
+  D_.Cs = d_les_;
+  D_.CTs = d_les_ ? d_les_ + Z : nullptr;
+  D_.CSs = d_les_ ? d_les_ + 2 * Z : nullptr;
+  D_.delg2 = d_les_ ? d_les_ + 3 * Z : nullptr;
   D_.rRe = rRe_;
   D_.rPr = rPr_;
   D_.rSc = rSc_;
   D_.g = gnow_;
-  D_.vles = D_.rles = D_.sles = 0;
+  D_.vles = ns->vmodel == ANEL_MODEL_SSM;
+  D_.rles = ns->rmodel == ANEL_MODEL_SSM;
+  D_.sles = ns->smodel == ANEL_MODEL_SSM;
   D_.ew = ns->ew;
   D_.scal1_on = ns->scal1_on;
   // r = densityBG = 1 until set
@@ -231,9 +278,9 @@ int NSSolver::cn_factors(int slot, double rkdt, cudaStream_t s) {
   auto dzc = [&](int k) { return m_[2][3][k - 1]; };
   for (int vi = 0; vi < 5; ++vi) {
     const int var = kVarCode[vi];
-    double* base = h_cn_ + ((size_t)(slot * 5 + vi) * 7) * Z;
+    double* base = h_cn_ + ((size_t)(slot * 5 + vi) * 9) * Z;
     double *ap = base, *bp = base + Z, *c = base + 2 * Z, *t1a = base + 3 * Z, *t2a = base + 4 * Z,
-           *rb = base + 5 * Z, *isbc = base + 6 * Z;
+           *rb = base + 5 * Z, *isbc = base + 6 * Z, *suba = base + 7 * Z, *diaga = base + 8 * Z;
     std::vector<double> sub(n, 0.0), diag(n, 0.0), sup(n, 0.0);
     for (int q = 0; q < n; ++q) {
       t1a[q] = t2a[q] = rb[q] = isbc[q] = 0.0;
@@ -306,10 +353,12 @@ int NSSolver::cn_factors(int slot, double rkdt, cudaStream_t s) {
       ap[q] = (q == 0) ? 0.0 : a[q];
       bp[q] = b[q];
       c[q] = sup[q];
+      suba[q] = sub[q];
+      diaga[q] = diag[q];
     }
   }
-  double* dst = d_cn_ + (size_t)slot * 5 * 7 * Z;
-  ANEL_CUDA_TRY(cudaMemcpyAsync(dst, h_cn_ + (size_t)slot * 5 * 7 * Z, 5 * 7 * (size_t)Z * sizeof(double),
+  double* dst = d_cn_ + (size_t)slot * 5 * 9 * Z;
+  ANEL_CUDA_TRY(cudaMemcpyAsync(dst, h_cn_ + (size_t)slot * 5 * 9 * Z, 5 * 9 * (size_t)Z * sizeof(double),
                                 cudaMemcpyHostToDevice, s));
   cn_rkdt_[slot] = rkdt;
   return ANEL_OK;
@@ -317,8 +366,9 @@ int NSSolver::cn_factors(int slot, double rkdt, cudaStream_t s) {
 
 CNFacHost NSSolver::fac(int slot, int vi) const {
   const int Z = nz_ + 2;
-  const double* base = d_cn_ + ((size_t)(slot * 5 + vi) * 7) * Z;
-  return CNFacHost{base, base + Z, base + 2 * Z, base + 3 * Z, base + 4 * Z, base + 5 * Z, base + 6 * Z};
+  const double* base = d_cn_ + ((size_t)(slot * 5 + vi) * 9) * Z;
+  return CNFacHost{base,         base + Z,     base + 2 * Z, base + 3 * Z, base + 4 * Z,
+                   base + 5 * Z, base + 6 * Z, base + 7 * Z, base + 8 * Z};
 }
 
 // --------------------------------------------------------------- fields
@@ -329,8 +379,8 @@ int NSSolver::set_fields(const anel_fields* f, int mem, cudaStream_t s) {
   double* const* src = reinterpret_cast<double* const*>(f);
   const cudaMemcpyKind kind = mem == ANEL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   bool density = false;
-  for (int q = 0; q < 14; ++q) {
-    if (!src[q]) continue;
+  for (int q = 0; q < 17; ++q) {
+    if (!src[q] || !d_fields_[q]) continue;  // LES fields exist only with a subgrid model
     ANEL_CUDA_TRY(cudaMemcpyAsync(d_fields_[q], src[q], G_ * sizeof(double), kind, s));
     if (q == 6 || q == 7) density = true;
   }
@@ -371,8 +421,9 @@ int NSSolver::get_fields(const anel_fields* f, int mem, cudaStream_t s) {
   if (!s) s = stream_;
   double* const* dst = reinterpret_cast<double* const*>(f);
   const cudaMemcpyKind kind = mem == ANEL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-  for (int q = 0; q < 14; ++q)
-    if (dst[q]) ANEL_CUDA_TRY(cudaMemcpyAsync(dst[q], d_fields_[q], G_ * sizeof(double), kind, s));
+  for (int q = 0; q < 17; ++q)
+    if (dst[q] && d_fields_[q])
+      ANEL_CUDA_TRY(cudaMemcpyAsync(dst[q], d_fields_[q], G_ * sizeof(double), kind, s));
   ANEL_CUDA_TRY(cudaStreamSynchronize(s));
   return ANEL_OK;
 }
@@ -395,12 +446,18 @@ int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, 
   D_.g = gnow_;
   launch_rhs_accum(D_, a1, a2, dt, q_zero && a1 == 0.0, s);
   const ZRule ru = zrule(NV_U), rv = zrule(NV_V), rw = zrule(NV_W);
-  launch_cn(D_, 1, D_.u, D_.qu, fac(slot, 0), a3, dt_rk, ru, s);
-  launch_cn(D_, 2, D_.v, D_.qv, fac(slot, 1), a3, dt_rk, rv, s);
-  launch_cn(D_, 3, D_.w, D_.qw, fac(slot, 2), a3, dt_rk, rw, s);
+  // var_advance_CN_PL: with Vmodel = SSM every variable gets the eddy
+  // terms (the LES block is gated on Vmodel, NSsolver.F90:3160-3190)
+  auto cn = [&](int var, double* f, const double* q, int vi, const ZRule& R, const double* kT) {
+    if (D_.vles) launch_cn_les(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, kT, d_cnb_, d_cnc_, s);
+    else launch_cn(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, s);
+  };
+  cn(1, D_.u, D_.qu, 0, ru, D_.nuT);
+  cn(2, D_.v, D_.qv, 1, rv, D_.nuT);
+  cn(3, D_.w, D_.qw, 2, rw, D_.nuT);
   launch_psource(D_, dt_rk, s);
-  launch_cn(D_, 5, D_.rho, D_.qr, fac(slot, 3), a3, dt_rk, zrule(NV_RHO), s);
-  if (prm_.scal1_on) launch_cn(D_, 8, D_.s, D_.qs, fac(slot, 4), a3, dt_rk, zrule(NV_SCAL1), s);
+  cn(5, D_.rho, D_.qr, 3, zrule(NV_RHO), D_.kT);
+  if (prm_.scal1_on) cn(8, D_.s, D_.qs, 4, zrule(NV_SCAL1), D_.nT);
   anel_mg_report rep{};
   const int st = mg_->solve_device(D_.p, D_.psrc, s, &rep);
   if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
@@ -411,6 +468,46 @@ int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, 
   if (iters) *iters = rep.iter;
   if (relmax) *relmax = rep.relmax;
   return check_launch("rk substep");
+}
+
+// les_coeffs: the filter width delg (straincal.F90:126-134) and the
+// model coefficients Csgs, CTsgs, CSsgs (SSM.F90:27,60,97) are functions of
+// the grid only; with uniform x/y spacing they depend on k alone and are
+// kept as profiles (evaluated on the host with the same libm as the
+// reference's build).  Recomputed on the reference's cadence; the values do
+// not change between calls.
+int NSSolver::les_coeffs(cudaStream_t s) {
+  if (les_coeffs_done_) return ANEL_OK;
+  const int Z = nz_ + 2;
+  std::vector<double> prof(4 * (size_t)Z, 0.0);
+  const double dxc = m_[0][3][1], dyc = m_[1][3][1];
+  const double c = prm_.ssm_const;
+  for (int k = 2; k <= nz_ + 1; ++k) {
+    const double dzc = m_[2][3][k - 1];
+    double dg;
+    if (prm_.les_delta == ANEL_DELTA_3ROOT) dg = std::pow(dxc * dyc * dzc, 1.0 / 3.0);
+    else dg = std::pow(dxc * dxc + dyc * dyc + dzc * dzc, 1.0 / 2.0);
+    double damp_u = 1.0, damp_t = 1.0;
+    if (prm_.les_damp == ANEL_DAMP_LITERAL) {
+      // REAL(4) literals 0.41 and 0.3 (SSMrho); 0.3d0 in SSM
+      const double k41 = (double)(float)0.41;
+      const double zo_u = 0.3, zo_t = (double)(float)0.3;
+      const double zc = m_[2][1][k - 1];
+      const double a = k41 * (zc + zo_u);
+      damp_u = (a * a) / ((a * a) + c * (dg * dg));
+      const double b = k41 * (zc + zo_t);
+      damp_t = (b * b) / ((b * b) + c * (dg * dg));
+    }
+    const double cs = c * damp_u;
+    prof[k - 1] = cs;
+    prof[Z + k - 1] = cs / prm_.pr_sgs * damp_t;
+    prof[2 * (size_t)Z + k - 1] = cs / prm_.pr_sgs * damp_u;
+    prof[3 * (size_t)Z + k - 1] = dg * dg;
+  }
+  ANEL_CUDA_TRY(cudaMemcpyAsync(d_les_, prof.data(), prof.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  les_coeffs_done_ = true;
+  return ANEL_OK;
 }
 
 double NSSolver::calcdt(cudaStream_t s, int* st) {
@@ -448,8 +545,16 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
     if (time_ < prm_.gt1) gnow_ = 0.0;
     else if (time_ > prm_.gt1 && time_ < prm_.gt2) gnow_ = g_orig_ * (time_ - prm_.gt1) / (prm_.gt2 - prm_.gt1);
     else if (time_ >= prm_.gt2) gnow_ = g_orig_;
+    // LES model coefficients and eddy viscosities (NSsolver.F90:86-100):
+    // les_coeffs on the step cadence, SGSdiff before every sub-step
+    const bool les = D_.vles != 0;
+    if (les && nstep_ >= prm_.les_start && nstep_ % prm_.les_freq == 0) {
+      st = les_coeffs(s);
+      if (st != ANEL_OK) return st;
+    }
     const double DTR[3] = {1.0 / 3.0 * delt, 5.0 / 12.0 * delt, 1.0 / 4.0 * delt};
     for (int q = 0; q < 3; ++q) {
+      if (les && nstep_ > prm_.les_start) launch_sgs(D_, zrule(NV_CFLUC), s);
       st = substep(A1[q], 1.0, A3[q], DTR[q], delt, s, &r.mg_iter[q], &r.mg_relmax[q], true);
       if (st != ANEL_OK) return st;
     }

@@ -38,6 +38,7 @@ class NSSolver {
   int cn_factors(int slot, double rkdt, cudaStream_t s);
   ZRule zrule(int vtype) const;
   double calcdt(cudaStream_t s, int* st);
+  int les_coeffs(cudaStream_t s);
 
   anel_ns_params prm_{};
   int device_ = 0;
@@ -55,7 +56,12 @@ class NSSolver {
   double* d_fields_[17] = {nullptr};
   double* d_metric_ = nullptr;      // rdxe rdxc rdye rdyc rdze rdzc dze dzc
   double* d_prof_ = nullptr;        // rz bgz
-  double* d_cn_ = nullptr;          // CN factors: 3 slots x 5 vars x 7 arrays x (nz+2)
+  double* d_les_ = nullptr;         // LES profiles: Csgs CTsgs CSsgs delg^2 (nz+2 each)
+  double* d_cnb_ = nullptr;         // LES CN: eliminated diagonal per cell
+  double* d_cnc_ = nullptr;         // LES CN: super-diagonal per cell
+  bool les_any_ = false;            // a subgrid model is on: nuT/kappaT/nappaT exist
+  bool les_coeffs_done_ = false;
+  double* d_cn_ = nullptr;          // CN factors: 3 slots x 5 vars x 9 arrays x (nz+2)
   double* h_cn_ = nullptr;          // pinned staging of the same
   double cn_rkdt_[3] = {-1, -1, -1};
   int cn_next_ = 0;

@@ -21,13 +21,13 @@ CMP = ("u", "v", "w", "p", "rho", "scal1")
 
 
 def setup_case(n=(32, 16, 32), ew=1, precision=abi.PREC_FP64, tol=1e-10, mode=abi.MODE_METRIC,
-               scal1_on=1, Re=1000.0, g=-0.12):
+               scal1_on=1, Re=1000.0, g=-0.12, amp=1e-3, **nskw):
     g_ = G.shear_layer_grid(*n, stretched=True)
     mgp = abi.make_mg_params(levels_for(g_), maxcy=200, tolmax=tol, pre=2, post=2,
                              tbc=(0, 1, 0, 1, 0, 0), mode=mode, stop=abi.STOP_RESID,
                              precision=abi.PREC_FP64)
-    nsp = abi.make_ns_params(Re=Re, Pr=1.0, g=g, dtmax=0.01, ew=ew, scal1_on=scal1_on)
-    f = shear.shear_layer_fields(g_)
+    nsp = abi.make_ns_params(Re=Re, Pr=1.0, g=g, dtmax=0.01, ew=ew, scal1_on=scal1_on, **nskw)
+    f = shear.shear_layer_fields(g_, amp=amp)
     o = OracleNS(g_, mgp, nsp, f)
     for name, vt in (("u", 0), ("v", 1), ("w", 2), ("rho", 4), ("scal1", 12)):
         o.ghost(f[name], vt)
@@ -148,3 +148,46 @@ def test_mixed_precision_stepper_within_tolerance():
     for name in ("u", "v", "w", "rho"):
         assert rel_l2(got[name], f[name]) < 1e-8, name
     assert rel_l2(remove_mean(got["p"]), remove_mean(f["p"])) < 1e-9
+
+
+# ------------------------------------------------------------------- LES
+LES_CASES = {
+    # SSM with f_damp = 1 and the cube-root filter width, model on from step 1
+    "ssm": dict(),
+    # wall damping with the REAL(4) literals, 2-norm filter width, model
+    # coefficients on a cadence of 2 from step 2 (nuT = 0 before)
+    "ssm_damped_cadence": dict(les_damp=abi.DAMP_LITERAL, les_delta=abi.DELTA_2ROOT, les_start=2,
+                               les_freq=2),
+}
+
+
+@pytest.mark.parametrize("case", list(LES_CASES))
+def test_les_steps_bitwise(case):
+    """LES of the shear layer (config 3 form, SSM_const 0.0289, Pr_sgs 0.7,
+    Re 50000, Ri 0.1, amplitude 1e-2): SGSdiff, the eddy terms of every RHS
+    and the per-column LES Crank-Nicolson solve, FP64 GPU == oracle bitwise
+    after four steps, eddy viscosities included."""
+    g_, o, s, f, start = setup_case(Re=50000.0, g=-0.1, amp=1e-2, les=True, **LES_CASES[case])
+    for n in range(4):
+        ro = o.step()
+        rg = s.step(1)
+        assert ro.dt == rg.dt
+        assert list(ro.mg_iter) == list(rg.mg_iter)
+    names = CMP + ("nuT", "kappaT", "nappaT")
+    got = s.get_fields(names)
+    assert np.abs(f["nuT"]).max() > 0.0
+    for name in names:
+        np.testing.assert_array_equal(got[name], f[name], err_msg=name)
+
+
+def test_les_mixed_precision_within_tolerance():
+    """LES with the mixed-precision multigrid: fields within 1e-8 relative
+    L2 of the FP64 oracle after three steps."""
+    g_, o, s, f, start = setup_case(Re=50000.0, g=-0.1, amp=1e-2, les=True,
+                                    precision=abi.PREC_MIXED, tol=1e-12)
+    for n in range(3):
+        o.step()
+    s.step(3)
+    got = s.get_fields(CMP + ("nuT",))
+    for name in ("u", "v", "w", "rho", "nuT"):
+        assert rel_l2(got[name], f[name]) < 1e-8, name
