@@ -50,6 +50,10 @@ WORKLOADS = {
     "dns": ("dns", (512, 256, 512), (9, 8, 9), dict(Re=4000.0, g=-0.08, amp=1e-3, cfl=0.5)),
     "dns256": ("dns", (256, 256, 256), (8, 8, 8), dict(Re=4000.0, g=-0.08, amp=1e-3, cfl=0.5)),
     "dns_small": ("dns", (64, 32, 64), (6, 5, 6), dict(Re=1000.0, g=-0.12, amp=1e-3, cfl=0.5)),
+    # LES shear layer: constant-coefficient Smagorinsky (Cs^2 = 0.0289, f_damp = 1),
+    # eddy diffusivity with Pr_sgs = 0.7
+    "les": ("dns", (768, 384, 384), (9, 8, 8), dict(Re=50000.0, g=-0.1, amp=1e-2, cfl=0.5, les=True)),
+    "les_small": ("dns", (96, 48, 48), (6, 5, 5), dict(Re=50000.0, g=-0.1, amp=1e-2, cfl=0.5, les=True)),
     "poisson": ("poisson", (512, 256, 512), (9, 8, 9), {}),
     "poisson256": ("poisson", (256, 256, 256), (8, 8, 8), {}),
     "poisson_small": ("poisson", (64, 32, 64), (6, 5, 6), {}),
@@ -148,7 +152,8 @@ def ns_params(phys):
 
     # DeltaT_max large: the CFL condition sets the step (calcdt)
     return abi.make_ns_params(Re=phys["Re"], Pr=1.0, g=phys["g"], cfl=phys["cfl"], dtmax=1e9,
-                              ew=1, scal1_on=0)
+                              ew=1, scal1_on=0, les=phys.get("les", False), ssm_const=0.0289,
+                              pr_sgs=0.7, les_damp=abi.DAMP_NONE, les_start=0, les_freq=1)
 
 
 def poisson_rhs(g):
@@ -413,15 +418,19 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     kind, n, lv, phys = WORKLOADS[args.workload]
     nx, ny, nz = n
+    field_mb = (nx + 2) * (ny + 2) * (nz + 2) * 8 / 1e6
+    l2note = (f"inputs larger than L2 ({field_mb:.0f} MB per FP64 field)" if field_mb > 126
+              else f"small ({field_mb:.1f} MB per FP64 field)")
     if kind == "dns":
         metric = "cell-updates/s (RK3 step incl. 3 projections)"
         unit = "cell-updates/s"
-        config = {"workload": f"DNS shear layer {nx}x{ny}x{nz}: Re={phys['Re']:g}, Pr=1, "
+        model = "LES (SSM, Cs^2=0.0289, Pr_sgs=0.7)" if phys.get("les") else "DNS"
+        config = {"workload": f"{model} shear layer {nx}x{ny}x{nz}: Re={phys['Re']:g}, Pr=1, "
                               f"Ri={-phys['g']:g}, amp {phys['amp']:g}, CFL {phys['cfl']:g}, "
                               f"MG to ||f-A p||/||f|| <= {TOL:g} each sub-step",
                   "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V({args.pre},{args.post}), metric, {args.prec}",
                   "ew": 1, "scal1": "off (zero)", "parallelism": f"replicas x{args.gpus}",
-                  "l2": "inputs larger than L2 (545 MB per FP64 field)" if nx >= 256 else "small"}
+                  "l2": l2note}
     else:
         metric = "MG solve throughput to 1e-10 relative residual (cell-solves/s)"
         unit = "cell-solves/s"
@@ -429,7 +438,7 @@ def main():
                               f"x/y, Neumann z, to ||f-A phi||/||f|| <= {TOL:g} from phi0 = 0",
                   "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V({args.pre},{args.post}), metric, {args.prec}",
                   "parallelism": f"replicas x{args.gpus}",
-                  "l2": "inputs larger than L2 (545 MB per FP64 field)" if nx >= 256 else "small"}
+                  "l2": l2note}
     threads = os.cpu_count() or 1
     if args.impl == "reference":
         if rank != 0:
