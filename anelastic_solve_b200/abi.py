@@ -140,6 +140,30 @@ class Fields(C.Structure):
 FIELD_NAMES = [n for n, _ in Fields._fields_]
 
 
+INIT_SHEAR = 0
+INIT_FIELDS = 1
+
+
+class Request(C.Structure):
+    """anel_request: one serving member."""
+    _fields_ = [("grid", GridDesc), ("mg", MGParams), ("ns", NSParams), ("nsteps", C.c_int32),
+                ("init", C.c_int32), ("seed", C.c_uint32), ("reserved", C.c_int32),
+                ("amp", C.c_double), ("fields_in", C.POINTER(Fields)),
+                ("fields_out", C.POINTER(Fields))]
+
+
+class Result(C.Structure):
+    _fields_ = [("id", C.c_int64), ("status", C.c_int32), ("nsteps", C.c_int32),
+                ("cells", C.c_int64), ("queue_ms", C.c_double), ("run_ms", C.c_double),
+                ("latency_ms", C.c_double), ("dt_last", C.c_double), ("max_div", C.c_double)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("bytes_in_use", C.c_int64), ("peak_bytes", C.c_int64), ("active", C.c_int32),
+                ("peak_active", C.c_int32), ("contexts", C.c_int32), ("queued", C.c_int32)]
+
+
 class StepReport(C.Structure):
     _fields_ = [("nstep", C.c_int32), ("mg_iter", C.c_int32 * 3), ("dt", C.c_double),
                 ("time", C.c_double), ("mg_relmax", C.c_double * 3), ("max_div", C.c_double),

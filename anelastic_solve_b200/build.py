@@ -31,6 +31,7 @@ SOURCES = {
     "ns_kernels.cu": ["-fmad=false"],
     "ns_solver.cu": ["-fmad=false"],
     "noalloc.cu": ["-fmad=false"],
+    "serve.cu": ["-fmad=false"],
 }
 
 

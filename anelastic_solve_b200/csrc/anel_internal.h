@@ -31,6 +31,9 @@ const char* last_error();
 extern std::atomic<int64_t> g_launches;
 inline void count_launch(int64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 int check_launch(const char* what);
+// Raise a kernel's dynamic shared-memory limit once per (device, kernel);
+// safe to call from several host threads.
+void set_smem_limit_once(const void* func, int bytes);
 
 // ------------------------------------------------------------ level maps
 // One multigrid level, 1-based Fortran conventions of mg_init.F90:

@@ -2,6 +2,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <mutex>
+#include <vector>
 
 #include "mg_solver.h"
 #include "ns_solver.h"
@@ -18,6 +19,18 @@ void set_error(const char* fmt, ...) {
   va_end(ap);
 }
 const char* last_error() { return t_err; }
+
+void set_smem_limit_once(const void* func, int bytes) {
+  static std::mutex mu;
+  static std::vector<std::pair<int, const void*>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  for (const auto& d : done)
+    if (d.first == dev && d.second == func) return;
+  cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  done.emplace_back(dev, func);
+}
 
 int check_launch(const char* what) {
   const cudaError_t e = cudaGetLastError();

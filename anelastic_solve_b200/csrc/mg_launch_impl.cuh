@@ -28,11 +28,7 @@ void launch_zline(const DevLevel<T>& L, int color, const T* ap, const T* bp, cud
     const int warps = 4;
     const size_t sm = (size_t)warps * 4 * NMAX * sizeof(T);
     const unsigned blocks = (unsigned)((cols + warps - 1) / warps);
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_zline_pcr<T, NMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      attr = true;
-    }
+    set_smem_limit_once((const void*)k_zline_pcr<T, NMAX>, (int)sm);
     k_zline_pcr<T, NMAX><<<blocks, 32 * warps, sm, s>>>(L, color);
     count_launch();
     return;
@@ -46,12 +42,7 @@ template <typename T>
 void launch_zline_seg(const DevLevel<T>& L, int color, const SegFac<T>& F, cudaStream_t s) {
   const int64_t cols = (int64_t)((L.nx + 1) / 2) * L.ny;
   const size_t sm = (size_t)kZSegRows * kZSeg * 32 * sizeof(T);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_zline_seg<T, kZSeg, kZSegRows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sm);
-    attr = true;
-  }
+  set_smem_limit_once((const void*)k_zline_seg<T, kZSeg, kZSegRows>, (int)sm);
   dim3 block(32, kZSeg, 1);
   k_zline_seg<T, kZSeg, kZSegRows><<<(unsigned)((cols + 31) / 32), block, sm, s>>>(L, color, F);
   count_launch();

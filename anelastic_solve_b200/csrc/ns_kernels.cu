@@ -849,12 +849,8 @@ void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFa
   const int tx = kCNThreads;
   CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc, F.sub, F.diag};
   const size_t sm = 9 * (size_t)(D.nz + 3) * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_cn_column<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_cn_column<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  set_smem_limit_once((const void*)k_cn_column<1>, 200 * 1024);
+  set_smem_limit_once((const void*)k_cn_column<3>, 200 * 1024);
   if (var == 3) k_cn_column<3><<<col_grid(D, tx), tx, sm, s>>>(D, fld, q, f, a3, rkdt, R);
   else k_cn_column<1><<<col_grid(D, tx), tx, sm, s>>>(D, fld, q, f, a3, rkdt, R);
   count_launch();
@@ -866,15 +862,10 @@ void launch_cn_les(const NSDev& D, int var, double* fld, const double* q, const 
   const int tx = kCNThreads;
   CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc, F.sub, F.diag};
   const size_t sm = 10 * (size_t)(D.nz + 3) * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_cn_column_les<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_cn_column_les<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_cn_column_les<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_cn_column_les<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_cn_column_les<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  for (const void* f : {(const void*)k_cn_column_les<1>, (const void*)k_cn_column_les<2>,
+                        (const void*)k_cn_column_les<3>, (const void*)k_cn_column_les<5>,
+                        (const void*)k_cn_column_les<8>})
+    set_smem_limit_once(f, 200 * 1024);
   const dim3 g = col_grid(D, tx);
   switch (var) {
     case 1: k_cn_column_les<1><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
@@ -892,6 +883,49 @@ void launch_sgs(const NSDev& D, const ZRule& cfluc, cudaStream_t s) {
   for (double* a : {D.nuT, D.kT, D.nT}) k_ghost_field<<<col_grid(D, 64), 64, 0, s>>>(D, a, cfluc);
   count_launch(4);
   launch_images(D, D.nuT, D.kT, D.nT, s);
+}
+
+// Park-Miller minimal standard: element n (0-based) of the sequence of a
+// seed is seed * 16807^(n+1) mod (2^31-1) (Park & Miller, CACM 31(10),
+// 1988); the power by binary exponentiation, products below 2^62.
+__device__ __forceinline__ double park_miller_at(uint64_t seed, uint64_t n) {
+  const uint64_t m = 2147483647ull;
+  uint64_t r = 1, b = 16807ull, e = n + 1;
+  while (e) {
+    if (e & 1) r = (r * b) % m;
+    b = (b * b) % m;
+    e >>= 1;
+  }
+  const uint64_t x = (seed * r) % m;
+  return (double)x / 2147483647.0;
+}
+
+__global__ void k_init_shear(NSDev D, const double* __restrict__ prof, uint64_t seed, double amp,
+                             double zmax) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < D.G;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int k = 1 + (int)(c / D.XY);
+    const double th = prof[k - 1];
+    const bool in = prof[D.Z + k - 1] < zmax;
+    double pert[3];
+    for (int q = 0; q < 3; ++q)
+      pert[q] = in ? amp * (2.0 * park_miller_at(seed, (uint64_t)q * D.G + c) - 1.0) : 0.0;
+    D.u[c] = th + pert[0];
+    D.v[c] = 0.0 + pert[1];
+    D.w[c] = 0.0 + pert[2];
+    D.rho[c] = -th;
+    D.p[c] = 0.0;
+    D.s[c] = 0.0;
+  }
+}
+
+void launch_init_shear(const NSDev& D, const double* prof, uint32_t seed, double amp, double zmax,
+                       cudaStream_t s) {
+  int64_t b = (D.G + 255) / 256;
+  if (b > 148 * 8) b = 148 * 8;
+  const uint64_t sd = (uint64_t)seed % 2147483647ull;
+  k_init_shear<<<(unsigned)b, 256, 0, s>>>(D, prof, sd ? sd : 1ull, amp, zmax);
+  count_launch();
 }
 
 void launch_psource(const NSDev& D, double dt, cudaStream_t s) {

@@ -27,6 +27,11 @@ void launch_cn_les(const NSDev& D, int var, double* fld, const double* q, const 
 // interior from the model profiles, then their ghosts ('cfluc').
 void launch_sgs(const NSDev& D, const ZRule& cfluc, cudaStream_t s);
 void launch_psource(const NSDev& D, double dt, cudaStream_t s);
+// shear-layer initial state (NSSolver::init_shear): prof = tanh(zc)[Z],
+// |zc|[Z]; noise from the Park-Miller sequence of seed, element q*G + c
+// for u (q = 0), v (1), w (2) at Fortran linear index c.
+void launch_init_shear(const NSDev& D, const double* prof, uint32_t seed, double amp, double zmax,
+                       cudaStream_t s);
 void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, const ZRule& Rw,
                   cudaStream_t s);
 void launch_ghost_field(const NSDev& D, double* a, const ZRule& R, cudaStream_t s);

@@ -32,6 +32,7 @@ NSSolver::~NSSolver() {
   cudaFree(d_prof_);
   cudaFree(d_cn_);
   cudaFree(d_les_);
+  cudaFree(d_ic_);
   cudaFree(d_cnb_);
   cudaFree(d_cnc_);
   cudaFree(d_red_);
@@ -468,6 +469,56 @@ int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, 
   if (iters) *iters = rep.iter;
   if (relmax) *relmax = rep.relmax;
   return check_launch("rk substep");
+}
+
+int NSSolver::reset(const anel_ns_params* ns, cudaStream_t s) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  const bool les = ns->vmodel == ANEL_MODEL_SSM || ns->rmodel == ANEL_MODEL_SSM ||
+                   ns->smodel == ANEL_MODEL_SSM;
+  if (les != les_any_ || (ns->vmodel == ANEL_MODEL_SSM) != (D_.vles != 0) || ns->ew != prm_.ew ||
+      std::memcmp(ns->tb, prm_.tb, sizeof(prm_.tb)) != 0 ||
+      std::memcmp(ns->vb, prm_.vb, sizeof(prm_.vb)) != 0) {
+    set_error("reset: models, edge-node flag and boundary conditions must match the context");
+    return ANEL_ERR_ARG;
+  }
+  prm_ = *ns;
+  rRe_ = 1.0 / ns->Re;
+  rPr_ = 1.0 / ns->Pr;
+  rSc_ = 1.0 / ns->Sc;
+  g_orig_ = ns->g_final;
+  gnow_ = ns->g_init;
+  D_.rRe = rRe_;
+  D_.rPr = rPr_;
+  D_.rSc = rSc_;
+  D_.g = gnow_;
+  D_.rles = ns->rmodel == ANEL_MODEL_SSM;
+  D_.sles = ns->smodel == ANEL_MODEL_SSM;
+  D_.scal1_on = ns->scal1_on;
+  for (double& r : cn_rkdt_) r = -1.0;  // the CN factors depend on Re, Pr, Sc
+  time_ = 0.0;
+  nstep_ = 1;
+  for (int q = 8; q < 17; ++q)
+    if (d_fields_[q]) ANEL_CUDA_TRY(cudaMemsetAsync(d_fields_[q], 0, G_ * sizeof(double), s));
+  if (d_les_) ANEL_CUDA_TRY(cudaMemsetAsync(d_les_, 0, 4 * (size_t)(nz_ + 2) * sizeof(double), s));
+  les_coeffs_done_ = false;
+  return ANEL_OK;
+}
+
+int NSSolver::init_shear(uint32_t seed, double amp, double zmax, cudaStream_t s) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  const int Z = nz_ + 2;
+  if (!d_ic_) ANEL_CUDA_TRY(cudaMalloc(&d_ic_, 2 * (size_t)Z * sizeof(double)));
+  std::vector<double> prof(2 * (size_t)Z);
+  for (int k = 0; k < Z; ++k) {
+    prof[k] = std::tanh(m_[2][1][k]);
+    prof[Z + k] = std::fabs(m_[2][1][k]);
+  }
+  ANEL_CUDA_TRY(cudaMemcpyAsync(d_ic_, prof.data(), prof.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  launch_init_shear(D_, d_ic_, seed, amp, zmax, s);
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));  // prof lives on the host stack
+  return check_launch("init_shear");
 }
 
 // les_coeffs: the filter width delg (straincal.F90:126-134) and the

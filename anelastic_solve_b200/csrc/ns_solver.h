@@ -23,6 +23,15 @@ class NSSolver {
   int step(int nsteps, cudaStream_t s, anel_step_report* rep);
   int project(cudaStream_t s, int* iters, double* relmax);
   int divergence(cudaStream_t s, double* out);
+  // Re-target a context to a new member with the same grid, models and
+  // boundary conditions (serving pool): new physics parameters, clock at
+  // step 1, time 0, accumulators and eddy fields zeroed.
+  int reset(const anel_ns_params* ns, cudaStream_t s);
+  // Seeded shear-layer state on the device (the layout of shear.py's
+  // shear_layer_fields): u = tanh(zc) + noise, v, w = noise, rho =
+  // -tanh(zc), noise amp*(2U-1) on |zc| < zmax from the Park-Miller
+  // sequence of the seed; p, scal1 = 0.
+  int init_shear(uint32_t seed, double amp, double zmax, cudaStream_t s);
   void set_clock(double time, int nstep) {
     time_ = time;
     nstep_ = nstep;
@@ -57,6 +66,7 @@ class NSSolver {
   double* d_metric_ = nullptr;      // rdxe rdxc rdye rdyc rdze rdzc dze dzc
   double* d_prof_ = nullptr;        // rz bgz
   double* d_les_ = nullptr;         // LES profiles: Csgs CTsgs CSsgs delg^2 (nz+2 each)
+  double* d_ic_ = nullptr;          // tanh(zc) and |zc| profiles of init_shear
   double* d_cnb_ = nullptr;         // LES CN: eliminated diagonal per cell
   double* d_cnc_ = nullptr;         // LES CN: super-diagonal per cell
   bool les_any_ = false;            // a subgrid model is on: nuT/kappaT/nappaT exist

@@ -1,0 +1,415 @@
+// serve.cu -- continuous-batching serving engine for ensembles of
+// independent shear-layer members (many short runs of uneven grid sizes).
+// It has no counterpart in the reference, where every run is its own job.
+//
+// Design:
+//   * requests enter a FIFO queue (anel_serve_submit returns at once);
+//   * max_active worker threads each drive one member at a time on the
+//     member's own CUDA stream, so the kernels of different members overlap
+//     on the device (small members leave most SMs idle on their own);
+//   * a member is admitted when the device memory it needs fits the HBM
+//     budget: an idle context of the same bucket (same grid, models,
+//     multigrid and boundary setup) is re-used without allocating;
+//     otherwise idle contexts of other buckets are released, least recently
+//     used first, until the new context fits;
+//   * contexts stay resident between members of their bucket (fields,
+//     multigrid hierarchy, factor caches, ghost tables);
+//   * results (status, queue/run/total latency) are collected by
+//     anel_serve_poll.
+// A member's arithmetic does not depend on what else runs: its kernels
+// read and write only its own buffers, so its fields are bit-identical
+// alone and in the mix.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "ns_solver.h"
+
+namespace anel {
+
+using Clock = std::chrono::steady_clock;
+
+static double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+static uint64_t fnv1a(const void* p, size_t n, uint64_t h) {
+  const unsigned char* c = static_cast<const unsigned char*>(p);
+  for (size_t i = 0; i < n; ++i) {
+    h ^= c[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+struct ServeJob {
+  int64_t id = 0;
+  anel_request req{};
+  anel_grid_desc grid{};
+  std::vector<double> metric;  // owned copies of the 18 metric arrays
+  anel_fields fin{}, fout{};
+  bool has_in = false, has_out = false;
+  Clock::time_point t_submit;
+  std::string key;
+  int64_t est_bytes = 0;
+};
+
+struct ServeCtx {
+  NSSolver* s = nullptr;
+  std::string key;
+  int64_t bytes = 0;
+  Clock::time_point last_used;
+};
+
+class ServeEngine {
+ public:
+  int init(int device, int64_t budget, int max_active) {
+    if (budget <= 0 || max_active < 1) {
+      set_error("serve: budget must be positive and max_active >= 1");
+      return ANEL_ERR_ARG;
+    }
+    device_ = device;
+    budget_ = budget;
+    ANEL_CUDA_TRY(cudaSetDevice(device_));
+    for (int t = 0; t < max_active; ++t) threads_.emplace_back([this] { worker(); });
+    return ANEL_OK;
+  }
+
+  ~ServeEngine() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_work_.notify_all();
+    for (auto& t : threads_) t.join();
+    cudaSetDevice(device_);
+    for (ServeCtx* c : idle_) {
+      delete c->s;
+      delete c;
+    }
+    for (ServeJob* j : queue_) delete j;
+  }
+
+  int submit(const anel_request* r, int64_t* id) {
+    if (!r) {
+      set_error("serve: null request");
+      return ANEL_ERR_ARG;
+    }
+    const anel_grid_desc& g = r->grid;
+    if (g.nx < 1 || g.ny < 1 || g.nz < 1 || r->nsteps < 0) {
+      set_error("serve: bad grid sizes or step count");
+      return ANEL_ERR_ARG;
+    }
+    if (r->init != ANEL_INIT_SHEAR && !(r->init == ANEL_INIT_FIELDS && r->fields_in)) {
+      set_error("serve: init must be ANEL_INIT_SHEAR, or ANEL_INIT_FIELDS with fields_in");
+      return ANEL_ERR_ARG;
+    }
+    auto* job = new ServeJob();
+    job->req = *r;
+    // own copies of the metric arrays (the caller's may go away)
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const double* src[18] = {g.xe, g.xc, g.dxe, g.dxc, g.rdxe, g.rdxc, g.ye, g.yc, g.dye,
+                             g.dyc, g.rdye, g.rdyc, g.ze, g.zc, g.dze, g.dzc, g.rdze, g.rdzc};
+    size_t tot = 0;
+    for (int a = 0; a < 18; ++a) {
+      if (!src[a]) {
+        delete job;
+        set_error("serve: grid metric array %d is null", a);
+        return ANEL_ERR_ARG;
+      }
+      tot += n[a / 6] + 2;
+    }
+    job->metric.resize(tot);
+    const double** dst[18] = {&job->grid.xe, &job->grid.xc, &job->grid.dxe, &job->grid.dxc,
+                              &job->grid.rdxe, &job->grid.rdxc, &job->grid.ye, &job->grid.yc,
+                              &job->grid.dye, &job->grid.dyc, &job->grid.rdye, &job->grid.rdyc,
+                              &job->grid.ze, &job->grid.zc, &job->grid.dze, &job->grid.dzc,
+                              &job->grid.rdze, &job->grid.rdzc};
+    job->grid.nx = g.nx;
+    job->grid.ny = g.ny;
+    job->grid.nz = g.nz;
+    job->grid.xL = g.xL;
+    job->grid.yL = g.yL;
+    job->grid.zL = g.zL;
+    size_t off = 0;
+    uint64_t h = 1469598103934665603ull;
+    for (int a = 0; a < 18; ++a) {
+      const size_t len = n[a / 6] + 2;
+      std::memcpy(job->metric.data() + off, src[a], len * sizeof(double));
+      *dst[a] = job->metric.data() + off;
+      h = fnv1a(src[a], len * sizeof(double), h);
+      off += len;
+    }
+    if (r->fields_in) {
+      job->fin = *r->fields_in;
+      job->has_in = true;
+    }
+    if (r->fields_out) {
+      job->fout = *r->fields_out;
+      job->has_out = true;
+    }
+    // bucket: grid, multigrid setup, models, edge flag, boundary tables and
+    // the kind of initial state (a context that took caller fields may
+    // carry a non-unit density)
+    const anel_ns_params& nk = r->ns;
+    h = fnv1a(&r->mg, sizeof(r->mg), h);
+    h = fnv1a(nk.tb, sizeof(nk.tb), h);
+    h = fnv1a(nk.vb, sizeof(nk.vb), h);
+    const int flags[6] = {nk.vmodel, nk.rmodel, nk.smodel, nk.ew, r->init, 0};
+    h = fnv1a(flags, sizeof(flags), h);
+    job->key = std::to_string(g.nx) + "x" + std::to_string(g.ny) + "x" + std::to_string(g.nz) + ":" +
+               std::to_string(h);
+    // device memory of a context: FP64 fields (14, +3 eddy fields, +2
+    // LES-CN scratch), multigrid (FP64 fine pair, FP32 levels) and slack
+    const int64_t G = (int64_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
+    const bool les_any = nk.vmodel == ANEL_MODEL_SSM || nk.rmodel == ANEL_MODEL_SSM ||
+                         nk.smodel == ANEL_MODEL_SSM;
+    const int nf = 14 + (les_any ? 3 : 0) + (nk.vmodel == ANEL_MODEL_SSM ? 2 : 0);
+    const int64_t mgb = r->mg.precision == ANEL_PREC_MIXED ? 32 : 24;
+    job->est_bytes = G * (8 * nf + mgb) + ((int64_t)64 << 20);
+    std::lock_guard<std::mutex> lk(mu_);
+    job->id = next_id_++;
+    job->t_submit = Clock::now();
+    if (id) *id = job->id;
+    queue_.push_back(job);
+    ++submitted_;
+    cv_work_.notify_one();
+    return ANEL_OK;
+  }
+
+  int poll(anel_result* out, int cap, int* n, int wait_ms) {
+    std::unique_lock<std::mutex> lk(mu_);
+    if (results_.empty() && wait_ms > 0)
+      cv_done_.wait_for(lk, std::chrono::milliseconds(wait_ms), [this] { return !results_.empty(); });
+    int k = 0;
+    while (k < cap && !results_.empty()) {
+      out[k++] = results_.front();
+      results_.pop_front();
+    }
+    if (n) *n = k;
+    return ANEL_OK;
+  }
+
+  int drain() {
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_done_.wait(lk, [this] { return queue_.empty() && active_ == 0; });
+    return ANEL_OK;
+  }
+
+  void stats(anel_serve_stats* st) {
+    std::lock_guard<std::mutex> lk(mu_);
+    st->submitted = submitted_;
+    st->completed = completed_;
+    st->failed = failed_;
+    st->bytes_in_use = used_;
+    st->peak_bytes = peak_;
+    st->active = active_;
+    st->peak_active = peak_active_;
+    st->contexts = contexts_;
+    st->queued = (int32_t)queue_.size();
+  }
+
+ private:
+  // Admit the head of the queue if it fits (mu_ held).  Returns the job and
+  // sets ctx (a re-used idle context) or need_new (budget reserved).
+  ServeJob* admit(ServeCtx*& ctx, bool& need_new) {
+    ServeJob* head = queue_.front();
+    auto it = std::find_if(idle_.begin(), idle_.end(), [&](ServeCtx* c) { return c->key == head->key; });
+    if (it != idle_.end()) {
+      ctx = *it;
+      idle_.erase(it);
+      queue_.pop_front();
+      return head;
+    }
+    while (used_ + head->est_bytes > budget_ && !idle_.empty()) {
+      auto lru = std::min_element(idle_.begin(), idle_.end(),
+                                  [](ServeCtx* a, ServeCtx* b) { return a->last_used < b->last_used; });
+      ServeCtx* c = *lru;
+      idle_.erase(lru);
+      used_ -= c->bytes;
+      --contexts_;
+      delete c->s;
+      delete c;
+    }
+    if (used_ + head->est_bytes <= budget_) {
+      used_ += head->est_bytes;
+      peak_ = std::max(peak_, used_);
+      need_new = true;
+      queue_.pop_front();
+      return head;
+    }
+    return nullptr;
+  }
+
+  void worker() {
+    cudaSetDevice(device_);
+    for (;;) {
+      ServeJob* job = nullptr;
+      ServeCtx* ctx = nullptr;
+      bool need_new = false;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        for (;;) {
+          if (!queue_.empty()) {
+            job = admit(ctx, need_new);
+            if (job) break;
+            if (active_ == 0) {
+              // does not fit even with the device to itself
+              ServeJob* head = queue_.front();
+              queue_.pop_front();
+              anel_result r{};
+              r.id = head->id;
+              r.status = ANEL_ERR_NOMEM;
+              r.nsteps = head->req.nsteps;
+              results_.push_back(r);
+              ++failed_;
+              delete head;
+              cv_done_.notify_all();
+              continue;
+            }
+          } else if (stop_) {
+            return;
+          }
+          cv_work_.wait(lk);
+        }
+        ++active_;
+        peak_active_ = std::max(peak_active_, active_);
+      }
+      anel_result res{};
+      const int st = run(*job, ctx, need_new, res);
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        --active_;
+        if (ctx) {
+          if (st == ANEL_OK) {
+            ctx->last_used = Clock::now();
+            idle_.push_back(ctx);
+          } else {
+            used_ -= ctx->bytes;
+            --contexts_;
+            delete ctx->s;
+            delete ctx;
+          }
+        } else if (need_new) {
+          used_ -= job->est_bytes;
+        }
+        results_.push_back(res);
+        if (st == ANEL_OK) ++completed_;
+        else ++failed_;
+        delete job;
+      }
+      cv_work_.notify_all();
+      cv_done_.notify_all();
+    }
+  }
+
+  int run(ServeJob& job, ServeCtx*& ctx, bool need_new, anel_result& res) {
+    const Clock::time_point t0 = Clock::now();
+    res.id = job.id;
+    res.queue_ms = ms_between(job.t_submit, t0);
+    res.nsteps = job.req.nsteps;
+    res.cells = (int64_t)job.grid.nx * job.grid.ny * job.grid.nz;
+    int st = ANEL_OK;
+    if (need_new) {
+      NSSolver* s = NSSolver::create(&job.grid, &job.req.mg, &job.req.ns, device_, &st);
+      if (!s) {
+        res.status = st;
+        return st;
+      }
+      ctx = new ServeCtx{s, job.key, job.est_bytes, t0};
+      std::lock_guard<std::mutex> lk(mu_);
+      ++contexts_;
+    }
+    NSSolver* s = ctx->s;
+    cudaStream_t sm = s->stream();
+    st = s->reset(&job.req.ns, sm);
+    if (st == ANEL_OK) {
+      if (job.req.init == ANEL_INIT_SHEAR) st = s->init_shear(job.req.seed, job.req.amp, 2.0, sm);
+      else st = s->set_fields(&job.fin, ANEL_MEM_HOST, sm);
+    }
+    int it = 0;
+    double rm = 0.0;
+    if (st == ANEL_OK) st = s->project(sm, &it, &rm);
+    if (st == ANEL_ERR_NOCONV) st = ANEL_OK;
+    anel_step_report rep{};
+    if (st == ANEL_OK && job.req.nsteps > 0) st = s->step(job.req.nsteps, sm, &rep);
+    if (st == ANEL_OK && job.has_out) st = s->get_fields(&job.fout, ANEL_MEM_HOST, sm);
+    const Clock::time_point t1 = Clock::now();
+    res.status = st;
+    res.run_ms = ms_between(t0, t1);
+    res.latency_ms = ms_between(job.t_submit, t1);
+    res.dt_last = rep.dt;
+    res.max_div = rep.max_div;
+    return st;
+  }
+
+  std::mutex mu_;
+  std::condition_variable cv_work_, cv_done_;
+  std::deque<ServeJob*> queue_;
+  std::vector<ServeCtx*> idle_;
+  std::deque<anel_result> results_;
+  std::vector<std::thread> threads_;
+  int device_ = 0;
+  int64_t budget_ = 0, used_ = 0, peak_ = 0;
+  int active_ = 0, peak_active_ = 0, contexts_ = 0;
+  int64_t submitted_ = 0, completed_ = 0, failed_ = 0, next_id_ = 1;
+  bool stop_ = false;
+};
+
+}  // namespace anel
+
+struct anel_serve {
+  anel::ServeEngine* e;
+};
+
+extern "C" {
+
+anel_serve* anel_serve_create(int32_t device, int64_t hbm_budget_bytes, int32_t max_active,
+                              int32_t* status) {
+  auto* e = new anel::ServeEngine();
+  const int st = e->init(device, hbm_budget_bytes, max_active);
+  if (status) *status = st;
+  if (st != ANEL_OK) {
+    delete e;
+    return nullptr;
+  }
+  return new anel_serve{e};
+}
+
+int anel_serve_submit(anel_serve* e, const anel_request* req, int64_t* id) {
+  if (!e) return ANEL_ERR_ARG;
+  return e->e->submit(req, id);
+}
+
+int anel_serve_poll(anel_serve* e, anel_result* out, int32_t cap, int32_t* n, int32_t wait_ms) {
+  if (!e || (!out && cap > 0)) return ANEL_ERR_ARG;
+  int k = 0;
+  const int st = e->e->poll(out, cap, &k, wait_ms);
+  if (n) *n = k;
+  return st;
+}
+
+int anel_serve_drain(anel_serve* e) {
+  if (!e) return ANEL_ERR_ARG;
+  return e->e->drain();
+}
+
+int anel_serve_stats_get(anel_serve* e, anel_serve_stats* st) {
+  if (!e || !st) return ANEL_ERR_ARG;
+  e->e->stats(st);
+  return ANEL_OK;
+}
+
+void anel_serve_destroy(anel_serve* e) {
+  if (!e) return;
+  delete e->e;
+  delete e;
+}
+
+}  // extern "C"

@@ -9,6 +9,8 @@ drawn in Fortran order (i fastest) for u, then v, then w.
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 from . import abi
@@ -52,8 +54,11 @@ def shear_layer_fields(grid, amp: float = 1e-3, seed: int = 12345, zmax: float =
     sh = grid.ghosted
     zc = grid.z.xc
     f = {n: np.zeros(sh, order="F") for n in abi.FIELD_NAMES}
-    f["u"][:] = np.tanh(zc)[None, None, :]
-    f["rho"][:] = -np.tanh(zc)[None, None, :]
+    # tanh per level by the C library (not numpy's vectorised tanh), so the
+    # device generator of the serving engine reproduces this state exactly
+    th = np.array([math.tanh(z) for z in zc])
+    f["u"][:] = th[None, None, :]
+    f["rho"][:] = -th[None, None, :]
     f["r"][:] = 1.0
     f["densityBG"][:] = 1.0
     mask = (np.abs(zc) < zmax)[None, None, :]

@@ -300,6 +300,63 @@ int anel_divergence_noalloc(int32_t nx, int32_t ny, int32_t nz, const double* u,
                             const double* w, const double* rdxc, const double* rdyc,
                             const double* rdzc, double* out, void* stream);
 
+/* ---- serving: continuous batching of independent members ----------------
+ * An engine that runs many short, independent shear-layer members (an
+ * ensemble, or a request stream) on one GPU.  Not a reference routine:
+ * each reference run is its own job.  Requests queue in FIFO order;
+ * max_active host threads each drive one member on its own stream, so
+ * members overlap on the device; a member is admitted when its device
+ * memory fits the HBM budget, re-using an idle context of the same grid /
+ * model / multigrid setup or releasing idle contexts of other setups
+ * (least recently used first).  A member's fields do not depend on what
+ * else runs.  Caller arrays named in a request (fields_in, fields_out) must
+ * stay alive until its result is polled. */
+typedef struct anel_serve anel_serve;
+enum { ANEL_INIT_SHEAR = 0, ANEL_INIT_FIELDS = 1 };
+typedef struct {
+  anel_grid_desc grid;   /* host metric arrays: copied at submit */
+  anel_mg_params mg;
+  anel_ns_params ns;
+  int32_t nsteps;        /* RK3 steps after the initial projection */
+  int32_t init;          /* ANEL_INIT_SHEAR: shear layer U = tanh(zc), rho = -tanh(zc), noise
+                          * amp*(2U-1) on |zc| < 2 from the Park-Miller sequence of seed;
+                          * ANEL_INIT_FIELDS: the host fields of fields_in */
+  uint32_t seed;
+  int32_t reserved;
+  double amp;
+  const anel_fields* fields_in;  /* host; ANEL_INIT_FIELDS only */
+  anel_fields* fields_out;       /* host, may be NULL: fields after the last step */
+} anel_request;
+typedef struct {
+  int64_t id;
+  int32_t status;        /* ANEL_OK or the member's error (ANEL_ERR_NOMEM: larger than the budget) */
+  int32_t nsteps;
+  int64_t cells;         /* interior cells */
+  double queue_ms;       /* submit -> start (host steady clock) */
+  double run_ms;         /* start -> fields ready */
+  double latency_ms;     /* submit -> fields ready */
+  double dt_last;        /* time step of the last step */
+  double max_div;        /* max |div u| after the last step */
+} anel_result;
+typedef struct {
+  int64_t submitted, completed, failed;
+  int64_t bytes_in_use, peak_bytes;  /* admitted context memory (estimates) */
+  int32_t active, peak_active, contexts, queued;
+} anel_serve_stats;
+
+anel_serve* anel_serve_create(int32_t device, int64_t hbm_budget_bytes, int32_t max_active,
+                              int32_t* status);
+/* queue a member; returns at once with its id */
+int anel_serve_submit(anel_serve* e, const anel_request* req, int64_t* id);
+/* up to cap finished members into out (n of them); waits up to wait_ms
+ * for the first when none is ready */
+int anel_serve_poll(anel_serve* e, anel_result* out, int32_t cap, int32_t* n, int32_t wait_ms);
+/* wait until every submitted member has finished */
+int anel_serve_drain(anel_serve* e);
+int anel_serve_stats_get(anel_serve* e, anel_serve_stats* st);
+/* finishes queued and running members, then frees every context */
+void anel_serve_destroy(anel_serve* e);
+
 /* Drop-in form for the Fortran driver: bind the module arrays (host)
  * once, then call anel_rk_substep with the reference's rk_ss arguments;
  * every call copies the bound fields to the device and back. */

@@ -5,6 +5,7 @@ import re
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 from anelastic_solve_b200 import _lib, abi
 from anelastic_solve_b200 import grid as G
@@ -70,3 +71,27 @@ def test_tanh_grid_shape():
     assert dz.argmin() in (0, 63)
     np.testing.assert_allclose(dz, dz[::-1], rtol=1e-12)
     np.testing.assert_allclose(ax.xc[1:-1], 0.5 * (ax.xe[1:-1] + ax.xe[:-2]), rtol=0, atol=1e-14)
+
+
+def test_struct_sizes_match_the_c_header(tmp_path):
+    """ctypes mirrors of every struct have the C compiler's size."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    names = {"anel_grid_desc": abi.GridDesc, "anel_mg_params": abi.MGParams,
+             "anel_mg_report": abi.MGReport, "anel_ns_params": abi.NSParams,
+             "anel_fields": abi.Fields, "anel_step_report": abi.StepReport,
+             "anel_request": abi.Request, "anel_result": abi.Result,
+             "anel_serve_stats": abi.ServeStats}
+    src = tmp_path / "sz.c"
+    src.write_text('#include <stdio.h>\n#include "anel.h"\nint main(void){\n' +
+                   "".join(f'printf("%zu\\n", sizeof({n}));\n' for n in names) + "return 0;}\n")
+    exe = tmp_path / "sz"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
+                                            check=True).stdout.split()]
+    for (n, cls), got in zip(names.items(), sizes):
+        assert C.sizeof(cls) == got, (n, C.sizeof(cls), got)
