@@ -28,8 +28,14 @@ const char* last_error();
 
 // Every kernel launch of this library goes through count_launch() so the
 // total is observable through anel_kernel_launch_count().
+// The thread-local count gives per-call reports (solve, step) that are
+// right when several host threads drive contexts at once.
 extern std::atomic<int64_t> g_launches;
-inline void count_launch(int64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+extern thread_local int64_t t_launches;
+inline void count_launch(int64_t n = 1) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  t_launches += n;
+}
 int check_launch(const char* what);
 // Raise a kernel's dynamic shared-memory limit once per (device, kernel);
 // safe to call from several host threads.

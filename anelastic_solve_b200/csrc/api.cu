@@ -10,6 +10,7 @@
 namespace anel {
 
 std::atomic<int64_t> g_launches{0};
+thread_local int64_t t_launches = 0;
 static thread_local char t_err[1024] = "";
 
 void set_error(const char* fmt, ...) {

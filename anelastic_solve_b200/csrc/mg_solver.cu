@@ -230,6 +230,7 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
 
 MGSolver::~MGSolver() {
   if (device_ >= 0) cudaSetDevice(device_);
+  if (g32x_) cudaGraphExecDestroy(g32x_);
   for (int l = 0; l <= ANEL_MAX_LEVELS; ++l) {
     cudaFree(d_phi64_[l]);
     cudaFree(d_src64_[l]);
@@ -991,7 +992,7 @@ int MGSolver::solve_device(double* d_phi, const double* d_rhs, cudaStream_t s,
   ANEL_CUDA_TRY(cudaSetDevice(device_));
   if (!s) s = stream_;
   anel_mg_report r{};
-  const int64_t launches0 = g_launches.load();
+  const int64_t launches0 = t_launches;
   prof_n_ = 0;
   ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
   const int st = prm_.precision == ANEL_PREC_MIXED ? solve_mixed(d_phi, d_rhs, s, &r)
@@ -1004,7 +1005,7 @@ int MGSolver::solve_device(double* d_phi, const double* d_rhs, cudaStream_t s,
   if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
   const int le = check_launch("mg solve");
   if (le != ANEL_OK) return le;
-  r.launches = g_launches.load() - launches0;
+  r.launches = t_launches - launches0;
   const int pe = prof_collect(&r);
   if (pe != ANEL_OK) return pe;
   r.resid = true_resid(d_phi, d_rhs, s, nullptr);
@@ -1072,6 +1073,49 @@ int MGSolver::solve_fp64(double* d_phi, const double* d_rhs, cudaStream_t s,
 // iteration.  FP64: fine residual, correction update, norms, boundary
 // pass of the solution.  FP32: smoothing, restriction, prolongation and
 // every coarse level, on the error equation (homogeneous wall values).
+// The FP32 cycle is ~100-200 small launches whose arguments never change
+// for a solver, so from the second call on it is captured once (thread-
+// local capture mode: other host threads driving other contexts are not
+// affected) and replayed as one graph launch.  The same kernels run in the
+// same order, so results are unchanged.  Profiling runs (events between
+// sweeps) and the legacy default stream stay uncaptured.
+void MGSolver::run_cycle32(cudaStream_t s) {
+  const DevLevel<float> E = L32(ngrid_, true);
+  const bool can = !prof_ && !g32_off_ && s != nullptr && s != cudaStreamLegacy &&
+                   s != cudaStreamPerThread;
+  if (!can || (++g32_calls_ < 2 && !g32x_)) {
+    cudaMemsetAsync(E.phi, 0, E.G * sizeof(float), s);
+    cycle32(s);
+    return;
+  }
+  if (!g32x_) {
+    const int64_t l0 = t_launches;
+    bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      cudaMemsetAsync(E.phi, 0, E.G * sizeof(float), s);
+      cycle32(s);
+      cudaGraph_t g = nullptr;
+      ok = cudaStreamEndCapture(s, &g) == cudaSuccess && g;
+      const int64_t n = t_launches - l0;  // counted while capturing, not run
+      g_launches.fetch_sub(n, std::memory_order_relaxed);
+      t_launches -= n;
+      g32_launches_ = n;
+      if (ok) ok = cudaGraphInstantiate(&g32x_, g, 0) == cudaSuccess;
+      if (g) cudaGraphDestroy(g);
+    }
+    if (!ok) {
+      cudaGetLastError();
+      g32x_ = nullptr;
+      g32_off_ = true;
+      cudaMemsetAsync(E.phi, 0, E.G * sizeof(float), s);
+      cycle32(s);
+      return;
+    }
+  }
+  cudaGraphLaunch(g32x_, s);
+  count_launch(g32_launches_);
+}
+
 int MGSolver::solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s,
                           anel_mg_report* rep) {
   const int ng = ngrid_;
@@ -1092,8 +1136,7 @@ int MGSolver::solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s,
       break;
     }
     if (iter == prm_.maxcy) break;
-    ANEL_CUDA_TRY(cudaMemsetAsync(E.phi, 0, E.G * sizeof(float), s));
-    cycle32(s);
+    run_cycle32(s);
     launch_add_correction(Fu, d_phi, E.phi, s);
     launch_bdry(Fu, d_phi, s);
   }

@@ -49,6 +49,13 @@ class MGSolver {
   void cycle64(cudaStream_t s);
   void relax32(int l, int iters, cudaStream_t s);
   void cycle32(cudaStream_t s);
+  // correction reset + FP32 V-cycle, replayed from a CUDA graph after the
+  // first call (kernel pointers are fixed per solver)
+  void run_cycle32(cudaStream_t s);
+  cudaGraphExec_t g32x_ = nullptr;
+  int64_t g32_launches_ = 0;
+  int g32_calls_ = 0;
+  bool g32_off_ = false;
   int solve_fp64(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
   int solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
   int coarsen_dirs(int lC) const;

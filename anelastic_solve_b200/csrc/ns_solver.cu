@@ -583,7 +583,7 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   anel_step_report r{};
   acc_mg_ms_ = acc_sweep_ms_ = 0.0;
   acc_sweeps_ = 0;
-  const int64_t launches0 = g_launches.load();
+  const int64_t launches0 = t_launches;
   ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
   for (int n = 0; n < nsteps; ++n) {
     // zero_temps (memManage.F90:844-853)
@@ -623,7 +623,7 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   r.mg_ms = acc_mg_ms_;
   r.fine_sweep_ms = acc_sweep_ms_;
   r.fine_sweeps = acc_sweeps_;
-  r.launches = g_launches.load() - launches0;
+  r.launches = t_launches - launches0;
   double dv[2];
   const int st = divergence(s, dv);
   if (st != ANEL_OK) return st;
@@ -636,6 +636,11 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
 int NSSolver::project(cudaStream_t s, int* iters, double* relmax) {
   ANEL_CUDA_TRY(cudaSetDevice(device_));
   if (!s) s = stream_;
+  // the velocity ghosts first: with the wall values in place the boundary
+  // flux of Psource vanishes and the Neumann problem is compatible
+  launch_ghost_field(D_, D_.u, zrule(NV_U), s);
+  launch_ghost_field(D_, D_.v, zrule(NV_V), s);
+  launch_ghost_field(D_, D_.w, zrule(NV_W), s);
   launch_psource(D_, 1.0, s);
   anel_mg_report rep{};
   const int st = mg_->solve_device(D_.p, D_.psrc, s, &rep);

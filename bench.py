@@ -54,6 +54,10 @@ WORKLOADS = {
     # eddy diffusivity with Pr_sgs = 0.7
     "les": ("dns", (768, 384, 384), (9, 8, 8), dict(Re=50000.0, g=-0.1, amp=1e-2, cfl=0.5, les=True)),
     "les_small": ("dns", (96, 48, 48), (6, 5, 5), dict(Re=50000.0, g=-0.1, amp=1e-2, cfl=0.5, les=True)),
+    # one member of the serving stream, for the CPU baseline of "serve"
+    "dns64": ("dns", (64, 64, 64), (6, 6, 6), dict(Re=1000.0, g=-0.12, amp=1e-3, cfl=0.5)),
+    # ensemble serving: a Poisson stream of shear-layer members (sizes below)
+    "serve": ("serve", (256, 256, 256), None, {}),
     "poisson": ("poisson", (512, 256, 512), (9, 8, 9), {}),
     "poisson256": ("poisson", (256, 256, 256), (8, 8, 8), {}),
     "poisson_small": ("poisson", (64, 32, 64), (6, 5, 6), {}),
@@ -207,7 +211,6 @@ def run_dns(args, rank, world, local_rank):
     for _ in range(args.warmup):
         s.step(1, stream=h)
     torch.cuda.synchronize()
-    s.set_profiling(True)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = []
     barrier()
@@ -221,12 +224,16 @@ def run_dns(args, rank, world, local_rank):
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
     barrier()
-    s.set_profiling(False)
     ms_step = ev0.elapsed_time(ev1) / args.steps
+    # one more step with the smoother launches timed by events (profiling
+    # runs the V-cycles launch by launch), for the roofline of the smoother
+    s.set_profiling(True)
+    prep = s.step(1, stream=h)
+    s.set_profiling(False)
     out = {"N": N, "ms_step": ms_step, "clocks": clk.summary(),
            "launches": int(sum(r.launches for r in reps)),
-           "sweeps": int(sum(r.fine_sweeps for r in reps)),
-           "sweep_ms": float(sum(r.fine_sweep_ms for r in reps)),
+           "sweeps": int(prep.fine_sweeps),
+           "sweep_ms": float(prep.fine_sweep_ms),
            "mg_ms_step": float(np.mean([r.mg_ms for r in reps])),
            "mg_iters": [list(r.mg_iter) for r in reps],
            "dt": reps[-1].dt, "max_div": reps[-1].max_div,
@@ -303,9 +310,8 @@ def run_poisson(args, rank, world, local_rank):
             dphi.zero_()
         s.solve(dphi, dsrc, stream=st.cuda_stream)
     st.synchronize()
-    s.set_profiling(True)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    iters, sweep_ms, sweeps = [], 0.0, 0
+    iters = []
     launches0 = _lib.launch_count()
     torch.cuda.synchronize()
     with ClockSampler(local_rank) as clk:
@@ -316,14 +322,20 @@ def run_poisson(args, rank, world, local_rank):
                 dphi.zero_()
             s.solve(dphi, dsrc, stream=st.cuda_stream)
             iters.append(s.last_report.iter)
-            sweep_ms += s.last_report.fine_sweep_ms
-            sweeps += s.last_report.fine_sweeps
         ev1.record(st)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
+    launches = _lib.launch_count() - launches0
+    # one more solve with the smoother launches timed by events, for the
+    # roofline of the smoother
+    s.set_profiling(True)
+    with torch.cuda.stream(st):
+        dphi.zero_()
+    s.solve(dphi, dsrc, stream=st.cuda_stream)
+    sweep_ms, sweeps = s.last_report.fine_sweep_ms, s.last_report.fine_sweeps
     s.set_profiling(False)
     out = {"N": N, "ms_step": ev0.elapsed_time(ev1) / args.steps, "clocks": clk.summary(),
-           "launches": _lib.launch_count() - launches0, "sweeps": sweeps, "sweep_ms": sweep_ms,
+           "launches": launches, "sweeps": sweeps, "sweep_ms": sweep_ms,
            "iters": iters, "resid": s.last_report.resid}
     if not args.no_e2e:
         ph = np.asfortranarray(torch.zeros(dsrc.shape, dtype=torch.float64).pin_memory().numpy().T)
@@ -395,6 +407,171 @@ def cpu_sample_poisson(workload, threads):
     return time.perf_counter() - t, g.x.n * g.y.n * g.z.n
 
 
+# ------------------------------------------------------------ ours: serve
+SERVE_SIZES = [(32, 32, 32), (64, 64, 64), (96, 48, 96), (128, 128, 128), (192, 96, 192),
+               (256, 256, 256)]
+
+
+def levels_of(n):
+    """Level count per direction: halve while the coarse size stays >= 2."""
+    L = 1
+    while n % 2 == 0 and n // 2 >= 2:
+        n //= 2
+        L += 1
+    return L
+
+
+def serve_stream(n_req, seed, rate):
+    """Seeded request stream: Poisson arrivals at `rate`/s, grid uniform
+    over SERVE_SIZES, Ri ~ U[0.05, 0.3], Re log-uniform on [500, 4000], a
+    perturbation seed per request."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    size = rng.integers(0, len(SERVE_SIZES), n_req)
+    Ri = rng.uniform(0.05, 0.3, n_req)
+    Re = np.exp(rng.uniform(math.log(500.0), math.log(4000.0), n_req))
+    sd = rng.integers(1, 2 ** 31 - 1, n_req)
+    return [dict(t=float(t[q]), size=SERVE_SIZES[int(size[q])], Ri=float(Ri[q]), Re=float(Re[q]),
+                 seed=int(sd[q])) for q in range(n_req)]
+
+
+def run_serve(args, rank, world, local_rank):
+    import torch
+
+    from anelastic_solve_b200 import _lib, abi
+    from anelastic_solve_b200 import grid as G
+    from anelastic_solve_b200.serve import ServeEngine
+
+    torch.cuda.set_device(local_rank)
+    grids = {n: G.shear_layer_grid(*n, stretched=True) for n in SERVE_SIZES}
+    mgp = {}
+    for n in SERVE_SIZES:
+        SMOOTHER.update(smoother=args.smoother, pre=args.pre, post=args.post)
+        mgp[n] = mg_params(tuple(levels_of(v) for v in n),
+                           abi.PREC_MIXED if args.prec == "mixed" else abi.PREC_FP64)
+
+    def nsp(Re, Ri):
+        return abi.make_ns_params(Re=Re, Pr=1.0, g=-Ri, cfl=0.5, dtmax=1e9, ew=1, scal1_on=0)
+
+    e = ServeEngine(int(args.budget_gb * 1e9), max_active=args.workers, device=local_rank)
+    # warm-up: one member of every size (contexts of every bucket created)
+    for n in SERVE_SIZES:
+        e.submit(grids[n], mgp[n], nsp(1000.0, 0.12), nsteps=1, seed=1)
+    e.drain()
+    e.poll(cap=1024)
+    reqs = serve_stream(args.requests, 7 + rank, args.rate)
+    res = []
+    launches0 = _lib.launch_count()
+    with ClockSampler(local_rank) as clk:
+        t0 = time.perf_counter()
+        for r in reqs:
+            while True:
+                now = time.perf_counter() - t0
+                if now >= r["t"]:
+                    break
+                res += e.poll(wait_ms=max(1, int(1000 * (r["t"] - now))))
+            e.submit(grids[r["size"]], mgp[r["size"]], nsp(r["Re"], r["Ri"]), nsteps=args.serve_steps,
+                     seed=r["seed"], amp=1e-3)
+        e.drain()
+        t1 = time.perf_counter()
+        while len(res) < len(reqs):
+            res += e.poll(wait_ms=100, cap=1024)
+    st = e.stats()
+    e.close()
+    ok = [x for x in res if x["status"] == abi.OK]
+    lat = np.array([x["latency_ms"] for x in ok])
+    cu = float(sum(x["cells"] * x["nsteps"] for x in ok))
+    meta = np.array([sum(n[0] * n[1] * n[2] for n in [r["size"]]) for r in reqs])
+    out = {"makespan_s": t1 - t0, "cell_updates": cu, "ok": len(ok), "failed": len(res) - len(ok),
+           "lat": lat, "queue": np.array([x["queue_ms"] for x in ok]),
+           "run": np.array([x["run_ms"] for x in ok]), "stats": st, "clocks": clk.summary(),
+           "launches": _lib.launch_count() - launches0,
+           "h2d": int(sum(8 * 6 * (2 * (r["size"][0] + r["size"][1] + r["size"][2]) + 6) for r in reqs)),
+           "d2h": 8 * 8 * len(reqs), "arrival_span_s": reqs[-1]["t"], "mean_cells": float(meta.mean())}
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([out["makespan_s"], out["cell_updates"]], device=torch.device("cuda", local_rank),
+                         dtype=torch.float64)
+        mk = t.clone()
+        dist.all_reduce(mk, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        out["makespan_s"], out["cell_updates"] = float(mk[0]), float(t[1])
+    return out
+
+
+def main_serve(args, rank, world, local_rank, threads):
+    sizes = "{" + ", ".join("x".join(map(str, n)) for n in SERVE_SIZES) + "}"
+    metric = "cell-updates/s (ensemble serving, aggregate)"
+    unit = "cell-updates/s"
+    config = {"workload": f"serving stream: {args.requests} shear-layer requests, Poisson arrivals at "
+                          f"{args.rate:g}/s, grid uniform over {sizes}, Ri~U[0.05,0.3], Re "
+                          f"log-uniform [500,4000], {args.serve_steps} RK3 steps each",
+              "hbm_budget_gb": args.budget_gb, "workers": args.workers,
+              "mg": f"{args.smoother.upper()} V({args.pre},{args.post}), metric, {args.prec}, to 1e-10",
+              "parallelism": f"replicas x{world}", "l2": "mixed sizes (32^3 .. 256^3)"}
+    if args.impl == "reference" or not args.no_cpu:
+        SMOOTHER.update(smoother="rbpgs", pre=2, post=2)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        t, it, N = cpu_sample_dns("dns64", threads)
+        value = N / (3.0 * t)
+        sample = (f"one 64^3 member: first FP64 RK3 sub-step after projection, oracle restatement "
+                  f"({t:.2f} s, {it} MG V-cycles), x3 per step; members run one after another")
+        line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": 0,
+                "steps": args.requests, "warmup": args.warmup, "ms_per_step": 3 * t * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": dict(config, mg="RBPGS V(2,2), metric, fp64 (host)"),
+                "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    r = run_serve(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    value = r["cell_updates"] / r["makespan_s"]
+    pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None  # noqa: E731
+    cpu = None
+    if not args.no_cpu:
+        t, it, N = cpu_sample_dns("dns64", threads)
+        cpu = {"value": N / (3.0 * t), "unit": unit, "cores": threads, "kind": "port",
+               "sample": f"one 64^3 member: first FP64 RK3 sub-step after projection, oracle "
+                         f"restatement ({t:.2f} s, {it} MG V-cycles), x3 per step"}
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.requests,
+            "warmup": len(SERVE_SIZES), "ms_per_step": 1e3 * r["makespan_s"] / max(1, args.requests),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (MG f32-in-f64)" if args.prec == "mixed" else "f64", "data": "synthetic",
+            "config": config,
+            "latency_ms": {"p50": pct(r["lat"], 50), "p99": pct(r["lat"], 99),
+                           "queue_p50": pct(r["queue"], 50), "queue_p99": pct(r["queue"], 99),
+                           "run_p50": pct(r["run"], 50), "run_p99": pct(r["run"], 99)},
+            "requests_ok": r["ok"], "requests_failed": r["failed"],
+            "makespan_s": r["makespan_s"], "arrival_span_s": r["arrival_span_s"],
+            "peak_active": r["stats"]["peak_active"], "peak_bytes": r["stats"]["peak_bytes"],
+            "contexts": r["stats"]["contexts"],
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": r["h2d"] // max(1, args.requests),
+                    "d2h_bytes_per_step": r["d2h"] // max(1, args.requests),
+                    "note": "serving is timed end to end on the host clock: submit through the "
+                            "C-ABI (grid copied in, state generated on the device from the seed) "
+                            "to the member's result record"},
+            "roofline": None, "cpu_baseline": cpu, "clocks": r["clocks"],
+            "gpu_launches": r["launches"]}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -411,11 +588,19 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 multigrid companion")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the stream")
+    ap.add_argument("--rate", type=float, default=50.0, help="serve: arrivals per second")
+    ap.add_argument("--serve-steps", type=int, default=10, help="serve: RK3 steps per request")
+    ap.add_argument("--workers", type=int, default=8, help="serve: members in flight")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM budget (GB)")
     args = ap.parse_args()
     SMOOTHER.update(smoother=args.smoother, pre=args.pre, post=args.post)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if WORKLOADS[args.workload][0] == "serve":
+        main_serve(args, rank, world, local_rank, os.cpu_count() or 1)
+        return
     kind, n, lv, phys = WORKLOADS[args.workload]
     nx, ny, nz = n
     field_mb = (nx + 2) * (ny + 2) * (nz + 2) * 8 / 1e6

@@ -275,8 +275,9 @@ int anel_ns_ctx_set_profiling(anel_ns_ctx* ctx, int32_t on);
 /* time and step counter (time, nstep of the Parameters module) */
 int anel_ns_ctx_set_clock(anel_ns_ctx* ctx, double time, int32_t nstep);
 /* Projection of the current velocity onto divergence-free fields (used to
- * prepare initial conditions): Psource with dt = 1, one MG solve starting
- * from p, Pgrad with dt = 1 and the velocity ghost passes. */
+ * prepare initial conditions): the velocity ghost passes, Psource with
+ * dt = 1, one MG solve starting from p, Pgrad with dt = 1 and the velocity
+ * ghost passes. */
 int anel_ns_ctx_project(anel_ns_ctx* ctx, int32_t* mg_iter, double* mg_relmax);
 /* divergence() (Routines.F90:54-183) of the current velocity:
  * out[0] = volume-weighted mean |div|, out[1] = max |div|. */

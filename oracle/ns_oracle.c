@@ -1118,11 +1118,16 @@ int orc_ns_step(orc_ns* s, anel_step_report* rep) {
 }
 
 /* Projection of the initial field (not a reference routine: the
- * shear-layer benchmark starts from a divergence-free field): Psource
- * with dt = 1, one MG solve from p, Pgrad with dt = 1, velocity ghosts. */
+ * shear-layer benchmark starts from a divergence-free field): velocity
+ * ghosts, Psource with dt = 1, one MG solve from p, Pgrad with dt = 1,
+ * velocity ghosts. */
 int orc_ns_project(orc_ns* s, int* iters, double* relmax) {
   const orc_dom* D = &s->d;
   anel_fields* f = &s->f;
+  /* velocity ghosts first, so the wall flux of Psource vanishes */
+  ghost(s, f->u, VT_U);
+  ghost(s, f->v, VT_V);
+  ghost(s, f->w, VT_W);
   memset(f->psrc, 0, sizeof(double) * D->G);
   psource(s, f->psrc, 1.0);
   memcpy(s->Ftemp, f->p, sizeof(double) * D->G);
