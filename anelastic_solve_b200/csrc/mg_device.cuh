@@ -287,7 +287,10 @@ struct ZFac {
   const T* bp;  // eliminated diagonal
 };
 
-template <typename T>
+// kLJ: the reference's mg_relaxLz boundary rows (mg_relax.F90:507-518):
+// the ghost term sits inside the neighbour sum, and with one row only the
+// top row's form is kept.
+template <typename T, bool kLJ>
 __global__ void k_zline(DevLevel<T> L, int color, ZFac<T> F) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;  // pair index
   const int j = 2 + blockIdx.y;
@@ -315,9 +318,16 @@ __global__ void k_zline(DevLevel<T> L, int color, ZFac<T> F) {
       const int k = kb + u;
       if (k <= nz + 1) {
         const int64_t c = c0 + (int64_t)(k - 1) * XY;
-        r[u] = src[c] - (a1 * phi[c - 1] + a2 * phi[c + 1] + a3 * phi[c - X] + a4 * phi[c + X]);
-        if (k == 2) r[u] = r[u] - cz5[1] * phi[c - XY];
-        if (k == nz + 1) r[u] = r[u] - cz6[nz] * phi[c + XY];
+        if (kLJ) {
+          T sum = a1 * phi[c - 1] + a2 * phi[c + 1] + a3 * phi[c - X] + a4 * phi[c + X];
+          if (k == nz + 1) sum = sum + cz6[nz] * phi[c + XY];
+          else if (k == 2) sum = sum + cz5[1] * phi[c - XY];
+          r[u] = src[c] - sum;
+        } else {
+          r[u] = src[c] - (a1 * phi[c - 1] + a2 * phi[c + 1] + a3 * phi[c - X] + a4 * phi[c + X]);
+          if (k == 2) r[u] = r[u] - cz5[1] * phi[c - XY];
+          if (k == nz + 1) r[u] = r[u] - cz6[nz] * phi[c + XY];
+        }
       }
     }
 #pragma unroll

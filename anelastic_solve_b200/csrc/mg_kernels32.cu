@@ -9,6 +9,7 @@ namespace anel {
 template void launch_bdry<float>(const DevLevel<float>&, float*, cudaStream_t);
 template void launch_rb_sweep<float>(const DevLevel<float>&, int, cudaStream_t);
 template void launch_zline<float>(const DevLevel<float>&, int, const float*, const float*, cudaStream_t);
+template void launch_zline_lj<float>(const DevLevel<float>&, int, const float*, const float*, cudaStream_t);
 template void launch_zline_seg<float>(const DevLevel<float>&, int, const SegFac<float>&, cudaStream_t);
 
 void launch_ghost_table(const DevLevel<float>& L, int2* tab, cudaStream_t s) {

@@ -9,6 +9,7 @@ namespace anel {
 template void launch_bdry<double>(const DevLevel<double>&, double*, cudaStream_t);
 template void launch_rb_sweep<double>(const DevLevel<double>&, int, cudaStream_t);
 template void launch_zline<double>(const DevLevel<double>&, int, const double*, const double*, cudaStream_t);
+template void launch_zline_lj<double>(const DevLevel<double>&, int, const double*, const double*, cudaStream_t);
 template void launch_restrict<double>(const DevLevel<double>&, const DevLevel<double>&, int,
                                       cudaStream_t);
 template void launch_prolong<double>(const DevLevel<double>&, const DevLevel<double>&, int,

@@ -21,6 +21,9 @@ template <typename T>
 void launch_rb_sweep(const DevLevel<T>& L, int color, cudaStream_t s);
 template <typename T>
 void launch_zline(const DevLevel<T>& L, int color, const T* ap, const T* bp, cudaStream_t s);
+// LJ z-line sweep (L.coef = the pcf line coefficients)
+template <typename T>
+void launch_zline_lj(const DevLevel<T>& L, int color, const T* ap, const T* bp, cudaStream_t s);
 // partitioned FP32 z-line solver: kZSeg segments per line, each of
 // 2..kZSegRows rows (lines of nz = kZSeg * m rows)
 constexpr int kZSeg = 16;

@@ -35,7 +35,15 @@ void launch_zline(const DevLevel<T>& L, int color, const T* ap, const T* bp, cud
   }
   const int tx = 64;
   dim3 grid((unsigned)((pairs + tx - 1) / tx), (unsigned)L.ny, 1u);
-  k_zline<T><<<grid, tx, 0, s>>>(L, color, ZFac<T>{ap, bp});
+  k_zline<T, false><<<grid, tx, 0, s>>>(L, color, ZFac<T>{ap, bp});
+  count_launch();
+}
+template <typename T>
+void launch_zline_lj(const DevLevel<T>& L, int color, const T* ap, const T* bp, cudaStream_t s) {
+  const int pairs = (L.nx + 1) / 2;
+  const int tx = 64;
+  dim3 grid((unsigned)((pairs + tx - 1) / tx), (unsigned)L.ny, 1u);
+  k_zline<T, true><<<grid, tx, 0, s>>>(L, color, ZFac<T>{ap, bp});
   count_launch();
 }
 template <typename T>

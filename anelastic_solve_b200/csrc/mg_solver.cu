@@ -52,10 +52,6 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
     set_error("unknown smoother %d", p->smoother);
     return ANEL_ERR_ARG;
   }
-  if (p->smoother == ANEL_SMOOTHER_LJ) {
-    set_error("the reference's LJ z-line smoother is not available in this build (use ZLINE)");
-    return ANEL_ERR_UNSUPPORTED;
-  }
   if (p->mode != ANEL_MODE_LITERAL && p->mode != ANEL_MODE_METRIC) {
     set_error("unknown mode %d", p->mode);
     return ANEL_ERR_ARG;
@@ -153,6 +149,7 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
     for (int l = ngrid_ - 1; l >= 1; --l) phibc_[l][f] = 0.0;
   }
   build_metric_hierarchy();
+  if (p->smoother == ANEL_SMOOTHER_LJ) build_lj_coefficients();
   build_agglomerated();
   // boundary rules; spacings indexed without the level offset, exactly as
   // mg_bdry.F90:106-181 (dyck(eym) etc.)
@@ -187,6 +184,12 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
       ANEL_CUDA_TRY(cudaMemset(d_src64_[l], 0, G * sizeof(double)));
     }
     ANEL_CUDA_TRY(cudaMalloc(&d_coef64_[l], ncoef * sizeof(double)));
+    if (p->smoother == ANEL_SMOOTHER_LJ) {
+      ANEL_CUDA_TRY(cudaMalloc(&d_zf64_[l], 2 * (size_t)geo_[l].Z * sizeof(double)));
+      ANEL_CUDA_TRY(cudaMalloc(&d_zf32_[l], 2 * (size_t)geo_[l].Z * sizeof(float)));
+      ANEL_CUDA_TRY(cudaMalloc(&d_ljc64_[l], ncoef * sizeof(double)));
+      if (mixed) ANEL_CUDA_TRY(cudaMalloc(&d_ljc32_[l], ncoef * sizeof(float)));
+    }
     if (p->smoother == ANEL_SMOOTHER_ZLINE) {
       ANEL_CUDA_TRY(cudaMalloc(&d_zf64_[l], 2 * (size_t)geo_[l].Z * sizeof(double)));
       ANEL_CUDA_TRY(cudaMalloc(&d_zf32_[l], 2 * (size_t)geo_[l].Z * sizeof(float)));
@@ -239,6 +242,8 @@ MGSolver::~MGSolver() {
     cudaFree(d_src32_[l]);
     cudaFree(d_coef32_[l]);
     cudaFree(d_zf64_[l]);
+    cudaFree(d_ljc64_[l]);
+    cudaFree(d_ljc32_[l]);
     cudaFree(d_zf32_[l]);
     cudaFree(d_zseg32_[l]);
     cudaFree(d_gtab32_[l]);
@@ -514,18 +519,56 @@ int MGSolver::build_coefficients(const std::vector<double>& rz) {
 // with c7 = -(c1+c2+c3+c4+d5+d6).  With x/y-uniform coefficients every
 // column has the same system, so the Thomas elimination (mg_relax.F90:
 // 563-566) is done once per level here; the kernel runs the substitution.
-int MGSolver::build_zline_factors() {
+// LJ (mg_relaxLz, mg_relax.F90:423-538) solves its lines with the 1-D
+// coefficients pcf_1..6 of mg_coeff.F90:77-145 (not the level operator):
+// x: pcf_1, pcf_2; y: pcf_3, pcf_4; z: sub pcf_5, super pcf_6 and diagonal
+// -(pcf_1+pcf_2+pcf_3+pcf_4+pcf_5+pcf_6).  Kept in the level-coefficient
+// layout (dz5 = cz5 = pcf_5, dz6 = cz6 = pcf_6) so the z-line kernel reads
+// them in place of the operator; the finest level's Neumann faces are
+// zeroed as mg_coeff.F90:123-145 does.
+void MGSolver::build_lj_coefficients() {
   for (int l = 1; l <= ngrid_; ++l) {
     const LevelGeom& G = geo_[l];
-    const LevelCoef& c = coef_[l];
+    LevelCoef& c = ljc_[l];
+    const int dims[3] = {G.X, G.Y, G.Z};
+    std::vector<double>* A[3] = {&c.cx1, &c.cy3, &c.cz5};
+    std::vector<double>* B[3] = {&c.cx2, &c.cy4, &c.cz6};
+    for (int d = 0; d < 3; ++d) {
+      A[d]->assign(dims[d], 0.0);
+      B[d]->assign(dims[d], 0.0);
+      const int s0 = G.kpx[d];
+      for (int q = 2; q <= G.nk[d]; ++q) {
+        (*A[d])[q - 1] = pA_[d][s0 + q - 1];
+        (*B[d])[q - 1] = pB_[d][s0 + q - 1];
+      }
+    }
+    if (l == ngrid_) {
+      const int* t = prm_.tbc;
+      if (t[4] == 1) c.cx1[1] = 0.0;
+      if (t[5] == 1) c.cx2[G.nk[0] - 1] = 0.0;
+      if (t[2] == 1) c.cy3[1] = 0.0;
+      if (t[0] == 1) c.cy4[G.nk[1] - 1] = 0.0;
+      if (t[1] == 1) c.cz5[1] = 0.0;
+      if (t[3] == 1) c.cz6[G.nk[2] - 1] = 0.0;
+    }
+    c.dz5 = c.cz5;
+    c.dz6 = c.cz6;
+  }
+}
+
+int MGSolver::build_zline_factors() {
+  const bool lj = prm_.smoother == ANEL_SMOOTHER_LJ;
+  for (int l = 1; l <= ngrid_; ++l) {
+    const LevelGeom& G = geo_[l];
+    const LevelCoef& c = lj ? ljc_[l] : coef_[l];
     for (int i = G.s[0]; i <= G.e[0]; ++i)
       if (!(c.cx1[i - 1] == c.cx1[G.s[0] - 1] && c.cx2[i - 1] == c.cx2[G.s[0] - 1])) {
-        set_error("ZLINE needs x-uniform level coefficients (level %d)", l);
+        set_error("the z-line smoothers need x-uniform line coefficients (level %d)", l);
         return ANEL_ERR_UNSUPPORTED;
       }
     for (int j = G.s[1]; j <= G.e[1]; ++j)
       if (!(c.cy3[j - 1] == c.cy3[G.s[1] - 1] && c.cy4[j - 1] == c.cy4[G.s[1] - 1])) {
-        set_error("ZLINE needs y-uniform level coefficients (level %d)", l);
+        set_error("the z-line smoothers need y-uniform line coefficients (level %d)", l);
         return ANEL_ERR_UNSUPPORTED;
       }
     const double a1 = c.cx1[G.s[0] - 1], a2 = c.cx2[G.s[0] - 1];
@@ -682,10 +725,25 @@ int zline_segment_factors(int n, int P, const std::vector<double>& sub, const st
 
 int MGSolver::upload_coefficients() {
   ANEL_CUDA_TRY(cudaSetDevice(device_));
-  if (prm_.smoother == ANEL_SMOOTHER_ZLINE) {
+  if (prm_.smoother == ANEL_SMOOTHER_ZLINE || prm_.smoother == ANEL_SMOOTHER_LJ) {
     const int st = build_zline_factors();
     if (st != ANEL_OK) return st;
   }
+  if (prm_.smoother == ANEL_SMOOTHER_LJ)
+    for (int l = 1; l <= ngrid_; ++l) {
+      const LevelCoef& c = ljc_[l];
+      std::vector<double> packed;
+      for (const std::vector<double>* v :
+           {&c.cx1, &c.cx2, &c.cy3, &c.cy4, &c.cz5, &c.cz6, &c.dz5, &c.dz6})
+        packed.insert(packed.end(), v->begin(), v->end());
+      ANEL_CUDA_TRY(cudaMemcpy(d_ljc64_[l], packed.data(), packed.size() * sizeof(double),
+                               cudaMemcpyHostToDevice));
+      if (d_ljc32_[l]) {
+        std::vector<float> p32(packed.begin(), packed.end());
+        ANEL_CUDA_TRY(cudaMemcpy(d_ljc32_[l], p32.data(), p32.size() * sizeof(float),
+                                 cudaMemcpyHostToDevice));
+      }
+    }
   for (int l = 1; l <= ngrid_; ++l) {
     const LevelCoef& c = coef_[l];
     std::vector<double> packed;
@@ -802,11 +860,15 @@ void MGSolver::relax64(int l, int iters, cudaStream_t s) {
   const DevLevel<double> L = L64(l);
   const bool prof = prof_ && l == ngrid_;
   const bool zl = prm_.smoother == ANEL_SMOOTHER_ZLINE;
+  const bool lj = prm_.smoother == ANEL_SMOOTHER_LJ;
   const double* zf = d_zf64_[l];
+  DevLevel<double> Lj = L;  // LJ lines use the pcf coefficients
+  if (lj) Lj.coef = d_ljc64_[l];
   for (int it = 0; it < iters; ++it) {
     for (int color = 0; color < 2; ++color) {
       if (prof) prof_begin(s);
       if (zl) launch_zline(L, color, zf, zf + geo_[l].Z, s);
+      else if (lj) launch_zline_lj(Lj, color, zf, zf + geo_[l].Z, s);
       else launch_rb_sweep(L, color, s);
       if (prof) prof_end(s);
       launch_bdry(L, L.phi, s);
@@ -840,14 +902,18 @@ void MGSolver::relax32(int l, int iters, cudaStream_t s) {
   const DevLevel<float> L = L32(l, true);
   const bool prof = prof_ && l == ngrid_;
   const bool zl = prm_.smoother == ANEL_SMOOTHER_ZLINE;
+  const bool lj = prm_.smoother == ANEL_SMOOTHER_LJ;
   const float* zf = d_zf32_[l];
   const float* zs = d_zseg32_[l];
   const SegFac<float> sf = segfac32(l);
+  DevLevel<float> Lj = L;
+  if (lj) Lj.coef = d_ljc32_[l];
   for (int it = 0; it < iters; ++it) {
     for (int color = 0; color < 2; ++color) {
       if (prof) prof_begin(s);
       if (zl && zs) launch_zline_seg(L, color, sf, s);
       else if (zl) launch_zline(L, color, zf, zf + geo_[l].Z, s);
+      else if (lj) launch_zline_lj(Lj, color, zf, zf + geo_[l].Z, s);
       else launch_rb_sweep(L, color, s);
       if (prof) prof_end(s);
       if (!(zl && zs && sf.img)) launch_bdry(L, L.phi, s);

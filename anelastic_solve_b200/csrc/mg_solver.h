@@ -78,6 +78,10 @@ class MGSolver {
   std::vector<double> ag_[ANEL_MAX_LEVELS + 1][3][4];
   void build_agglomerated();
   LevelCoef coef_[ANEL_MAX_LEVELS + 1];
+  LevelCoef ljc_[ANEL_MAX_LEVELS + 1];  // LJ line coefficients (pcf_1..6)
+  void build_lj_coefficients();
+  double* d_ljc64_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  float* d_ljc32_[ANEL_MAX_LEVELS + 1] = {nullptr};
   BdryRule rule_[ANEL_MAX_LEVELS + 1];
   BdryRule rule_hom_[ANEL_MAX_LEVELS + 1];  // same with phibc = 0 (error equation)
   bool coef_ready_ = false;

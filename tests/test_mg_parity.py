@@ -224,3 +224,38 @@ def test_zline_mixed_precision():
     assert s.last_report.status == abi.OK and s.last_report.resid <= 1e-12
     assert s.last_report.iter <= 24
     assert rel_l2(remove_mean(to_host(dphi)), remove_mean(ref)) < 1e-9
+
+
+# ------------------------------------------------------------------- LJ
+# The reference's own z-line smoother (mg_relaxLz with its pcf line
+# coefficients, mg_relax.F90:423-595): FP64 bit-identical to the oracle.
+LJ_CASES = ["shear_uniform", "shear_stretched_vbc", "partial_coarsening"]
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_LITERAL, abi.MODE_METRIC])
+@pytest.mark.parametrize("name", LJ_CASES)
+@pytest.mark.parametrize("which", [0, 2])
+def test_lj_pass_bitwise(name, mode, which):
+    g, p, o, s = _pair(name, mode, smoother=abi.SMOOTHER_LJ)
+    rng = np.random.default_rng(41 + which)
+    phi = field(g, rng)
+    src = field(g, rng)
+    ref = phi.copy(order="F")
+    o.debug_pass(which, ref, src.copy(order="F"))
+    dphi = to_dev(phi)
+    s.debug_pass(which, dphi, to_dev(src))
+    np.testing.assert_array_equal(to_host(dphi), ref)
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_LITERAL, abi.MODE_METRIC])
+@pytest.mark.parametrize("name", LJ_CASES)
+def test_lj_solve_bitwise(name, mode):
+    g, p, o, s = _pair(name, mode, smoother=abi.SMOOTHER_LJ, maxcy=40, tolmax=1e-9)
+    rng = np.random.default_rng(6)
+    src = compatible(field(g, rng), g, mode)
+    ref = zeros(g)
+    it_o, rm_o = o.solve(ref, src.copy(order="F"))
+    dphi = to_dev(zeros(g))
+    it_g, rm_g = s.solve(dphi, to_dev(src))
+    assert (it_g, rm_g) == (it_o, rm_o)
+    np.testing.assert_array_equal(to_host(dphi), ref)
