@@ -287,7 +287,7 @@ struct ZFac {
   const T* bp;  // eliminated diagonal
 };
 
-// kLJ: the reference's mg_relaxLz boundary rows (mg_relax.F90:507-518):
+// kLJ: the reference's mg_relaxLz boundary rows (mg_relax.F90:514-520):
 // the ghost term sits inside the neighbour sum, and with one row only the
 // top row's form is kept.
 template <typename T, bool kLJ>
