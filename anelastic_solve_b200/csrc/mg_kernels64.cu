@@ -72,39 +72,59 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return s;
 }
 
-// The interior is walked as x-rows (j, k): a CTA takes rows blockIdx.x,
-// blockIdx.x + gridDim.x, ... and its threads run along i, so the index
-// math is one 32-bit division per row.  The per-thread accumulation order
-// is fixed by the launch shape, so the sums are deterministic.
+// One interior cell per thread: grid (ceil(nx/kResidX), ny, nz), no loops,
+// so every resident thread has its stencil loads in flight.  Each CTA
+// writes its partial sums (fixed order); two fixed-order fold stages
+// follow, so the norms are deterministic.
+constexpr int kResidX = 128;
+constexpr int kFoldBlocks = 1024;
+
 template <bool kStore>
-__global__ void __launch_bounds__(kNormThreads) k_resid_norm(DevLevel<double> L,
-                                                            const double* __restrict__ phi,
-                                                            const double* __restrict__ f,
-                                                            float* __restrict__ r32,
-                                                            double* __restrict__ part) {
-  __shared__ double sh[kNormThreads / 32];
+__global__ void __launch_bounds__(kResidX) k_resid_norm(DevLevel<double> L, const double* __restrict__ phi,
+                                                       const double* __restrict__ f,
+                                                       float* __restrict__ r32,
+                                                       double* __restrict__ part) {
+  __shared__ double sh[kResidX / 32];
+  const int i = 2 + blockIdx.x * kResidX + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
   double rr = 0.0, ff = 0.0;
-  DevLevel<double> Lp = L;
-  Lp.phi = const_cast<double*>(phi);
-  Lp.src = const_cast<double*>(f);
-  const int nrow = L.ny * L.nz;
-  for (int row = blockIdx.x; row < nrow; row += gridDim.x) {
-    const int j = 2 + row % L.ny;
-    const int k = 2 + row / L.ny;
-    const int64_t base = cidx(0, j, k, L.X, L.XY);
-    for (int i = 2 + threadIdx.x; i <= L.nx + 1; i += blockDim.x) {
-      const int64_t c = base + i;
-      const double res = fine_resid(Lp, i, j, k);
-      if (kStore) r32[c] = (float)res;
-      rr += res * res;
-      ff += f[c] * f[c];
-    }
+  if (i <= L.nx + 1) {
+    DevLevel<double> Lp = L;
+    Lp.phi = const_cast<double*>(phi);
+    Lp.src = const_cast<double*>(f);
+    const int64_t c = cidx(i, j, k, L.X, L.XY);
+    const double res = fine_resid(Lp, i, j, k);
+    if (kStore) r32[c] = (float)res;
+    rr = res * res;
+    const double fc = f[c];
+    ff = fc * fc;
   }
   const double s1 = block_sum(rr, sh);
   const double s2 = block_sum(ff, sh);
   if (threadIdx.x == 0) {
-    part[2 * blockIdx.x] = s1;
-    part[2 * blockIdx.x + 1] = s2;
+    const int64_t b = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
+    part[2 * b] = s1;
+    part[2 * b + 1] = s2;
+  }
+}
+
+// part[0..2n) -> out2[0..2*gridDim.x): CTA b sums its contiguous chunk
+__global__ void k_fold_chunks(const double* __restrict__ part, int64_t n, double* __restrict__ out2) {
+  __shared__ double sh[kNormThreads / 32];
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t b0 = blockIdx.x * chunk;
+  const int64_t b1 = b0 + chunk < n ? b0 + chunk : n;
+  double a = 0.0, c = 0.0;
+  for (int64_t q = b0 + threadIdx.x; q < b1; q += blockDim.x) {
+    a += part[2 * q];
+    c += part[2 * q + 1];
+  }
+  const double s1 = block_sum(a, sh);
+  const double s2 = block_sum(c, sh);
+  if (threadIdx.x == 0) {
+    out2[2 * blockIdx.x] = s1;
+    out2[2 * blockIdx.x + 1] = s2;
   }
 }
 
@@ -123,25 +143,35 @@ __global__ void k_fold(const double* __restrict__ part, int nb, double* out) {
   }
 }
 
-int resid_norm_blocks(const DevLevel<double>& L) {
-  const int64_t rows = (int64_t)L.ny * L.nz;
-  return (int)(rows < 148 * 8 ? rows : 148 * 8);
+static dim3 resid_grid(const DevLevel<double>& L) {
+  return dim3((unsigned)((L.nx + kResidX - 1) / kResidX), (unsigned)L.ny, (unsigned)L.nz);
+}
+
+int64_t resid_part_doubles(const DevLevel<double>& L) {
+  const dim3 g = resid_grid(L);
+  return 2 * (int64_t)g.x * g.y * g.z + 2 * kFoldBlocks;
+}
+
+template <bool kStore>
+static void launch_resid(const DevLevel<double>& L, const double* phi, const double* f, float* r32,
+                         double* part, double* out, cudaStream_t s) {
+  const dim3 g = resid_grid(L);
+  const int64_t n = (int64_t)g.x * g.y * g.z;
+  k_resid_norm<kStore><<<g, kResidX, 0, s>>>(L, phi, f, r32, part);
+  double* part2 = part + 2 * n;
+  k_fold_chunks<<<kFoldBlocks, kNormThreads, 0, s>>>(part, n, part2);
+  k_fold<<<1, kNormThreads, 0, s>>>(part2, kFoldBlocks, out);
+  count_launch(3);
 }
 
 void launch_resid_norm(const DevLevel<double>& L, const double* phi, const double* f, double* part,
                        double* out, cudaStream_t s) {
-  const int nb = resid_norm_blocks(L);
-  k_resid_norm<false><<<nb, kNormThreads, 0, s>>>(L, phi, f, nullptr, part);
-  k_fold<<<1, kNormThreads, 0, s>>>(part, nb, out);
-  count_launch(2);
+  launch_resid<false>(L, phi, f, nullptr, part, out, s);
 }
 
 void launch_resid_store(const DevLevel<double>& L, const double* phi, const double* f, float* r32,
                         double* part, double* out, cudaStream_t s) {
-  const int nb = resid_norm_blocks(L);
-  k_resid_norm<true><<<nb, kNormThreads, 0, s>>>(L, phi, f, r32, part);
-  k_fold<<<1, kNormThreads, 0, s>>>(part, nb, out);
-  count_launch(2);
+  launch_resid<true>(L, phi, f, r32, part, out, s);
 }
 
 __global__ void __launch_bounds__(256) k_add_correction(DevLevel<double> L, double* __restrict__ phi,

@@ -48,7 +48,8 @@ void launch_relmax_copy(const DevLevel<double>& L, const double* phin, double* p
 //   folds the partials in index order into out[0], out[1].
 void launch_resid_norm(const DevLevel<double>& L, const double* phi, const double* f, double* part,
                        double* out, cudaStream_t s);
-int resid_norm_blocks(const DevLevel<double>& L);
+// doubles of partial sums the two launches below need
+int64_t resid_part_doubles(const DevLevel<double>& L);
 
 // FP64 fine residual r = f - A phi written to r (interior; ghosts 0) and
 // its squared norm partials, for the mixed-precision defect correction.

@@ -221,7 +221,7 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
       if (st != ANEL_OK) return st;
     }
   ANEL_CUDA_TRY(cudaMalloc(&d_max_, 2 * sizeof(unsigned long long)));
-  ANEL_CUDA_TRY(cudaMalloc(&d_part_, 2 * (size_t)gs_blocks(1LL << 40) * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_part_, (size_t)resid_part_doubles(L64(ngrid_)) * sizeof(double)));
   ANEL_CUDA_TRY(cudaMalloc(&d_norm_, 2 * sizeof(double)));
   ANEL_CUDA_TRY(cudaHostAlloc(&h_pin_, 4 * sizeof(double), cudaHostAllocDefault));
   // default density r == 1
