@@ -671,19 +671,16 @@ __device__ __forceinline__ T fine_resid(const DevLevel<T>& F, int i, int j, int 
 }
 
 template <typename T>
-__device__ __forceinline__ void restrict_range(const DevLevel<T>& F, const DevLevel<T>& Cl, int cdir,
-                                               int64_t t0, int64_t stride) {
-  for (int64_t t = t0; t < Cl.G; t += stride) {
-    const int ic = 1 + (int)(t % Cl.X);
-    const int64_t r = t / Cl.X;
-    const int jc = 1 + (int)(r % Cl.Y);
-    const int kc = 1 + (int)(r / Cl.Y);
+__device__ __forceinline__ void restrict_cell(const DevLevel<T>& F, const DevLevel<T>& Cl, int cdir,
+                                              int ic, int jc, int kc) {
+  {
+    const int64_t t = cidx(ic, jc, kc, Cl.X, Cl.XY);
     Cl.phi[t] = T(0);
     const bool interior =
         ic >= 2 && ic <= Cl.nx + 1 && jc >= 2 && jc <= Cl.ny + 1 && kc >= 2 && kc <= Cl.nz + 1;
     if (!interior) {
       Cl.src[t] = T(0);
-      continue;
+      return;
     }
     const bool cx = cdir & 1, cy = cdir & 2, cz = cdir & 4;
     const int i = cx ? 2 * ic - 2 : ic;
@@ -729,10 +726,12 @@ __device__ __forceinline__ void restrict_range(const DevLevel<T>& F, const DevLe
   }
 }
 
+// one coarse cell per thread, ghosts included: grid (ceil(X/128), Y, Z)
 template <typename T>
-__global__ void k_restrict(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
-  restrict_range(F, Cl, cdir, blockIdx.x * (int64_t)blockDim.x + threadIdx.x,
-                 (int64_t)gridDim.x * blockDim.x);
+__global__ void __launch_bounds__(128) k_restrict(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
+  const int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (ic > Cl.X) return;
+  restrict_cell(F, Cl, cdir, ic, 1 + (int)blockIdx.y, 1 + (int)blockIdx.z);
 }
 
 // -------------------------------------------------------------- prolong
@@ -741,14 +740,9 @@ __global__ void k_restrict(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
 // direction fine index f uses coarse ic = (f+1)/2 (f odd, near point ic) or
 // ic = f/2 (f even, near point ic+1); weights 3 (near) and 1 (far).
 template <typename T>
-__device__ __forceinline__ void prolong_range(const DevLevel<T>& F, const DevLevel<T>& Cl, int cdir,
-                                              int64_t t0, int64_t stride) {
-  const int64_t total = (int64_t)F.nx * F.ny * F.nz;
-  for (int64_t t = t0; t < total; t += stride) {
-    const int i = 2 + (int)(t % F.nx);
-    const int64_t r = t / F.nx;
-    const int j = 2 + (int)(r % F.ny);
-    const int k = 2 + (int)(r / F.ny);
+__device__ __forceinline__ void prolong_cell(const DevLevel<T>& F, const DevLevel<T>& Cl, int cdir, int i,
+                                             int j, int k) {
+  {
     const bool cx = cdir & 1, cy = cdir & 2, cz = cdir & 4;
     const int ic = cx ? ((i & 1) ? (i + 1) >> 1 : i >> 1) : i;
     const int jc = cy ? ((j & 1) ? (j + 1) >> 1 : j >> 1) : j;
@@ -802,10 +796,12 @@ __device__ __forceinline__ void prolong_range(const DevLevel<T>& F, const DevLev
   }
 }
 
+// one fine interior cell per thread: grid (ceil(nx/128), ny, nz)
 template <typename T>
-__global__ void k_prolong(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
-  prolong_range(F, Cl, cdir, blockIdx.x * (int64_t)blockDim.x + threadIdx.x,
-                (int64_t)gridDim.x * blockDim.x);
+__global__ void __launch_bounds__(128) k_prolong(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > F.nx + 1) return;
+  prolong_cell(F, Cl, cdir, i, 2 + (int)blockIdx.y, 2 + (int)blockIdx.z);
 }
 
 }  // namespace anel
