@@ -180,6 +180,34 @@ def initial_state(g, phys):
 STATE = ("u", "v", "w", "p", "rho")
 
 
+# ------------------------------------------------------------ multi-rank
+def combine_ranks(world, device, maxes=(), sums=()):
+    """Replicas: the max over ranks of each timing in `maxes` and the sum
+    of each count in `sums` (every rank takes the same collective steps in
+    the same order).  Returns (maxes, sums) as lists."""
+    maxes, sums = [float(v) for v in maxes], [float(v) for v in sums]
+    if world <= 1:
+        return maxes, sums
+    import torch
+    import torch.distributed as dist
+
+    if maxes:
+        t = torch.tensor(maxes, dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        maxes = t.tolist()
+    if sums:
+        t = torch.tensor(sums, dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        sums = t.tolist()
+    return maxes, sums
+
+
+def weak_value(world, cells, ms_step):
+    """Whole-job throughput of N replicas: every rank advanced `cells` in
+    the slowest rank's time."""
+    return world * cells / (ms_step / 1e3)
+
+
 # ---------------------------------------------------------------- ours: dns
 def run_dns(args, rank, world, local_rank):
     import torch
@@ -277,12 +305,8 @@ def run_dns(args, rank, world, local_rank):
     out["umax"] = float(max(np.abs(fu[k][1:-1, 1:-1, 1:-1]).max() for k in ("u", "v", "w")))
     out["dzmin"] = float(g.z.dxc[1:-1].min())
     s.close()
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([out["ms_step"], out.get("e2e_ms", 0.0)], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        out["ms_step"], out["e2e_ms"] = float(t[0]), float(t[1])
+    keys = [k for k in ("ms_step", "e2e_ms") if k in out]
+    out.update(zip(keys, combine_ranks(world, dev, maxes=[out[k] for k in keys])[0]))
     return out
 
 
@@ -351,6 +375,8 @@ def run_poisson(args, rank, world, local_rank):
         out["e2e_ms"] = e0.elapsed_time(e1) / ne
         out["bytes_io"] = (2 * dsrc.numel() * 8, dsrc.numel() * 8)
     s.close()
+    keys = [k for k in ("ms_step", "e2e_ms") if k in out]
+    out.update(zip(keys, combine_ranks(world, dev, maxes=[out[k] for k in keys])[0]))
     return out
 
 
@@ -488,15 +514,8 @@ def run_serve(args, rank, world, local_rank):
            "launches": _lib.launch_count() - launches0,
            "h2d": int(sum(8 * 6 * (2 * (r["size"][0] + r["size"][1] + r["size"][2]) + 6) for r in reqs)),
            "d2h": 8 * 8 * len(reqs), "arrival_span_s": reqs[-1]["t"], "mean_cells": float(meta.mean())}
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([out["makespan_s"], out["cell_updates"]], device=torch.device("cuda", local_rank),
-                         dtype=torch.float64)
-        mk = t.clone()
-        dist.all_reduce(mk, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        out["makespan_s"], out["cell_updates"] = float(mk[0]), float(t[1])
+    (out["makespan_s"],), (out["cell_updates"],) = combine_ranks(
+        world, torch.device("cuda", local_rank), maxes=(out["makespan_s"],), sums=(out["cell_updates"],))
     return out
 
 
@@ -673,7 +692,7 @@ def main():
         return
     peak, peak_kind = load_peaks()
     N = r["N"]
-    value = world * N / (r["ms_step"] / 1e3)
+    value = weak_value(world, N, r["ms_step"])
     # smoother bytes per cell and launch (one colour): reads of the other
     # colour's phi (the neighbours, half the cells), f of this colour and
     # the write of this colour's phi -> 12 B FP64, 6 B FP32.  The FP64
