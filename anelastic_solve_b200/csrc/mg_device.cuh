@@ -726,12 +726,20 @@ __device__ __forceinline__ void restrict_cell(const DevLevel<T>& F, const DevLev
   }
 }
 
-// one coarse cell per thread, ghosts included: grid (ceil(X/128), Y, Z)
+// kZBatch consecutive z-cells per thread (their loads in flight together):
+// one cell of 4 or 8 bytes per thread leaves too few bytes in flight per SM
+// to keep HBM busy.
+constexpr int kZBatch = 4;
+
+// coarse cells, ghosts included: grid (ceil(X/128), Y, ceil(Z/kZBatch))
 template <typename T>
 __global__ void __launch_bounds__(128) k_restrict(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
   const int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   if (ic > Cl.X) return;
-  restrict_cell(F, Cl, cdir, ic, 1 + (int)blockIdx.y, 1 + (int)blockIdx.z);
+  const int k0 = 1 + blockIdx.z * kZBatch;
+#pragma unroll
+  for (int q = 0; q < kZBatch; ++q)
+    if (k0 + q <= Cl.Z) restrict_cell(F, Cl, cdir, ic, 1 + (int)blockIdx.y, k0 + q);
 }
 
 // -------------------------------------------------------------- prolong
@@ -796,12 +804,15 @@ __device__ __forceinline__ void prolong_cell(const DevLevel<T>& F, const DevLeve
   }
 }
 
-// one fine interior cell per thread: grid (ceil(nx/128), ny, nz)
+// fine interior cells: grid (ceil(nx/128), ny, ceil(nz/kZBatch))
 template <typename T>
 __global__ void __launch_bounds__(128) k_prolong(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i > F.nx + 1) return;
-  prolong_cell(F, Cl, cdir, i, 2 + (int)blockIdx.y, 2 + (int)blockIdx.z);
+  const int k0 = 2 + blockIdx.z * kZBatch;
+#pragma unroll
+  for (int q = 0; q < kZBatch; ++q)
+    if (k0 + q <= F.nz + 1) prolong_cell(F, Cl, cdir, i, 2 + (int)blockIdx.y, k0 + q);
 }
 
 }  // namespace anel

@@ -72,8 +72,8 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return s;
 }
 
-// One interior cell per thread: grid (ceil(nx/kResidX), ny, nz), no loops,
-// so every resident thread has its stencil loads in flight.  Each CTA
+// kZBatch interior cells per thread (consecutive k): grid (ceil(nx/kResidX),
+// ny, ceil(nz/kZBatch)), their stencil loads in flight together.  Each CTA
 // writes its partial sums (fixed order); two fixed-order fold stages
 // follow, so the norms are deterministic.
 constexpr int kResidX = 128;
@@ -87,18 +87,30 @@ __global__ void __launch_bounds__(kResidX) k_resid_norm(DevLevel<double> L, cons
   __shared__ double sh[kResidX / 32];
   const int i = 2 + blockIdx.x * kResidX + threadIdx.x;
   const int j = 2 + blockIdx.y;
-  const int k = 2 + blockIdx.z;
+  const int k0 = 2 + blockIdx.z * kZBatch;
   double rr = 0.0, ff = 0.0;
   if (i <= L.nx + 1) {
     DevLevel<double> Lp = L;
     Lp.phi = const_cast<double*>(phi);
     Lp.src = const_cast<double*>(f);
-    const int64_t c = cidx(i, j, k, L.X, L.XY);
-    const double res = fine_resid(Lp, i, j, k);
-    if (kStore) r32[c] = (float)res;
-    rr = res * res;
-    const double fc = f[c];
-    ff = fc * fc;
+    double res[kZBatch], fv[kZBatch];
+#pragma unroll
+    for (int q = 0; q < kZBatch; ++q) {
+      const int k = k0 + q;
+      if (k <= L.nz + 1) {
+        res[q] = fine_resid(Lp, i, j, k);
+        fv[q] = f[cidx(i, j, k, L.X, L.XY)];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kZBatch; ++q) {
+      const int k = k0 + q;
+      if (k <= L.nz + 1) {
+        if (kStore) r32[cidx(i, j, k, L.X, L.XY)] = (float)res[q];
+        rr += res[q] * res[q];
+        ff += fv[q] * fv[q];
+      }
+    }
   }
   const double s1 = block_sum(rr, sh);
   const double s2 = block_sum(ff, sh);
@@ -144,7 +156,8 @@ __global__ void k_fold(const double* __restrict__ part, int nb, double* out) {
 }
 
 static dim3 resid_grid(const DevLevel<double>& L) {
-  return dim3((unsigned)((L.nx + kResidX - 1) / kResidX), (unsigned)L.ny, (unsigned)L.nz);
+  return dim3((unsigned)((L.nx + kResidX - 1) / kResidX), (unsigned)L.ny,
+              (unsigned)((L.nz + kZBatch - 1) / kZBatch));
 }
 
 int64_t resid_part_doubles(const DevLevel<double>& L) {

@@ -57,12 +57,14 @@ void launch_zline_seg(const DevLevel<T>& L, int color, const SegFac<T>& F, cudaS
 }
 template <typename T>
 void launch_restrict(const DevLevel<T>& F, const DevLevel<T>& C, int cdir, cudaStream_t s) {
-  k_restrict<T><<<dim3((unsigned)((C.X + 127) / 128), (unsigned)C.Y, (unsigned)C.Z), 128, 0, s>>>(F, C, cdir);
+  k_restrict<T><<<dim3((unsigned)((C.X + 127) / 128), (unsigned)C.Y,
+                       (unsigned)((C.Z + kZBatch - 1) / kZBatch)), 128, 0, s>>>(F, C, cdir);
   count_launch();
 }
 template <typename T>
 void launch_prolong(const DevLevel<T>& F, const DevLevel<T>& C, int cdir, cudaStream_t s) {
-  k_prolong<T><<<dim3((unsigned)((F.nx + 127) / 128), (unsigned)F.ny, (unsigned)F.nz), 128, 0, s>>>(F, C, cdir);
+  k_prolong<T><<<dim3((unsigned)((F.nx + 127) / 128), (unsigned)F.ny,
+                      (unsigned)((F.nz + kZBatch - 1) / kZBatch)), 128, 0, s>>>(F, C, cdir);
   count_launch();
 }
 
