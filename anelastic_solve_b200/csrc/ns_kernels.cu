@@ -8,8 +8,15 @@ namespace anel {
 static constexpr double R12 = 1.0 / 2.0;  // ratios::r_1_2 (modules.F90:203)
 
 // --------------------------------------------------------------- RHS
+// Inside the RHS functions a field access FA(a, i+di, j+dj, k+dk) is the
+// centre offset c0_ plus a neighbour offset that folds to a constant
+// (integer index arithmetic only; the floating-point expressions are
+// unchanged).
+#undef FA
+#define FA(a, I, J, K) (a)[c0_ + ((I) - i) + (int64_t)D.X * ((J) - j) + D.XY * ((K) - k)]
 // u1_rhs (NSsolver.F90:646-804): returns Utemp(i,j,k) before ghosting.
 __device__ __forceinline__ double rhs_u(const NSDev& D, int i, int j, int k) {
+  const int64_t c0_ = NS_IX(i, j, k);
   const double* un = D.u;
   const double* vn = D.v;
   const double* wn = D.w;
@@ -69,6 +76,7 @@ __device__ __forceinline__ double rhs_u(const NSDev& D, int i, int j, int k) {
 
 // u2_rhs (NSsolver.F90:912-1081)
 __device__ __forceinline__ double rhs_v(const NSDev& D, int i, int j, int k) {
+  const int64_t c0_ = NS_IX(i, j, k);
   const double* un = D.u;
   const double* vn = D.v;
   const double* wn = D.w;
@@ -129,6 +137,7 @@ __device__ __forceinline__ double rhs_v(const NSDev& D, int i, int j, int k) {
 
 // u3_rhs (NSsolver.F90:1195-1377); rows above nz+1-EW carry no terms.
 __device__ __forceinline__ double rhs_w(const NSDev& D, int i, int j, int k) {
+  const int64_t c0_ = NS_IX(i, j, k);
   if (k > D.nz + 1 - D.ew) return 0.0;
   const double* un = D.u;
   const double* vn = D.v;
@@ -190,6 +199,7 @@ __device__ __forceinline__ double rhs_w(const NSDev& D, int i, int j, int k) {
 // rho_rhs (NSsolver.F90:1720-1815) and scal1_rhs (:1890-1985)
 template <bool kRho>
 __device__ __forceinline__ double rhs_scalar(const NSDev& D, int i, int j, int k) {
+  const int64_t c0_ = NS_IX(i, j, k);
   const double* un = D.u;
   const double* vn = D.v;
   const double* wn = D.w;
@@ -240,6 +250,9 @@ __device__ __forceinline__ double rhs_scalar(const NSDev& D, int i, int j, int k
   }
   return acc;
 }
+
+#undef FA
+#define FA(a, i, j, k) (a)[NS_IX(i, j, k)]
 
 // K1: all right-hand sides and the low-storage accumulation
 // q = a1*q + a2*F*dt (var_advance, NSsolver.F90:2225-2264) in one pass.
