@@ -670,76 +670,95 @@ __device__ __forceinline__ T fine_resid(const DevLevel<T>& F, int i, int j, int 
   return F.src[c] - acc;
 }
 
-template <typename T>
-__device__ __forceinline__ void restrict_cell(const DevLevel<T>& F, const DevLevel<T>& Cl, int cdir,
-                                              int ic, int jc, int kc) {
-  {
-    const int64_t t = cidx(ic, jc, kc, Cl.X, Cl.XY);
-    Cl.phi[t] = T(0);
-    const bool interior =
-        ic >= 2 && ic <= Cl.nx + 1 && jc >= 2 && jc <= Cl.ny + 1 && kc >= 2 && kc <= Cl.nz + 1;
-    if (!interior) {
-      Cl.src[t] = T(0);
-      return;
-    }
-    const bool cx = cdir & 1, cy = cdir & 2, cz = cdir & 4;
-    const int i = cx ? 2 * ic - 2 : ic;
-    const int j = cy ? 2 * jc - 2 : jc;
-    const int k = cz ? 2 * kc - 2 : kc;
-    T v;
-    if (cx && cy && cz) {
-      T s = fine_resid(F, i, j, k);
-      s = s + fine_resid(F, i, j + 1, k);
-      s = s + fine_resid(F, i, j, k + 1);
-      s = s + fine_resid(F, i, j + 1, k + 1);
-      s = s + fine_resid(F, i + 1, j, k);
-      s = s + fine_resid(F, i + 1, j + 1, k + 1);
-      s = s + fine_resid(F, i + 1, j + 1, k);
-      s = s + fine_resid(F, i + 1, j, k + 1);
-      v = T(0.125) * s;
-    } else if (!cx && !cy) {  // z only
-      v = T(0.5) * (fine_resid(F, i, j, k) + fine_resid(F, i, j, k + 1));
-    } else if (!cx && !cz) {  // y only
-      v = T(0.5) * (fine_resid(F, i, j, k) + fine_resid(F, i, j + 1, k));
-    } else if (!cy && !cz) {  // x only
-      v = T(0.5) * (fine_resid(F, i, j, k) + fine_resid(F, i + 1, j, k));
-    } else if (!cx) {  // y,z
-      T s = fine_resid(F, i, j, k);
-      s = s + fine_resid(F, i, j + 1, k);
-      s = s + fine_resid(F, i, j, k + 1);
-      s = s + fine_resid(F, i, j + 1, k + 1);
-      v = T(0.25) * s;
-    } else if (!cy) {  // x,z
-      T s = fine_resid(F, i, j, k);
-      s = s + fine_resid(F, i, j, k + 1);
-      s = s + fine_resid(F, i + 1, j, k);
-      s = s + fine_resid(F, i + 1, j, k + 1);
-      v = T(0.25) * s;
-    } else {  // x,y
-      T s = fine_resid(F, i, j, k);
-      s = s + fine_resid(F, i + 1, j, k);
-      s = s + fine_resid(F, i, j + 1, k);
-      s = s + fine_resid(F, i + 1, j + 1, k);
-      v = T(0.25) * s;
-    }
-    Cl.src[t] = v;
+// Value of interior coarse cell (ic,jc,kc) for the coarsening variant CD:
+// the scaled sum of the children's residuals in the reference order.
+template <typename T, int CD>
+__device__ __forceinline__ T restrict_value(const DevLevel<T>& F, int ic, int jc, int kc) {
+  constexpr bool cx = CD & 1, cy = CD & 2, cz = CD & 4;
+  const int i = cx ? 2 * ic - 2 : ic;
+  const int j = cy ? 2 * jc - 2 : jc;
+  const int k = cz ? 2 * kc - 2 : kc;
+  if constexpr (cx && cy && cz) {
+    T s = fine_resid(F, i, j, k);
+    s = s + fine_resid(F, i, j + 1, k);
+    s = s + fine_resid(F, i, j, k + 1);
+    s = s + fine_resid(F, i, j + 1, k + 1);
+    s = s + fine_resid(F, i + 1, j, k);
+    s = s + fine_resid(F, i + 1, j + 1, k + 1);
+    s = s + fine_resid(F, i + 1, j + 1, k);
+    s = s + fine_resid(F, i + 1, j, k + 1);
+    return T(0.125) * s;
+  } else if constexpr (!cx && !cy) {  // z only
+    return T(0.5) * (fine_resid(F, i, j, k) + fine_resid(F, i, j, k + 1));
+  } else if constexpr (!cx && !cz) {  // y only
+    return T(0.5) * (fine_resid(F, i, j, k) + fine_resid(F, i, j + 1, k));
+  } else if constexpr (!cy && !cz) {  // x only
+    return T(0.5) * (fine_resid(F, i, j, k) + fine_resid(F, i + 1, j, k));
+  } else if constexpr (!cx) {  // y,z
+    T s = fine_resid(F, i, j, k);
+    s = s + fine_resid(F, i, j + 1, k);
+    s = s + fine_resid(F, i, j, k + 1);
+    s = s + fine_resid(F, i, j + 1, k + 1);
+    return T(0.25) * s;
+  } else if constexpr (!cy) {  // x,z
+    T s = fine_resid(F, i, j, k);
+    s = s + fine_resid(F, i, j, k + 1);
+    s = s + fine_resid(F, i + 1, j, k);
+    s = s + fine_resid(F, i + 1, j, k + 1);
+    return T(0.25) * s;
+  } else {  // x,y
+    T s = fine_resid(F, i, j, k);
+    s = s + fine_resid(F, i + 1, j, k);
+    s = s + fine_resid(F, i, j + 1, k);
+    s = s + fine_resid(F, i + 1, j + 1, k);
+    return T(0.25) * s;
   }
 }
 
-// kZBatch consecutive z-cells per thread (their loads in flight together):
-// one cell of 4 or 8 bytes per thread leaves too few bytes in flight per SM
-// to keep HBM busy.
+// kZBatch consecutive z-cells per thread, every load issued before the
+// first store (a store to one array may not be moved past a load of
+// another by the compiler, so interleaving would serialise the cells).
 constexpr int kZBatch = 4;
 
-// coarse cells, ghosts included: grid (ceil(X/128), Y, ceil(Z/kZBatch))
-template <typename T>
-__global__ void __launch_bounds__(128) k_restrict(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
-  const int ic = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (ic > Cl.X) return;
+// Coarse cells: grid (ceil(nx/128), Y, ceil(Z/kZBatch)); thread ic covers
+// interior column ic, and the threads of columns 2 and nx+1 also zero the
+// ghost columns 1 and nx+2.  Coarse phi <- 0 everywhere, coarse f <- 0 on
+// ghosts.
+template <typename T, int CD>
+__global__ void __launch_bounds__(128) k_restrict(DevLevel<T> F, DevLevel<T> Cl) {
+  const int ic = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (ic > Cl.nx + 1) return;
+  const int jc = 1 + blockIdx.y;
   const int k0 = 1 + blockIdx.z * kZBatch;
+  const bool row_in = jc >= 2 && jc <= Cl.ny + 1;
+  T v[kZBatch];
+  if (row_in && k0 >= 2 && k0 + kZBatch - 1 <= Cl.nz + 1) {
 #pragma unroll
-  for (int q = 0; q < kZBatch; ++q)
-    if (k0 + q <= Cl.Z) restrict_cell(F, Cl, cdir, ic, 1 + (int)blockIdx.y, k0 + q);
+    for (int q = 0; q < kZBatch; ++q) v[q] = restrict_value<T, CD>(F, ic, jc, k0 + q);
+  } else {
+#pragma unroll
+    for (int q = 0; q < kZBatch; ++q) {
+      const int kc = k0 + q;
+      v[q] = (row_in && kc >= 2 && kc <= Cl.nz + 1) ? restrict_value<T, CD>(F, ic, jc, kc) : T(0);
+    }
+  }
+  const int64_t t0 = cidx(ic, jc, k0, Cl.X, Cl.XY);
+  const bool g_lo = ic == 2, g_hi = ic == Cl.nx + 1;  // ghost columns beside this one
+#pragma unroll
+  for (int q = 0; q < kZBatch; ++q) {
+    if (k0 + q > Cl.Z) break;
+    const int64_t t = t0 + q * Cl.XY;
+    Cl.phi[t] = T(0);
+    Cl.src[t] = v[q];
+    if (g_lo) {
+      Cl.phi[t - 1] = T(0);
+      Cl.src[t - 1] = T(0);
+    }
+    if (g_hi) {
+      Cl.phi[t + 1] = T(0);
+      Cl.src[t + 1] = T(0);
+    }
+  }
 }
 
 // -------------------------------------------------------------- prolong
@@ -747,72 +766,81 @@ __global__ void __launch_bounds__(128) k_restrict(DevLevel<T> F, DevLevel<T> Cl,
 // boundary pass that follows, as in the reference).  In a coarsened
 // direction fine index f uses coarse ic = (f+1)/2 (f odd, near point ic) or
 // ic = f/2 (f even, near point ic+1); weights 3 (near) and 1 (far).
-template <typename T>
-__device__ __forceinline__ void prolong_cell(const DevLevel<T>& F, const DevLevel<T>& Cl, int cdir, int i,
-                                             int j, int k) {
-  {
-    const bool cx = cdir & 1, cy = cdir & 2, cz = cdir & 4;
-    const int ic = cx ? ((i & 1) ? (i + 1) >> 1 : i >> 1) : i;
-    const int jc = cy ? ((j & 1) ? (j + 1) >> 1 : j >> 1) : j;
-    const int kc = cz ? ((k & 1) ? (k + 1) >> 1 : k >> 1) : k;
-    // weight of coarse offset o (0/1) in each direction
-    const T wx0 = cx ? ((i & 1) ? T(3) : T(1)) : T(1), wx1 = cx ? ((i & 1) ? T(1) : T(3)) : T(0);
-    const T wy0 = cy ? ((j & 1) ? T(3) : T(1)) : T(1), wy1 = cy ? ((j & 1) ? T(1) : T(3)) : T(0);
-    const T wz0 = cz ? ((k & 1) ? T(3) : T(1)) : T(1), wz1 = cz ? ((k & 1) ? T(1) : T(3)) : T(0);
-    const int64_t c0 = cidx(ic, jc, kc, Cl.X, Cl.XY);
-    const T* __restrict__ pc = Cl.phi;
-    const int64_t ox = 1, oy = Cl.X, oz = Cl.XY;
-    T corr;
-    if (cx && cy && cz) {
-      // order (x,y,z) offsets: 000 010 001 011 100 110 101 111
-      T s = (wx0 * wy0 * wz0) * pc[c0];
-      s = s + (wx0 * wy1 * wz0) * pc[c0 + oy];
-      s = s + (wx0 * wy0 * wz1) * pc[c0 + oz];
-      s = s + (wx0 * wy1 * wz1) * pc[c0 + oy + oz];
-      s = s + (wx1 * wy0 * wz0) * pc[c0 + ox];
-      s = s + (wx1 * wy1 * wz0) * pc[c0 + ox + oy];
-      s = s + (wx1 * wy0 * wz1) * pc[c0 + ox + oz];
-      s = s + (wx1 * wy1 * wz1) * pc[c0 + ox + oy + oz];
-      corr = s / T(64);
-    } else if (!cx && !cy) {  // z only
-      corr = (wz0 * pc[c0] + wz1 * pc[c0 + oz]) / T(4);
-    } else if (!cx && !cz) {  // y only
-      corr = (wy0 * pc[c0] + wy1 * pc[c0 + oy]) / T(4);
-    } else if (!cy && !cz) {  // x only
-      corr = (wx0 * pc[c0] + wx1 * pc[c0 + ox]) / T(4);
-    } else if (!cx) {  // y,z: (y,z) 00 10 01 11
-      T s = (wy0 * wz0) * pc[c0];
-      s = s + (wy1 * wz0) * pc[c0 + oy];
-      s = s + (wy0 * wz1) * pc[c0 + oz];
-      s = s + (wy1 * wz1) * pc[c0 + oy + oz];
-      corr = s / T(16);
-    } else if (!cy) {  // x,z: (x,z) 00 10 01 11
-      T s = (wx0 * wz0) * pc[c0];
-      s = s + (wx1 * wz0) * pc[c0 + ox];
-      s = s + (wx0 * wz1) * pc[c0 + oz];
-      s = s + (wx1 * wz1) * pc[c0 + ox + oz];
-      corr = s / T(16);
-    } else {  // x,y: (x,y) 00 10 01 11
-      T s = (wx0 * wy0) * pc[c0];
-      s = s + (wx1 * wy0) * pc[c0 + ox];
-      s = s + (wx0 * wy1) * pc[c0 + oy];
-      s = s + (wx1 * wy1) * pc[c0 + ox + oy];
-      corr = s / T(16);
-    }
-    const int64_t cf = cidx(i, j, k, F.X, F.XY);
-    F.phi[cf] = F.phi[cf] + corr;
+template <typename T, int CD>
+__device__ __forceinline__ T prolong_corr(const DevLevel<T>& Cl, int i, int j, int k) {
+  constexpr bool cx = CD & 1, cy = CD & 2, cz = CD & 4;
+  const int ic = cx ? ((i & 1) ? (i + 1) >> 1 : i >> 1) : i;
+  const int jc = cy ? ((j & 1) ? (j + 1) >> 1 : j >> 1) : j;
+  const int kc = cz ? ((k & 1) ? (k + 1) >> 1 : k >> 1) : k;
+  // weight of coarse offset o (0/1) in each direction
+  const T wx0 = cx ? ((i & 1) ? T(3) : T(1)) : T(1), wx1 = cx ? ((i & 1) ? T(1) : T(3)) : T(0);
+  const T wy0 = cy ? ((j & 1) ? T(3) : T(1)) : T(1), wy1 = cy ? ((j & 1) ? T(1) : T(3)) : T(0);
+  const T wz0 = cz ? ((k & 1) ? T(3) : T(1)) : T(1), wz1 = cz ? ((k & 1) ? T(1) : T(3)) : T(0);
+  const T* __restrict__ pc = Cl.phi + cidx(ic, jc, kc, Cl.X, Cl.XY);
+  const int64_t ox = 1, oy = Cl.X, oz = Cl.XY;
+  if constexpr (cx && cy && cz) {
+    // order (x,y,z) offsets: 000 010 001 011 100 110 101 111
+    T s = (wx0 * wy0 * wz0) * pc[0];
+    s = s + (wx0 * wy1 * wz0) * pc[oy];
+    s = s + (wx0 * wy0 * wz1) * pc[oz];
+    s = s + (wx0 * wy1 * wz1) * pc[oy + oz];
+    s = s + (wx1 * wy0 * wz0) * pc[ox];
+    s = s + (wx1 * wy1 * wz0) * pc[ox + oy];
+    s = s + (wx1 * wy0 * wz1) * pc[ox + oz];
+    s = s + (wx1 * wy1 * wz1) * pc[ox + oy + oz];
+    return s / T(64);
+  } else if constexpr (!cx && !cy) {  // z only
+    return (wz0 * pc[0] + wz1 * pc[oz]) / T(4);
+  } else if constexpr (!cx && !cz) {  // y only
+    return (wy0 * pc[0] + wy1 * pc[oy]) / T(4);
+  } else if constexpr (!cy && !cz) {  // x only
+    return (wx0 * pc[0] + wx1 * pc[ox]) / T(4);
+  } else if constexpr (!cx) {  // y,z: (y,z) 00 10 01 11
+    T s = (wy0 * wz0) * pc[0];
+    s = s + (wy1 * wz0) * pc[oy];
+    s = s + (wy0 * wz1) * pc[oz];
+    s = s + (wy1 * wz1) * pc[oy + oz];
+    return s / T(16);
+  } else if constexpr (!cy) {  // x,z: (x,z) 00 10 01 11
+    T s = (wx0 * wz0) * pc[0];
+    s = s + (wx1 * wz0) * pc[ox];
+    s = s + (wx0 * wz1) * pc[oz];
+    s = s + (wx1 * wz1) * pc[ox + oz];
+    return s / T(16);
+  } else {  // x,y: (x,y) 00 10 01 11
+    T s = (wx0 * wy0) * pc[0];
+    s = s + (wx1 * wy0) * pc[ox];
+    s = s + (wx0 * wy1) * pc[oy];
+    s = s + (wx1 * wy1) * pc[ox + oy];
+    return s / T(16);
   }
 }
 
-// fine interior cells: grid (ceil(nx/128), ny, ceil(nz/kZBatch))
-template <typename T>
-__global__ void __launch_bounds__(128) k_prolong(DevLevel<T> F, DevLevel<T> Cl, int cdir) {
+// fine interior cells: grid (ceil(nx/128), ny, ceil(nz/kZBatch)); the
+// corrections and old values of all kZBatch cells are loaded before the
+// first store.
+template <typename T, int CD>
+__global__ void __launch_bounds__(128) k_prolong(DevLevel<T> F, DevLevel<T> Cl) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   if (i > F.nx + 1) return;
+  const int j = 2 + blockIdx.y;
   const int k0 = 2 + blockIdx.z * kZBatch;
+  T* p = F.phi + cidx(i, j, k0, F.X, F.XY);
+  const int64_t XY = F.XY;
+  T val[kZBatch];
+  if (k0 + kZBatch - 1 <= F.nz + 1) {
 #pragma unroll
-  for (int q = 0; q < kZBatch; ++q)
-    if (k0 + q <= F.nz + 1) prolong_cell(F, Cl, cdir, i, 2 + (int)blockIdx.y, k0 + q);
+    for (int q = 0; q < kZBatch; ++q) val[q] = p[q * XY] + prolong_corr<T, CD>(Cl, i, j, k0 + q);
+#pragma unroll
+    for (int q = 0; q < kZBatch; ++q) p[q * XY] = val[q];
+  } else {
+#pragma unroll
+    for (int q = 0; q < kZBatch; ++q)
+      if (k0 + q <= F.nz + 1) val[q] = p[q * XY] + prolong_corr<T, CD>(Cl, i, j, k0 + q);
+#pragma unroll
+    for (int q = 0; q < kZBatch; ++q)
+      if (k0 + q <= F.nz + 1) p[q * XY] = val[q];
+  }
 }
 
 }  // namespace anel

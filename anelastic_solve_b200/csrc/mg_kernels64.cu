@@ -187,20 +187,37 @@ void launch_resid_store(const DevLevel<double>& L, const double* phi, const doub
   launch_resid<true>(L, phi, f, r32, part, out, s);
 }
 
+// phi += e on the interior: rows (j,k) walked kACRows at a time, the loads
+// of all those rows issued before their stores.
+constexpr int kACRows = 4;
 __global__ void __launch_bounds__(256) k_add_correction(DevLevel<double> L, double* __restrict__ phi,
                                                        const float* __restrict__ e) {
   const int nrow = L.ny * L.nz;
-  for (int row = blockIdx.x; row < nrow; row += gridDim.x) {
-    const int j = 2 + row % L.ny;
-    const int k = 2 + row / L.ny;
-    const int64_t base = cidx(0, j, k, L.X, L.XY);
-    for (int i = 2 + threadIdx.x; i <= L.nx + 1; i += blockDim.x) phi[base + i] = phi[base + i] + (double)e[base + i];
+  for (int row0 = blockIdx.x * kACRows; row0 < nrow; row0 += gridDim.x * kACRows) {
+    int64_t base[kACRows];
+#pragma unroll
+    for (int u = 0; u < kACRows; ++u) {
+      const int row = row0 + u < nrow ? row0 + u : nrow - 1;
+      base[u] = cidx(0, 2 + row % L.ny, 2 + row / L.ny, L.X, L.XY);
+    }
+    for (int i = 2 + threadIdx.x; i <= L.nx + 1; i += blockDim.x) {
+      double pv[kACRows];
+      float ev[kACRows];
+#pragma unroll
+      for (int u = 0; u < kACRows; ++u) {
+        pv[u] = phi[base[u] + i];
+        ev[u] = e[base[u] + i];
+      }
+#pragma unroll
+      for (int u = 0; u < kACRows; ++u)
+        if (row0 + u < nrow) phi[base[u] + i] = pv[u] + (double)ev[u];
+    }
   }
 }
 
 void launch_add_correction(const DevLevel<double>& L, double* phi, const float* e, cudaStream_t s) {
-  const int64_t rows = (int64_t)L.ny * L.nz;
-  k_add_correction<<<(unsigned)(rows < 148 * 8 ? rows : 148 * 8), 256, 0, s>>>(L, phi, e);
+  const int64_t groups = ((int64_t)L.ny * L.nz + kACRows - 1) / kACRows;
+  k_add_correction<<<(unsigned)(groups < 148 * 8 ? groups : 148 * 8), 256, 0, s>>>(L, phi, e);
   count_launch();
 }
 

@@ -57,14 +57,32 @@ void launch_zline_seg(const DevLevel<T>& L, int color, const SegFac<T>& F, cudaS
 }
 template <typename T>
 void launch_restrict(const DevLevel<T>& F, const DevLevel<T>& C, int cdir, cudaStream_t s) {
-  k_restrict<T><<<dim3((unsigned)((C.X + 127) / 128), (unsigned)C.Y,
-                       (unsigned)((C.Z + kZBatch - 1) / kZBatch)), 128, 0, s>>>(F, C, cdir);
+  const dim3 g((unsigned)((C.nx + 127) / 128), (unsigned)C.Y, (unsigned)((C.Z + kZBatch - 1) / kZBatch));
+  switch (cdir & 7) {
+    case 0: k_restrict<T, 0><<<g, 128, 0, s>>>(F, C); break;
+    case 1: k_restrict<T, 1><<<g, 128, 0, s>>>(F, C); break;
+    case 2: k_restrict<T, 2><<<g, 128, 0, s>>>(F, C); break;
+    case 3: k_restrict<T, 3><<<g, 128, 0, s>>>(F, C); break;
+    case 4: k_restrict<T, 4><<<g, 128, 0, s>>>(F, C); break;
+    case 5: k_restrict<T, 5><<<g, 128, 0, s>>>(F, C); break;
+    case 6: k_restrict<T, 6><<<g, 128, 0, s>>>(F, C); break;
+    default: k_restrict<T, 7><<<g, 128, 0, s>>>(F, C); break;
+  }
   count_launch();
 }
 template <typename T>
 void launch_prolong(const DevLevel<T>& F, const DevLevel<T>& C, int cdir, cudaStream_t s) {
-  k_prolong<T><<<dim3((unsigned)((F.nx + 127) / 128), (unsigned)F.ny,
-                      (unsigned)((F.nz + kZBatch - 1) / kZBatch)), 128, 0, s>>>(F, C, cdir);
+  const dim3 g((unsigned)((F.nx + 127) / 128), (unsigned)F.ny, (unsigned)((F.nz + kZBatch - 1) / kZBatch));
+  switch (cdir & 7) {
+    case 0: k_prolong<T, 0><<<g, 128, 0, s>>>(F, C); break;
+    case 1: k_prolong<T, 1><<<g, 128, 0, s>>>(F, C); break;
+    case 2: k_prolong<T, 2><<<g, 128, 0, s>>>(F, C); break;
+    case 3: k_prolong<T, 3><<<g, 128, 0, s>>>(F, C); break;
+    case 4: k_prolong<T, 4><<<g, 128, 0, s>>>(F, C); break;
+    case 5: k_prolong<T, 5><<<g, 128, 0, s>>>(F, C); break;
+    case 6: k_prolong<T, 6><<<g, 128, 0, s>>>(F, C); break;
+    default: k_prolong<T, 7><<<g, 128, 0, s>>>(F, C); break;
+  }
   count_launch();
 }
 
