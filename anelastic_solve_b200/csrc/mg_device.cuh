@@ -487,6 +487,10 @@ struct SegFac {
   // ghost of every column (0: zero, 1: row k=2, 2: row k=nz+1)
   const int* img;
   int z1, zZ;
+  // cyclic-reduction multipliers of the level's line matrix (k_zline_cr),
+  // or null: crs steps of alpha[nz] and gamma[nz], then 1/b[nz]
+  const T* cr;
+  int crs;
 };
 constexpr int kNoImage = -2147483647 - 1;
 
@@ -644,6 +648,95 @@ __global__ void __launch_bounds__(32 * P, 2) k_zline_seg(DevLevel<T> L, int colo
   __shared__ ZSegShared<T, P, MR> S;
   zseg_stage(L, F, S);
   zseg_chunk(L, color, F, S, reinterpret_cast<T*>(zs_smem), (int64_t)blockIdx.x * 32);
+}
+
+// ------------------------------------------ z-line solve, cyclic reduction
+// Levels with few lines (the coarse levels of the FP32 cycle): one CTA per
+// line, one thread per row.  Every line of a level has the same tridiagonal
+// matrix, so the multipliers of parallel cyclic reduction are precomputed
+// on the host: step s (stride 2^s) updates d_r += alpha_s[r] d_(r-2^s) +
+// gamma_s[r] d_(r+2^s), and after the last step x_r = d_r / b_r.  The
+// dependent chain is ceil(log2 nz) steps (the partitioned solver's is
+// 2 x 32 rows), so a sweep over a handful of lines costs a few
+// microseconds instead of one long per-thread chain.  The right-hand side
+// and the ghost copies are those of k_zline_seg.
+constexpr int kCRMaxSteps = 10;
+constexpr int kCRMaxRows = 1 << kCRMaxSteps;
+template <typename T>
+__global__ void __launch_bounds__(kCRMaxRows) k_zline_cr(DevLevel<T> L, int color, SegFac<T> F) {
+  __shared__ T D[2][kCRMaxRows];
+  const int n = L.nz;
+  const int pairs = (L.nx + 1) >> 1;
+  const int t = blockIdx.x;  // line of this colour
+  const int j = 2 + t / pairs;
+  const int i0 = 2 + 2 * (t % pairs);
+  const int i = i0 + ((color + i0 + j) & 1);
+  if (i > L.nx + 1) return;  // the whole CTA: no barrier reached
+  const int r = threadIdx.x;
+  const bool row = r < n;
+  const int64_t X = L.X, XY = L.XY;
+  const int64_t cb = cidx(i, j, 2, L.X, L.XY);  // row 0 (k = 2)
+  const int64_t c = cb + (int64_t)(row ? r : 0) * XY;
+  T al[kCRMaxSteps], ga[kCRMaxSteps];
+  T d = T(0), rb = T(0);
+  if (row) {
+    const T a1 = cx1p(L)[i - 1], a2 = cx2p(L)[i - 1];
+    const T a3 = cy3p(L)[j - 1], a4 = cy4p(L)[j - 1];
+    const T* __restrict__ phi = L.phi;
+    d = L.src[c] - (a1 * phi[c - 1] + a2 * phi[c + 1] + a3 * phi[c - X] + a4 * phi[c + X]);
+    if (r == 0) d -= cz5p(L)[1] * phi[c - XY];
+    if (r == n - 1) d -= cz6p(L)[n] * phi[c + XY];
+#pragma unroll
+    for (int q = 0; q < kCRMaxSteps; ++q)
+      if (q < F.crs) {
+        al[q] = F.cr[(size_t)(2 * q) * n + r];
+        ga[q] = F.cr[(size_t)(2 * q + 1) * n + r];
+      }
+    rb = F.cr[(size_t)(2 * F.crs) * n + r];
+    D[0][r] = d;
+  }
+  __syncthreads();
+  int b = 0;
+#pragma unroll
+  for (int q = 0; q < kCRMaxSteps; ++q) {
+    if (q >= F.crs) break;  // uniform across the CTA
+    const int st = 1 << q;
+    if (row) {
+      T v = d;
+      if (r - st >= 0) v += al[q] * D[b][r - st];
+      if (r + st < n) v += ga[q] * D[b][r + st];
+      d = v;
+      D[b ^ 1][r] = d;
+    }
+    b ^= 1;
+    __syncthreads();  // (double buffer: one barrier per step)
+  }
+  const T x = d * rb;
+  if (row) D[b ^ 1][r] = x;
+  __syncthreads();
+  if (!row) return;
+  T* phi = L.phi;
+  int d0 = kNoImage, d1 = kNoImage, d2 = kNoImage;
+  if (F.img) {
+    const int* im = F.img + 3 * ((i - 2) + (int64_t)L.nx * (j - 2));
+    d0 = im[0];
+    d1 = im[1];
+    d2 = im[2];
+  }
+  auto put = [&](int64_t cc, T v) {
+    phi[cc] = v;
+    if (d0 != kNoImage) phi[cc + d0] = v;
+    if (d1 != kNoImage) phi[cc + d1] = v;
+    if (d2 != kNoImage) phi[cc + d2] = v;
+  };
+  put(c, x);
+  if (F.img) {
+    // z ghosts of the column and of its images (rows k=1 and k=Z)
+    const T* xs = D[b ^ 1];
+    auto zval = [&](int code) -> T { return code == 0 ? T(0) : (code == 1 ? xs[0] : xs[n - 1]); };
+    if (r == 0) put(cb - XY, zval(F.z1));
+    if (r == n - 1) put(cb + (int64_t)n * XY, zval(F.zZ));
+  }
 }
 
 // ----------------------------------------------------- residual + restrict

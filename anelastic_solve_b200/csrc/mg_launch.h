@@ -28,6 +28,11 @@ void launch_zline_lj(const DevLevel<T>& L, int color, const T* ap, const T* bp, 
 // 2..kZSegRows rows (lines of nz = kZSeg * m rows)
 constexpr int kZSeg = 16;
 constexpr int kZSegRows = 32;
+// levels with at most this many lines of a colour use the cyclic-reduction
+// line solve (one CTA per line) when its multipliers exist: about 6 us per
+// sweep up to a few hundred lines, where the partitioned solver's per-CTA
+// chain costs about 20 us; from ~1000 lines on the partitioned one is faster
+constexpr int64_t kCRMaxLines = 512;
 template <typename T>
 void launch_zline_seg(const DevLevel<T>& L, int color, const SegFac<T>& F, cudaStream_t s);
 // ghost table of an FP32 level with a homogeneous rule (L.gtab ignored)

@@ -49,6 +49,11 @@ void launch_zline_lj(const DevLevel<T>& L, int color, const T* ap, const T* bp, 
 template <typename T>
 void launch_zline_seg(const DevLevel<T>& L, int color, const SegFac<T>& F, cudaStream_t s) {
   const int64_t cols = (int64_t)((L.nx + 1) / 2) * L.ny;
+  if (F.cr && cols <= kCRMaxLines && L.nz <= kCRMaxRows) {
+    k_zline_cr<T><<<(unsigned)cols, (unsigned)((L.nz + 31) / 32 * 32), 0, s>>>(L, color, F);
+    count_launch();
+    return;
+  }
   const size_t sm = (size_t)kZSegRows * kZSeg * 32 * sizeof(T);
   set_smem_limit_once((const void*)k_zline_seg<T, kZSeg, kZSegRows>, (int)sm);
   dim3 block(32, kZSeg, 1);

@@ -15,6 +15,8 @@ namespace anel {
 static inline int imax(int a, int b) { return a > b ? a : b; }
 int zline_segment_factors(int n, int P, const std::vector<double>& sub, const std::vector<double>& dia,
                           const std::vector<double>& sup, std::vector<double>& out);
+int zline_cr_factors(int n, int S, const std::vector<double>& sub, const std::vector<double>& dia,
+                     const std::vector<double>& sup, std::vector<double>& out);
 
 // ------------------------------------------------------------------ init
 MGSolver* MGSolver::create(const anel_grid_desc* g, const anel_mg_params* p, int device,
@@ -197,8 +199,16 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
       // (the kernel indexes a segment's rows with 32-bit offsets m * X * Y)
       if (mixed && nz % kZSeg == 0 && nz >= 2 * kZSeg && nz <= kZSeg * kZSegRows &&
           (int64_t)(nz / kZSeg + 1) * geo_[l].X * geo_[l].Y < (int64_t)1 << 31)
+      {
         ANEL_CUDA_TRY(cudaMalloc(&d_zseg32_[l], (4 * (size_t)geo_[l].Z + 4 * kZSeg * kZSeg) *
                                                     sizeof(float)));
+        if (nz <= kCRMaxRows) {
+          int st = 0;
+          while ((1 << st) < nz) ++st;
+          zcr_steps_[l] = st;
+          ANEL_CUDA_TRY(cudaMalloc(&d_zcr32_[l], (2 * (size_t)st + 1) * nz * sizeof(float)));
+        }
+      }
     }
     if (mixed) {
       ANEL_CUDA_TRY(cudaMalloc(&d_phi32_[l], G * sizeof(float)));
@@ -246,6 +256,7 @@ MGSolver::~MGSolver() {
     cudaFree(d_ljc32_[l]);
     cudaFree(d_zf32_[l]);
     cudaFree(d_zseg32_[l]);
+    cudaFree(d_zcr32_[l]);
     cudaFree(d_gtab32_[l]);
     cudaFree(d_img32_[l]);
   }
@@ -615,6 +626,14 @@ int MGSolver::build_zline_factors() {
       for (int q = 0; q < 4 * kZSeg * kZSeg; ++q) f32[4 * (size_t)G.Z + q] = (float)seg[4 * (size_t)n + q];
       ANEL_CUDA_TRY(cudaMemcpy(d_zseg32_[l], f32.data(), f32.size() * sizeof(float),
                                cudaMemcpyHostToDevice));
+      if (d_zcr32_[l]) {
+        std::vector<double> cr;
+        const int st2 = zline_cr_factors(n, zcr_steps_[l], sub, dia, sup, cr);
+        if (st2 != ANEL_OK) return st2;
+        std::vector<float> c32(cr.begin(), cr.end());
+        ANEL_CUDA_TRY(cudaMemcpy(d_zcr32_[l], c32.data(), c32.size() * sizeof(float),
+                                 cudaMemcpyHostToDevice));
+      }
     }
   }
   return ANEL_OK;
@@ -629,6 +648,50 @@ int MGSolver::build_zline_factors() {
 //           (u, coupling -sub[lo]) and in the row after it (v, -sup[hi-1]);
 //   minv    inverse of I - K, K coupling the interface unknowns
 //           (F_0, L_0, F_1, L_1, ...) = first/last row of each segment.
+// Multipliers of parallel cyclic reduction for the tridiagonal system
+// (sub, dia, sup) of n rows (sub[0] and sup[n-1] unused): for steps
+// q = 0..S-1 (stride 2^q) alpha_q[r] = -a_r / b_(r-2^q) and gamma_q[r] =
+// -c_r / b_(r+2^q) of the current reduced system (0 past either end), then
+// the reciprocal of the final diagonal.  out = alpha_0, gamma_0, ...,
+// alpha_(S-1), gamma_(S-1), 1/b, n values each.
+int zline_cr_factors(int n, int S, const std::vector<double>& sub, const std::vector<double>& dia,
+                     const std::vector<double>& sup, std::vector<double>& out) {
+  out.assign((2 * (size_t)S + 1) * n, 0.0);
+  std::vector<double> a(sub), b(dia), c(sup), na(n), nb(n), nc(n);
+  a[0] = 0.0;
+  c[n - 1] = 0.0;
+  for (int q = 0; q < S; ++q) {
+    const int st = 1 << q;
+    double* al = out.data() + (size_t)(2 * q) * n;
+    double* ga = al + n;
+    for (int r = 0; r < n; ++r) {
+      const bool lo = r - st >= 0, hi = r + st < n;
+      al[r] = lo ? -a[r] / b[r - st] : 0.0;
+      ga[r] = hi ? -c[r] / b[r + st] : 0.0;
+      nb[r] = b[r] + (lo ? al[r] * c[r - st] : 0.0) + (hi ? ga[r] * a[r + st] : 0.0);
+      na[r] = lo ? al[r] * a[r - st] : 0.0;
+      nc[r] = hi ? ga[r] * c[r + st] : 0.0;
+    }
+    a.swap(na);
+    b.swap(nb);
+    c.swap(nc);
+  }
+  double* rb = out.data() + (size_t)(2 * S) * n;
+  for (int r = 0; r < n; ++r) {
+    if (!(std::isfinite(b[r]) && b[r] != 0.0)) {
+      set_error("z-line cyclic reduction is singular at row %d", r);
+      return ANEL_ERR_NONFINITE;
+    }
+    rb[r] = 1.0 / b[r];
+  }
+  for (double v : out)
+    if (!std::isfinite(v)) {
+      set_error("z-line cyclic reduction multipliers are not finite");
+      return ANEL_ERR_NONFINITE;
+    }
+  return ANEL_OK;
+}
+
 int zline_segment_factors(int n, int P, const std::vector<double>& sub, const std::vector<double>& dia,
                           const std::vector<double>& sup, std::vector<double>& out) {
   const int m = n / P;
@@ -955,6 +1018,8 @@ SegFac<float> MGSolver::segfac32(int l) const {
   f.img = d_img32_[l];
   f.z1 = zcode_[l][0];
   f.zZ = zcode_[l][1];
+  f.cr = d_zcr32_[l];
+  f.crs = zcr_steps_[l];
   return f;
 }
 

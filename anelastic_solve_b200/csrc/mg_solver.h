@@ -99,6 +99,10 @@ class MGSolver {
   // then the 2P x 2P interface inverse), null where the level's nz does
   // not split into kZSeg segments of at least two rows
   float* d_zseg32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  // cyclic-reduction multipliers of the FP32 line matrix (see SegFac::cr),
+  // on the levels that have partitioned factors and nz <= kCRMaxRows
+  float* d_zcr32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  int zcr_steps_[ANEL_MAX_LEVELS + 1] = {};
   // ghost tables of the FP32 levels under the homogeneous rule
   int2* d_gtab32_[ANEL_MAX_LEVELS + 1] = {nullptr};
   // ghost copies done by the partitioned z-line sweep itself (null: the
