@@ -208,21 +208,36 @@ def test_zline_solve_bitwise(name, stop):
     np.testing.assert_array_equal(to_host(dphi), ref)
 
 
-def test_zline_mixed_precision():
-    g = G.shear_layer_grid(32, 16, 32, stretched=True)
+# Mixed-precision ZLINE solves.  A level with at most 512 lines of a colour
+# is swept by cyclic reduction (one CTA per line), a larger one by the
+# partitioned solver: 32x16x32 has 256 lines on its finest level (cyclic
+# reduction on every level); 64x32x64 and 64x32x256 have 1024 there
+# (partitioned on the finest level, segments of 4 and 16 rows; cyclic
+# reduction below).
+ZMIX = {
+    "cr_32x16x32": ((32, 16, 32), (5, 4, 1), 24),
+    "seg_64x32x64": ((64, 32, 64), (6, 5, 1), 30),
+    "seg_64x32x256": ((64, 32, 256), (6, 5, 1), 30),
+}
+
+
+@pytest.mark.parametrize("name", list(ZMIX))
+def test_zline_mixed_precision(name):
+    (nx, ny, nz), lv, max_it = ZMIX[name]
+    g = G.shear_layer_grid(nx, ny, nz, stretched=True)
     rng = np.random.default_rng(22)
     src = compatible(field(g, rng), g, abi.MODE_METRIC)
-    po = mg_params(g, levels=(5, 4, 1), mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE,
+    po = mg_params(g, levels=lv, mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE,
                    maxcy=100, tolmax=1e-13, stop=abi.STOP_RESID)
     ref = zeros(g)
     OracleMG(g, po).solve(ref, src.copy(order="F"))
-    pm = mg_params(g, levels=(5, 4, 1), mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE,
+    pm = mg_params(g, levels=lv, mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE,
                    maxcy=60, tolmax=1e-12, stop=abi.STOP_RESID, precision=abi.PREC_MIXED)
     s = MGSolver(g, pm)
     dphi = to_dev(zeros(g))
     s.solve(dphi, to_dev(src))
     assert s.last_report.status == abi.OK and s.last_report.resid <= 1e-12
-    assert s.last_report.iter <= 24
+    assert s.last_report.iter <= max_it
     assert rel_l2(remove_mean(to_host(dphi)), remove_mean(ref)) < 1e-9
 
 
