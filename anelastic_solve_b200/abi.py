@@ -169,7 +169,14 @@ class StepReport(C.Structure):
                 ("time", C.c_double), ("mg_relmax", C.c_double * 3), ("max_div", C.c_double),
                 ("avg_div", C.c_double), ("ms", C.c_double), ("mg_ms", C.c_double),
                 ("launches", C.c_int64), ("fine_sweeps", C.c_int32), ("reserved", C.c_int32),
-                ("fine_sweep_ms", C.c_double)]
+                ("fine_sweep_ms", C.c_double), ("diag_ms", C.c_double)]
+
+
+# plane statistics of the driver's dk/dt block (NSsolver.F90:288-395)
+DIAG_LITERAL = 0    # center_velocity's stretched-axis interpolation as written
+DIAG_CORRECTED = 1  # the same 5-point interpolation of the values over the coordinates
+DIAG_NAMES = ["U1", "U2", "T", "S", "MKE", "TKE", "t2", "s2",
+              "dU1dt", "dU2dt", "dTdt", "dSdt", "dMKEdt", "dkdt", "dt2dt", "ds2dt"]
 
 
 def free_slip_bcs(p: NSParams, rho_value=(0.0, 0.0)):

@@ -215,6 +215,25 @@ int anel_ns_ctx_set_clock(anel_ns_ctx* ctx, double time, int32_t nstep) {
   return ANEL_OK;
 }
 
+int anel_ns_ctx_set_diagnostics(anel_ns_ctx* ctx, int32_t on, int32_t mode, const int32_t* stretched) {
+  if (!ctx) return ANEL_ERR_ARG;
+  int str[3] = {0, 0, 1};
+  if (stretched)
+    for (int d = 0; d < 3; ++d) str[d] = stretched[d];
+  return ctx->s->set_diagnostics(on, mode, str);
+}
+
+int anel_ns_ctx_compute_diagnostics(anel_ns_ctx* ctx, void* stream) {
+  if (!ctx) return ANEL_ERR_ARG;
+  return ctx->s->compute_diagnostics(static_cast<cudaStream_t>(stream));
+}
+
+int anel_ns_ctx_get_diagnostics(anel_ns_ctx* ctx, double* out, int32_t mem) {
+  if (!ctx || !out) return ANEL_ERR_ARG;
+  if (mem != ANEL_MEM_HOST && mem != ANEL_MEM_DEVICE) return ANEL_ERR_ARG;
+  return ctx->s->get_diagnostics(out, mem);
+}
+
 int anel_ns_ctx_divergence(anel_ns_ctx* ctx, double* out) {
   if (!ctx || !out) return ANEL_ERR_ARG;
   return ctx->s->divergence(nullptr, out);

@@ -898,6 +898,154 @@ void launch_sgs(const NSDev& D, const ZRule& cfluc, cudaStream_t s) {
   launch_images(D, D.nuT, D.kT, D.nT, s);
 }
 
+// ------------------------------------------------------ plane statistics
+// The driver's per-step dk/dt block (NSsolver.F90:288-395).
+
+// Newton form through five points (divdiffs + interpoly,
+// StatTools.F90:563-653) of y over the abscissae x, evaluated at loc.
+__device__ __forceinline__ double newton5(const double (&x)[5], const double (&y)[5], double loc) {
+  double Dm[5][5];
+#pragma unroll
+  for (int k = 0; k <= 4; ++k) Dm[k][0] = y[k];
+#pragma unroll
+  for (int j = 1; j <= 4; ++j)
+#pragma unroll
+    for (int k = j; k <= 4; ++k) Dm[k][j] = (Dm[k][j - 1] - Dm[k - 1][j - 1]) / (x[k] - x[k - j]);
+  double sum1 = Dm[4][4];
+#pragma unroll
+  for (int k = 3; k >= 0; --k) sum1 = sum1 * (loc - x[k]) + Dm[k][k];
+  return sum1;
+}
+
+// center_velocity (StatTools.F90:87-289) of the component staggered in
+// direction dir, interior cells: the mean of the two faces on a uniform
+// axis; on a stretched one interpoly(dep, ind, loc, 4) over the window
+// q-2..q+2 (sx-1..sx+3 at sx, ex-3..ex+1 at ex).  As written (corrected =
+// 0) interpoly hands the values to divdiffs as the abscissae; corrected
+// interpolates the values over the coordinates.  e, c: the edge and
+// centre coordinates of the axis.
+__global__ void k_center(NSDev D, const double* __restrict__ in, double* __restrict__ out, int dir,
+                         int stretched, int corrected, const double* __restrict__ e,
+                         const double* __restrict__ c) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > D.nx + 1) return;
+  const int64_t o = NS_IX(i, j, k);
+  const int64_t st = dir == 1 ? 1 : (dir == 2 ? (int64_t)D.X : D.XY);
+  if (!stretched) {
+    out[o] = R12 * (in[o] + in[o - st]);
+    return;
+  }
+  const int q = dir == 1 ? i : (dir == 2 ? j : k);
+  const int n = dir == 1 ? D.nx : (dir == 2 ? D.ny : D.nz);
+  const int lo = q == 2 ? 1 : (q == n + 1 ? n - 2 : q - 2);
+  double dep[5], ind[5];
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    dep[m] = in[o + (int64_t)(lo + m - q) * st];
+    ind[m] = e[lo + m - 1];
+  }
+  out[o] = corrected ? newton5(ind, dep, c[q - 1]) : newton5(dep, ind, c[q - 1]);
+}
+
+// Squared fluctuation (a - mean(k))^2 on the interior (NSsolver.F90:316-
+// 352, 364-393); the ghost pass of the field's rule that follows rebuilds
+// every ghost cell from the interior, as avgX1X2's ghost call does.
+__global__ void k_fluct_sq(NSDev D, const double* __restrict__ a, const double* __restrict__ mean,
+                           double* __restrict__ out) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > D.nx + 1) return;
+  const int64_t o = NS_IX(i, j, k);
+  const double t = a[o] - mean[k - 1];
+  out[o] = t * t;
+}
+
+// avgX1X2 (Average.F90:279-368) for cell-centred types: per plane k = 1..Z
+// the sum of a(i,j,k)*dxc(i)*dyc(j) over the interior (i,j), as
+// kPlaneBlocks partial sums per plane (block b takes rows j = 2+b, 2+b+B,
+// ...), then a fixed-order fold divided by Area.  Deterministic for a
+// given grid; the order differs from the reference's single running sum.
+constexpr int kPlaneBlocks = 32;
+constexpr int kPlaneThreads = 256;
+__global__ void __launch_bounds__(kPlaneThreads) k_plane_part(NSDev D, const double* __restrict__ a,
+                                                             const double* __restrict__ wx,
+                                                             const double* __restrict__ wy,
+                                                             double* __restrict__ part) {
+  __shared__ double sh[kPlaneThreads / 32];
+  const int k = 1 + blockIdx.y;
+  double acc = 0.0;
+  for (int j = 2 + blockIdx.x; j <= D.ny + 1; j += gridDim.x) {
+    const double wyj = wy[j - 1];
+    const int64_t base = NS_IX(0, j, k);
+    for (int i = 2 + threadIdx.x; i <= D.nx + 1; i += blockDim.x) acc += a[base + i] * wx[i - 1] * wyj;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kPlaneThreads / 32; ++w) t += sh[w];
+    part[(int64_t)(k - 1) * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+__global__ void k_plane_fold(int Z, int nb, const double* __restrict__ part, double area,
+                             double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= Z) return;
+  double t = 0.0;
+  for (int b = 0; b < nb; ++b) t += part[(int64_t)k * nb + b];
+  out[k] = t / area;
+}
+
+// The profile bookkeeping of the block: m = plane means (uc, vc, rho,
+// scal1, wc) then second moments (u'u', v'v', w'w', t't', s's'), Z each;
+// dg = U1, U2, T, S, MKE, TKE, t2, s2 (previous values in, new out), then
+// their derivatives (new - old) / dtt.
+__global__ void k_diag_update(int Z, double dtt, const double* __restrict__ m, double* __restrict__ dg) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= Z) return;
+  const double m1 = m[k], m2 = m[Z + k], m3 = m[2 * Z + k], m4 = m[3 * Z + k];
+  const double uu = m[5 * Z + k], vv = m[6 * Z + k], ww = m[7 * Z + k];
+  const double tt = m[8 * Z + k], ss = m[9 * Z + k];
+  const double tr = m1 + m2;
+  const double tke = 1.0 / 2.0 * (uu + vv + ww);
+  const double now[8] = {m1, m2, m3, m4, tr, tke, tt, ss};
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    dg[(8 + q) * Z + k] = (now[q] - dg[q * Z + k]) / dtt;
+    dg[q * Z + k] = now[q];
+  }
+}
+
+void launch_center(const NSDev& D, const double* in, double* out, int dir, int stretched, int corrected,
+                   const double* e, const double* c, cudaStream_t s) {
+  k_center<<<cell_grid(D, 128), 128, 0, s>>>(D, in, out, dir, stretched, corrected, e, c);
+  count_launch();
+}
+
+void launch_fluct_sq(const NSDev& D, const double* a, const double* mean, double* out, cudaStream_t s) {
+  k_fluct_sq<<<cell_grid(D, 128), 128, 0, s>>>(D, a, mean, out);
+  count_launch();
+}
+
+int64_t plane_part_doubles(const NSDev& D) { return (int64_t)kPlaneBlocks * D.Z; }
+
+void launch_plane_avg(const NSDev& D, const double* a, const double* wx, const double* wy, double area,
+                      double* part, double* out, cudaStream_t s) {
+  k_plane_part<<<dim3(kPlaneBlocks, (unsigned)D.Z), kPlaneThreads, 0, s>>>(D, a, wx, wy, part);
+  k_plane_fold<<<(D.Z + 127) / 128, 128, 0, s>>>(D.Z, kPlaneBlocks, part, area, out);
+  count_launch(2);
+}
+
+void launch_diag_update(int Z, double dtt, const double* m, double* dg, cudaStream_t s) {
+  k_diag_update<<<(Z + 127) / 128, 128, 0, s>>>(Z, dtt, m, dg);
+  count_launch();
+}
+
 // Park-Miller minimal standard: element n (0-based) of the sequence of a
 // seed is seed * 16807^(n+1) mod (2^31-1) (Park & Miller, CACM 31(10),
 // 1988); the power by binary exponentiation, products below 2^62.

@@ -37,6 +37,16 @@ void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, c
 void launch_ghost_field(const NSDev& D, double* a, const ZRule& R, cudaStream_t s);
 void launch_cfl_max(const NSDev& D, unsigned long long* out, cudaStream_t s);
 int64_t divergence_blocks(const NSDev& D);
+// plane statistics (NSsolver.F90:288-395): center_velocity of one
+// component, squared fluctuations, weighted x-y plane averages of every
+// plane (part: plane_part_doubles scratch) and the profile update
+void launch_center(const NSDev& D, const double* in, double* out, int dir, int stretched, int corrected,
+                   const double* e, const double* c, cudaStream_t s);
+void launch_fluct_sq(const NSDev& D, const double* a, const double* mean, double* out, cudaStream_t s);
+int64_t plane_part_doubles(const NSDev& D);
+void launch_plane_avg(const NSDev& D, const double* a, const double* wx, const double* wy, double area,
+                      double* part, double* out, cudaStream_t s);
+void launch_diag_update(int Z, double dtt, const double* m, double* dg, cudaStream_t s);
 void launch_divergence(const NSDev& D, unsigned long long* mx, double* part, cudaStream_t s);
 
 }  // namespace anel

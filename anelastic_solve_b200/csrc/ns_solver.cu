@@ -41,6 +41,13 @@ NSSolver::~NSSolver() {
   if (h_red_) cudaFreeHost(h_red_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
+  cudaFree(d_diag_);
+  cudaFree(d_dgA_);
+  cudaFree(d_dgB_);
+  cudaFree(d_dgm_);
+  cudaFree(d_dgpart_);
+  if (dev0_) cudaEventDestroy(dev0_);
+  if (dev1_) cudaEventDestroy(dev1_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -497,7 +504,9 @@ int NSSolver::reset(const anel_ns_params* ns, cudaStream_t s) {
   D_.scal1_on = ns->scal1_on;
   for (double& r : cn_rkdt_) r = -1.0;  // the CN factors depend on Re, Pr, Sc
   time_ = 0.0;
+  told_ = 1.0e-16;
   nstep_ = 1;
+  if (d_diag_) ANEL_CUDA_TRY(cudaMemsetAsync(d_diag_, 0, 26 * (size_t)(nz_ + 2) * sizeof(double), s));
   for (int q = 8; q < 17; ++q)
     if (d_fields_[q]) ANEL_CUDA_TRY(cudaMemsetAsync(d_fields_[q], 0, G_ * sizeof(double), s));
   if (d_les_) ANEL_CUDA_TRY(cudaMemsetAsync(d_les_, 0, 4 * (size_t)(nz_ + 2) * sizeof(double), s));
@@ -582,6 +591,7 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   static const double A3[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
   anel_step_report r{};
   acc_mg_ms_ = acc_sweep_ms_ = 0.0;
+  acc_diag_ms_ = 0.0;
   acc_sweeps_ = 0;
   const int64_t launches0 = t_launches;
   ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
@@ -609,7 +619,20 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
       st = substep(A1[q], 1.0, A3[q], DTR[q], delt, s, &r.mg_iter[q], &r.mg_relmax[q], true);
       if (st != ANEL_OK) return st;
     }
+    told_ = time_;  // told = time; time = time + delt (NSsolver.F90:272-274)
     time_ = time_ + delt;
+    if (diag_on_) {
+      st = ensure_diag();
+      if (st != ANEL_OK) return st;
+      ANEL_CUDA_TRY(cudaEventRecord(dev0_, s));
+      st = compute_diagnostics(s);
+      if (st != ANEL_OK) return st;
+      ANEL_CUDA_TRY(cudaEventRecord(dev1_, s));
+      ANEL_CUDA_TRY(cudaEventSynchronize(dev1_));
+      float dms = 0.f;
+      cudaEventElapsedTime(&dms, dev0_, dev1_);
+      acc_diag_ms_ += dms;
+    }
     r.nstep = nstep_;
     r.dt = delt;
     r.time = time_;
@@ -623,6 +646,7 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   r.mg_ms = acc_mg_ms_;
   r.fine_sweep_ms = acc_sweep_ms_;
   r.fine_sweeps = acc_sweeps_;
+  r.diag_ms = acc_diag_ms_;
   r.launches = t_launches - launches0;
   double dv[2];
   const int st = divergence(s, dv);
@@ -630,6 +654,122 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   r.avg_div = dv[0];
   r.max_div = dv[1];
   if (rep) *rep = r;
+  return ANEL_OK;
+}
+
+// --------------------------------------------------- plane statistics
+int NSSolver::set_diagnostics(int on, int mode, const int* stretched) {
+  if (mode != ANEL_DIAG_LITERAL && mode != ANEL_DIAG_CORRECTED) {
+    set_error("diagnostics mode must be ANEL_DIAG_LITERAL or ANEL_DIAG_CORRECTED");
+    return ANEL_ERR_ARG;
+  }
+  const int n[3] = {nx_, ny_, nz_};
+  for (int d = 0; d < 3; ++d) {
+    const int v = stretched ? stretched[d] : (d == 2);
+    if (v && n[d] < 4) {
+      set_error("a stretched axis needs at least 4 cells for center_velocity's 5-point window");
+      return ANEL_ERR_SIZE;
+    }
+    diag_str_[d] = v ? 1 : 0;
+  }
+  diag_mode_ = mode;
+  diag_on_ = on != 0;
+  return ANEL_OK;
+}
+
+int NSSolver::ensure_diag() {
+  if (d_diag_) return ANEL_OK;
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  const int X = nx_ + 2, Y = ny_ + 2, Z = nz_ + 2;
+  ANEL_CUDA_TRY(cudaMalloc(&d_diag_, 26 * (size_t)Z * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMemset(d_diag_, 0, 26 * (size_t)Z * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_dgA_, G_ * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_dgB_, G_ * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_dgpart_, (size_t)plane_part_doubles(D_) * sizeof(double)));
+  // dxc[X] dyc[Y] xe[X] xc[X] ye[Y] yc[Y] ze[Z] zc[Z] (m_[d] = xe xc dxe dxc rdxe rdxc)
+  std::vector<double> h;
+  for (const std::vector<double>* v : {&m_[0][3], &m_[1][3], &m_[0][0], &m_[0][1], &m_[1][0], &m_[1][1],
+                                       &m_[2][0], &m_[2][1]})
+    h.insert(h.end(), v->begin(), v->end());
+  ANEL_CUDA_TRY(cudaMalloc(&d_dgm_, h.size() * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMemcpy(d_dgm_, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // Area of avgX1X2 (Average.F90:351-356), summed in its order
+  double area = 0.0;
+  for (int j = 2; j <= ny_ + 1; ++j)
+    for (int i = 2; i <= nx_ + 1; ++i) area = area + m_[0][3][i - 1] * m_[1][3][j - 1];
+  diag_area_ = area;
+  ANEL_CUDA_TRY(cudaEventCreate(&dev0_));
+  ANEL_CUDA_TRY(cudaEventCreate(&dev1_));
+  (void)X;
+  (void)Y;
+  return ANEL_OK;
+}
+
+int NSSolver::compute_diagnostics(cudaStream_t s) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  const int st = ensure_diag();
+  if (st != ANEL_OK) return st;
+  const int X = nx_ + 2, Y = ny_ + 2, Z = nz_ + 2;
+  double* m = d_diag_ + 16 * (size_t)Z;  // plane averages, see k_diag_update
+  const double* dxc = d_dgm_;
+  const double* dyc = dxc + X;
+  const double* ax_e[3] = {dyc + Y, dyc + Y + 2 * X, dyc + 3 * Y + 2 * X};
+  const double* ax_c[3] = {ax_e[0] + X, ax_e[1] + Y, ax_e[2] + Z};
+  const double area = diag_area_;
+  const bool corr = diag_mode_ == ANEL_DIAG_CORRECTED;
+  // u, v, w: centre (then ghost 'u'/'v'/'w'), mean, squared fluctuation
+  // (NSsolver.F90:291-358)
+  const double* vel[3] = {D_.u, D_.v, D_.w};
+  const int vt[3] = {NV_U, NV_V, NV_W};
+  const int mean_slot[3] = {0, 1, 4}, sq_slot[3] = {5, 6, 7};
+  for (int d = 0; d < 3; ++d) {
+    launch_center(D_, vel[d], d_dgA_, d + 1, diag_str_[d], corr, ax_e[d], ax_c[d], s);
+    launch_ghost_field(D_, d_dgA_, zrule(vt[d]), s);
+    double* mean = m + (size_t)mean_slot[d] * Z;
+    launch_plane_avg(D_, d_dgA_, dxc, dyc, area, d_dgpart_, mean, s);
+    launch_fluct_sq(D_, d_dgA_, mean, d_dgB_, s);
+    launch_ghost_field(D_, d_dgB_, zrule(vt[d]), s);
+    launch_plane_avg(D_, d_dgB_, dxc, dyc, area, d_dgpart_, m + (size_t)sq_slot[d] * Z, s);
+  }
+  // rho and scal1: avgX1X2 ghosts the field itself first (:299-300, 364-393)
+  double* sc[2] = {D_.rho, D_.s};
+  const int svt[2] = {NV_RHO, NV_SCAL1};
+  const int smean[2] = {2, 3}, ssq[2] = {8, 9};
+  for (int q = 0; q < 2; ++q) {
+    double* mean = m + (size_t)smean[q] * Z;
+    double* sq = m + (size_t)ssq[q] * Z;
+    if (!sc[q]) {
+      ANEL_CUDA_TRY(cudaMemsetAsync(mean, 0, Z * sizeof(double), s));
+      ANEL_CUDA_TRY(cudaMemsetAsync(sq, 0, Z * sizeof(double), s));
+      continue;
+    }
+    launch_ghost_field(D_, sc[q], zrule(svt[q]), s);
+    launch_plane_avg(D_, sc[q], dxc, dyc, area, d_dgpart_, mean, s);
+    launch_fluct_sq(D_, sc[q], mean, d_dgB_, s);
+    launch_ghost_field(D_, d_dgB_, zrule(svt[q]), s);
+    launch_plane_avg(D_, d_dgB_, dxc, dyc, area, d_dgpart_, sq, s);
+  }
+  launch_diag_update(Z, time_ - told_, m, d_diag_, s);
+  ANEL_CUDA_TRY(cudaGetLastError());
+  return ANEL_OK;
+}
+
+int NSSolver::get_diagnostics(double* out, int mem) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!out) {
+    set_error("null output");
+    return ANEL_ERR_ARG;
+  }
+  const size_t bytes = 16 * (size_t)(nz_ + 2) * sizeof(double);
+  if (!d_diag_) {
+    if (mem == ANEL_MEM_DEVICE) ANEL_CUDA_TRY(cudaMemset(out, 0, bytes));
+    else std::memset(out, 0, bytes);
+    return ANEL_OK;
+  }
+  ANEL_CUDA_TRY(cudaStreamSynchronize(stream_));
+  ANEL_CUDA_TRY(cudaMemcpy(out, d_diag_, bytes,
+                           mem == ANEL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
   return ANEL_OK;
 }
 

@@ -36,6 +36,12 @@ class NSSolver {
     time_ = time;
     nstep_ = nstep;
   }
+  // Plane statistics of the driver's dk/dt block (NSsolver.F90:288-395):
+  // with on, step() runs it after every step; compute_diagnostics runs it
+  // once on the current fields; get_diagnostics copies the 16 profiles.
+  int set_diagnostics(int on, int mode, const int* stretched);
+  int compute_diagnostics(cudaStream_t s);
+  int get_diagnostics(double* out, int mem);
   MGSolver* mg() { return mg_; }
   cudaStream_t stream() const { return stream_; }
   int64_t cells() const { return (int64_t)nx_ * ny_ * nz_; }
@@ -58,7 +64,23 @@ class NSSolver {
   std::vector<double> rz_, bgz_;
   double rRe_ = 0, rPr_ = 0, rSc_ = 0, g_orig_ = 0, gnow_ = 0;
   double time_ = 0.0;
+  double told_ = 1.0e-16;  // time at the start of the last step (NSsolver.F90:47, 272-273)
   int nstep_ = 1;
+  // plane statistics: 16 profiles + 10 plane averages of Z values, two
+  // G-sized scratch fields, the metrics they use (dxc dyc xe xc ye yc ze
+  // zc) and the plane partial sums; allocated on first use
+  bool diag_on_ = false;
+  int diag_mode_ = ANEL_DIAG_LITERAL;
+  int diag_str_[3] = {0, 0, 0};
+  double diag_area_ = 0.0;
+  double acc_diag_ms_ = 0.0;
+  double* d_diag_ = nullptr;
+  double* d_dgA_ = nullptr;
+  double* d_dgB_ = nullptr;
+  double* d_dgm_ = nullptr;
+  double* d_dgpart_ = nullptr;
+  cudaEvent_t dev0_ = nullptr, dev1_ = nullptr;
+  int ensure_diag();
   MGSolver* mg_ = nullptr;
   NSDev D_{};
   // device allocations

@@ -98,3 +98,22 @@ class NSSolver:
         out = (C.c_double * 2)()
         check(lib().anel_ns_ctx_divergence(self._h, out))
         return out[0], out[1]
+
+    def set_diagnostics(self, on: bool = True, mode: int = abi.DIAG_LITERAL, stretched=(0, 0, 1)):
+        """Run the driver's per-step plane statistics (NSsolver.F90:288-395)
+        after every step(); ``stretched[d]`` marks the axes whose grid file
+        says 'stretched'."""
+        st = (C.c_int32 * 3)(*[int(v) for v in stretched])
+        check(lib().anel_ns_ctx_set_diagnostics(self._h, 1 if on else 0, int(mode), st))
+
+    def compute_diagnostics(self):
+        """One pass of the plane statistics on the current fields."""
+        check(lib().anel_ns_ctx_compute_diagnostics(self._h, None))
+
+    def diagnostics(self) -> dict:
+        """{name: profile of nz+2 values (k = 1..nz+2)} for abi.DIAG_NAMES."""
+        Z = self._desc.nz + 2
+        out = np.zeros(16 * Z)
+        check(lib().anel_ns_ctx_get_diagnostics(self._h, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                                abi.MEM_HOST))
+        return {n: out[q * Z:(q + 1) * Z].copy() for q, n in enumerate(abi.DIAG_NAMES)}

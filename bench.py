@@ -258,7 +258,17 @@ def run_dns(args, rank, world, local_rank):
     s.set_profiling(True)
     prep = s.step(1, stream=h)
     s.set_profiling(False)
+    diag_ms = None
+    if args.diag:
+        # the driver's per-step plane statistics (stretched z, corrected
+        # interpolation), timed by the step report after their own warm-up
+        s.set_diagnostics(True, abi.DIAG_CORRECTED, (0, 0, 1))
+        s.step(1, stream=h)
+        dreps = [s.step(1, stream=h) for _ in range(2)]
+        s.set_diagnostics(False, abi.DIAG_CORRECTED, (0, 0, 1))
+        diag_ms = float(np.mean([r.diag_ms for r in dreps]))
     out = {"N": N, "ms_step": ms_step, "clocks": clk.summary(),
+           "diag_ms_step": diag_ms,
            "launches": int(sum(r.launches for r in reps)),
            "sweeps": int(prep.fine_sweeps),
            "sweep_ms": float(prep.fine_sweep_ms),
@@ -612,6 +622,8 @@ def main():
     ap.add_argument("--serve-steps", type=int, default=10, help="serve: RK3 steps per request")
     ap.add_argument("--workers", type=int, default=8, help="serve: members in flight")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM budget (GB)")
+    ap.add_argument("--diag", action="store_true",
+                    help="dns/les: also time the per-step plane statistics (outside the timed steps)")
     args = ap.parse_args()
     SMOOTHER.update(smoother=args.smoother, pre=args.pre, post=args.post)
     rank = int(os.environ.get("RANK", 0))
@@ -735,6 +747,8 @@ def main():
             "config": config}
     if kind == "dns":
         line["mg_ms_per_step"] = round(r["mg_ms_step"], 3)
+        if r.get("diag_ms_step") is not None:
+            line["diag_ms_per_step"] = round(r["diag_ms_step"], 3)
         line["mg_iters_last_step"] = r["mg_iters"][-1]
         line["dt"] = r["dt"]
         line["max_div"] = r["max_div"]

@@ -248,6 +248,7 @@ typedef struct {
   int32_t fine_sweeps;  /* finest-level smoother launches timed (profiling on) */
   int32_t reserved;
   double fine_sweep_ms; /* their summed device time (profiling on) */
+  double diag_ms;       /* device time of the plane statistics (diagnostics on) */
 } anel_step_report;
 
 typedef struct anel_ns_ctx anel_ns_ctx;
@@ -279,6 +280,30 @@ int anel_ns_ctx_set_clock(anel_ns_ctx* ctx, double time, int32_t nstep);
  * dt = 1, one MG solve starting from p, Pgrad with dt = 1 and the velocity
  * ghost passes. */
 int anel_ns_ctx_project(anel_ns_ctx* ctx, int32_t* mg_iter, double* mg_relmax);
+/* Plane statistics of the driver's per-step dk/dt block
+ * (NSsolver.F90:288-395): cell-centred velocities (center_velocity,
+ * StatTools.F90:87-289), x-y plane averages (avgX1X2, Average.F90:279-368),
+ * the mean profiles U1, U2, T, S and MKE = U1 + U2, the second moments of
+ * the fluctuations (TKE = (<u'u'> + <v'v'> + <w'w'>)/2, t2 = <t't'>,
+ * s2 = <s's'>) and the time derivative of each over the last step
+ * ((new - old)/(time - told)).  The previous profiles start at 0.
+ * stretched[d] = 1 where axis d's grid file says 'stretched': there
+ * center_velocity interpolates over five points.  mode LITERAL keeps the
+ * reference's interpolation as written (StatTools.F90:611-653 hands the
+ * values to divdiffs as abscissae: the inverse interpolant, which divides
+ * by differences of the values and is Inf/NaN where two of them are
+ * equal); CORRECTED interpolates the values over the coordinates.
+ * With on = 1, anel_ns_ctx_step runs the block after every step
+ * (as the reference driver does); the report's diag_ms is its time. */
+enum { ANEL_DIAG_LITERAL = 0, ANEL_DIAG_CORRECTED = 1 };
+enum { ANEL_DIAG_PROFILES = 16 };
+int anel_ns_ctx_set_diagnostics(anel_ns_ctx* ctx, int32_t on, int32_t mode, const int32_t* stretched);
+/* Run the block once on the current fields (between steps). */
+int anel_ns_ctx_compute_diagnostics(anel_ns_ctx* ctx, void* stream);
+/* Copy the 16 profiles of nz+2 values (k = 1..nz+2), in the order U1, U2,
+ * T, S, MKE, TKE, t2, s2, dU1dt, dU2dt, dTdt, dSdt, dMKEdt, dkdt, dt2dt,
+ * ds2dt, to out (mem = ANEL_MEM_HOST or ANEL_MEM_DEVICE). */
+int anel_ns_ctx_get_diagnostics(anel_ns_ctx* ctx, double* out, int32_t mem);
 /* divergence() (Routines.F90:54-183) of the current velocity:
  * out[0] = volume-weighted mean |div|, out[1] = max |div|. */
 int anel_ns_ctx_divergence(anel_ns_ctx* ctx, double* out);

@@ -38,6 +38,9 @@ struct orc_ns {
   double* Ftemp;  /* RHS scratch */
   double *Csgs, *CTsgs, *CSsgs, *delg, *modS;
   double* work[4];
+  double told;    /* time at the start of the last step (NSsolver.F90:272-273) */
+  double* dg;     /* 16 plane-statistics profiles of Z values (orc_ns_diagnostics) */
+  double *dgA, *dgB, *dgC, *dgR; /* their G-sized scratch */
 };
 
 #define IX(i, j, k) (((long)(i) - 1) + D->X * (((long)(j) - 1) + D->Y * ((long)(k) - 1)))
@@ -244,6 +247,7 @@ orc_ns* orc_ns_create(const anel_grid_desc* g, const anel_mg_params* mgp, const 
   s->modS = (double*)calloc(D->G, sizeof(double));
   for (int q = 0; q < 4; ++q) s->work[q] = (double*)calloc(D->G, sizeof(double));
   s->nstep = 1;
+  s->told = 1.0e-16; /* NSsolver.F90:47 */
   return s;
 }
 
@@ -257,6 +261,11 @@ void orc_ns_destroy(orc_ns* s) {
   free(s->delg);
   free(s->modS);
   for (int q = 0; q < 4; ++q) free(s->work[q]);
+  free(s->dg);
+  free(s->dgA);
+  free(s->dgB);
+  free(s->dgC);
+  free(s->dgR);
   free(s);
 }
 
@@ -1103,6 +1112,7 @@ int orc_ns_step(orc_ns* s, anel_step_report* rep) {
     if (les && s->nstep > s->p.les_start) sgsdiff(s);
     orc_ns_substep(s, A1[q], 1.0, A3[q], DTR[q], delt, &it[q], &rm[q]);
   }
+  s->told = s->time; /* told = time; time = time + delt (NSsolver.F90:272-274) */
   s->time = s->time + delt;
   if (rep) {
     rep->nstep = s->nstep;
@@ -1161,4 +1171,179 @@ void orc_ns_divergence(orc_ns* s, double* out) {
       }
   out[0] = sum / vol;
   out[1] = mx;
+}
+
+/* ---------------------------------------------------- plane statistics
+ * The driver's per-step dk/dt block (NSsolver.F90:288-395): cell-centred
+ * velocities (center_velocity, StatTools.F90:87-289), x-y plane averages
+ * (avgX1X2, Average.F90:279-368, summed in its j-outer, i-inner order),
+ * the time derivatives of the mean profiles and of the second moments of
+ * the fluctuations. */
+
+/* divdiffs(x, y, a, 4) (StatTools.F90:563-609): divided differences of y
+ * over the abscissae x. */
+static void divdiffs4(const double* x, const double* y, double* a) {
+  double Dm[5][5];
+  for (int k = 0; k <= 4; ++k) Dm[k][0] = y[k];
+  for (int j = 1; j <= 4; ++j)
+    for (int k = j; k <= 4; ++k) Dm[k][j] = (Dm[k][j - 1] - Dm[k - 1][j - 1]) / (x[k] - x[k - j]);
+  for (int k = 0; k <= 4; ++k) a[k] = Dm[k][k];
+}
+
+/* interpoly(dep, ind, loc, 4) (StatTools.F90:611-653).  As written
+ * (corrected = 0) it passes the values as the abscissae of divdiffs and
+ * steps the Newton form by (loc - dep(k)): the inverse interpolant,
+ * evaluated at a coordinate.  corrected = 1 interpolates dep over ind. */
+static double interpoly4(const double* dep, const double* ind, double loc, int corrected) {
+  const double* x = corrected ? ind : dep;
+  const double* y = corrected ? dep : ind;
+  double a[5];
+  divdiffs4(x, y, a);
+  double sum1 = a[4];
+  for (int k = 3; k >= 0; --k) sum1 = sum1 * (loc - x[k]) + a[k];
+  return sum1;
+}
+
+/* center_velocity(Uin, Ucen, dir) (StatTools.F90:87-289): Ucen = 0, the
+ * interior from the two faces (uniform axis) or the 5-point interpolation
+ * (stretched axis; windows q-2..q+2, sx-1..sx+3 at sx, ex-3..ex+1 at ex),
+ * then ghost(Ucen, 'u' / 'v' / 'w'). */
+static void center_velocity(orc_ns* s, const double* in, double* out, int dir, int stretched,
+                            int corrected) {
+  const orc_dom* D = &s->d;
+  memset(out, 0, sizeof(double) * D->G);
+  const double* e = dir == 1 ? D->xe : (dir == 2 ? D->ye : D->ze);
+  const double* c = dir == 1 ? D->xc : (dir == 2 ? D->yc : D->zc);
+  const int n = dir == 1 ? D->nx : (dir == 2 ? D->ny : D->nz);
+  const long st = dir == 1 ? 1 : (dir == 2 ? D->X : D->X * D->Y);
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i) {
+        const long o = IX(i, j, k);
+        const int q = dir == 1 ? i : (dir == 2 ? j : k);
+        if (!stretched) {
+          out[o] = R12 * (in[o] + in[o - st]);
+        } else {
+          const int lo = q == 2 ? 1 : (q == n + 1 ? n - 2 : q - 2);
+          double dep[5], ind[5];
+          for (int m = 0; m < 5; ++m) {
+            dep[m] = in[o + (long)(lo + m - q) * st];
+            ind[m] = M(e, lo + m);
+          }
+          out[o] = interpoly4(dep, ind, M(c, q), corrected);
+        }
+      }
+  ghost(s, out, dir == 1 ? VT_U : (dir == 2 ? VT_V : VT_W));
+}
+
+/* avgX1X2(Var, outm, vtype) for the cell-centred types (dxc, dyc
+ * weights): ghost(Var, vt), then outm(k) = sum Var*dxc*dyc / Area for
+ * k = sz-1..ez+1. */
+static void avg_x1x2(orc_ns* s, double* var, double* outm, int vt) {
+  const orc_dom* D = &s->d;
+  ghost(s, var, vt);
+  double Area = 0.0;
+  for (int j = 2; j <= D->ny + 1; ++j)
+    for (int i = 2; i <= D->nx + 1; ++i) Area = Area + M(D->dxc, i) * M(D->dyc, j);
+  for (int k = 1; k <= D->Z; ++k) {
+    double rsum = 0.0;
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i) rsum = rsum + A_(var, i, j, k) * M(D->dxc, i) * M(D->dyc, j);
+    outm[k - 1] = rsum / Area;
+  }
+}
+
+/* Fluctuation a - mean(k) on the interior, ghost 'cfluc', squared over
+ * the whole array (NSsolver.F90:316-352, 364-393). */
+static void fluct_sq(orc_ns* s, const double* a, const double* mean, double* out) {
+  const orc_dom* D = &s->d;
+  memcpy(out, a, sizeof(double) * D->G);
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i) A_(out, i, j, k) = A_(out, i, j, k) - mean[k - 1];
+  ghost(s, out, VT_CFLUC);
+  for (long c = 0; c < D->G; ++c) out[c] = out[c] * out[c];
+}
+
+/* One pass of the block on the current fields; out = the 16 profiles
+ * (Z values each, k = 1..Z): U1, U2, T, S, MKE, TKE, t2, s2 (the *_old
+ * arrays after the update), then dU1dt, dU2dt, dTdt, dSdt, dMKEdt, dkdt,
+ * dt2dt, ds2dt.  The *_old arrays start at 0.  stretched[d]: axis d uses
+ * the interpolation of center_velocity. */
+int orc_ns_diagnostics(orc_ns* s, int corrected, const int* stretched, double* out) {
+  const orc_dom* D = &s->d;
+  const long Z = D->Z, G = D->G;
+  for (int d = 0; d < 3; ++d) {
+    const int n = d == 0 ? D->nx : (d == 1 ? D->ny : D->nz);
+    if (stretched[d] && n < 4) return -1;
+  }
+  if (!s->dg) {
+    s->dg = (double*)calloc(16 * Z, sizeof(double));
+    s->dgA = (double*)calloc(G, sizeof(double));
+    s->dgB = (double*)calloc(G, sizeof(double));
+    s->dgC = (double*)calloc(G, sizeof(double));
+    s->dgR = (double*)calloc(G, sizeof(double));
+  }
+  double* U1o = s->dg;
+  double *U2o = U1o + Z, *To = U2o + Z, *So = To + Z, *MKEo = So + Z, *ko = MKEo + Z, *t2o = ko + Z,
+         *s2o = t2o + Z;
+  double *dU1 = s2o + Z, *dU2 = dU1 + Z, *dT = dU2 + Z, *dS = dT + Z, *dMKE = dS + Z, *dk = dMKE + Z,
+         *dt2 = dk + Z, *ds2 = dt2 + Z;
+  double* m = (double*)calloc(10 * Z, sizeof(double));
+  double *m1 = m, *m2 = m + Z, *m3 = m + 2 * Z, *m4 = m + 3 * Z, *mean = m + 4 * Z, *uu = m + 5 * Z,
+         *vv = m + 6 * Z, *ww = m + 7 * Z, *tt = m + 8 * Z, *ss = m + 9 * Z;
+  const double dtt = s->time - s->told;
+  anel_fields* f = &s->f;
+  center_velocity(s, f->u, s->dgA, 1, stretched[0], corrected);
+  center_velocity(s, f->v, s->dgB, 2, stretched[1], corrected);
+  center_velocity(s, f->w, s->dgC, 3, stretched[2], corrected);
+  avg_x1x2(s, s->dgA, m1, VT_U);
+  avg_x1x2(s, s->dgB, m2, VT_V);
+  avg_x1x2(s, f->rho, m3, VT_RHO);
+  avg_x1x2(s, f->scal1, m4, VT_SCAL1);
+  for (long k = 0; k < Z; ++k) {
+    dU1[k] = (m1[k] - U1o[k]) / dtt;
+    U1o[k] = m1[k];
+    dU2[k] = (m2[k] - U2o[k]) / dtt;
+    U2o[k] = m2[k];
+    dT[k] = (m3[k] - To[k]) / dtt;
+    To[k] = m3[k];
+    dS[k] = (m4[k] - So[k]) / dtt;
+    So[k] = m4[k];
+    const double tr = m1[k] + m2[k];
+    dMKE[k] = (tr - MKEo[k]) / dtt;
+    MKEo[k] = tr;
+  }
+  /* u', v', w' and their squares */
+  const int vts[3] = {VT_U, VT_V, VT_W};
+  double* cen[3] = {s->dgA, s->dgB, s->dgC};
+  double* sq[3] = {uu, vv, ww};
+  for (int d = 0; d < 3; ++d) {
+    avg_x1x2(s, cen[d], mean, vts[d]);
+    fluct_sq(s, cen[d], mean, s->dgR);
+    avg_x1x2(s, s->dgR, sq[d], vts[d]);
+  }
+  for (long k = 0; k < Z; ++k) {
+    const double tke = 1.0 / 2.0 * (uu[k] + vv[k] + ww[k]);
+    dk[k] = (tke - ko[k]) / dtt;
+    ko[k] = tke;
+  }
+  /* t' and s' */
+  avg_x1x2(s, f->rho, mean, VT_RHO);
+  fluct_sq(s, f->rho, mean, s->dgR);
+  avg_x1x2(s, s->dgR, tt, VT_RHO);
+  for (long k = 0; k < Z; ++k) {
+    dt2[k] = (tt[k] - t2o[k]) / dtt;
+    t2o[k] = tt[k];
+  }
+  avg_x1x2(s, f->scal1, mean, VT_SCAL1);
+  fluct_sq(s, f->scal1, mean, s->dgR);
+  avg_x1x2(s, s->dgR, ss, VT_SCAL1);
+  for (long k = 0; k < Z; ++k) {
+    ds2[k] = (ss[k] - s2o[k]) / dtt;
+    s2o[k] = ss[k];
+  }
+  memcpy(out, s->dg, sizeof(double) * 16 * Z);
+  free(m);
+  return 0;
 }

@@ -118,6 +118,8 @@ def _ns_lib():
         L.orc_ns_project.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.orc_ns_divergence.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         L.orc_ns_ghost.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
+        L.orc_ns_diagnostics.restype = C.c_int
+        L.orc_ns_diagnostics.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L._ns_ready = True
     return L
 
@@ -174,3 +176,16 @@ class OracleNS:
 
     def ghost(self, a, vt: int):
         _ns_lib().orc_ns_ghost(self._h, abi.dptr(_f(a)), vt)
+
+    def diagnostics(self, mode: int = abi.DIAG_LITERAL, stretched=(0, 0, 1)) -> dict:
+        """The driver's per-step plane statistics (NSsolver.F90:288-395) on
+        the current fields: {name: profile of nz+2 values} for
+        abi.DIAG_NAMES."""
+        Z = self._desc.nz + 2
+        out = np.zeros(16 * Z)
+        st = (C.c_int * 3)(*[int(v) for v in stretched])
+        r = _ns_lib().orc_ns_diagnostics(self._h, int(mode == abi.DIAG_CORRECTED), st,
+                                         out.ctypes.data_as(C.POINTER(C.c_double)))
+        if r != 0:
+            raise ValueError("a stretched axis needs at least 4 cells")
+        return {n: out[q * Z:(q + 1) * Z].copy() for q, n in enumerate(abi.DIAG_NAMES)}
