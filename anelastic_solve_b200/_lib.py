@@ -49,6 +49,12 @@ SIGNATURES = {
     "anel_ns_ctx_set_diagnostics": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "anel_ns_ctx_compute_diagnostics": (C.c_int, [_P, _P]),
     "anel_ns_ctx_get_diagnostics": (C.c_int, [_P, _DP, C.c_int32]),
+    "anel_restart_write": (C.c_int, [C.c_char_p, C.c_int32, _P, C.c_int32, C.c_int32, C.c_int32,
+                                     C.POINTER(_DP)]),
+    "anel_restart_read": (C.c_int, [C.c_char_p, C.c_int32, _P, C.c_int32, C.c_int32, C.c_int32,
+                                    C.POINTER(_DP)]),
+    "anel_ns_ctx_write_restart": (C.c_int, [_P, C.c_char_p, C.c_int32, _P]),
+    "anel_ns_ctx_read_restart": (C.c_int, [_P, C.c_char_p, C.c_int32, C.c_int32, _P]),
     "anel_serve_create": (_P, [C.c_int32, C.c_int64, C.c_int32, _IP]),
     "anel_serve_submit": (C.c_int, [_P, C.POINTER(abi.Request), C.POINTER(C.c_int64)]),
     "anel_serve_poll": (C.c_int, [_P, C.POINTER(abi.Result), C.c_int32, _IP, C.c_int32]),

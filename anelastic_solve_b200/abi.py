@@ -172,6 +172,18 @@ class StepReport(C.Structure):
                 ("fine_sweep_ms", C.c_double), ("diag_ms", C.c_double)]
 
 
+class RestartHeader(C.Structure):
+    """Header record of a restart file (Restart.F90 write_flow_*)."""
+    _fields_ = [("nstep", C.c_int32), ("time", C.c_double), ("delt", C.c_double), ("g", C.c_double),
+                ("rho_0", C.c_double), ("scal1_0", C.c_double), ("Re", C.c_double), ("Pr", C.c_double),
+                ("Sc", C.c_double)]
+
+
+RESTART_SMALL = 0  # serial dump (write_flow_small / Greadfile)
+RESTART_BIG = 1    # one rank's file (write_flow_big / start_big)
+RESTART_FIELDS = ("u", "v", "w", "p", "rho", "scal1")
+
+
 # plane statistics of the driver's dk/dt block (NSsolver.F90:288-395)
 DIAG_LITERAL = 0    # center_velocity's stretched-axis interpolation as written
 DIAG_CORRECTED = 1  # the same 5-point interpolation of the values over the coordinates

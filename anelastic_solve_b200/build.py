@@ -32,6 +32,7 @@ SOURCES = {
     "ns_solver.cu": ["-fmad=false"],
     "noalloc.cu": ["-fmad=false"],
     "serve.cu": ["-fmad=false"],
+    "restart.cu": ["-fmad=false"],
 }
 
 

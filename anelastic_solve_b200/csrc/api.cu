@@ -47,9 +47,6 @@ int check_launch(const char* what) {
 struct anel_mg_ctx {
   anel::MGSolver* s;
 };
-struct anel_ns_ctx {
-  anel::NSSolver* s;
-};
 
 namespace {
 std::mutex g_default_mu;

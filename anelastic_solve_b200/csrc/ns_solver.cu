@@ -657,6 +657,17 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   return ANEL_OK;
 }
 
+int NSSolver::ghost_state(cudaStream_t s) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  double* f[6] = {D_.u, D_.v, D_.w, D_.p, D_.rho, D_.s};
+  const int vt[6] = {NV_U, NV_V, NV_W, NV_P, NV_RHO, NV_SCAL1};
+  for (int q = 0; q < 6; ++q)
+    if (f[q]) launch_ghost_field(D_, f[q], zrule(vt[q]), s);
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  return ANEL_OK;
+}
+
 // --------------------------------------------------- plane statistics
 int NSSolver::set_diagnostics(int on, int mode, const int* stretched) {
   if (mode != ANEL_DIAG_LITERAL && mode != ANEL_DIAG_CORRECTED) {

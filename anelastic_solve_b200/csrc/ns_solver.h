@@ -45,6 +45,15 @@ class NSSolver {
   MGSolver* mg() { return mg_; }
   cudaStream_t stream() const { return stream_; }
   int64_t cells() const { return (int64_t)nx_ * ny_ * nz_; }
+  int64_t ghosted_cells() const { return G_; }
+  void sizes(int* nx, int* ny, int* nz) const {
+    *nx = nx_;
+    *ny = ny_;
+    *nz = nz_;
+  }
+  // ghost() of u, v, w, p, rho and scal1 with their own rules, as after a
+  // restart read (Restart.F90:425-430)
+  int ghost_state(cudaStream_t s);
 
  private:
   NSSolver() = default;
@@ -107,4 +116,13 @@ class NSSolver {
   int acc_sweeps_ = 0;
 };
 
+}  // namespace anel
+
+// The C-ABI handle of a stepper context.
+struct anel_ns_ctx {
+  anel::NSSolver* s;
+};
+
+namespace anel {
+inline NSSolver* ctx_solver(anel_ns_ctx* c) { return c->s; }
 }  // namespace anel

@@ -110,6 +110,24 @@ class NSSolver:
         """One pass of the plane statistics on the current fields."""
         check(lib().anel_ns_ctx_compute_diagnostics(self._h, None))
 
+    def write_restart(self, path, hdr: abi.RestartHeader, layout: int = abi.RESTART_SMALL):
+        """The context's u, v, w, p, rho, scal1 to a restart file in the
+        reference's layout (Restart.F90)."""
+        import os
+
+        check(lib().anel_ns_ctx_write_restart(self._h, os.fsencode(path), int(layout), C.byref(hdr)))
+
+    def read_restart(self, path, layout: int = abi.RESTART_SMALL, icparam: bool = True):
+        """Load a restart file into the context (fields ghosted as the
+        reference's start_small/start_big do); with icparam the clock
+        (time, nstep) comes from the file.  Returns the header."""
+        import os
+
+        h = abi.RestartHeader()
+        check(lib().anel_ns_ctx_read_restart(self._h, os.fsencode(path), int(layout), 1 if icparam else 0,
+                                             C.byref(h)))
+        return h
+
     def diagnostics(self) -> dict:
         """{name: profile of nz+2 values (k = 1..nz+2)} for abi.DIAG_NAMES."""
         Z = self._desc.nz + 2

@@ -304,6 +304,37 @@ int anel_ns_ctx_compute_diagnostics(anel_ns_ctx* ctx, void* stream);
  * T, S, MKE, TKE, t2, s2, dU1dt, dU2dt, dTdt, dSdt, dMKEdt, dkdt, dt2dt,
  * ds2dt, to out (mem = ANEL_MEM_HOST or ANEL_MEM_DEVICE). */
 int anel_ns_ctx_get_diagnostics(anel_ns_ctx* ctx, double* out, int32_t mem);
+/* Restart files in the reference's layout (Restart.F90): Fortran
+ * sequential unformatted records (4-byte little-endian length markers)
+ * holding the header nstep, time, delt, g, rho_0, scal1_0, Re, Pr, Sc; the
+ * extents; then u, v, w, p, rho, scal1, each the whole ghosted array.
+ * SMALL is the serial dump of write_flow_small / Greadfile (extents nx+2,
+ * ny+2, nz+2; file name basename//nstep); BIG is one rank's file of
+ * write_flow_big / start_big (extents sx, ex, sy, ey, sz, ez = 2, nx+1,
+ * 2, ny+1, 2, nz+1 for the single rank; file name
+ * basename//c1_c2_c3.nstep).  Readers refuse other extents
+ * (ANEL_ERR_SIZE) and malformed records; a field record above 2^31-1
+ * bytes is refused. */
+enum { ANEL_RESTART_SMALL = 0, ANEL_RESTART_BIG = 1 };
+typedef struct {
+  int32_t nstep;
+  double time, delt, g, rho_0, scal1_0, Re, Pr, Sc;
+} anel_restart_header;
+/* Host arrays u, v, w, p, rho, scal1 ((nx+2)(ny+2)(nz+2) each, Fortran
+ * order); no GPU involved. */
+int anel_restart_write(const char* path, int32_t layout, const anel_restart_header* hdr, int32_t nx,
+                       int32_t ny, int32_t nz, const double* const* fields);
+int anel_restart_read(const char* path, int32_t layout, anel_restart_header* hdr, int32_t nx, int32_t ny,
+                      int32_t nz, double* const* fields);
+/* The context's fields to / from a restart file.  Reading ghosts the six
+ * fields as start_small / start_big do; icparam = 1 also takes the clock
+ * (time, nstep) from the header, as the reference's icparam does for its
+ * Parameters (Re, Pr, Sc, g are returned in hdr: a context is built with
+ * its physics). */
+int anel_ns_ctx_write_restart(anel_ns_ctx* ctx, const char* path, int32_t layout,
+                              const anel_restart_header* hdr);
+int anel_ns_ctx_read_restart(anel_ns_ctx* ctx, const char* path, int32_t layout, int32_t icparam,
+                             anel_restart_header* hdr);
 /* divergence() (Routines.F90:54-183) of the current velocity:
  * out[0] = volume-weighted mean |div|, out[1] = max |div|. */
 int anel_ns_ctx_divergence(anel_ns_ctx* ctx, double* out);
