@@ -111,6 +111,7 @@ def make_mg_params(levels, maxcy=99, tolmax=1e-10, pre=None, post=None, tbc=(0, 
 # ------------------------------------------------------------------ stepper
 MODEL_DNS = 0
 MODEL_SSM = 1
+MODEL_DSM = 2
 DELTA_3ROOT = 0
 DELTA_2ROOT = 1
 DAMP_LITERAL = 0
@@ -128,7 +129,9 @@ class NSParams(C.Structure):
                 ("smodel", C.c_int32), ("les_delta", C.c_int32), ("les_damp", C.c_int32),
                 ("ssm_const", C.c_double), ("pr_sgs", C.c_double), ("les_start", C.c_int32),
                 ("les_freq", C.c_int32), ("tb", ((C.c_int32 * 8) * 2) * 3),
-                ("vb", ((C.c_double * 8) * 2) * 3), ("ew", C.c_int32), ("scal1_on", C.c_int32)]
+                ("vb", ((C.c_double * 8) * 2) * 3), ("ew", C.c_int32), ("scal1_on", C.c_int32),
+                ("test_ratio", C.c_double), ("filt", C.c_int32 * 3), ("stretched", C.c_int32 * 3),
+                ("interp", C.c_int32), ("reserved2", C.c_int32)]
 
 
 class Fields(C.Structure):
@@ -211,7 +214,9 @@ def free_slip_bcs(p: NSParams, rho_value=(0.0, 0.0)):
 
 def make_ns_params(Re=1000.0, Pr=1.0, Sc=1.0, cfl=1e6, dtmax=0.01, g=-0.12, les=False,
                    ssm_const=0.0289, pr_sgs=0.7, les_start=0, les_freq=1,
-                   les_damp=DAMP_NONE, les_delta=DELTA_3ROOT, ew=1, scal1_on=1) -> NSParams:
+                   les_damp=DAMP_NONE, les_delta=DELTA_3ROOT, ew=1, scal1_on=1, models=None,
+                   test_ratio=2.449489742783178, filt=(1, 1, 1), stretched=(0, 0, 0),
+                   interp=None) -> NSParams:
     """Shear-layer parameters: gravity constant g from t = 0 (Ginit = Gfinal
     = g, GT1 = GT2 = 0), free-slip z walls, periodic x and y."""
     p = NSParams()
@@ -220,7 +225,13 @@ def make_ns_params(Re=1000.0, Pr=1.0, Sc=1.0, cfl=1e6, dtmax=0.01, g=-0.12, les=
     p.g_init = p.g_final = float(g)
     p.gt1 = p.gt2 = 0.0
     m = MODEL_SSM if les else MODEL_DNS
-    p.vmodel = p.rmodel = p.smodel = m
+    p.vmodel, p.rmodel, p.smodel = models if models is not None else (m, m, m)
+    # TestGrid_ratio / xfilter.. of the reference's runfile (run_dir/Sturb.ini:15-18)
+    p.test_ratio = float(test_ratio)
+    for d in range(3):
+        p.filt[d] = int(filt[d])
+        p.stretched[d] = int(stretched[d])
+    p.interp = int(DIAG_LITERAL if interp is None else interp)
     p.les_delta, p.les_damp = int(les_delta), int(les_damp)
     p.ssm_const, p.pr_sgs = float(ssm_const), float(pr_sgs)
     p.les_start, p.les_freq = int(les_start), int(les_freq)

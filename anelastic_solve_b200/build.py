@@ -33,6 +33,7 @@ SOURCES = {
     "noalloc.cu": ["-fmad=false"],
     "serve.cu": ["-fmad=false"],
     "restart.cu": ["-fmad=false"],
+    "ns_dsm.cu": ["-fmad=false"],
 }
 
 

@@ -49,4 +49,30 @@ struct NSDev {
 #define FA(a, i, j, k) (a)[NS_IX(i, j, k)]
 #define MT(a, i) (a)[(i) - 1]
 
+// straincal's strain magnitude (straincal.F90:48-73) of (l1, l2, l3) at an
+// interior cell; x**2.d0 is x*x.
+__device__ __forceinline__ double strain_mag(const NSDev& D, const double* l1, const double* l2,
+                                             const double* l3, int i, int j, int k) {
+  const double TS11 = (FA(l1, i + 1, j, k) - FA(l1, i, j, k)) * MT(D.rdxc, i);
+  const double TS22 = (FA(l2, i, j + 1, k) - FA(l2, i, j, k)) * MT(D.rdyc, j);
+  const double TS33 = (FA(l3, i, j, k + 1) - FA(l3, i, j, k)) * MT(D.rdzc, k);
+  double t1 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j + 1, k) + FA(l1, i + 1, j + 1, k));
+  double t2 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j - 1, k) + FA(l1, i + 1, j - 1, k));
+  double t3 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i + 1, j, k) + FA(l2, i + 1, j + 1, k));
+  double t4 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i - 1, j, k) + FA(l2, i - 1, j + 1, k));
+  const double TS12 = 0.5 * ((t1 - t2) * MT(D.rdyc, j) + (t3 - t4) * MT(D.rdxc, i));
+  t1 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j, k + 1) + FA(l1, i + 1, j, k + 1));
+  t2 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j, k - 1) + FA(l1, i + 1, j, k - 1));
+  t3 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i + 1, j, k) + FA(l3, i + 1, j, k + 1));
+  t4 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i - 1, j, k) + FA(l3, i - 1, j, k + 1));
+  const double TS13 = 0.5 * ((t1 - t2) * MT(D.rdzc, k) + (t3 - t4) * MT(D.rdxc, i));
+  t1 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i, j, k + 1) + FA(l2, i, j + 1, k + 1));
+  t2 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i, j, k - 1) + FA(l2, i, j + 1, k - 1));
+  t3 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i, j + 1, k) + FA(l3, i, j + 1, k + 1));
+  t4 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i, j - 1, k) + FA(l3, i, j - 1, k + 1));
+  const double TS23 = 0.5 * ((t1 - t2) * MT(D.rdzc, k) + (t3 - t4) * MT(D.rdyc, j));
+  return sqrt(2.0) * sqrt(TS11 * TS11 + TS22 * TS22 + TS33 * TS33 + 2.0 * (TS12 * TS12) + 2.0 * (TS13 * TS13) +
+                          2.0 * (TS23 * TS23));
+}
+
 }  // namespace anel

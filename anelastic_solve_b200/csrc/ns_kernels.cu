@@ -684,27 +684,7 @@ __global__ void __launch_bounds__(128) k_sgs(NSDev D) {
   const int j = 2 + blockIdx.y;
   const int k = 2 + blockIdx.z;
   if (i > D.nx + 1) return;
-  const double *l1 = D.u, *l2 = D.v, *l3 = D.w;
-  const double TS11 = (FA(l1, i + 1, j, k) - FA(l1, i, j, k)) * MT(D.rdxc, i);
-  const double TS22 = (FA(l2, i, j + 1, k) - FA(l2, i, j, k)) * MT(D.rdyc, j);
-  const double TS33 = (FA(l3, i, j, k + 1) - FA(l3, i, j, k)) * MT(D.rdzc, k);
-  double t1 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j + 1, k) + FA(l1, i + 1, j + 1, k));
-  double t2 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j - 1, k) + FA(l1, i + 1, j - 1, k));
-  double t3 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i + 1, j, k) + FA(l2, i + 1, j + 1, k));
-  double t4 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i - 1, j, k) + FA(l2, i - 1, j + 1, k));
-  const double TS12 = 0.5 * ((t1 - t2) * MT(D.rdyc, j) + (t3 - t4) * MT(D.rdxc, i));
-  t1 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j, k + 1) + FA(l1, i + 1, j, k + 1));
-  t2 = 0.25 * (FA(l1, i, j, k) + FA(l1, i + 1, j, k) + FA(l1, i, j, k - 1) + FA(l1, i + 1, j, k - 1));
-  t3 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i + 1, j, k) + FA(l3, i + 1, j, k + 1));
-  t4 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i - 1, j, k) + FA(l3, i - 1, j, k + 1));
-  const double TS13 = 0.5 * ((t1 - t2) * MT(D.rdzc, k) + (t3 - t4) * MT(D.rdxc, i));
-  t1 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i, j, k + 1) + FA(l2, i, j + 1, k + 1));
-  t2 = 0.25 * (FA(l2, i, j, k) + FA(l2, i, j + 1, k) + FA(l2, i, j, k - 1) + FA(l2, i, j + 1, k - 1));
-  t3 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i, j + 1, k) + FA(l3, i, j + 1, k + 1));
-  t4 = 0.25 * (FA(l3, i, j, k) + FA(l3, i, j, k + 1) + FA(l3, i, j - 1, k) + FA(l3, i, j - 1, k + 1));
-  const double TS23 = 0.5 * ((t1 - t2) * MT(D.rdzc, k) + (t3 - t4) * MT(D.rdyc, j));
-  const double modS = sqrt(2.0) * sqrt(TS11 * TS11 + TS22 * TS22 + TS33 * TS33 + 2.0 * (TS12 * TS12) +
-                                        2.0 * (TS13 * TS13) + 2.0 * (TS23 * TS23));
+  const double modS = strain_mag(D, D.u, D.v, D.w, i, j, k);
   const double dg2 = D.delg2[k - 1];
   FA(D.nuT, i, j, k) = -(D.Cs[k - 1] + 0.0) * dg2 * modS + 0.0;
   FA(D.kT, i, j, k) = -(D.CTs[k - 1] + 0.0) * dg2 * modS + 0.0;

@@ -46,6 +46,9 @@ NSSolver::~NSSolver() {
   cudaFree(d_dgB_);
   cudaFree(d_dgm_);
   cudaFree(d_dgpart_);
+  cudaFree(d_dyn_);
+  cudaFree(d_dyn_m_);
+  cudaFree(d_dyn_axes_);
   if (dev0_) cudaEventDestroy(dev0_);
   if (dev1_) cudaEventDestroy(dev1_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -82,12 +85,26 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
     }
   }
   for (int m : {ns->vmodel, ns->rmodel, ns->smodel})
-    if (m != ANEL_MODEL_DNS && m != ANEL_MODEL_SSM) {
+    if (m != ANEL_MODEL_DNS && m != ANEL_MODEL_SSM && m != ANEL_MODEL_DSM) {
       set_error("unknown subgrid model %d", m);
       return ANEL_ERR_ARG;
     }
-  les_any_ = ns->vmodel == ANEL_MODEL_SSM || ns->rmodel == ANEL_MODEL_SSM || ns->smodel == ANEL_MODEL_SSM;
-  if (ns->vmodel == ANEL_MODEL_SSM) {
+  les_any_ = ns->vmodel != ANEL_MODEL_DNS || ns->rmodel != ANEL_MODEL_DNS || ns->smodel != ANEL_MODEL_DNS;
+  if (ns->vmodel == ANEL_MODEL_DSM || ns->rmodel == ANEL_MODEL_DSM || ns->smodel == ANEL_MODEL_DSM) {
+    // the test filter's boundary formulas reach three cells in; the
+    // centring interpolation needs four
+    const int n[3] = {g->nx, g->ny, g->nz};
+    for (int d = 0; d < 3; ++d)
+      if (n[d] < 4) {
+        set_error("the dynamic models need at least 4 cells in every direction");
+        return ANEL_ERR_SIZE;
+      }
+    if (!(ns->test_ratio > 0.0) || (ns->interp != ANEL_DIAG_LITERAL && ns->interp != ANEL_DIAG_CORRECTED)) {
+      set_error("dynamic model: test_ratio must be positive and interp LITERAL or CORRECTED");
+      return ANEL_ERR_ARG;
+    }
+  }
+  if (ns->vmodel != ANEL_MODEL_DNS) {
     if (ns->les_freq < 1) {
       set_error("les_freq must be >= 1");
       return ANEL_ERR_ARG;
@@ -150,7 +167,7 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
     ANEL_CUDA_TRY(cudaMalloc(&d_les_, 4 * (size_t)Z * sizeof(double)));
     ANEL_CUDA_TRY(cudaMemset(d_les_, 0, 4 * (size_t)Z * sizeof(double)));
   }
-  if (ns->vmodel == ANEL_MODEL_SSM) {
+  if (ns->vmodel != ANEL_MODEL_DNS) {
     // per-column eliminated diagonal and super-diagonal of the LES CN solve
     ANEL_CUDA_TRY(cudaMalloc(&d_cnb_, G_ * sizeof(double)));
     ANEL_CUDA_TRY(cudaMalloc(&d_cnc_, G_ * sizeof(double)));
@@ -213,9 +230,9 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
   D_.rPr = rPr_;
   D_.rSc = rSc_;
   D_.g = gnow_;
-  D_.vles = ns->vmodel == ANEL_MODEL_SSM;
-  D_.rles = ns->rmodel == ANEL_MODEL_SSM;
-  D_.sles = ns->smodel == ANEL_MODEL_SSM;
+  D_.vles = ns->vmodel != ANEL_MODEL_DNS;
+  D_.rles = ns->rmodel != ANEL_MODEL_DNS;
+  D_.sles = ns->smodel != ANEL_MODEL_DNS;
   D_.ew = ns->ew;
   D_.scal1_on = ns->scal1_on;
   // r = densityBG = 1 until set
@@ -481,9 +498,13 @@ int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, 
 int NSSolver::reset(const anel_ns_params* ns, cudaStream_t s) {
   ANEL_CUDA_TRY(cudaSetDevice(device_));
   if (!s) s = stream_;
-  const bool les = ns->vmodel == ANEL_MODEL_SSM || ns->rmodel == ANEL_MODEL_SSM ||
-                   ns->smodel == ANEL_MODEL_SSM;
-  if (les != les_any_ || (ns->vmodel == ANEL_MODEL_SSM) != (D_.vles != 0) || ns->ew != prm_.ew ||
+  const bool les = ns->vmodel != ANEL_MODEL_DNS || ns->rmodel != ANEL_MODEL_DNS ||
+                   ns->smodel != ANEL_MODEL_DNS;
+  const bool dyn = ns->vmodel == ANEL_MODEL_DSM || ns->rmodel == ANEL_MODEL_DSM || ns->smodel == ANEL_MODEL_DSM;
+  if (les != les_any_ || (ns->vmodel != ANEL_MODEL_DNS) != (D_.vles != 0) || ns->ew != prm_.ew ||
+      (dyn && (ns->test_ratio != prm_.test_ratio || std::memcmp(ns->filt, prm_.filt, sizeof(prm_.filt)) != 0 ||
+               std::memcmp(ns->stretched, prm_.stretched, sizeof(prm_.stretched)) != 0 ||
+               ns->interp != prm_.interp)) ||
       std::memcmp(ns->tb, prm_.tb, sizeof(prm_.tb)) != 0 ||
       std::memcmp(ns->vb, prm_.vb, sizeof(prm_.vb)) != 0) {
     set_error("reset: models, edge-node flag and boundary conditions must match the context");
@@ -499,8 +520,8 @@ int NSSolver::reset(const anel_ns_params* ns, cudaStream_t s) {
   D_.rPr = rPr_;
   D_.rSc = rSc_;
   D_.g = gnow_;
-  D_.rles = ns->rmodel == ANEL_MODEL_SSM;
-  D_.sles = ns->smodel == ANEL_MODEL_SSM;
+  D_.rles = ns->rmodel != ANEL_MODEL_DNS;
+  D_.sles = ns->smodel != ANEL_MODEL_DNS;
   D_.scal1_on = ns->scal1_on;
   for (double& r : cn_rkdt_) r = -1.0;  // the CN factors depend on Re, Pr, Sc
   time_ = 0.0;
@@ -538,8 +559,9 @@ int NSSolver::init_shear(uint32_t seed, double amp, double zmax, cudaStream_t s)
 // not change between calls.
 int NSSolver::les_coeffs(cudaStream_t s) {
   if (les_coeffs_done_) return ANEL_OK;
+  const bool dyn = prm_.vmodel == ANEL_MODEL_DSM || prm_.rmodel == ANEL_MODEL_DSM || prm_.smodel == ANEL_MODEL_DSM;
   const int Z = nz_ + 2;
-  std::vector<double> prof(4 * (size_t)Z, 0.0);
+  std::vector<double> prof(4 * (size_t)Z, 0.0), damp_u(Z, 1.0), damp_t(Z, 1.0);
   const double dxc = m_[0][3][1], dyc = m_[1][3][1];
   const double c = prm_.ssm_const;
   for (int k = 2; k <= nz_ + 1; ++k) {
@@ -547,26 +569,43 @@ int NSSolver::les_coeffs(cudaStream_t s) {
     double dg;
     if (prm_.les_delta == ANEL_DELTA_3ROOT) dg = std::pow(dxc * dyc * dzc, 1.0 / 3.0);
     else dg = std::pow(dxc * dxc + dyc * dyc + dzc * dzc, 1.0 / 2.0);
-    double damp_u = 1.0, damp_t = 1.0;
     if (prm_.les_damp == ANEL_DAMP_LITERAL) {
       // REAL(4) literals 0.41 and 0.3 (SSMrho); 0.3d0 in SSM
       const double k41 = (double)(float)0.41;
       const double zo_u = 0.3, zo_t = (double)(float)0.3;
       const double zc = m_[2][1][k - 1];
       const double a = k41 * (zc + zo_u);
-      damp_u = (a * a) / ((a * a) + c * (dg * dg));
+      damp_u[k - 1] = (a * a) / ((a * a) + c * (dg * dg));
       const double b = k41 * (zc + zo_t);
-      damp_t = (b * b) / ((b * b) + c * (dg * dg));
+      damp_t[k - 1] = (b * b) / ((b * b) + c * (dg * dg));
     }
-    const double cs = c * damp_u;
-    prof[k - 1] = cs;
-    prof[Z + k - 1] = cs / prm_.pr_sgs * damp_t;
-    prof[2 * (size_t)Z + k - 1] = cs / prm_.pr_sgs * damp_u;
+    prof[k - 1] = c * damp_u[k - 1];
     prof[3 * (size_t)Z + k - 1] = dg * dg;
+  }
+  // the driver's order (NSsolver.F90:83-130): the velocity model's Csgs,
+  // then SSMrho / SSMscal1 from that Csgs, or their dynamic forms
+  std::vector<double> dynp(Z, 0.0);
+  int st = ANEL_OK;
+  dyn_ready_ = false;  // the models of this update share one dyn_prepare
+  if (prm_.vmodel == ANEL_MODEL_DSM) {
+    if ((st = dsm_velocity(s, dynp.data())) != ANEL_OK) return st;
+    for (int k = 2; k <= nz_ + 1; ++k) prof[k - 1] = dynp[k - 1];
+  }
+  for (int q = 0; q < 2; ++q) {
+    const int model = q == 0 ? prm_.rmodel : prm_.smodel;
+    double* dst = prof.data() + (size_t)(q + 1) * Z;
+    if (model == ANEL_MODEL_DSM) {
+      const double* field = q == 0 ? D_.rho : D_.s;
+      if ((st = dsm_scalar(field, s, dynp.data())) != ANEL_OK) return st;
+      for (int k = 2; k <= nz_ + 1; ++k) dst[k - 1] = dynp[k - 1];
+    } else {
+      const std::vector<double>& dmp = q == 0 ? damp_t : damp_u;
+      for (int k = 2; k <= nz_ + 1; ++k) dst[k - 1] = prof[k - 1] / prm_.pr_sgs * dmp[k - 1];
+    }
   }
   ANEL_CUDA_TRY(cudaMemcpyAsync(d_les_, prof.data(), prof.size() * sizeof(double), cudaMemcpyHostToDevice, s));
   ANEL_CUDA_TRY(cudaStreamSynchronize(s));
-  les_coeffs_done_ = true;
+  les_coeffs_done_ = !dyn;  // the dynamic coefficients follow the fields
   return ANEL_OK;
 }
 

@@ -90,6 +90,23 @@ class NSSolver {
   double* d_dgpart_ = nullptr;
   cudaEvent_t dev0_ = nullptr, dev1_ = nullptr;
   int ensure_diag();
+  // dynamic Smagorinsky models (ns_dsm.cu): scratch fields, metrics
+  // (dxc dyc delg, two profiles), plane partial sums and coordinates
+  double* d_dyn_ = nullptr;
+  double* d_dyn_m_ = nullptr;
+  double* dyn_part_ = nullptr;
+  double* d_dyn_axes_ = nullptr;
+  const double* d_dyn_ax_[6] = {nullptr};
+  double dyn_area_ = 0.0;
+  bool dyn_ready_ = false;  // dyn_prepare done for the current les_coeffs
+  int ensure_dyn();
+  int dyn_prepare(cudaStream_t s);
+  void dyn_filter(const double* in, double* out, int vt, int hf, cudaStream_t s);
+  void dyn_ew(int op, double* out, const double* a, const double* b, const double* c, cudaStream_t s);
+  int dyn_ratio(double* num, double* den, double* out, cudaStream_t s);
+  int dyn_profile(const double* a, double* host, cudaStream_t s);
+  int dsm_velocity(cudaStream_t s, double* cs);
+  int dsm_scalar(const double* c, cudaStream_t s, double* out);
   MGSolver* mg_ = nullptr;
   NSDev D_{};
   // device allocations

@@ -163,14 +163,21 @@ class ServeEngine {
     h = fnv1a(nk.vb, sizeof(nk.vb), h);
     const int flags[6] = {nk.vmodel, nk.rmodel, nk.smodel, nk.ew, r->init, 0};
     h = fnv1a(flags, sizeof(flags), h);
+    // the dynamic models' filter setup is fixed per context
+    h = fnv1a(&nk.test_ratio, sizeof(nk.test_ratio), h);
+    h = fnv1a(nk.filt, sizeof(nk.filt), h);
+    h = fnv1a(nk.stretched, sizeof(nk.stretched), h);
+    h = fnv1a(&nk.interp, sizeof(nk.interp), h);
     job->key = std::to_string(g.nx) + "x" + std::to_string(g.ny) + "x" + std::to_string(g.nz) + ":" +
                std::to_string(h);
     // device memory of a context: FP64 fields (14, +3 eddy fields, +2
     // LES-CN scratch), multigrid (FP64 fine pair, FP32 levels) and slack
     const int64_t G = (int64_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
-    const bool les_any = nk.vmodel == ANEL_MODEL_SSM || nk.rmodel == ANEL_MODEL_SSM ||
-                         nk.smodel == ANEL_MODEL_SSM;
-    const int nf = 14 + (les_any ? 3 : 0) + (nk.vmodel == ANEL_MODEL_SSM ? 2 : 0);
+    const bool les_any = nk.vmodel != ANEL_MODEL_DNS || nk.rmodel != ANEL_MODEL_DNS ||
+                         nk.smodel != ANEL_MODEL_DNS;
+    const bool dyn = nk.vmodel == ANEL_MODEL_DSM || nk.rmodel == ANEL_MODEL_DSM || nk.smodel == ANEL_MODEL_DSM;
+    // (+16 scratch fields of the dynamic models)
+    const int nf = 14 + (les_any ? 3 : 0) + (nk.vmodel != ANEL_MODEL_DNS ? 2 : 0) + (dyn ? 16 : 0);
     const int64_t mgb = r->mg.precision == ANEL_PREC_MIXED ? 32 : 24;
     job->est_bytes = G * (8 * nf + mgb) + ((int64_t)64 << 20);
     std::lock_guard<std::mutex> lk(mu_);

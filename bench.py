@@ -54,6 +54,10 @@ WORKLOADS = {
     # eddy diffusivity with Pr_sgs = 0.7
     "les": ("dns", (768, 384, 384), (9, 8, 8), dict(Re=50000.0, g=-0.1, amp=1e-2, cfl=0.5, les=True)),
     "les_small": ("dns", (96, 48, 48), (6, 5, 5), dict(Re=50000.0, g=-0.1, amp=1e-2, cfl=0.5, les=True)),
+    # config 3's grid with the reference runfile's dynamic models (DSM,
+    # DSMrho, DSMscal1; TestGrid_ratio sqrt(6), filters in x, y, z)
+    "les_dsm": ("dns", (768, 384, 384), (9, 8, 8), dict(Re=50000.0, g=-0.1, amp=1e-2, cfl=0.5, les=True,
+                                                       dsm=True)),
     # one member of the serving stream, for the CPU baseline of "serve"
     "dns64": ("dns", (64, 64, 64), (6, 6, 6), dict(Re=1000.0, g=-0.12, amp=1e-3, cfl=0.5)),
     # ensemble serving: a Poisson stream of shear-layer members (sizes below)
@@ -155,9 +159,12 @@ def ns_params(phys):
     from anelastic_solve_b200 import abi
 
     # DeltaT_max large: the CFL condition sets the step (calcdt)
+    dsm = phys.get("dsm", False)
     return abi.make_ns_params(Re=phys["Re"], Pr=1.0, g=phys["g"], cfl=phys["cfl"], dtmax=1e9,
                               ew=1, scal1_on=0, les=phys.get("les", False), ssm_const=0.0289,
-                              pr_sgs=0.7, les_damp=abi.DAMP_NONE, les_start=0, les_freq=1)
+                              pr_sgs=0.7, les_damp=abi.DAMP_NONE, les_start=0, les_freq=1,
+                              models=(abi.MODEL_DSM,) * 3 if dsm else None, stretched=(0, 0, 1),
+                              interp=abi.DIAG_CORRECTED)
 
 
 def poisson_rhs(g):
@@ -640,7 +647,10 @@ def main():
     if kind == "dns":
         metric = "cell-updates/s (RK3 step incl. 3 projections)"
         unit = "cell-updates/s"
-        model = "LES (SSM, Cs^2=0.0289, Pr_sgs=0.7)" if phys.get("les") else "DNS"
+        if phys.get("dsm"):
+            model = "LES (DSM/DSMrho/DSMscal1 every step, test ratio sqrt(6), x-y averaged)"
+        else:
+            model = "LES (SSM, Cs^2=0.0289, Pr_sgs=0.7)" if phys.get("les") else "DNS"
         config = {"workload": f"{model} shear layer {nx}x{ny}x{nz}: Re={phys['Re']:g}, Pr=1, "
                               f"Ri={-phys['g']:g}, amp {phys['amp']:g}, CFL {phys['cfl']:g}, "
                               f"MG to ||f-A p||/||f|| <= {TOL:g} each sub-step",

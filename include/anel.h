@@ -183,8 +183,10 @@ int anel_mg_ctx_debug_pass(anel_mg_ctx* ctx, int32_t which, double* d_phi,
 
 /* velocity / scalar models (the Vmodel/Rmodel/Smodel ini keys,
  * ANELASTIC_SL/dns/input.F90): DNS, or the constant-coefficient
- * Smagorinsky model (SSM, SSMrho, SSMscal1). */
-enum { ANEL_MODEL_DNS = 0, ANEL_MODEL_SSM = 1 };
+ * Smagorinsky model (SSM, SSMrho, SSMscal1), or the dynamic Smagorinsky
+ * model (DSM, DSMrho, DSMscal1, les/DSM*.F90) with x-y plane-averaged
+ * coefficients (their C_avg_dir = 12). */
+enum { ANEL_MODEL_DNS = 0, ANEL_MODEL_SSM = 1, ANEL_MODEL_DSM = 2 };
 /* LES filter width (les_grid_size, straincal.F90:126-134) */
 enum { ANEL_DELTA_3ROOT = 0, ANEL_DELTA_2ROOT = 1 };
 /* LES wall damping: LITERAL = Mason damping of SSM.F90:27,60 with its
@@ -218,6 +220,16 @@ typedef struct {
    * accumulator) at zero, valid when scal1 starts at zero with zero wall
    * values -- it then stays zero in the reference as well. */
   int32_t scal1_on;
+  /* Dynamic models: TestGrid_ratio (r_dgt_dg), the test filter's
+   * directions xfilter/yfilter/zfilter, and for center_velocity the
+   * Gridtype of each axis (1 = stretched) and the interpolation mode on a
+   * stretched axis (ANEL_DIAG_LITERAL / ANEL_DIAG_CORRECTED, see the plane
+   * statistics). */
+  double test_ratio;
+  int32_t filt[3];
+  int32_t stretched[3];
+  int32_t interp;
+  int32_t reserved2;
 } anel_ns_params;
 
 /* Host (or device) pointers to the ghosted FP64 fields of the Flow and

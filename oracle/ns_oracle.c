@@ -276,7 +276,7 @@ void orc_ns_set_clock(orc_ns* s, double time, int nstep) {
 }
 
 static int les_on(const orc_ns* s) {
-  return s->p.vmodel == ANEL_MODEL_SSM;
+  return s->p.vmodel != ANEL_MODEL_DNS;
 }
 
 /* ---------------------------------------------------------------- u1_rhs
@@ -582,7 +582,7 @@ static void scalar_rhs(orc_ns* s, double* St, int is_rho) {
               A_(St, i, j, k) + (A_(wn, i, j, k - 1) * c1 - A_(wn, i, j, k) * c2) * M(D->rdzc, k);
         }
       }
-  if (model == ANEL_MODEL_SSM) {
+  if (model != ANEL_MODEL_DNS) {
     #pragma omp parallel for schedule(static)
     for (int k = sz; k <= ez; ++k)
       for (int j = sy; j <= ey; ++j)
@@ -998,11 +998,10 @@ static void gravity(orc_ns* s) {
   else if (t >= t2) s->gnow = s->g_orig;
 }
 
-/* straincal modS (straincal.F90:48-73) and delg (:126-134) */
-static void straincal(orc_ns* s) {
+/* straincal's strain magnitude (straincal.F90:48-73) of (l1, l2, l3) into
+ * modS, ghost 'cfluc' */
+static void modS_of(orc_ns* s, const double* l1, const double* l2, const double* l3, double* modS) {
   const orc_dom* D = &s->d;
-  const double *l1 = s->f.u, *l2 = s->f.v, *l3 = s->f.w;
-  double* modS = s->modS;
   memset(modS, 0, sizeof(double) * D->G);
   for (int k = 2; k <= D->nz + 1; ++k)
     for (int j = 2; j <= D->ny + 1; ++j)
@@ -1032,6 +1031,310 @@ static void straincal(orc_ns* s) {
   ghost(s, modS, VT_CFLUC);
 }
 
+/* straincal modS of the current velocity */
+static void straincal(orc_ns* s) { modS_of(s, s->f.u, s->f.v, s->f.w, s->modS); }
+
+static void center_velocity(orc_ns* s, const double* in, double* out, int dir, int stretched,
+                            int corrected);
+static void avg_x1x2(orc_ns* s, double* var, double* outm, int vt);
+
+/* ------------------------------------------------------ dynamic models
+ * DSM (les/DSM.F90:1-258), DSMrho and DSMscal1 (les/DSMrho.F90,
+ * DSMscal1.F90) with C_avg_dir = 12: the model coefficients are x-y plane
+ * averages (LagAvg is not reached).  Test filter: filter(.., 2, xfil,
+ * yfil, zfil, ..) (les/filter.F90:1-149); smoothing of the coefficient:
+ * filterHF(.., 2, 1, 1, 1, ..) (:152-288).  Whole-array Fortran
+ * assignments are whole-array loops here (ghost cells included). */
+static long dyn_G(const orc_ns* s) { return s->d.G; }
+
+/* filter(var, out, 2, xfil, yfil, zfil, vt): per direction a pass of
+ * weights (1/4, 1/2, 1/4) over the interior, written with the source's
+ * zero weights and its boundary formulas (the upper one sums from the
+ * ghost inwards), then ghost(out, vt). */
+static void filter2(orc_ns* s, const double* var, double* out, int vt) {
+  const orc_dom* D = &s->d;
+  static const double wa[5] = {0.0, 1.0 / 4.0, 1.0 / 2.0, 1.0 / 4.0, 0.0};
+  static const double wab[5] = {1.0 / 4.0, 1.0 / 2.0, 1.0 / 4.0, 0.0, 0.0};
+  memcpy(out, var, sizeof(double) * D->G);
+  const int n[3] = {D->nx, D->ny, D->nz};
+  double pen[4096];
+  for (int d = 0; d < 3; ++d) {
+    if (s->p.filt[d]) {
+      const long st = d == 0 ? 1 : (d == 1 ? D->X : D->X * D->Y);
+      const int sa = 2, ea = n[d] + 1;
+      for (int k = 2; k <= D->nz + 1; ++k)
+        for (int j = 2; j <= D->ny + 1; ++j)
+          for (int i = 2; i <= D->nx + 1; ++i) {
+            const int q = d == 0 ? i : (d == 1 ? j : k);
+            if (q != 2) continue; /* one pencil per (other two indices) */
+            const long b = IX(i, j, k) - (long)q * st;
+            for (int t = sa - 1; t <= ea + 1; ++t) pen[t] = out[b + (long)t * st];
+            for (int t = sa + 1; t <= ea - 1; ++t)
+              out[b + (long)t * st] = wa[0] * pen[t - 2] + wa[1] * pen[t - 1] + wa[2] * pen[t] +
+                                      wa[3] * pen[t + 1] + wa[4] * pen[t + 2];
+            out[b + (long)sa * st] = wab[0] * pen[sa - 1] + wab[1] * pen[sa] + wab[2] * pen[sa + 1] +
+                                     wab[3] * pen[sa + 2] + wab[4] * pen[sa + 3];
+            out[b + (long)ea * st] = wab[0] * pen[ea + 1] + wab[1] * pen[ea] + wab[2] * pen[ea - 1] +
+                                     wab[3] * pen[ea - 2] + wab[4] * pen[ea - 3];
+          }
+    }
+    ghost(s, out, vt);
+  }
+}
+
+/* filterHF(var, out, 2, 1, 1, 1, vt, ..): in each direction a point that
+ * is a strict local extremum of its pencil takes the 3-point average when
+ * that average is still an extremum of the same kind. */
+static void filterHF2(orc_ns* s, const double* var, double* out, int vt) {
+  const orc_dom* D = &s->d;
+  static const double wa[3] = {1.0 / 4.0, 1.0 / 2.0, 1.0 / 4.0};
+  memcpy(out, var, sizeof(double) * D->G);
+  const int n[3] = {D->nx, D->ny, D->nz};
+  double pen[4096];
+  for (int d = 0; d < 3; ++d) {
+    const long st = d == 0 ? 1 : (d == 1 ? D->X : D->X * D->Y);
+    const int sa = 2, ea = n[d] + 1;
+    for (int k = 2; k <= D->nz + 1; ++k)
+      for (int j = 2; j <= D->ny + 1; ++j)
+        for (int i = 2; i <= D->nx + 1; ++i) {
+          const int q = d == 0 ? i : (d == 1 ? j : k);
+          if (q != 2) continue;
+          const long b = IX(i, j, k) - (long)q * st;
+          for (int t = sa - 1; t <= ea + 1; ++t) pen[t] = out[b + (long)t * st];
+          for (int t = sa; t <= ea; ++t) {
+            const double p0 = pen[t], pm = pen[t - 1], pp = pen[t + 1];
+            if (p0 < pp && p0 < pm) {
+              const double x = wa[0] * pm + wa[1] * p0 + wa[2] * pp;
+              if (x < pp && x < pm) out[b + (long)t * st] = x;
+            } else if (p0 > pp && p0 > pm) {
+              const double x = wa[0] * pm + wa[1] * p0 + wa[2] * pp;
+              if (x > pp && x > pm) out[b + (long)t * st] = x;
+            }
+          }
+        }
+    ghost(s, out, vt);
+  }
+}
+
+/* DSM's lestmp1 for component ij (DSM.F90:38-86): the diagonal strain, and
+ * for ij = 4..6 half the difference of the two cross derivatives (the
+ * source subtracts where straincal adds). */
+static double dsm_component(const orc_dom* D, const double* l1, const double* l2, const double* l3, int ij,
+                            int i, int j, int k) {
+  double t1, t2, t3, t4;
+  switch (ij) {
+    case 1: return (A_(l1, i + 1, j, k) - A_(l1, i, j, k)) * M(D->rdxc, i);
+    case 2: return (A_(l2, i, j + 1, k) - A_(l2, i, j, k)) * M(D->rdyc, j);
+    case 3: return (A_(l3, i, j, k + 1) - A_(l3, i, j, k)) * M(D->rdzc, k);
+    case 4:
+      t1 = 0.25 * (A_(l1, i, j, k) + A_(l1, i + 1, j, k) + A_(l1, i, j + 1, k) + A_(l1, i + 1, j + 1, k));
+      t2 = 0.25 * (A_(l1, i, j, k) + A_(l1, i + 1, j, k) + A_(l1, i, j - 1, k) + A_(l1, i + 1, j - 1, k));
+      t3 = 0.25 * (A_(l2, i, j, k) + A_(l2, i, j + 1, k) + A_(l2, i + 1, j, k) + A_(l2, i + 1, j + 1, k));
+      t4 = 0.25 * (A_(l2, i, j, k) + A_(l2, i, j + 1, k) + A_(l2, i - 1, j, k) + A_(l2, i - 1, j + 1, k));
+      return 0.5 * ((t1 - t2) * M(D->rdyc, j) - (t3 - t4) * M(D->rdxc, i));
+    case 5:
+      t1 = 0.25 * (A_(l1, i, j, k) + A_(l1, i + 1, j, k) + A_(l1, i, j, k + 1) + A_(l1, i + 1, j, k + 1));
+      t2 = 0.25 * (A_(l1, i, j, k) + A_(l1, i + 1, j, k) + A_(l1, i, j, k - 1) + A_(l1, i + 1, j, k - 1));
+      t3 = 0.25 * (A_(l3, i, j, k) + A_(l3, i, j, k + 1) + A_(l3, i + 1, j, k) + A_(l3, i + 1, j, k + 1));
+      t4 = 0.25 * (A_(l3, i, j, k) + A_(l3, i, j, k + 1) + A_(l3, i - 1, j, k) + A_(l3, i - 1, j, k + 1));
+      return 0.5 * ((t1 - t2) * M(D->rdzc, k) - (t3 - t4) * M(D->rdxc, i));
+    default:
+      t1 = 0.25 * (A_(l2, i, j, k) + A_(l2, i, j + 1, k) + A_(l2, i, j, k + 1) + A_(l2, i, j + 1, k + 1));
+      t2 = 0.25 * (A_(l2, i, j, k) + A_(l2, i, j + 1, k) + A_(l2, i, j, k - 1) + A_(l2, i, j + 1, k - 1));
+      t3 = 0.25 * (A_(l3, i, j, k) + A_(l3, i, j, k + 1) + A_(l3, i, j + 1, k) + A_(l3, i, j + 1, k + 1));
+      t4 = 0.25 * (A_(l3, i, j, k) + A_(l3, i, j, k + 1) + A_(l3, i, j - 1, k) + A_(l3, i, j - 1, k + 1));
+      return 0.5 * ((t1 - t2) * M(D->rdzc, k) - (t3 - t4) * M(D->rdyc, j));
+  }
+}
+
+typedef struct {
+  double *modS, *fmodS, *c[3], *fc[3], *l1, *l2, *l3, *l4, *P, *a, *b;
+} dyn_work;
+
+static double* dyn_alloc(const orc_ns* s) { return (double*)calloc(dyn_G(s), sizeof(double)); }
+
+/* the fields every dynamic model starts from: straincal's modS and fmodS
+ * (the strain magnitude of the filtered velocity, get_fmodS,
+ * straincal.F90:166-229), the centred velocities and their filtered
+ * forms (center_velocity, then filter(.., 'cfluc')) */
+static void dyn_prepare(orc_ns* s, dyn_work* w) {
+  anel_fields* f = &s->f;
+  w->modS = dyn_alloc(s);
+  w->fmodS = dyn_alloc(s);
+  w->l1 = dyn_alloc(s);
+  w->l2 = dyn_alloc(s);
+  w->l3 = dyn_alloc(s);
+  w->l4 = dyn_alloc(s);
+  w->P = dyn_alloc(s);
+  w->a = dyn_alloc(s);
+  w->b = dyn_alloc(s);
+  modS_of(s, f->u, f->v, f->w, w->modS);
+  filter2(s, f->u, w->l1, VT_U);
+  filter2(s, f->v, w->l2, VT_V);
+  filter2(s, f->w, w->l3, VT_W);
+  modS_of(s, w->l1, w->l2, w->l3, w->fmodS);
+  const double* vel[3] = {f->u, f->v, f->w};
+  for (int d = 0; d < 3; ++d) {
+    w->c[d] = dyn_alloc(s);
+    w->fc[d] = dyn_alloc(s);
+    center_velocity(s, vel[d], w->c[d], d + 1, s->p.stretched[d], s->p.interp == ANEL_DIAG_CORRECTED);
+    filter2(s, w->c[d], w->fc[d], VT_CFLUC);
+  }
+}
+
+static void dyn_free(dyn_work* w) {
+  double* p[] = {w->modS, w->fmodS, w->l1, w->l2, w->l3, w->l4, w->P, w->a, w->b,
+                 w->c[0], w->c[1], w->c[2], w->fc[0], w->fc[1], w->fc[2]};
+  for (unsigned q = 0; q < sizeof(p) / sizeof(p[0]); ++q) free(p[q]);
+}
+
+/* the plane averaging and ratio common to the three models (DSM.F90:
+ * 196-256, DSMrho.F90:166-240): num and den are averaged over x-y planes,
+ * the interior takes the plane values (num clipped at 0), then
+ * out = 0.5 num / den (1e-20 where den == 0), smoothed by filterHF */
+static void dyn_ratio(orc_ns* s, double* num, double* den, double* out, dyn_work* w) {
+  const orc_dom* D = &s->d;
+  const long Z = D->Z;
+  double* pn = (double*)calloc(Z, sizeof(double));
+  double* pd = (double*)calloc(Z, sizeof(double));
+  ghost(s, num, VT_CFLUC);
+  ghost(s, den, VT_CFLUC);
+  avg_x1x2(s, num, pn, VT_CFLUC);
+  avg_x1x2(s, den, pd, VT_CFLUC);
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i) {
+        A_(num, i, j, k) = pn[k - 1];
+        A_(den, i, j, k) = pd[k - 1];
+        if (A_(num, i, j, k) < 0.0) A_(num, i, j, k) = 0.0;
+      }
+  ghost(s, num, VT_CFLUC);
+  ghost(s, den, VT_CFLUC);
+  for (int k = 2; k <= D->nz + 1; ++k)
+    for (int j = 2; j <= D->ny + 1; ++j)
+      for (int i = 2; i <= D->nx + 1; ++i) {
+        if (A_(den, i, j, k) == 0.0) A_(out, i, j, k) = 1.0e-20;
+        else A_(out, i, j, k) = 0.5 * A_(num, i, j, k) / A_(den, i, j, k);
+      }
+  ghost(s, out, VT_CFLUC);
+  filterHF2(s, out, w->P, VT_CFLUC);
+  memcpy(out, w->P, sizeof(double) * D->G);
+  ghost(s, out, VT_CFLUC);
+  free(pn);
+  free(pd);
+}
+
+/* DSM (DSM.F90:1-258) into Csgs */
+static void dsm(orc_ns* s, double* Csgs) {
+  const orc_dom* D = &s->d;
+  const long G = D->G;
+  const anel_fields* f = &s->f;
+  dyn_work w;
+  dyn_prepare(s, &w);
+  const double rt = s->p.test_ratio;
+  double *l1 = w.l1, *l2 = w.l2, *l3 = w.l3, *l4 = w.l4;
+  memset(l4, 0, sizeof(double) * G);
+  memset(Csgs, 0, sizeof(double) * G);
+  static const int pa[7] = {0, 0, 1, 2, 0, 0, 1}, pb[7] = {0, 0, 1, 2, 1, 2, 2};
+  for (int ij = 1; ij <= 6; ++ij) {
+    for (int k = 2; k <= D->nz + 1; ++k)
+      for (int j = 2; j <= D->ny + 1; ++j)
+        for (int i = 2; i <= D->nx + 1; ++i) A_(l1, i, j, k) = dsm_component(D, f->u, f->v, f->w, ij, i, j, k);
+    ghost(s, l1, VT_CFLUC);
+    for (int k = 2; k <= D->nz + 1; ++k)
+      for (int j = 2; j <= D->ny + 1; ++j)
+        for (int i = 2; i <= D->nx + 1; ++i) {
+          const double dg = A_(s->delg, i, j, k);
+          A_(l2, i, j, k) = (dg * dg) * A_(w.modS, i, j, k) * A_(l1, i, j, k);
+        }
+    ghost(s, l2, VT_CFLUC);
+    filter2(s, l2, l3, VT_CFLUC);
+    filter2(s, l1, l2, VT_CFLUC);
+    memcpy(l1, w.fmodS, sizeof(double) * G);
+    for (int k = 2; k <= D->nz + 1; ++k)
+      for (int j = 2; j <= D->ny + 1; ++j)
+        for (int i = 2; i <= D->nx + 1; ++i) {
+          const double rd = rt * A_(s->delg, i, j, k);
+          A_(l2, i, j, k) = (rd * rd) * A_(l1, i, j, k) * A_(l2, i, j, k);
+        }
+    ghost(s, l2, VT_CFLUC);
+    for (long c = 0; c < G; ++c) l3[c] = l3[c] - l2[c];
+    ghost(s, l3, VT_CFLUC);
+    const double *ca = w.c[pa[ij]], *cb = w.c[pb[ij]];
+    for (long c = 0; c < G; ++c) w.a[c] = ca[c] * cb[c];
+    filter2(s, w.a, l2, VT_CFLUC);
+    const double *fa = w.fc[pa[ij]], *fb = w.fc[pb[ij]];
+    if (ij <= 3) {
+      for (long c = 0; c < G; ++c) l4[c] = l4[c] + l3[c] * l2[c];
+      for (long c = 0; c < G; ++c) l4[c] = l4[c] - l3[c] * fa[c] * fb[c];
+      for (long c = 0; c < G; ++c) Csgs[c] = Csgs[c] + l3[c] * l3[c];
+    } else {
+      for (long c = 0; c < G; ++c) l4[c] = l4[c] + 2.0 * l3[c] * l2[c];
+      for (long c = 0; c < G; ++c) l4[c] = l4[c] - 2.0 * l3[c] * fa[c] * fb[c];
+      for (long c = 0; c < G; ++c) Csgs[c] = Csgs[c] + 2.0 * l3[c] * l3[c];
+    }
+  }
+  /* Csgs = 0.5 <LM> / <MM> */
+  memcpy(w.b, Csgs, sizeof(double) * G);
+  dyn_ratio(s, l4, w.b, Csgs, &w);
+  dyn_free(&w);
+}
+
+/* DSMrho / DSMscal1 (DSMrho.F90:1-240) of the scalar c into C */
+static void dsm_scalar(orc_ns* s, const double* c, double* C) {
+  const orc_dom* D = &s->d;
+  const long G = D->G;
+  const anel_fields* f = &s->f;
+  dyn_work w;
+  dyn_prepare(s, &w);
+  const double rt = s->p.test_ratio;
+  double *l1 = w.l1, *l2 = w.l2, *l3 = w.l3, *l4 = w.l4;
+  memset(l4, 0, sizeof(double) * G);
+  memset(C, 0, sizeof(double) * G);
+  const double* vel[3] = {f->u, f->v, f->w};
+  for (int ij = 1; ij <= 3; ++ij) {
+    const long st = ij == 1 ? 1 : (ij == 2 ? D->X : D->X * D->Y);
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int k = 2; k <= D->nz + 1; ++k)
+        for (int j = 2; j <= D->ny + 1; ++j)
+          for (int i = 2; i <= D->nx + 1; ++i) {
+            const long o = IX(i, j, k);
+            const double t1 = 0.5 * (c[o] + c[o - st]);
+            const double t2 = 0.5 * (c[o] + c[o + st]);
+            const double rd = ij == 1 ? M(D->rdxc, i) : (ij == 2 ? M(D->rdyc, j) : M(D->rdzc, k));
+            const double dg = A_(s->delg, i, j, k);
+            l1[o] = pass == 0 ? (dg * dg) * A_(w.modS, i, j, k) * (t2 - t1) * rd : (t2 - t1) * rd;
+          }
+      ghost(s, l1, VT_CFLUC);
+      filter2(s, l1, pass == 0 ? l2 : l3, VT_CFLUC);
+    }
+    memcpy(l1, w.fmodS, sizeof(double) * G);
+    for (int k = 2; k <= D->nz + 1; ++k)
+      for (int j = 2; j <= D->ny + 1; ++j)
+        for (int i = 2; i <= D->nx + 1; ++i) {
+          const double rd = rt * A_(s->delg, i, j, k);
+          A_(l2, i, j, k) = A_(l2, i, j, k) - (rd * rd) * A_(l1, i, j, k) * A_(l3, i, j, k);
+        }
+    ghost(s, l2, VT_CFLUC);
+    for (int k = 2; k <= D->nz + 1; ++k)
+      for (int j = 2; j <= D->ny + 1; ++j)
+        for (int i = 2; i <= D->nx + 1; ++i) {
+          const long o = IX(i, j, k);
+          l1[o] = c[o] * 0.5 * (vel[ij - 1][o - st] + vel[ij - 1][o]);
+        }
+    ghost(s, l1, VT_CFLUC);
+    filter2(s, l1, l3, VT_CFLUC);
+    filter2(s, c, w.a, VT_CFLUC);
+    for (long q = 0; q < G; ++q) l3[q] = l3[q] - w.a[q] * w.fc[ij - 1][q];
+    ghost(s, l3, VT_CFLUC);
+    for (long q = 0; q < G; ++q) l4[q] = l4[q] + l2[q] * l2[q];
+    for (long q = 0; q < G; ++q) C[q] = C[q] + l2[q] * l3[q];
+  }
+  memcpy(w.b, C, sizeof(double) * G);
+  dyn_ratio(s, w.b, l4, C, &w);
+  dyn_free(&w);
+}
+
 /* grid-only LES quantities: delg (straincal.F90:126-134) and the model
  * coefficients Csgs/CTsgs/CSsgs (SSM.F90:27,60,97) */
 static void les_coeffs(orc_ns* s) {
@@ -1059,14 +1362,28 @@ static void les_coeffs(orc_ns* s) {
           damp_u = 1.0;
           damp_t = 1.0;
         }
-        A_(s->Csgs, i, j, k) = c * damp_u;
-        A_(s->CTsgs, i, j, k) = A_(s->Csgs, i, j, k) / s->p.pr_sgs * damp_t;
-        A_(s->CSsgs, i, j, k) = A_(s->Csgs, i, j, k) / s->p.pr_sgs * damp_u;
+        if (s->p.vmodel != ANEL_MODEL_DSM) A_(s->Csgs, i, j, k) = c * damp_u;
+        A_(s->work[0], i, j, k) = damp_t;
+        A_(s->work[1], i, j, k) = damp_u;
       }
   ghost(s, s->delg, VT_CFLUC);
+  /* the driver's order (NSsolver.F90:83-130): the velocity model, then
+   * SSMrho / SSMscal1 from its Csgs, or their dynamic forms */
+  if (s->p.vmodel == ANEL_MODEL_DSM) dsm(s, s->Csgs);
   ghost(s, s->Csgs, VT_CFLUC);
-  ghost(s, s->CTsgs, VT_CFLUC);
-  ghost(s, s->CSsgs, VT_CFLUC);
+  for (int q = 0; q < 2; ++q) {
+    double* C = q == 0 ? s->CTsgs : s->CSsgs;
+    const int model = q == 0 ? s->p.rmodel : s->p.smodel;
+    if (model == ANEL_MODEL_DSM) {
+      dsm_scalar(s, q == 0 ? s->f.rho : s->f.scal1, C);
+    } else {
+      for (int k = 2; k <= D->nz + 1; ++k)
+        for (int j = 2; j <= D->ny + 1; ++j)
+          for (int i = 2; i <= D->nx + 1; ++i)
+            A_(C, i, j, k) = A_(s->Csgs, i, j, k) / s->p.pr_sgs * A_(s->work[q], i, j, k);
+    }
+    ghost(s, C, VT_CFLUC);
+  }
 }
 
 /* SGSdiff (straincal.F90:339-414): nuT, kappaT, nappaT */
@@ -1101,7 +1418,7 @@ int orc_ns_step(orc_ns* s, anel_step_report* rep) {
   memset(f->q_s, 0, sizeof(double) * G);
   const double delt = calcdt(s);
   gravity(s);
-  const int les = s->p.vmodel == ANEL_MODEL_SSM;
+  const int les = s->p.vmodel != ANEL_MODEL_DNS;
   if (les && s->nstep >= s->p.les_start && s->nstep % s->p.les_freq == 0) les_coeffs(s);
   static const double A1[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
   static const double A3[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
