@@ -46,6 +46,8 @@ SIGNATURES = {
     "anel_ns_ctx_set_profiling": (C.c_int, [_P, C.c_int32]),
     "anel_ns_ctx_project": (C.c_int, [_P, _IP, _DP]),
     "anel_ns_ctx_divergence": (C.c_int, [_P, _DP]),
+    "anel_ns_ctx_step_host": (C.c_int, [_P, C.POINTER(abi.Fields), C.POINTER(abi.Fields), C.c_int32, _P,
+                                        C.POINTER(abi.StepReport)]),
     "anel_ns_ctx_set_diagnostics": (C.c_int, [_P, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "anel_ns_ctx_compute_diagnostics": (C.c_int, [_P, _P]),
     "anel_ns_ctx_get_diagnostics": (C.c_int, [_P, _DP, C.c_int32]),

@@ -40,6 +40,16 @@ int check_launch(const char* what);
 // Raise a kernel's dynamic shared-memory limit once per (device, kernel);
 // safe to call from several host threads.
 void set_smem_limit_once(const void* func, int bytes);
+// Copy nwords 8-byte words by a kernel, between device memory and pinned
+// host memory allocated with cudaHostAllocMapped (either direction).  Small
+// readbacks and uploads of the step path go this way instead of through a
+// copy engine, so they never queue behind large copies that other streams
+// have in flight; the host reads a readback after synchronising the stream.
+void copy_words(const void* src, void* dst, int64_t nwords, cudaStream_t s);
+// Fixed-order fold of n (a, b) partial pairs into out[0..1] on the device;
+// scratch holds fold_scratch_doubles() doubles.
+int64_t fold_scratch_doubles();
+void launch_fold_pairs(const double* part, int64_t n, double* scratch, double* out, cudaStream_t s);
 
 // ------------------------------------------------------------ level maps
 // One multigrid level, 1-based Fortran conventions of mg_init.F90:

@@ -33,6 +33,21 @@ void set_smem_limit_once(const void* func, int bytes) {
   done.emplace_back(dev, func);
 }
 
+__global__ void k_copy_words(const unsigned long long* __restrict__ src, unsigned long long* __restrict__ dst,
+                             int64_t n) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    dst[t] = src[t];
+}
+
+void copy_words(const void* src, void* dst, int64_t nwords, cudaStream_t s) {
+  int64_t blocks = (nwords + 255) / 256;
+  if (blocks > 64) blocks = 64;
+  if (blocks < 1) blocks = 1;
+  k_copy_words<<<(unsigned)blocks, 256, 0, s>>>(static_cast<const unsigned long long*>(src),
+                                               static_cast<unsigned long long*>(dst), nwords);
+  count_launch();
+}
+
 int check_launch(const char* what) {
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -210,6 +225,12 @@ int anel_ns_ctx_set_clock(anel_ns_ctx* ctx, double time, int32_t nstep) {
   if (!ctx) return ANEL_ERR_ARG;
   ctx->s->set_clock(time, nstep);
   return ANEL_OK;
+}
+
+int anel_ns_ctx_step_host(anel_ns_ctx* ctx, const anel_fields* in, const anel_fields* out, int32_t nsteps,
+                          void* stream, anel_step_report* report) {
+  if (!ctx) return ANEL_ERR_ARG;
+  return ctx->s->step_host(in, out, nsteps, static_cast<cudaStream_t>(stream), report);
 }
 
 int anel_ns_ctx_set_diagnostics(anel_ns_ctx* ctx, int32_t on, int32_t mode, const int32_t* stretched) {

@@ -177,6 +177,14 @@ static void launch_resid(const DevLevel<double>& L, const double* phi, const dou
   count_launch(3);
 }
 
+int64_t fold_scratch_doubles() { return 2 * (int64_t)kFoldBlocks; }
+
+void launch_fold_pairs(const double* part, int64_t n, double* scratch, double* out, cudaStream_t s) {
+  k_fold_chunks<<<kFoldBlocks, kNormThreads, 0, s>>>(part, n, scratch);
+  k_fold<<<1, kNormThreads, 0, s>>>(scratch, kFoldBlocks, out);
+  count_launch(2);
+}
+
 void launch_resid_norm(const DevLevel<double>& L, const double* phi, const double* f, double* part,
                        double* out, cudaStream_t s) {
   launch_resid<false>(L, phi, f, nullptr, part, out, s);

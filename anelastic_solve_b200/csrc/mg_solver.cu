@@ -233,7 +233,7 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
   ANEL_CUDA_TRY(cudaMalloc(&d_max_, 2 * sizeof(unsigned long long)));
   ANEL_CUDA_TRY(cudaMalloc(&d_part_, (size_t)resid_part_doubles(L64(ngrid_)) * sizeof(double)));
   ANEL_CUDA_TRY(cudaMalloc(&d_norm_, 2 * sizeof(double)));
-  ANEL_CUDA_TRY(cudaHostAlloc(&h_pin_, 4 * sizeof(double), cudaHostAllocDefault));
+  ANEL_CUDA_TRY(cudaHostAlloc(&h_pin_, 4 * sizeof(double), cudaHostAllocMapped));
   // default density r == 1
   std::vector<double> rz(geo_[ngrid_].Z, 1.0);
   int st = build_coefficients(rz);
@@ -1108,7 +1108,7 @@ double MGSolver::true_resid(const double* d_phi, const double* d_rhs, cudaStream
                             double* fnorm) {
   const DevLevel<double> F = fine_view(const_cast<double*>(d_phi), d_rhs);
   launch_resid_norm(F, d_phi, d_rhs, d_part_, d_norm_, s);
-  cudaMemcpyAsync(h_pin_, d_norm_, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  copy_words(d_norm_, h_pin_, 2, s);
   cudaStreamSynchronize(s);
   if (fnorm) *fnorm = std::sqrt(h_pin_[1]);
   return h_pin_[1] > 0.0 ? std::sqrt(h_pin_[0] / h_pin_[1]) : std::sqrt(h_pin_[0]);
@@ -1174,7 +1174,7 @@ int MGSolver::solve_fp64(double* d_phi, const double* d_rhs, cudaStream_t s,
     } else {
       ANEL_CUDA_TRY(cudaMemsetAsync(d_max_, 0, 2 * sizeof(unsigned long long), s));
       launch_relmax_copy(W, W.phi, d_phi, d_max_, s);
-      ANEL_CUDA_TRY(cudaMemcpyAsync(h_pin_, d_max_, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+      copy_words(d_max_, h_pin_, 2, s);
       ANEL_CUDA_TRY(cudaStreamSynchronize(s));
       const double v1 = h_pin_[0], v2 = h_pin_[1];  // bit patterns of the maxima
       relmax = v1 > 0.0 ? v2 / v1 : 0.0;
@@ -1258,7 +1258,7 @@ int MGSolver::solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s,
   bool conv = false;
   for (iter = 0; iter <= prm_.maxcy; ++iter) {
     launch_resid_store(Fu, d_phi, d_rhs, E.src, d_part_, d_norm_, s);
-    ANEL_CUDA_TRY(cudaMemcpyAsync(h_pin_, d_norm_, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    copy_words(d_norm_, h_pin_, 2, s);
     ANEL_CUDA_TRY(cudaStreamSynchronize(s));
     rel = h_pin_[1] > 0.0 ? std::sqrt(h_pin_[0] / h_pin_[1]) : std::sqrt(h_pin_[0]);
     if (prm_.verbose) std::fprintf(stderr, "       Defect: %5d  RESID= %22.15e\n", iter, rel);

@@ -51,6 +51,9 @@ NSSolver::~NSSolver() {
   cudaFree(d_dyn_axes_);
   if (dev0_) cudaEventDestroy(dev0_);
   if (dev1_) cudaEventDestroy(dev1_);
+  for (cudaEvent_t e : io_ev_)
+    if (e) cudaEventDestroy(e);
+  if (io_stream_) cudaStreamDestroy(io_stream_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -184,9 +187,9 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
   ANEL_CUDA_TRY(cudaMalloc(&d_prof_, 2 * (size_t)Z * sizeof(double)));
   const size_t ncn = 3 * 5 * 9 * (size_t)Z;
   ANEL_CUDA_TRY(cudaMalloc(&d_cn_, ncn * sizeof(double)));
-  ANEL_CUDA_TRY(cudaHostAlloc(&h_cn_, ncn * sizeof(double), cudaHostAllocDefault));
+  ANEL_CUDA_TRY(cudaHostAlloc(&h_cn_, ncn * sizeof(double), cudaHostAllocMapped));
   ANEL_CUDA_TRY(cudaMalloc(&d_red_, 4 * sizeof(unsigned long long)));
-  ANEL_CUDA_TRY(cudaHostAlloc(&h_red_, 4 * sizeof(double), cudaHostAllocDefault));
+  ANEL_CUDA_TRY(cudaHostAlloc(&h_red_, 4 * sizeof(double), cudaHostAllocMapped));
   // device view
   D_.nx = nx_;
   D_.ny = ny_;
@@ -383,8 +386,9 @@ int NSSolver::cn_factors(int slot, double rkdt, cudaStream_t s) {
     }
   }
   double* dst = d_cn_ + (size_t)slot * 5 * 9 * Z;
-  ANEL_CUDA_TRY(cudaMemcpyAsync(dst, h_cn_ + (size_t)slot * 5 * 9 * Z, 5 * 9 * (size_t)Z * sizeof(double),
-                                cudaMemcpyHostToDevice, s));
+  // by a kernel from the mapped staging slot: a copy-engine upload would
+  // queue behind large uploads other streams have in flight
+  copy_words(h_cn_ + (size_t)slot * 5 * 9 * Z, dst, 5 * 9 * (int64_t)Z, s);
   cn_rkdt_[slot] = rkdt;
   return ANEL_OK;
 }
@@ -483,9 +487,27 @@ int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, 
   launch_psource(D_, dt_rk, s);
   cn(5, D_.rho, D_.qr, 3, zrule(NV_RHO), D_.kT);
   if (prm_.scal1_on) cn(8, D_.s, D_.qs, 4, zrule(NV_SCAL1), D_.nT);
+  const size_t fb = G_ * sizeof(double);
+  if (io_last_sub_ && io_out_) {
+    // rho and scal1 are final: copy them out during the pressure solve
+    ANEL_CUDA_TRY(cudaEventRecord(io_ev_[1], s));
+    ANEL_CUDA_TRY(cudaStreamWaitEvent(io_stream_, io_ev_[1], 0));
+    if (io_out_->rho) ANEL_CUDA_TRY(cudaMemcpyAsync(io_out_->rho, D_.rho, fb, cudaMemcpyDeviceToHost, io_stream_));
+    if (io_out_->scal1)
+      ANEL_CUDA_TRY(cudaMemcpyAsync(io_out_->scal1, D_.s, fb, cudaMemcpyDeviceToHost, io_stream_));
+  }
+  if (io_wait_p_) {  // p (the solve's initial guess) arrives on the copy stream
+    ANEL_CUDA_TRY(cudaStreamWaitEvent(s, io_ev_[0], 0));
+    io_wait_p_ = false;
+  }
   anel_mg_report rep{};
   const int st = mg_->solve_device(D_.p, D_.psrc, s, &rep);
   if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
+  if (io_last_sub_ && io_out_ && io_out_->p) {  // p is final: copy it out during Pgrad
+    ANEL_CUDA_TRY(cudaEventRecord(io_ev_[2], s));
+    ANEL_CUDA_TRY(cudaStreamWaitEvent(io_stream_, io_ev_[2], 0));
+    ANEL_CUDA_TRY(cudaMemcpyAsync(io_out_->p, D_.p, fb, cudaMemcpyDeviceToHost, io_stream_));
+  }
   acc_mg_ms_ += rep.ms;
   acc_sweep_ms_ += rep.fine_sweep_ms;
   acc_sweeps_ += rep.fine_sweeps;
@@ -612,7 +634,7 @@ int NSSolver::les_coeffs(cudaStream_t s) {
 double NSSolver::calcdt(cudaStream_t s, int* st) {
   cudaMemsetAsync(d_red_, 0, sizeof(unsigned long long), s);
   launch_cfl_max(D_, d_red_, s);
-  cudaMemcpyAsync(h_red_, d_red_, sizeof(double), cudaMemcpyDeviceToHost, s);
+  copy_words(d_red_, h_red_, 1, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) {
     *st = ANEL_ERR_CUDA;
     return 0.0;
@@ -655,7 +677,9 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
     const double DTR[3] = {1.0 / 3.0 * delt, 5.0 / 12.0 * delt, 1.0 / 4.0 * delt};
     for (int q = 0; q < 3; ++q) {
       if (les && nstep_ > prm_.les_start) launch_sgs(D_, zrule(NV_CFLUC), s);
+      io_last_sub_ = io_out_ && n == nsteps - 1 && q == 2;
       st = substep(A1[q], 1.0, A3[q], DTR[q], delt, s, &r.mg_iter[q], &r.mg_relmax[q], true);
+      io_last_sub_ = false;
       if (st != ANEL_OK) return st;
     }
     told_ = time_;  // told = time; time = time + delt (NSsolver.F90:272-274)
@@ -823,6 +847,58 @@ int NSSolver::get_diagnostics(double* out, int mem) {
   return ANEL_OK;
 }
 
+int NSSolver::step_host(const anel_fields* in, const anel_fields* out, int nsteps, cudaStream_t s,
+                        anel_step_report* rep) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  if (!in || !out || nsteps < 1) {
+    set_error("step_host: null fields or nsteps < 1");
+    return ANEL_ERR_ARG;
+  }
+  if (!io_stream_) {
+    ANEL_CUDA_TRY(cudaStreamCreateWithFlags(&io_stream_, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : io_ev_) ANEL_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  const size_t fb = G_ * sizeof(double);
+  double* const* src = reinterpret_cast<double* const*>(in);
+  double* const* dst = reinterpret_cast<double* const*>(out);
+  // everything but p in on the step's stream (r and densityBG keep their
+  // z-profile check of set_fields)
+  anel_fields rest = *in;
+  rest.p = nullptr;
+  int st = set_fields(&rest, ANEL_MEM_HOST, s);
+  if (st != ANEL_OK) return st;
+  if (in->p) {
+    // p in on the copy stream once the others are in, ahead of its first use
+    ANEL_CUDA_TRY(cudaEventRecord(io_ev_[3], s));
+    ANEL_CUDA_TRY(cudaStreamWaitEvent(io_stream_, io_ev_[3], 0));
+    ANEL_CUDA_TRY(cudaMemcpyAsync(D_.p, in->p, fb, cudaMemcpyHostToDevice, io_stream_));
+    ANEL_CUDA_TRY(cudaEventRecord(io_ev_[0], io_stream_));
+    io_wait_p_ = true;
+  }
+  io_out_ = out;
+  st = step(nsteps, s, rep);
+  io_out_ = nullptr;
+  if (io_wait_p_) {  // no pressure solve consumed it (cannot happen in a step)
+    cudaStreamWaitEvent(s, io_ev_[0], 0);
+    io_wait_p_ = false;
+  }
+  if (st != ANEL_OK) {
+    cudaStreamSynchronize(io_stream_);
+    return st;
+  }
+  // the remaining fields out on the step's stream
+  for (int q = 0; q < 17; ++q) {
+    if (!dst[q] || !d_fields_[q] || q == 3 || q == 4 || q == 5) continue;  // p, rho, scal1: done
+    ANEL_CUDA_TRY(cudaMemcpyAsync(dst[q], d_fields_[q], fb, cudaMemcpyDeviceToHost, s));
+  }
+  ANEL_CUDA_TRY(cudaEventRecord(io_ev_[3], io_stream_));
+  ANEL_CUDA_TRY(cudaStreamWaitEvent(s, io_ev_[3], 0));
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  (void)src;
+  return ANEL_OK;
+}
+
 int NSSolver::project(cudaStream_t s, int* iters, double* relmax) {
   ANEL_CUDA_TRY(cudaSetDevice(device_));
   if (!s) s = stream_;
@@ -846,19 +922,17 @@ int NSSolver::divergence(cudaStream_t s, double* out) {
   ANEL_CUDA_TRY(cudaSetDevice(device_));
   if (!s) s = stream_;
   const int64_t nb = divergence_blocks(D_);
-  if (!d_part_) ANEL_CUDA_TRY(cudaMalloc(&d_part_, 2 * nb * sizeof(double)));
+  // partial pairs, fold scratch, the two sums
+  if (!d_part_)
+    ANEL_CUDA_TRY(cudaMalloc(&d_part_, (2 * nb + fold_scratch_doubles() + 2) * sizeof(double)));
+  double* sums = d_part_ + 2 * nb + fold_scratch_doubles();
   ANEL_CUDA_TRY(cudaMemsetAsync(d_red_ + 1, 0, sizeof(unsigned long long), s));
   launch_divergence(D_, d_red_ + 1, d_part_, s);
-  std::vector<double> part(2 * nb);
-  ANEL_CUDA_TRY(cudaMemcpyAsync(part.data(), d_part_, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, s));
-  ANEL_CUDA_TRY(cudaMemcpyAsync(h_red_ + 1, d_red_ + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+  launch_fold_pairs(d_part_, nb, d_part_ + 2 * nb, sums, s);
+  copy_words(d_red_ + 1, h_red_ + 1, 1, s);
+  copy_words(sums, h_red_ + 2, 2, s);
   ANEL_CUDA_TRY(cudaStreamSynchronize(s));
-  double a = 0.0, b = 0.0;
-  for (int64_t q = 0; q < nb; ++q) {
-    a += part[2 * q];
-    b += part[2 * q + 1];
-  }
-  out[0] = a / b;
+  out[0] = h_red_[2] / h_red_[3];
   out[1] = h_red_[1];
   return check_launch("divergence");
 }

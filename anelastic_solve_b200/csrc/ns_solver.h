@@ -21,6 +21,14 @@ class NSSolver {
   int substep(double a1, double a2, double a3, double dt_rk, double dt, cudaStream_t s, int* iters,
               double* relmax, bool q_zero = false);
   int step(int nsteps, cudaStream_t s, anel_step_report* rep);
+  // nsteps from the host state `in` to the host state `out` (may be the
+  // same arrays): the fields are copied in, stepped and copied out, with
+  // the copy of p in overlapping sub-step 1 up to its pressure solve and
+  // the copies of rho/scal1 and p out overlapping the last sub-step's
+  // pressure solve and Pgrad.  Results equal set_fields + step +
+  // get_fields.
+  int step_host(const anel_fields* in, const anel_fields* out, int nsteps, cudaStream_t s,
+                anel_step_report* rep);
   int project(cudaStream_t s, int* iters, double* relmax);
   int divergence(cudaStream_t s, double* out);
   // Re-target a context to a new member with the same grid, models and
@@ -99,6 +107,13 @@ class NSSolver {
   const double* d_dyn_ax_[6] = {nullptr};
   double dyn_area_ = 0.0;
   bool dyn_ready_ = false;  // dyn_prepare done for the current les_coeffs
+  // host-state stepping (step_host): copy stream, events and the hooks
+  // the sub-steps read
+  cudaStream_t io_stream_ = nullptr;
+  cudaEvent_t io_ev_[4] = {nullptr, nullptr, nullptr, nullptr};  // p in, rho out, p out, all in
+  bool io_wait_p_ = false;       // the next pressure solve waits for p's copy in
+  bool io_last_sub_ = false;     // this sub-step is the last of the call
+  const anel_fields* io_out_ = nullptr;
   int ensure_dyn();
   int dyn_prepare(cudaStream_t s);
   void dyn_filter(const double* in, double* out, int vt, int hf, cudaStream_t s);

@@ -82,6 +82,20 @@ class NSSolver:
         check(lib().anel_ns_ctx_step(self._h, int(n), s, C.byref(rep)))
         return rep
 
+    def step_host(self, fields_in: dict, fields_out: dict, n: int = 1, stream=None) -> abi.StepReport:
+        """n steps from host arrays fields_in to host arrays fields_out (may
+        be the same dict), copies overlapped with the step where the data
+        allow it (anel_ns_ctx_step_host).  Use pinned arrays for
+        asynchronous copies."""
+        fi, mi = self._fields(fields_in)
+        fo, mo = self._fields(fields_out)
+        if mi != abi.MEM_HOST or mo != abi.MEM_HOST:
+            raise TypeError("step_host takes host arrays")
+        rep = abi.StepReport()
+        s = C.c_void_p(int(stream)) if stream is not None else None
+        check(lib().anel_ns_ctx_step_host(self._h, C.byref(fi), C.byref(fo), int(n), s, C.byref(rep)))
+        return rep
+
     def set_profiling(self, on: bool):
         check(lib().anel_ns_ctx_set_profiling(self._h, 1 if on else 0))
 

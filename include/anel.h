@@ -282,6 +282,15 @@ int anel_ns_ctx_substep(anel_ns_ctx* ctx, double a1, double a2, double a3, doubl
  * output/statistics diagnostics): calcdt, gravity, LES update, three
  * sub-steps.  report (may be NULL) describes the last step. */
 int anel_ns_ctx_step(anel_ns_ctx* ctx, int32_t nsteps, void* stream, anel_step_report* report);
+/* nsteps from host fields `in` to host fields `out` (the same arrays
+ * allowed; null members are skipped): the caller's state stays in host
+ * memory, as with the reference's rk_ss on its module arrays.  The copy
+ * of p in overlaps sub-step 1 up to its pressure solve, the copies of rho,
+ * scal1 and p out overlap the last sub-step's pressure solve and Pgrad;
+ * the results equal set_fields + step + get_fields.  Pinned host memory
+ * lets the copies run asynchronously. */
+int anel_ns_ctx_step_host(anel_ns_ctx* ctx, const anel_fields* in, const anel_fields* out, int32_t nsteps,
+                          void* stream, anel_step_report* report);
 /* Profiling of the multigrid inside the steps (see
  * anel_mg_ctx_set_profiling); totals land in the step report. */
 int anel_ns_ctx_set_profiling(anel_ns_ctx* ctx, int32_t on);

@@ -191,3 +191,23 @@ def test_les_mixed_precision_within_tolerance():
     got = s.get_fields(CMP + ("nuT",))
     for name in ("u", "v", "w", "rho", "nuT"):
         assert rel_l2(got[name], f[name]) < 1e-8, name
+
+
+def test_step_host_equals_device_steps():
+    """anel_ns_ctx_step_host (host state in and out, copies overlapped with
+    the step) gives the same fields as set_fields + step + get_fields."""
+    import torch
+
+    g_, o, s, f, start = setup_case(ew=1, precision=abi.PREC_MIXED)
+    keys = ("u", "v", "w", "p", "rho", "scal1")
+    host = {k: np.asfortranarray(torch.zeros(g_.ghosted[::-1], dtype=torch.float64).pin_memory().numpy().T)
+            for k in keys}
+    for k in keys:
+        host[k][...] = start[k]
+    for _ in range(2):
+        s.step_host(host, host, 1)
+    ref = setup_case(ew=1, precision=abi.PREC_MIXED)[2]  # same start, device-resident steps
+    ref.step(2)
+    got = ref.get_fields(keys)
+    for k in keys:
+        np.testing.assert_array_equal(host[k], got[k], err_msg=k)
