@@ -54,7 +54,7 @@ WORKLOADS = {
     # eddy diffusivity with Pr_sgs = 0.7
     "les": ("dns", (768, 384, 384), (9, 8, 8), dict(Re=50000.0, g=-0.1, amp=1e-2, cfl=0.5, les=True)),
     "les_small": ("dns", (96, 48, 48), (6, 5, 5), dict(Re=50000.0, g=-0.1, amp=1e-2, cfl=0.5, les=True)),
-    # config 3's grid with the reference runfile's dynamic models (DSM,
+    # the 768x384x384 LES grid with the reference runfile's dynamic models (DSM,
     # DSMrho, DSMscal1; TestGrid_ratio sqrt(6), filters in x, y, z)
     "les_dsm": ("dns", (768, 384, 384), (9, 8, 8), dict(Re=50000.0, g=-0.1, amp=1e-2, cfl=0.5, les=True,
                                                        dsm=True)),

@@ -7,7 +7,7 @@ The profiles are host inputs (no GPU arithmetic): their test checks the
 single-precision literal semantics and the stratification.  On the GPU the
 FP64 multigrid passes and capped solves, and the FP64 steps, must be
 bit-identical to the oracle with the same profiles; the mixed-precision
-step stays within north_star's 1e-8 relative L2 of the FP64 oracle.
+step stays within the 1e-8 relative L2 field tolerance of the FP64 oracle.
 """
 import numpy as np
 import pytest

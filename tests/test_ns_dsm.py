@@ -5,7 +5,7 @@ les/filter.F90 and the reference's x-y plane averaging of the coefficients.
 Every per-cell expression equals the oracle's; the plane averages are a
 parallel fixed-order sum on the GPU and a running sum in the oracle, so the
 eddy viscosity and diffusivities after a step agree within 1e-9 relative to
-their largest magnitude, and the fields after two steps within north_star's
+their largest magnitude, and the fields after two steps within the
 1e-8 relative L2.  Cases: the reference runfile's setup (Vel/Rho/Scal1 =
 DSM/DSMrho/DSMscal1, TestGrid_ratio = sqrt(6), filters in x, y and z,
 uniform grids; run_dir/Sturb.ini:8-18, 89-91), and a tanh-stretched z axis

@@ -71,7 +71,7 @@ def test_steps_bitwise(ew):
 
 
 def test_divergence_bound_after_steps():
-    """north_star bound: max|div u| <= 1e-10 max|u| / dz_min (ew = 1)."""
+    """Divergence bound: max|div u| <= 1e-10 max|u| / dz_min (ew = 1)."""
     g_, o, s, f, start = setup_case(ew=1)
     rep = s.step(3)
     got = s.get_fields(("u", "v", "w"))
@@ -137,7 +137,7 @@ def test_shear_layer_config0_20_steps():
 
 
 def test_mixed_precision_stepper_within_tolerance():
-    """Mixed-precision MG inside the projection (config 2/3 form): fields
+    """Mixed-precision MG inside the projection (the DNS and LES form): fields
     within 1e-8 rel L2 of the FP64 oracle after 5 steps; MG solved to
     1e-12 so the projection error stays below the tolerance."""
     g_, o, s, f, start = setup_case(precision=abi.PREC_MIXED, tol=1e-12)
@@ -163,7 +163,7 @@ LES_CASES = {
 
 @pytest.mark.parametrize("case", list(LES_CASES))
 def test_les_steps_bitwise(case):
-    """LES of the shear layer (config 3 form, SSM_const 0.0289, Pr_sgs 0.7,
+    """LES of the shear layer (the 768x384x384 LES setup: SSM_const 0.0289, Pr_sgs 0.7,
     Re 50000, Ri 0.1, amplitude 1e-2): SGSdiff, the eddy terms of every RHS
     and the per-column LES Crank-Nicolson solve, FP64 GPU == oracle bitwise
     after four steps, eddy viscosities included."""
