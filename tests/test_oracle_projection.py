@@ -11,7 +11,9 @@ diagnostics (CPU only).
 After the oracle's initial projection, solved to a relative residual of
 1e-12, the restated divergence equals the oracle's report.  It is within
 the bound max|div u| <= 1e-10 max|u| / dz_min for r = 1, and the restated
-Psource is below 1e-9 of its value before the projection for r(z).
+Psource is below 1e-9 of its value before the projection for r(z).  The
+first step's time step is calcdt's (dns/Routines.F90:186-258, capped by
+dtmax as in dns/NSsolver.F90:72-73), restated in its own sum order.
 """
 import numpy as np
 import pytest
@@ -48,11 +50,12 @@ def psource(f, g):
             + (rp * w[1:-1, 1:-1, 1:-1] - rm * w[1:-1, 1:-1, :-2]) * _bc(g.z.rdxc[1:-1], 2))
 
 
-def _projected(anel):
+def _projected(anel, cfl=None):
     g = G.shear_layer_grid(32, 16, 32, stretched=True)
     mgp = abi.make_mg_params(levels_for(g), maxcy=300, tolmax=1e-12, tbc=(0, 1, 0, 1, 0, 0),
                              mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE, stop=abi.STOP_RESID)
-    nsp = abi.make_ns_params(Re=1000.0, Pr=1.0, g=-0.12, dtmax=0.01, ew=1, scal1_on=1)
+    kw = {"cfl": cfl, "dtmax": 1e9} if cfl else {"dtmax": 0.01}
+    nsp = abi.make_ns_params(Re=1000.0, Pr=1.0, g=-0.12, ew=1, scal1_on=1, **kw)
     f = shear.shear_layer_fields(g, amp=1e-2)
     if anel:
         anelastic.set_density_bg(f, g, x3center=-1000.0)
@@ -83,3 +86,13 @@ def test_anelastic_projection_zeroes_psource():
     assert np.abs(after).max() <= 1e-9 * np.abs(before).max()
     # the plain divergence is not what the anelastic projection zeroes
     assert np.abs(divergence(f, g)).max() > 1e3 * np.abs(after).max()
+
+
+def test_calcdt_restated():
+    g, f, o, _ = _projected(False, cfl=0.5)
+    u, v, w = f["u"], f["v"], f["w"]
+    adv = _bc(g.x.rdxc[1:-1], 0) * np.abs(0.5 * (u[1:-1, 1:-1, 1:-1] + u[:-2, 1:-1, 1:-1]))
+    adv = adv + _bc(g.z.rdxc[1:-1], 2) * np.abs(0.5 * (w[1:-1, 1:-1, 1:-1] + w[1:-1, 1:-1, :-2]))
+    adv = adv + _bc(g.y.rdxc[1:-1], 1) * np.abs(0.5 * (v[1:-1, 1:-1, 1:-1] + v[1:-1, :-2, 1:-1]))
+    dt = min(0.5 / adv.max(), 1e9)
+    assert o.step().dt == dt
