@@ -1471,6 +1471,18 @@ int orc_ns_project(orc_ns* s, int* iters, double* relmax) {
 /* ghost() of one field by type name index (tests) */
 void orc_ns_ghost(orc_ns* s, double* var, int vt) { ghost(s, var, vt); }
 
+/* one explicit right-hand side on the bound fields (tests) */
+void orc_ns_rhs(orc_ns* s, int which, double* out) {
+  gravity(s);
+  switch (which) {
+    case 0: u1_rhs(s, out); break;
+    case 1: u2_rhs(s, out); break;
+    case 2: u3_rhs(s, out); break;
+    case 3: scalar_rhs(s, out, 1); break;
+    default: scalar_rhs(s, out, 0); break;
+  }
+}
+
 /* divergence (Routines.F90:54-183): out[0] avg, out[1] max |div| */
 void orc_ns_divergence(orc_ns* s, double* out) {
   const orc_dom* D = &s->d;

@@ -67,6 +67,10 @@ void orc_ns_divergence(orc_ns* s, double* out);
 /* vt: 0 u 1 v 2 w 3 p 4 rho 5 cfluc 6 psource 7 utemp 8 vtemp 9 wtemp
  *     10 rtemp 11 s1temp 12 scal1 13 scal1temp */
 void orc_ns_ghost(orc_ns* s, double* var, int vt);
+/* explicit right-hand side of one field on the bound fields (tests):
+ * which 0..4 = u1_rhs, u2_rhs, u3_rhs, rho_rhs, scal1_rhs, into the ghosted
+ * array out (gravity at the context's current time) */
+void orc_ns_rhs(orc_ns* s, int which, double* out);
 /* the driver's per-step plane statistics (NSsolver.F90:288-395) on the
  * current fields: 16 profiles of nz+2 values into out */
 int orc_ns_diagnostics(orc_ns* s, int corrected, const int* stretched, double* out);

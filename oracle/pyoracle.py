@@ -118,6 +118,7 @@ def _ns_lib():
         L.orc_ns_project.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.orc_ns_divergence.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         L.orc_ns_ghost.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
+        L.orc_ns_rhs.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
         L.orc_ns_diagnostics.restype = C.c_int
         L.orc_ns_diagnostics.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L._ns_ready = True
@@ -176,6 +177,15 @@ class OracleNS:
 
     def ghost(self, a, vt: int):
         _ns_lib().orc_ns_ghost(self._h, abi.dptr(_f(a)), vt)
+
+    RHS = ("u", "v", "w", "rho", "scal1")
+
+    def rhs(self, name: str) -> np.ndarray:
+        """The explicit right-hand side of one field (u1_rhs .. scal1_rhs)
+        on the current fields, ghosted as the routine leaves it."""
+        out = np.zeros_like(self.fields["u"], order="F")
+        _ns_lib().orc_ns_rhs(self._h, self.RHS.index(name), abi.dptr(out))
+        return out
 
     def diagnostics(self, mode: int = abi.DIAG_LITERAL, stretched=(0, 0, 1)) -> dict:
         """The driver's per-step plane statistics (NSsolver.F90:288-395) on

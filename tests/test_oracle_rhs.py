@@ -1,0 +1,168 @@
+"""The oracle's explicit right-hand sides, restated from the reference
+(CPU only).
+
+u1_rhs, u2_rhs, u3_rhs, rho_rhs and scal1_rhs
+(ANELASTIC_SL/dns/NSsolver.F90:585-2020, the DNS terms of the
+Crank-Nicolson configuration: x/y diffusion, flux-form advection with the
+anelastic r(z) weights, buoyancy against densityBG) are written here as
+whole-array numpy expressions.  Each expression keeps the Fortran
+statement's operand order, so the interior values must equal the oracle's
+bit for bit.  The fields are random on a stretched grid with a non-uniform
+r(z) and densityBG(z), so every term and weight contributes.
+"""
+import numpy as np
+import pytest
+
+from anelastic_solve_b200 import abi, anelastic, shear
+from anelastic_solve_b200 import grid as G
+from oracle.pyoracle import OracleNS
+
+from .helpers import levels_for
+
+RE, PR, SC, GRAV = 1000.0, 0.7, 2.0, -0.12
+
+
+class _Shift:
+    """S(a, di, dj, dk): the interior block of a shifted by (di, dj, dk);
+    M(axis, name, off): a metric array at Fortran index i + off, broadcast
+    along its direction."""
+
+    def __init__(self, g):
+        self.g = g
+        self.n = g.shape
+
+    def S(self, a, di=0, dj=0, dk=0):
+        nx, ny, nz = self.n
+        return a[1 + di:1 + nx + di, 1 + dj:1 + ny + dj, 1 + dk:1 + nz + dk]
+
+    def M(self, d, name, off=0):
+        ax = (self.g.x, self.g.y, self.g.z)[d]
+        v = getattr(ax, name)[1 + off:1 + ax.n + off]
+        sl = [None, None, None]
+        sl[d] = slice(None)
+        return v[tuple(sl)]
+
+
+def u1_rhs(f, h, rRe):
+    S, M = h.S, h.M
+    u, v, w, r = f["u"], f["v"], f["w"], f["r"]
+    Ut = 0.0 + (rRe * ((S(u, 1) - S(u)) * M(0, "rdxc", 1) - (S(u) - S(u, -1)) * M(0, "rdxc")) * M(0, "rdxe")
+                + rRe * ((S(u, 0, 1) - S(u)) * M(1, "rdxe") - (S(u) - S(u, 0, -1)) * M(1, "rdxe", -1))
+                * M(1, "rdxc"))
+    ua2 = 0.5 * (S(u, 1) + S(u))
+    ua1 = 0.5 * (S(u) + S(u, -1))
+    Ut = Ut + (ua1 * ua1 - ua2 * ua2) * M(0, "rdxe")
+    ua2 = 0.5 * (S(u, 0, 0, 1) + S(u))
+    ua1 = 0.5 * (S(u) + S(u, 0, 0, -1))
+    ra2 = 0.5 * (S(r, 0, 0, 1) + S(r))
+    ra1 = 0.5 * (S(r) + S(r, 0, 0, -1))
+    wa2 = 0.5 * (S(w, 1) + S(w))
+    wa1 = 0.5 * (S(w, 1, 0, -1) + S(w, 0, 0, -1))
+    Ut = Ut + (ra1 * ua1 * wa1 - ra2 * ua2 * wa2) * M(2, "rdxc") / S(r)
+    ua2 = 0.5 * (S(u, 0, 1) + S(u))
+    ua1 = 0.5 * (S(u) + S(u, 0, -1))
+    va2 = 0.5 * (S(v, 1) + S(v))
+    va1 = 0.5 * (S(v, 1, -1) + S(v, 0, -1))
+    return Ut + (ua1 * va1 - ua2 * va2) * M(1, "rdxc")
+
+
+def u2_rhs(f, h, rRe):
+    S, M = h.S, h.M
+    u, v, w, r = f["u"], f["v"], f["w"], f["r"]
+    Vt = 0.0 + (rRe * ((S(v, 1) - S(v)) * M(0, "rdxe") - (S(v) - S(v, -1)) * M(0, "rdxe", -1)) * M(0, "rdxc")
+                + rRe * ((S(v, 0, 1) - S(v)) * M(1, "rdxc", 1) - (S(v) - S(v, 0, -1)) * M(1, "rdxc"))
+                * M(1, "rdxe"))
+    va1 = 0.5 * (S(v, 0, 1) + S(v))
+    va2 = 0.5 * (S(v) + S(v, 0, -1))
+    Vt = Vt - (va1 * va1 - va2 * va2) * M(1, "rdxe")
+    va1 = 0.5 * (S(v, 1) + S(v))
+    va2 = 0.5 * (S(v) + S(v, -1))
+    ua1 = 0.5 * (S(u, 0, 1) + S(u))
+    ua2 = 0.5 * (S(u, -1, 1) + S(u, -1))
+    Vt = Vt - (ua1 * va1 - ua2 * va2) * M(0, "rdxc")
+    va1 = 0.5 * (S(v, 0, 0, 1) + S(v))
+    va2 = 0.5 * (S(v) + S(v, 0, 0, -1))
+    ra1 = 0.5 * (S(r, 0, 0, 1) + S(r))
+    ra2 = 0.5 * (S(r) + S(r, 0, 0, -1))
+    wa1 = 0.5 * (S(w, 0, 1) + S(w))
+    wa2 = 0.5 * (S(w, 0, 1, -1) + S(w, 0, 0, -1))
+    return Vt - (ra1 * wa1 * va1 - ra2 * wa2 * va2) * M(2, "rdxc") / S(r)
+
+
+def u3_rhs(f, h, rRe, g, ew):
+    S, M = h.S, h.M
+    u, v, w, r, rho, bg = f["u"], f["v"], f["w"], f["r"], f["rho"], f["densityBG"]
+    Wt = 0.0 + 0.5 * g * ((S(rho, 0, 0, 1) - S(bg, 0, 0, 1)) + (S(rho) - S(bg))) / (
+        0.5 * (S(bg, 0, 0, 1) + S(bg)))
+    # Wtemp + x-term + y-term, added left to right onto the buoyancy
+    Wt = (Wt + rRe * ((S(w, 1) - S(w)) * M(0, "rdxe") - (S(w) - S(w, -1)) * M(0, "rdxe", -1)) * M(0, "rdxc")
+          + rRe * ((S(w, 0, 1) - S(w)) * M(1, "rdxe") - (S(w) - S(w, 0, -1)) * M(1, "rdxe", -1)) * M(1, "rdxc"))
+    wa1 = 0.5 * (S(w, 0, 0, 1) + S(w))
+    wa2 = 0.5 * (S(w) + S(w, 0, 0, -1))
+    Wt = Wt - (S(r) * wa1 * wa1 - S(r, 0, 0, 1) * wa2 * wa2) * M(2, "rdxe") / (0.5 * (S(r) + S(r, 0, 0, 1)))
+    wa1 = 0.5 * (S(w, 1) + S(w))
+    wa2 = 0.5 * (S(w) + S(w, -1))
+    ua1 = 0.5 * (S(u, 0, 0, 1) + S(u))
+    ua2 = 0.5 * (S(u, -1, 0, 1) + S(u, -1))
+    Wt = Wt - (ua1 * wa1 - ua2 * wa2) * M(0, "rdxc")
+    wa1 = 0.5 * (S(w, 0, 1) + S(w))
+    wa2 = 0.5 * (S(w) + S(w, 0, -1))
+    va1 = 0.5 * (S(v, 0, 0, 1) + S(v))
+    va2 = 0.5 * (S(v, 0, -1, 1) + S(v, 0, -1))
+    Wt = Wt - (va1 * wa1 - va2 * wa2) * M(1, "rdxc")
+    if ew:  # the loops run to k = ez - EW
+        Wt[:, :, -1] = 0.0
+    return Wt
+
+
+def scalar_rhs(f, h, name, D, r_weighted):
+    S, M = h.S, h.M
+    u, v, w, r, c = f["u"], f["v"], f["w"], f["r"], f[name]
+    St = 0.0 + (D * ((S(c, 1) - S(c)) * M(0, "rdxe") - (S(c) - S(c, -1)) * M(0, "rdxe", -1)) * M(0, "rdxc")
+                + D * ((S(c, 0, 1) - S(c)) * M(1, "rdxe") - (S(c) - S(c, 0, -1)) * M(1, "rdxe", -1))
+                * M(1, "rdxc"))
+    c2 = 0.5 * (S(c, 1) + S(c))
+    c1 = 0.5 * (S(c) + S(c, -1))
+    St = St + (S(u, -1) * c1 - S(u) * c2) * M(0, "rdxc")
+    c2 = 0.5 * (S(c, 0, 1) + S(c))
+    c1 = 0.5 * (S(c) + S(c, 0, -1))
+    St = St + (S(v, 0, -1) * c1 - S(v) * c2) * M(1, "rdxc")
+    c2 = 0.5 * (S(c, 0, 0, 1) + S(c))
+    c1 = 0.5 * (S(c) + S(c, 0, 0, -1))
+    if r_weighted:
+        ra2 = 0.5 * (S(r, 0, 0, 1) + S(r))
+        ra1 = 0.5 * (S(r) + S(r, 0, 0, -1))
+        return St + (ra1 * S(w, 0, 0, -1) * c1 - ra2 * S(w) * c2) * M(2, "rdxc") / S(r)
+    return St + (S(w, 0, 0, -1) * c1 - S(w) * c2) * M(2, "rdxc")
+
+
+@pytest.fixture(scope="module")
+def case():
+    g = G.shear_layer_grid(16, 8, 24, stretched=True)
+    mgp = abi.make_mg_params(levels_for(g), tbc=(0, 1, 0, 1, 0, 0), mode=abi.MODE_METRIC)
+    nsp = abi.make_ns_params(Re=RE, Pr=PR, Sc=SC, g=GRAV, ew=1, scal1_on=1)
+    rng = np.random.default_rng(3)
+    f = shear.shear_layer_fields(g)
+    for k in ("u", "v", "w", "rho", "scal1"):
+        f[k][...] = rng.standard_normal(g.ghosted)
+    anelastic.set_density_bg(f, g, x3center=-1000.0)
+    f["rho"] += f["densityBG"]
+    o = OracleNS(g, mgp, nsp, f)
+    for name, vt in (("u", 0), ("v", 1), ("w", 2), ("rho", 4), ("scal1", 12)):
+        o.ghost(f[name], vt)
+    return g, f, o
+
+
+@pytest.mark.parametrize("name", ["u", "v", "w", "rho", "scal1"])
+def test_rhs_equals_restatement(case, name):
+    g, f, o = case
+    h = _Shift(g)
+    rRe = 1.0 / RE
+    ref = {"u": lambda: u1_rhs(f, h, rRe),
+           "v": lambda: u2_rhs(f, h, rRe),
+           "w": lambda: u3_rhs(f, h, rRe, GRAV, ew=1),
+           "rho": lambda: scalar_rhs(f, h, "rho", rRe * (1.0 / PR), True),
+           "scal1": lambda: scalar_rhs(f, h, "scal1", rRe * (1.0 / SC), False)}[name]()
+    got = o.rhs(name)[1:-1, 1:-1, 1:-1]
+    assert np.abs(ref).max() > 0
+    np.testing.assert_array_equal(got, ref)
