@@ -1471,6 +1471,11 @@ int orc_ns_project(orc_ns* s, int* iters, double* relmax) {
 /* ghost() of one field by type name index (tests) */
 void orc_ns_ghost(orc_ns* s, double* var, int vt) { ghost(s, var, vt); }
 
+/* one Crank-Nicolson solve on caller arrays (tests) */
+void orc_ns_cn(orc_ns* s, const double* q, double* u, double a3, double rkdt, int var) {
+  cn_pl(s, q, u, a3, rkdt, var);
+}
+
 /* one explicit right-hand side on the bound fields (tests) */
 void orc_ns_rhs(orc_ns* s, int which, double* out) {
   gravity(s);

@@ -119,6 +119,8 @@ def _ns_lib():
         L.orc_ns_divergence.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         L.orc_ns_ghost.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
         L.orc_ns_rhs.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
+        L.orc_ns_cn.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                C.c_double, C.c_int]
         L.orc_ns_diagnostics.restype = C.c_int
         L.orc_ns_diagnostics.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L._ns_ready = True
@@ -177,6 +179,14 @@ class OracleNS:
 
     def ghost(self, a, vt: int):
         _ns_lib().orc_ns_ghost(self._h, abi.dptr(_f(a)), vt)
+
+    def crank_nicolson(self, q: np.ndarray, u: np.ndarray, a3: float, rkdt: float, var: int) -> np.ndarray:
+        """var_advance_CN_PL(q, u, 1, a3, 1, rkdt, var) on copies: the
+        solved, ghosted field (var 1 u, 2 v, 3 w, 5 rho, 8 scal1)."""
+        out = np.array(u, dtype=np.float64, order="F", copy=True)
+        qq = np.array(q, dtype=np.float64, order="F", copy=True)
+        _ns_lib().orc_ns_cn(self._h, abi.dptr(qq), abi.dptr(out), a3, rkdt, var)
+        return out
 
     RHS = ("u", "v", "w", "rho", "scal1")
 
