@@ -42,7 +42,7 @@ def thomas(a, b, c, G_):
     return G_
 
 
-def cn_restated(g, nsp, r, q, u, var):
+def cn_restated(g, nsp, r, q, u, var, a3=A3, rkdt=RKDT):
     """The solved interior of var_advance_CN_PL(q, u, 1, a3, 1, rkdt, var)."""
     nx, ny, nz = g.shape
     z = g.z
@@ -55,7 +55,7 @@ def cn_restated(g, nsp, r, q, u, var):
     k = np.arange(1, nz + 1)          # array index of Fortran k = 2..nz+1
     rdze, rdzc = z.rdxe, z.rdxc
     rk, rkp, rkm = R[:, :, k], R[:, :, k + 1], R[:, :, k - 1]
-    rhs[:, :, k] = 1.0 * U[:, :, k] + A3 * Q[:, :, k] * 1.0
+    rhs[:, :, k] = 1.0 * U[:, :, k] + a3 * Q[:, :, k] * 1.0
     if var != 3:
         raver1 = 0.5 * (rkp + rk)
         raver2 = 0.5 * (rk + rkm)
@@ -68,19 +68,19 @@ def cn_restated(g, nsp, r, q, u, var):
         else:
             t1 = np.broadcast_to(rRe * (1.0 / SC) + 0.0, rk.shape)
             t2 = t1
-        sub[:, :, k] = -0.5 * RKDT * t1 * rdze[k - 1] * rdzc[k]
-        sup[:, :, k] = -0.5 * RKDT * t2 * rdze[k] * rdzc[k]
-        diag[:, :, k] = 1.0 + 0.5 * RKDT * (t1 * rdze[k - 1] + t2 * rdze[k]) * rdzc[k]
-        rhs[:, :, k] = rhs[:, :, k] + RKDT * 0.5 * (
+        sub[:, :, k] = -0.5 * rkdt * t1 * rdze[k - 1] * rdzc[k]
+        sup[:, :, k] = -0.5 * rkdt * t2 * rdze[k] * rdzc[k]
+        diag[:, :, k] = 1.0 + 0.5 * rkdt * (t1 * rdze[k - 1] + t2 * rdze[k]) * rdzc[k]
+        rhs[:, :, k] = rhs[:, :, k] + rkdt * 0.5 * (
             t2 * (U[:, :, k + 1] - U[:, :, k]) * rdze[k] - t1 * (U[:, :, k] - U[:, :, k - 1]) * rdze[k - 1]
         ) * rdzc[k]
     else:
         t1 = (rRe + 0.0) * rk / (0.5 * (rkp + rk))
         t2 = (rRe + 0.0) * rkp / (0.5 * (rkp + rk))
-        sub[:, :, k] = -0.5 * RKDT * t1 * rdze[k] * rdzc[k]
-        sup[:, :, k] = -0.5 * RKDT * t2 * rdze[k] * rdzc[k + 1]
-        diag[:, :, k] = 1.0 + 0.5 * RKDT * (t1 * rdzc[k] + t2 * rdzc[k + 1]) * rdze[k]
-        rhs[:, :, k] = rhs[:, :, k] + RKDT * 0.5 * (
+        sub[:, :, k] = -0.5 * rkdt * t1 * rdze[k] * rdzc[k]
+        sup[:, :, k] = -0.5 * rkdt * t2 * rdze[k] * rdzc[k + 1]
+        diag[:, :, k] = 1.0 + 0.5 * rkdt * (t1 * rdzc[k] + t2 * rdzc[k + 1]) * rdze[k]
+        rhs[:, :, k] = rhs[:, :, k] + rkdt * 0.5 * (
             t2 * (U[:, :, k + 1] - U[:, :, k]) * rdzc[k + 1] - t1 * (U[:, :, k] - U[:, :, k - 1]) * rdzc[k]
         ) * rdze[k]
 

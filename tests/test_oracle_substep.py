@@ -1,0 +1,108 @@
+"""One RK sub-step of the oracle against the restated pieces (CPU only).
+
+rk_ss (ANELASTIC_SL/dns/NSsolver.F90:418-583, the Crank-Nicolson branch)
+is composed here from this suite's numpy restatements: the five explicit
+right-hand sides, var_advance, the Crank-Nicolson z solves, Psource, a
+dense direct solve of the pressure equation (the projection operator
+Psource(Pgrad(.)), so no multigrid is involved) and Pgrad
+(NSsolver.F90:2023-2085).  The boundary passes between those steps use
+the oracle's ghost() (the plumbing every piece shares).
+
+The scalars do not see the pressure, so rho and scal1 must equal the
+oracle's bit for bit.  The velocities agree to the pressure solve's
+accuracy: the oracle's multigrid is solved to a relative residual of 1e-13,
+so they are held to 1e-9 relative L2.  The case has a stretched z axis, an
+anelastic r(z), random velocities, scalars and RK accumulators, and the
+coefficients of the second RK3 sub-step, so every term contributes.
+"""
+import numpy as np
+
+from anelastic_solve_b200 import abi, anelastic, shear
+from anelastic_solve_b200 import grid as G
+from oracle.pyoracle import OracleNS
+
+from .helpers import levels_for, rel_l2
+from .test_oracle_cn import cn_restated
+from .test_oracle_direct import dense_operator, psource_pgrad, _wrap_xy
+from .test_oracle_projection import psource
+from .test_oracle_rhs import _Shift, scalar_rhs, u1_rhs, u2_rhs, u3_rhs
+
+RE, PR, SC, GRAV = 1000.0, 0.7, 2.0, -0.12
+# second sub-step of the low-storage RK3 (a1, a2, a3 = a1 + a2 of rk_ss)
+A1, A2 = -17.0 / 60.0, 5.0 / 12.0
+DT = 0.02
+VT = {"u": 0, "v": 1, "w": 2, "rho": 4, "scal1": 12, "q_u": 7, "q_v": 8, "q_w": 9, "q_rho": 10, "q_s": 11}
+
+
+def test_substep_equals_restated_composition():
+    g = G.shear_layer_grid(16, 8, 16, stretched=True)
+    mgp = abi.make_mg_params(levels_for(g), maxcy=300, tolmax=1e-13, tbc=(0, 1, 0, 1, 0, 0),
+                             mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE, stop=abi.STOP_RESID)
+    nsp = abi.make_ns_params(Re=RE, Pr=PR, Sc=SC, g=GRAV, ew=1, scal1_on=1)
+    rng = np.random.default_rng(17)
+    f = shear.shear_layer_fields(g)
+    for k in ("u", "v", "w", "rho", "scal1", "q_u", "q_v", "q_w", "q_rho", "q_s"):
+        f[k][...] = 0.1 * rng.standard_normal(g.ghosted)
+    anelastic.set_density_bg(f, g, x3center=-1000.0)
+    o = OracleNS(g, mgp, nsp, f)
+    for k in ("u", "v", "w", "rho", "scal1", "q_u", "q_v", "q_w", "q_rho", "q_s"):
+        o.ghost(f[k], VT[k])
+    n = {k: v.copy(order="F") for k, v in f.items()}  # the restated state
+    a3 = A1 + A2
+    dt_rk = a3 * DT
+
+    # the oracle's sub-step, in place on f
+    o.substep(A1, A2, a3, dt_rk, DT)
+
+    # the restated one on n
+    h = _Shift(g)
+    rRe = 1.0 / RE
+    rhs = {"q_u": u1_rhs(n, h, rRe), "q_v": u2_rhs(n, h, rRe), "q_w": u3_rhs(n, h, rRe, GRAV, ew=1),
+           "q_rho": scalar_rhs(n, h, "rho", rRe * (1.0 / PR), True),
+           "q_s": scalar_rhs(n, h, "scal1", rRe * (1.0 / SC), False)}
+    for q, F in rhs.items():  # var_advance(F, q, a1, a2, dt): q = a1 q + a2 F dt (interior)
+        n[q][1:-1, 1:-1, 1:-1] = A1 * n[q][1:-1, 1:-1, 1:-1] + A2 * F * DT
+        o.ghost(n[q], VT[q])
+
+    def cn(q, name, var):
+        n[name][1:-1, 1:-1, 1:-1] = cn_restated(g, nsp, n["r"], n[q], n[name], var, a3, dt_rk)
+        o.ghost(n[name], VT[name])
+
+    cn("q_u", "u", 1)
+    cn("q_v", "v", 2)
+    cn("q_w", "w", 3)
+    src = psource(n, g) * (1.0 / dt_rk)
+    cn("q_rho", "rho", 5)
+    cn("q_s", "scal1", 8)
+
+    # pressure: div(r grad(p/r)) = src, solved directly (null vector r)
+    r = n["r"]
+
+    def apply(p):
+        a = p.copy(order="F")
+        _wrap_xy(a)
+        return psource_pgrad(a, g, r)
+
+    A = dense_operator(apply, g)
+    p_int = np.linalg.lstsq(A, src.reshape(-1, order="F"), rcond=None)[0]
+    p = np.zeros(g.ghosted, order="F")
+    p[1:-1, 1:-1, 1:-1] = p_int.reshape(g.shape, order="F")
+    _wrap_xy(p)
+    # Pgrad with dt_rk, each velocity ghosted after its update
+    S, M = h.S, h.M
+    n["u"][1:-1, 1:-1, 1:-1] = S(n["u"]) - (S(p, 1) / S(r) - S(p) / S(r)) * M(0, "rdxe") * dt_rk
+    o.ghost(n["u"], VT["q_u"])
+    n["v"][1:-1, 1:-1, 1:-1] = S(n["v"]) - (S(p, 0, 1) / S(r) - S(p) / S(r)) * M(1, "rdxe") * dt_rk
+    o.ghost(n["v"], VT["q_v"])
+    w = n["w"][1:-1, 1:-1, 1:-1]
+    pw = S(p, 0, 0, 1)[:, :, :-1] / S(r, 0, 0, 1)[:, :, :-1] - S(p)[:, :, :-1] / S(r)[:, :, :-1]
+    w[:, :, :-1] = w[:, :, :-1] - pw * M(2, "rdxe")[:, :, :-1] * dt_rk  # k = sz..ez-EW
+    o.ghost(n["w"], VT["q_w"])
+    for k in ("u", "v", "w", "rho", "scal1"):
+        o.ghost(n[k], VT[k])
+
+    for k in ("rho", "scal1"):
+        np.testing.assert_array_equal(n[k][1:-1, 1:-1, 1:-1], f[k][1:-1, 1:-1, 1:-1], err_msg=k)
+    for k in ("u", "v", "w"):
+        assert rel_l2(n[k], f[k]) < 1e-9, (k, rel_l2(n[k], f[k]))
+        assert rel_l2(n[k], f[k]) > 0.0  # not the oracle's own numbers
