@@ -8,7 +8,8 @@ explicit half of the z diffusion in the right-hand side, the wall rows of
 the boundary codes TB (free-slip walls: u, v Neumann; w Dirichlet, with the
 edge-node row when ew = 1; rho and scal1 Neumann on two rows each side),
 and the reference's Thomas routine (mgMK/mg_relax.F90:541-595) over
-k = 1..nz+2, vectorised across columns; then the parts of the field's ghost
+k = 1..nz+2, vectorised across columns, with and without the LES eddy
+terms (random nuT, kappaT, nappaT); then the parts of the field's ghost
 pass that touch the interior (w's edge node, the scalars' two-point
 Neumann rows).  Every expression keeps the
 Fortran operand order, so the interior of the solved field must equal the
@@ -42,8 +43,41 @@ def thomas(a, b, c, G_):
     return G_
 
 
-def cn_restated(g, nsp, r, q, u, var, a3=A3, rkdt=RKDT):
-    """The solved interior of var_advance_CN_PL(q, u, 1, a3, 1, rkdt, var)."""
+def _eddy_pair(var, E, g, R, k):
+    """The LES face coefficients (tmp1, tmp2) of var_advance_CN_PL
+    (NSsolver.F90:3130-3160) on the interior columns, or None without LES.
+    u and v pair the upper-face density average with the lower-face eddy
+    average, as the reference writes them."""
+    if E is None:
+        return None
+    nx, ny, _ = g.shape
+
+    def col(a, di=0, dj=0):
+        return a[1 + di:nx + 1 + di, 1 + dj:ny + 1 + dj, :]
+
+    rk, rkp, rkm = R[:, :, k], R[:, :, k + 1], R[:, :, k - 1]
+    if var == 3:
+        nu = col(E["nuT"])
+        return (-nu[:, :, k] * rk / (0.5 * (rkp + rk)), -nu[:, :, k + 1] * rkp / (0.5 * (rkp + rk)))
+    raver1 = 0.5 * (rkp + rk)
+    raver2 = 0.5 * (rk + rkm)
+    if var in (1, 2):
+        a, b = col(E["nuT"]), col(E["nuT"], 1, 0) if var == 1 else col(E["nuT"], 0, 1)
+        t1 = -0.25 * (a[:, :, k] + b[:, :, k] + a[:, :, k - 1] + b[:, :, k - 1]) * raver1 / rk
+        t2 = -0.25 * (a[:, :, k] + b[:, :, k] + a[:, :, k + 1] + b[:, :, k + 1]) * raver2 / rk
+        return t1, t2
+    kT = col(E["kappaT"] if var == 5 else E["nappaT"])
+    t1 = -0.5 * (kT[:, :, k] + kT[:, :, k - 1])
+    t2 = -0.5 * (kT[:, :, k] + kT[:, :, k + 1])
+    if var == 5:
+        t1 = t1 * raver1 / rk
+        t2 = t2 * raver2 / rk
+    return t1, t2
+
+
+def cn_restated(g, nsp, r, q, u, var, a3=A3, rkdt=RKDT, eddy=None):
+    """The solved interior of var_advance_CN_PL(q, u, 1, a3, 1, rkdt, var);
+    eddy = {nuT, kappaT, nappaT} (ghosted) adds the LES terms."""
     nx, ny, nz = g.shape
     z = g.z
     rRe = 1.0 / RE
@@ -74,6 +108,15 @@ def cn_restated(g, nsp, r, q, u, var, a3=A3, rkdt=RKDT):
         rhs[:, :, k] = rhs[:, :, k] + rkdt * 0.5 * (
             t2 * (U[:, :, k + 1] - U[:, :, k]) * rdze[k] - t1 * (U[:, :, k] - U[:, :, k - 1]) * rdze[k - 1]
         ) * rdzc[k]
+        e = _eddy_pair(var, eddy, g, R, k)
+        if e is not None:
+            e1, e2 = e
+            sub[:, :, k] = sub[:, :, k] - 1 * 0.5 * rkdt * e1 * rdze[k - 1] * rdzc[k]
+            sup[:, :, k] = sup[:, :, k] - 1 * 0.5 * rkdt * e2 * rdze[k] * rdzc[k]
+            diag[:, :, k] = diag[:, :, k] + 1 * 0.5 * rkdt * (e1 * rdze[k - 1] + e2 * rdze[k]) * rdzc[k]
+            rhs[:, :, k] = rhs[:, :, k] + 1 * rkdt * 0.5 * (
+                e2 * (U[:, :, k + 1] - U[:, :, k]) * rdze[k] - e1 * (U[:, :, k] - U[:, :, k - 1]) * rdze[k - 1]
+            ) * rdzc[k]
     else:
         t1 = (rRe + 0.0) * rk / (0.5 * (rkp + rk))
         t2 = (rRe + 0.0) * rkp / (0.5 * (rkp + rk))
@@ -83,6 +126,15 @@ def cn_restated(g, nsp, r, q, u, var, a3=A3, rkdt=RKDT):
         rhs[:, :, k] = rhs[:, :, k] + rkdt * 0.5 * (
             t2 * (U[:, :, k + 1] - U[:, :, k]) * rdzc[k + 1] - t1 * (U[:, :, k] - U[:, :, k - 1]) * rdzc[k]
         ) * rdze[k]
+        e = _eddy_pair(var, eddy, g, R, k)
+        if e is not None:
+            e1, e2 = e
+            sub[:, :, k] = sub[:, :, k] - 1 * 1.0 * rkdt * e1 * rdze[k] * rdzc[k]
+            sup[:, :, k] = sup[:, :, k] - 1 * 1.0 * rkdt * e2 * rdze[k] * rdzc[k + 1]
+            diag[:, :, k] = diag[:, :, k] + 1 * 1.0 * rkdt * (e1 * rdzc[k] + e2 * rdzc[k + 1]) * rdze[k]
+            rhs[:, :, k] = rhs[:, :, k] + 1 * rkdt * 1.0 * (
+                e2 * (U[:, :, k + 1] - U[:, :, k]) * rdzc[k + 1] - e1 * (U[:, :, k] - U[:, :, k - 1]) * rdzc[k]
+            ) * rdze[k]
 
     def row(kk, a, b, c, d):
         sub[:, :, kk], diag[:, :, kk], sup[:, :, kk], rhs[:, :, kk] = a, b, c, d
@@ -127,25 +179,32 @@ def cn_restated(g, nsp, r, q, u, var, a3=A3, rkdt=RKDT):
     return x
 
 
-@pytest.fixture(scope="module")
-def case():
+@pytest.fixture(scope="module", params=[False, True], ids=["dns", "les"])
+def case(request):
+    les = request.param
     g = G.shear_layer_grid(12, 8, 20, stretched=True)
     mgp = abi.make_mg_params(levels_for(g), tbc=(0, 1, 0, 1, 0, 0), mode=abi.MODE_METRIC)
-    nsp = abi.make_ns_params(Re=RE, Pr=PR, Sc=SC, ew=1, scal1_on=1)
+    nsp = abi.make_ns_params(Re=RE, Pr=PR, Sc=SC, ew=1, scal1_on=1, les=les)
     f = shear.shear_layer_fields(g)
+    eddy = None
+    if les:  # eddy coefficients of either sign, ghosts included
+        rng = np.random.default_rng(99)
+        for k in ("nuT", "kappaT", "nappaT"):
+            f[k] = np.asfortranarray(0.01 * rng.standard_normal(g.ghosted))
+        eddy = {k: f[k] for k in ("nuT", "kappaT", "nappaT")}
     anelastic.set_density_bg(f, g, x3center=-1000.0)
     o = OracleNS(g, mgp, nsp, f)
-    return g, nsp, f, o
+    return g, nsp, f, o, eddy
 
 
 @pytest.mark.parametrize("var", [1, 2, 3, 5, 8])
 def test_crank_nicolson_equals_restatement(case, var):
-    g, nsp, f, o = case
+    g, nsp, f, o, eddy = case
     rng = np.random.default_rng(var)
     u = np.asfortranarray(rng.standard_normal(g.ghosted))
     q = np.asfortranarray(rng.standard_normal(g.ghosted))
     got = o.crank_nicolson(q, u, A3, RKDT, var)[1:-1, 1:-1, 1:-1]
-    ref = cn_restated(g, nsp, f["r"], q, u, var)
+    ref = cn_restated(g, nsp, f["r"], q, u, var, eddy=eddy)
     assert np.abs(ref).max() > 0
     if var == 3:
         # ew = 1: the ghost pass that follows the solve makes w at the top
