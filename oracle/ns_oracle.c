@@ -1476,6 +1476,12 @@ void orc_ns_cn(orc_ns* s, const double* q, double* u, double a3, double rkdt, in
   cn_pl(s, q, u, a3, rkdt, var);
 }
 
+/* the LES update on the bound fields (tests) */
+void orc_ns_les_update(orc_ns* s) {
+  les_coeffs(s);
+  sgsdiff(s);
+}
+
 /* one explicit right-hand side on the bound fields (tests) */
 void orc_ns_rhs(orc_ns* s, int which, double* out) {
   gravity(s);

@@ -74,6 +74,9 @@ void orc_ns_rhs(orc_ns* s, int which, double* out);
 /* var_advance_CN_PL(q, u, 1, a3, 1, rkdt, var) (tests): u is replaced by
  * the solved, ghosted field; var 1 u, 2 v, 3 w, 5 rho, 8 scal1 */
 void orc_ns_cn(orc_ns* s, const double* q, double* u, double a3, double rkdt, int var);
+/* the LES update on the bound fields (tests): model coefficients, then
+ * SGSdiff's nuT, kappaT, nappaT */
+void orc_ns_les_update(orc_ns* s);
 /* the driver's per-step plane statistics (NSsolver.F90:288-395) on the
  * current fields: 16 profiles of nz+2 values into out */
 int orc_ns_diagnostics(orc_ns* s, int corrected, const int* stretched, double* out);

@@ -121,6 +121,7 @@ def _ns_lib():
         L.orc_ns_rhs.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
         L.orc_ns_cn.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
                                 C.c_double, C.c_int]
+        L.orc_ns_les_update.argtypes = [C.c_void_p]
         L.orc_ns_diagnostics.restype = C.c_int
         L.orc_ns_diagnostics.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L._ns_ready = True
@@ -187,6 +188,11 @@ class OracleNS:
         qq = np.array(q, dtype=np.float64, order="F", copy=True)
         _ns_lib().orc_ns_cn(self._h, abi.dptr(qq), abi.dptr(out), a3, rkdt, var)
         return out
+
+    def les_update(self):
+        """The model coefficients and SGSdiff's nuT, kappaT, nappaT from the
+        current fields (into the bound arrays)."""
+        _ns_lib().orc_ns_les_update(self._h)
 
     RHS = ("u", "v", "w", "rho", "scal1")
 
