@@ -5,8 +5,8 @@ is composed here from this suite's numpy restatements: the five explicit
 right-hand sides, var_advance, the Crank-Nicolson z solves, Psource, a
 dense direct solve of the pressure equation (the projection operator
 Psource(Pgrad(.)), so no multigrid is involved) and Pgrad
-(NSsolver.F90:2023-2085).  The boundary passes between those steps use
-the oracle's ghost() (the plumbing every piece shares).
+(NSsolver.F90:2023-2085), with the restated boundary pass (ghost,
+dns/BC.F90) between them, so no routine of the oracle is used.
 
 The scalars do not see the pressure, so rho and scal1 must equal the
 oracle's bit for bit.  The velocities agree to the pressure solve's
@@ -24,6 +24,7 @@ from oracle.pyoracle import OracleNS
 from .helpers import levels_for, rel_l2
 from .test_oracle_cn import cn_restated
 from .test_oracle_direct import dense_operator, psource_pgrad, _wrap_xy
+from .test_oracle_ghost import ghost as ghost_restated
 from .test_oracle_projection import psource
 from .test_oracle_rhs import _Shift, scalar_rhs, u1_rhs, u2_rhs, u3_rhs
 
@@ -48,6 +49,9 @@ def test_substep_equals_restated_composition():
     for k in ("u", "v", "w", "rho", "scal1", "q_u", "q_v", "q_w", "q_rho", "q_s"):
         o.ghost(f[k], VT[k])
     n = {k: v.copy(order="F") for k, v in f.items()}  # the restated state
+
+    def gh(name):
+        ghost_restated(n[name], g, VT[name], nsp.tb, nsp.vb, 1)
     a3 = A1 + A2
     dt_rk = a3 * DT
 
@@ -62,11 +66,11 @@ def test_substep_equals_restated_composition():
            "q_s": scalar_rhs(n, h, "scal1", rRe * (1.0 / SC), False)}
     for q, F in rhs.items():  # var_advance(F, q, a1, a2, dt): q = a1 q + a2 F dt (interior)
         n[q][1:-1, 1:-1, 1:-1] = A1 * n[q][1:-1, 1:-1, 1:-1] + A2 * F * DT
-        o.ghost(n[q], VT[q])
+        gh(q)
 
     def cn(q, name, var):
         n[name][1:-1, 1:-1, 1:-1] = cn_restated(g, nsp, n["r"], n[q], n[name], var, a3, dt_rk)
-        o.ghost(n[name], VT[name])
+        gh(name)
 
     cn("q_u", "u", 1)
     cn("q_v", "v", 2)
@@ -91,15 +95,15 @@ def test_substep_equals_restated_composition():
     # Pgrad with dt_rk, each velocity ghosted after its update
     S, M = h.S, h.M
     n["u"][1:-1, 1:-1, 1:-1] = S(n["u"]) - (S(p, 1) / S(r) - S(p) / S(r)) * M(0, "rdxe") * dt_rk
-    o.ghost(n["u"], VT["q_u"])
+    ghost_restated(n["u"], g, VT["q_u"], nsp.tb, nsp.vb, 1)
     n["v"][1:-1, 1:-1, 1:-1] = S(n["v"]) - (S(p, 0, 1) / S(r) - S(p) / S(r)) * M(1, "rdxe") * dt_rk
-    o.ghost(n["v"], VT["q_v"])
+    ghost_restated(n["v"], g, VT["q_v"], nsp.tb, nsp.vb, 1)
     w = n["w"][1:-1, 1:-1, 1:-1]
     pw = S(p, 0, 0, 1)[:, :, :-1] / S(r, 0, 0, 1)[:, :, :-1] - S(p)[:, :, :-1] / S(r)[:, :, :-1]
     w[:, :, :-1] = w[:, :, :-1] - pw * M(2, "rdxe")[:, :, :-1] * dt_rk  # k = sz..ez-EW
-    o.ghost(n["w"], VT["q_w"])
+    ghost_restated(n["w"], g, VT["q_w"], nsp.tb, nsp.vb, 1)
     for k in ("u", "v", "w", "rho", "scal1"):
-        o.ghost(n[k], VT[k])
+        gh(k)
 
     for k in ("rho", "scal1"):
         np.testing.assert_array_equal(n[k][1:-1, 1:-1, 1:-1], f[k][1:-1, 1:-1, 1:-1], err_msg=k)
