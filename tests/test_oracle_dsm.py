@@ -9,10 +9,12 @@ center_velocity (dns/StatTools.F90:87-289), the x-y plane averages of
 avgX1X2 (dns/Average.F90:279-368, summed sequentially in its j-outer,
 i-inner order) and the restated boundary pass, all in numpy.  DSM's
 off-diagonal strain components subtract the two cross derivatives, as the
-source writes them.  On random velocities the oracle's dynamic Csgs, and the
-nuT that SGSdiff makes from it, must equal the restatement bit for bit, on
-the reference runfile's uniform grid with filters in x, y and z and with
-the filter off in one direction.
+source writes them.  DSMrho and DSMscal1 (les/DSMrho.F90:1-240, the
+same routine on scal1 in DSMscal1.F90) are restated the same way.  On
+random fields the oracle's nuT, kappaT and nappaT from the dynamic
+coefficients must equal the restatement bit for bit, on the reference
+runfile's uniform grid with filters in x, y and z, and for the velocity
+model also with the filter off in one direction.
 """
 import math
 
@@ -199,6 +201,70 @@ def dsm_csgs(c, f):
     return out, dg, modS
 
 
+def dsm_scalar(c, f, name):
+    """DSMrho / DSMscal1 (les/DSMrho.F90:1-240; DSMscal1.F90 is the same
+    routine on scal1) of the scalar `name`: the dynamic coefficient."""
+    g = c.g
+    h = _Shift(g)
+    S, M = h.S, h.M
+    inner = (slice(1, -1),) * 3
+    dg = np.broadcast_to(filter_width(h, abi.DELTA_3ROOT), (g.x.n, g.y.n, g.z.n))
+    modS = strain_magnitude(f, h)
+    filt_vel = {k: filter2(c, f[k], vt) for k, vt in (("u", VT_U), ("v", VT_V), ("w", VT_W))}
+    fmodS = np.zeros(g.ghosted, order="F")
+    fmodS[inner] = strain_magnitude(filt_vel, h)
+    c.ghost(fmodS, CFLUC)
+    q = f[name]
+    vel = (f["u"], f["v"], f["w"])
+    l4 = np.zeros(g.ghosted, order="F")
+    C = np.zeros(g.ghosted, order="F")
+    for ij in (1, 2, 3):
+        d = ij - 1
+        sh = [0, 0, 0]
+        sh[d] = 1
+        t1 = 0.5 * (S(q) + S(q, *[-v for v in sh]))
+        t2 = 0.5 * (S(q) + S(q, *sh))
+        rd = M(d, "rdxc")
+        l1 = np.zeros(g.ghosted, order="F")
+        l1[inner] = (dg * dg) * modS * (t2 - t1) * rd
+        c.ghost(l1, CFLUC)
+        l2 = filter2(c, l1, CFLUC)
+        l1 = np.zeros(g.ghosted, order="F")
+        l1[inner] = (t2 - t1) * rd
+        c.ghost(l1, CFLUC)
+        l3 = filter2(c, l1, CFLUC)
+        l1 = fmodS.copy(order="F")
+        rr = RATIO * dg
+        l2[inner] = l2[inner] - (rr * rr) * l1[inner] * l3[inner]
+        c.ghost(l2, CFLUC)
+        l1 = np.zeros(g.ghosted, order="F")
+        l1[inner] = S(q) * 0.5 * (S(vel[d], *[-v for v in sh]) + S(vel[d]))
+        c.ghost(l1, CFLUC)
+        l3 = filter2(c, l1, CFLUC)
+        fc = filter2(c, center_uniform(c, vel[d], d), CFLUC)
+        fq = filter2(c, q, CFLUC)
+        l3 = l3 - fq * fc
+        c.ghost(l3, CFLUC)
+        l4 = l4 + l2 * l2
+        C = C + l2 * l3
+    num, den = C.copy(order="F"), l4.copy(order="F")
+    c.ghost(num, CFLUC)
+    c.ghost(den, CFLUC)
+    pn, pd = avg_x1x2(c, num), avg_x1x2(c, den)
+    num[inner] = np.broadcast_to(pn[1:-1], num[inner].shape)
+    den[inner] = np.broadcast_to(pd[1:-1], den[inner].shape)
+    num[inner] = np.where(num[inner] < 0.0, 0.0, num[inner])
+    c.ghost(num, CFLUC)
+    c.ghost(den, CFLUC)
+    out = np.zeros(g.ghosted, order="F")
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out[inner] = np.where(den[inner] == 0.0, 1.0e-20, 0.5 * num[inner] / den[inner])
+    c.ghost(out, CFLUC)
+    out = filter_hf(c, out, CFLUC)
+    c.ghost(out, CFLUC)
+    return out, dg, modS
+
+
 @pytest.mark.parametrize("filt", [(1, 1, 1), (1, 0, 1)], ids=["xyz", "xz"])
 def test_dynamic_csgs_equals_restatement(filt):
     g = G.shear_layer_grid(16, 8, 16, stretched=False)
@@ -221,3 +287,27 @@ def test_dynamic_csgs_equals_restatement(filt):
     ref = -(csgs[1:-1, 1:-1, 1:-1] + 0.0) * (dg * dg) * modS + 0.0
     assert np.abs(ref).max() > 0
     np.testing.assert_array_equal(f["nuT"][1:-1, 1:-1, 1:-1], ref)
+
+
+def test_dynamic_scalar_models_equal_restatement():
+    """DSM, DSMrho and DSMscal1 together (the reference runfile's models)."""
+    g = G.shear_layer_grid(16, 8, 16, stretched=False)
+    mgp = abi.make_mg_params(levels_for(g), tbc=(0, 1, 0, 1, 0, 0), mode=abi.MODE_METRIC)
+    nsp = abi.make_ns_params(Re=50000.0, g=-0.1, ew=1, scal1_on=1, les=True, models=(abi.MODEL_DSM,) * 3,
+                             test_ratio=RATIO, filt=(1, 1, 1), stretched=(0, 0, 0), interp=abi.DIAG_LITERAL)
+    rng = np.random.default_rng(8)
+    f = shear.shear_layer_fields(g)
+    for k in ("u", "v", "w", "rho", "scal1"):
+        f[k][...] = rng.standard_normal(g.ghosted)
+    for k in ("nuT", "kappaT", "nappaT"):
+        f[k] = np.zeros(g.ghosted, order="F")
+    o = OracleNS(g, mgp, nsp, f)
+    c = _Ctx(g, nsp, (1, 1, 1))
+    for k, vt in (("u", VT_U), ("v", VT_V), ("w", VT_W), ("rho", 4), ("scal1", 12)):
+        c.ghost(f[k], vt)
+    o.les_update()
+    for name, eddy in (("rho", "kappaT"), ("scal1", "nappaT")):
+        C, dg, modS = dsm_scalar(c, f, name)
+        ref = -(C[1:-1, 1:-1, 1:-1] + 0.0) * (dg * dg) * modS + 0.0
+        assert np.abs(ref).max() > 0
+        np.testing.assert_array_equal(f[eddy][1:-1, 1:-1, 1:-1], ref, err_msg=eddy)
