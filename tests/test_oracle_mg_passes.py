@@ -1,0 +1,128 @@
+"""The oracle's finest-level multigrid passes, restated from the reference
+(CPU only).
+
+- mg_bdry (ANELASTIC_SL/mgMK/mg_bdry.F90:72-190), serial form: the periodic
+  wrap of all six ghost planes, then the faces in the order X2max, X3min,
+  X2min, X3max, X1min, X1max, each over its whole plane: Neumann
+  phi_g = phi_b -/+ phibc * dc (the level's cell size next to the face),
+  Dirichlet phi_g = phibc;
+- one mg_relaxRB iteration (mgMK/mg_relax.F90:85-179): colour (i+j+k) even,
+  boundary pass, colour odd, boundary pass, each cell
+  phi = (f - (c1 phi_W + c2 phi_E + c3 phi_S + c4 phi_N + c5 phi_B +
+  c6 phi_T)) / c7 in that order, with mgdpfpde's fine coefficients
+  (mgMK/mg_pfpde.F90:34-56, literal mode, anelastic r(z)).
+
+Both are numpy on whole planes or colours; the oracle's ghost cells and
+interior must equal them bit for bit, for periodic-x/y walls-in-z and for
+walls everywhere with non-zero boundary values.
+"""
+import numpy as np
+import pytest
+
+from anelastic_solve_b200 import abi, anelastic
+from anelastic_solve_b200 import grid as G
+from oracle.pyoracle import OracleMG
+
+from .helpers import levels_for
+
+CASES = {
+    "periodic_xy": ((0, 1, 0, 1, 0, 0), (0.0, 0.3, 0.0, -0.7, 0.0, 0.0)),
+    "walls": ((2, 1, 1, 2, 1, 2), (0.4, -0.2, 0.9, 1.3, -0.6, 0.25)),
+}
+
+
+def mg_bdry(phi, g, tbc, vbc):
+    p = phi
+    p[0, :, :] = p[-2, :, :]
+    p[-1, :, :] = p[1, :, :]
+    p[:, 0, :] = p[:, -2, :]
+    p[:, -1, :] = p[:, 1, :]
+    p[:, :, 0] = p[:, :, -2]
+    p[:, :, -1] = p[:, :, 1]
+    dx, dy, dz = g.x.dxc, g.y.dxc, g.z.dxc
+    nx, ny, nz = g.shape
+    # X2max, X3min, X2min, X3max, X1min, X1max
+    if tbc[0] == 1:
+        p[:, -1, :] = p[:, -2, :] + vbc[0] * dy[ny]
+    elif tbc[0] == 2:
+        p[:, -1, :] = vbc[0]
+    if tbc[1] == 1:
+        p[:, :, 0] = p[:, :, 1] - vbc[1] * dz[1]
+    elif tbc[1] == 2:
+        p[:, :, 0] = vbc[1]
+    if tbc[2] == 1:
+        p[:, 0, :] = p[:, 1, :] - vbc[2] * dy[1]
+    elif tbc[2] == 2:
+        p[:, 0, :] = vbc[2]
+    if tbc[3] == 1:
+        p[:, :, -1] = p[:, :, -2] + vbc[3] * dz[nz]
+    elif tbc[3] == 2:
+        p[:, :, -1] = vbc[3]
+    if tbc[4] == 1:
+        p[0, :, :] = p[1, :, :] - vbc[4] * dx[1]
+    elif tbc[4] == 2:
+        p[0, :, :] = vbc[4]
+    if tbc[5] == 1:
+        p[-1, :, :] = p[-2, :, :] + vbc[5] * dx[nx]
+    elif tbc[5] == 2:
+        p[-1, :, :] = vbc[5]
+
+
+def literal_coefficients(g, r):
+    """mgdpfpde: c1..c7 on the interior (r ghosted)."""
+    nx, ny, nz = g.shape
+    t = [1.0 / ((ax.L / float(np.float32(ax.n))) * (ax.L / float(np.float32(ax.n)))) for ax in (g.x, g.y, g.z)]
+    rk, rm, rp = r[1:-1, 1:-1, 1:-1], r[1:-1, 1:-1, :-2], r[1:-1, 1:-1, 2:]
+    h = float(np.float32(0.5))
+    c5 = t[2] * h * (rk + rm) / rm
+    c6 = t[2] * h * (rk + rp) / rp
+    c7 = -(t[0] + t[0] + t[1] + t[1] + (t[2] * h * (rk + rm) / rk) + (t[2] * h * (rk + rp) / rk))
+    return t[0], t[0], t[1], t[1], c5, c6, c7
+
+
+def rb_iteration(phi, src, g, r, tbc, vbc):
+    c1, c2, c3, c4, c5, c6, c7 = literal_coefficients(g, r)
+    nx, ny, nz = g.shape
+    i, j, k = np.meshgrid(np.arange(2, nx + 2), np.arange(2, ny + 2), np.arange(2, nz + 2), indexing="ij")
+    for colour in (0, 1):
+        p = phi
+        new = (src[1:-1, 1:-1, 1:-1] - (c1 * p[:-2, 1:-1, 1:-1] + c2 * p[2:, 1:-1, 1:-1] + c3 * p[1:-1, :-2, 1:-1]
+                                         + c4 * p[1:-1, 2:, 1:-1] + c5 * p[1:-1, 1:-1, :-2]
+                                         + c6 * p[1:-1, 1:-1, 2:])) / c7
+        mask = (i + j + k) % 2 == colour
+        p[1:-1, 1:-1, 1:-1] = np.where(mask, new, p[1:-1, 1:-1, 1:-1])
+        mg_bdry(phi, g, tbc, vbc)
+
+
+def _case(name):
+    tbc, vbc = CASES[name]
+    g = G.shear_layer_grid(16, 8, 16, stretched=True)
+    p = abi.make_mg_params(levels_for(g), tbc=tbc, vbc=vbc, mode=abi.MODE_LITERAL)
+    o = OracleMG(g, p)
+    f = {"r": np.zeros(g.ghosted, order="F"), "densityBG": np.zeros(g.ghosted, order="F")}
+    anelastic.set_density_bg(f, g, x3center=-1000.0)
+    o.set_density(f["r"])
+    return g, o, f["r"], tbc, vbc
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_boundary_pass_equals_restatement(name):
+    g, o, r, tbc, vbc = _case(name)
+    rng = np.random.default_rng(2)
+    phi = np.asfortranarray(rng.standard_normal(g.ghosted))
+    ref = phi.copy(order="F")
+    o.debug_pass(1, phi, np.zeros(g.ghosted, order="F"))
+    mg_bdry(ref, g, tbc, vbc)
+    np.testing.assert_array_equal(phi, ref)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_rb_iteration_equals_restatement(name):
+    g, o, r, tbc, vbc = _case(name)
+    rng = np.random.default_rng(4)
+    phi = np.asfortranarray(rng.standard_normal(g.ghosted))
+    src = np.asfortranarray(rng.standard_normal(g.ghosted))
+    ref = phi.copy(order="F")
+    o.debug_pass(0, phi, src.copy(order="F"))
+    rb_iteration(ref, src, g, r, tbc, vbc)
+    np.testing.assert_array_equal(phi, ref)
