@@ -10,9 +10,12 @@
   boundary pass, colour odd, boundary pass, each cell
   phi = (f - (c1 phi_W + c2 phi_E + c3 phi_S + c4 phi_N + c5 phi_B +
   c6 phi_T)) / c7 in that order, with mgdpfpde's fine coefficients
-  (mgMK/mg_pfpde.F90:34-56, literal mode, anelastic r(z)).
+  (mgMK/mg_pfpde.F90:34-56, literal mode, anelastic r(z));
+- one mg_relaxLz iteration (the LJ smoother, mgMK/mg_relax.F90:423-538):
+  (i+j) red-black z-lines with mg_coeff's 1-D coefficients and the
+  reference's Thomas routine.
 
-Both are numpy on whole planes or colours; the oracle's ghost cells and
+All are numpy on whole planes or colours; the oracle's ghost cells and
 interior must equal them bit for bit, for periodic-x/y walls-in-z and for
 walls everywhere with non-zero boundary values.
 """
@@ -125,4 +128,75 @@ def test_rb_iteration_equals_restatement(name):
     ref = phi.copy(order="F")
     o.debug_pass(0, phi, src.copy(order="F"))
     rb_iteration(ref, src, g, r, tbc, vbc)
+    np.testing.assert_array_equal(phi, ref)
+
+
+def pcf_fine(g, tbc):
+    """mg_coeff's 1-D line coefficients on the finest level
+    (mgMK/mg_coeff.F90:77-145): p1 = 1/(dxc(i) dxe(i-1)), p2 = 1/(dxc(i)
+    dxe(i)), and the same in y and z, with the finest level's Neumann
+    zeroing of the wall coefficients.  Arrays over the interior."""
+    out = []
+    for ax, lo, hi in ((g.x, 4, 5), (g.y, 2, 0), (g.z, 1, 3)):
+        n = ax.n
+        dc, de = ax.dxc[1:n + 1], ax.dxe
+        pm = 1.0 / (dc * de[0:n])
+        pp = 1.0 / (dc * de[1:n + 1])
+        if tbc[lo] == 1:
+            pm[0] = 0.0
+        if tbc[hi] == 1:
+            pp[-1] = 0.0
+        out += [pm, pp]
+    return out
+
+
+def lz_iteration(phi, src, g, tbc, vbc):
+    """One mg_relaxLz iteration (mgMK/mg_relax.F90:423-538): (i+j)
+    red-black z-lines, each the tridiagonal (a = p5, b = -(p1+p2+p3+p4+p5+p6),
+    c = p6) with the ghost term inside the neighbour sum of the end rows,
+    solved by the reference's Thomas routine; boundary pass per colour."""
+    p1, p2, p3, p4, p5, p6 = pcf_fine(g, tbc)
+    nx, ny, nz = g.shape
+    P1, P2 = p1[:, None, None], p2[:, None, None]
+    P3, P4 = p3[None, :, None], p4[None, :, None]
+    a = np.broadcast_to(p5[None, None, :], (nx, ny, nz)).copy()
+    b = np.broadcast_to(-(P1 + P2 + P3 + P4 + p5[None, None, :] + p6[None, None, :]), (nx, ny, nz)).copy()
+    c = np.broadcast_to(p6[None, None, :], (nx, ny, nz)).copy()
+    i, j = np.meshgrid(np.arange(2, nx + 2), np.arange(2, ny + 2), indexing="ij")
+    for colour in (0, 1):
+        p = phi
+        W, E = p[:-2, 1:-1, 1:-1], p[2:, 1:-1, 1:-1]
+        S_, N = p[1:-1, :-2, 1:-1], p[1:-1, 2:, 1:-1]
+        f = src[1:-1, 1:-1, 1:-1]
+        rhs = f - (P1 * W + P2 * E + P3 * S_ + P4 * N)
+        rhs[:, :, 0] = f[:, :, 0] - (P1[:, :, 0] * W[:, :, 0] + P2[:, :, 0] * E[:, :, 0] + P3[:, :, 0] * S_[:, :, 0]
+                                     + P4[:, :, 0] * N[:, :, 0] + p5[0] * p[1:-1, 1:-1, 0])
+        rhs[:, :, -1] = f[:, :, -1] - (P1[:, :, 0] * W[:, :, -1] + P2[:, :, 0] * E[:, :, -1]
+                                       + P3[:, :, 0] * S_[:, :, -1] + P4[:, :, 0] * N[:, :, -1]
+                                       + p6[-1] * p[1:-1, 1:-1, -1])
+        aa, bb, G_ = a.copy(), b.copy(), rhs
+        for q in range(nz - 1):
+            aa[..., q + 1] = -aa[..., q + 1] / bb[..., q]
+            bb[..., q + 1] = bb[..., q + 1] + aa[..., q + 1] * c[..., q]
+            G_[..., q + 1] = G_[..., q + 1] + aa[..., q + 1] * G_[..., q]
+        G_[..., nz - 1] = G_[..., nz - 1] / bb[..., nz - 1]
+        for q in range(nz - 2, -1, -1):
+            G_[..., q] = (G_[..., q] - c[..., q] * G_[..., q + 1]) / bb[..., q]
+        mask = ((i + j) % 2 == colour)[:, :, None]
+        p[1:-1, 1:-1, 1:-1] = np.where(mask, G_, p[1:-1, 1:-1, 1:-1])
+        mg_bdry(phi, g, tbc, vbc)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_lz_iteration_equals_restatement(name):
+    tbc, vbc = CASES[name]
+    g = G.shear_layer_grid(16, 8, 16, stretched=True)
+    p = abi.make_mg_params(levels_for(g), tbc=tbc, vbc=vbc, mode=abi.MODE_LITERAL, smoother=abi.SMOOTHER_LJ)
+    o = OracleMG(g, p)
+    rng = np.random.default_rng(6)
+    phi = np.asfortranarray(rng.standard_normal(g.ghosted))
+    src = np.asfortranarray(rng.standard_normal(g.ghosted))
+    ref = phi.copy(order="F")
+    o.debug_pass(0, phi, src.copy(order="F"))
+    lz_iteration(ref, src, g, tbc, vbc)
     np.testing.assert_array_equal(phi, ref)
