@@ -13,7 +13,10 @@
   (mgMK/mg_pfpde.F90:34-56, literal mode, anelastic r(z));
 - one mg_relaxLz iteration (the LJ smoother, mgMK/mg_relax.F90:423-538):
   (i+j) red-black z-lines with mg_coeff's 1-D coefficients and the
-  reference's Thomas routine.
+  reference's Thomas routine;
+- one iteration of this build's ZLINE smoother in metric mode, against its
+  description: (i+j) red-black z-lines of the level's own 7-point operator
+  (the projection's Psource(Pgrad(.)) with face densities), Thomas order.
 
 All are numpy on whole planes or colours; the oracle's ghost cells and
 interior must equal them bit for bit, for periodic-x/y walls-in-z and for
@@ -199,4 +202,89 @@ def test_lz_iteration_equals_restatement(name):
     ref = phi.copy(order="F")
     o.debug_pass(0, phi, src.copy(order="F"))
     lz_iteration(ref, src, g, tbc, vbc)
+    np.testing.assert_array_equal(phi, ref)
+
+
+def metric_coefficients(g, r, tbc):
+    """The metric-mode fine operator (this build's extension, the
+    projection's Psource(Pgrad(.)) in coefficient form): a1 = rdxc(i)
+    rdxe(i-1), a2 = rdxc(i) rdxe(i) and likewise in y and z, a Neumann wall
+    face's coefficient zeroed, the z ones weighted by the face densities,
+    and the diagonal minus the sum of the six."""
+    nx, ny, nz = g.shape
+
+    def pair(ax):
+        n = ax.n
+        return ax.rdxc[1:n + 1] * ax.rdxe[0:n], ax.rdxc[1:n + 1] * ax.rdxe[1:n + 1]
+
+    (a1, a2), (a3, a4), (a5, a6) = pair(g.x), pair(g.y), pair(g.z)
+    a1 = np.broadcast_to(a1[:, None, None], (nx, ny, nz)).copy()
+    a2 = np.broadcast_to(a2[:, None, None], (nx, ny, nz)).copy()
+    a3 = np.broadcast_to(a3[None, :, None], (nx, ny, nz)).copy()
+    a4 = np.broadcast_to(a4[None, :, None], (nx, ny, nz)).copy()
+    a5 = np.broadcast_to(a5[None, None, :], (nx, ny, nz)).copy()
+    a6 = np.broadcast_to(a6[None, None, :], (nx, ny, nz)).copy()
+    if tbc[4] == 1:
+        a1[0] = 0.0
+    if tbc[5] == 1:
+        a2[-1] = 0.0
+    if tbc[2] == 1:
+        a3[:, 0] = 0.0
+    if tbc[0] == 1:
+        a4[:, -1] = 0.0
+    if tbc[1] == 1:
+        a5[:, :, 0] = 0.0
+    if tbc[3] == 1:
+        a6[:, :, -1] = 0.0
+    rp, rb, rt = r[1:-1, 1:-1, 1:-1], r[1:-1, 1:-1, :-2], r[1:-1, 1:-1, 2:]
+    w5 = 0.5 * (rp + rb)
+    w6 = 0.5 * (rp + rt)
+    c7 = -(a1 + a2 + a3 + a4 + a5 * w5 / rp + a6 * w6 / rp)
+    return a1, a2, a3, a4, a5 * w5 / rb, a6 * w6 / rt, c7
+
+
+def zline_iteration(phi, src, g, r, tbc, vbc):
+    """One ZLINE iteration: (i+j) red-black z-lines of the level's own
+    7-point operator (a = c5, b = c7, c = c6; the ghost terms subtracted
+    after the horizontal neighbour sum), the reference's Thomas routine,
+    and the boundary pass after each colour."""
+    c1, c2, c3, c4, c5, c6, c7 = metric_coefficients(g, r, tbc)
+    nx, ny, nz = g.shape
+    i, j = np.meshgrid(np.arange(2, nx + 2), np.arange(2, ny + 2), indexing="ij")
+    for colour in (0, 1):
+        p = phi
+        rhs = src[1:-1, 1:-1, 1:-1] - (c1 * p[:-2, 1:-1, 1:-1] + c2 * p[2:, 1:-1, 1:-1] + c3 * p[1:-1, :-2, 1:-1]
+                                        + c4 * p[1:-1, 2:, 1:-1])
+        rhs[:, :, 0] = rhs[:, :, 0] - c5[:, :, 0] * p[1:-1, 1:-1, 0]
+        rhs[:, :, -1] = rhs[:, :, -1] - c6[:, :, -1] * p[1:-1, 1:-1, -1]
+        aa, bb, G_ = c5.copy(), c7.copy(), rhs
+        for q in range(nz - 1):
+            aa[..., q + 1] = -aa[..., q + 1] / bb[..., q]
+            bb[..., q + 1] = bb[..., q + 1] + aa[..., q + 1] * c6[..., q]
+            G_[..., q + 1] = G_[..., q + 1] + aa[..., q + 1] * G_[..., q]
+        G_[..., nz - 1] = G_[..., nz - 1] / bb[..., nz - 1]
+        for q in range(nz - 2, -1, -1):
+            G_[..., q] = (G_[..., q] - c6[..., q] * G_[..., q + 1]) / bb[..., q]
+        mask = ((i + j) % 2 == colour)[:, :, None]
+        p[1:-1, 1:-1, 1:-1] = np.where(mask, G_, p[1:-1, 1:-1, 1:-1])
+        mg_bdry(phi, g, tbc, vbc)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_zline_iteration_equals_restatement(name):
+    """The ZLINE smoother of the metric mode (this build's extension) against
+    its description, with an anelastic r(z) on the stretched grid."""
+    tbc, vbc = CASES[name]
+    g = G.shear_layer_grid(16, 8, 16, stretched=True)
+    p = abi.make_mg_params(levels_for(g), tbc=tbc, vbc=vbc, mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE)
+    o = OracleMG(g, p)
+    f = {"r": np.zeros(g.ghosted, order="F"), "densityBG": np.zeros(g.ghosted, order="F")}
+    anelastic.set_density_bg(f, g, x3center=-1000.0)
+    o.set_density(f["r"])
+    rng = np.random.default_rng(9)
+    phi = np.asfortranarray(rng.standard_normal(g.ghosted))
+    src = np.asfortranarray(rng.standard_normal(g.ghosted))
+    ref = phi.copy(order="F")
+    o.debug_pass(0, phi, src.copy(order="F"))
+    zline_iteration(ref, src, g, f["r"], tbc, vbc)
     np.testing.assert_array_equal(phi, ref)
