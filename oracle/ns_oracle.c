@@ -1420,6 +1420,22 @@ int orc_ns_step(orc_ns* s, anel_step_report* rep) {
   gravity(s);
   const int les = s->p.vmodel != ANEL_MODEL_DNS;
   if (les && s->nstep >= s->p.les_start && s->nstep % s->p.les_freq == 0) les_coeffs(s);
+  /* every 50 steps the scalar LES models smooth rho and scal1 with
+   * filterHF(.., 2, 1, 1, 1, 'rho' / 'scal1', ..) (NSsolver.F90:144-164;
+   * its EDIFF and tol arguments are unused, filter.F90:209,237,266): a
+   * whole-array copy back, then the field's ghost pass */
+  if (s->time > 0.0 && s->nstep % 50 == 0) {
+    if (s->p.rmodel != ANEL_MODEL_DNS) {
+      filterHF2(s, f->rho, s->work[3], VT_RHO);
+      memcpy(f->rho, s->work[3], sizeof(double) * G);
+      ghost(s, f->rho, VT_RHO);
+    }
+    if (s->p.smodel != ANEL_MODEL_DNS) {
+      filterHF2(s, f->scal1, s->work[3], VT_SCAL1);
+      memcpy(f->scal1, s->work[3], sizeof(double) * G);
+      ghost(s, f->scal1, VT_SCAL1);
+    }
+  }
   static const double A1[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
   static const double A3[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
   const double DTR[3] = {1.0 / 3.0 * delt, 5.0 / 12.0 * delt, 1.0 / 4.0 * delt};
