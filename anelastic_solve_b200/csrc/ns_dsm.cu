@@ -243,8 +243,8 @@ int NSSolver::ensure_dyn() {
 
 // filter(in, out, 2, xfil, yfil, zfil, vt) (hf = 0) or filterHF(in, out,
 // 2, 1, 1, 1, vt) (hf = 1): in is not modified
-void NSSolver::dyn_filter(const double* in, double* out, int vt, int hf, cudaStream_t s) {
-  double* tmp = d_dyn_ + (size_t)DY_TMP * G_;
+void NSSolver::dyn_filter(const double* in, double* out, int vt, int hf, cudaStream_t s, double* tmp) {
+  if (!tmp) tmp = d_dyn_ + (size_t)DY_TMP * G_;
   const double* cur = in;
   for (int d = 0; d < 3; ++d) {
     if (hf || prm_.filt[d]) {
@@ -259,6 +259,27 @@ void NSSolver::dyn_filter(const double* in, double* out, int vt, int hf, cudaStr
     launch_ghost_field(D_, const_cast<double*>(cur), zrule(vt), s);
   }
   if (cur != out) cudaMemcpyAsync(out, cur, G_ * sizeof(double), cudaMemcpyDeviceToDevice, s);
+}
+
+// Every 50 steps the driver smooths the scalars of the LES scalar models
+// with filterHF(.., 2, 1, 1, 1, 'rho' / 'scal1', ..) (NSsolver.F90:144-164;
+// its EDIFF and tol arguments are unused, filter.F90:209,237,266): a
+// whole-array copy back, then the field's ghost pass.  q_rho and q_s are
+// the scratch (the driver's zero_temps comes first) and are zeroed again.
+int NSSolver::smooth_scalars(cudaStream_t s) {
+  double* a = D_.qr;
+  double* b = D_.qs;
+  double* f[2] = {D_.rles ? D_.rho : nullptr, D_.sles ? D_.s : nullptr};
+  const int vt[2] = {NV_RHO, NV_SCAL1};
+  for (int q = 0; q < 2; ++q) {
+    if (!f[q]) continue;
+    dyn_filter(f[q], a, vt[q], 1, s, b);
+    ANEL_CUDA_TRY(cudaMemcpyAsync(f[q], a, G_ * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    launch_ghost_field(D_, f[q], zrule(vt[q]), s);
+  }
+  ANEL_CUDA_TRY(cudaMemsetAsync(a, 0, G_ * sizeof(double), s));
+  ANEL_CUDA_TRY(cudaMemsetAsync(b, 0, G_ * sizeof(double), s));
+  return ANEL_OK;
 }
 
 void NSSolver::dyn_ew(int op, double* out, const double* a, const double* b, const double* c, cudaStream_t s) {

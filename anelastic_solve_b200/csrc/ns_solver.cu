@@ -674,6 +674,12 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
       st = les_coeffs(s);
       if (st != ANEL_OK) return st;
     }
+    // the scalar models' smoothing of rho and scal1 every 50 steps
+    // (NSsolver.F90:144-164), after the coefficients, before SGSdiff
+    if (time_ > 0.0 && nstep_ % 50 == 0 && (D_.rles || D_.sles)) {
+      st = smooth_scalars(s);
+      if (st != ANEL_OK) return st;
+    }
     const double DTR[3] = {1.0 / 3.0 * delt, 5.0 / 12.0 * delt, 1.0 / 4.0 * delt};
     for (int q = 0; q < 3; ++q) {
       if (les && nstep_ > prm_.les_start) launch_sgs(D_, zrule(NV_CFLUC), s);

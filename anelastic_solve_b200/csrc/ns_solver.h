@@ -116,7 +116,9 @@ class NSSolver {
   const anel_fields* io_out_ = nullptr;
   int ensure_dyn();
   int dyn_prepare(cudaStream_t s);
-  void dyn_filter(const double* in, double* out, int vt, int hf, cudaStream_t s);
+  // tmp: second scratch field (null: the dynamic models' own)
+  void dyn_filter(const double* in, double* out, int vt, int hf, cudaStream_t s, double* tmp = nullptr);
+  int smooth_scalars(cudaStream_t s);
   void dyn_ew(int op, double* out, const double* a, const double* b, const double* c, cudaStream_t s);
   int dyn_ratio(double* num, double* den, double* out, cudaStream_t s);
   int dyn_profile(const double* a, double* host, cudaStream_t s);

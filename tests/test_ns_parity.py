@@ -180,6 +180,34 @@ def test_les_steps_bitwise(case):
         np.testing.assert_array_equal(got[name], f[name], err_msg=name)
 
 
+def test_les_step_fifty_smooths_scalars_like_oracle():
+    """At nstep = 50 with time > 0 the driver smooths rho and scal1 with
+    filterHF under the LES scalar models (NSsolver.F90:144-164): the GPU
+    step equals the oracle's bit for bit, and the smoothing changed the
+    scalars (a step at nstep = 51 differs)."""
+    g_, o, s, f, start = setup_case(Re=50000.0, g=-0.1, amp=1e-2, les=True)
+    # scalars with local extrema, so that filterHF has something to do
+    rng = np.random.default_rng(50)
+    f["rho"][...] += 0.05 * rng.standard_normal(g_.ghosted)
+    f["scal1"][...] = rng.standard_normal(g_.ghosted)
+    for name, vt in (("rho", 4), ("scal1", 12)):
+        o.ghost(f[name], vt)
+    start = {k: v.copy(order="F") for k, v in f.items()}
+    s.set_fields({k: start[k] for k in ("rho", "scal1")})
+    o.set_clock(0.5, 50)
+    s.set_clock(0.5, 50)
+    o.step()
+    s.step(1)
+    got = s.get_fields(CMP)
+    for name in CMP:
+        np.testing.assert_array_equal(got[name], f[name], err_msg=name)
+    s.set_fields({k: start[k] for k in ("u", "v", "w", "p", "rho", "scal1")})
+    s.set_clock(0.5, 51)
+    s.step(1)
+    other = s.get_fields(("rho",))
+    assert not np.array_equal(other["rho"], got["rho"])
+
+
 def test_les_mixed_precision_within_tolerance():
     """LES with the mixed-precision multigrid: fields within 1e-8 relative
     L2 of the FP64 oracle after three steps."""
