@@ -236,3 +236,29 @@ def test_rhs_equals_restatement(case, name):
     got = o.rhs(name)[1:-1, 1:-1, 1:-1]
     assert np.abs(ref).max() > 0
     np.testing.assert_array_equal(got, ref)
+
+
+def test_gravity_ramp_in_buoyancy():
+    """gravity (ANELASTIC_SL/dns/Routines.F90:27-52): g = 0 before GT1, the
+    linear ramp g_orig (t - GT1)/(GT2 - GT1) strictly between, g_orig from
+    GT2 on, and at t = GT1 < GT2 the previous value is kept (no branch
+    applies).  Checked through u3_rhs's buoyancy term at several times."""
+    g = G.shear_layer_grid(16, 8, 24, stretched=True)
+    mgp = abi.make_mg_params(levels_for(g), tbc=(0, 1, 0, 1, 0, 0), mode=abi.MODE_METRIC)
+    nsp = abi.make_ns_params(Re=RE, Pr=PR, Sc=SC, g=GRAV, ew=1, scal1_on=1)
+    g_init, g_final, t1, t2 = -0.03, -0.2, 0.5, 1.5
+    nsp.g_init, nsp.g_final, nsp.gt1, nsp.gt2 = g_init, g_final, t1, t2
+    rng = np.random.default_rng(9)
+    f = shear.shear_layer_fields(g)
+    for k in ("u", "v", "w", "rho", "scal1"):
+        f[k][...] = rng.standard_normal(g.ghosted)
+    o = OracleNS(g, mgp, nsp, f)
+    for name, vt in (("u", 0), ("v", 1), ("w", 2), ("rho", 4), ("scal1", 12)):
+        o.ghost(f[name], vt)
+    h = _Shift(g)
+    expect = [(1.0, g_final * (1.0 - t1) / (t2 - t1)), (0.2, 0.0), (t1, 0.0), (2.0, g_final),
+              (t1, g_final)]
+    for t, gv in expect:  # t1 keeps the value of the call before it
+        o.set_clock(t, 1)
+        ref = u3_rhs(f, h, 1.0 / RE, gv, ew=1)
+        np.testing.assert_array_equal(o.rhs("w")[1:-1, 1:-1, 1:-1], ref, err_msg=f"t={t}")
