@@ -13,8 +13,9 @@ source writes them.  DSMrho and DSMscal1 (les/DSMrho.F90:1-240, the
 same routine on scal1 in DSMscal1.F90) are restated the same way.  On
 random fields the oracle's nuT, kappaT and nappaT from the dynamic
 coefficients must equal the restatement bit for bit, on the reference
-runfile's uniform grid with filters in x, y and z, and for the velocity
-model also with the filter off in one direction.
+runfile's uniform grid with filters in x, y and z, for the velocity model
+also with the filter off in one direction, and on a tanh-stretched z axis
+with the corrected five-point centring.
 """
 import math
 
@@ -101,6 +102,42 @@ def center_uniform(c, a, d):
     return out
 
 
+def _newton5(x, y, loc):
+    """divdiffs(x, y, a, 4) and the Newton form at loc (StatTools.F90:563-653)."""
+    d = [list(y)]
+    for j in range(1, 5):
+        prev = d[-1]
+        d.append([None] * j + [(prev[k] - prev[k - 1]) / (x[k] - x[k - j]) for k in range(j, 5)])
+    a = [d[k][k] for k in range(5)]
+    s = a[4]
+    for k in range(3, -1, -1):
+        s = s * (loc - x[k]) + a[k]
+    return s
+
+
+def center(c, a, d):
+    """center_velocity along d: the two-point mean on a uniform axis, else
+    the five-point interpolation (the values over the edges when the
+    interpolation is CORRECTED; LITERAL hands the values to divdiffs as
+    abscissae, as the reference does)."""
+    if not c.nsp.stretched[d]:
+        return center_uniform(c, a, d)
+    out = np.zeros_like(a, order="F")
+    src, dst = _pencils(a, d), _pencils(out, d)
+    ax = (c.g.x, c.g.y, c.g.z)[d]
+    n = ax.n
+    corrected = c.nsp.interp == abi.DIAG_CORRECTED
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for q in range(2, n + 2):  # Fortran index of the centred value
+            lo = 1 if q == 2 else (n - 2 if q == n + 1 else q - 2)
+            dep = [src[..., lo - 1 + m] for m in range(5)]
+            ind = [ax.xe[lo - 1 + m] for m in range(5)]
+            loc = ax.xc[q - 1]
+            dst[..., q - 1] = _newton5(ind, dep, loc) if corrected else _newton5(dep, ind, loc)
+    c.ghost(out, (VT_U, VT_V, VT_W)[d])
+    return out
+
+
 def dsm_component(f, h, ij):
     S, M = h.S, h.M
     u, v, w = f["u"], f["v"], f["w"]
@@ -153,7 +190,7 @@ def dsm_csgs(c, f):
     fmodS = np.zeros(g.ghosted, order="F")
     fmodS[inner] = strain_magnitude(filt_vel, h)
     c.ghost(fmodS, CFLUC)
-    cen = [center_uniform(c, f[k], d) for d, k in enumerate(("u", "v", "w"))]
+    cen = [center(c, f[k], d) for d, k in enumerate(("u", "v", "w"))]
     fcen = [filter2(c, a, CFLUC) for a in cen]
     pa, pb = (0, 0, 1, 2, 0, 0, 1), (0, 0, 1, 2, 1, 2, 2)
     l4 = np.zeros(g.ghosted, order="F")
@@ -241,7 +278,7 @@ def dsm_scalar(c, f, name):
         l1[inner] = S(q) * 0.5 * (S(vel[d], *[-v for v in sh]) + S(vel[d]))
         c.ghost(l1, CFLUC)
         l3 = filter2(c, l1, CFLUC)
-        fc = filter2(c, center_uniform(c, vel[d], d), CFLUC)
+        fc = filter2(c, center(c, vel[d], d), CFLUC)
         fq = filter2(c, q, CFLUC)
         l3 = l3 - fq * fc
         c.ghost(l3, CFLUC)
@@ -310,4 +347,32 @@ def test_dynamic_scalar_models_equal_restatement():
         C, dg, modS = dsm_scalar(c, f, name)
         ref = -(C[1:-1, 1:-1, 1:-1] + 0.0) * (dg * dg) * modS + 0.0
         assert np.abs(ref).max() > 0
+        np.testing.assert_array_equal(f[eddy][1:-1, 1:-1, 1:-1], ref, err_msg=eddy)
+
+
+@pytest.mark.parametrize("interp", [abi.DIAG_CORRECTED], ids=["corrected"])
+def test_dynamic_models_on_stretched_z(interp):
+    """The same restatement on a tanh-stretched z axis: the cell-centred
+    velocities come from the five-point interpolation, delg varies with k."""
+    g = G.shear_layer_grid(16, 8, 16, stretched=True)
+    mgp = abi.make_mg_params(levels_for(g), tbc=(0, 1, 0, 1, 0, 0), mode=abi.MODE_METRIC)
+    nsp = abi.make_ns_params(Re=50000.0, g=-0.1, ew=1, scal1_on=1, les=True, models=(abi.MODEL_DSM,) * 3,
+                             test_ratio=RATIO, filt=(1, 1, 1), stretched=(0, 0, 1), interp=interp)
+    rng = np.random.default_rng(31)
+    f = shear.shear_layer_fields(g)
+    for k in ("u", "v", "w", "rho", "scal1"):
+        f[k][...] = rng.standard_normal(g.ghosted)
+    for k in ("nuT", "kappaT", "nappaT"):
+        f[k] = np.zeros(g.ghosted, order="F")
+    o = OracleNS(g, mgp, nsp, f)
+    c = _Ctx(g, nsp, (1, 1, 1))
+    for k, vt in (("u", VT_U), ("v", VT_V), ("w", VT_W), ("rho", 4), ("scal1", 12)):
+        c.ghost(f[k], vt)
+    o.les_update()
+    csgs, dg, modS = dsm_csgs(c, f)
+    ref = -(csgs[1:-1, 1:-1, 1:-1] + 0.0) * (dg * dg) * modS + 0.0
+    np.testing.assert_array_equal(f["nuT"][1:-1, 1:-1, 1:-1], ref, err_msg="nuT")
+    for name, eddy in (("rho", "kappaT"), ("scal1", "nappaT")):
+        C, dg, modS = dsm_scalar(c, f, name)
+        ref = -(C[1:-1, 1:-1, 1:-1] + 0.0) * (dg * dg) * modS + 0.0
         np.testing.assert_array_equal(f[eddy][1:-1, 1:-1, 1:-1], ref, err_msg=eddy)
