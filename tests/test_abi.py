@@ -74,7 +74,8 @@ def test_tanh_grid_shape():
 
 
 def test_struct_sizes_match_the_c_header(tmp_path):
-    """ctypes mirrors of every struct have the C compiler's size."""
+    """ctypes mirrors of every struct have the C compiler's size, and the
+    header compiles as strict C99."""
     import shutil
     import subprocess
 
@@ -85,12 +86,14 @@ def test_struct_sizes_match_the_c_header(tmp_path):
              "anel_mg_report": abi.MGReport, "anel_ns_params": abi.NSParams,
              "anel_fields": abi.Fields, "anel_step_report": abi.StepReport,
              "anel_request": abi.Request, "anel_result": abi.Result,
-             "anel_serve_stats": abi.ServeStats}
+             "anel_serve_stats": abi.ServeStats, "anel_restart_header": abi.RestartHeader}
     src = tmp_path / "sz.c"
     src.write_text('#include <stdio.h>\n#include "anel.h"\nint main(void){\n' +
                    "".join(f'printf("%zu\\n", sizeof({n}));\n' for n in names) + "return 0;}\n")
     exe = tmp_path / "sz"
-    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    # the header is plain C99 and compiles without warnings
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", str(ROOT / "include"),
+                    str(src), "-o", str(exe)], check=True)
     sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
                                             check=True).stdout.split()]
     for (n, cls), got in zip(names.items(), sizes):
