@@ -98,3 +98,20 @@ def test_struct_sizes_match_the_c_header(tmp_path):
                                             check=True).stdout.split()]
     for (n, cls), got in zip(names.items(), sizes):
         assert C.sizeof(cls) == got, (n, C.sizeof(cls), got)
+
+
+def test_header_compiles_as_cpp(tmp_path):
+    """The header is usable from C++ too (extern "C" linkage, no C-only
+    constructs): a translation unit that takes the address of one drop-in
+    entry point compiles cleanly with g++."""
+    import shutil
+    import subprocess
+
+    cxx = shutil.which("g++")
+    if not cxx:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "h.cpp"
+    src.write_text('#include "anel.h"\nvoid (*fp)(double*, double*, int32_t*, double*) = anel_mg_solve;\n'
+                   "int main() { return fp ? 0 : 1; }\n")
+    subprocess.run([cxx, "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"), "-c",
+                    str(src), "-o", str(tmp_path / "h.o")], check=True)
