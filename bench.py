@@ -141,16 +141,17 @@ class ClockSampler:
 SMOOTHER = {"smoother": "rbpgs", "pre": 2, "post": 2}
 
 
-def mg_params(lv, precision, mode=None):
+def mg_params(lv, precision, mode=None, smoother=None):
     """V(2,2) cycles, metric operator, true-residual stop.  With the ZLINE
-    smoother the z direction is not coarsened (horizontal semi-coarsening)."""
+    smoother the z direction is not coarsened (horizontal semi-coarsening).
+    `smoother` ("zline" | "rbpgs") overrides the run's choice."""
     from anelastic_solve_b200 import abi
 
-    zl = SMOOTHER["smoother"] == "zline"
+    zl = (smoother or SMOOTHER["smoother"]) == "zline"
     levels = (lv[0], lv[1], 1) if zl else lv
-    return abi.make_mg_params(levels, maxcy=400, tolmax=TOL, pre=SMOOTHER["pre"],
-                              post=SMOOTHER["post"], tbc=(0, 1, 0, 1, 0, 0),
-                              precision=precision,
+    pre, post = (SMOOTHER["pre"], SMOOTHER["post"]) if smoother is None else (2, 2)
+    return abi.make_mg_params(levels, maxcy=400, tolmax=TOL, pre=pre, post=post,
+                              tbc=(0, 1, 0, 1, 0, 0), precision=precision,
                               smoother=abi.SMOOTHER_ZLINE if zl else abi.SMOOTHER_RBPGS,
                               mode=abi.MODE_METRIC if mode is None else mode, stop=abi.STOP_RESID)
 
@@ -233,6 +234,7 @@ def run_dns(args, rank, world, local_rank):
     s = NSSolver(g, mg_params(lv, prec), ns_params(phys), device=local_rank)
     f = initial_state(g, phys)
     s.set_fields({k: f[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
+    del f
     s.project()
     st = torch.cuda.Stream(device=dev)
     h = st.cuda_stream
@@ -303,13 +305,19 @@ def run_dns(args, rank, world, local_rank):
         nb = len(STATE) * int(np.prod(g.ghosted)) * 8
         out["bytes_io"] = (nb, nb)
     # mixed vs FP64 multigrid on this workload's pressure equation: cold
-    # solves (phi0 = 0) of the last sub-step's right-hand side
+    # solves (phi0 = 0) of the last sub-step's right-hand side, with this
+    # run's multigrid and with the plain FP64 path (the reference's
+    # red-black point smoother, full coarsening: the one-for-one mg_solver
+    # replacement)
     if rank == 0 and not args.no_fp64:
         fld = s.get_fields(("psrc",))
         rhs = torch.from_numpy(np.ascontiguousarray(fld["psrc"].T)).to(dev)
         mg = {}
-        for name, pr in (("mixed", abi.PREC_MIXED), ("fp64", abi.PREC_FP64)):
-            m = MGSolver(g, mg_params(lv, pr), device=local_rank)
+        for name, pr, sm in (("mixed", abi.PREC_MIXED, None), (f"fp64_{args.smoother}", abi.PREC_FP64, None),
+                             ("fp64_rbpgs", abi.PREC_FP64, "rbpgs")):
+            if name in mg:
+                continue
+            m = MGSolver(g, mg_params(lv, pr, smoother=sm), device=local_rank)
             phi = torch.zeros_like(rhs)
             m.solve(phi, rhs, stream=h)
             phi.zero_()
@@ -317,10 +325,42 @@ def run_dns(args, rank, world, local_rank):
             r = m.last_report
             mg[name] = {"ms": round(r.ms, 3), "iter": r.iter, "resid": r.resid}
             m.close()
+        del rhs
         out["mg_cold"] = mg
+    # the plain FP64 GPU path (FP64 multigrid, red-black point Gauss-Seidel,
+    # full coarsening) on the same state: whole steps timed like the main
+    # run, so that mixed vs plain FP64 is measured in the same process
+    if not args.no_fp64 and kind == "dns":
+        names = ("u", "v", "w", "p", "rho", "scal1", "nuT", "kappaT", "nappaT")
+        st_now = s.get_fields(names)
+        s64 = NSSolver(g, mg_params(lv, abi.PREC_FP64, smoother="rbpgs"), ns_params(phys), device=local_rank)
+        s64.set_fields({k: st_now[k] for k in ("u", "v", "w", "p", "rho", "scal1")})
+        one = np.ones(g.ghosted, order="F")
+        s64.set_fields({"r": one, "densityBG": one})
+        del one
+        s64.step(1, stream=h)
+        torch.cuda.synchronize()
+        n64 = 3
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        reps64 = [s64.step(1, stream=h) for _ in range(n64)]
+        e1.record(st)
+        torch.cuda.synchronize()
+        out["fp64_plain"] = {"ms_per_step": e0.elapsed_time(e1) / n64, "steps": n64,
+                             "mg_iters": [list(x.mg_iter) for x in reps64],
+                             "mg_ms_per_step": float(np.mean([x.mg_ms for x in reps64]))}
+        s64.close()
+        del st_now
     fu = s.get_fields(("u", "v", "w"))
     out["umax"] = float(max(np.abs(fu[k][1:-1, 1:-1, 1:-1]).max() for k in ("u", "v", "w")))
     out["dzmin"] = float(g.z.dxc[1:-1].min())
+    # the benchmarked sub-step against the FP64 oracle at full size, from
+    # this run's state after its timed steps: the GPU's sub-step (this
+    # run's multigrid) and the oracle's (FP64, the reference's red-black
+    # point smoother) from the same fields.  The oracle's time is the CPU
+    # baseline (one steady-state sub-step on the host cores, x3 per step).
+    if rank == 0 and world == 1 and not args.no_cpu and kind == "dns":
+        out["oracle_leg"] = oracle_leg(s, g, lv, phys, os.cpu_count() or 1, h)
     s.close()
     keys = [k for k in ("ms_step", "e2e_ms") if k in out]
     out.update(zip(keys, combine_ranks(world, dev, maxes=[out[k] for k in keys])[0]))
@@ -398,10 +438,28 @@ def run_poisson(args, rank, world, local_rank):
 
 
 # ------------------------------------------------------------ CPU samples
-def cpu_sample_dns(workload, threads):
-    """One FP64 RK3 sub-step of the oracle restatement on the host cores at
-    the full workload size, from the projected initial state (the first
-    sub-step of step 1).  Returns (seconds, MG cycles, cells)."""
+def oracle_fields(g, state):
+    """Fortran-ordered host fields for the oracle: every array of
+    abi.FIELD_NAMES (zeros), r = densityBG = 1, then the given state."""
+    from anelastic_solve_b200 import abi
+
+    f = {n: np.zeros(g.ghosted, order="F") for n in abi.FIELD_NAMES}
+    f["r"][...] = 1.0
+    f["densityBG"][...] = 1.0
+    for k, v in state.items():
+        f[k][...] = v
+    return f
+
+
+def cpu_reference_step(workload, threads):
+    """The reference's algorithm on the host cores at the full workload
+    size: the oracle restatement, FP64, red-black point Gauss-Seidel with
+    full coarsening, metric operator, stop at a true relative residual of
+    1e-10.  Untimed warm-up: the initial projection and one whole RK3 step
+    (its first sub-step, from the projected state, needs about three times
+    the cycles of a steady one).  Timed: the next whole step.  Returns a
+    dict with the seconds of the timed step, its cycles per sub-step, the
+    warm-up's cycles and the interior cell count."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from anelastic_solve_b200 import abi
     from anelastic_solve_b200 import grid as G
@@ -410,14 +468,60 @@ def cpu_sample_dns(workload, threads):
     kind, n, lv, phys = WORKLOADS[workload]
     g = G.shear_layer_grid(*n, stretched=True)
     f = initial_state(g, phys)
-    o = OracleNS(g, mg_params(lv, abi.PREC_FP64), ns_params(phys), f)
+    o = OracleNS(g, mg_params(lv, abi.PREC_FP64, smoother="rbpgs"), ns_params(phys), f)
     for name, vt in (("u", 0), ("v", 1), ("w", 2), ("rho", 4), ("scal1", 12)):
         o.ghost(f[name], vt)
-    o.project()
-    dt = cfl_dt(g, f, phys["cfl"])
+    pit, _ = o.project()
+    warm = o.step()
     t = time.perf_counter()
-    it, _ = o.substep(0.0, 1.0, 1.0 / 3.0, 1.0 / 3.0 * dt, dt)
-    return time.perf_counter() - t, it, g.x.n * g.y.n * g.z.n
+    rep = o.step()
+    sec = time.perf_counter() - t
+    return {"seconds": sec, "cycles": list(rep.mg_iter), "warm_cycles": [pit] + list(warm.mg_iter),
+            "cells": g.x.n * g.y.n * g.z.n}
+
+
+def oracle_leg(s, g, lv, phys, threads, stream):
+    """One RK3 sub-step (the first of a step) from the GPU run's current
+    state, on the GPU with the run's own multigrid and on the host with the
+    FP64 oracle (the reference's red-black point smoother, full
+    coarsening, to the same 1e-10 residual).  Returns the oracle's time
+    and cycles (the CPU baseline sample) and the relative L2 error of each
+    GPU field against the oracle's (pressure after removing the volume
+    mean)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from anelastic_solve_b200 import abi
+    from anelastic_solve_b200.ns import RK3
+    from oracle.pyoracle import OracleNS
+
+    names = ("u", "v", "w", "p", "rho", "scal1", "nuT", "kappaT", "nappaT")
+    state = s.get_fields(names)
+    dt = cfl_dt(g, state, phys["cfl"])
+    a1, a2, a3, ec, fr = RK3[0]
+    it_g, _ = s.substep(a1, a2, a3, fr * dt, dt, stream=stream)
+    gpu = s.get_fields(("u", "v", "w", "p", "rho"))
+    f = oracle_fields(g, state)
+    del state
+    o = OracleNS(g, mg_params(lv, abi.PREC_FP64, smoother="rbpgs"), ns_params(phys), f)
+    t = time.perf_counter()
+    it_o, _ = o.substep(a1, a2, a3, fr * dt, dt)
+    sec = time.perf_counter() - t
+
+    def rel(a, b):
+        a, b = a[1:-1, 1:-1, 1:-1], b[1:-1, 1:-1, 1:-1]
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    def vmean(a):
+        vol = g.x.dxc[1:-1, None, None] * g.y.dxc[None, 1:-1, None] * g.z.dxc[None, None, 1:-1]
+        inner = a[1:-1, 1:-1, 1:-1]
+        return inner - (inner * vol).sum() / vol.sum()
+
+    err = {k: rel(gpu[k], f[k]) for k in ("u", "v", "w", "rho")}
+    num = sum(np.linalg.norm((gpu[k] - f[k])[1:-1, 1:-1, 1:-1]) ** 2 for k in "uvw")
+    den = sum(np.linalg.norm(f[k][1:-1, 1:-1, 1:-1]) ** 2 for k in "uvw")
+    err["velocity"] = float(np.sqrt(num / den))
+    pg, po = vmean(gpu["p"]), vmean(f["p"])
+    err["p"] = float(np.linalg.norm(pg - po) / np.linalg.norm(po))
+    return {"seconds": sec, "oracle_cycles": it_o, "gpu_cycles": it_g, "err": err, "dt": dt}
 
 
 def cfl_dt(g, f, cfl):
@@ -430,7 +534,10 @@ def cfl_dt(g, f, cfl):
 
 
 def cpu_sample_poisson(workload, threads):
-    """One FP64 V-cycle of the oracle restatement at full size."""
+    """One whole pressure solve of the workload on the host cores: the
+    oracle restatement, FP64, the reference's red-black point Gauss-Seidel
+    with full coarsening, from phi0 = 0 to a true relative residual of
+    1e-10.  Returns (seconds, cycles, interior cells)."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     from anelastic_solve_b200 import abi
     from anelastic_solve_b200 import grid as G
@@ -439,15 +546,11 @@ def cpu_sample_poisson(workload, threads):
     kind, n, lv, phys = WORKLOADS[workload]
     g = G.shear_layer_grid(*n, stretched=True)
     fF = np.asfortranarray(poisson_rhs(g).T)
-    p = mg_params(lv, abi.PREC_FP64)
-    p.maxcy = 1
-    p.tolmax = 0.0
-    o = OracleMG(g, p)
+    o = OracleMG(g, mg_params(lv, abi.PREC_FP64, smoother="rbpgs"))
     phi = np.zeros(g.ghosted, order="F")
-    o.solve(phi, fF.copy(order="F"))
     t = time.perf_counter()
-    o.solve(phi, fF.copy(order="F"))
-    return time.perf_counter() - t, g.x.n * g.y.n * g.z.n
+    it, _ = o.solve(phi, fF.copy(order="F"))
+    return time.perf_counter() - t, it, g.x.n * g.y.n * g.z.n
 
 
 # ------------------------------------------------------------ ours: serve
@@ -546,17 +649,17 @@ def main_serve(args, rank, world, local_rank, threads):
               "hbm_budget_gb": args.budget_gb, "workers": args.workers,
               "mg": f"{args.smoother.upper()} V({args.pre},{args.post}), metric, {args.prec}, to 1e-10",
               "parallelism": f"replicas x{world}", "l2": "mixed sizes (32^3 .. 256^3)"}
-    if args.impl == "reference" or not args.no_cpu:
-        SMOOTHER.update(smoother="rbpgs", pre=2, post=2)
     if args.impl == "reference":
         if rank != 0:
             return
-        t, it, N = cpu_sample_dns("dns64", threads)
-        value = N / (3.0 * t)
-        sample = (f"one 64^3 member: first FP64 RK3 sub-step after projection, oracle restatement "
-                  f"({t:.2f} s, {it} MG V-cycles), x3 per step; members run one after another")
+        c = cpu_reference_step("dns64", threads)
+        t, N = c["seconds"], c["cells"]
+        value = N / t
+        sample = (f"one 64^3 member, oracle restatement: one steady RK3 step ({t:.2f} s, "
+                  f"MG V-cycles per sub-step {c['cycles']}) after the initial projection and one "
+                  f"warm-up step; members run one after another")
         line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": 0,
-                "steps": args.requests, "warmup": args.warmup, "ms_per_step": 3 * t * 1e3,
+                "steps": 1, "warmup": 1, "requested_steps": args.requests, "ms_per_step": t * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": dict(config, mg="RBPGS V(2,2), metric, fp64 (host)"),
                 "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
@@ -582,10 +685,11 @@ def main_serve(args, rank, world, local_rank, threads):
     pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None  # noqa: E731
     cpu = None
     if not args.no_cpu:
-        t, it, N = cpu_sample_dns("dns64", threads)
-        cpu = {"value": N / (3.0 * t), "unit": unit, "cores": threads, "kind": "port",
-               "sample": f"one 64^3 member: first FP64 RK3 sub-step after projection, oracle "
-                         f"restatement ({t:.2f} s, {it} MG V-cycles), x3 per step"}
+        c = cpu_reference_step("dns64", threads)
+        cpu = {"value": c["cells"] / c["seconds"], "unit": unit, "cores": threads, "kind": "port",
+               "sample": f"one 64^3 member, oracle restatement (FP64 RBPGS): one steady RK3 step "
+                         f"({c['seconds']:.2f} s, MG V-cycles per sub-step {c['cycles']}) after the "
+                         f"initial projection and one warm-up step"}
     line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.requests,
             "warmup": len(SERVE_SIZES), "ms_per_step": 1e3 * r["makespan_s"] / max(1, args.requests),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -670,27 +774,22 @@ def main():
         if rank != 0:
             return
         # the reference's own algorithm: red-black point GS, full coarsening
-        SMOOTHER.update(smoother="rbpgs", pre=2, post=2)
         config = dict(config, mg=f"RBPGS V(2,2), metric, fp64 (the reference's algorithm on the host)")
-        samples = []
-        for _ in range(max(1, args.warmup + args.steps) if kind == "poisson" else 1):
-            samples.append(cpu_sample_dns(args.workload, threads) if kind == "dns"
-                           else cpu_sample_poisson(args.workload, threads))
         if kind == "dns":
-            t, it, N = samples[-1]
-            value = N / (3.0 * t)
-            sample = (f"first FP64 RK3 sub-step after the initial projection, oracle restatement "
-                      f"at full size ({t:.1f} s, {it} MG V-cycles), x3 per step")
-            ms = 3 * t * 1e3
+            c = cpu_reference_step(args.workload, threads)
+            t, N = c["seconds"], c["cells"]
+            value = N / t
+            sample = (f"oracle restatement at full size: one steady RK3 step ({t:.1f} s, MG V-cycles "
+                      f"per sub-step {c['cycles']}) after the untimed initial projection and one "
+                      f"warm-up step (cycles {c['warm_cycles']})")
+            ms, steps, warm = t * 1e3, 1, 1
         else:
-            t = float(np.mean([x[0] for x in samples[args.warmup:]] or [samples[-1][0]]))
-            N = samples[-1][1]
-            cyc = 48
-            value = N / (t * cyc)
-            sample = f"1 FP64 V-cycle of the oracle restatement at full size ({t:.2f} s) x {cyc}"
-            ms = t * cyc * 1e3
+            t, it, N = cpu_sample_poisson(args.workload, threads)
+            value = N / t
+            sample = f"oracle restatement at full size: one whole solve from phi0 = 0 ({t:.1f} s, {it} V-cycles)"
+            ms, steps, warm = t * 1e3, 1, 0
         line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": 0,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "steps": steps, "warmup": warm, "requested_steps": args.steps, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": config,
                 "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
@@ -738,18 +837,18 @@ def main():
                 "mean_launch_ms": round(t_launch * 1e3, 4),
                 "share_note": "finest-level smoother launches only; share of step time in profiles/"}
     cpu = None
-    SMOOTHER.update(smoother="rbpgs", pre=2, post=2)  # the CPU baseline: the reference's algorithm
     if not args.no_cpu:
-        if kind == "dns":
-            t, it, _ = cpu_sample_dns(args.workload, threads)
-            cpu = {"value": N / (3.0 * t), "unit": unit, "cores": threads, "kind": "port",
-                   "sample": f"first FP64 RK3 sub-step after the initial projection, oracle "
-                             f"restatement at full size ({t:.1f} s, {it} MG V-cycles), x3 per step"}
-        else:
-            t, _ = cpu_sample_poisson(args.workload, threads)
-            cyc = r["iters"][-1] if args.prec == "fp64" else 48
-            cpu = {"value": N / (t * cyc), "unit": unit, "cores": threads, "kind": "port",
-                   "sample": f"1 FP64 V-cycle of the oracle restatement at full size ({t:.2f} s) x {cyc}"}
+        if kind == "dns" and "oracle_leg" in r:
+            c = r["oracle_leg"]
+            cpu = {"value": N / (3.0 * c["seconds"]), "unit": unit, "cores": threads, "kind": "port",
+                   "sample": f"one steady RK3 sub-step at full size from this run's state after its "
+                             f"timed steps: oracle restatement, FP64 RBPGS ({c['seconds']:.1f} s, "
+                             f"{c['oracle_cycles']} MG V-cycles), x3 per step"}
+        elif kind == "poisson":
+            t, it, _ = cpu_sample_poisson(args.workload, threads)
+            cpu = {"value": N / t, "unit": unit, "cores": threads, "kind": "port",
+                   "sample": f"one whole FP64 RBPGS solve of the oracle restatement at full size "
+                             f"({t:.1f} s, {it} V-cycles)"}
     line = {"metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
@@ -765,6 +864,22 @@ def main():
         line["div_bound"] = 1e-10 * r["umax"] / r["dzmin"]
         if "mg_cold" in r:
             line["mg_solve_ms"] = r["mg_cold"]
+        if "fp64_plain" in r:
+            fp = r["fp64_plain"]
+            line["fp64_plain"] = {"ms_per_step": round(fp["ms_per_step"], 3),
+                                  "mg_ms_per_step": round(fp["mg_ms_per_step"], 3),
+                                  "mg_iters": fp["mg_iters"], "steps": fp["steps"],
+                                  "mg": "RBPGS V(2,2), metric, fp64, full coarsening (the one-for-one "
+                                        "mg_solver replacement)",
+                                  "speedup_of_this_run": round(fp["ms_per_step"] / r["ms_step"], 3)}
+        if "oracle_leg" in r:
+            c = r["oracle_leg"]
+            line["err_vs_fp64_oracle"] = dict(
+                {k: float(f"{v:.3e}") for k, v in c["err"].items()},
+                sample="one RK3 sub-step at full size from this run's state after its timed steps: "
+                       "this run's multigrid on the GPU vs the FP64 oracle (RBPGS) on the host, both "
+                       "to 1e-10; relative L2 over the interior, p after removing the volume mean",
+                gpu_cycles=c["gpu_cycles"], oracle_cycles=c["oracle_cycles"])
     else:
         line["mg_iters"] = r["iters"][-1]
         line["resid"] = r["resid"]

@@ -373,7 +373,10 @@ int anel_ns_ctx_divergence(anel_ns_ctx* ctx, double* out);
  * (larger: ANEL_ERR_SIZE) and is shared by all calls on a device, so
  * calls whose GPU work overlaps race; run them on one stream.  The first
  * call on a device looks up that array's address and keeps it: make it
- * before any stream capture on the device.  Waits for stream. */
+ * before any stream capture on the device.  The kept address belongs to
+ * the device's primary context: after cudaDeviceReset (or any teardown of
+ * that context) it is stale, so a process that resets the device must not
+ * call this entry point again.  Waits for stream. */
 int anel_divergence_noalloc(int32_t nx, int32_t ny, int32_t nz, const double* u, const double* v,
                             const double* w, const double* rdxc, const double* rdyc,
                             const double* rdzc, double* out, void* stream);

@@ -274,3 +274,39 @@ def test_lj_solve_bitwise(name, mode):
     it_g, rm_g = s.solve(dphi, to_dev(src))
     assert (it_g, rm_g) == (it_o, rm_o)
     np.testing.assert_array_equal(to_host(dphi), ref)
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_LITERAL, abi.MODE_METRIC])
+def test_dropin_mg_solve_equals_oracle(mode):
+    """The drop-in anel_mg_init / anel_mg_solve / anel_mg_finalize (host
+    arrays by reference, the argument list of mg_solver(phif, rhsf, iter,
+    relmax), mgMK/mg_solver.F90:48-141) against the oracle's mg_solver:
+    the same solution bit for bit, the same iteration count and relmax,
+    on two solves in a row (the second from the first's solution)."""
+    import ctypes as C
+
+    from anelastic_solve_b200 import _lib
+
+    name = "shear_stretched_vbc"
+    mk, tbc, vbc, lv = CASES[name]
+    g = mk()
+    p = mg_params(g, levels=levels_for(g), tbc=tbc, vbc=vbc, mode=mode, maxcy=40, tolmax=1e-9)
+    o = OracleMG(g, p)
+    L = _lib.lib()
+    desc, keep = abi.make_grid_desc(g)
+    _lib.check(L.anel_mg_init(C.byref(desc), C.byref(p)))
+    try:
+        rng = np.random.default_rng(61)
+        ref = zeros(g)
+        phi = zeros(g)
+        for _ in range(2):
+            src = compatible(field(g, rng), g, mode)
+            it_o, rm_o = o.solve(ref, src.copy(order="F"))
+            it = C.c_int32(-7)
+            rm = C.c_double(-7.0)
+            L.anel_mg_solve(abi.dptr(phi), abi.dptr(src.copy(order="F")), C.byref(it), C.byref(rm))
+            assert it.value > 0, _lib.last_error()
+            assert (it.value, rm.value) == (it_o, rm_o)
+            np.testing.assert_array_equal(phi, ref)
+    finally:
+        L.anel_mg_finalize()

@@ -239,3 +239,64 @@ def test_step_host_equals_device_steps():
     got = ref.get_fields(keys)
     for k in keys:
         np.testing.assert_array_equal(host[k], got[k], err_msg=k)
+
+
+def test_divergence_matches_oracle():
+    """anel_ns_ctx_divergence against the oracle's divergence
+    (Routines.F90:54-183): the largest |div| bit for bit and the
+    volume-weighted mean |div| within summation-order rounding, after FP64
+    steps (identical fields) and on a field that is not divergence-free."""
+    g_, o, s, f, start = setup_case()
+    for _ in range(2):
+        o.step()
+    s.step(2)
+    avg_g, max_g = s.divergence()
+    avg_o, max_o = o.divergence()
+    assert max_g == max_o and max_g > 0.0
+    assert abs(avg_g - avg_o) <= 1e-12 * abs(avg_o)
+    # a perturbed (not solenoidal) velocity, ghosted by both sides
+    rng = np.random.default_rng(27)
+    f["u"][...] += 1e-2 * rng.standard_normal(g_.ghosted)
+    o.ghost(f["u"], 0)
+    s.set_fields({"u": f["u"]})
+    assert np.array_equal(s.get_fields(("u",))["u"], f["u"])
+    avg_g, max_g = s.divergence()
+    avg_o, max_o = o.divergence()
+    assert max_g == max_o and max_g > 1e-3
+    assert abs(avg_g - avg_o) <= 1e-12 * abs(avg_o)
+
+
+def test_gravity_ramp_steps_bitwise():
+    """Gravity switched on by the ramp of Routines.F90:27-52 (Ginit = 0,
+    Gfinal = -Ri, GT1 = 0.01, GT2 = 0.045, dt = 0.01): g = 0 before GT1, the
+    kept value at time == GT1, the linear ramp in between and Gfinal from
+    GT2 on.  Six FP64 steps cover every branch; fields bit for bit."""
+    import ctypes as C
+
+    g_ = G.shear_layer_grid(32, 16, 32, stretched=True)
+    mgp = abi.make_mg_params(levels_for(g_), maxcy=200, tolmax=1e-10, pre=2, post=2,
+                             tbc=(0, 1, 0, 1, 0, 0), mode=abi.MODE_METRIC, stop=abi.STOP_RESID)
+    nsp = abi.make_ns_params(Re=1000.0, Pr=1.0, g=-0.12, dtmax=0.01, ew=1, scal1_on=1)
+    nsp.g_init, nsp.g_final, nsp.gt1, nsp.gt2 = 0.0, -0.12, 0.01, 0.045
+    f = shear.shear_layer_fields(g_, amp=1e-3)
+    o = OracleNS(g_, mgp, nsp, f)
+    for name, vt in (("u", 0), ("v", 1), ("w", 2), ("rho", 4), ("scal1", 12)):
+        o.ghost(f[name], vt)
+    o.project()
+    start = {k: v.copy(order="F") for k, v in f.items()}
+    s = NSSolver(g_, mgp, nsp)
+    s.set_fields({k: start[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
+    for n in range(6):
+        ro = o.step()
+        rg = s.step(1)
+        assert ro.time == rg.time and ro.dt == rg.dt
+        assert list(ro.mg_iter) == list(rg.mg_iter)
+    got = s.get_fields(CMP)
+    for name in CMP:
+        np.testing.assert_array_equal(got[name], f[name], err_msg=name)
+    # the ramp changed the flow: constant gravity from t = 0 gives other fields
+    nsp2 = abi.make_ns_params(Re=1000.0, Pr=1.0, g=-0.12, dtmax=0.01, ew=1, scal1_on=1)
+    s2 = NSSolver(g_, mgp, nsp2)
+    s2.set_fields({k: start[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
+    s2.step(6)
+    assert not np.array_equal(s2.get_fields(("w",))["w"], got["w"])

@@ -68,6 +68,25 @@ def test_two_calls_match_context_entry_point(case):
     assert a == b
 
 
+def test_further_calls_leave_device_memory_unchanged(case):
+    """What the entry point is for: after a first call on the device, more
+    calls leave the device's free memory exactly as it was (no cudaMalloc,
+    no allocating library routine)."""
+    import torch
+
+    g, ref, (u, v, w), (rx, ry, rz) = case
+    st, first = _noalloc(g, u, v, w, rx, ry, rz)
+    assert st == abi.OK, _lib.last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        st, got = _noalloc(g, u, v, w, rx, ry, rz)
+        assert st == abi.OK and got == first
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+
+
 def test_rejects_nz_beyond_fixed_scratch(case):
     g, ref, (u, v, w), (rx, ry, rz) = case
     st, out = _noalloc(g, u, v, w, rx, ry, rz, nz=4097)
