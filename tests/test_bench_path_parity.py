@@ -12,13 +12,11 @@ problem.
 Tolerances (relative L2 over the interior; pressure after removing the
 volume mean, the problem being singular):
 
-* velocity, as one vector field (u, v, w): 1e-8; u, v, rho: 1e-8 each;
-* w on its own: 1e-7.  w is the perturbation (|w| ~ 1e-3 of |u|), so a
-  solve stopped at a relative residual of 1e-10 leaves it a relative error
-  about a hundred times the others'.  Two FP64 oracle runs of the same
-  algorithm stopped at 1e-10 and at the FP64 floor differ by 1.05e-8 in w
-  on this grid;
-* pressure: 1e-9 after the steps, 1e-9 for the standalone 256^3 solve.
+* after five steps: u, v, w, rho and the velocity as one vector field
+  within 1e-8, pressure within 1e-9 (measured on a B200: w 9.9e-10,
+  p 9.0e-11, the rest below 1e-11);
+* the standalone 256^3 solve: see its docstring (the white-noise
+  right-hand side amplifies the stopping residual into the solution).
 
 Each test prints the errors it measured.
 """
@@ -84,9 +82,8 @@ def test_mixed_zline_stepper_at_bench_settings():
     err["p"] = rel_l2(remove_vmean(got["p"], g), remove_vmean(f["p"], g))
     print(f"\nmixed ZLINE stepper vs FP64 oracle after 5 steps: {err}; cycles gpu {it_g} oracle {it_o}")
     assert err["velocity"] < 1e-8
-    for k in ("u", "v", "rho"):
+    for k in ("u", "v", "w", "rho"):
         assert err[k] < 1e-8, k
-    assert err["w"] < 1e-7
     assert err["p"] < 1e-9
     # the same algorithm in both: the cycle counts of a sub-step agree
     # within one (the FP32 inner cycles converge a little differently)
@@ -96,25 +93,36 @@ def test_mixed_zline_stepper_at_bench_settings():
 def test_mixed_zline_poisson_256_cubed():
     """The 256^3 standalone pressure solve (the tanh-stretched shear-layer
     grid, periodic x/y, Neumann z, seeded N(0, 1) right-hand side with the
-    volume mean removed) with the benchmark's mixed ZLINE multigrid to
-    1e-10, against the oracle's FP64 solve of the same system to 1e-12."""
+    volume mean removed) with the benchmark's mixed ZLINE multigrid, against
+    the oracle's FP64 solve of the same system to 1e-13.
+
+    At the benchmark's stop (relative residual 1e-10) the solution error
+    is the residual amplified by the operator: about 1e3 for this
+    white-noise right-hand side (measured 9.2e-8 at a residual of 8.3e-11),
+    so that solve is checked against 2e3 x its residual.  Asked for 1e-13,
+    the same mixed-precision solver agrees with the oracle within 1e-9:
+    its defect correction converges to the FP64 operator's solution."""
+    import torch
+
     n, lv = (256, 256, 256), (8, 8, 1)
     g = G.shear_layer_grid(*n, stretched=True)
     rng = np.random.default_rng(1)
     src = compatible(field(g, rng), g, abi.MODE_METRIC)
     ref = zeros(g)
-    it_o, _ = OracleMG(g, zline_params(lv, abi.PREC_FP64, tol=1e-12, maxcy=60)).solve(ref, src.copy(order="F"))
-    s = MGSolver(g, zline_params(lv, abi.PREC_MIXED))
-    import torch
-
-    dphi = torch.zeros(g.ghosted[::-1], dtype=torch.float64, device="cuda")
-    s.solve(dphi, torch.from_numpy(np.ascontiguousarray(src.T)).cuda())
-    rep = s.last_report
-    got = np.asfortranarray(dphi.cpu().numpy().T)
-    s.close()
-    e = rel_l2(remove_vmean(got, g), remove_vmean(ref, g))
-    print(f"\n256^3 mixed ZLINE solve: {rep.iter} cycles, resid {rep.resid:.3e}; oracle {it_o} cycles; "
-          f"rel-L2 vs oracle {e:.3e}")
-    assert rep.status == abi.OK and rep.resid <= TOL
-    assert it_o <= 60
-    assert e < 1e-9
+    it_o, _ = OracleMG(g, zline_params(lv, abi.PREC_FP64, tol=1e-13, maxcy=80)).solve(ref, src.copy(order="F"))
+    assert it_o <= 80
+    dsrc = torch.from_numpy(np.ascontiguousarray(src.T)).cuda()
+    out = {}
+    for tol in (TOL, 1e-13):
+        s = MGSolver(g, zline_params(lv, abi.PREC_MIXED, tol=tol))
+        dphi = torch.zeros(g.ghosted[::-1], dtype=torch.float64, device="cuda")
+        s.solve(dphi, dsrc)
+        rep = s.last_report
+        got = np.asfortranarray(dphi.cpu().numpy().T)
+        s.close()
+        assert rep.status == abi.OK and rep.resid <= tol
+        out[tol] = (rep.iter, rep.resid, rel_l2(remove_vmean(got, g), remove_vmean(ref, g)))
+    print(f"\n256^3 mixed ZLINE solves (cycles, resid, rel-L2 vs oracle): {out}; oracle {it_o} cycles")
+    it, res, e = out[TOL]
+    assert e < 2e3 * res
+    assert out[1e-13][2] < 1e-9
