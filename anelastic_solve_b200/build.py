@@ -34,6 +34,8 @@ SOURCES = {
     "serve.cu": ["-fmad=false"],
     "restart.cu": ["-fmad=false"],
     "ns_dsm.cu": ["-fmad=false"],
+    "mg_col.cu": ["-fmad=true"],
+    "mg_col64.cu": ["-fmad=false"],
 }
 
 

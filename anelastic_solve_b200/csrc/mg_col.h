@@ -1,0 +1,29 @@
+// mg_col.h -- launchers of the column-layout FP32 cycle (mg_col.cuh) and of
+// the FP64 <-> column transfers of the defect correction.
+#pragma once
+
+#include "mg_col.cuh"
+
+namespace anel {
+
+// rows per lane the column sweep is built for (nz = 32 * M)
+inline bool col_rows_supported(int M) {
+  return M == 2 || M == 3 || M == 4 || M == 6 || M == 8 || M == 12 || M == 16;
+}
+void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, cudaStream_t s);
+// coarse f from the fine residual (cdir: bit 0 x, bit 1 y coarsened); the
+// caller zeroes coarse phi first
+void launch_col_restrict(const ColLevel& F, const ColLevel& C, int cdir, cudaStream_t s);
+// fine phi += interpolated coarse correction, ghost copies included
+void launch_col_prolong(const ColLevel& F, const ColLevel& C, int cdir, cudaStream_t s);
+
+// FP64 fine residual r = f - A phi (reference layout) stored as FP32 into
+// E.src (column layout), with the squared norms of r and f folded into
+// out[0], out[1] in a fixed order.
+void launch_col_resid_store(const DevLevel<double>& L, const double* phi, const double* f,
+                            const ColLevel& E, double* part, double* out, cudaStream_t s);
+int64_t col_resid_part_doubles(const DevLevel<double>& L);
+// phi += (double) E.phi on the interior (phi in the reference layout)
+void launch_col_add_correction(const DevLevel<double>& L, double* phi, const ColLevel& E, cudaStream_t s);
+
+}  // namespace anel

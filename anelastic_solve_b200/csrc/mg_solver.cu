@@ -6,6 +6,7 @@
 // host compiler so the coefficients round exactly as the reference's.
 #include "mg_solver.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -17,6 +18,8 @@ int zline_segment_factors(int n, int P, const std::vector<double>& sub, const st
                           const std::vector<double>& sup, std::vector<double>& out);
 int zline_cr_factors(int n, int S, const std::vector<double>& sub, const std::vector<double>& dia,
                      const std::vector<double>& sup, std::vector<double>& out);
+int col_sweep_factors(int n, int M, const std::vector<double>& sub, const std::vector<double>& dia,
+                      const std::vector<double>& sup, std::vector<float>& out);
 
 // ------------------------------------------------------------------ init
 MGSolver* MGSolver::create(const anel_grid_desc* g, const anel_mg_params* p, int device,
@@ -176,8 +179,15 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
   ANEL_CUDA_TRY(cudaEventCreate(&ev0_));
   ANEL_CUDA_TRY(cudaEventCreate(&ev1_));
   const bool mixed = p->precision == ANEL_PREC_MIXED;
+  // column layout of the FP32 levels: z never coarsened, nz = 32*M
+  bool col_ok = mixed && p->smoother == ANEL_SMOOTHER_ZLINE && nz_ % 32 == 0 &&
+                col_rows_supported(nz_ / 32);
+  for (int l = 1; l <= ngrid_ && col_ok; ++l) col_ok = geo_[l].n[2] == nz_;
   for (int l = 1; l <= ngrid_; ++l) {
     const int64_t G = geo_[l].G;
+    // FP32 arrays are sized for either layout, so the choice can still
+    // fall back to the row-major one below
+    const int64_t G32 = col_ok ? std::max<int64_t>(G, (int64_t)geo_[l].X * geo_[l].Y * col_stride(nz_)) : G;
     const size_t ncoef = 2 * (size_t)geo_[l].X + 2 * (size_t)geo_[l].Y + 4 * (size_t)geo_[l].Z;
     if (!mixed || l == ngrid_) {
       ANEL_CUDA_TRY(cudaMalloc(&d_phi64_[l], G * sizeof(double)));
@@ -211,10 +221,10 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
       }
     }
     if (mixed) {
-      ANEL_CUDA_TRY(cudaMalloc(&d_phi32_[l], G * sizeof(float)));
-      ANEL_CUDA_TRY(cudaMalloc(&d_src32_[l], G * sizeof(float)));
-      ANEL_CUDA_TRY(cudaMemset(d_phi32_[l], 0, G * sizeof(float)));
-      ANEL_CUDA_TRY(cudaMemset(d_src32_[l], 0, G * sizeof(float)));
+      ANEL_CUDA_TRY(cudaMalloc(&d_phi32_[l], G32 * sizeof(float)));
+      ANEL_CUDA_TRY(cudaMalloc(&d_src32_[l], G32 * sizeof(float)));
+      ANEL_CUDA_TRY(cudaMemset(d_phi32_[l], 0, G32 * sizeof(float)));
+      ANEL_CUDA_TRY(cudaMemset(d_src32_[l], 0, G32 * sizeof(float)));
       ANEL_CUDA_TRY(cudaMalloc(&d_coef32_[l], ncoef * sizeof(float)));
       // ghost table of the FP32 cycle's homogeneous rule (32-bit indices)
       if (G < ((int64_t)1 << 31)) {
@@ -226,12 +236,21 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
   }
   ANEL_CUDA_TRY(cudaStreamSynchronize(stream_));
   for (int l = 1; l <= ngrid_; ++l)
-    if (d_zseg32_[l] && d_gtab32_[l]) {
+    if ((d_zseg32_[l] || col_ok) && d_gtab32_[l]) {
       const int st = build_self_ghosting(l);
       if (st != ANEL_OK) return st;
     }
+  for (int l = 1; l <= ngrid_ && col_ok; ++l) col_ok = d_img32_[l] != nullptr;
+  col_ = col_ok;
+  if (col_) {
+    colM_ = nz_ / 32;
+    for (int l = 1; l <= ngrid_; ++l)
+      ANEL_CUDA_TRY(cudaMalloc(&d_colfac_[l], (size_t)col_fac_floats(colM_) * sizeof(float)));
+  }
   ANEL_CUDA_TRY(cudaMalloc(&d_max_, 2 * sizeof(unsigned long long)));
-  ANEL_CUDA_TRY(cudaMalloc(&d_part_, (size_t)resid_part_doubles(L64(ngrid_)) * sizeof(double)));
+  int64_t npart = resid_part_doubles(L64(ngrid_));
+  if (col_) npart = std::max(npart, col_resid_part_doubles(L64(ngrid_)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_part_, (size_t)npart * sizeof(double)));
   ANEL_CUDA_TRY(cudaMalloc(&d_norm_, 2 * sizeof(double)));
   ANEL_CUDA_TRY(cudaHostAlloc(&h_pin_, 4 * sizeof(double), cudaHostAllocMapped));
   // default density r == 1
@@ -259,6 +278,7 @@ MGSolver::~MGSolver() {
     cudaFree(d_zcr32_[l]);
     cudaFree(d_gtab32_[l]);
     cudaFree(d_img32_[l]);
+    cudaFree(d_colfac_[l]);
   }
   cudaFree(d_max_);
   cudaFree(d_part_);
@@ -605,6 +625,19 @@ int MGSolver::build_zline_factors() {
     ANEL_CUDA_TRY(cudaMemcpy(d_zf64_[l], both.data(), both.size() * sizeof(double), cudaMemcpyHostToDevice));
     std::vector<float> b32(both.begin(), both.end());
     ANEL_CUDA_TRY(cudaMemcpy(d_zf32_[l], b32.data(), b32.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (d_colfac_[l]) {
+      std::vector<double> sub(n), dia(n), sup(n);
+      for (int r = 0; r < n; ++r) {
+        const int k = r + 2;
+        sub[r] = c.cz5[k - 1];
+        sup[r] = c.cz6[k - 1];
+        dia[r] = -(a1 + a2 + a3 + a4 + c.dz5[k - 1] + c.dz6[k - 1]);
+      }
+      std::vector<float> cf;
+      const int st = col_sweep_factors(n, colM_, sub, dia, sup, cf);
+      if (st != ANEL_OK) return st;
+      ANEL_CUDA_TRY(cudaMemcpy(d_colfac_[l], cf.data(), cf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
     if (d_zseg32_[l]) {
       std::vector<double> sub(n), dia(n), sup(n);
       for (int r = 0; r < n; ++r) {
@@ -687,6 +720,107 @@ int zline_cr_factors(int n, int S, const std::vector<double>& sub, const std::ve
   for (double v : out)
     if (!std::isfinite(v)) {
       set_error("z-line cyclic reduction multipliers are not finite");
+      return ANEL_ERR_NONFINITE;
+    }
+  return ANEL_OK;
+}
+
+// Factors of the column sweep (k_col_sweep) for a line of n = 32*M rows
+// (sub, dia, sup; sub[0] and sup[n-1] belong to the z ghosts and are not
+// part of the system): lane s owns rows s*M .. s*M+M-1, the last of them a
+// separator.  Per lane and inner row w (rows s*M+w, w < M-1): the Thomas
+// factors ap, 1/bp and sup of the inner rows taken alone, and the spikes L
+// (their solution for a unit value in the previous separator, coupling
+// -sub of the first inner row; 0 on lane 0) and R (for a unit value in the
+// own separator, coupling -sup of the last inner row).  Eliminating the
+// inner rows leaves, in the separators X_s,
+//   sub[h] L_s(last) X_(s-1) + (dia[h] + sub[h] R_s(last) + sup[h] L_(s+1)(first)) X_s
+//     + sup[h] R_(s+1)(first) X_(s+1) = rhs[h] - sub[h] y_s(last) - sup[h] y_(s+1)(first)
+// (h the separator row, y the inner rows' local solution), whose cyclic
+// reduction multipliers come from zline_cr_factors.  Layout: see
+// col_fac_floats.
+int col_sweep_factors(int n, int M, const std::vector<double>& sub, const std::vector<double>& dia,
+                      const std::vector<double>& sup, std::vector<float>& out) {
+  constexpr int P = 32;
+  if (M < 2 || n != P * M) {
+    set_error("column sweep needs nz = 32*M rows with M >= 2 (nz = %d)", n);
+    return ANEL_ERR_UNSUPPORTED;
+  }
+  const int I = M - 1;  // inner rows per lane
+  std::vector<double> ap((size_t)I * P, 0.0), rbp((size_t)I * P, 0.0), sp((size_t)I * P, 0.0),
+      Ls((size_t)I * P, 0.0), Rs((size_t)I * P, 0.0);
+  auto at = [&](std::vector<double>& a, int w, int s) -> double& { return a[(size_t)w * P + s]; };
+  std::vector<double> bp(I), w1(I), w2(I);
+  for (int s = 0; s < P; ++s) {
+    const int lo = s * M;
+    bp[0] = dia[lo];
+    for (int w = 1; w < I; ++w) {
+      at(ap, w, s) = -sub[lo + w] / bp[w - 1];
+      bp[w] = dia[lo + w] + at(ap, w, s) * sup[lo + w - 1];
+    }
+    for (int w = 0; w < I; ++w) {
+      if (!(std::isfinite(bp[w]) && bp[w] != 0.0)) {
+        set_error("column sweep: inner rows of lane %d are singular", s);
+        return ANEL_ERR_NONFINITE;
+      }
+      at(rbp, w, s) = 1.0 / bp[w];
+      at(sp, w, s) = sup[lo + w];
+    }
+    // solve T x = e on the inner rows
+    auto solve = [&](std::vector<double>& e) {
+      double g = e[0];
+      e[0] = g;
+      for (int w = 1; w < I; ++w) {
+        g = e[w] + at(ap, w, s) * g;
+        e[w] = g;
+      }
+      double x = g / bp[I - 1];
+      e[I - 1] = x;
+      for (int w = I - 2; w >= 0; --w) {
+        x = (e[w] - sup[lo + w] * x) / bp[w];
+        e[w] = x;
+      }
+    };
+    std::fill(w1.begin(), w1.end(), 0.0);
+    if (s > 0) {
+      w1[0] = -sub[lo];
+      solve(w1);
+    }
+    std::fill(w2.begin(), w2.end(), 0.0);
+    w2[I - 1] = -sup[lo + I - 1];
+    solve(w2);
+    for (int w = 0; w < I; ++w) {
+      at(Ls, w, s) = w1[w];
+      at(Rs, w, s) = w2[w];
+    }
+  }
+  std::vector<double> A(P, 0.0), B(P, 0.0), C(P, 0.0), subh(P, 0.0), suph(P, 0.0);
+  for (int s = 0; s < P; ++s) {
+    const int h = s * M + I;
+    subh[s] = sub[h];
+    suph[s] = s < P - 1 ? sup[h] : 0.0;
+    A[s] = s > 0 ? sub[h] * at(Ls, I - 1, s) : 0.0;
+    B[s] = dia[h] + sub[h] * at(Rs, I - 1, s) + (s < P - 1 ? sup[h] * at(Ls, 0, s + 1) : 0.0);
+    C[s] = s < P - 1 ? sup[h] * at(Rs, 0, s + 1) : 0.0;
+  }
+  std::vector<double> cr;
+  const int st = zline_cr_factors(P, 5, A, B, C, cr);
+  if (st != ANEL_OK) return st;
+  out.assign((size_t)col_fac_floats(M), 0.0f);
+  size_t o = 0;
+  for (const std::vector<double>* a : {&ap, &rbp, &sp, &Ls, &Rs})
+    for (double v : *a) out[o++] = (float)v;
+  for (int s = 0; s < P; ++s) out[o + s] = (float)subh[s];
+  for (int s = 0; s < P; ++s) out[o + P + s] = (float)suph[s];
+  for (int q = 0; q < 5; ++q)
+    for (int s = 0; s < P; ++s) {
+      out[o + (2 + q) * P + s] = (float)cr[(size_t)(2 * q) * P + s];
+      out[o + (7 + q) * P + s] = (float)cr[(size_t)(2 * q + 1) * P + s];
+    }
+  for (int s = 0; s < P; ++s) out[o + 12 * P + s] = (float)cr[(size_t)10 * P + s];
+  for (float v : out)
+    if (!std::isfinite(v)) {
+      set_error("column sweep factors are not finite in FP32");
       return ANEL_ERR_NONFINITE;
     }
   return ANEL_OK;
@@ -901,6 +1035,38 @@ DevLevel<float> MGSolver::L32(int l, bool hom) const {
   return L;
 }
 
+ColLevel MGSolver::C32(int l) const {
+  const LevelGeom& G = geo_[l];
+  const LevelCoef& c = coef_[l];
+  ColLevel L;
+  L.nx = G.n[0];
+  L.ny = G.n[1];
+  L.nz = G.n[2];
+  L.X = G.X;
+  L.Y = G.Y;
+  L.CS = col_stride(G.n[2]);
+  L.phi = d_phi32_[l];
+  L.src = d_src32_[l];
+  // x/y-uniform line coefficients (checked by build_zline_factors)
+  L.a1 = (float)c.cx1[G.s[0] - 1];
+  L.a2 = (float)c.cx2[G.s[0] - 1];
+  L.a3 = (float)c.cy3[G.s[1] - 1];
+  L.a4 = (float)c.cy4[G.s[1] - 1];
+  const float* z = d_coef32_[l] + 2 * (size_t)G.X + 2 * (size_t)G.Y;
+  L.cz5 = z;
+  L.cz6 = z + G.Z;
+  L.dz5 = z + 2 * G.Z;
+  L.dz6 = z + 3 * G.Z;
+  L.img = d_img32_[l];
+  L.z1 = zcode_[l][0];
+  L.zZ = zcode_[l][1];
+  return L;
+}
+
+int64_t MGSolver::fp32_elems(int l) const {
+  return col_ ? (int64_t)geo_[l].X * geo_[l].Y * col_stride(geo_[l].n[2]) : geo_[l].G;
+}
+
 DevLevel<double> MGSolver::fine_view(double* phi, const double* src) const {
   DevLevel<double> L = L64(ngrid_);
   L.phi = phi;
@@ -1003,6 +1169,42 @@ void MGSolver::cycle32(cudaStream_t s) {
     launch_bdry(F, F.phi, s);
   }
   relax32(ng, post[ng - 1], s);
+}
+
+// The FP32 cycle on the column layout: cycle32's schedule, the boundary
+// pass after each prolongation folded into the prolongation, the coarse
+// correction zeroed before each restriction.
+void MGSolver::relax_col(int l, int iters, cudaStream_t s) {
+  const ColLevel L = C32(l);
+  const bool prof = prof_ && l == ngrid_;
+  for (int it = 0; it < iters; ++it)
+    for (int color = 0; color < 2; ++color) {
+      if (prof) prof_begin(s);
+      launch_col_sweep(L, color, d_colfac_[l], colM_, s);
+      if (prof) prof_end(s);
+    }
+}
+
+void MGSolver::cycle_col(cudaStream_t s) {
+  const int ng = ngrid_;
+  const int* pre = prm_.pre_relax;
+  const int* post = prm_.post_relax;
+  auto down = [&](int l) {
+    cudaMemsetAsync(d_phi32_[l - 1], 0, fp32_elems(l - 1) * sizeof(float), s);
+    launch_col_restrict(C32(l), C32(l - 1), coarsen_dirs(l - 1), s);
+  };
+  relax_col(ng, pre[ng - 1], s);
+  down(ng);
+  for (int l = ng - 1; l >= 2; --l) {
+    relax_col(l, pre[l - 1], s);
+    down(l);
+  }
+  relax_col(1, pre[0], s);
+  for (int l = 1; l <= ng - 1; ++l) {
+    relax_col(l, post[l - 1], s);
+    launch_col_prolong(C32(l + 1), C32(l), coarsen_dirs(l), s);
+  }
+  relax_col(ng, post[ng - 1], s);
 }
 
 SegFac<float> MGSolver::segfac32(int l) const {
@@ -1211,20 +1413,24 @@ int MGSolver::solve_fp64(double* d_phi, const double* d_rhs, cudaStream_t s,
 // same order, so results are unchanged.  Profiling runs (events between
 // sweeps) and the legacy default stream stay uncaptured.
 void MGSolver::run_cycle32(cudaStream_t s) {
-  const DevLevel<float> E = L32(ngrid_, true);
+  float* const e = d_phi32_[ngrid_];
+  const int64_t ne = fp32_elems(ngrid_);
+  auto cycle = [&]() {
+    cudaMemsetAsync(e, 0, ne * sizeof(float), s);
+    if (col_) cycle_col(s);
+    else cycle32(s);
+  };
   const bool can = !prof_ && !g32_off_ && s != nullptr && s != cudaStreamLegacy &&
                    s != cudaStreamPerThread;
   if (!can || (++g32_calls_ < 2 && !g32x_)) {
-    cudaMemsetAsync(E.phi, 0, E.G * sizeof(float), s);
-    cycle32(s);
+    cycle();
     return;
   }
   if (!g32x_) {
     const int64_t l0 = t_launches;
     bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     if (ok) {
-      cudaMemsetAsync(E.phi, 0, E.G * sizeof(float), s);
-      cycle32(s);
+      cycle();
       cudaGraph_t g = nullptr;
       ok = cudaStreamEndCapture(s, &g) == cudaSuccess && g;
       const int64_t n = t_launches - l0;  // counted while capturing, not run
@@ -1238,8 +1444,7 @@ void MGSolver::run_cycle32(cudaStream_t s) {
       cudaGetLastError();
       g32x_ = nullptr;
       g32_off_ = true;
-      cudaMemsetAsync(E.phi, 0, E.G * sizeof(float), s);
-      cycle32(s);
+      cycle();
       return;
     }
   }
@@ -1256,8 +1461,10 @@ int MGSolver::solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s,
   double rel = 0.0;
   int iter = 0;
   bool conv = false;
+  const ColLevel Ec = col_ ? C32(ng) : ColLevel{};
   for (iter = 0; iter <= prm_.maxcy; ++iter) {
-    launch_resid_store(Fu, d_phi, d_rhs, E.src, d_part_, d_norm_, s);
+    if (col_) launch_col_resid_store(Fu, d_phi, d_rhs, Ec, d_part_, d_norm_, s);
+    else launch_resid_store(Fu, d_phi, d_rhs, E.src, d_part_, d_norm_, s);
     copy_words(d_norm_, h_pin_, 2, s);
     ANEL_CUDA_TRY(cudaStreamSynchronize(s));
     rel = h_pin_[1] > 0.0 ? std::sqrt(h_pin_[0] / h_pin_[1]) : std::sqrt(h_pin_[0]);
@@ -1268,7 +1475,8 @@ int MGSolver::solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s,
     }
     if (iter == prm_.maxcy) break;
     run_cycle32(s);
-    launch_add_correction(Fu, d_phi, E.phi, s);
+    if (col_) launch_col_add_correction(Fu, d_phi, Ec, s);
+    else launch_add_correction(Fu, d_phi, E.phi, s);
     launch_bdry(Fu, d_phi, s);
   }
   rep->iter = conv ? iter : prm_.maxcy + 1;

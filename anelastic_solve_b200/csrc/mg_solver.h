@@ -4,6 +4,7 @@
 #include <memory>
 #include <vector>
 
+#include "mg_col.h"
 #include "mg_launch.h"
 
 namespace anel {
@@ -56,6 +57,16 @@ class MGSolver {
   int64_t g32_launches_ = 0;
   int g32_calls_ = 0;
   bool g32_off_ = false;
+  // column layout of the FP32 levels (mg_col.cuh): used by the mixed
+  // ZLINE cycle with x/y semi-coarsening when nz = 32*M (M a supported
+  // row count) and every level's ghosts are copies the sweeps can write
+  bool col_ = false;
+  int colM_ = 0;
+  float* d_colfac_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  ColLevel C32(int l) const;
+  int64_t fp32_elems(int l) const;
+  void relax_col(int l, int iters, cudaStream_t s);
+  void cycle_col(cudaStream_t s);
   int solve_fp64(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
   int solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
   int coarsen_dirs(int lC) const;

@@ -821,7 +821,10 @@ def main():
     # in place (+4 B); the FP32 partitioned z-line kernel keeps them on chip.
     zl = args.smoother == "zline"
     bpc = 6.0 if args.prec == "mixed" else (16.0 if zl else 12.0)
-    if zl and args.prec == "mixed" and nz % 16 == 0 and 32 <= nz <= 512:
+    if zl and args.prec == "mixed" and nz % 32 == 0 and nz // 32 in (2, 3, 4, 6, 8, 12, 16):
+        # the column-layout FP32 cycle (one warp per z-line)
+        kernel = f"k_col_sweep<{nz // 32}>"
+    elif zl and args.prec == "mixed" and nz % 16 == 0 and 32 <= nz <= 512:
         kernel = "k_zline_seg<float,16,32>"
     else:
         kname = "k_zline" if zl else "k_rb_sweep"
