@@ -23,6 +23,7 @@ SIGNATURES = {
     "anel_last_error": (C.c_char_p, []),
     "anel_version": (C.c_int, []),
     "anel_kernel_launch_count": (C.c_int64, []),
+    "anel_tuning_report": (C.c_int32, [C.c_char_p, C.c_int32]),
     "anel_mg_init": (C.c_int, [C.POINTER(abi.GridDesc), C.POINTER(abi.MGParams)]),
     "anel_mg_set_density": (C.c_int, [_DP]),
     "anel_mg_solve": (None, [_DP, _DP, _IP, _DP]),
@@ -106,3 +107,11 @@ def check(code: int, allow=(abi.OK,)) -> int:
 
 def launch_count() -> int:
     return int(lib().anel_kernel_launch_count())
+
+
+def tuning_report() -> str:
+    """The autotuner's choices so far (anel_tuning_report)."""
+    n = int(lib().anel_tuning_report(None, 0))
+    buf = C.create_string_buffer(n + 1)
+    lib().anel_tuning_report(buf, n + 1)
+    return buf.value.decode()

@@ -36,6 +36,7 @@ SOURCES = {
     "ns_dsm.cu": ["-fmad=false"],
     "mg_col.cu": ["-fmad=true"],
     "mg_col64.cu": ["-fmad=false"],
+    "tune.cu": [],
 }
 
 

@@ -1,10 +1,12 @@
 // api.cu -- the extern "C" boundary declared in include/anel.h.
 #include <cstdarg>
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
 #include "mg_solver.h"
+#include "tune.h"
 #include "ns_solver.h"
 
 namespace anel {
@@ -76,6 +78,16 @@ extern "C" {
 const char* anel_last_error(void) { return anel::last_error(); }
 int anel_version(void) { return 100; }
 int64_t anel_kernel_launch_count(void) { return anel::g_launches.load(); }
+
+int32_t anel_tuning_report(char* buf, int32_t cap) {
+  const std::string r = anel::tune_report();
+  if (buf && cap > 0) {
+    const size_t n = r.size() < (size_t)(cap - 1) ? r.size() : (size_t)(cap - 1);
+    std::memcpy(buf, r.data(), n);
+    buf[n] = '\0';
+  }
+  return (int32_t)r.size();
+}
 
 // ------------------------------------------------------------ drop-in MG
 int anel_mg_init(const anel_grid_desc* grid, const anel_mg_params* params) {

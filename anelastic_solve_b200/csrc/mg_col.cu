@@ -5,41 +5,63 @@
 
 namespace anel {
 
-void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, cudaStream_t s) {
+template <int M, int NL, int MINB>
+static void col_sweep_launch(const ColLevel& L, int color, const float* fac, cudaStream_t s) {
   const int64_t nlines = (int64_t)((L.nx + 1) / 2) * L.ny;
-  int64_t b = (nlines + kColWarps - 1) / kColWarps;
-  const int64_t cap = 148 * 6;
+  const int64_t per = (int64_t)kColWarps * NL;
+  int64_t b = (nlines + per - 1) / per;
+  const int64_t cap = 148 * MINB * 2;
   if (b > cap) b = cap;
   if (b < 1) b = 1;
-  const dim3 grid((unsigned)b), block(32 * kColWarps);
+  k_col_sweep<M, NL, MINB><<<(unsigned)b, 32 * kColWarps, 0, s>>>(L, color, fac);
+}
+
+template <int M>
+static void col_sweep_variant(const ColLevel& L, int color, const float* fac, int variant, cudaStream_t s) {
+  switch (variant) {
+    case 1: col_sweep_launch<M, 1, 4>(L, color, fac, s); break;
+    case 2: col_sweep_launch<M, 2, 2>(L, color, fac, s); break;
+    default: col_sweep_launch<M, 1, 3>(L, color, fac, s); break;
+  }
+}
+
+void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, int variant, cudaStream_t s) {
   switch (M) {
-    case 2: k_col_sweep<2><<<grid, block, 0, s>>>(L, color, fac); break;
-    case 3: k_col_sweep<3><<<grid, block, 0, s>>>(L, color, fac); break;
-    case 4: k_col_sweep<4><<<grid, block, 0, s>>>(L, color, fac); break;
-    case 6: k_col_sweep<6><<<grid, block, 0, s>>>(L, color, fac); break;
-    case 8: k_col_sweep<8><<<grid, block, 0, s>>>(L, color, fac); break;
-    case 12: k_col_sweep<12><<<grid, block, 0, s>>>(L, color, fac); break;
-    default: k_col_sweep<16><<<grid, block, 0, s>>>(L, color, fac); break;
+    case 2: col_sweep_variant<2>(L, color, fac, variant, s); break;
+    case 3: col_sweep_variant<3>(L, color, fac, variant, s); break;
+    case 4: col_sweep_variant<4>(L, color, fac, variant, s); break;
+    case 6: col_sweep_variant<6>(L, color, fac, variant, s); break;
+    case 8: col_sweep_variant<8>(L, color, fac, variant, s); break;
+    case 12: col_sweep_variant<12>(L, color, fac, variant, s); break;
+    default: col_sweep_variant<16>(L, color, fac, variant, s); break;
   }
   count_launch();
 }
 
+static unsigned col_xfer_blocks(int64_t items) {
+  int64_t b = (items + kColXferThreads - 1) / kColXferThreads;
+  const int64_t cap = 148 * 8;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
 void launch_col_restrict(const ColLevel& F, const ColLevel& C, int cdir, cudaStream_t s) {
-  const dim3 g((unsigned)((int64_t)C.nx * C.ny), (unsigned)((C.nz + 127) / 128));
+  const unsigned g = col_xfer_blocks((int64_t)C.nx * C.ny * (C.nz / 4));
   switch (cdir & 3) {
-    case 1: k_col_restrict<1><<<g, 128, 0, s>>>(F, C); break;
-    case 2: k_col_restrict<2><<<g, 128, 0, s>>>(F, C); break;
-    default: k_col_restrict<3><<<g, 128, 0, s>>>(F, C); break;
+    case 1: k_col_restrict<1><<<g, kColXferThreads, 0, s>>>(F, C); break;
+    case 2: k_col_restrict<2><<<g, kColXferThreads, 0, s>>>(F, C); break;
+    default: k_col_restrict<3><<<g, kColXferThreads, 0, s>>>(F, C); break;
   }
   count_launch();
 }
 
 void launch_col_prolong(const ColLevel& F, const ColLevel& C, int cdir, cudaStream_t s) {
-  const dim3 g((unsigned)((int64_t)F.nx * F.ny), (unsigned)((F.nz + 127) / 128));
+  const unsigned g = col_xfer_blocks((int64_t)F.nx * F.ny * (F.nz / 4));
   switch (cdir & 3) {
-    case 1: k_col_prolong<1><<<g, 128, 0, s>>>(F, C); break;
-    case 2: k_col_prolong<2><<<g, 128, 0, s>>>(F, C); break;
-    default: k_col_prolong<3><<<g, 128, 0, s>>>(F, C); break;
+    case 1: k_col_prolong<1><<<g, kColXferThreads, 0, s>>>(F, C); break;
+    case 2: k_col_prolong<2><<<g, kColXferThreads, 0, s>>>(F, C); break;
+    default: k_col_prolong<3><<<g, kColXferThreads, 0, s>>>(F, C); break;
   }
   count_launch();
 }

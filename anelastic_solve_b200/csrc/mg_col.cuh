@@ -79,210 +79,324 @@ __device__ __forceinline__ void col_put(float* __restrict__ P, int64_t c, float 
 // (i + j) % 2 == color, in the pairing of k_zline_seg.  Each line's
 // right-hand side takes the other colour's horizontal neighbours and the
 // line's own z-ghosts as known; the new values are written with their
-// ghost copies.
-template <int M>
-__global__ void __launch_bounds__(32 * kColWarps, 3) k_col_sweep(ColLevel L, int color,
-                                                                 const float* __restrict__ fac) {
+// ghost copies.  A warp takes NL consecutive lines of a row per step (they
+// share horizontal neighbours, and the per-lane factors are read once for
+// all of them); MINB is the occupancy the register budget is set for.
+template <int M, int NL, int MINB>
+__global__ void __launch_bounds__(32 * kColWarps, MINB) k_col_sweep(ColLevel L, int color,
+                                                                    const float* __restrict__ fac) {
   constexpr int NF = col_fac_floats(M);
   constexpr int N = 32 * M;
   __shared__ float sf[NF];
-  __shared__ float sy[kColWarps][N + M];
+  __shared__ float sy[kColWarps][NL][N + M];
   for (int q = threadIdx.x; q < NF; q += blockDim.x) sf[q] = fac[q];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float* ys = sy[warp];
   const float* Fap = sf;
   const float* Frbp = sf + (M - 1) * 32;
   const float* Fsup = sf + 2 * (M - 1) * 32;
   const float* FL = sf + 3 * (M - 1) * 32;
   const float* FR = sf + 4 * (M - 1) * 32;
   const float* Fg = sf + 5 * (M - 1) * 32;
-  const float sub_h = Fg[lane], sup_h = Fg[32 + lane], rb = Fg[12 * 32 + lane];
   const int pairs = (L.nx + 1) >> 1;
   const int64_t nlines = (int64_t)pairs * L.ny;
   const int64_t CS = L.CS, XC = (int64_t)L.X * L.CS;
   const float a1 = L.a1, a2 = L.a2, a3 = L.a3, a4 = L.a4;
   const float c5b = L.cz5[1], c6t = L.cz6[L.nz];  // row 0 to its k=1 ghost, row n-1 to k=Z
-  for (int64_t t = (int64_t)blockIdx.x * kColWarps + warp; t < nlines; t += (int64_t)gridDim.x * kColWarps) {
-    const int j = 2 + (int)(t / pairs);
-    const int i0 = 2 + 2 * (int)(t % pairs);
-    const int i = i0 + ((color + i0 + j) & 1);
-    if (i > L.nx + 1) continue;  // uniform across the warp
-    const int64_t c0 = col_cell(L, i, j, 2);  // row 0
+  for (int64_t t0 = ((int64_t)blockIdx.x * kColWarps + warp) * NL; t0 < nlines;
+       t0 += (int64_t)gridDim.x * kColWarps * NL) {
+    int64_t c0[NL];
+    bool on[NL];
+    int ii[NL], jj[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+      const int64_t t = t0 + l;
+      const int j = 2 + (int)(t / pairs);
+      const int i0 = 2 + 2 * (int)(t % pairs);
+      const int i = i0 + ((color + i0 + j) & 1);
+      on[l] = t < nlines && i <= L.nx + 1;  // uniform across the warp
+      ii[l] = i;
+      jj[l] = j;
+      c0[l] = on[l] ? col_cell(L, i, j, 2) : 0;  // row 0
+    }
     const float* __restrict__ P = L.phi;
     const float* __restrict__ S = L.src;
-    float v[M];
+    float y[NL][M];
 #pragma unroll
-    for (int q = 0; q < M; ++q) {
-      const int64_t c = c0 + lane + 32 * q;
-      v[q] = S[c] - (a1 * P[c - CS] + a2 * P[c + CS] + a3 * P[c - XC] + a4 * P[c + XC]);
+    for (int l = 0; l < NL; ++l) {
+      float v[M];
+      if (on[l]) {
+#pragma unroll
+        for (int q = 0; q < M; ++q) {
+          const int64_t c = c0[l] + lane + 32 * q;
+          v[q] = S[c] - (a1 * P[c - CS] + a2 * P[c + CS] + a3 * P[c - XC] + a4 * P[c + XC]);
+        }
+        if (lane == 0) v[0] -= c5b * P[c0[l] - 1];
+        if (lane == 31) v[M - 1] -= c6t * P[c0[l] + N];
+      } else {
+#pragma unroll
+        for (int q = 0; q < M; ++q) v[q] = 0.f;
+      }
+      // row order -> segment order (lane s: rows s*M .. s*M+M-1)
+#pragma unroll
+      for (int q = 0; q < M; ++q) sy[warp][l][col_pad(lane + 32 * q)] = v[q];
     }
-    if (lane == 0) v[0] -= c5b * P[c0 - 1];
-    if (lane == 31) v[M - 1] -= c6t * P[c0 + N];
-    // row order -> segment order (lane s: rows s*M .. s*M+M-1)
-#pragma unroll
-    for (int q = 0; q < M; ++q) ys[col_pad(lane + 32 * q)] = v[q];
     __syncwarp();
-    float y[M];
 #pragma unroll
-    for (int w = 0; w < M; ++w) y[w] = ys[col_pad(lane * M + w)];
+    for (int l = 0; l < NL; ++l)
+#pragma unroll
+      for (int w = 0; w < M; ++w) y[l][w] = sy[warp][l][col_pad(lane * M + w)];
     __syncwarp();
     // inner rows 0..M-2: local solution with both separators at zero
-    float g = y[0];
+    float g[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) g[l] = y[l][0];
 #pragma unroll
     for (int w = 1; w < M - 1; ++w) {
-      g = y[w] + Fap[w * 32 + lane] * g;
-      y[w] = g;
+      const float a = Fap[w * 32 + lane];
+#pragma unroll
+      for (int l = 0; l < NL; ++l) {
+        g[l] = y[l][w] + a * g[l];
+        y[l][w] = g[l];
+      }
     }
-    float x = g * Frbp[(M - 2) * 32 + lane];
-    y[M - 2] = x;
+    {
+      const float r = Frbp[(M - 2) * 32 + lane];
+#pragma unroll
+      for (int l = 0; l < NL; ++l) {
+        g[l] = g[l] * r;
+        y[l][M - 2] = g[l];
+      }
+    }
 #pragma unroll
     for (int w = M - 3; w >= 0; --w) {
-      x = (y[w] - Fsup[w * 32 + lane] * x) * Frbp[w * 32 + lane];
-      y[w] = x;
+      const float c = Fsup[w * 32 + lane], r = Frbp[w * 32 + lane];
+#pragma unroll
+      for (int l = 0; l < NL; ++l) {
+        g[l] = (y[l][w] - c * g[l]) * r;
+        y[l][w] = g[l];
+      }
     }
     // separator system across the lanes
-    const float ynext = __shfl_down_sync(kFull, y[0], 1);
-    float h = y[M - 1] - sub_h * y[M - 2] - (lane < 31 ? sup_h * ynext : 0.f);
+    const float sub_h = Fg[lane], sup_h = Fg[32 + lane];
+    float h[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+      const float ynext = __shfl_down_sync(kFull, y[l][0], 1);
+      h[l] = y[l][M - 1] - sub_h * y[l][M - 2] - (lane < 31 ? sup_h * ynext : 0.f);
+    }
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
       const int st = 1 << q;
-      const float up = __shfl_up_sync(kFull, h, st);
-      const float dn = __shfl_down_sync(kFull, h, st);
-      h = h + Fg[(2 + q) * 32 + lane] * up + Fg[(7 + q) * 32 + lane] * dn;
-    }
-    const float xs = h * rb;
-    const float xprev = __shfl_up_sync(kFull, xs, 1);  // lane 0: L = 0
+      const float al = Fg[(2 + q) * 32 + lane], ga = Fg[(7 + q) * 32 + lane];
 #pragma unroll
-    for (int w = 0; w < M - 1; ++w) y[w] = y[w] + FL[w * 32 + lane] * xprev + FR[w * 32 + lane] * xs;
-    y[M - 1] = xs;
+      for (int l = 0; l < NL; ++l) {
+        const float up = __shfl_up_sync(kFull, h[l], st);
+        const float dn = __shfl_down_sync(kFull, h[l], st);
+        h[l] = h[l] + al * up + ga * dn;
+      }
+    }
+    float xs[NL], xprev[NL];
+    {
+      const float rb = Fg[12 * 32 + lane];
+#pragma unroll
+      for (int l = 0; l < NL; ++l) {
+        xs[l] = h[l] * rb;
+        xprev[l] = __shfl_up_sync(kFull, xs[l], 1);  // lane 0: L = 0
+      }
+    }
+#pragma unroll
+    for (int w = 0; w < M - 1; ++w) {
+      const float fl = FL[w * 32 + lane], fr = FR[w * 32 + lane];
+#pragma unroll
+      for (int l = 0; l < NL; ++l) y[l][w] = y[l][w] + fl * xprev[l] + fr * xs[l];
+    }
+#pragma unroll
+    for (int l = 0; l < NL; ++l) y[l][M - 1] = xs[l];
     // segment order -> row order
 #pragma unroll
-    for (int w = 0; w < M; ++w) ys[col_pad(lane * M + w)] = y[w];
-    __syncwarp();
+    for (int l = 0; l < NL; ++l)
 #pragma unroll
-    for (int q = 0; q < M; ++q) v[q] = ys[col_pad(lane + 32 * q)];
+      for (int w = 0; w < M; ++w) sy[warp][l][col_pad(lane * M + w)] = y[l][w];
     __syncwarp();
-    int d0 = kNoImage, d1 = kNoImage, d2 = kNoImage;
-    if (L.img) {
-      const int* im = L.img + 3 * ((i - 2) + (int64_t)L.nx * (j - 2));
-      d0 = im[0];
-      d1 = im[1];
-      d2 = im[2];
-    }
-    const bool h0 = d0 != kNoImage, h1 = d1 != kNoImage, h2 = d2 != kNoImage;
-    const int64_t o0 = h0 ? (int64_t)d0 * CS : 0, o1 = h1 ? (int64_t)d1 * CS : 0,
-                  o2 = h2 ? (int64_t)d2 * CS : 0;
     float* __restrict__ Pw = L.phi;
 #pragma unroll
-    for (int q = 0; q < M; ++q) col_put(Pw, c0 + lane + 32 * q, v[q], o0, o1, o2, h0, h1, h2);
-    // z ghosts of the column and of its images
-    const float r0 = __shfl_sync(kFull, v[0], 0);
-    const float rn = __shfl_sync(kFull, v[M - 1], 31);
-    if (lane == 0 || lane == 31) {
-      const int code = lane == 0 ? L.z1 : L.zZ;
-      const float gv = code == 0 ? 0.f : (code == 1 ? r0 : rn);
-      col_put(Pw, lane == 0 ? c0 - 1 : c0 + N, gv, o0, o1, o2, h0, h1, h2);
+    for (int l = 0; l < NL; ++l) {
+      float v[M];
+#pragma unroll
+      for (int q = 0; q < M; ++q) v[q] = sy[warp][l][col_pad(lane + 32 * q)];
+      if (!on[l]) continue;
+      int d0 = kNoImage, d1 = kNoImage, d2 = kNoImage;
+      if (L.img) {
+        const int* im = L.img + 3 * ((ii[l] - 2) + (int64_t)L.nx * (jj[l] - 2));
+        d0 = im[0];
+        d1 = im[1];
+        d2 = im[2];
+      }
+      const bool h0 = d0 != kNoImage, h1 = d1 != kNoImage, h2 = d2 != kNoImage;
+      const int64_t o0 = h0 ? (int64_t)d0 * CS : 0, o1 = h1 ? (int64_t)d1 * CS : 0,
+                    o2 = h2 ? (int64_t)d2 * CS : 0;
+#pragma unroll
+      for (int q = 0; q < M; ++q) col_put(Pw, c0[l] + lane + 32 * q, v[q], o0, o1, o2, h0, h1, h2);
+      // z ghosts of the column and of its images
+      const float r0 = __shfl_sync(kFull, v[0], 0);
+      const float rn = __shfl_sync(kFull, v[M - 1], 31);
+      if (lane == 0 || lane == 31) {
+        const int code = lane == 0 ? L.z1 : L.zZ;
+        const float gv = code == 0 ? 0.f : (code == 1 ? r0 : rn);
+        col_put(Pw, lane == 0 ? c0[l] - 1 : c0[l] + N, gv, o0, o1, o2, h0, h1, h2);
+      }
     }
+    __syncwarp();
   }
 }
 
-// Residual f - A phi of fine cell (i,j,k), in the order of fine_resid.
-__device__ __forceinline__ float col_resid(const ColLevel& F, int i, int j, int k) {
+// Residuals f - A phi of fine cells (i,j,k..k+3) (k-2 a multiple of 4, so
+// the four cells are one aligned 16-byte vector), in fine_resid's order.
+__device__ __forceinline__ float4 col_resid4(const ColLevel& F, int i, int j, int k) {
   const int64_t c = col_cell(F, i, j, k);
   const float* __restrict__ p = F.phi;
-  const int64_t XC = (int64_t)F.X * F.CS;
-  const float diag = -(F.a1 + F.a2 + F.a3 + F.a4 + F.dz5[k - 1] + F.dz6[k - 1]);
-  float acc = F.a1 * p[c - F.CS];
-  acc = acc + F.a2 * p[c + F.CS];
-  acc = acc + F.a3 * p[c - XC];
-  acc = acc + F.a4 * p[c + XC];
-  acc = acc + F.cz5[k - 1] * p[c - 1];
-  acc = acc + F.cz6[k - 1] * p[c + 1];
-  acc = acc + diag * p[c];
-  return F.src[c] - acc;
+  const int64_t CS = F.CS, XC = (int64_t)F.X * F.CS;
+  const float4 C = *reinterpret_cast<const float4*>(p + c);
+  const float4 W = *reinterpret_cast<const float4*>(p + c - CS);
+  const float4 E = *reinterpret_cast<const float4*>(p + c + CS);
+  const float4 S = *reinterpret_cast<const float4*>(p + c - XC);
+  const float4 N = *reinterpret_cast<const float4*>(p + c + XC);
+  const float4 Fv = *reinterpret_cast<const float4*>(F.src + c);
+  const float pm = p[c - 1], pp = p[c + 4];
+  const float cv[4] = {C.x, C.y, C.z, C.w}, wv[4] = {W.x, W.y, W.z, W.w}, ev[4] = {E.x, E.y, E.z, E.w};
+  const float sv[4] = {S.x, S.y, S.z, S.w}, nv[4] = {N.x, N.y, N.z, N.w}, fv[4] = {Fv.x, Fv.y, Fv.z, Fv.w};
+  const float dv[4] = {pm, C.x, C.y, C.z}, uv[4] = {C.y, C.z, C.w, pp};
+  float r[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int kq = k + q;
+    const float diag = -(F.a1 + F.a2 + F.a3 + F.a4 + F.dz5[kq - 1] + F.dz6[kq - 1]);
+    float acc = F.a1 * wv[q];
+    acc = acc + F.a2 * ev[q];
+    acc = acc + F.a3 * sv[q];
+    acc = acc + F.a4 * nv[q];
+    acc = acc + F.cz5[kq - 1] * dv[q];
+    acc = acc + F.cz6[kq - 1] * uv[q];
+    acc = acc + diag * cv[q];
+    r[q] = fv[q] - acc;
+  }
+  return make_float4(r[0], r[1], r[2], r[3]);
 }
 
-// mg_restr's x/y variants (z is not coarsened): coarse f of interior cell
-// (ic,jc,k) from the residuals of its children, in restrict_value's order.
-// Grid (coarse interior columns, ceil(nz/128)); the caller zeroes coarse phi.
+__device__ __forceinline__ float4 f4add(float4 a, float4 b) {
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ float4 f4scale(float s, float4 a) {
+  return make_float4(s * a.x, s * a.y, s * a.z, s * a.w);
+}
+
+constexpr int kColXferThreads = 256;
+
+// mg_restr's x/y variants (z is not coarsened): coarse f of interior cells
+// (ic,jc,k..k+3) from the residuals of their children, in restrict_value's
+// order.  One thread per coarse column and 4-row chunk (grid-stride); the
+// caller zeroes coarse phi.
 template <int CD>
-__global__ void __launch_bounds__(128) k_col_restrict(ColLevel F, ColLevel C) {
-  const int k = 2 + blockIdx.y * 128 + threadIdx.x;
-  if (k > C.nz + 1) return;
-  const int64_t col = blockIdx.x;
-  const int ic = 2 + (int)(col % C.nx), jc = 2 + (int)(col / C.nx);
+__global__ void __launch_bounds__(kColXferThreads) k_col_restrict(ColLevel F, ColLevel C) {
+  const int nch = C.nz >> 2;
+  const int64_t items = (int64_t)C.nx * C.ny * nch;
   constexpr bool cx = CD & 1, cy = CD & 2;
-  const int i = cx ? 2 * ic - 2 : ic;
-  const int j = cy ? 2 * jc - 2 : jc;
-  float v;
-  if constexpr (cx && cy) {
-    float s = col_resid(F, i, j, k);
-    s = s + col_resid(F, i + 1, j, k);
-    s = s + col_resid(F, i, j + 1, k);
-    s = s + col_resid(F, i + 1, j + 1, k);
-    v = 0.25f * s;
-  } else if constexpr (cx) {
-    v = 0.5f * (col_resid(F, i, j, k) + col_resid(F, i + 1, j, k));
-  } else {
-    v = 0.5f * (col_resid(F, i, j, k) + col_resid(F, i, j + 1, k));
+  for (int64_t t = (int64_t)blockIdx.x * kColXferThreads + threadIdx.x; t < items;
+       t += (int64_t)gridDim.x * kColXferThreads) {
+    const int ch = (int)(t % nch);
+    const int64_t col = t / nch;
+    const int ic = 2 + (int)(col % C.nx), jc = 2 + (int)(col / C.nx);
+    const int k = 2 + 4 * ch;
+    const int i = cx ? 2 * ic - 2 : ic;
+    const int j = cy ? 2 * jc - 2 : jc;
+    float4 v;
+    if constexpr (cx && cy) {
+      float4 s = col_resid4(F, i, j, k);
+      s = f4add(s, col_resid4(F, i + 1, j, k));
+      s = f4add(s, col_resid4(F, i, j + 1, k));
+      s = f4add(s, col_resid4(F, i + 1, j + 1, k));
+      v = f4scale(0.25f, s);
+    } else if constexpr (cx) {
+      v = f4scale(0.5f, f4add(col_resid4(F, i, j, k), col_resid4(F, i + 1, j, k)));
+    } else {
+      v = f4scale(0.5f, f4add(col_resid4(F, i, j, k), col_resid4(F, i, j + 1, k)));
+    }
+    *reinterpret_cast<float4*>(C.src + col_cell(C, ic, jc, k)) = v;
   }
-  C.src[col_cell(C, ic, jc, k)] = v;
 }
 
 // mg_cor's x/y variants for the fine interior, in prolong_corr's order,
 // with the ghost copies of the updated cells written alongside (the
-// boundary pass of the row-major cycle).  Grid (fine interior columns,
-// ceil(nz/128)).
+// boundary pass of the row-major cycle).  One thread per fine column and
+// 4-row chunk (grid-stride).
 template <int CD>
-__global__ void __launch_bounds__(128) k_col_prolong(ColLevel F, ColLevel C) {
-  const int k = 2 + blockIdx.y * 128 + threadIdx.x;
-  if (k > F.nz + 1) return;
-  const int64_t col = blockIdx.x;
-  const int i = 2 + (int)(col % F.nx), j = 2 + (int)(col / F.nx);
+__global__ void __launch_bounds__(kColXferThreads) k_col_prolong(ColLevel F, ColLevel C) {
+  const int nch = F.nz >> 2;
+  const int64_t items = (int64_t)F.nx * F.ny * nch;
   constexpr bool cx = CD & 1, cy = CD & 2;
-  const int ic = cx ? ((i + 1) >> 1) : i;
-  const int jc = cy ? ((j + 1) >> 1) : j;
-  const float wx0 = cx ? ((i & 1) ? 3.f : 1.f) : 1.f, wx1 = cx ? ((i & 1) ? 1.f : 3.f) : 0.f;
-  const float wy0 = cy ? ((j & 1) ? 3.f : 1.f) : 1.f, wy1 = cy ? ((j & 1) ? 1.f : 3.f) : 0.f;
-  const float* __restrict__ pc = C.phi + col_cell(C, ic, jc, k);
-  const int64_t ox = C.CS, oy = (int64_t)C.X * C.CS;
-  float corr;
-  if constexpr (cx && cy) {
-    float s = (wx0 * wy0) * pc[0];
-    s = s + (wx1 * wy0) * pc[ox];
-    s = s + (wx0 * wy1) * pc[oy];
-    s = s + (wx1 * wy1) * pc[ox + oy];
-    corr = s / 16.f;
-  } else if constexpr (cx) {
-    corr = (wx0 * pc[0] + wx1 * pc[ox]) / 4.f;
-  } else {
-    corr = (wy0 * pc[0] + wy1 * pc[oy]) / 4.f;
-  }
-  const int64_t c = col_cell(F, i, j, k);
-  float* __restrict__ P = F.phi;
-  const float v = P[c] + corr;
-  int d0 = kNoImage, d1 = kNoImage, d2 = kNoImage;
-  if (F.img) {
-    const int* im = F.img + 3 * ((i - 2) + (int64_t)F.nx * (j - 2));
-    d0 = im[0];
-    d1 = im[1];
-    d2 = im[2];
-  }
-  const bool h0 = d0 != kNoImage, h1 = d1 != kNoImage, h2 = d2 != kNoImage;
-  const int64_t o0 = h0 ? (int64_t)d0 * F.CS : 0, o1 = h1 ? (int64_t)d1 * F.CS : 0,
-                o2 = h2 ? (int64_t)d2 * F.CS : 0;
-  col_put(P, c, v, o0, o1, o2, h0, h1, h2);
-  // z ghosts: the k = 2 thread writes the ghosts that copy row k = 2 or
-  // are zero, the k = nz+1 thread those that copy row k = nz+1
-  const int64_t g1 = c - (k - 1), gZ = c + (F.nz + 2 - k);
-  if (k == 2) {
-    if (F.z1 != 2) col_put(P, g1, F.z1 == 1 ? v : 0.f, o0, o1, o2, h0, h1, h2);
-    if (F.zZ != 2) col_put(P, gZ, F.zZ == 1 ? v : 0.f, o0, o1, o2, h0, h1, h2);
-  }
-  if (k == F.nz + 1) {
-    if (F.z1 == 2) col_put(P, g1, v, o0, o1, o2, h0, h1, h2);
-    if (F.zZ == 2) col_put(P, gZ, v, o0, o1, o2, h0, h1, h2);
+  for (int64_t t = (int64_t)blockIdx.x * kColXferThreads + threadIdx.x; t < items;
+       t += (int64_t)gridDim.x * kColXferThreads) {
+    const int ch = (int)(t % nch);
+    const int64_t col = t / nch;
+    const int i = 2 + (int)(col % F.nx), j = 2 + (int)(col / F.nx);
+    const int k = 2 + 4 * ch;
+    const int ic = cx ? ((i + 1) >> 1) : i;
+    const int jc = cy ? ((j + 1) >> 1) : j;
+    const float wx0 = cx ? ((i & 1) ? 3.f : 1.f) : 1.f, wx1 = cx ? ((i & 1) ? 1.f : 3.f) : 0.f;
+    const float wy0 = cy ? ((j & 1) ? 3.f : 1.f) : 1.f, wy1 = cy ? ((j & 1) ? 1.f : 3.f) : 0.f;
+    const float* __restrict__ pc = C.phi + col_cell(C, ic, jc, k);
+    const int64_t ox = C.CS, oy = (int64_t)C.X * C.CS;
+    const float4 c00 = *reinterpret_cast<const float4*>(pc);
+    float4 corr;
+    if constexpr (cx && cy) {
+      const float4 c10 = *reinterpret_cast<const float4*>(pc + ox);
+      const float4 c01 = *reinterpret_cast<const float4*>(pc + oy);
+      const float4 c11 = *reinterpret_cast<const float4*>(pc + ox + oy);
+      const float w00 = wx0 * wy0, w10 = wx1 * wy0, w01 = wx0 * wy1, w11 = wx1 * wy1;
+      auto one = [&](float a, float b, float c, float d) {
+        float s = w00 * a;
+        s = s + w10 * b;
+        s = s + w01 * c;
+        s = s + w11 * d;
+        return s / 16.f;
+      };
+      corr = make_float4(one(c00.x, c10.x, c01.x, c11.x), one(c00.y, c10.y, c01.y, c11.y),
+                         one(c00.z, c10.z, c01.z, c11.z), one(c00.w, c10.w, c01.w, c11.w));
+    } else {
+      const float4 c1 = *reinterpret_cast<const float4*>(pc + (cx ? ox : oy));
+      const float w0 = cx ? wx0 : wy0, w1 = cx ? wx1 : wy1;
+      corr = make_float4((w0 * c00.x + w1 * c1.x) / 4.f, (w0 * c00.y + w1 * c1.y) / 4.f,
+                         (w0 * c00.z + w1 * c1.z) / 4.f, (w0 * c00.w + w1 * c1.w) / 4.f);
+    }
+    const int64_t c = col_cell(F, i, j, k);
+    float* __restrict__ P = F.phi;
+    const float4 old = *reinterpret_cast<const float4*>(P + c);
+    const float4 v = f4add(old, corr);
+    int d0 = kNoImage, d1 = kNoImage, d2 = kNoImage;
+    if (F.img) {
+      const int* im = F.img + 3 * ((i - 2) + (int64_t)F.nx * (j - 2));
+      d0 = im[0];
+      d1 = im[1];
+      d2 = im[2];
+    }
+    const int64_t o0 = (int64_t)d0 * F.CS, o1 = (int64_t)d1 * F.CS, o2 = (int64_t)d2 * F.CS;
+    *reinterpret_cast<float4*>(P + c) = v;
+    if (d0 != kNoImage) *reinterpret_cast<float4*>(P + c + o0) = v;
+    if (d1 != kNoImage) *reinterpret_cast<float4*>(P + c + o1) = v;
+    if (d2 != kNoImage) *reinterpret_cast<float4*>(P + c + o2) = v;
+    // z ghosts: the first chunk writes the ghosts that copy row k = 2 or
+    // are zero, the last chunk those that copy row k = nz+1
+    const bool h0 = d0 != kNoImage, h1 = d1 != kNoImage, h2 = d2 != kNoImage;
+    const int64_t g1 = c - (k - 1), gZ = c + (F.nz + 2 - k);
+    if (ch == 0) {
+      if (F.z1 != 2) col_put(P, g1, F.z1 == 1 ? v.x : 0.f, o0, o1, o2, h0, h1, h2);
+      if (F.zZ != 2) col_put(P, gZ, F.zZ == 1 ? v.x : 0.f, o0, o1, o2, h0, h1, h2);
+    }
+    if (ch == nch - 1) {
+      if (F.z1 == 2) col_put(P, g1, v.w, o0, o1, o2, h0, h1, h2);
+      if (F.zZ == 2) col_put(P, gZ, v.w, o0, o1, o2, h0, h1, h2);
+    }
   }
 }
 

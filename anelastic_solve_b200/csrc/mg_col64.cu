@@ -1,15 +1,17 @@
 // mg_col64.cu -- the FP64 side of the column-layout cycle: the fine
 // residual of the defect correction written into the FP32 column layout,
-// and the correction added back into the reference layout.  Both move
-// tiles of 32 (i) x 8 (j) x 32 (k) cells through shared memory, so the
-// FP64 accesses run along i and the FP32 ones along k, each coalesced.
+// and the correction added back into the reference layout.  A thread owns
+// kColRows consecutive z-cells of one (i,j) column: its FP64 accesses run
+// along i across the warp (coalesced) and march along k with the z
+// neighbours kept in registers, and its FP32 accesses are two 16-byte
+// vectors of one column that together fill a 32-byte sector.
 // Compiled with -fmad=false: the FP64 residual is the value fine_resid
 // gives in the reference's order (the same numbers as the row-major path).
 #include "mg_col.h"
 
 namespace anel {
 
-constexpr int kTI = 32, kTJ = 8, kTK = 32;
+constexpr int kTI = 32, kTJ = 8, kColRows = 8;
 
 __device__ __forceinline__ double col_block_sum(double v, double* sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -23,36 +25,54 @@ __device__ __forceinline__ double col_block_sum(double v, double* sh) {
   return s;
 }
 
+// grid (ceil(nx/32), ceil(ny/8), nz/kColRows), block 32 x 8
 __global__ void __launch_bounds__(kTI * kTJ) k_col_resid_store(DevLevel<double> L, const double* __restrict__ phi,
                                                              const double* __restrict__ f, ColLevel E,
                                                              double* __restrict__ part) {
-  __shared__ float tile[kTJ][kTI][kTK + 1];
   __shared__ double sh[kTJ];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int i0 = 2 + blockIdx.x * kTI, j = 2 + blockIdx.y * kTJ + ty, k0 = 2 + blockIdx.z * kTK;
-  const int i = i0 + tx;
-  const bool row = j <= L.ny + 1;
+  const int i = 2 + blockIdx.x * kTI + (threadIdx.x & 31);
+  const int j = 2 + blockIdx.y * kTJ + (threadIdx.x >> 5);
+  const int k0 = 2 + blockIdx.z * kColRows;
   double rr = 0.0, ff = 0.0;
-  if (row && i <= L.nx + 1) {
-    DevLevel<double> Lp = L;
-    Lp.phi = const_cast<double*>(phi);
-    Lp.src = const_cast<double*>(f);
-    const int kn = min(kTK, L.nz + 2 - k0);
-#pragma unroll 4
-    for (int kk = 0; kk < kn; ++kk) {
-      const int k = k0 + kk;
-      const double r = fine_resid(Lp, i, j, k);
-      const double fv = f[cidx(i, j, k, L.X, L.XY)];
-      tile[ty][tx][kk] = (float)r;
-      rr += r * r;
+  if (i <= L.nx + 1 && j <= L.ny + 1) {
+    const double* cx1 = cx1p(L);
+    const double* cx2 = cx2p(L);
+    const double* cy3 = cy3p(L);
+    const double* cy4 = cy4p(L);
+    const double* cz5 = cz5p(L);
+    const double* cz6 = cz6p(L);
+    const double* dz5 = dz5p(L);
+    const double* dz6 = dz6p(L);
+    const double a1 = cx1[i - 1], a2 = cx2[i - 1], a3 = cy3[j - 1], a4 = cy4[j - 1];
+    const int64_t X = L.X, XY = L.XY;
+    int64_t c = cidx(i, j, k0, L.X, L.XY);
+    double pm = phi[c - XY], pc = phi[c];
+    float r[kColRows];
+#pragma unroll
+    for (int q = 0; q < kColRows; ++q) {
+      const int k = k0 + q;
+      const double pp = phi[c + XY];
+      // fine_resid's order: c1 W + c2 E + c3 S + c4 N + c5 B + c6 T + c7 P
+      const double diag = -(a1 + a2 + a3 + a4 + dz5[k - 1] + dz6[k - 1]);
+      double acc = a1 * phi[c - 1];
+      acc = acc + a2 * phi[c + 1];
+      acc = acc + a3 * phi[c - X];
+      acc = acc + a4 * phi[c + X];
+      acc = acc + cz5[k - 1] * pm;
+      acc = acc + cz6[k - 1] * pp;
+      acc = acc + diag * pc;
+      const double fv = f[c];
+      const double res = fv - acc;
+      r[q] = (float)res;
+      rr += res * res;
       ff += fv * fv;
+      pm = pc;
+      pc = pp;
+      c += XY;
     }
-  }
-  __syncthreads();
-  // warp ty writes the columns of its row j, lane = k offset
-  if (row && k0 + tx <= L.nz + 1) {
-    const int in = min(kTI, L.nx + 2 - i0);
-    for (int ii = 0; ii < in; ++ii) E.src[col_cell(E, i0 + ii, j, k0 + tx)] = tile[ty][ii][tx];
+    float4* o = reinterpret_cast<float4*>(E.src + col_cell(E, i, j, k0));
+#pragma unroll
+    for (int q = 0; q < kColRows / 4; ++q) o[q] = make_float4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
   }
   const double s1 = col_block_sum(rr, sh);
   const double s2 = col_block_sum(ff, sh);
@@ -65,29 +85,31 @@ __global__ void __launch_bounds__(kTI * kTJ) k_col_resid_store(DevLevel<double> 
 
 __global__ void __launch_bounds__(kTI * kTJ) k_col_add_correction(DevLevel<double> L, double* __restrict__ phi,
                                                                 ColLevel E) {
-  __shared__ float tile[kTJ][kTI][kTK + 1];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int i0 = 2 + blockIdx.x * kTI, j = 2 + blockIdx.y * kTJ + ty, k0 = 2 + blockIdx.z * kTK;
-  const bool row = j <= L.ny + 1;
-  if (row && k0 + tx <= L.nz + 1) {
-    const int in = min(kTI, L.nx + 2 - i0);
-    for (int ii = 0; ii < in; ++ii) tile[ty][ii][tx] = E.phi[col_cell(E, i0 + ii, j, k0 + tx)];
+  const int i = 2 + blockIdx.x * kTI + (threadIdx.x & 31);
+  const int j = 2 + blockIdx.y * kTJ + (threadIdx.x >> 5);
+  const int k0 = 2 + blockIdx.z * kColRows;
+  if (i > L.nx + 1 || j > L.ny + 1) return;
+  const float4* e4 = reinterpret_cast<const float4*>(E.phi + col_cell(E, i, j, k0));
+  float e[kColRows];
+#pragma unroll
+  for (int q = 0; q < kColRows / 4; ++q) {
+    const float4 v = e4[q];
+    e[4 * q] = v.x;
+    e[4 * q + 1] = v.y;
+    e[4 * q + 2] = v.z;
+    e[4 * q + 3] = v.w;
   }
-  __syncthreads();
-  const int i = i0 + tx;
-  if (row && i <= L.nx + 1) {
-    const int kn = min(kTK, L.nz + 2 - k0);
-#pragma unroll 4
-    for (int kk = 0; kk < kn; ++kk) {
-      const int64_t c = cidx(i, j, k0 + kk, L.X, L.XY);
-      phi[c] = phi[c] + (double)tile[ty][tx][kk];
-    }
-  }
+  const int64_t c = cidx(i, j, k0, L.X, L.XY), XY = L.XY;
+  double p[kColRows];
+#pragma unroll
+  for (int q = 0; q < kColRows; ++q) p[q] = phi[c + q * XY];
+#pragma unroll
+  for (int q = 0; q < kColRows; ++q) phi[c + q * XY] = p[q] + (double)e[q];
 }
 
 static dim3 col_tiles(const DevLevel<double>& L) {
   return dim3((unsigned)((L.nx + kTI - 1) / kTI), (unsigned)((L.ny + kTJ - 1) / kTJ),
-              (unsigned)((L.nz + kTK - 1) / kTK));
+              (unsigned)(L.nz / kColRows));
 }
 
 int64_t col_resid_part_doubles(const DevLevel<double>& L) {

@@ -5,6 +5,7 @@
 // sm_100a kernels of mg_device.cuh.  Built with -ffp-contract=off for the
 // host compiler so the coefficients round exactly as the reference's.
 #include "mg_solver.h"
+#include "tune.h"
 
 #include <algorithm>
 #include <cmath>
@@ -257,7 +258,48 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
   std::vector<double> rz(geo_[ngrid_].Z, 1.0);
   int st = build_coefficients(rz);
   if (st != ANEL_OK) return st;
-  return upload_coefficients();
+  st = upload_coefficients();
+  if (st != ANEL_OK) return st;
+  return col_ ? tune_col() : ANEL_OK;
+}
+
+// Autotuning of the column sweep: every variant of launch_col_sweep timed
+// on each level's own arrays (scratch at this point: the cycle overwrites
+// them) with CUDA events, one warm-up sweep pair and then kTuneReps pairs;
+// the fastest is kept per (device, rows per lane, level columns) for the
+// whole process.
+int MGSolver::tune_col() {
+  constexpr int kTuneReps = 4;
+  for (int l = 1; l <= ngrid_; ++l) {
+    char key[128];
+    std::snprintf(key, sizeof(key), "k_col_sweep dev%d M=%d lines=%dx%d", device_, colM_, geo_[l].n[0],
+                  geo_[l].n[1]);
+    int v = tune_lookup(key);
+    if (v < 0 && !tune_enabled()) v = 0;
+    if (v < 0) {
+      const ColLevel L = C32(l);
+      std::vector<double> ms(kColSweepVariants, 0.0);
+      for (int q = 0; q < kColSweepVariants; ++q) {
+        for (int c = 0; c < 2; ++c) launch_col_sweep(L, c, d_colfac_[l], colM_, q, stream_);
+        ANEL_CUDA_TRY(cudaEventRecord(ev0_, stream_));
+        for (int r = 0; r < kTuneReps; ++r)
+          for (int c = 0; c < 2; ++c) launch_col_sweep(L, c, d_colfac_[l], colM_, q, stream_);
+        ANEL_CUDA_TRY(cudaEventRecord(ev1_, stream_));
+        ANEL_CUDA_TRY(cudaEventSynchronize(ev1_));
+        float t = 0.f;
+        ANEL_CUDA_TRY(cudaEventElapsedTime(&t, ev0_, ev1_));
+        ms[q] = t / (2.0 * kTuneReps);
+      }
+      const int le = check_launch("column sweep tuning");
+      if (le != ANEL_OK) return le;
+      v = 0;
+      for (int q = 1; q < kColSweepVariants; ++q)
+        if (ms[q] < ms[v]) v = q;
+      tune_store(key, v, ms);
+    }
+    colvar_[l] = v;
+  }
+  return ANEL_OK;
 }
 
 MGSolver::~MGSolver() {
@@ -1180,7 +1222,7 @@ void MGSolver::relax_col(int l, int iters, cudaStream_t s) {
   for (int it = 0; it < iters; ++it)
     for (int color = 0; color < 2; ++color) {
       if (prof) prof_begin(s);
-      launch_col_sweep(L, color, d_colfac_[l], colM_, s);
+      launch_col_sweep(L, color, d_colfac_[l], colM_, colvar_[l], s);
       if (prof) prof_end(s);
     }
 }
@@ -1341,7 +1383,10 @@ int MGSolver::solve_device(double* d_phi, const double* d_rhs, cudaStream_t s,
   r.launches = t_launches - launches0;
   const int pe = prof_collect(&r);
   if (pe != ANEL_OK) return pe;
-  r.resid = true_resid(d_phi, d_rhs, s, nullptr);
+  // the mixed solve's last defect is the true residual of the returned phi
+  // (computed after the last correction and boundary pass); the FP64 solve
+  // stopped on relmax needs its own pass
+  if (prm_.precision != ANEL_PREC_MIXED) r.resid = true_resid(d_phi, d_rhs, s, nullptr);
   r.status = st;
   if (rep) *rep = r;
   return st;
@@ -1481,6 +1526,7 @@ int MGSolver::solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s,
   }
   rep->iter = conv ? iter : prm_.maxcy + 1;
   rep->relmax = rel;
+  rep->resid = rel;
   return conv ? ANEL_OK : ANEL_ERR_NOCONV;
 }
 

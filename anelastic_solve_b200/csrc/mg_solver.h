@@ -63,6 +63,8 @@ class MGSolver {
   bool col_ = false;
   int colM_ = 0;
   float* d_colfac_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  int colvar_[ANEL_MAX_LEVELS + 1] = {};  // sweep variant per level (tune_col)
+  int tune_col();
   ColLevel C32(int l) const;
   int64_t fp32_elems(int l) const;
   void relax_col(int l, int iters, cudaStream_t s);

@@ -43,6 +43,7 @@ struct NSDev {
   int vles, rles, sles;  // Vmodel / Rmodel / Smodel are SSM
   int ew;
   int scal1_on;
+  int unit_r;  // r and densityBG are 1 on every plane (ghosts included)
 };
 
 #define NS_IX(i, j, k) ((int64_t)((i) - 1) + (int64_t)D.X * ((j) - 1) + D.XY * ((k) - 1))

@@ -8,244 +8,256 @@ namespace anel {
 static constexpr double R12 = 1.0 / 2.0;  // ratios::r_1_2 (modules.F90:203)
 
 // --------------------------------------------------------------- RHS
-// Inside the RHS functions a field access FA(a, i+di, j+dj, k+dk) is the
-// centre offset c0_ plus a neighbour offset that folds to a constant
-// (integer index arithmetic only; the floating-point expressions are
-// unchanged).
+// The right-hand-side functions read their fields through an accessor A_:
+// FU/FV/FW/FR(i+di, j+dj, k+dk) are u, v, w, rho at a constant offset from
+// the cell, FC the scalar of rhs_scalar (rho or scal1), FN/FK the LES
+// eddy coefficients.  The floating-point expressions are the same for every
+// accessor; only where the values come from differs (global memory around
+// the cell, or the shared-memory planes of the tiled kernel).
 #undef FA
-#define FA(a, I, J, K) (a)[c0_ + ((I) - i) + (int64_t)D.X * ((J) - j) + D.XY * ((K) - k)]
+#define FU(I, J, K) A_.u((I) - i, (J) - j, (K) - k)
+#define FV(I, J, K) A_.v((I) - i, (J) - j, (K) - k)
+#define FW(I, J, K) A_.w((I) - i, (J) - j, (K) - k)
+#define FR(I, J, K) A_.r((I) - i, (J) - j, (K) - k)
+#define FC(I, J, K) (kRho ? A_.r((I) - i, (J) - j, (K) - k) : A_.g(D.s, (I) - i, (J) - j, (K) - k))
+#define FN(I, J, K) A_.g(D.nuT, (I) - i, (J) - j, (K) - k)
+#define FK(I, J, K) A_.g(kT, (I) - i, (J) - j, (K) - k)
+// r(z) and densityBG(z) at profile index q; with kU (both identically 1,
+// the Boussinesq configurations) the constant 1.0, so that products with
+// them and quotients by them fold away: x*1 and x/1 are exact, so the
+// results are the same bits as with the profile values.
+#define RZ(q) (kU ? 1.0 : D.rz[q])
+#define BG(q) (kU ? 1.0 : D.bgz[q])
+
+// Every field from global memory around the cell c0.
+struct GlobalAcc {
+  const NSDev& D;
+  int64_t c0;
+  __device__ __forceinline__ int64_t o(int di, int dj, int dk) const {
+    return c0 + di + (int64_t)D.X * dj + D.XY * dk;
+  }
+  __device__ __forceinline__ double u(int a, int b, int c) const { return D.u[o(a, b, c)]; }
+  __device__ __forceinline__ double v(int a, int b, int c) const { return D.v[o(a, b, c)]; }
+  __device__ __forceinline__ double w(int a, int b, int c) const { return D.w[o(a, b, c)]; }
+  __device__ __forceinline__ double r(int a, int b, int c) const { return D.rho[o(a, b, c)]; }
+  __device__ __forceinline__ double g(const double* p, int a, int b, int c) const { return p[o(a, b, c)]; }
+};
+
 // u1_rhs (NSsolver.F90:646-804): returns Utemp(i,j,k) before ghosting.
-__device__ __forceinline__ double rhs_u(const NSDev& D, int i, int j, int k) {
-  const int64_t c0_ = NS_IX(i, j, k);
-  const double* un = D.u;
-  const double* vn = D.v;
-  const double* wn = D.w;
+template <bool kU, class Acc>
+__device__ __forceinline__ double rhs_u(const NSDev& D, const Acc& A_, int i, int j, int k) {
   const double rRe = D.rRe;
-  const double rk = D.rz[k - 1];
+  const double rk = RZ(k - 1);
   double acc = 0.0;
   acc = acc +
-        rRe * ((FA(un, i + 1, j, k) - FA(un, i, j, k)) * MT(D.rdxc, i + 1) -
-               (FA(un, i, j, k) - FA(un, i - 1, j, k)) * MT(D.rdxc, i)) *
+        rRe * ((FU(i + 1, j, k) - FU(i, j, k)) * MT(D.rdxc, i + 1) -
+               (FU(i, j, k) - FU(i - 1, j, k)) * MT(D.rdxc, i)) *
             MT(D.rdxe, i);
   acc = acc +
-        rRe * ((FA(un, i, j + 1, k) - FA(un, i, j, k)) * MT(D.rdye, j) -
-               (FA(un, i, j, k) - FA(un, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+        rRe * ((FU(i, j + 1, k) - FU(i, j, k)) * MT(D.rdye, j) -
+               (FU(i, j, k) - FU(i, j - 1, k)) * MT(D.rdye, j - 1)) *
             MT(D.rdyc, j);
-  double ua2 = R12 * (FA(un, i + 1, j, k) + FA(un, i, j, k));
-  double ua1 = R12 * (FA(un, i, j, k) + FA(un, i - 1, j, k));
+  double ua2 = R12 * (FU(i + 1, j, k) + FU(i, j, k));
+  double ua1 = R12 * (FU(i, j, k) + FU(i - 1, j, k));
   acc = acc + (ua1 * ua1 - ua2 * ua2) * MT(D.rdxe, i);
-  ua2 = R12 * (FA(un, i, j, k + 1) + FA(un, i, j, k));
-  ua1 = R12 * (FA(un, i, j, k) + FA(un, i, j, k - 1));
-  const double ra2 = R12 * (D.rz[k] + rk);
-  const double ra1 = R12 * (rk + D.rz[k - 2]);
-  const double wa2 = R12 * (FA(wn, i + 1, j, k) + FA(wn, i, j, k));
-  const double wa1 = R12 * (FA(wn, i + 1, j, k - 1) + FA(wn, i, j, k - 1));
+  ua2 = R12 * (FU(i, j, k + 1) + FU(i, j, k));
+  ua1 = R12 * (FU(i, j, k) + FU(i, j, k - 1));
+  const double ra2 = R12 * (RZ(k) + rk);
+  const double ra1 = R12 * (rk + RZ(k - 2));
+  const double wa2 = R12 * (FW(i + 1, j, k) + FW(i, j, k));
+  const double wa1 = R12 * (FW(i + 1, j, k - 1) + FW(i, j, k - 1));
   acc = acc + (ra1 * ua1 * wa1 - ra2 * ua2 * wa2) * MT(D.rdzc, k) / rk;
-  ua2 = R12 * (FA(un, i, j + 1, k) + FA(un, i, j, k));
-  ua1 = R12 * (FA(un, i, j, k) + FA(un, i, j - 1, k));
-  const double va2 = R12 * (FA(vn, i + 1, j, k) + FA(vn, i, j, k));
-  const double va1 = R12 * (FA(vn, i + 1, j - 1, k) + FA(vn, i, j - 1, k));
+  ua2 = R12 * (FU(i, j + 1, k) + FU(i, j, k));
+  ua1 = R12 * (FU(i, j, k) + FU(i, j - 1, k));
+  const double va2 = R12 * (FV(i + 1, j, k) + FV(i, j, k));
+  const double va1 = R12 * (FV(i + 1, j - 1, k) + FV(i, j - 1, k));
   acc = acc + (ua1 * va1 - ua2 * va2) * MT(D.rdyc, j);
   if (D.vles) {  // NSsolver.F90:761-804
-    const double* nuT = D.nuT;
     acc = acc - 2.0 *
-                    (FA(nuT, i + 1, j, k) * (FA(un, i + 1, j, k) - FA(un, i, j, k)) * MT(D.rdxc, i + 1) -
-                     FA(nuT, i, j, k) * (FA(un, i, j, k) - FA(un, i - 1, j, k)) * MT(D.rdxc, i)) *
+                    (FN(i + 1, j, k) * (FU(i + 1, j, k) - FU(i, j, k)) * MT(D.rdxc, i + 1) -
+                     FN(i, j, k) * (FU(i, j, k) - FU(i - 1, j, k)) * MT(D.rdxc, i)) *
                     MT(D.rdxe, i);
-    double n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j - 1, k) +
-                        FA(nuT, i + 1, j - 1, k));
-    double n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j + 1, k) +
-                        FA(nuT, i + 1, j + 1, k));
+    double n1 = 0.25 * (FN(i, j, k) + FN(i + 1, j, k) + FN(i, j - 1, k) +
+                        FN(i + 1, j - 1, k));
+    double n2 = 0.25 * (FN(i, j, k) + FN(i + 1, j, k) + FN(i, j + 1, k) +
+                        FN(i + 1, j + 1, k));
     acc = acc - 1.0 *
-                    (n2 * (FA(un, i, j + 1, k) - FA(un, i, j, k)) * MT(D.rdye, j) -
-                     n1 * (FA(un, i, j, k) - FA(un, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+                    (n2 * (FU(i, j + 1, k) - FU(i, j, k)) * MT(D.rdye, j) -
+                     n1 * (FU(i, j, k) - FU(i, j - 1, k)) * MT(D.rdye, j - 1)) *
                     MT(D.rdyc, j);
     acc = acc - 1.0 *
-                    (n2 * (FA(vn, i + 1, j + 1, k) - FA(vn, i, j + 1, k)) * MT(D.rdxe, i) -
-                     n1 * (FA(vn, i + 1, j, k) - FA(vn, i, j, k)) * MT(D.rdxe, i)) *
+                    (n2 * (FV(i + 1, j + 1, k) - FV(i, j + 1, k)) * MT(D.rdxe, i) -
+                     n1 * (FV(i + 1, j, k) - FV(i, j, k)) * MT(D.rdxe, i)) *
                     MT(D.rdyc, j);
-    n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j, k - 1) + FA(nuT, i + 1, j, k - 1));
-    n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j, k + 1) + FA(nuT, i + 1, j, k + 1));
+    n1 = 0.25 * (FN(i, j, k) + FN(i + 1, j, k) + FN(i, j, k - 1) + FN(i + 1, j, k - 1));
+    n2 = 0.25 * (FN(i, j, k) + FN(i + 1, j, k) + FN(i, j, k + 1) + FN(i + 1, j, k + 1));
     acc = acc - 1.0 *
-                    (ra2 * n2 * (FA(wn, i + 1, j, k) - FA(wn, i, j, k)) * MT(D.rdxe, i) -
-                     ra1 * n1 * (FA(wn, i + 1, j, k - 1) - FA(wn, i, j, k - 1)) * MT(D.rdxe, i)) *
+                    (ra2 * n2 * (FW(i + 1, j, k) - FW(i, j, k)) * MT(D.rdxe, i) -
+                     ra1 * n1 * (FW(i + 1, j, k - 1) - FW(i, j, k - 1)) * MT(D.rdxe, i)) *
                     MT(D.rdzc, k) / rk;
   }
   return acc;
 }
 
 // u2_rhs (NSsolver.F90:912-1081)
-__device__ __forceinline__ double rhs_v(const NSDev& D, int i, int j, int k) {
-  const int64_t c0_ = NS_IX(i, j, k);
-  const double* un = D.u;
-  const double* vn = D.v;
-  const double* wn = D.w;
+template <bool kU, class Acc>
+__device__ __forceinline__ double rhs_v(const NSDev& D, const Acc& A_, int i, int j, int k) {
   const double rRe = D.rRe;
-  const double rk = D.rz[k - 1];
+  const double rk = RZ(k - 1);
   double acc = 0.0;
   acc = acc +
-        rRe * ((FA(vn, i + 1, j, k) - FA(vn, i, j, k)) * MT(D.rdxe, i) -
-               (FA(vn, i, j, k) - FA(vn, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+        rRe * ((FV(i + 1, j, k) - FV(i, j, k)) * MT(D.rdxe, i) -
+               (FV(i, j, k) - FV(i - 1, j, k)) * MT(D.rdxe, i - 1)) *
             MT(D.rdxc, i);
   acc = acc +
-        rRe * ((FA(vn, i, j + 1, k) - FA(vn, i, j, k)) * MT(D.rdyc, j + 1) -
-               (FA(vn, i, j, k) - FA(vn, i, j - 1, k)) * MT(D.rdyc, j)) *
+        rRe * ((FV(i, j + 1, k) - FV(i, j, k)) * MT(D.rdyc, j + 1) -
+               (FV(i, j, k) - FV(i, j - 1, k)) * MT(D.rdyc, j)) *
             MT(D.rdye, j);
-  double va1 = 0.5 * (FA(vn, i, j + 1, k) + FA(vn, i, j, k));
-  double va2 = 0.5 * (FA(vn, i, j, k) + FA(vn, i, j - 1, k));
+  double va1 = 0.5 * (FV(i, j + 1, k) + FV(i, j, k));
+  double va2 = 0.5 * (FV(i, j, k) + FV(i, j - 1, k));
   acc = acc - (va1 * va1 - va2 * va2) * MT(D.rdye, j);
-  va1 = 0.5 * (FA(vn, i + 1, j, k) + FA(vn, i, j, k));
-  va2 = 0.5 * (FA(vn, i, j, k) + FA(vn, i - 1, j, k));
-  const double ua1 = 0.5 * (FA(un, i, j + 1, k) + FA(un, i, j, k));
-  const double ua2 = 0.5 * (FA(un, i - 1, j + 1, k) + FA(un, i - 1, j, k));
+  va1 = 0.5 * (FV(i + 1, j, k) + FV(i, j, k));
+  va2 = 0.5 * (FV(i, j, k) + FV(i - 1, j, k));
+  const double ua1 = 0.5 * (FU(i, j + 1, k) + FU(i, j, k));
+  const double ua2 = 0.5 * (FU(i - 1, j + 1, k) + FU(i - 1, j, k));
   acc = acc - (ua1 * va1 - ua2 * va2) * MT(D.rdxc, i);
-  va1 = 0.5 * (FA(vn, i, j, k + 1) + FA(vn, i, j, k));
-  va2 = 0.5 * (FA(vn, i, j, k) + FA(vn, i, j, k - 1));
-  const double ra1 = 0.5 * (D.rz[k] + rk);
-  const double ra2 = 0.5 * (rk + D.rz[k - 2]);
-  const double wa1 = 0.5 * (FA(wn, i, j + 1, k) + FA(wn, i, j, k));
-  const double wa2 = 0.5 * (FA(wn, i, j + 1, k - 1) + FA(wn, i, j, k - 1));
+  va1 = 0.5 * (FV(i, j, k + 1) + FV(i, j, k));
+  va2 = 0.5 * (FV(i, j, k) + FV(i, j, k - 1));
+  const double ra1 = 0.5 * (RZ(k) + rk);
+  const double ra2 = 0.5 * (rk + RZ(k - 2));
+  const double wa1 = 0.5 * (FW(i, j + 1, k) + FW(i, j, k));
+  const double wa2 = 0.5 * (FW(i, j + 1, k - 1) + FW(i, j, k - 1));
   acc = acc - (ra1 * wa1 * va1 - ra2 * wa2 * va2) * MT(D.rdzc, k) / rk;
   if (D.vles) {  // NSsolver.F90:1038-1081
-    const double* nuT = D.nuT;
-    double n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i - 1, j, k) + FA(nuT, i, j + 1, k) +
-                        FA(nuT, i - 1, j + 1, k));
-    double n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j + 1, k) +
-                        FA(nuT, i + 1, j + 1, k));
+    double n1 = 0.25 * (FN(i, j, k) + FN(i - 1, j, k) + FN(i, j + 1, k) +
+                        FN(i - 1, j + 1, k));
+    double n2 = 0.25 * (FN(i, j, k) + FN(i + 1, j, k) + FN(i, j + 1, k) +
+                        FN(i + 1, j + 1, k));
     acc = acc - 1.0 *
-                    (n2 * (FA(vn, i + 1, j, k) - FA(vn, i, j, k)) * MT(D.rdxe, i) -
-                     n1 * (FA(vn, i, j, k) - FA(vn, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+                    (n2 * (FV(i + 1, j, k) - FV(i, j, k)) * MT(D.rdxe, i) -
+                     n1 * (FV(i, j, k) - FV(i - 1, j, k)) * MT(D.rdxe, i - 1)) *
                     MT(D.rdxc, i);
     acc = acc - 1.0 *
-                    (n2 * (FA(un, i + 1, j + 1, k) - FA(un, i + 1, j, k)) * MT(D.rdye, j) -
-                     n1 * (FA(un, i, j + 1, k) - FA(un, i, j, k)) * MT(D.rdye, j)) *
+                    (n2 * (FU(i + 1, j + 1, k) - FU(i + 1, j, k)) * MT(D.rdye, j) -
+                     n1 * (FU(i, j + 1, k) - FU(i, j, k)) * MT(D.rdye, j)) *
                     MT(D.rdxc, i);
     acc = acc - 2.0 *
-                    (FA(nuT, i, j + 1, k) * (FA(vn, i, j + 1, k) - FA(vn, i, j, k)) * MT(D.rdyc, j + 1) -
-                     FA(nuT, i, j, k) * (FA(vn, i, j, k) - FA(vn, i, j - 1, k)) * MT(D.rdyc, j)) *
+                    (FN(i, j + 1, k) * (FV(i, j + 1, k) - FV(i, j, k)) * MT(D.rdyc, j + 1) -
+                     FN(i, j, k) * (FV(i, j, k) - FV(i, j - 1, k)) * MT(D.rdyc, j)) *
                     MT(D.rdye, j);
-    n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i, j + 1, k) + FA(nuT, i, j, k - 1) + FA(nuT, i, j + 1, k - 1));
-    n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i, j + 1, k) + FA(nuT, i, j, k + 1) + FA(nuT, i, j + 1, k + 1));
+    n1 = 0.25 * (FN(i, j, k) + FN(i, j + 1, k) + FN(i, j, k - 1) + FN(i, j + 1, k - 1));
+    n2 = 0.25 * (FN(i, j, k) + FN(i, j + 1, k) + FN(i, j, k + 1) + FN(i, j + 1, k + 1));
     // the reference pairs raver2 (lower face) with nuTaver2 (upper face)
     acc = acc - 1.0 *
-                    (ra2 * n2 * (FA(wn, i, j + 1, k) - FA(wn, i, j, k)) * MT(D.rdye, j) -
-                     ra1 * n1 * (FA(wn, i, j + 1, k - 1) - FA(wn, i, j, k - 1)) * MT(D.rdye, j)) *
+                    (ra2 * n2 * (FW(i, j + 1, k) - FW(i, j, k)) * MT(D.rdye, j) -
+                     ra1 * n1 * (FW(i, j + 1, k - 1) - FW(i, j, k - 1)) * MT(D.rdye, j)) *
                     MT(D.rdzc, k) / rk;
   }
   return acc;
 }
 
 // u3_rhs (NSsolver.F90:1195-1377); rows above nz+1-EW carry no terms.
-__device__ __forceinline__ double rhs_w(const NSDev& D, int i, int j, int k) {
-  const int64_t c0_ = NS_IX(i, j, k);
+template <bool kU, class Acc>
+__device__ __forceinline__ double rhs_w(const NSDev& D, const Acc& A_, int i, int j, int k) {
   if (k > D.nz + 1 - D.ew) return 0.0;
-  const double* un = D.u;
-  const double* vn = D.v;
-  const double* wn = D.w;
   const double rRe = D.rRe;
-  const double rk = D.rz[k - 1], rkp = D.rz[k];
+  const double rk = RZ(k - 1), rkp = RZ(k);
   double acc = 0.0;
-  acc = acc + R12 * D.g * ((FA(D.rho, i, j, k + 1) - D.bgz[k]) + (FA(D.rho, i, j, k) - D.bgz[k - 1])) /
-                  (R12 * (D.bgz[k] + D.bgz[k - 1]));
+  acc = acc + R12 * D.g * ((FR(i, j, k + 1) - BG(k)) + (FR(i, j, k) - BG(k - 1))) /
+                  (R12 * (BG(k) + BG(k - 1)));
   acc = acc +
-        rRe * ((FA(wn, i + 1, j, k) - FA(wn, i, j, k)) * MT(D.rdxe, i) -
-               (FA(wn, i, j, k) - FA(wn, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+        rRe * ((FW(i + 1, j, k) - FW(i, j, k)) * MT(D.rdxe, i) -
+               (FW(i, j, k) - FW(i - 1, j, k)) * MT(D.rdxe, i - 1)) *
             MT(D.rdxc, i);
   acc = acc +
-        rRe * ((FA(wn, i, j + 1, k) - FA(wn, i, j, k)) * MT(D.rdye, j) -
-               (FA(wn, i, j, k) - FA(wn, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+        rRe * ((FW(i, j + 1, k) - FW(i, j, k)) * MT(D.rdye, j) -
+               (FW(i, j, k) - FW(i, j - 1, k)) * MT(D.rdye, j - 1)) *
             MT(D.rdyc, j);
-  double wa1 = 0.5 * (FA(wn, i, j, k + 1) + FA(wn, i, j, k));
-  double wa2 = 0.5 * (FA(wn, i, j, k) + FA(wn, i, j, k - 1));
+  double wa1 = 0.5 * (FW(i, j, k + 1) + FW(i, j, k));
+  double wa2 = 0.5 * (FW(i, j, k) + FW(i, j, k - 1));
   acc = acc - (rk * wa1 * wa1 - rkp * wa2 * wa2) * MT(D.rdze, k) / (0.5 * (rk + rkp));
-  wa1 = 0.5 * (FA(wn, i + 1, j, k) + FA(wn, i, j, k));
-  wa2 = 0.5 * (FA(wn, i, j, k) + FA(wn, i - 1, j, k));
-  const double ua1 = 0.5 * (FA(un, i, j, k + 1) + FA(un, i, j, k));
-  const double ua2 = 0.5 * (FA(un, i - 1, j, k + 1) + FA(un, i - 1, j, k));
+  wa1 = 0.5 * (FW(i + 1, j, k) + FW(i, j, k));
+  wa2 = 0.5 * (FW(i, j, k) + FW(i - 1, j, k));
+  const double ua1 = 0.5 * (FU(i, j, k + 1) + FU(i, j, k));
+  const double ua2 = 0.5 * (FU(i - 1, j, k + 1) + FU(i - 1, j, k));
   acc = acc - (ua1 * wa1 - ua2 * wa2) * MT(D.rdxc, i);
-  wa1 = 0.5 * (FA(wn, i, j + 1, k) + FA(wn, i, j, k));
-  wa2 = 0.5 * (FA(wn, i, j, k) + FA(wn, i, j - 1, k));
-  const double va1 = 0.5 * (FA(vn, i, j, k + 1) + FA(vn, i, j, k));
-  const double va2 = 0.5 * (FA(vn, i, j - 1, k + 1) + FA(vn, i, j - 1, k));
+  wa1 = 0.5 * (FW(i, j + 1, k) + FW(i, j, k));
+  wa2 = 0.5 * (FW(i, j, k) + FW(i, j - 1, k));
+  const double va1 = 0.5 * (FV(i, j, k + 1) + FV(i, j, k));
+  const double va2 = 0.5 * (FV(i, j - 1, k + 1) + FV(i, j - 1, k));
   acc = acc - (va1 * wa1 - va2 * wa2) * MT(D.rdyc, j);
   if (D.vles) {  // NSsolver.F90:1339-1377
-    const double* nuT = D.nuT;
-    double n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i - 1, j, k) + FA(nuT, i, j, k + 1) +
-                        FA(nuT, i - 1, j, k + 1));
-    double n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i + 1, j, k) + FA(nuT, i, j, k + 1) +
-                        FA(nuT, i + 1, j, k + 1));
+    double n1 = 0.25 * (FN(i, j, k) + FN(i - 1, j, k) + FN(i, j, k + 1) +
+                        FN(i - 1, j, k + 1));
+    double n2 = 0.25 * (FN(i, j, k) + FN(i + 1, j, k) + FN(i, j, k + 1) +
+                        FN(i + 1, j, k + 1));
     acc = acc - 1.0 *
-                    (n2 * (FA(wn, i + 1, j, k) - FA(wn, i, j, k)) * MT(D.rdxe, i) -
-                     n1 * (FA(wn, i, j, k) - FA(wn, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+                    (n2 * (FW(i + 1, j, k) - FW(i, j, k)) * MT(D.rdxe, i) -
+                     n1 * (FW(i, j, k) - FW(i - 1, j, k)) * MT(D.rdxe, i - 1)) *
                     MT(D.rdxc, i);
     acc = acc - 1.0 *
-                    (n2 * (FA(un, i + 1, j, k + 1) - FA(un, i + 1, j, k)) * MT(D.rdze, k) -
-                     n1 * (FA(un, i, j, k + 1) - FA(un, i, j, k)) * MT(D.rdze, k)) *
+                    (n2 * (FU(i + 1, j, k + 1) - FU(i + 1, j, k)) * MT(D.rdze, k) -
+                     n1 * (FU(i, j, k + 1) - FU(i, j, k)) * MT(D.rdze, k)) *
                     MT(D.rdxc, i);
-    n1 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i, j - 1, k) + FA(nuT, i, j, k + 1) + FA(nuT, i, j - 1, k + 1));
-    n2 = 0.25 * (FA(nuT, i, j, k) + FA(nuT, i, j + 1, k) + FA(nuT, i, j, k + 1) + FA(nuT, i, j + 1, k + 1));
+    n1 = 0.25 * (FN(i, j, k) + FN(i, j - 1, k) + FN(i, j, k + 1) + FN(i, j - 1, k + 1));
+    n2 = 0.25 * (FN(i, j, k) + FN(i, j + 1, k) + FN(i, j, k + 1) + FN(i, j + 1, k + 1));
     acc = acc - 1.0 *
-                    (n2 * (FA(wn, i, j + 1, k) - FA(wn, i, j, k)) * MT(D.rdye, j) -
-                     n1 * (FA(wn, i, j, k) - FA(wn, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+                    (n2 * (FW(i, j + 1, k) - FW(i, j, k)) * MT(D.rdye, j) -
+                     n1 * (FW(i, j, k) - FW(i, j - 1, k)) * MT(D.rdye, j - 1)) *
                     MT(D.rdyc, j);
     acc = acc - 1.0 *
-                    (n2 * (FA(vn, i, j + 1, k + 1) - FA(vn, i, j + 1, k)) * MT(D.rdze, k) -
-                     n1 * (FA(vn, i, j, k + 1) - FA(vn, i, j, k)) * MT(D.rdze, k)) *
+                    (n2 * (FV(i, j + 1, k + 1) - FV(i, j + 1, k)) * MT(D.rdze, k) -
+                     n1 * (FV(i, j, k + 1) - FV(i, j, k)) * MT(D.rdze, k)) *
                     MT(D.rdyc, j);
   }
   return acc;
 }
 
 // rho_rhs (NSsolver.F90:1720-1815) and scal1_rhs (:1890-1985)
-template <bool kRho>
-__device__ __forceinline__ double rhs_scalar(const NSDev& D, int i, int j, int k) {
-  const int64_t c0_ = NS_IX(i, j, k);
-  const double* un = D.u;
-  const double* vn = D.v;
-  const double* wn = D.w;
-  const double* c = kRho ? D.rho : D.s;
+template <bool kRho, bool kU, class Acc>
+__device__ __forceinline__ double rhs_scalar(const NSDev& D, const Acc& A_, int i, int j, int k) {
   const double Dk = kRho ? D.rRe * D.rPr : D.rRe * D.rSc;
   double acc = 0.0;
   acc = acc +
-        Dk * ((FA(c, i + 1, j, k) - FA(c, i, j, k)) * MT(D.rdxe, i) -
-              (FA(c, i, j, k) - FA(c, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+        Dk * ((FC(i + 1, j, k) - FC(i, j, k)) * MT(D.rdxe, i) -
+              (FC(i, j, k) - FC(i - 1, j, k)) * MT(D.rdxe, i - 1)) *
             MT(D.rdxc, i);
   acc = acc +
-        Dk * ((FA(c, i, j + 1, k) - FA(c, i, j, k)) * MT(D.rdye, j) -
-              (FA(c, i, j, k) - FA(c, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+        Dk * ((FC(i, j + 1, k) - FC(i, j, k)) * MT(D.rdye, j) -
+              (FC(i, j, k) - FC(i, j - 1, k)) * MT(D.rdye, j - 1)) *
             MT(D.rdyc, j);
-  double c2 = 0.5 * (FA(c, i + 1, j, k) + FA(c, i, j, k));
-  double c1 = 0.5 * (FA(c, i, j, k) + FA(c, i - 1, j, k));
-  acc = acc + (FA(un, i - 1, j, k) * c1 - FA(un, i, j, k) * c2) * MT(D.rdxc, i);
-  c2 = 0.5 * (FA(c, i, j + 1, k) + FA(c, i, j, k));
-  c1 = 0.5 * (FA(c, i, j, k) + FA(c, i, j - 1, k));
-  acc = acc + (FA(vn, i, j - 1, k) * c1 - FA(vn, i, j, k) * c2) * MT(D.rdyc, j);
-  c2 = 0.5 * (FA(c, i, j, k + 1) + FA(c, i, j, k));
-  c1 = 0.5 * (FA(c, i, j, k) + FA(c, i, j, k - 1));
+  double c2 = 0.5 * (FC(i + 1, j, k) + FC(i, j, k));
+  double c1 = 0.5 * (FC(i, j, k) + FC(i - 1, j, k));
+  acc = acc + (FU(i - 1, j, k) * c1 - FU(i, j, k) * c2) * MT(D.rdxc, i);
+  c2 = 0.5 * (FC(i, j + 1, k) + FC(i, j, k));
+  c1 = 0.5 * (FC(i, j, k) + FC(i, j - 1, k));
+  acc = acc + (FV(i, j - 1, k) * c1 - FV(i, j, k) * c2) * MT(D.rdyc, j);
+  c2 = 0.5 * (FC(i, j, k + 1) + FC(i, j, k));
+  c1 = 0.5 * (FC(i, j, k) + FC(i, j, k - 1));
   if (kRho) {
-    const double rk = D.rz[k - 1];
-    const double ra2 = 0.5 * (D.rz[k] + rk);
-    const double ra1 = 0.5 * (rk + D.rz[k - 2]);
-    acc = acc + (ra1 * FA(wn, i, j, k - 1) * c1 - ra2 * FA(wn, i, j, k) * c2) * MT(D.rdzc, k) / rk;
+    const double rk = RZ(k - 1);
+    const double ra2 = 0.5 * (RZ(k) + rk);
+    const double ra1 = 0.5 * (rk + RZ(k - 2));
+    acc = acc + (ra1 * FW(i, j, k - 1) * c1 - ra2 * FW(i, j, k) * c2) * MT(D.rdzc, k) / rk;
   } else {
-    acc = acc + (FA(wn, i, j, k - 1) * c1 - FA(wn, i, j, k) * c2) * MT(D.rdzc, k);
+    acc = acc + (FW(i, j, k - 1) * c1 - FW(i, j, k) * c2) * MT(D.rdzc, k);
   }
   if (kRho ? D.rles : D.sles) {
     const double* kT = kRho ? D.kT : D.nT;
-    double k2 = 0.5 * (FA(kT, i + 1, j, k) + FA(kT, i, j, k));
+    double k2 = 0.5 * (FK(i + 1, j, k) + FK(i, j, k));
     // scal1_rhs keeps the reference's sign slip in the lower average
-    double k1 = kRho ? 0.5 * (FA(kT, i, j, k) + FA(kT, i - 1, j, k))
-                     : 0.5 * (FA(kT, i, j, k) - FA(kT, i - 1, j, k));
+    double k1 = kRho ? 0.5 * (FK(i, j, k) + FK(i - 1, j, k))
+                     : 0.5 * (FK(i, j, k) - FK(i - 1, j, k));
     acc = acc - 1.0 *
-                    (k2 * (FA(c, i + 1, j, k) - FA(c, i, j, k)) * MT(D.rdxe, i) -
-                     k1 * (FA(c, i, j, k) - FA(c, i - 1, j, k)) * MT(D.rdxe, i - 1)) *
+                    (k2 * (FC(i + 1, j, k) - FC(i, j, k)) * MT(D.rdxe, i) -
+                     k1 * (FC(i, j, k) - FC(i - 1, j, k)) * MT(D.rdxe, i - 1)) *
                     MT(D.rdxc, i);
-    k2 = 0.5 * (FA(kT, i, j + 1, k) + FA(kT, i, j, k));
-    k1 = kRho ? 0.5 * (FA(kT, i, j, k) + FA(kT, i, j - 1, k))
-              : 0.5 * (FA(kT, i, j, k) - FA(kT, i, j - 1, k));
+    k2 = 0.5 * (FK(i, j + 1, k) + FK(i, j, k));
+    k1 = kRho ? 0.5 * (FK(i, j, k) + FK(i, j - 1, k))
+              : 0.5 * (FK(i, j, k) - FK(i, j - 1, k));
     acc = acc - 1.0 *
-                    (k2 * (FA(c, i, j + 1, k) - FA(c, i, j, k)) * MT(D.rdye, j) -
-                     k1 * (FA(c, i, j, k) - FA(c, i, j - 1, k)) * MT(D.rdye, j - 1)) *
+                    (k2 * (FC(i, j + 1, k) - FC(i, j, k)) * MT(D.rdye, j) -
+                     k1 * (FC(i, j, k) - FC(i, j - 1, k)) * MT(D.rdye, j - 1)) *
                     MT(D.rdyc, j);
   }
   return acc;
@@ -258,29 +270,102 @@ __device__ __forceinline__ double rhs_scalar(const NSDev& D, int i, int j, int k
 // q = a1*q + a2*F*dt (var_advance, NSsolver.F90:2225-2264) in one pass.
 // first = substep with a1 = 0 after zero_temps: q is known to be zero,
 // so it is not read (0*0 + x == 0 + x).
-template <bool kFirst>
-__global__ void __launch_bounds__(128, 8) k_rhs_accum(NSDev D, double a1, double a2, double dt) {
-  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = 2 + blockIdx.y;
-  const int k = 2 + blockIdx.z;
-  if (i > D.nx + 1) return;
-  const int64_t c = NS_IX(i, j, k);
-  const double fu = rhs_u(D, i, j, k);
-  const double fv = rhs_v(D, i, j, k);
-  const double fw = rhs_w(D, i, j, k);
-  const double fr = rhs_scalar<true>(D, i, j, k);
-  const double q0u = kFirst ? 0.0 : D.qu[c];
-  const double q0v = kFirst ? 0.0 : D.qv[c];
-  const double q0w = kFirst ? 0.0 : D.qw[c];
-  const double q0r = kFirst ? 0.0 : D.qr[c];
-  D.qu[c] = a1 * q0u + a2 * fu * dt;
-  D.qv[c] = a1 * q0v + a2 * fv * dt;
-  D.qw[c] = a1 * q0w + a2 * fw * dt;
-  D.qr[c] = a1 * q0r + a2 * fr * dt;
-  if (D.scal1_on) {
-    const double fs = rhs_scalar<false>(D, i, j, k);
-    const double q0s = kFirst ? 0.0 : D.qs[c];
-    D.qs[c] = a1 * q0s + a2 * fs * dt;
+//
+// Tiled: a block owns 32 (i) x 8 (j) columns and marches kRT_K planes in
+// z.  u, v, w and rho are staged in shared memory plane by plane (the
+// tile plus a one-cell halo), four planes per field in a ring: the
+// functions read planes k-1, k, k+1 while the block brings plane k+2 in
+// with asynchronous copies, so every field value is read from global memory once
+// per tile instead of once per use.  scal1 and the LES coefficients are
+// read from global memory.
+constexpr int kRT_I = 32, kRT_J = 8, kRT_K = 32;
+constexpr int kRT_W = kRT_I + 2, kRT_PL = kRT_W * (kRT_J + 2);
+constexpr int kRT_PER = (kRT_PL + kRT_I * kRT_J - 1) / (kRT_I * kRT_J);  // plane elements per thread
+
+// u, v, w, rho from the ring of shared planes (slot of plane k = k & 3),
+// the rest from global memory around c0.
+struct TileAcc {
+  const double* sm;  // [field u v w rho][slot][j + 1][i + 1]
+  int idx;           // (ty + 1) * kRT_W + tx + 1
+  int k;
+  const NSDev& D;
+  int64_t c0;
+  __device__ __forceinline__ double f(int fi, int a, int b, int c) const {
+    return sm[(fi * 4 + ((k + c) & 3)) * kRT_PL + idx + b * kRT_W + a];
+  }
+  __device__ __forceinline__ double u(int a, int b, int c) const { return f(0, a, b, c); }
+  __device__ __forceinline__ double v(int a, int b, int c) const { return f(1, a, b, c); }
+  __device__ __forceinline__ double w(int a, int b, int c) const { return f(2, a, b, c); }
+  __device__ __forceinline__ double r(int a, int b, int c) const { return f(3, a, b, c); }
+  __device__ __forceinline__ double g(const double* p, int a, int b, int c) const {
+    return p[c0 + a + (int64_t)D.X * b + D.XY * c];
+  }
+};
+
+template <bool kFirst, bool kU>
+__global__ void __launch_bounds__(kRT_I * kRT_J, 2) k_rhs_accum(NSDev D, double a1, double a2, double dt) {
+  __shared__ double sm[4 * 4 * kRT_PL];
+  const int t = threadIdx.x;
+  const int tx = t & 31, ty = t >> 5;
+  const int i0 = 2 + blockIdx.x * kRT_I, j0 = 2 + blockIdx.y * kRT_J, k0 = 2 + blockIdx.z * kRT_K;
+  const int i = i0 + tx, j = j0 + ty;
+  const int kend = min(k0 + kRT_K, D.nz + 2);  // exclusive
+  const double* fld[4] = {D.u, D.v, D.w, D.rho};
+  // plane element e of the tile (halo included) -> global offset, or -1
+  int64_t off[kRT_PER];
+#pragma unroll
+  for (int q = 0; q < kRT_PER; ++q) {
+    const int e = t + q * kRT_I * kRT_J;
+    const int gi = i0 - 1 + e % kRT_W, gj = j0 - 1 + e / kRT_W;
+    off[q] = (e < kRT_PL && gi <= D.X && gj <= D.Y) ? NS_IX(gi, gj, 1) : -1;
+  }
+  // plane p of the four fields into its ring slot, by asynchronous copies
+  // (elements outside the array are never read and are skipped)
+  auto fetch = [&](int p) {
+#pragma unroll
+    for (int q = 0; q < kRT_PER; ++q) {
+      if (off[q] < 0) continue;
+      const int e = t + q * kRT_I * kRT_J;
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const unsigned dst =
+            (unsigned)__cvta_generic_to_shared(&sm[(f * 4 + (p & 3)) * kRT_PL + e]);
+        const double* src = fld[f] + off[q] + D.XY * (p - 1);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  for (int p = k0 - 1; p <= k0 + 1; ++p) fetch(p);
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
+  const bool in = i <= D.nx + 1 && j <= D.ny + 1;
+  for (int k = k0; k < kend; ++k) {
+    const bool pre = k + 1 < kend;  // the next plane's neighbour k+2 is needed
+    if (pre) fetch(k + 2);
+    if (in) {
+      const int64_t c = NS_IX(i, j, k);
+      const TileAcc A{sm, (ty + 1) * kRT_W + tx + 1, k, D, c};
+      const double fu = rhs_u<kU>(D, A, i, j, k);
+      const double fv = rhs_v<kU>(D, A, i, j, k);
+      const double fw = rhs_w<kU>(D, A, i, j, k);
+      const double fr = rhs_scalar<true, kU>(D, A, i, j, k);
+      const double q0u = kFirst ? 0.0 : D.qu[c];
+      const double q0v = kFirst ? 0.0 : D.qv[c];
+      const double q0w = kFirst ? 0.0 : D.qw[c];
+      const double q0r = kFirst ? 0.0 : D.qr[c];
+      D.qu[c] = a1 * q0u + a2 * fu * dt;
+      D.qv[c] = a1 * q0v + a2 * fv * dt;
+      D.qw[c] = a1 * q0w + a2 * fw * dt;
+      D.qr[c] = a1 * q0r + a2 * fr * dt;
+      if (D.scal1_on) {
+        const double fs = rhs_scalar<false, kU>(D, A, i, j, k);
+        const double q0s = kFirst ? 0.0 : D.qs[c];
+        D.qs[c] = a1 * q0s + a2 * fs * dt;
+      }
+    }
+    if (pre) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
   }
 }
 
@@ -774,21 +859,33 @@ __global__ void __launch_bounds__(256) k_cfl_max(NSDev D, unsigned long long* ou
 
 // divergence (Routines.F90:121-146): max |div| (exact) and the
 // volume-weighted sums of |div| and volume (block partials, fixed order)
-__global__ void k_divergence(NSDev D, unsigned long long* mx, double* part) {
-  __shared__ double sh[2][8];
+// divergence() (Routines.F90:54-183): kDivRows consecutive z-cells per
+// thread (w of the cell below kept from the previous row), per-block sums
+// of |div|*vol and vol in a fixed order, and one atomic maximum per block
+// on the bit pattern of max |div| (exact in any order).
+constexpr int kDivRows = 8;
+__global__ void __launch_bounds__(128) k_divergence(NSDev D, unsigned long long* mx, double* part) {
+  __shared__ double sh[2][4];
+  __shared__ unsigned long long shm[4];
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
-  const int k = 2 + blockIdx.z;
+  const int k0 = 2 + blockIdx.z * kDivRows;
   double s1 = 0.0, s2 = 0.0;
   unsigned long long m = 0;
   if (i <= D.nx + 1) {
-    const double d = (FA(D.u, i, j, k) - FA(D.u, i - 1, j, k)) * MT(D.rdxc, i) +
-                     (FA(D.v, i, j, k) - FA(D.v, i, j - 1, k)) * MT(D.rdyc, j) +
-                     (FA(D.w, i, j, k) - FA(D.w, i, j, k - 1)) * MT(D.rdzc, k);
-    const double vol = 1.0 / (MT(D.rdxc, i) * MT(D.rdyc, j) * MT(D.rdzc, k));
-    s1 = fabs(d) * vol;
-    s2 = vol;
-    m = __double_as_longlong(fabs(d));
+    double wb = FA(D.w, i, j, k0 - 1);
+    for (int k = k0; k < k0 + kDivRows && k <= D.nz + 1; ++k) {
+      const double wt = FA(D.w, i, j, k);
+      const double d = (FA(D.u, i, j, k) - FA(D.u, i - 1, j, k)) * MT(D.rdxc, i) +
+                       (FA(D.v, i, j, k) - FA(D.v, i, j - 1, k)) * MT(D.rdyc, j) +
+                       (wt - wb) * MT(D.rdzc, k);
+      const double vol = 1.0 / (MT(D.rdxc, i) * MT(D.rdyc, j) * MT(D.rdzc, k));
+      s1 += fabs(d) * vol;
+      s2 += vol;
+      const unsigned long long a = __double_as_longlong(fabs(d));
+      m = a > m ? a : m;
+      wb = wt;
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
     s1 += __shfl_xor_sync(0xffffffffu, s1, o);
@@ -800,15 +897,18 @@ __global__ void k_divergence(NSDev D, unsigned long long* mx, double* part) {
   if ((threadIdx.x & 31) == 0) {
     sh[0][wid] = s1;
     sh[1][wid] = s2;
-    atomicMax(mx, m);
+    shm[wid] = m;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     double a = 0.0, b = 0.0;
+    unsigned long long mm = 0;
     for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
       a += sh[0][q];
       b += sh[1][q];
+      mm = shm[q] > mm ? shm[q] : mm;
     }
+    atomicMax(mx, mm);
     const int64_t bid = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
     part[2 * bid] = a;
     part[2 * bid + 1] = b;
@@ -831,9 +931,15 @@ static dim3 col_grid(const NSDev& D, int tx) {
 }
 
 void launch_rhs_accum(const NSDev& D, double a1, double a2, double dt, bool first, cudaStream_t s) {
-  const int tx = 128;
-  if (first) k_rhs_accum<true><<<cell_grid(D, tx), tx, 0, s>>>(D, a1, a2, dt);
-  else k_rhs_accum<false><<<cell_grid(D, tx), tx, 0, s>>>(D, a1, a2, dt);
+  const dim3 g((unsigned)((D.nx + kRT_I - 1) / kRT_I), (unsigned)((D.ny + kRT_J - 1) / kRT_J),
+               (unsigned)((D.nz + kRT_K - 1) / kRT_K));
+  const int sel = (first ? 2 : 0) + (D.unit_r ? 1 : 0);
+  switch (sel) {
+    case 0: k_rhs_accum<false, false><<<g, kRT_I * kRT_J, 0, s>>>(D, a1, a2, dt); break;
+    case 1: k_rhs_accum<false, true><<<g, kRT_I * kRT_J, 0, s>>>(D, a1, a2, dt); break;
+    case 2: k_rhs_accum<true, false><<<g, kRT_I * kRT_J, 0, s>>>(D, a1, a2, dt); break;
+    default: k_rhs_accum<true, true><<<g, kRT_I * kRT_J, 0, s>>>(D, a1, a2, dt); break;
+  }
   count_launch();
 }
 
@@ -1098,14 +1204,17 @@ void launch_cfl_max(const NSDev& D, unsigned long long* out, cudaStream_t s) {
   count_launch();
 }
 
+static dim3 divergence_grid(const NSDev& D) {
+  return dim3((unsigned)((D.nx + 127) / 128), (unsigned)D.ny, (unsigned)((D.nz + kDivRows - 1) / kDivRows));
+}
+
 int64_t divergence_blocks(const NSDev& D) {
-  const int tx = 128;
-  return (int64_t)((D.nx + tx - 1) / tx) * D.ny * D.nz;
+  const dim3 g = divergence_grid(D);
+  return (int64_t)g.x * g.y * g.z;
 }
 
 void launch_divergence(const NSDev& D, unsigned long long* mx, double* part, cudaStream_t s) {
-  const int tx = 128;
-  k_divergence<<<cell_grid(D, tx), tx, 0, s>>>(D, mx, part);
+  k_divergence<<<divergence_grid(D), 128, 0, s>>>(D, mx, part);
   count_launch();
 }
 

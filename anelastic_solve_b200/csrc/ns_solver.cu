@@ -251,6 +251,9 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
 }
 
 int NSSolver::upload_profiles() {
+  D_.unit_r = 1;
+  for (int k = 0; k < (int)rz_.size(); ++k)
+    if (!(rz_[k] == 1.0 && bgz_[k] == 1.0)) D_.unit_r = 0;
   std::vector<double> pr(rz_);
   pr.insert(pr.end(), bgz_.begin(), bgz_.end());
   ANEL_CUDA_TRY(cudaMemcpy(d_prof_, pr.data(), pr.size() * sizeof(double), cudaMemcpyHostToDevice));

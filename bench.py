@@ -362,6 +362,7 @@ def run_dns(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu and kind == "dns":
         out["oracle_leg"] = oracle_leg(s, g, lv, phys, os.cpu_count() or 1, h)
     s.close()
+    out["tuning"] = _lib.tuning_report().splitlines()
     keys = [k for k in ("ms_step", "e2e_ms") if k in out]
     out.update(zip(keys, combine_ranks(world, dev, maxes=[out[k] for k in keys])[0]))
     return out
@@ -432,6 +433,7 @@ def run_poisson(args, rank, world, local_rank):
         out["e2e_ms"] = e0.elapsed_time(e1) / ne
         out["bytes_io"] = (2 * dsrc.numel() * 8, dsrc.numel() * 8)
     s.close()
+    out["tuning"] = _lib.tuning_report().splitlines()
     keys = [k for k in ("ms_step", "e2e_ms") if k in out]
     out.update(zip(keys, combine_ranks(world, dev, maxes=[out[k] for k in keys])[0]))
     return out
@@ -891,7 +893,7 @@ def main():
                        "h2d_bytes_per_step": r["bytes_io"][0], "d2h_bytes_per_step": r["bytes_io"][1],
                        "ms_per_step": r["e2e_ms"]}
     line.update({"roofline": roof, "cpu_baseline": cpu, "clocks": r["clocks"],
-                 "gpu_launches": r["launches"]})
+                 "gpu_launches": r["launches"], "tuning": r.get("tuning")})
     print(json.dumps(line))
 
 

@@ -125,6 +125,14 @@ const char* anel_last_error(void);
 int anel_version(void);
 /* Number of this library's kernels launched since load (all contexts). */
 int64_t anel_kernel_launch_count(void);
+/* The autotuner's choices so far, one line per tuned kernel shape:
+ * "<kernel> dev<d> <shape>: variant <v> (<ms of each variant> ms)".  Kernels
+ * with several launch shapes are timed once per device and shape (when a
+ * context that uses them is created) and the fastest is kept for the
+ * process; ANEL_TUNE=0 in the environment keeps every default.  Copies at
+ * most cap-1 characters and a NUL into buf; returns the report's length.
+ * Library introspection: no counterpart in the reference. */
+int32_t anel_tuning_report(char* buf, int32_t cap);
 
 /* ---- multigrid: drop-in calls ------------------------------------------ */
 
