@@ -37,6 +37,7 @@ SOURCES = {
     "mg_col.cu": ["-fmad=true"],
     "mg_col64.cu": ["-fmad=false"],
     "tune.cu": [],
+    "mg_coarse.cu": ["-fmad=true"],
 }
 
 

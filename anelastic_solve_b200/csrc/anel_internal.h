@@ -37,8 +37,9 @@ inline void count_launch(int64_t n = 1) {
   t_launches += n;
 }
 int check_launch(const char* what);
-// Raise a kernel's dynamic shared-memory limit once per (device, kernel);
-// safe to call from several host threads.
+// Raise a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes` (set once per device and kernel, raised again only when a
+// larger launch asks); safe to call from several host threads.
 void set_smem_limit_once(const void* func, int bytes);
 // Copy nwords 8-byte words by a kernel, between device memory and pinned
 // host memory allocated with cudaHostAllocMapped (either direction).  Small

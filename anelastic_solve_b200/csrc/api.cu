@@ -24,15 +24,27 @@ void set_error(const char* fmt, ...) {
 const char* last_error() { return t_err; }
 
 void set_smem_limit_once(const void* func, int bytes) {
+  struct Entry {
+    int dev;
+    const void* func;
+    int bytes;
+  };
   static std::mutex mu;
-  static std::vector<std::pair<int, const void*>> done;
+  static std::vector<Entry> done;
   int dev = 0;
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lk(mu);
-  for (const auto& d : done)
-    if (d.first == dev && d.second == func) return;
+  for (auto& d : done)
+    if (d.dev == dev && d.func == func) {
+      // the attribute is a maximum: raise it when a larger launch comes
+      if (bytes > d.bytes) {
+        cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        d.bytes = bytes;
+      }
+      return;
+    }
   cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  done.emplace_back(dev, func);
+  done.push_back(Entry{dev, func, bytes});
 }
 
 __global__ void k_copy_words(const unsigned long long* __restrict__ src, unsigned long long* __restrict__ dst,

@@ -17,23 +17,40 @@ static void col_sweep_launch(const ColLevel& L, int color, const float* fac, cud
 }
 
 template <int M>
-static void col_sweep_variant(const ColLevel& L, int color, const float* fac, int variant, cudaStream_t s) {
+static void col_sweep_tma_launch(const ColLevel& L, int color, const float* fac, int* err, cudaStream_t s) {
+  const int64_t nlines = (int64_t)((L.nx + 1) / 2) * L.ny;
+  int64_t b = (nlines + kColTmaWarps - 1) / kColTmaWarps;
+  const int64_t cap = 148 * 2 * 4;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  const size_t sm = col_tma_smem<M>(kColTmaWarps);
+  set_smem_limit_once((const void*)k_col_sweep_tma<M>, (int)sm);
+  k_col_sweep_tma<M><<<(unsigned)b, 32 * kColTmaWarps, sm, s>>>(L, color, fac, err);
+}
+
+template <int M>
+static void col_sweep_variant(const ColLevel& L, int color, const float* fac, int variant, int* err,
+                              cudaStream_t s) {
+  // the TMA-staged kernel needs every line of a colour to exist (even nx)
+  if (variant == 3 && (L.nx % 2 != 0 || !err)) variant = 0;
   switch (variant) {
     case 1: col_sweep_launch<M, 1, 4>(L, color, fac, s); break;
     case 2: col_sweep_launch<M, 2, 2>(L, color, fac, s); break;
+    case 3: col_sweep_tma_launch<M>(L, color, fac, err, s); break;
     default: col_sweep_launch<M, 1, 3>(L, color, fac, s); break;
   }
 }
 
-void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, int variant, cudaStream_t s) {
+void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, int variant, int* err,
+                      cudaStream_t s) {
   switch (M) {
-    case 2: col_sweep_variant<2>(L, color, fac, variant, s); break;
-    case 3: col_sweep_variant<3>(L, color, fac, variant, s); break;
-    case 4: col_sweep_variant<4>(L, color, fac, variant, s); break;
-    case 6: col_sweep_variant<6>(L, color, fac, variant, s); break;
-    case 8: col_sweep_variant<8>(L, color, fac, variant, s); break;
-    case 12: col_sweep_variant<12>(L, color, fac, variant, s); break;
-    default: col_sweep_variant<16>(L, color, fac, variant, s); break;
+    case 2: col_sweep_variant<2>(L, color, fac, variant, err, s); break;
+    case 3: col_sweep_variant<3>(L, color, fac, variant, err, s); break;
+    case 4: col_sweep_variant<4>(L, color, fac, variant, err, s); break;
+    case 6: col_sweep_variant<6>(L, color, fac, variant, err, s); break;
+    case 8: col_sweep_variant<8>(L, color, fac, variant, err, s); break;
+    case 12: col_sweep_variant<12>(L, color, fac, variant, err, s); break;
+    default: col_sweep_variant<16>(L, color, fac, variant, err, s); break;
   }
   count_launch();
 }

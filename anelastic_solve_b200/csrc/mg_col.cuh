@@ -251,6 +251,195 @@ __global__ void __launch_bounds__(32 * kColWarps, MINB) k_col_sweep(ColLevel L, 
   }
 }
 
+// ------------------------------------------------ TMA-staged variant
+// The same sweep with the line's five source columns (f of the line, phi of
+// its four horizontal neighbours: 2 KB each at nz = 512) brought into
+// shared memory by 1-D bulk copies (cp.async.bulk, this GPU's own memory,
+// no multicast) that complete on an mbarrier.  Each warp double-buffers:
+// while it solves one line, the copies of its next line are in flight, so
+// the loads need no registers and no load instructions of the warp.  Every
+// wait is bounded: after kColWaitLimit polls the kernel records the timeout
+// in *err (host-mapped), waits a bounded time more for its copies and
+// returns.
+constexpr int kColTmaWarps = 4;
+constexpr int kColWaitLimit = 1 << 20;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  for (int it = 0; it < kColWaitLimit; ++it)
+    if (mbar_try(bar, parity)) return true;
+  return false;
+}
+
+template <int M>
+__host__ __device__ constexpr size_t col_tma_smem(int warps) {
+  // per warp: 2 buffers x 5 columns x N floats, the transpose row, then
+  // the factors, then two mbarriers per warp
+  return ((size_t)warps * (10 * 32 * M + 33 * M) + col_fac_floats(M)) * sizeof(float) + 16 * warps + 16;
+}
+
+template <int M>
+__global__ void __launch_bounds__(32 * kColTmaWarps, 2) k_col_sweep_tma(ColLevel L, int color,
+                                                                        const float* __restrict__ fac,
+                                                                        int* err) {
+  constexpr int NF = col_fac_floats(M);
+  constexpr int N = 32 * M;
+  extern __shared__ __align__(128) float csm[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* stage = csm + (size_t)warp * 10 * N;                    // [buf][5][N]
+  float* ys = csm + (size_t)kColTmaWarps * 10 * N + (size_t)warp * (N + M);
+  float* sf = csm + (size_t)kColTmaWarps * (10 * N + N + M);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(
+      (reinterpret_cast<uintptr_t>(sf + NF) + 15) & ~(uintptr_t)15);
+  for (int q = threadIdx.x; q < NF; q += blockDim.x) sf[q] = fac[q];
+  if (lane == 0) {
+    for (int b = 0; b < 2; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[2 * warp + b])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  const float* Fap = sf;
+  const float* Frbp = sf + (M - 1) * 32;
+  const float* Fsup = sf + 2 * (M - 1) * 32;
+  const float* FL = sf + 3 * (M - 1) * 32;
+  const float* FR = sf + 4 * (M - 1) * 32;
+  const float* Fg = sf + 5 * (M - 1) * 32;
+  const int pairs = (L.nx + 1) >> 1;
+  const int64_t nlines = (int64_t)pairs * L.ny;
+  const int64_t CS = L.CS, XC = (int64_t)L.X * L.CS;
+  const float a1 = L.a1, a2 = L.a2, a3 = L.a3, a4 = L.a4;
+  const float c5b = L.cz5[1], c6t = L.cz6[L.nz];
+  const int64_t stride = (int64_t)gridDim.x * kColTmaWarps;
+  auto line = [&](int64_t t, int& i, int& j) -> bool {
+    j = 2 + (int)(t / pairs);
+    const int i0 = 2 + 2 * (int)(t % pairs);
+    i = i0 + ((color + i0 + j) & 1);
+    return t < nlines && i <= L.nx + 1;
+  };
+  // lane 0: the five source columns of line t into buffer b
+  auto issue = [&](int64_t t, int b) {
+    int i, j;
+    if (!line(t, i, j)) return;
+    const int64_t c0 = col_cell(L, i, j, 2);
+    const unsigned bar = smem_u32(&bars[2 * warp + b]);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(5 * N * 4) : "memory");
+    const float* src[5] = {L.src + c0, L.phi + c0 - CS, L.phi + c0 + CS, L.phi + c0 - XC, L.phi + c0 + XC};
+#pragma unroll
+    for (int a = 0; a < 5; ++a)
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+              smem_u32(stage + (size_t)(b * 5 + a) * N)),
+          "l"(src[a]), "r"(N * 4), "r"(bar)
+          : "memory");
+  };
+  // (every line is valid for even nx, which the launcher requires, so the
+  // u-th line of a warp is the (u/2)-th use of buffer u%2: parity u/2 % 2)
+  int64_t t = (int64_t)blockIdx.x * kColTmaWarps + warp;
+  if (lane == 0) issue(t, 0);
+  int u = 0;
+  bool ok = true;
+  for (; t < nlines; ++u, t += stride) {
+    const int b = u & 1;
+    if (lane == 0) issue(t + stride, b ^ 1);
+    int i, j;
+    (void)line(t, i, j);
+    if (!mbar_wait(smem_u32(&bars[2 * warp + b]), (unsigned)((u >> 1) & 1))) {
+      ok = false;
+      break;
+    }
+    const int64_t c0 = col_cell(L, i, j, 2);
+    const float* sb = stage + (size_t)b * 5 * N;
+    float v[M];
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      const int r = lane + 32 * q;
+      v[q] = sb[r] - (a1 * sb[N + r] + a2 * sb[2 * N + r] + a3 * sb[3 * N + r] + a4 * sb[4 * N + r]);
+    }
+    if (lane == 0) v[0] -= c5b * L.phi[c0 - 1];
+    if (lane == 31) v[M - 1] -= c6t * L.phi[c0 + N];
+#pragma unroll
+    for (int q = 0; q < M; ++q) ys[col_pad(lane + 32 * q)] = v[q];
+    __syncwarp();
+    float y[M];
+#pragma unroll
+    for (int w = 0; w < M; ++w) y[w] = ys[col_pad(lane * M + w)];
+    __syncwarp();
+    float g = y[0];
+#pragma unroll
+    for (int w = 1; w < M - 1; ++w) {
+      g = y[w] + Fap[w * 32 + lane] * g;
+      y[w] = g;
+    }
+    float x = g * Frbp[(M - 2) * 32 + lane];
+    y[M - 2] = x;
+#pragma unroll
+    for (int w = M - 3; w >= 0; --w) {
+      x = (y[w] - Fsup[w * 32 + lane] * x) * Frbp[w * 32 + lane];
+      y[w] = x;
+    }
+    const float ynext = __shfl_down_sync(kFull, y[0], 1);
+    float h = y[M - 1] - Fg[lane] * y[M - 2] - (lane < 31 ? Fg[32 + lane] * ynext : 0.f);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const int st = 1 << q;
+      const float up = __shfl_up_sync(kFull, h, st);
+      const float dn = __shfl_down_sync(kFull, h, st);
+      h = h + Fg[(2 + q) * 32 + lane] * up + Fg[(7 + q) * 32 + lane] * dn;
+    }
+    const float xs = h * Fg[12 * 32 + lane];
+    const float xprev = __shfl_up_sync(kFull, xs, 1);
+#pragma unroll
+    for (int w = 0; w < M - 1; ++w) y[w] = y[w] + FL[w * 32 + lane] * xprev + FR[w * 32 + lane] * xs;
+    y[M - 1] = xs;
+#pragma unroll
+    for (int w = 0; w < M; ++w) ys[col_pad(lane * M + w)] = y[w];
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < M; ++q) v[q] = ys[col_pad(lane + 32 * q)];
+    int d0 = kNoImage, d1 = kNoImage, d2 = kNoImage;
+    if (L.img) {
+      const int* im = L.img + 3 * ((i - 2) + (int64_t)L.nx * (j - 2));
+      d0 = im[0];
+      d1 = im[1];
+      d2 = im[2];
+    }
+    const bool h0 = d0 != kNoImage, h1 = d1 != kNoImage, h2 = d2 != kNoImage;
+    const int64_t o0 = h0 ? (int64_t)d0 * CS : 0, o1 = h1 ? (int64_t)d1 * CS : 0, o2 = h2 ? (int64_t)d2 * CS : 0;
+    float* __restrict__ Pw = L.phi;
+#pragma unroll
+    for (int q = 0; q < M; ++q) col_put(Pw, c0 + lane + 32 * q, v[q], o0, o1, o2, h0, h1, h2);
+    const float r0 = __shfl_sync(kFull, v[0], 0);
+    const float rn = __shfl_sync(kFull, v[M - 1], 31);
+    if (lane == 0 || lane == 31) {
+      const int code = lane == 0 ? L.z1 : L.zZ;
+      const float gv = code == 0 ? 0.f : (code == 1 ? r0 : rn);
+      col_put(Pw, lane == 0 ? c0 - 1 : c0 + N, gv, o0, o1, o2, h0, h1, h2);
+    }
+    __syncwarp();  // every lane is done with buffer b before it is refilled
+  }
+  if (!ok) {
+    if (lane == 0) *reinterpret_cast<volatile int*>(err) = 1;
+    // bounded wait for this warp's copies still in flight (line t in
+    // buffer u%2, and line t+stride in the other buffer if it exists),
+    // then return
+    (void)mbar_wait(smem_u32(&bars[2 * warp + (u & 1)]), (unsigned)((u >> 1) & 1));
+    if (t + stride < nlines)
+      (void)mbar_wait(smem_u32(&bars[2 * warp + ((u + 1) & 1)]), (unsigned)(((u + 1) >> 1) & 1));
+  }
+}
+
 // Residuals f - A phi of fine cells (i,j,k..k+3) (k-2 a multiple of 4, so
 // the four cells are one aligned 16-byte vector), in fine_resid's order.
 __device__ __forceinline__ float4 col_resid4(const ColLevel& F, int i, int j, int k) {

@@ -10,10 +10,13 @@ namespace anel {
 inline bool col_rows_supported(int M) {
   return M == 2 || M == 3 || M == 4 || M == 6 || M == 8 || M == 12 || M == 16;
 }
-// variants of the sweep (k_col_sweep<M, NL, MINB>): 0 = one line per warp
-// step, 3 CTAs/SM; 1 = one line, 4 CTAs/SM; 2 = two lines, 2 CTAs/SM
-constexpr int kColSweepVariants = 3;
-void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, int variant, cudaStream_t s);
+// variants of the sweep: k_col_sweep<M, NL, MINB> with 0 = one line per
+// warp step, 3 CTAs/SM; 1 = one line, 4 CTAs/SM; 2 = two lines, 2 CTAs/SM;
+// 3 = k_col_sweep_tma (source columns staged by bulk copies; err: a
+// host-mapped int set to 1 if a copy wait ran out)
+constexpr int kColSweepVariants = 4;
+void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, int variant, int* err,
+                      cudaStream_t s);
 // coarse f from the fine residual (cdir: bit 0 x, bit 1 y coarsened); the
 // caller zeroes coarse phi first
 void launch_col_restrict(const ColLevel& F, const ColLevel& C, int cdir, cudaStream_t s);

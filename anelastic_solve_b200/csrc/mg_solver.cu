@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace anel {
@@ -21,6 +22,8 @@ int zline_cr_factors(int n, int S, const std::vector<double>& sub, const std::ve
                      const std::vector<double>& sup, std::vector<double>& out);
 int col_sweep_factors(int n, int M, const std::vector<double>& sub, const std::vector<double>& dia,
                       const std::vector<double>& sup, std::vector<float>& out);
+int col_sweep_factors_d(int n, int M, const std::vector<double>& sub, const std::vector<double>& dia,
+                        const std::vector<double>& sup, std::vector<double>& out);
 
 // ------------------------------------------------------------------ init
 MGSolver* MGSolver::create(const anel_grid_desc* g, const anel_mg_params* p, int device,
@@ -244,6 +247,9 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
   for (int l = 1; l <= ngrid_ && col_ok; ++l) col_ok = d_img32_[l] != nullptr;
   col_ = col_ok;
   if (col_) {
+    ANEL_CUDA_TRY(cudaHostAlloc(&h_err_, sizeof(int), cudaHostAllocMapped));
+    *h_err_ = 0;
+    ANEL_CUDA_TRY(cudaHostGetDevicePointer((void**)&d_err_, h_err_, 0));
     colM_ = nz_ / 32;
     for (int l = 1; l <= ngrid_; ++l)
       ANEL_CUDA_TRY(cudaMalloc(&d_colfac_[l], (size_t)col_fac_floats(colM_) * sizeof(float)));
@@ -254,6 +260,7 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
   ANEL_CUDA_TRY(cudaMalloc(&d_part_, (size_t)npart * sizeof(double)));
   ANEL_CUDA_TRY(cudaMalloc(&d_norm_, 2 * sizeof(double)));
   ANEL_CUDA_TRY(cudaHostAlloc(&h_pin_, 4 * sizeof(double), cudaHostAllocMapped));
+  choose_direct_level();
   // default density r == 1
   std::vector<double> rz(geo_[ngrid_].Z, 1.0);
   int st = build_coefficients(rz);
@@ -268,8 +275,30 @@ int MGSolver::init(const anel_grid_desc* g, const anel_mg_params* p, int device)
 // them) with CUDA events, one warm-up sweep pair and then kTuneReps pairs;
 // the fastest is kept per (device, rows per lane, level columns) for the
 // whole process.
+// A sweep that gave up on a copy wait leaves *h_err_ = 1 (after the stream
+// has been synchronised): report it once as a timeout.
+int MGSolver::take_kernel_error(const char* what) {
+  if (h_err_ && *reinterpret_cast<volatile int*>(h_err_) != 0) {
+    *reinterpret_cast<volatile int*>(h_err_) = 0;
+    set_error("%s: a bounded wait for a bulk copy ran out in the column sweep", what);
+    return ANEL_ERR_TIMEOUT;
+  }
+  return ANEL_OK;
+}
+
 int MGSolver::tune_col() {
   constexpr int kTuneReps = 4;
+  // ANEL_COL_VARIANT=v forces one variant everywhere (no timing): for tests
+  const char* force = std::getenv("ANEL_COL_VARIANT");
+  if (force && *force) {
+    const int v = std::atoi(force);
+    if (v < 0 || v >= kColSweepVariants) {
+      set_error("ANEL_COL_VARIANT=%s: variants are 0..%d", force, kColSweepVariants - 1);
+      return ANEL_ERR_ARG;
+    }
+    for (int l = 1; l <= ngrid_; ++l) colvar_[l] = v;
+    return ANEL_OK;
+  }
   for (int l = 1; l <= ngrid_; ++l) {
     char key[128];
     std::snprintf(key, sizeof(key), "k_col_sweep dev%d M=%d lines=%dx%d", device_, colM_, geo_[l].n[0],
@@ -280,10 +309,10 @@ int MGSolver::tune_col() {
       const ColLevel L = C32(l);
       std::vector<double> ms(kColSweepVariants, 0.0);
       for (int q = 0; q < kColSweepVariants; ++q) {
-        for (int c = 0; c < 2; ++c) launch_col_sweep(L, c, d_colfac_[l], colM_, q, stream_);
+        for (int c = 0; c < 2; ++c) launch_col_sweep(L, c, d_colfac_[l], colM_, q, d_err_, stream_);
         ANEL_CUDA_TRY(cudaEventRecord(ev0_, stream_));
         for (int r = 0; r < kTuneReps; ++r)
-          for (int c = 0; c < 2; ++c) launch_col_sweep(L, c, d_colfac_[l], colM_, q, stream_);
+          for (int c = 0; c < 2; ++c) launch_col_sweep(L, c, d_colfac_[l], colM_, q, d_err_, stream_);
         ANEL_CUDA_TRY(cudaEventRecord(ev1_, stream_));
         ANEL_CUDA_TRY(cudaEventSynchronize(ev1_));
         float t = 0.f;
@@ -292,6 +321,8 @@ int MGSolver::tune_col() {
       }
       const int le = check_launch("column sweep tuning");
       if (le != ANEL_OK) return le;
+      const int ke = take_kernel_error("column sweep tuning");
+      if (ke != ANEL_OK) return ke;
       v = 0;
       for (int q = 1; q < kColSweepVariants; ++q)
         if (ms[q] < ms[v]) v = q;
@@ -322,6 +353,9 @@ MGSolver::~MGSolver() {
     cudaFree(d_img32_[l]);
     cudaFree(d_colfac_[l]);
   }
+  direct_free(dir_);
+  direct_free(dirfine_);
+  if (h_err_) cudaFreeHost(h_err_);
   cudaFree(d_max_);
   cudaFree(d_part_);
   cudaFree(d_norm_);
@@ -629,8 +663,48 @@ void MGSolver::build_lj_coefficients() {
   }
 }
 
+// The coarsest level the column cycle solves directly: the finest level
+// below the fine one whose columns fit the direct solver, with x and y
+// periodic.  ANEL_DIRECT_COARSE=0 in the environment keeps the relaxation
+// down to level 1 (the reference's schedule).
+void MGSolver::choose_direct_level() {
+  dirL_ = 0;
+  if (!col_) return;
+  const char* env = std::getenv("ANEL_DIRECT_COARSE");
+  if (env && std::strcmp(env, "0") == 0) return;
+  const int* t = prm_.tbc;
+  if (!(t[4] == 0 && t[5] == 0 && t[0] == 0 && t[2] == 0)) return;
+  for (int l = ngrid_ - 1; l >= 1; --l) {
+    const int nx = geo_[l].n[0], ny = geo_[l].n[1];
+    if (nx <= kDirMaxN && ny <= kDirMaxN && nx * ny <= kDirMaxModes) {
+      dirL_ = l;
+      return;
+    }
+  }
+}
+
+int MGSolver::build_direct(int l, DirectHost& D) {
+  const LevelGeom& G = geo_[l];
+  const LevelCoef& c = coef_[l];
+  return direct_build(D, G.n[0], G.n[1], G.n[2], c.cx1[G.s[0] - 1], c.cx2[G.s[0] - 1], c.cy3[G.s[1] - 1],
+                      c.cy4[G.s[1] - 1], c.cz5.data(), c.cz6.data(), c.dz5.data(), c.dz6.data(),
+                      zcode_[l][0], zcode_[l][1]);
+}
+
 int MGSolver::build_zline_factors() {
   const bool lj = prm_.smoother == ANEL_SMOOTHER_LJ;
+  if (dirL_ > 0) {
+    // coefficients changed (density): rebuild the direct solve; a level
+    // that does not qualify keeps the relaxation
+    const int st = build_direct(dirL_, dir_);
+    if (st == ANEL_ERR_UNSUPPORTED) {
+      direct_free(dir_);
+      dirL_ = 0;
+    } else if (st != ANEL_OK) {
+      return st;
+    }
+  }
+  direct_free(dirfine_);
   for (int l = 1; l <= ngrid_; ++l) {
     const LevelGeom& G = geo_[l];
     const LevelCoef& c = lj ? ljc_[l] : coef_[l];
@@ -783,6 +857,21 @@ int zline_cr_factors(int n, int S, const std::vector<double>& sub, const std::ve
 // col_fac_floats.
 int col_sweep_factors(int n, int M, const std::vector<double>& sub, const std::vector<double>& dia,
                       const std::vector<double>& sup, std::vector<float>& out) {
+  std::vector<double> d;
+  const int st = col_sweep_factors_d(n, M, sub, dia, sup, d);
+  if (st != ANEL_OK) return st;
+  out.assign(d.begin(), d.end());
+  for (float v : out)
+    if (!std::isfinite(v)) {
+      set_error("column sweep factors are not finite in FP32");
+      return ANEL_ERR_NONFINITE;
+    }
+  return ANEL_OK;
+}
+
+// the same factors in FP64 (the coarse direct solve uses them per mode)
+int col_sweep_factors_d(int n, int M, const std::vector<double>& sub, const std::vector<double>& dia,
+                        const std::vector<double>& sup, std::vector<double>& out) {
   constexpr int P = 32;
   if (M < 2 || n != P * M) {
     set_error("column sweep needs nz = 32*M rows with M >= 2 (nz = %d)", n);
@@ -848,21 +937,21 @@ int col_sweep_factors(int n, int M, const std::vector<double>& sub, const std::v
   std::vector<double> cr;
   const int st = zline_cr_factors(P, 5, A, B, C, cr);
   if (st != ANEL_OK) return st;
-  out.assign((size_t)col_fac_floats(M), 0.0f);
+  out.assign((size_t)col_fac_floats(M), 0.0);
   size_t o = 0;
   for (const std::vector<double>* a : {&ap, &rbp, &sp, &Ls, &Rs})
-    for (double v : *a) out[o++] = (float)v;
-  for (int s = 0; s < P; ++s) out[o + s] = (float)subh[s];
-  for (int s = 0; s < P; ++s) out[o + P + s] = (float)suph[s];
+    for (double v : *a) out[o++] = v;
+  for (int s = 0; s < P; ++s) out[o + s] = subh[s];
+  for (int s = 0; s < P; ++s) out[o + P + s] = suph[s];
   for (int q = 0; q < 5; ++q)
     for (int s = 0; s < P; ++s) {
-      out[o + (2 + q) * P + s] = (float)cr[(size_t)(2 * q) * P + s];
-      out[o + (7 + q) * P + s] = (float)cr[(size_t)(2 * q + 1) * P + s];
+      out[o + (2 + q) * P + s] = cr[(size_t)(2 * q) * P + s];
+      out[o + (7 + q) * P + s] = cr[(size_t)(2 * q + 1) * P + s];
     }
-  for (int s = 0; s < P; ++s) out[o + 12 * P + s] = (float)cr[(size_t)10 * P + s];
-  for (float v : out)
+  for (int s = 0; s < P; ++s) out[o + 12 * P + s] = cr[(size_t)10 * P + s];
+  for (double v : out)
     if (!std::isfinite(v)) {
-      set_error("column sweep factors are not finite in FP32");
+      set_error("column sweep factors are not finite");
       return ANEL_ERR_NONFINITE;
     }
   return ANEL_OK;
@@ -1222,7 +1311,7 @@ void MGSolver::relax_col(int l, int iters, cudaStream_t s) {
   for (int it = 0; it < iters; ++it)
     for (int color = 0; color < 2; ++color) {
       if (prof) prof_begin(s);
-      launch_col_sweep(L, color, d_colfac_[l], colM_, colvar_[l], s);
+      launch_col_sweep(L, color, d_colfac_[l], colM_, colvar_[l], d_err_, s);
       if (prof) prof_end(s);
     }
 }
@@ -1235,15 +1324,22 @@ void MGSolver::cycle_col(cudaStream_t s) {
     cudaMemsetAsync(d_phi32_[l - 1], 0, fp32_elems(l - 1) * sizeof(float), s);
     launch_col_restrict(C32(l), C32(l - 1), coarsen_dirs(l - 1), s);
   };
+  // with a direct level L0 the levels below it are never visited: L0 is
+  // solved exactly in place of its relaxation and of the coarser cycle
+  const int L0 = dirL_ > 0 ? dirL_ : 1;
   relax_col(ng, pre[ng - 1], s);
-  down(ng);
-  for (int l = ng - 1; l >= 2; --l) {
-    relax_col(l, pre[l - 1], s);
+  for (int l = ng; l > L0; --l) {
+    if (l < ng) relax_col(l, pre[l - 1], s);
     down(l);
   }
-  relax_col(1, pre[0], s);
-  for (int l = 1; l <= ng - 1; ++l) {
-    relax_col(l, post[l - 1], s);
+  if (dirL_ > 0) {
+    launch_direct_col(dir_.f, C32(L0), s);
+  } else {
+    relax_col(1, pre[0], s);
+    relax_col(1, post[0], s);
+  }
+  for (int l = L0; l < ng; ++l) {
+    if (l > L0) relax_col(l, post[l - 1], s);
     launch_col_prolong(C32(l + 1), C32(l), coarsen_dirs(l), s);
   }
   relax_col(ng, post[ng - 1], s);
@@ -1380,6 +1476,8 @@ int MGSolver::solve_device(double* d_phi, const double* d_rhs, cudaStream_t s,
   if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
   const int le = check_launch("mg solve");
   if (le != ANEL_OK) return le;
+  const int ke = take_kernel_error("mg solve");
+  if (ke != ANEL_OK) return ke;
   r.launches = t_launches - launches0;
   const int pe = prof_collect(&r);
   if (pe != ANEL_OK) return pe;
@@ -1569,6 +1667,20 @@ int MGSolver::debug_pass(int which, double* d_phi, const double* d_src, cudaStre
     ANEL_CUDA_TRY(cudaMemcpyAsync(W.src, d_src, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
     cycle64(s);
     ANEL_CUDA_TRY(cudaMemcpyAsync(d_phi, W.phi, W.G * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  } else if (which == 3) {
+    // the FP64 direct solve applied to the fine level itself (A phi = src,
+    // gauge pinned), then the fine boundary pass: for testing the solver
+    if (!col_) {
+      set_error("debug pass 3 needs the column-layout cycle (mixed ZLINE, z not coarsened)");
+      return ANEL_ERR_UNSUPPORTED;
+    }
+    if (!dirfine_.d_buf) {
+      const int st = build_direct(ng, dirfine_);
+      if (st != ANEL_OK) return st;
+    }
+    const DevLevel<double> F = fine_view(d_phi, d_src);
+    launch_direct_row(dirfine_.f, d_src, d_phi, F.X, F.XY, s);
+    launch_bdry(F, d_phi, s);
   } else {
     set_error("unknown debug pass %d", which);
     return ANEL_ERR_ARG;

@@ -4,6 +4,7 @@
 #include <memory>
 #include <vector>
 
+#include "mg_coarse.h"
 #include "mg_col.h"
 #include "mg_launch.h"
 
@@ -64,7 +65,18 @@ class MGSolver {
   int colM_ = 0;
   float* d_colfac_[ANEL_MAX_LEVELS + 1] = {nullptr};
   int colvar_[ANEL_MAX_LEVELS + 1] = {};  // sweep variant per level (tune_col)
+  int* h_err_ = nullptr;  // host-mapped flag: a bounded copy wait of the sweep ran out
+  int* d_err_ = nullptr;  // its device address
+  int take_kernel_error(const char* what);
   int tune_col();
+  // FP64 direct solve of level dirL_ in the column cycle (0: none; the
+  // cycle then relaxes down to level 1), and of the fine level for the
+  // debug pass that checks it
+  int dirL_ = 0;
+  DirectHost dir_;
+  DirectHost dirfine_;
+  int build_direct(int l, DirectHost& D);
+  void choose_direct_level();
   ColLevel C32(int l) const;
   int64_t fp32_elems(int l) const;
   void relax_col(int l, int iters, cudaStream_t s);

@@ -345,15 +345,16 @@ __global__ void __launch_bounds__(kRT_I * kRT_J, 2) k_rhs_accum(NSDev D, double 
     if (pre) fetch(k + 2);
     if (in) {
       const int64_t c = NS_IX(i, j, k);
+      // the accumulators' loads first: their latency overlaps the RHS
+      const double q0u = kFirst ? 0.0 : D.qu[c];
+      const double q0v = kFirst ? 0.0 : D.qv[c];
+      const double q0w = kFirst ? 0.0 : D.qw[c];
+      const double q0r = kFirst ? 0.0 : D.qr[c];
       const TileAcc A{sm, (ty + 1) * kRT_W + tx + 1, k, D, c};
       const double fu = rhs_u<kU>(D, A, i, j, k);
       const double fv = rhs_v<kU>(D, A, i, j, k);
       const double fw = rhs_w<kU>(D, A, i, j, k);
       const double fr = rhs_scalar<true, kU>(D, A, i, j, k);
-      const double q0u = kFirst ? 0.0 : D.qu[c];
-      const double q0v = kFirst ? 0.0 : D.qv[c];
-      const double q0w = kFirst ? 0.0 : D.qw[c];
-      const double q0r = kFirst ? 0.0 : D.qr[c];
       D.qu[c] = a1 * q0u + a2 * fu * dt;
       D.qv[c] = a1 * q0v + a2 * fv * dt;
       D.qw[c] = a1 * q0w + a2 * fw * dt;

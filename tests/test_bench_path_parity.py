@@ -85,9 +85,10 @@ def test_mixed_zline_stepper_at_bench_settings():
     for k in ("u", "v", "w", "rho"):
         assert err[k] < 1e-8, k
     assert err["p"] < 1e-9
-    # the same algorithm in both: the cycle counts of a sub-step agree
-    # within one (the FP32 inner cycles converge a little differently)
-    assert all(abs(a - b) <= 1 for ra, rb in zip(it_g, it_o) for a, b in zip(ra, rb))
+    # the GPU cycle solves its coarse level directly (FP64) where the
+    # oracle relaxes down to level 1: never more than one cycle more per
+    # sub-step, usually fewer from a cold start
+    assert all(a <= b + 1 for ra, rb in zip(it_g, it_o) for a, b in zip(ra, rb))
 
 
 def test_mixed_zline_poisson_256_cubed():

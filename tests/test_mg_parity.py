@@ -310,3 +310,56 @@ def test_dropin_mg_solve_equals_oracle(mode):
             np.testing.assert_array_equal(phi, ref)
     finally:
         L.anel_mg_finalize()
+
+
+def test_direct_coarse_solve_matches_oracle():
+    """The FP64 direct solve the z-line cycle uses on its coarse level
+    (real Fourier modes in the periodic x and y, one tridiagonal z-system
+    per mode, the constant mode's gauge pinned), applied to a whole fine
+    level (debug pass 3): the same solution as the oracle's FP64 multigrid
+    solve to 1e-13, modulo the constant, and a true residual at FP64
+    rounding level."""
+    g = G.shear_layer_grid(32, 16, 128, stretched=True)
+    lv = (5, 4, 1)
+    rng = np.random.default_rng(71)
+    src = compatible(field(g, rng), g, abi.MODE_METRIC)
+    po = mg_params(g, levels=lv, mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE, maxcy=200,
+                   tolmax=1e-13, stop=abi.STOP_RESID)
+    ref = zeros(g)
+    o = OracleMG(g, po)
+    it_o, _ = o.solve(ref, src.copy(order="F"))
+    assert it_o <= 200
+    pm = mg_params(g, levels=lv, mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE, precision=abi.PREC_MIXED)
+    s = MGSolver(g, pm)
+    dphi = to_dev(zeros(g))
+    s.debug_pass(3, dphi, to_dev(src))
+    got = to_host(dphi)
+    from .helpers import remove_vmean
+
+    assert rel_l2(remove_vmean(got, g), remove_vmean(ref, g)) < 1e-10
+    assert o.true_resid(got, src) < 1e-12
+
+
+@pytest.mark.parametrize("n", [(64, 32, 256), (32, 16, 512)])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_column_sweep_variants(variant, n, monkeypatch):
+    """Every launch variant of the column-layout z-line sweep (the
+    autotuner's candidates, forced here through ANEL_COL_VARIANT; 3 is the
+    bulk-copy staged kernel): the mixed ZLINE solve reaches the oracle's
+    FP64 solution within 1e-9."""
+    monkeypatch.setenv("ANEL_COL_VARIANT", str(variant))
+    g = G.shear_layer_grid(*n, stretched=True)
+    lv = levels_for(g)[:2] + (1,)
+    rng = np.random.default_rng(23)
+    src = compatible(field(g, rng), g, abi.MODE_METRIC)
+    po = mg_params(g, levels=lv, mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE, maxcy=100,
+                   tolmax=1e-13, stop=abi.STOP_RESID)
+    ref = zeros(g)
+    OracleMG(g, po).solve(ref, src.copy(order="F"))
+    pm = mg_params(g, levels=lv, mode=abi.MODE_METRIC, smoother=abi.SMOOTHER_ZLINE, maxcy=60,
+                   tolmax=1e-12, stop=abi.STOP_RESID, precision=abi.PREC_MIXED)
+    s = MGSolver(g, pm)
+    dphi = to_dev(zeros(g))
+    s.solve(dphi, to_dev(src))
+    assert s.last_report.status == abi.OK and s.last_report.resid <= 1e-12
+    assert rel_l2(remove_mean(to_host(dphi)), remove_mean(ref)) < 1e-9
