@@ -117,6 +117,12 @@ int direct_build(DirectHost& D, int nx, int ny, int nz, double a1, double a2, do
   D.f.By = put(By);
   D.f.fac = put(fac);
   D.f.work = p;
+  // launch attributes set here, outside any stream capture
+  const int sm = (int)dir_smem_bytes(nx, ny);
+  set_smem_limit_once((const void*)k_dir_forward<DirColIn>, sm);
+  set_smem_limit_once((const void*)k_dir_inverse<DirColOut>, sm);
+  set_smem_limit_once((const void*)k_dir_forward<DirRowIn>, sm);
+  set_smem_limit_once((const void*)k_dir_inverse<DirRowOut>, sm);
   ANEL_CUDA_TRY(cudaGetLastError());
   return ANEL_OK;
 }

@@ -41,6 +41,18 @@ static void col_sweep_variant(const ColLevel& L, int color, const float* fac, in
   }
 }
 
+void col_sweep_prepare(int M) {
+  switch (M) {
+    case 2: set_smem_limit_once((const void*)k_col_sweep_tma<2>, (int)col_tma_smem<2>(kColTmaWarps)); break;
+    case 3: set_smem_limit_once((const void*)k_col_sweep_tma<3>, (int)col_tma_smem<3>(kColTmaWarps)); break;
+    case 4: set_smem_limit_once((const void*)k_col_sweep_tma<4>, (int)col_tma_smem<4>(kColTmaWarps)); break;
+    case 6: set_smem_limit_once((const void*)k_col_sweep_tma<6>, (int)col_tma_smem<6>(kColTmaWarps)); break;
+    case 8: set_smem_limit_once((const void*)k_col_sweep_tma<8>, (int)col_tma_smem<8>(kColTmaWarps)); break;
+    case 12: set_smem_limit_once((const void*)k_col_sweep_tma<12>, (int)col_tma_smem<12>(kColTmaWarps)); break;
+    default: set_smem_limit_once((const void*)k_col_sweep_tma<16>, (int)col_tma_smem<16>(kColTmaWarps)); break;
+  }
+}
+
 void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, int variant, int* err,
                       cudaStream_t s) {
   switch (M) {

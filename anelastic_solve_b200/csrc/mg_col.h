@@ -17,6 +17,9 @@ inline bool col_rows_supported(int M) {
 constexpr int kColSweepVariants = 4;
 void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, int variant, int* err,
                       cudaStream_t s);
+// sets the launch attributes every sweep variant for M needs (call before
+// any stream capture)
+void col_sweep_prepare(int M);
 // coarse f from the fine residual (cdir: bit 0 x, bit 1 y coarsened); the
 // caller zeroes coarse phi first
 void launch_col_restrict(const ColLevel& F, const ColLevel& C, int cdir, cudaStream_t s);

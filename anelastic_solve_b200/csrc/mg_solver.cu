@@ -24,6 +24,7 @@ int col_sweep_factors(int n, int M, const std::vector<double>& sub, const std::v
                       const std::vector<double>& sup, std::vector<float>& out);
 int col_sweep_factors_d(int n, int M, const std::vector<double>& sub, const std::vector<double>& dia,
                         const std::vector<double>& sup, std::vector<double>& out);
+static bool graph_solve_enabled();
 
 // ------------------------------------------------------------------ init
 MGSolver* MGSolver::create(const anel_grid_desc* g, const anel_mg_params* p, int device,
@@ -288,6 +289,8 @@ int MGSolver::take_kernel_error(const char* what) {
 
 int MGSolver::tune_col() {
   constexpr int kTuneReps = 4;
+  // kernel attributes of every variant are set here, outside any capture
+  col_sweep_prepare(colM_);
   // ANEL_COL_VARIANT=v forces one variant everywhere (no timing): for tests
   const char* force = std::getenv("ANEL_COL_VARIANT");
   if (force && *force) {
@@ -356,6 +359,9 @@ MGSolver::~MGSolver() {
   direct_free(dir_);
   direct_free(dirfine_);
   if (h_err_) cudaFreeHost(h_err_);
+  if (gsolve_) cudaGraphExecDestroy(gsolve_);
+  if (side_) cudaStreamDestroy(side_);
+  cudaFree(d_conv_);
   cudaFree(d_max_);
   cudaFree(d_part_);
   cudaFree(d_norm_);
@@ -1466,8 +1472,13 @@ int MGSolver::solve_device(double* d_phi, const double* d_rhs, cudaStream_t s,
   const int64_t launches0 = t_launches;
   prof_n_ = 0;
   ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
-  const int st = prm_.precision == ANEL_PREC_MIXED ? solve_mixed(d_phi, d_rhs, s, &r)
-                                                   : solve_fp64(d_phi, d_rhs, s, &r);
+  // the graph solve when it applies: column cycle, no per-sweep profiling,
+  // no per-cycle printing, a capturable stream
+  const bool graph_ok = col_ && !prof_ && !prm_.verbose && gsolve_state_ >= 0 && s != nullptr &&
+                        s != cudaStreamLegacy && s != cudaStreamPerThread && !g32_off_ && graph_solve_enabled();
+  const int st = prm_.precision != ANEL_PREC_MIXED ? solve_fp64(d_phi, d_rhs, s, &r)
+                 : graph_ok                        ? solve_mixed_graph(d_phi, d_rhs, s, &r)
+                                                   : solve_mixed(d_phi, d_rhs, s, &r);
   ANEL_CUDA_TRY(cudaEventRecord(ev1_, s));
   ANEL_CUDA_TRY(cudaEventSynchronize(ev1_));
   float ms = 0.f;
@@ -1593,6 +1604,150 @@ void MGSolver::run_cycle32(cudaStream_t s) {
   }
   cudaGraphLaunch(g32x_, s);
   count_launch(g32_launches_);
+}
+
+// ------------------------------------------- device-side convergence loop
+// ANEL_GRAPH_SOLVE=0 in the environment keeps the host-driven loop
+static bool graph_solve_enabled() {
+  const char* v = std::getenv("ANEL_GRAPH_SOLVE");
+  return !(v && std::strcmp(v, "0") == 0);
+}
+
+struct ConvState {
+  double rel;
+  int iter;
+  int conv;
+};
+
+__device__ __forceinline__ double conv_rel(const double* n) {
+  return n[1] > 0.0 ? sqrt(n[0] / n[1]) : sqrt(n[0]);
+}
+
+// the first defect: stop before any cycle if it already meets the tolerance
+__global__ void k_conv_init(const double* norm, ConvState* st, double tol, int maxcy,
+                            cudaGraphConditionalHandle h) {
+  const double rel = conv_rel(norm);
+  const int c = rel <= tol;
+  st->rel = rel;
+  st->iter = 0;
+  st->conv = c;
+  cudaGraphSetConditional(h, (!c && maxcy > 0) ? 1u : 0u);
+}
+
+// after a cycle: the loop of solve_mixed (iteration count, stop at the
+// tolerance or after maxcy cycles), decided on the device
+__global__ void k_conv_step(const double* norm, ConvState* st, double tol, int maxcy,
+                            cudaGraphConditionalHandle h) {
+  const double rel = conv_rel(norm);
+  const int it = st->iter + 1;
+  const int c = rel <= tol;
+  st->rel = rel;
+  st->iter = it;
+  st->conv = c;
+  cudaGraphSetConditional(h, (!c && it < maxcy) ? 1u : 0u);
+}
+
+int MGSolver::build_solve_graph(double* d_phi, const double* d_rhs, cudaStream_t s) {
+  if (gsolve_) {
+    cudaGraphExecDestroy(gsolve_);
+    gsolve_ = nullptr;
+  }
+  if (!side_) ANEL_CUDA_TRY(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+  if (!d_conv_) ANEL_CUDA_TRY(cudaMalloc(&d_conv_, sizeof(ConvState)));
+  const int ng = ngrid_;
+  const DevLevel<double> Fu = fine_view(d_phi, d_rhs);
+  const ColLevel Ec = C32(ng);
+  ConvState* cs = static_cast<ConvState*>(d_conv_);
+  const double tol = prm_.tolmax;
+  const int maxcy = prm_.maxcy;
+  cudaGraph_t g = nullptr;
+  bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
+  cudaGraphConditionalHandle h{};
+  if (ok) ok = cudaGraphConditionalHandleCreate(&h, g, 0, 0) == cudaSuccess;
+  // head: boundary pass, first defect, the loop's entry test
+  const int64_t l0 = t_launches;
+  if (ok) ok = cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+               cudaSuccess;
+  cudaGraphNode_t cnode = nullptr;
+  cudaGraph_t body = nullptr;
+  if (ok) {
+    launch_bdry(Fu, d_phi, s);
+    launch_col_resid_store(Fu, d_phi, d_rhs, Ec, d_part_, d_norm_, s);
+    k_conv_init<<<1, 1, 0, s>>>(d_norm_, cs, tol, maxcy, h);
+    count_launch();
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    ok = cudaStreamGetCaptureInfo(s, &cst, nullptr, nullptr, &deps, &ndeps) == cudaSuccess &&
+         cst == cudaStreamCaptureStatusActive;
+    if (ok) {
+      cudaGraphNodeParams cp{};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      ok = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp) == cudaSuccess;
+      if (ok) body = cp.conditional.phGraph_out[0];
+      if (ok) ok = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies) ==
+                   cudaSuccess;
+    }
+    cudaGraph_t gout = nullptr;
+    const bool ended = cudaStreamEndCapture(s, &gout) == cudaSuccess;
+    ok = ok && ended;
+  }
+  gsolve_head_launches_ = t_launches - l0;
+  // body: one FP32 cycle, the correction, the next defect and its test
+  const int64_t l1 = t_launches;
+  if (ok) ok = cudaStreamBeginCaptureToGraph(side_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+               cudaSuccess;
+  if (ok) {
+    cudaMemsetAsync(d_phi32_[ng], 0, fp32_elems(ng) * sizeof(float), side_);
+    cycle_col(side_);
+    launch_col_add_correction(Fu, d_phi, Ec, side_);
+    launch_bdry(Fu, d_phi, side_);
+    launch_col_resid_store(Fu, d_phi, d_rhs, Ec, d_part_, d_norm_, side_);
+    k_conv_step<<<1, 1, 0, side_>>>(d_norm_, cs, tol, maxcy, h);
+    count_launch();
+    cudaGraph_t gout = nullptr;
+    ok = cudaStreamEndCapture(side_, &gout) == cudaSuccess;
+  }
+  gsolve_body_launches_ = t_launches - l1;
+  // launches counted while capturing did not run
+  g_launches.fetch_sub(gsolve_head_launches_ + gsolve_body_launches_, std::memory_order_relaxed);
+  t_launches -= gsolve_head_launches_ + gsolve_body_launches_;
+  if (ok) ok = cudaGraphInstantiate(&gsolve_, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  if (!ok) {
+    cudaGetLastError();
+    gsolve_ = nullptr;
+    gsolve_state_ = -1;
+    return ANEL_OK;
+  }
+  gsolve_phi_ = d_phi;
+  gsolve_rhs_ = d_rhs;
+  gsolve_state_ = 1;
+  return ANEL_OK;
+}
+
+int MGSolver::solve_mixed_graph(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep) {
+  if (!gsolve_ || gsolve_phi_ != d_phi || gsolve_rhs_ != d_rhs) {
+    const int st = build_solve_graph(d_phi, d_rhs, s);
+    if (st != ANEL_OK) return st;
+    if (gsolve_state_ < 0) return solve_mixed(d_phi, d_rhs, s, rep);
+  }
+  ANEL_CUDA_TRY(cudaGraphLaunch(gsolve_, s));
+  copy_words(d_conv_, h_pin_, 2, s);  // rel, then (iter, conv)
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  const double rel = h_pin_[0];
+  int iv[2];
+  std::memcpy(iv, &h_pin_[1], sizeof(iv));
+  const int iter = iv[0];
+  const bool conv = iv[1] != 0;
+  count_launch(gsolve_head_launches_ + (int64_t)iter * gsolve_body_launches_);
+  rep->iter = conv ? iter : prm_.maxcy + 1;
+  rep->relmax = rel;
+  rep->resid = rel;
+  return conv ? ANEL_OK : ANEL_ERR_NOCONV;
 }
 
 int MGSolver::solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s,

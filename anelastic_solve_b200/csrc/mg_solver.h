@@ -83,6 +83,20 @@ class MGSolver {
   void cycle_col(cudaStream_t s);
   int solve_fp64(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
   int solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
+  // the mixed solve as one CUDA graph: the defect-correction loop is a
+  // conditional while node whose body (FP32 cycle, correction, FP64
+  // residual) ends in a kernel that tests convergence on the device, so a
+  // solve needs one host synchronisation instead of one per cycle.  Built
+  // per (phi, rhs) pair; 0 = not built, -1 = not available (host loop)
+  int solve_mixed_graph(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
+  int build_solve_graph(double* d_phi, const double* d_rhs, cudaStream_t s);
+  cudaGraphExec_t gsolve_ = nullptr;
+  const double* gsolve_phi_ = nullptr;
+  const double* gsolve_rhs_ = nullptr;
+  int gsolve_state_ = 0;
+  int64_t gsolve_head_launches_ = 0, gsolve_body_launches_ = 0;
+  cudaStream_t side_ = nullptr;   // stream the conditional body is captured on
+  void* d_conv_ = nullptr;        // device convergence state of the graph solve
   int coarsen_dirs(int lC) const;
   double true_resid(const double* d_phi, const double* d_rhs, cudaStream_t s, double* fnorm);
 

@@ -498,8 +498,11 @@ struct CNFac {
 constexpr int kCNU = 8;
 constexpr int kCNThreads = 256;
 
-template <int kVar>
-__global__ void __launch_bounds__(kCNThreads) k_cn_column(NSDev D, double* __restrict__ fld,
+// U rows per batch, TPB threads (columns) per block: the launch variants
+// the autotuner chooses from (launch_cn); the arithmetic does not depend
+// on them.
+template <int kVar, int U = kCNU, int TPB = kCNThreads>
+__global__ void __launch_bounds__(TPB) k_cn_column(NSDev D, double* __restrict__ fld,
                                                           const double* __restrict__ q, CNFac F,
                                                           double a3, double rkdt, ZRule R) {
   extern __shared__ double cn_sm[];
@@ -537,17 +540,17 @@ __global__ void __launch_bounds__(kCNThreads) k_cn_column(NSDev D, double* __res
   double uk = fld[base + XY];  // u_old(k)
   double g = s_rb[0];          // row 1 is a wall row
   fld[base] = g;
-  for (int kb = 2; kb <= n; kb += kCNU) {
-    double up[kCNU], qv[kCNU];
+  for (int kb = 2; kb <= n; kb += U) {
+    double up[U], qv[U];
 #pragma unroll
-    for (int u = 0; u < kCNU; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int k = kb + u;
       const int64_t o = base + (int64_t)(k - 1) * XY;
       up[u] = (k < n) ? fld[o + XY] : 0.0;  // u_old(k+1)
       qv[u] = (k <= n) ? q[o] : 0.0;
     }
 #pragma unroll
-    for (int u = 0; u < kCNU; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int k = kb + u;
       if (k <= n) {
         double rhs;
@@ -576,15 +579,15 @@ __global__ void __launch_bounds__(kCNThreads) k_cn_column(NSDev D, double* __res
   // back substitution: G(n) = G(n)/bp(n); G(k) = (G(k) - c(k) G(k+1))/bp(k)
   double gn = g / s_bp[n - 1];
   fld[base + (int64_t)(n - 1) * XY] = gn;
-  for (int kb = n - 1; kb >= 1; kb -= kCNU) {
-    double gv[kCNU];
+  for (int kb = n - 1; kb >= 1; kb -= U) {
+    double gv[U];
 #pragma unroll
-    for (int u = 0; u < kCNU; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int k = kb - u;
       gv[u] = (k >= 1) ? fld[base + (int64_t)(k - 1) * XY] : 0.0;
     }
 #pragma unroll
-    for (int u = 0; u < kCNU; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int k = kb - u;
       if (k >= 1) {
         gn = (gv[u] - s_c[k - 1] * gn) / s_bp[k - 1];
@@ -944,15 +947,30 @@ void launch_rhs_accum(const NSDev& D, double a1, double a2, double dt, bool firs
   count_launch();
 }
 
-void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
-               double rkdt, const ZRule& R, cudaStream_t s) {
-  const int tx = kCNThreads;
-  CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc, F.sub, F.diag};
+template <int kVar, int U, int TPB>
+static void cn_launch(const NSDev& D, double* fld, const double* q, const CNFac& f, double a3, double rkdt,
+                      const ZRule& R, cudaStream_t s) {
   const size_t sm = 9 * (size_t)(D.nz + 3) * sizeof(double);
-  set_smem_limit_once((const void*)k_cn_column<1>, 200 * 1024);
-  set_smem_limit_once((const void*)k_cn_column<3>, 200 * 1024);
-  if (var == 3) k_cn_column<3><<<col_grid(D, tx), tx, sm, s>>>(D, fld, q, f, a3, rkdt, R);
-  else k_cn_column<1><<<col_grid(D, tx), tx, sm, s>>>(D, fld, q, f, a3, rkdt, R);
+  set_smem_limit_once((const void*)k_cn_column<kVar, U, TPB>, 200 * 1024);
+  k_cn_column<kVar, U, TPB><<<col_grid(D, TPB), TPB, sm, s>>>(D, fld, q, f, a3, rkdt, R);
+}
+
+template <int kVar>
+static void cn_variant(const NSDev& D, double* fld, const double* q, const CNFac& f, double a3, double rkdt,
+                       const ZRule& R, int variant, cudaStream_t s) {
+  switch (variant) {
+    case 1: cn_launch<kVar, 16, 128>(D, fld, q, f, a3, rkdt, R, s); break;
+    case 2: cn_launch<kVar, 16, 256>(D, fld, q, f, a3, rkdt, R, s); break;
+    case 3: cn_launch<kVar, 32, 128>(D, fld, q, f, a3, rkdt, R, s); break;
+    default: cn_launch<kVar, kCNU, kCNThreads>(D, fld, q, f, a3, rkdt, R, s); break;
+  }
+}
+
+void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
+               double rkdt, const ZRule& R, int variant, cudaStream_t s) {
+  CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc, F.sub, F.diag};
+  if (var == 3) cn_variant<3>(D, fld, q, f, a3, rkdt, R, variant, s);
+  else cn_variant<1>(D, fld, q, f, a3, rkdt, R, variant, s);
   count_launch();
   launch_images(D, fld, nullptr, nullptr, s);
 }

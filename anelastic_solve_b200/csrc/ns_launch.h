@@ -16,8 +16,12 @@ struct CNFacHost {
 };
 
 void launch_rhs_accum(const NSDev& D, double a1, double a2, double dt, bool first, cudaStream_t s);
+// variant: rows per load batch and columns per block of the column solve
+// (0: 8 rows, 256; 1: 16, 128; 2: 16, 256; 3: 32, 128), chosen by the
+// autotuner; every variant computes the same bits
+constexpr int kCNVariants = 4;
 void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
-               double rkdt, const ZRule& R, cudaStream_t s);
+               double rkdt, const ZRule& R, int variant, cudaStream_t s);
 // var_advance_CN_PL with the eddy terms (Vmodel = SSM): per-column
 // elimination; b, c: G-sized scratch for the eliminated diagonal and the
 // super-diagonal.  kT = nuT (u, v, w), kappaT (rho), nappaT (scal1).

@@ -4,8 +4,10 @@
 // Host code is compiled with -ffp-contract=off so the factors round as
 // the reference's expressions.
 #include "ns_solver.h"
+#include "tune.h"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace anel {
@@ -247,7 +249,61 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
     std::vector<double> one(G_, 1.0);
     ANEL_CUDA_TRY(cudaMemcpy(d_fields_[q], one.data(), G_ * sizeof(double), cudaMemcpyHostToDevice));
   }
-  return upload_profiles();
+  const int ps = upload_profiles();
+  if (ps != ANEL_OK) return ps;
+  return tune_cn();
+}
+
+// Autotuning of the DNS column solve: every launch variant of launch_cn
+// timed with CUDA events on this context's own u and q (all zero at this
+// point; the factors of a placeholder rkdt are dropped afterwards), the
+// fastest kept per (device, grid) for the process.  The variants compute
+// the same bits.
+int NSSolver::tune_cn() {
+  // ANEL_CN_VARIANT=v forces one variant (no timing): for tests
+  const char* force = std::getenv("ANEL_CN_VARIANT");
+  if (force && *force) {
+    const int v = std::atoi(force);
+    if (v < 0 || v >= kCNVariants) {
+      set_error("ANEL_CN_VARIANT=%s: variants are 0..%d", force, kCNVariants - 1);
+      return ANEL_ERR_ARG;
+    }
+    cnvar_ = v;
+    return ANEL_OK;
+  }
+  char key[128];
+  std::snprintf(key, sizeof(key), "k_cn_column dev%d %dx%dx%d", device_, nx_, ny_, nz_);
+  int v = tune_lookup(key);
+  if (v < 0 && !tune_enabled()) v = 0;
+  if (v < 0) {
+    constexpr int kReps = 3;
+    const int st = cn_factors(0, 1e-3, stream_);
+    if (st != ANEL_OK) return st;
+    const ZRule R = zrule(NV_U);
+    std::vector<double> ms(kCNVariants, 0.0);
+    for (int q = 0; q < kCNVariants; ++q) {
+      launch_cn(D_, 1, D_.u, D_.qu, fac(0, 0), 1.0 / 3.0, 1e-3, R, q, stream_);
+      ANEL_CUDA_TRY(cudaEventRecord(ev0_, stream_));
+      for (int r = 0; r < kReps; ++r) launch_cn(D_, 1, D_.u, D_.qu, fac(0, 0), 1.0 / 3.0, 1e-3, R, q, stream_);
+      ANEL_CUDA_TRY(cudaEventRecord(ev1_, stream_));
+      ANEL_CUDA_TRY(cudaEventSynchronize(ev1_));
+      float t = 0.f;
+      ANEL_CUDA_TRY(cudaEventElapsedTime(&t, ev0_, ev1_));
+      ms[q] = t / kReps;
+    }
+    const int le = check_launch("column solve tuning");
+    if (le != ANEL_OK) return le;
+    v = 0;
+    for (int q = 1; q < kCNVariants; ++q)
+      if (ms[q] < ms[v]) v = q;
+    tune_store(key, v, ms);
+    // back to the state of a fresh context
+    ANEL_CUDA_TRY(cudaMemsetAsync(D_.u, 0, G_ * sizeof(double), stream_));
+    ANEL_CUDA_TRY(cudaStreamSynchronize(stream_));
+    cn_rkdt_[0] = -1.0;
+  }
+  cnvar_ = v;
+  return ANEL_OK;
 }
 
 int NSSolver::upload_profiles() {
@@ -482,7 +538,7 @@ int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, 
   // terms (the LES block is gated on Vmodel, NSsolver.F90:3160-3190)
   auto cn = [&](int var, double* f, const double* q, int vi, const ZRule& R, const double* kT) {
     if (D_.vles) launch_cn_les(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, kT, d_cnb_, d_cnc_, s);
-    else launch_cn(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, s);
+    else launch_cn(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, cnvar_, s);
   };
   cn(1, D_.u, D_.qu, 0, ru, D_.nuT);
   cn(2, D_.v, D_.qv, 1, rv, D_.nuT);

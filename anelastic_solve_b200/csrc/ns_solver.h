@@ -139,6 +139,8 @@ class NSSolver {
   double* d_cn_ = nullptr;          // CN factors: 3 slots x 5 vars x 9 arrays x (nz+2)
   double* h_cn_ = nullptr;          // pinned staging of the same
   double cn_rkdt_[3] = {-1, -1, -1};
+  int cnvar_ = 0;  // launch variant of the DNS column solve (tune_cn)
+  int tune_cn();
   int cn_next_ = 0;
   unsigned long long* d_red_ = nullptr;
   double* d_part_ = nullptr;

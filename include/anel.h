@@ -181,7 +181,12 @@ int anel_mg_ctx_levels(const anel_mg_ctx* ctx, int32_t* out, int32_t cap);
  * of single kernels.  which: 0 = one RB-GS iteration (both colours + the
  * boundary pass after each, mg_relax.F90:146-172), 1 = boundary pass only
  * (mg_bdry.F90), 2 = one V-cycle with phif as initial guess
- * (mg_cycle.F90). */
+ * (mg_cycle.F90), 3 = the FP64 direct solve that the mixed z-line cycle
+ * uses on its coarse level, applied to the fine level itself (A phi = f
+ * with the gauge pinned, then the boundary pass; needs a context of the
+ * column-layout cycle and a fine level of at most 64 x 64 columns and 512
+ * of them in all: ANEL_ERR_UNSUPPORTED otherwise; no reference
+ * counterpart). */
 int anel_mg_ctx_debug_pass(anel_mg_ctx* ctx, int32_t which, double* d_phi,
                            const double* d_src, void* stream);
 

@@ -300,3 +300,19 @@ def test_gravity_ramp_steps_bitwise():
     s2.set_fields({k: start[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
     s2.step(6)
     assert not np.array_equal(s2.get_fields(("w",))["w"], got["w"])
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_cn_launch_variants_bitwise(variant, monkeypatch):
+    """Every launch variant of the DNS Crank-Nicolson column solve (rows per
+    load batch, columns per block: the autotuner's candidates, forced here
+    through ANEL_CN_VARIANT) gives the oracle's fields bit for bit over two
+    steps."""
+    monkeypatch.setenv("ANEL_CN_VARIANT", str(variant))
+    g_, o, s, f, start = setup_case()
+    for _ in range(2):
+        o.step()
+        s.step(1)
+    got = s.get_fields(CMP)
+    for name in CMP:
+        np.testing.assert_array_equal(got[name], f[name], err_msg=name)
