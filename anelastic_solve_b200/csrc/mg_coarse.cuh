@@ -105,14 +105,16 @@ __global__ void __launch_bounds__(256) k_dir_forward(DirectFac F, In in) {
   double* by = bx + nx * nx;
   double* P = by + ny * ny;
   double* T = P + nx * ny;
-  for (int q = threadIdx.x; q < nx * nx; q += blockDim.x) bx[q] = F.Bx[q];
+  // Bx transposed (bx[i*nx + p]): the lanes of a warp take consecutive p
+  // below and read consecutive words instead of one bank nx words apart
+  for (int q = threadIdx.x; q < nx * nx; q += blockDim.x) bx[(q % nx) * nx + q / nx] = F.Bx[q];
   for (int q = threadIdx.x; q < ny * ny; q += blockDim.x) by[q] = F.By[q];
   for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) P[q] = in.get(q % nx, q / nx, r);
   __syncthreads();
   for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) {  // T(p, j)
     const int p = q % nx, j = q / nx;
     double s = 0.0;
-    for (int i = 0; i < nx; ++i) s += bx[p * nx + i] * P[i + nx * j];
+    for (int i = 0; i < nx; ++i) s += bx[i * nx + p] * P[i + nx * j];
     T[q] = s;
   }
   __syncthreads();

@@ -28,6 +28,29 @@ static void col_sweep_tma_launch(const ColLevel& L, int color, const float* fac,
   k_col_sweep_tma<M><<<(unsigned)b, 32 * kColTmaWarps, sm, s>>>(L, color, fac, err);
 }
 
+// resident blocks per SM of k_col_sweep_rf<M> (set by col_sweep_prepare,
+// outside any capture)
+static int g_rf_occ[17];
+
+template <int M>
+static void col_sweep_rf_occupancy() {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_col_sweep_rf<M>, 32 * kColWarps, 0) != cudaSuccess ||
+      occ < 1)
+    occ = 1;
+  g_rf_occ[M] = occ;
+}
+
+template <int M>
+static void col_sweep_rf_launch(const ColLevel& L, int color, const float* fac, cudaStream_t s) {
+  const int64_t nlines = (int64_t)((L.nx + 1) / 2) * L.ny;
+  int64_t b = (nlines + kColWarps - 1) / kColWarps;
+  const int64_t cap = 148 * (int64_t)(g_rf_occ[M] > 0 ? g_rf_occ[M] : 1);
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  k_col_sweep_rf<M><<<(unsigned)b, 32 * kColWarps, 0, s>>>(L, color, fac);
+}
+
 template <int M>
 static void col_sweep_variant(const ColLevel& L, int color, const float* fac, int variant, int* err,
                               cudaStream_t s) {
@@ -37,11 +60,21 @@ static void col_sweep_variant(const ColLevel& L, int color, const float* fac, in
     case 1: col_sweep_launch<M, 1, 4>(L, color, fac, s); break;
     case 2: col_sweep_launch<M, 2, 2>(L, color, fac, s); break;
     case 3: col_sweep_tma_launch<M>(L, color, fac, err, s); break;
+    case 4: col_sweep_rf_launch<M>(L, color, fac, s); break;
     default: col_sweep_launch<M, 1, 3>(L, color, fac, s); break;
   }
 }
 
 void col_sweep_prepare(int M) {
+  switch (M) {
+    case 2: col_sweep_rf_occupancy<2>(); break;
+    case 3: col_sweep_rf_occupancy<3>(); break;
+    case 4: col_sweep_rf_occupancy<4>(); break;
+    case 6: col_sweep_rf_occupancy<6>(); break;
+    case 8: col_sweep_rf_occupancy<8>(); break;
+    case 12: col_sweep_rf_occupancy<12>(); break;
+    default: col_sweep_rf_occupancy<16>(); break;
+  }
   switch (M) {
     case 2: set_smem_limit_once((const void*)k_col_sweep_tma<2>, (int)col_tma_smem<2>(kColTmaWarps)); break;
     case 3: set_smem_limit_once((const void*)k_col_sweep_tma<3>, (int)col_tma_smem<3>(kColTmaWarps)); break;

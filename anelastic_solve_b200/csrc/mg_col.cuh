@@ -251,6 +251,143 @@ __global__ void __launch_bounds__(32 * kColWarps, MINB) k_col_sweep(ColLevel L, 
   }
 }
 
+// ------------------------------------------- register-factor variant
+// The same sweep with the line-independent factors held in registers for
+// the life of the warp (5(M-1)+13 per lane: 86 at M = 16) instead of being
+// read from shared memory for every line, which takes about a third of the
+// L1/shared-memory wavefronts of a line away.  One block of kColWarps warps
+// per SM, persistent: each warp walks its lines with a grid stride and,
+// before solving one, asks L2 for the five source columns of the next
+// (prefetch.global.L2), so their loads are L2 hits when it gets there.
+template <int M>
+__global__ void __launch_bounds__(32 * kColWarps, 1) k_col_sweep_rf(ColLevel L, int color,
+                                                                   const float* __restrict__ fac) {
+  constexpr int N = 32 * M;
+  constexpr int W = M > 1 ? M - 1 : 1;
+  __shared__ float sy[kColWarps][N + M];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float Fap[W], Frbp[W], Fsup[W], FL[W], FR[W];
+#pragma unroll
+  for (int w = 0; w < M - 1; ++w) {
+    Fap[w] = fac[w * 32 + lane];
+    Frbp[w] = fac[((M - 1) + w) * 32 + lane];
+    Fsup[w] = fac[(2 * (M - 1) + w) * 32 + lane];
+    FL[w] = fac[(3 * (M - 1) + w) * 32 + lane];
+    FR[w] = fac[(4 * (M - 1) + w) * 32 + lane];
+  }
+  const float* Fg = fac + 5 * (M - 1) * 32;
+  const float sub_h = Fg[lane], sup_h = Fg[32 + lane], rb = Fg[12 * 32 + lane];
+  float al[5], ga[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    al[q] = Fg[(2 + q) * 32 + lane];
+    ga[q] = Fg[(7 + q) * 32 + lane];
+  }
+  const int pairs = (L.nx + 1) >> 1;
+  const int64_t nlines = (int64_t)pairs * L.ny;
+  const int64_t CS = L.CS, XC = (int64_t)L.X * L.CS;
+  const float a1 = L.a1, a2 = L.a2, a3 = L.a3, a4 = L.a4;
+  const float c5b = L.cz5[1], c6t = L.cz6[L.nz];
+  const int64_t stride = (int64_t)gridDim.x * kColWarps;
+  auto line = [&](int64_t t, int& i, int& j) -> bool {
+    j = 2 + (int)(t / pairs);
+    const int i0 = 2 + 2 * (int)(t % pairs);
+    i = i0 + ((color + i0 + j) & 1);
+    return t < nlines && i <= L.nx + 1;
+  };
+  float* ys = sy[warp];
+  for (int64_t t = (int64_t)blockIdx.x * kColWarps + warp; t < nlines; t += stride) {
+    int i, j;
+    const bool on = line(t, i, j);
+    {
+      int in, jn;
+      if (line(t + stride, in, jn)) {
+        const int64_t cn = col_cell(L, in, jn, 2);
+        // the 5 x M 128-byte lines of the next line's source columns
+        for (int q = lane; q < 5 * M; q += 32) {
+          const int a = q / M, r = (q - a * M) * 32;
+          const float* base = a == 0 ? L.src + cn
+                                     : L.phi + cn + (a == 1 ? -CS : a == 2 ? CS : a == 3 ? -XC : XC);
+          asm volatile("prefetch.global.L2 [%0];\n" ::"l"(base + r));
+        }
+      }
+    }
+    if (!on) continue;  // uniform across the warp
+    const int64_t c0 = col_cell(L, i, j, 2);
+    const float* __restrict__ P = L.phi;
+    const float* __restrict__ S = L.src;
+    float v[M];
+#pragma unroll
+    for (int q = 0; q < M; ++q) {
+      const int64_t c = c0 + lane + 32 * q;
+      v[q] = S[c] - (a1 * P[c - CS] + a2 * P[c + CS] + a3 * P[c - XC] + a4 * P[c + XC]);
+    }
+    if (lane == 0) v[0] -= c5b * P[c0 - 1];
+    if (lane == 31) v[M - 1] -= c6t * P[c0 + N];
+#pragma unroll
+    for (int q = 0; q < M; ++q) ys[col_pad(lane + 32 * q)] = v[q];
+    __syncwarp();
+    float y[M];
+#pragma unroll
+    for (int w = 0; w < M; ++w) y[w] = ys[col_pad(lane * M + w)];
+    __syncwarp();
+    float g = y[0];
+#pragma unroll
+    for (int w = 1; w < M - 1; ++w) {
+      g = y[w] + Fap[w] * g;
+      y[w] = g;
+    }
+    if (M > 1) {
+      float x = g * Frbp[W - 1];
+      y[W - 1] = x;
+#pragma unroll
+      for (int w = M - 3; w >= 0; --w) {
+        x = (y[w] - Fsup[w] * x) * Frbp[w];
+        y[w] = x;
+      }
+    }
+    const float ynext = __shfl_down_sync(kFull, y[0], 1);
+    float h = y[M - 1] - sub_h * (M > 1 ? y[W - 1] : 0.f) - (lane < 31 ? sup_h * ynext : 0.f);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const int st = 1 << q;
+      const float up = __shfl_up_sync(kFull, h, st);
+      const float dn = __shfl_down_sync(kFull, h, st);
+      h = h + al[q] * up + ga[q] * dn;
+    }
+    const float xs = h * rb;
+    const float xprev = __shfl_up_sync(kFull, xs, 1);
+#pragma unroll
+    for (int w = 0; w < M - 1; ++w) y[w] = y[w] + FL[w] * xprev + FR[w] * xs;
+    y[M - 1] = xs;
+#pragma unroll
+    for (int w = 0; w < M; ++w) ys[col_pad(lane * M + w)] = y[w];
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < M; ++q) v[q] = ys[col_pad(lane + 32 * q)];
+    int d0 = kNoImage, d1 = kNoImage, d2 = kNoImage;
+    if (L.img) {
+      const int* im = L.img + 3 * ((i - 2) + (int64_t)L.nx * (j - 2));
+      d0 = im[0];
+      d1 = im[1];
+      d2 = im[2];
+    }
+    const bool h0 = d0 != kNoImage, h1 = d1 != kNoImage, h2 = d2 != kNoImage;
+    const int64_t o0 = h0 ? (int64_t)d0 * CS : 0, o1 = h1 ? (int64_t)d1 * CS : 0, o2 = h2 ? (int64_t)d2 * CS : 0;
+    float* __restrict__ Pw = L.phi;
+#pragma unroll
+    for (int q = 0; q < M; ++q) col_put(Pw, c0 + lane + 32 * q, v[q], o0, o1, o2, h0, h1, h2);
+    const float r0 = __shfl_sync(kFull, v[0], 0);
+    const float rn = __shfl_sync(kFull, v[M - 1], 31);
+    if (lane == 0 || lane == 31) {
+      const int code = lane == 0 ? L.z1 : L.zZ;
+      const float gv = code == 0 ? 0.f : (code == 1 ? r0 : rn);
+      col_put(Pw, lane == 0 ? c0 - 1 : c0 + N, gv, o0, o1, o2, h0, h1, h2);
+    }
+    __syncwarp();
+  }
+}
+
 // ------------------------------------------------ TMA-staged variant
 // The same sweep with the line's five source columns (f of the line, phi of
 // its four horizontal neighbours: 2 KB each at nz = 512) brought into

@@ -13,8 +13,9 @@ inline bool col_rows_supported(int M) {
 // variants of the sweep: k_col_sweep<M, NL, MINB> with 0 = one line per
 // warp step, 3 CTAs/SM; 1 = one line, 4 CTAs/SM; 2 = two lines, 2 CTAs/SM;
 // 3 = k_col_sweep_tma (source columns staged by bulk copies; err: a
-// host-mapped int set to 1 if a copy wait ran out)
-constexpr int kColSweepVariants = 4;
+// host-mapped int set to 1 if a copy wait ran out); 4 = k_col_sweep_rf
+// (factors in registers, persistent, next line prefetched into L2)
+constexpr int kColSweepVariants = 5;
 void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, int variant, int* err,
                       cudaStream_t s);
 // sets the launch attributes every sweep variant for M needs (call before

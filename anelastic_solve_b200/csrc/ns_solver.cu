@@ -471,6 +471,7 @@ int NSSolver::set_fields(const anel_fields* f, int mem, cudaStream_t s) {
     if (!src[q] || !d_fields_[q]) continue;  // LES fields exist only with a subgrid model
     ANEL_CUDA_TRY(cudaMemcpyAsync(d_fields_[q], src[q], G_ * sizeof(double), kind, s));
     if (q == 6 || q == 7) density = true;
+    if (q >= 8 && q <= 12) temps_clean_ = false;
   }
   if (density) {
     // profiles of r and densityBG: both must be functions of z only
@@ -592,6 +593,7 @@ int NSSolver::reset(const anel_ns_params* ns, cudaStream_t s) {
     return ANEL_ERR_ARG;
   }
   prm_ = *ns;
+  temps_clean_ = false;
   rRe_ = 1.0 / ns->Re;
   rPr_ = 1.0 / ns->Pr;
   rSc_ = 1.0 / ns->Sc;
@@ -716,9 +718,15 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   const int64_t launches0 = t_launches;
   ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
   for (int n = 0; n < nsteps; ++n) {
-    // zero_temps (memManage.F90:844-853)
+    // zero_temps (memManage.F90:844-853).  The accumulators q_u, q_v,
+    // q_w, q_rho, q_s are written, never read, by the first sub-step
+    // (a1 = 0) on every interior cell, and no kernel writes their ghost
+    // cells, so once zeroed they need no zeroing again until set_fields,
+    // reset or a scratch use touches them (temps_clean_); the Poisson
+    // right-hand side is zeroed every step.
     for (int q : {8, 9, 10, 11, 12, 13})
-      ANEL_CUDA_TRY(cudaMemsetAsync(d_fields_[q], 0, G_ * sizeof(double), s));
+      if (q == 13 || !temps_clean_) ANEL_CUDA_TRY(cudaMemsetAsync(d_fields_[q], 0, G_ * sizeof(double), s));
+    temps_clean_ = true;
     int st = ANEL_OK;
     const double delt = calcdt(s, &st);
     if (st != ANEL_OK) return st;

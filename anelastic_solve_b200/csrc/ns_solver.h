@@ -140,6 +140,11 @@ class NSSolver {
   double* h_cn_ = nullptr;          // pinned staging of the same
   double cn_rkdt_[3] = {-1, -1, -1};
   int cnvar_ = 0;  // launch variant of the DNS column solve (tune_cn)
+  // the RHS accumulators q_* hold zero ghost cells and the previous step's
+  // interior values only (no set_fields, reset or scratch use since the
+  // last zeroing): the first sub-step's a1 = 0 form overwrites every
+  // interior cell without reading it, so zero_temps can skip them
+  bool temps_clean_ = false;
   int tune_cn();
   int cn_next_ = 0;
   unsigned long long* d_red_ = nullptr;

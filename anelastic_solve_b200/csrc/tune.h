@@ -5,7 +5,8 @@
 // on the caller's data layout, and the fastest variant is kept for the
 // process: contexts of the same shape (serving buckets) reuse the choice.
 // ANEL_TUNE=0 in the environment turns timing off (every kernel keeps its
-// default variant).
+// default variant); ANEL_TUNE_CACHE=<file> keeps the choices in a file
+// that later processes read instead of timing again.
 #pragma once
 
 #include <string>

@@ -341,11 +341,11 @@ def test_direct_coarse_solve_matches_oracle():
 
 
 @pytest.mark.parametrize("n", [(64, 32, 256), (32, 16, 512)])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_column_sweep_variants(variant, n, monkeypatch):
     """Every launch variant of the column-layout z-line sweep (the
     autotuner's candidates, forced here through ANEL_COL_VARIANT; 3 is the
-    bulk-copy staged kernel): the mixed ZLINE solve reaches the oracle's
+    bulk-copy staged kernel, 4 the one with its factors in registers): the mixed ZLINE solve reaches the oracle's
     FP64 solution within 1e-9."""
     monkeypatch.setenv("ANEL_COL_VARIANT", str(variant))
     g = G.shear_layer_grid(*n, stretched=True)
