@@ -32,6 +32,8 @@ SIGNATURES = {
     "anel_mg_destroy": (None, [_P]),
     "anel_mg_ctx_set_density": (C.c_int, [_P, _DP, C.c_int32]),
     "anel_mg_ctx_solve": (C.c_int, [_P, _DP, _DP, C.c_int32, _P, C.POINTER(abi.MGReport)]),
+    "anel_mg_ctx_solve_batch": (C.c_int, [_P, C.c_int32, C.POINTER(_DP), C.POINTER(_DP), _P,
+                                          C.POINTER(abi.MGReport)]),
     "anel_mg_ctx_levels": (C.c_int, [_P, _IP, C.c_int32]),
     "anel_mg_ctx_set_profiling": (C.c_int, [_P, C.c_int32]),
     "anel_mg_ctx_debug_pass": (C.c_int, [_P, C.c_int32, _DP, _DP, _P]),
@@ -43,6 +45,8 @@ SIGNATURES = {
     "anel_ns_ctx_substep": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_double,
                                       C.c_double, _P, _IP, _DP]),
     "anel_ns_ctx_step": (C.c_int, [_P, C.c_int32, _P, C.POINTER(abi.StepReport)]),
+    "anel_ns_ctx_step_cohort": (C.c_int, [C.POINTER(_P), C.c_int32, C.c_int32, _P, _P,
+                                          C.POINTER(abi.StepReport)]),
     "anel_ns_ctx_set_clock": (C.c_int, [_P, C.c_double, C.c_int32]),
     "anel_ns_ctx_set_profiling": (C.c_int, [_P, C.c_int32]),
     "anel_ns_ctx_project": (C.c_int, [_P, _IP, _DP]),

@@ -164,7 +164,8 @@ class Result(C.Structure):
 class ServeStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
                 ("bytes_in_use", C.c_int64), ("peak_bytes", C.c_int64), ("active", C.c_int32),
-                ("peak_active", C.c_int32), ("contexts", C.c_int32), ("queued", C.c_int32)]
+                ("peak_active", C.c_int32), ("contexts", C.c_int32), ("queued", C.c_int32),
+                ("peak_cohort", C.c_int32), ("reserved", C.c_int32)]
 
 
 class StepReport(C.Structure):

@@ -51,6 +51,11 @@ void copy_words(const void* src, void* dst, int64_t nwords, cudaStream_t s);
 // scratch holds fold_scratch_doubles() doubles.
 int64_t fold_scratch_doubles();
 void launch_fold_pairs(const double* part, int64_t n, double* scratch, double* out, cudaStream_t s);
+// the same for nm members at once: member b's n pairs at part + b*pstride,
+// its sums to out[2b], out[2b+1] (the order of each member's fold is the
+// one-member order); scratch holds nm * fold_scratch_doubles() doubles
+void launch_fold_pairs_members(const double* part, int64_t n, int64_t pstride, double* scratch, double* out,
+                               int nm, cudaStream_t s);
 
 // ------------------------------------------------------------ level maps
 // One multigrid level, 1-based Fortran conventions of mg_init.F90:

@@ -182,6 +182,15 @@ int anel_mg_ctx_solve(anel_mg_ctx* ctx, double* phif, const double* rhsf, int32_
                                 : ctx->s->solve_host(phif, rhsf, s, report);
 }
 
+int anel_mg_ctx_solve_batch(anel_mg_ctx* ctx, int32_t n, double* const* d_phis, const double* const* d_rhss,
+                            void* stream, anel_mg_report* reports) {
+  if (!ctx) {
+    anel::set_error("null context");
+    return ANEL_ERR_ARG;
+  }
+  return ctx->s->solve_batch(n, d_phis, d_rhss, static_cast<cudaStream_t>(stream), reports);
+}
+
 int anel_mg_ctx_set_profiling(anel_mg_ctx* ctx, int32_t on) {
   if (!ctx) return ANEL_ERR_ARG;
   return ctx->s->set_profiling(on != 0);
@@ -238,6 +247,24 @@ int anel_ns_ctx_substep(anel_ns_ctx* ctx, double a1, double a2, double a3, doubl
 int anel_ns_ctx_step(anel_ns_ctx* ctx, int32_t nsteps, void* stream, anel_step_report* report) {
   if (!ctx || nsteps < 0) return ANEL_ERR_ARG;
   return ctx->s->step(nsteps, static_cast<cudaStream_t>(stream), report);
+}
+
+int anel_ns_ctx_step_cohort(anel_ns_ctx* const* ctxs, int32_t n, int32_t nsteps, anel_mg_ctx* batch,
+                            void* stream, anel_step_report* reports) {
+  if (!ctxs || n < 1 || nsteps < 0 || !reports) {
+    anel::set_error("step_cohort: n >= 1 contexts, nsteps >= 0 and reports required");
+    return ANEL_ERR_ARG;
+  }
+  std::vector<anel::NSSolver*> ms(n);
+  for (int b = 0; b < n; ++b) {
+    if (!ctxs[b]) {
+      anel::set_error("step_cohort: null context %d", b);
+      return ANEL_ERR_ARG;
+    }
+    ms[b] = ctxs[b]->s;
+  }
+  anel::MGSolver* bmg = batch ? batch->s : ms[0]->mg();
+  return anel::NSSolver::step_cohort(ms.data(), n, nsteps, bmg, static_cast<cudaStream_t>(stream), reports);
 }
 
 int anel_ns_ctx_set_profiling(anel_ns_ctx* ctx, int32_t on) {

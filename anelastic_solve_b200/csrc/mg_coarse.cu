@@ -134,13 +134,15 @@ void direct_free(DirectHost& D) {
   D.f = DirectFac{};
 }
 
-// One warp per mode: the mode's z-system (mode-major rows), in place, by
-// the column sweep's partitioned solve in FP64.
+// One warp per mode of a member: the mode's z-system (mode-major rows), in
+// place, by the column sweep's partitioned solve in FP64.
 template <int M>
 __global__ void __launch_bounds__(128) k_dir_solve(DirectFac F) {
   const int lane = threadIdx.x & 31;
-  const int m = blockIdx.x * 4 + (threadIdx.x >> 5);
-  if (m >= F.nm) return;  // the whole warp
+  const int q0 = blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (q0 >= F.nm * F.nmem) return;  // the whole warp
+  const int b = q0 / F.nm, m = q0 - b * F.nm;
+  if (F.act && !F.act[b]) return;
   constexpr int NF = col_fac_floats(M);
   const double* f = F.fac + (int64_t)m * dir_fac_per_mode(M);
   const double* Fap = f;
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(128) k_dir_solve(DirectFac F) {
   const double* FL = f + 3 * (M - 1) * 32;
   const double* FR = f + 4 * (M - 1) * 32;
   const double* Fg = f + 5 * (M - 1) * 32;
-  double* w = F.work + (int64_t)m * F.nz;
+  double* w = F.work + ((int64_t)b * F.nm + m) * F.nz;
   double y[M];
 #pragma unroll
   for (int q = 0; q < M; ++q) y[q] = w[lane * M + q];
@@ -198,7 +200,7 @@ __global__ void __launch_bounds__(128) k_dir_solve(DirectFac F) {
 }
 
 static void dir_solve_launch(const DirectFac& F, cudaStream_t s) {
-  const unsigned g = (unsigned)((F.nm + 3) / 4);
+  const unsigned g = (unsigned)((F.nm * F.nmem + 3) / 4);
   switch (F.M) {
     case 2: k_dir_solve<2><<<g, 128, 0, s>>>(F); break;
     case 3: k_dir_solve<3><<<g, 128, 0, s>>>(F); break;
@@ -215,14 +217,18 @@ static void direct_launch(const DirectFac& F, const In& in, const Out& out, cuda
   const size_t sm = dir_smem_bytes(F.nx, F.ny);
   set_smem_limit_once((const void*)k_dir_forward<In>, (int)sm);
   set_smem_limit_once((const void*)k_dir_inverse<Out>, (int)sm);
-  k_dir_forward<In><<<F.nz, 256, sm, s>>>(F, in);
+  k_dir_forward<In><<<F.nz * F.nmem, 256, sm, s>>>(F, in);
   dir_solve_launch(F, s);
-  k_dir_inverse<Out><<<F.nz, 256, sm, s>>>(F, out);
+  k_dir_inverse<Out><<<F.nz * F.nmem, 256, sm, s>>>(F, out);
   count_launch(3);
 }
 
-void launch_direct_col(const DirectFac& F, const ColLevel& L, cudaStream_t s) {
-  direct_launch(F, DirColIn{L}, DirColOut{L}, s);
+void launch_direct_col(const DirectFac& F, const ColLevel& L, double* work, cudaStream_t s) {
+  DirectFac Fb = F;
+  Fb.nmem = L.nm;
+  Fb.act = L.act;
+  if (work) Fb.work = work;
+  direct_launch(Fb, DirColIn{L}, DirColOut{L}, s);
 }
 
 void launch_direct_row(const DirectFac& F, const double* f, double* phi, int X, int64_t XY, cudaStream_t s) {

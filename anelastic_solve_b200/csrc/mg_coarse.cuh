@@ -39,12 +39,17 @@ struct DirectFac {
   const double* Bx;    // nx x nx, row p = basis function p over i
   const double* By;    // ny x ny
   const double* fac;   // [nm][dir_fac_per_mode(M)]
-  double* work;        // [nm][nz] modal right-hand side, then solution
+  double* work;        // [nmem][nm][nz] modal right-hand side, then solution
+  // members of a batch (the same level of independent problems): member b
+  // has its own work block; act[b] == 0 skips it (null: all active)
+  int nmem = 1;
+  const int* act = nullptr;
 };
 
 // input: the level's restricted FP32 right-hand side (column layout)
 struct DirColIn {
   ColLevel L;
+  __device__ __forceinline__ DirColIn member(int b) const { return DirColIn{col_member(L, b)}; }
   __device__ __forceinline__ double get(int i0, int j0, int r) const {
     return (double)L.src[col_cell(L, i0 + 2, j0 + 2, r + 2)];
   }
@@ -52,6 +57,7 @@ struct DirColIn {
 // output: the level's FP32 phi (column layout) with its ghost copies
 struct DirColOut {
   ColLevel L;
+  __device__ __forceinline__ DirColOut member(int b) const { return DirColOut{col_member(L, b)}; }
   __device__ __forceinline__ void put(int i0, int j0, int r, double v) const {
     const int i = i0 + 2, j = j0 + 2, k = r + 2;
     const float f = (float)v;
@@ -83,6 +89,7 @@ struct DirRowIn {
   const double* f;
   int X;
   int64_t XY;
+  __device__ __forceinline__ DirRowIn member(int) const { return *this; }
   __device__ __forceinline__ double get(int i0, int j0, int r) const {
     return f[cidx(i0 + 2, j0 + 2, r + 2, X, XY)];
   }
@@ -91,16 +98,21 @@ struct DirRowOut {
   double* phi;
   int X;
   int64_t XY;
+  __device__ __forceinline__ DirRowOut member(int) const { return *this; }
   __device__ __forceinline__ void put(int i0, int j0, int r, double v) const {
     phi[cidx(i0 + 2, j0 + 2, r + 2, X, XY)] = v;
   }
 };
 
-// One CTA per z-row: W = Bx F By^T of the row's plane.
+// One CTA per z-row of a member: W = Bx F By^T of the row's plane.
 template <class In>
-__global__ void __launch_bounds__(256) k_dir_forward(DirectFac F, In in) {
+__global__ void __launch_bounds__(256) k_dir_forward(DirectFac F, In inb) {
   extern __shared__ double dsm[];
-  const int nx = F.nx, ny = F.ny, r = blockIdx.x;
+  const int b = blockIdx.x / F.nz;
+  if (F.act && !F.act[b]) return;  // the whole CTA
+  const In in = inb.member(b);
+  double* work = F.work + (int64_t)b * F.nm * F.nz;
+  const int nx = F.nx, ny = F.ny, r = blockIdx.x - b * F.nz;
   double* bx = dsm;
   double* by = bx + nx * nx;
   double* P = by + ny * ny;
@@ -122,22 +134,26 @@ __global__ void __launch_bounds__(256) k_dir_forward(DirectFac F, In in) {
     const int p = q % nx, m = q / nx;
     double s = 0.0;
     for (int j = 0; j < ny; ++j) s += by[m * ny + j] * T[p + nx * j];
-    F.work[(int64_t)q * F.nz + r] = s;
+    work[(int64_t)q * F.nz + r] = s;
   }
 }
 
-// One CTA per z-row: phi = Bx^T W By of the row's modes.
+// One CTA per z-row of a member: phi = Bx^T W By of the row's modes.
 template <class Out>
-__global__ void __launch_bounds__(256) k_dir_inverse(DirectFac F, Out out) {
+__global__ void __launch_bounds__(256) k_dir_inverse(DirectFac F, Out outb) {
   extern __shared__ double dsm[];
-  const int nx = F.nx, ny = F.ny, r = blockIdx.x;
+  const int b = blockIdx.x / F.nz;
+  if (F.act && !F.act[b]) return;  // the whole CTA
+  const Out out = outb.member(b);
+  const double* work = F.work + (int64_t)b * F.nm * F.nz;
+  const int nx = F.nx, ny = F.ny, r = blockIdx.x - b * F.nz;
   double* bx = dsm;
   double* by = bx + nx * nx;
   double* W = by + ny * ny;
   double* T = W + nx * ny;
   for (int q = threadIdx.x; q < nx * nx; q += blockDim.x) bx[q] = F.Bx[q];
   for (int q = threadIdx.x; q < ny * ny; q += blockDim.x) by[q] = F.By[q];
-  for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) W[q] = F.work[(int64_t)q * F.nz + r];
+  for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) W[q] = work[(int64_t)q * F.nz + r];
   __syncthreads();
   for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) {  // T(i, m)
     const int i = q % nx, m = q / nx;

@@ -21,8 +21,10 @@ struct DirectHost {
 int direct_build(DirectHost& D, int nx, int ny, int nz, double a1, double a2, double a3, double a4,
                  const double* cz5, const double* cz6, const double* dz5, const double* dz6, int z1, int zZ);
 void direct_free(DirectHost& D);
-// solve of the level in the cycle: L.src -> L.phi (FP32 column layout, ghosts written)
-void launch_direct_col(const DirectFac& F, const ColLevel& L, cudaStream_t s);
+// solve of the level in the cycle: L.src -> L.phi (FP32 column layout, ghosts
+// written), for each of L's L.nm members (act: L.act); work: nm * nx*ny*nz
+// doubles for a batch (null: the level's own block, one member)
+void launch_direct_col(const DirectFac& F, const ColLevel& L, double* work, cudaStream_t s);
 // the same on FP64 reference-layout arrays (interior of phi written)
 void launch_direct_row(const DirectFac& F, const double* f, double* phi, int X, int64_t XY, cudaStream_t s);
 

@@ -7,7 +7,7 @@ namespace anel {
 
 template <int M, int NL, int MINB>
 static void col_sweep_launch(const ColLevel& L, int color, const float* fac, cudaStream_t s) {
-  const int64_t nlines = (int64_t)((L.nx + 1) / 2) * L.ny;
+  const int64_t nlines = (int64_t)((L.nx + 1) / 2) * L.ny * L.nm;
   const int64_t per = (int64_t)kColWarps * NL;
   int64_t b = (nlines + per - 1) / per;
   const int64_t cap = 148 * MINB * 2;
@@ -18,7 +18,7 @@ static void col_sweep_launch(const ColLevel& L, int color, const float* fac, cud
 
 template <int M>
 static void col_sweep_tma_launch(const ColLevel& L, int color, const float* fac, int* err, cudaStream_t s) {
-  const int64_t nlines = (int64_t)((L.nx + 1) / 2) * L.ny;
+  const int64_t nlines = (int64_t)((L.nx + 1) / 2) * L.ny * L.nm;
   int64_t b = (nlines + kColTmaWarps - 1) / kColTmaWarps;
   const int64_t cap = 148 * 2 * 4;
   if (b > cap) b = cap;
@@ -43,7 +43,7 @@ static void col_sweep_rf_occupancy() {
 
 template <int M>
 static void col_sweep_rf_launch(const ColLevel& L, int color, const float* fac, cudaStream_t s) {
-  const int64_t nlines = (int64_t)((L.nx + 1) / 2) * L.ny;
+  const int64_t nlines = (int64_t)((L.nx + 1) / 2) * L.ny * L.nm;
   int64_t b = (nlines + kColWarps - 1) / kColWarps;
   const int64_t cap = 148 * (int64_t)(g_rf_occ[M] > 0 ? g_rf_occ[M] : 1);
   if (b > cap) b = cap;
@@ -109,7 +109,7 @@ static unsigned col_xfer_blocks(int64_t items) {
 }
 
 void launch_col_restrict(const ColLevel& F, const ColLevel& C, int cdir, cudaStream_t s) {
-  const unsigned g = col_xfer_blocks((int64_t)C.nx * C.ny * (C.nz / 4));
+  const unsigned g = col_xfer_blocks((int64_t)C.nx * C.ny * (C.nz / 4) * C.nm);
   switch (cdir & 3) {
     case 1: k_col_restrict<1><<<g, kColXferThreads, 0, s>>>(F, C); break;
     case 2: k_col_restrict<2><<<g, kColXferThreads, 0, s>>>(F, C); break;
@@ -119,7 +119,7 @@ void launch_col_restrict(const ColLevel& F, const ColLevel& C, int cdir, cudaStr
 }
 
 void launch_col_prolong(const ColLevel& F, const ColLevel& C, int cdir, cudaStream_t s) {
-  const unsigned g = col_xfer_blocks((int64_t)F.nx * F.ny * (F.nz / 4));
+  const unsigned g = col_xfer_blocks((int64_t)F.nx * F.ny * (F.nz / 4) * F.nm);
   switch (cdir & 3) {
     case 1: k_col_prolong<1><<<g, kColXferThreads, 0, s>>>(F, C); break;
     case 2: k_col_prolong<2><<<g, kColXferThreads, 0, s>>>(F, C); break;

@@ -49,7 +49,28 @@ struct ColLevel {
   // 1 row k = 2, 2 row k = nz+1)
   const int* img;
   int z1, zZ;
+  // members of a batch (independent problems on the same level): member m's
+  // columns start at phi / src + m * ms; act[m] == 0 leaves member m alone
+  // (null: every member is active)
+  int nm = 1;
+  int64_t ms = 0;
+  const int* act = nullptr;
 };
+
+// FP64 fine arrays of one member of a batch (reference layout)
+struct MemberIO {
+  double* phi;
+  const double* rhs;
+};
+
+// the level of member m alone (its arrays; nm = 1)
+__host__ __device__ __forceinline__ ColLevel col_member(ColLevel L, int m) {
+  L.phi += m * L.ms;
+  L.src += m * L.ms;
+  L.nm = 1;
+  return L;
+}
+__device__ __forceinline__ bool col_active(const ColLevel& L, int m) { return !L.act || L.act[m] != 0; }
 
 __host__ __device__ __forceinline__ int64_t col_cell(const ColLevel& L, int i, int j, int k) {
   return ((int64_t)(i - 1) + (int64_t)L.X * (j - 1)) * L.CS + (kColPad - 2) + k;
@@ -99,25 +120,28 @@ __global__ void __launch_bounds__(32 * kColWarps, MINB) k_col_sweep(ColLevel L, 
   const float* FR = sf + 4 * (M - 1) * 32;
   const float* Fg = sf + 5 * (M - 1) * 32;
   const int pairs = (L.nx + 1) >> 1;
-  const int64_t nlines = (int64_t)pairs * L.ny;
+  const int64_t nlines = (int64_t)pairs * L.ny;  // of one member
+  const int64_t ntot = nlines * L.nm;
   const int64_t CS = L.CS, XC = (int64_t)L.X * L.CS;
   const float a1 = L.a1, a2 = L.a2, a3 = L.a3, a4 = L.a4;
   const float c5b = L.cz5[1], c6t = L.cz6[L.nz];  // row 0 to its k=1 ghost, row n-1 to k=Z
-  for (int64_t t0 = ((int64_t)blockIdx.x * kColWarps + warp) * NL; t0 < nlines;
+  for (int64_t t0 = ((int64_t)blockIdx.x * kColWarps + warp) * NL; t0 < ntot;
        t0 += (int64_t)gridDim.x * kColWarps * NL) {
     int64_t c0[NL];
     bool on[NL];
     int ii[NL], jj[NL];
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
-      const int64_t t = t0 + l;
+      const int64_t tt = t0 + l;
+      const int m = L.nm == 1 ? 0 : (int)(tt / nlines);
+      const int64_t t = tt - (int64_t)m * nlines;
       const int j = 2 + (int)(t / pairs);
       const int i0 = 2 + 2 * (int)(t % pairs);
       const int i = i0 + ((color + i0 + j) & 1);
-      on[l] = t < nlines && i <= L.nx + 1;  // uniform across the warp
+      on[l] = tt < ntot && i <= L.nx + 1 && col_active(L, m);  // uniform across the warp
       ii[l] = i;
       jj[l] = j;
-      c0[l] = on[l] ? col_cell(L, i, j, 2) : 0;  // row 0
+      c0[l] = on[l] ? m * L.ms + col_cell(L, i, j, 2) : 0;  // row 0
     }
     const float* __restrict__ P = L.phi;
     const float* __restrict__ S = L.src;
@@ -284,25 +308,32 @@ __global__ void __launch_bounds__(32 * kColWarps, 1) k_col_sweep_rf(ColLevel L, 
     ga[q] = Fg[(7 + q) * 32 + lane];
   }
   const int pairs = (L.nx + 1) >> 1;
-  const int64_t nlines = (int64_t)pairs * L.ny;
+  const int64_t nlines = (int64_t)pairs * L.ny;  // of one member
+  const int64_t ntot = nlines * L.nm;
   const int64_t CS = L.CS, XC = (int64_t)L.X * L.CS;
   const float a1 = L.a1, a2 = L.a2, a3 = L.a3, a4 = L.a4;
   const float c5b = L.cz5[1], c6t = L.cz6[L.nz];
   const int64_t stride = (int64_t)gridDim.x * kColWarps;
-  auto line = [&](int64_t t, int& i, int& j) -> bool {
+  // line tt of the batch: member m, column (i, j); base = m's offset
+  auto line = [&](int64_t tt, int& i, int& j, int64_t& base) -> bool {
+    const int m = L.nm == 1 ? 0 : (int)(tt / nlines);
+    const int64_t t = tt - (int64_t)m * nlines;
     j = 2 + (int)(t / pairs);
     const int i0 = 2 + 2 * (int)(t % pairs);
     i = i0 + ((color + i0 + j) & 1);
-    return t < nlines && i <= L.nx + 1;
+    base = m * L.ms;
+    return tt < ntot && i <= L.nx + 1 && col_active(L, m);
   };
   float* ys = sy[warp];
-  for (int64_t t = (int64_t)blockIdx.x * kColWarps + warp; t < nlines; t += stride) {
+  for (int64_t t = (int64_t)blockIdx.x * kColWarps + warp; t < ntot; t += stride) {
     int i, j;
-    const bool on = line(t, i, j);
+    int64_t mb;
+    const bool on = line(t, i, j, mb);
     {
       int in, jn;
-      if (line(t + stride, in, jn)) {
-        const int64_t cn = col_cell(L, in, jn, 2);
+      int64_t nb;
+      if (line(t + stride, in, jn, nb)) {
+        const int64_t cn = nb + col_cell(L, in, jn, 2);
         // the 5 x M 128-byte lines of the next line's source columns
         for (int q = lane; q < 5 * M; q += 32) {
           const int a = q / M, r = (q - a * M) * 32;
@@ -313,7 +344,7 @@ __global__ void __launch_bounds__(32 * kColWarps, 1) k_col_sweep_rf(ColLevel L, 
       }
     }
     if (!on) continue;  // uniform across the warp
-    const int64_t c0 = col_cell(L, i, j, 2);
+    const int64_t c0 = mb + col_cell(L, i, j, 2);
     const float* __restrict__ P = L.phi;
     const float* __restrict__ S = L.src;
     float v[M];
@@ -453,22 +484,32 @@ __global__ void __launch_bounds__(32 * kColTmaWarps, 2) k_col_sweep_tma(ColLevel
   const float* FR = sf + 4 * (M - 1) * 32;
   const float* Fg = sf + 5 * (M - 1) * 32;
   const int pairs = (L.nx + 1) >> 1;
-  const int64_t nlines = (int64_t)pairs * L.ny;
+  const int64_t nlines = (int64_t)pairs * L.ny;  // of one member
+  const int64_t ntot = nlines * L.nm;
   const int64_t CS = L.CS, XC = (int64_t)L.X * L.CS;
   const float a1 = L.a1, a2 = L.a2, a3 = L.a3, a4 = L.a4;
   const float c5b = L.cz5[1], c6t = L.cz6[L.nz];
   const int64_t stride = (int64_t)gridDim.x * kColTmaWarps;
-  auto line = [&](int64_t t, int& i, int& j) -> bool {
+  // line tt of the batch: member m (base = its offset), column (i, j);
+  // the lines of inactive members are copied in too (the buffer parity
+  // below counts every line) but not solved
+  auto line = [&](int64_t tt, int& i, int& j, int64_t& base, bool& act) -> bool {
+    const int m = L.nm == 1 ? 0 : (int)(tt / nlines);
+    const int64_t t = tt - (int64_t)m * nlines;
     j = 2 + (int)(t / pairs);
     const int i0 = 2 + 2 * (int)(t % pairs);
     i = i0 + ((color + i0 + j) & 1);
-    return t < nlines && i <= L.nx + 1;
+    base = m * L.ms;
+    act = tt < ntot && col_active(L, m);
+    return tt < ntot && i <= L.nx + 1;
   };
   // lane 0: the five source columns of line t into buffer b
   auto issue = [&](int64_t t, int b) {
     int i, j;
-    if (!line(t, i, j)) return;
-    const int64_t c0 = col_cell(L, i, j, 2);
+    int64_t base;
+    bool act;
+    if (!line(t, i, j, base, act)) return;
+    const int64_t c0 = base + col_cell(L, i, j, 2);
     const unsigned bar = smem_u32(&bars[2 * warp + b]);
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(5 * N * 4) : "memory");
@@ -487,16 +528,22 @@ __global__ void __launch_bounds__(32 * kColTmaWarps, 2) k_col_sweep_tma(ColLevel
   if (lane == 0) issue(t, 0);
   int u = 0;
   bool ok = true;
-  for (; t < nlines; ++u, t += stride) {
+  for (; t < ntot; ++u, t += stride) {
     const int b = u & 1;
     if (lane == 0) issue(t + stride, b ^ 1);
     int i, j;
-    (void)line(t, i, j);
+    int64_t mb;
+    bool act;
+    (void)line(t, i, j, mb, act);
     if (!mbar_wait(smem_u32(&bars[2 * warp + b]), (unsigned)((u >> 1) & 1))) {
       ok = false;
       break;
     }
-    const int64_t c0 = col_cell(L, i, j, 2);
+    if (!act) {  // uniform across the warp
+      __syncwarp();
+      continue;
+    }
+    const int64_t c0 = mb + col_cell(L, i, j, 2);
     const float* sb = stage + (size_t)b * 5 * N;
     float v[M];
 #pragma unroll
@@ -572,7 +619,7 @@ __global__ void __launch_bounds__(32 * kColTmaWarps, 2) k_col_sweep_tma(ColLevel
     // buffer u%2, and line t+stride in the other buffer if it exists),
     // then return
     (void)mbar_wait(smem_u32(&bars[2 * warp + (u & 1)]), (unsigned)((u >> 1) & 1));
-    if (t + stride < nlines)
+    if (t + stride < ntot)
       (void)mbar_wait(smem_u32(&bars[2 * warp + ((u + 1) & 1)]), (unsigned)(((u + 1) >> 1) & 1));
   }
 }
@@ -624,12 +671,17 @@ constexpr int kColXferThreads = 256;
 // order.  One thread per coarse column and 4-row chunk (grid-stride); the
 // caller zeroes coarse phi.
 template <int CD>
-__global__ void __launch_bounds__(kColXferThreads) k_col_restrict(ColLevel F, ColLevel C) {
-  const int nch = C.nz >> 2;
-  const int64_t items = (int64_t)C.nx * C.ny * nch;
+__global__ void __launch_bounds__(kColXferThreads) k_col_restrict(ColLevel Fb, ColLevel Cb) {
+  const int nch = Cb.nz >> 2;
+  const int64_t items = (int64_t)Cb.nx * Cb.ny * nch;  // of one member
   constexpr bool cx = CD & 1, cy = CD & 2;
-  for (int64_t t = (int64_t)blockIdx.x * kColXferThreads + threadIdx.x; t < items;
-       t += (int64_t)gridDim.x * kColXferThreads) {
+  for (int64_t tt = (int64_t)blockIdx.x * kColXferThreads + threadIdx.x; tt < items * Cb.nm;
+       tt += (int64_t)gridDim.x * kColXferThreads) {
+    const int m = Cb.nm == 1 ? 0 : (int)(tt / items);
+    if (!col_active(Cb, m)) continue;
+    const int64_t t = tt - (int64_t)m * items;
+    const ColLevel F = col_member(Fb, m);
+    const ColLevel C = col_member(Cb, m);
     const int ch = (int)(t % nch);
     const int64_t col = t / nch;
     const int ic = 2 + (int)(col % C.nx), jc = 2 + (int)(col / C.nx);
@@ -657,12 +709,17 @@ __global__ void __launch_bounds__(kColXferThreads) k_col_restrict(ColLevel F, Co
 // boundary pass of the row-major cycle).  One thread per fine column and
 // 4-row chunk (grid-stride).
 template <int CD>
-__global__ void __launch_bounds__(kColXferThreads) k_col_prolong(ColLevel F, ColLevel C) {
-  const int nch = F.nz >> 2;
-  const int64_t items = (int64_t)F.nx * F.ny * nch;
+__global__ void __launch_bounds__(kColXferThreads) k_col_prolong(ColLevel Fb, ColLevel Cb) {
+  const int nch = Fb.nz >> 2;
+  const int64_t items = (int64_t)Fb.nx * Fb.ny * nch;  // of one member
   constexpr bool cx = CD & 1, cy = CD & 2;
-  for (int64_t t = (int64_t)blockIdx.x * kColXferThreads + threadIdx.x; t < items;
-       t += (int64_t)gridDim.x * kColXferThreads) {
+  for (int64_t tt = (int64_t)blockIdx.x * kColXferThreads + threadIdx.x; tt < items * Fb.nm;
+       tt += (int64_t)gridDim.x * kColXferThreads) {
+    const int m = Fb.nm == 1 ? 0 : (int)(tt / items);
+    if (!col_active(Fb, m)) continue;
+    const int64_t t = tt - (int64_t)m * items;
+    const ColLevel F = col_member(Fb, m);
+    const ColLevel C = col_member(Cb, m);
     const int ch = (int)(t % nch);
     const int64_t col = t / nch;
     const int i = 2 + (int)(col % F.nx), j = 2 + (int)(col / F.nx);

@@ -36,4 +36,16 @@ int64_t col_resid_part_doubles(const DevLevel<double>& L);
 // phi += (double) E.phi on the interior (phi in the reference layout)
 void launch_col_add_correction(const DevLevel<double>& L, double* phi, const ColLevel& E, cudaStream_t s);
 
+// The same for the E.nm members of a batch, member b's FP64 arrays in mt[b]
+// (a device table) and E.act masking the inactive ones: the residual's
+// norms go to out[2b], out[2b+1], folded in the one-member order; part
+// holds col_resid_part_doubles_members(L, E.nm) doubles.  The ghost pass
+// needs the homogeneous ghost table of L (L.gtab).
+int64_t col_resid_part_doubles_members(const DevLevel<double>& L, int nm);
+void launch_col_resid_store_members(const DevLevel<double>& L, const MemberIO* mt, const ColLevel& E,
+                                    double* part, double* out, cudaStream_t s);
+void launch_col_add_correction_members(const DevLevel<double>& L, const MemberIO* mt, const ColLevel& E,
+                                       cudaStream_t s);
+void launch_bdry_members(const DevLevel<double>& L, const MemberIO* mt, const int* act, int nm, cudaStream_t s);
+
 }  // namespace anel

@@ -8,6 +8,7 @@
 // Compiled with -fmad=false: the FP64 residual is the value fine_resid
 // gives in the reference's order (the same numbers as the row-major path).
 #include "mg_col.h"
+#include "mg_launch.h"
 
 namespace anel {
 
@@ -25,14 +26,26 @@ __device__ __forceinline__ double col_block_sum(double v, double* sh) {
   return s;
 }
 
-// grid (ceil(nx/32), ceil(ny/8), nz/kColRows), block 32 x 8
+// grid (ceil(nx/32), ceil(ny/8), nz/kColRows * members), block 32 x 8.
+// Member b of a batch (mt non-null) takes its phi and f from mt[b], its
+// FP32 columns from E's member b and its partial sums from the b-th block
+// of part; an inactive member's blocks return at once.
 __global__ void __launch_bounds__(kTI * kTJ) k_col_resid_store(DevLevel<double> L, const double* __restrict__ phi,
-                                                             const double* __restrict__ f, ColLevel E,
-                                                             double* __restrict__ part) {
+                                                             const double* __restrict__ f, ColLevel Eb,
+                                                             double* __restrict__ part,
+                                                             const MemberIO* __restrict__ mt) {
   __shared__ double sh[kTJ];
+  const int nzb = L.nz / kColRows;
+  const int b = blockIdx.z / nzb;
+  if (!col_active(Eb, b)) return;  // the whole block
+  if (mt) {
+    phi = mt[b].phi;
+    f = mt[b].rhs;
+  }
+  const ColLevel E = col_member(Eb, b);
   const int i = 2 + blockIdx.x * kTI + (threadIdx.x & 31);
   const int j = 2 + blockIdx.y * kTJ + (threadIdx.x >> 5);
-  const int k0 = 2 + blockIdx.z * kColRows;
+  const int k0 = 2 + (blockIdx.z - b * nzb) * kColRows;
   double rr = 0.0, ff = 0.0;
   if (i <= L.nx + 1 && j <= L.ny + 1) {
     const double* cx1 = cx1p(L);
@@ -77,17 +90,22 @@ __global__ void __launch_bounds__(kTI * kTJ) k_col_resid_store(DevLevel<double> 
   const double s1 = col_block_sum(rr, sh);
   const double s2 = col_block_sum(ff, sh);
   if (threadIdx.x == 0) {
-    const int64_t b = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
-    part[2 * b] = s1;
-    part[2 * b + 1] = s2;
+    const int64_t q = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
+    part[2 * q] = s1;
+    part[2 * q + 1] = s2;
   }
 }
 
 __global__ void __launch_bounds__(kTI * kTJ) k_col_add_correction(DevLevel<double> L, double* __restrict__ phi,
-                                                                ColLevel E) {
+                                                                ColLevel Eb, const MemberIO* __restrict__ mt) {
+  const int nzb = L.nz / kColRows;
+  const int b = blockIdx.z / nzb;
+  if (!col_active(Eb, b)) return;
+  if (mt) phi = mt[b].phi;
+  const ColLevel E = col_member(Eb, b);
   const int i = 2 + blockIdx.x * kTI + (threadIdx.x & 31);
   const int j = 2 + blockIdx.y * kTJ + (threadIdx.x >> 5);
-  const int k0 = 2 + blockIdx.z * kColRows;
+  const int k0 = 2 + (blockIdx.z - b * nzb) * kColRows;
   if (i > L.nx + 1 || j > L.ny + 1) return;
   const float4* e4 = reinterpret_cast<const float4*>(E.phi + col_cell(E, i, j, k0));
   float e[kColRows];
@@ -107,9 +125,9 @@ __global__ void __launch_bounds__(kTI * kTJ) k_col_add_correction(DevLevel<doubl
   for (int q = 0; q < kColRows; ++q) phi[c + q * XY] = p[q] + (double)e[q];
 }
 
-static dim3 col_tiles(const DevLevel<double>& L) {
+static dim3 col_tiles(const DevLevel<double>& L, int nm = 1) {
   return dim3((unsigned)((L.nx + kTI - 1) / kTI), (unsigned)((L.ny + kTJ - 1) / kTJ),
-              (unsigned)(L.nz / kColRows));
+              (unsigned)(L.nz / kColRows * nm));
 }
 
 int64_t col_resid_part_doubles(const DevLevel<double>& L) {
@@ -121,13 +139,48 @@ void launch_col_resid_store(const DevLevel<double>& L, const double* phi, const 
                             const ColLevel& E, double* part, double* out, cudaStream_t s) {
   const dim3 g = col_tiles(L);
   const int64_t n = (int64_t)g.x * g.y * g.z;
-  k_col_resid_store<<<g, kTI * kTJ, 0, s>>>(L, phi, f, E, part);
+  k_col_resid_store<<<g, kTI * kTJ, 0, s>>>(L, phi, f, E, part, nullptr);
   count_launch();
   launch_fold_pairs(part, n, part + 2 * n, out, s);
 }
 
 void launch_col_add_correction(const DevLevel<double>& L, double* phi, const ColLevel& E, cudaStream_t s) {
-  k_col_add_correction<<<col_tiles(L), kTI * kTJ, 0, s>>>(L, phi, E);
+  k_col_add_correction<<<col_tiles(L), kTI * kTJ, 0, s>>>(L, phi, E, nullptr);
+  count_launch();
+}
+
+int64_t col_resid_part_doubles_members(const DevLevel<double>& L, int nm) {
+  const dim3 g = col_tiles(L);
+  return nm * (2 * (int64_t)g.x * g.y * g.z + fold_scratch_doubles());
+}
+
+void launch_col_resid_store_members(const DevLevel<double>& L, const MemberIO* mt, const ColLevel& E,
+                                    double* part, double* out, cudaStream_t s) {
+  const dim3 g1 = col_tiles(L);
+  const int64_t n = (int64_t)g1.x * g1.y * g1.z;  // blocks of one member
+  k_col_resid_store<<<col_tiles(L, E.nm), kTI * kTJ, 0, s>>>(L, nullptr, nullptr, E, part, mt);
+  count_launch();
+  // member b's partials are the b-th run of n pairs (blockIdx.z runs over
+  // the members' z-blocks in member order)
+  launch_fold_pairs_members(part, n, 2 * n, part + 2 * n * E.nm, out, E.nm, s);
+}
+
+void launch_col_add_correction_members(const DevLevel<double>& L, const MemberIO* mt, const ColLevel& E,
+                                       cudaStream_t s) {
+  k_col_add_correction<<<col_tiles(L, E.nm), kTI * kTJ, 0, s>>>(L, nullptr, E, mt);
+  count_launch();
+}
+
+// ghost pass of every active member's FP64 phi (blockIdx.y: member)
+__global__ void k_bdry_members(DevLevel<double> L, const MemberIO* __restrict__ mt, const int* __restrict__ act) {
+  const int b = blockIdx.y;
+  if (act && !act[b]) return;
+  bdry_range(L, mt[b].phi, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+}
+
+void launch_bdry_members(const DevLevel<double>& L, const MemberIO* mt, const int* act, int nm, cudaStream_t s) {
+  const int64_t ng = L.G - (int64_t)L.nx * L.ny * L.nz;
+  k_bdry_members<<<dim3((unsigned)gs_blocks(ng), (unsigned)nm), 256, 0, s>>>(L, mt, act);
   count_launch();
 }
 

@@ -122,8 +122,12 @@ __global__ void __launch_bounds__(kResidX) k_resid_norm(DevLevel<double> L, cons
 }
 
 // part[0..2n) -> out2[0..2*gridDim.x): CTA b sums its contiguous chunk
-__global__ void k_fold_chunks(const double* __restrict__ part, int64_t n, double* __restrict__ out2) {
+// (blockIdx.y: member of a batch, its arrays pstride / ostride doubles on)
+__global__ void k_fold_chunks(const double* __restrict__ part, int64_t n, double* __restrict__ out2,
+                              int64_t pstride = 0, int64_t ostride = 0) {
   __shared__ double sh[kNormThreads / 32];
+  part += blockIdx.y * pstride;
+  out2 += blockIdx.y * ostride;
   const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
   const int64_t b0 = blockIdx.x * chunk;
   const int64_t b1 = b0 + chunk < n ? b0 + chunk : n;
@@ -140,8 +144,10 @@ __global__ void k_fold_chunks(const double* __restrict__ part, int64_t n, double
   }
 }
 
-__global__ void k_fold(const double* __restrict__ part, int nb, double* out) {
+__global__ void k_fold(const double* __restrict__ part, int nb, double* out, int64_t pstride = 0) {
   __shared__ double sh[kNormThreads / 32];
+  part += blockIdx.x * pstride;
+  out += 2 * blockIdx.x;
   double a = 0.0, b = 0.0;
   for (int q = threadIdx.x; q < nb; q += blockDim.x) {
     a += part[2 * q];
@@ -182,6 +188,13 @@ int64_t fold_scratch_doubles() { return 2 * (int64_t)kFoldBlocks; }
 void launch_fold_pairs(const double* part, int64_t n, double* scratch, double* out, cudaStream_t s) {
   k_fold_chunks<<<kFoldBlocks, kNormThreads, 0, s>>>(part, n, scratch);
   k_fold<<<1, kNormThreads, 0, s>>>(scratch, kFoldBlocks, out);
+  count_launch(2);
+}
+
+void launch_fold_pairs_members(const double* part, int64_t n, int64_t pstride, double* scratch, double* out,
+                               int nm, cudaStream_t s) {
+  k_fold_chunks<<<dim3(kFoldBlocks, nm), kNormThreads, 0, s>>>(part, n, scratch, pstride, 2 * kFoldBlocks);
+  k_fold<<<nm, kNormThreads, 0, s>>>(scratch, kFoldBlocks, out, 2 * kFoldBlocks);
   count_launch(2);
 }
 

@@ -358,6 +358,7 @@ MGSolver::~MGSolver() {
   }
   direct_free(dir_);
   direct_free(dirfine_);
+  batch_free();
   if (h_err_) cudaFreeHost(h_err_);
   if (gsolve_) cudaGraphExecDestroy(gsolve_);
   if (side_) cudaStreamDestroy(side_);
@@ -1078,12 +1079,18 @@ int MGSolver::upload_coefficients() {
                                  cudaMemcpyHostToDevice));
       }
     }
+  uint64_t h = 1469598103934665603ull;  // FNV-1a over every level's coefficients
   for (int l = 1; l <= ngrid_; ++l) {
     const LevelCoef& c = coef_[l];
     std::vector<double> packed;
     for (const std::vector<double>* v :
          {&c.cx1, &c.cx2, &c.cy3, &c.cy4, &c.cz5, &c.cz6, &c.dz5, &c.dz6})
       packed.insert(packed.end(), v->begin(), v->end());
+    const unsigned char* pb = reinterpret_cast<const unsigned char*>(packed.data());
+    for (size_t q = 0; q < packed.size() * sizeof(double); ++q) {
+      h ^= pb[q];
+      h *= 1099511628211ull;
+    }
     ANEL_CUDA_TRY(cudaMemcpy(d_coef64_[l], packed.data(), packed.size() * sizeof(double),
                              cudaMemcpyHostToDevice));
     if (d_coef32_[l]) {
@@ -1092,6 +1099,7 @@ int MGSolver::upload_coefficients() {
                                cudaMemcpyHostToDevice));
     }
   }
+  op_hash_ = h;
   return ANEL_OK;
 }
 
@@ -1311,9 +1319,9 @@ void MGSolver::cycle32(cudaStream_t s) {
 // The FP32 cycle on the column layout: cycle32's schedule, the boundary
 // pass after each prolongation folded into the prolongation, the coarse
 // correction zeroed before each restriction.
-void MGSolver::relax_col(int l, int iters, cudaStream_t s) {
-  const ColLevel L = C32(l);
-  const bool prof = prof_ && l == ngrid_;
+void MGSolver::relax_col(int l, int iters, cudaStream_t s, int nb) {
+  const ColLevel L = nb > 0 ? C32b(l, nb) : C32(l);
+  const bool prof = prof_ && l == ngrid_ && nb == 0;
   for (int it = 0; it < iters; ++it)
     for (int color = 0; color < 2; ++color) {
       if (prof) prof_begin(s);
@@ -1322,33 +1330,45 @@ void MGSolver::relax_col(int l, int iters, cudaStream_t s) {
     }
 }
 
-void MGSolver::cycle_col(cudaStream_t s) {
+void MGSolver::cycle_col(cudaStream_t s, int nb) {
   const int ng = ngrid_;
   const int* pre = prm_.pre_relax;
   const int* post = prm_.post_relax;
+  auto C = [&](int l) { return nb > 0 ? C32b(l, nb) : C32(l); };
   auto down = [&](int l) {
-    cudaMemsetAsync(d_phi32_[l - 1], 0, fp32_elems(l - 1) * sizeof(float), s);
-    launch_col_restrict(C32(l), C32(l - 1), coarsen_dirs(l - 1), s);
+    float* ph = nb > 0 ? d_bphi32_[l - 1] : d_phi32_[l - 1];
+    cudaMemsetAsync(ph, 0, fp32_elems(l - 1) * (nb > 0 ? nb : 1) * sizeof(float), s);
+    launch_col_restrict(C(l), C(l - 1), coarsen_dirs(l - 1), s);
   };
   // with a direct level L0 the levels below it are never visited: L0 is
   // solved exactly in place of its relaxation and of the coarser cycle
   const int L0 = dirL_ > 0 ? dirL_ : 1;
-  relax_col(ng, pre[ng - 1], s);
+  relax_col(ng, pre[ng - 1], s, nb);
   for (int l = ng; l > L0; --l) {
-    if (l < ng) relax_col(l, pre[l - 1], s);
+    if (l < ng) relax_col(l, pre[l - 1], s, nb);
     down(l);
   }
   if (dirL_ > 0) {
-    launch_direct_col(dir_.f, C32(L0), s);
+    launch_direct_col(dir_.f, C(L0), nb > 0 ? d_bdir_ : nullptr, s);
   } else {
-    relax_col(1, pre[0], s);
-    relax_col(1, post[0], s);
+    relax_col(1, pre[0], s, nb);
+    relax_col(1, post[0], s, nb);
   }
   for (int l = L0; l < ng; ++l) {
-    if (l > L0) relax_col(l, post[l - 1], s);
-    launch_col_prolong(C32(l + 1), C32(l), coarsen_dirs(l), s);
+    if (l > L0) relax_col(l, post[l - 1], s, nb);
+    launch_col_prolong(C(l + 1), C(l), coarsen_dirs(l), s);
   }
-  relax_col(ng, post[ng - 1], s);
+  relax_col(ng, post[ng - 1], s, nb);
+}
+
+ColLevel MGSolver::C32b(int l, int nb) const {
+  ColLevel L = C32(l);
+  L.phi = d_bphi32_[l];
+  L.src = d_bsrc32_[l];
+  L.nm = nb;
+  L.ms = fp32_elems(l);
+  L.act = d_bact_;
+  return L;
 }
 
 SegFac<float> MGSolver::segfac32(int l) const {
@@ -1748,6 +1768,252 @@ int MGSolver::solve_mixed_graph(double* d_phi, const double* d_rhs, cudaStream_t
   rep->relmax = rel;
   rep->resid = rel;
   return conv ? ANEL_OK : ANEL_ERR_NOCONV;
+}
+
+// ------------------------------------------------------- batched solve
+// Members of a batch share this solver's levels, coefficients, factors and
+// tuned launch variants; each has its own FP32 levels (d_bphi32_ /
+// d_bsrc32_, member b at b * fp32_elems(l)), direct-solve work, partial
+// sums, norms and convergence state.  Every kernel takes the member from
+// its work index and skips members whose act flag is 0, so a member's
+// arithmetic is that of the one-member solve, whatever else is in the
+// batch.
+
+struct BatchConv {
+  double rel;
+  int iter;
+  int conv;
+};
+
+__global__ void k_fill_int(int* a, int n, int v) {
+  for (int q = threadIdx.x; q < n; q += blockDim.x) a[q] = v;
+}
+
+__global__ void k_bconv_init(const double* norm, BatchConv* st, int* act, int n, double tol, int maxcy,
+                             cudaGraphConditionalHandle h) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int b = threadIdx.x; b < n; b += blockDim.x) {
+    const double rel = conv_rel(norm + 2 * b);
+    const int c = rel <= tol;
+    st[b].rel = rel;
+    st[b].iter = 0;
+    st[b].conv = c;
+    const int a = (!c && maxcy > 0) ? 1 : 0;
+    act[b] = a;
+    if (a) atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+__global__ void k_bconv_step(const double* norm, BatchConv* st, int* act, int n, double tol, int maxcy,
+                             cudaGraphConditionalHandle h) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int b = threadIdx.x; b < n; b += blockDim.x) {
+    if (!act[b]) continue;  // stopped in an earlier cycle: its state stays
+    const double rel = conv_rel(norm + 2 * b);
+    const int it = st[b].iter + 1;
+    const int c = rel <= tol;
+    st[b].rel = rel;
+    st[b].iter = it;
+    st[b].conv = c;
+    const int a = (!c && it < maxcy) ? 1 : 0;
+    act[b] = a;
+    if (a) atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+bool MGSolver::batch_capable() const {
+  return col_ && prm_.precision == ANEL_PREC_MIXED && gsolve_state_ >= 0;
+}
+
+void MGSolver::batch_free() {
+  if (bgraph_) cudaGraphExecDestroy(bgraph_);
+  bgraph_ = nullptr;
+  bgraph_n_ = 0;
+  for (int l = 0; l <= ANEL_MAX_LEVELS; ++l) {
+    cudaFree(d_bphi32_[l]);
+    cudaFree(d_bsrc32_[l]);
+    d_bphi32_[l] = d_bsrc32_[l] = nullptr;
+  }
+  cudaFree(d_bdir_);
+  cudaFree(d_bpart_);
+  cudaFree(d_bnorm_);
+  cudaFree(d_bmt_);
+  cudaFree(d_bact_);
+  cudaFree(d_bconv_);
+  if (h_bmt_) cudaFreeHost(h_bmt_);
+  if (h_bconv_) cudaFreeHost(h_bconv_);
+  d_bdir_ = d_bpart_ = d_bnorm_ = nullptr;
+  d_bmt_ = h_bmt_ = nullptr;
+  d_bact_ = nullptr;
+  d_bconv_ = h_bconv_ = nullptr;
+  bcap_ = 0;
+}
+
+int MGSolver::batch_reserve(int n) {
+  if (n <= bcap_) return ANEL_OK;
+  ANEL_CUDA_TRY(cudaStreamSynchronize(stream_));
+  batch_free();
+  for (int l = 1; l <= ngrid_; ++l) {
+    const size_t b = (size_t)fp32_elems(l) * n * sizeof(float);
+    ANEL_CUDA_TRY(cudaMalloc(&d_bphi32_[l], b));
+    ANEL_CUDA_TRY(cudaMalloc(&d_bsrc32_[l], b));
+    ANEL_CUDA_TRY(cudaMemset(d_bphi32_[l], 0, b));
+    ANEL_CUDA_TRY(cudaMemset(d_bsrc32_[l], 0, b));
+  }
+  if (dirL_ > 0) {
+    const DirectFac& F = dir_.f;
+    ANEL_CUDA_TRY(cudaMalloc(&d_bdir_, (size_t)n * F.nm * F.nz * sizeof(double)));
+  }
+  ANEL_CUDA_TRY(cudaMalloc(&d_bpart_, (size_t)col_resid_part_doubles_members(L64(ngrid_), n) * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_bnorm_, (size_t)2 * n * sizeof(double)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_bmt_, (size_t)n * sizeof(MemberIO)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_bact_, (size_t)n * sizeof(int)));
+  ANEL_CUDA_TRY(cudaMalloc(&d_bconv_, (size_t)n * sizeof(BatchConv)));
+  ANEL_CUDA_TRY(cudaHostAlloc(&h_bmt_, (size_t)n * sizeof(MemberIO), cudaHostAllocDefault));
+  ANEL_CUDA_TRY(cudaHostAlloc(&h_bconv_, (size_t)n * sizeof(BatchConv), cudaHostAllocDefault));
+  bcap_ = n;
+  return ANEL_OK;
+}
+
+int MGSolver::build_batch_graph(int n, cudaStream_t s) {
+  if (bgraph_) {
+    cudaGraphExecDestroy(bgraph_);
+    bgraph_ = nullptr;
+    bgraph_n_ = 0;
+  }
+  if (!side_) ANEL_CUDA_TRY(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+  const int ng = ngrid_;
+  const DevLevel<double> Fu = L64(ng);  // geometry only: the arrays come from the member table
+  const ColLevel Ec = C32b(ng, n);
+  BatchConv* cs = static_cast<BatchConv*>(d_bconv_);
+  const double tol = prm_.tolmax;
+  const int maxcy = prm_.maxcy;
+  cudaGraph_t g = nullptr;
+  bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
+  cudaGraphConditionalHandle h{};
+  if (ok) ok = cudaGraphConditionalHandleCreate(&h, g, 0, 0) == cudaSuccess;
+  const int64_t l0 = t_launches;
+  if (ok) ok = cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+               cudaSuccess;
+  cudaGraph_t body = nullptr;
+  if (ok) {
+    // head: every member active for the boundary pass and first defect
+    k_fill_int<<<1, 256, 0, s>>>(d_bact_, n, 1);
+    launch_bdry_members(Fu, d_bmt_, d_bact_, n, s);
+    launch_col_resid_store_members(Fu, d_bmt_, Ec, d_bpart_, d_bnorm_, s);
+    k_bconv_init<<<1, 256, 0, s>>>(d_bnorm_, cs, d_bact_, n, tol, maxcy, h);
+    count_launch(2);
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    ok = cudaStreamGetCaptureInfo(s, &cst, nullptr, nullptr, &deps, &ndeps) == cudaSuccess &&
+         cst == cudaStreamCaptureStatusActive;
+    cudaGraphNode_t cnode = nullptr;
+    if (ok) {
+      cudaGraphNodeParams cp{};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      ok = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp) == cudaSuccess;
+      if (ok) body = cp.conditional.phGraph_out[0];
+      if (ok) ok = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies) ==
+                   cudaSuccess;
+    }
+    cudaGraph_t gout = nullptr;
+    const bool ended = cudaStreamEndCapture(s, &gout) == cudaSuccess;
+    ok = ok && ended;
+  }
+  bgraph_head_launches_ = t_launches - l0;
+  // body: one FP32 cycle of every active member, its correction, its next
+  // defect and the per-member tests
+  const int64_t l1 = t_launches;
+  if (ok) ok = cudaStreamBeginCaptureToGraph(side_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+               cudaSuccess;
+  if (ok) {
+    cudaMemsetAsync(d_bphi32_[ng], 0, fp32_elems(ng) * n * sizeof(float), side_);
+    cycle_col(side_, n);
+    launch_col_add_correction_members(Fu, d_bmt_, Ec, side_);
+    launch_bdry_members(Fu, d_bmt_, d_bact_, n, side_);
+    launch_col_resid_store_members(Fu, d_bmt_, Ec, d_bpart_, d_bnorm_, side_);
+    k_bconv_step<<<1, 256, 0, side_>>>(d_bnorm_, cs, d_bact_, n, tol, maxcy, h);
+    count_launch();
+    cudaGraph_t gout = nullptr;
+    ok = cudaStreamEndCapture(side_, &gout) == cudaSuccess;
+  }
+  bgraph_body_launches_ = t_launches - l1;
+  g_launches.fetch_sub(bgraph_head_launches_ + bgraph_body_launches_, std::memory_order_relaxed);
+  t_launches -= bgraph_head_launches_ + bgraph_body_launches_;
+  if (ok) ok = cudaGraphInstantiate(&bgraph_, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  if (!ok) {
+    cudaGetLastError();
+    bgraph_ = nullptr;
+    set_error("batched solve: CUDA graph capture failed");
+    return ANEL_ERR_CUDA;
+  }
+  bgraph_n_ = n;
+  return ANEL_OK;
+}
+
+int MGSolver::solve_batch(int n, double* const* phis, const double* const* rhss, cudaStream_t s,
+                          anel_mg_report* reps) {
+  if (n < 1 || !phis || !rhss || !reps) {
+    set_error("solve_batch: n >= 1 and non-null member arrays required");
+    return ANEL_ERR_ARG;
+  }
+  if (!batch_capable()) {
+    set_error("solve_batch: needs the column-layout mixed-precision z-line cycle");
+    return ANEL_ERR_UNSUPPORTED;
+  }
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  for (int b = 0; b < n; ++b)
+    if (!phis[b] || !rhss[b]) {
+      set_error("solve_batch: member %d has a null array", b);
+      return ANEL_ERR_ARG;
+    }
+  int st = batch_reserve(n);
+  if (st != ANEL_OK) return st;
+  if (bgraph_n_ != n) {
+    st = build_batch_graph(n, s);
+    if (st != ANEL_OK) return st;
+  }
+  for (int b = 0; b < n; ++b) h_bmt_[b] = MemberIO{phis[b], rhss[b]};
+  ANEL_CUDA_TRY(cudaMemcpyAsync(d_bmt_, h_bmt_, (size_t)n * sizeof(MemberIO), cudaMemcpyHostToDevice, s));
+  ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
+  ANEL_CUDA_TRY(cudaGraphLaunch(bgraph_, s));
+  ANEL_CUDA_TRY(cudaEventRecord(ev1_, s));
+  ANEL_CUDA_TRY(cudaMemcpyAsync(h_bconv_, d_bconv_, (size_t)n * sizeof(BatchConv), cudaMemcpyDeviceToHost, s));
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  ANEL_CUDA_TRY(cudaEventElapsedTime(&ms, ev0_, ev1_));
+  st = take_kernel_error("batched solve");
+  if (st != ANEL_OK) return st;
+  const BatchConv* cv = static_cast<const BatchConv*>(h_bconv_);
+  int itmax = 0, rc = ANEL_OK;
+  for (int b = 0; b < n; ++b) {
+    anel_mg_report& r = reps[b];
+    r = anel_mg_report{};
+    const bool conv = cv[b].conv != 0;
+    r.iter = conv ? cv[b].iter : prm_.maxcy + 1;
+    r.relmax = cv[b].rel;
+    r.resid = cv[b].rel;
+    r.status = conv ? ANEL_OK : ANEL_ERR_NOCONV;
+    r.ms = ms;
+    itmax = std::max(itmax, cv[b].iter);
+    if (!conv) rc = ANEL_ERR_NOCONV;
+  }
+  count_launch(bgraph_head_launches_ + (int64_t)itmax * bgraph_body_launches_);
+  return rc;
 }
 
 int MGSolver::solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s,

@@ -29,6 +29,23 @@ class MGSolver {
   // Same with host arrays (copies in and out through pinned staging).
   int solve_host(double* phi, const double* rhs, cudaStream_t s, anel_mg_report* rep);
 
+  // n independent problems on this solver's grid (same operator), each
+  // phis[b] / rhss[b] a device array pair as for solve_device, solved
+  // together: every kernel of the mixed z-line cycle runs over all members
+  // still iterating (one launch per level step for the whole batch, the
+  // defect-correction loop inside one CUDA graph per batch size), each
+  // member stopping at its own tolerance test.  Member b's result and
+  // report are those of solve_device on it alone.  Needs the column-layout
+  // mixed cycle (batch_capable); reps: n reports.
+  int solve_batch(int n, double* const* phis, const double* const* rhss, cudaStream_t s,
+                  anel_mg_report* reps);
+  bool batch_capable() const;
+  // room for batches of up to n members (solve_batch grows it on demand)
+  int batch_reserve(int n);
+  // identifies the operator: a hash of every level's coefficients (equal
+  // for solvers of one grid, parameters and density profile)
+  uint64_t operator_hash() const { return op_hash_; }
+
   int debug_pass(int which, double* d_phi, const double* d_src, cudaStream_t s);
   int set_profiling(bool on);
   int levels_table(int32_t* out, int cap) const;
@@ -79,8 +96,29 @@ class MGSolver {
   void choose_direct_level();
   ColLevel C32(int l) const;
   int64_t fp32_elems(int l) const;
-  void relax_col(int l, int iters, cudaStream_t s);
-  void cycle_col(cudaStream_t s);
+  // nb = 0: this solver's own FP32 levels; nb >= 1: the first nb members of
+  // the batch levels
+  void relax_col(int l, int iters, cudaStream_t s, int nb = 0);
+  void cycle_col(cudaStream_t s, int nb = 0);
+  ColLevel C32b(int l, int nb) const;
+  // batch state (solve_batch): capacity, FP32 levels and direct-solve work
+  // of bcap_ members, member table, active flags, norms, convergence states
+  int bcap_ = 0;
+  float* d_bphi32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  float* d_bsrc32_[ANEL_MAX_LEVELS + 1] = {nullptr};
+  double* d_bdir_ = nullptr;
+  double* d_bpart_ = nullptr;
+  double* d_bnorm_ = nullptr;
+  MemberIO* d_bmt_ = nullptr;
+  MemberIO* h_bmt_ = nullptr;  // pinned staging of the member table
+  int* d_bact_ = nullptr;
+  void* d_bconv_ = nullptr;
+  void* h_bconv_ = nullptr;    // pinned readback of the states
+  cudaGraphExec_t bgraph_ = nullptr;
+  int bgraph_n_ = 0;
+  int64_t bgraph_head_launches_ = 0, bgraph_body_launches_ = 0;
+  void batch_free();
+  int build_batch_graph(int n, cudaStream_t s);
   int solve_fp64(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
   int solve_mixed(double* d_phi, const double* d_rhs, cudaStream_t s, anel_mg_report* rep);
   // the mixed solve as one CUDA graph: the defect-correction loop is a
@@ -101,6 +139,7 @@ class MGSolver {
   double true_resid(const double* d_phi, const double* d_rhs, cudaStream_t s, double* fnorm);
 
   anel_mg_params prm_{};
+  uint64_t op_hash_ = 0;
   int device_ = 0;
   cudaStream_t stream_ = nullptr;
   int nx_ = 0, ny_ = 0, nz_ = 0;

@@ -518,10 +518,10 @@ int NSSolver::get_fields(const anel_fields* f, int mem, cudaStream_t s) {
 }
 
 // --------------------------------------------------------------- rk_ss
-int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, cudaStream_t s,
-                      int* iters, double* relmax, bool q_zero) {
-  ANEL_CUDA_TRY(cudaSetDevice(device_));
-  if (!s) s = stream_;
+// rk_ss (NSsolver.F90:418-583) in two halves around the pressure solve:
+// RHS, Crank-Nicolson columns and Psource, then (after the solve) Pgrad.
+int NSSolver::substep_pre(double a1, double a2, double a3, double dt_rk, double dt, cudaStream_t s,
+                          bool q_zero) {
   // slot of the factor cache (three rkdt values per step)
   int slot = -1;
   for (int q = 0; q < 3; ++q)
@@ -560,21 +560,35 @@ int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, 
     ANEL_CUDA_TRY(cudaStreamWaitEvent(s, io_ev_[0], 0));
     io_wait_p_ = false;
   }
-  anel_mg_report rep{};
-  const int st = mg_->solve_device(D_.p, D_.psrc, s, &rep);
-  if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
+  pend_dtrk_ = dt_rk;
+  return ANEL_OK;
+}
+
+int NSSolver::substep_post(const anel_mg_report& rep, cudaStream_t s, int* iters, double* relmax) {
   if (io_last_sub_ && io_out_ && io_out_->p) {  // p is final: copy it out during Pgrad
     ANEL_CUDA_TRY(cudaEventRecord(io_ev_[2], s));
     ANEL_CUDA_TRY(cudaStreamWaitEvent(io_stream_, io_ev_[2], 0));
-    ANEL_CUDA_TRY(cudaMemcpyAsync(io_out_->p, D_.p, fb, cudaMemcpyDeviceToHost, io_stream_));
+    ANEL_CUDA_TRY(cudaMemcpyAsync(io_out_->p, D_.p, G_ * sizeof(double), cudaMemcpyDeviceToHost, io_stream_));
   }
   acc_mg_ms_ += rep.ms;
   acc_sweep_ms_ += rep.fine_sweep_ms;
   acc_sweeps_ += rep.fine_sweeps;
-  launch_pgrad(D_, dt_rk, ru, rv, rw, s);
+  launch_pgrad(D_, pend_dtrk_, zrule(NV_U), zrule(NV_V), zrule(NV_W), s);
   if (iters) *iters = rep.iter;
   if (relmax) *relmax = rep.relmax;
   return check_launch("rk substep");
+}
+
+int NSSolver::substep(double a1, double a2, double a3, double dt_rk, double dt, cudaStream_t s,
+                      int* iters, double* relmax, bool q_zero) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  int st = substep_pre(a1, a2, a3, dt_rk, dt, s, q_zero);
+  if (st != ANEL_OK) return st;
+  anel_mg_report rep{};
+  st = mg_->solve_device(D_.p, D_.psrc, s, &rep);
+  if (st != ANEL_OK && st != ANEL_ERR_NOCONV) return st;
+  return substep_post(rep, s, iters, relmax);
 }
 
 int NSSolver::reset(const anel_ns_params* ns, cudaStream_t s) {
@@ -706,11 +720,86 @@ double NSSolver::calcdt(cudaStream_t s, int* st) {
   return dt;
 }
 
+static const double kA1[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+static const double kA3[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+
+// Start of a step (NSsolver.F90:63-164): zero_temps, calcdt, gravity, the
+// LES coefficients on their cadence and the scalar smoothing.
+int NSSolver::step_begin(cudaStream_t s, double* delt_out) {
+  // zero_temps (memManage.F90:844-853).  The accumulators q_u, q_v,
+  // q_w, q_rho, q_s are written, never read, by the first sub-step
+  // (a1 = 0) on every interior cell, and no kernel writes their ghost
+  // cells, so once zeroed they need no zeroing again until set_fields,
+  // reset or a scratch use touches them (temps_clean_); the Poisson
+  // right-hand side is zeroed every step.
+  for (int q : {8, 9, 10, 11, 12, 13})
+    if (q == 13 || !temps_clean_) ANEL_CUDA_TRY(cudaMemsetAsync(d_fields_[q], 0, G_ * sizeof(double), s));
+  temps_clean_ = true;
+  int st = ANEL_OK;
+  const double delt = calcdt(s, &st);
+  if (st != ANEL_OK) return st;
+  // gravity (Routines.F90:27-52)
+  if (time_ < prm_.gt1) gnow_ = 0.0;
+  else if (time_ > prm_.gt1 && time_ < prm_.gt2) gnow_ = g_orig_ * (time_ - prm_.gt1) / (prm_.gt2 - prm_.gt1);
+  else if (time_ >= prm_.gt2) gnow_ = g_orig_;
+  // LES model coefficients and eddy viscosities (NSsolver.F90:86-100):
+  // les_coeffs on the step cadence, SGSdiff before every sub-step
+  const bool les = D_.vles != 0;
+  if (les && nstep_ >= prm_.les_start && nstep_ % prm_.les_freq == 0) {
+    st = les_coeffs(s);
+    if (st != ANEL_OK) return st;
+  }
+  // the scalar models' smoothing of rho and scal1 every 50 steps
+  // (NSsolver.F90:144-164), after the coefficients, before SGSdiff
+  if (time_ > 0.0 && nstep_ % 50 == 0 && (D_.rles || D_.sles)) {
+    st = smooth_scalars(s);
+    if (st != ANEL_OK) return st;
+  }
+  *delt_out = delt;
+  return ANEL_OK;
+}
+
+// End of a step: the clock (NSsolver.F90:272-274) and the diagnostics.
+int NSSolver::step_end(double delt, cudaStream_t s, anel_step_report* r) {
+  told_ = time_;  // told = time; time = time + delt
+  time_ = time_ + delt;
+  if (diag_on_) {
+    int st = ensure_diag();
+    if (st != ANEL_OK) return st;
+    ANEL_CUDA_TRY(cudaEventRecord(dev0_, s));
+    st = compute_diagnostics(s);
+    if (st != ANEL_OK) return st;
+    ANEL_CUDA_TRY(cudaEventRecord(dev1_, s));
+    ANEL_CUDA_TRY(cudaEventSynchronize(dev1_));
+    float dms = 0.f;
+    cudaEventElapsedTime(&dms, dev0_, dev1_);
+    acc_diag_ms_ += dms;
+  }
+  r->nstep = nstep_;
+  r->dt = delt;
+  r->time = time_;
+  nstep_ += 1;
+  return ANEL_OK;
+}
+
+// After the last step: accumulated times and the divergence check.
+int NSSolver::step_finish(cudaStream_t s, int64_t launches0, anel_step_report* r) {
+  r->mg_ms = acc_mg_ms_;
+  r->fine_sweep_ms = acc_sweep_ms_;
+  r->fine_sweeps = acc_sweeps_;
+  r->diag_ms = acc_diag_ms_;
+  r->launches = t_launches - launches0;
+  double dv[2];
+  const int st = divergence(s, dv);
+  if (st != ANEL_OK) return st;
+  r->avg_div = dv[0];
+  r->max_div = dv[1];
+  return ANEL_OK;
+}
+
 int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   ANEL_CUDA_TRY(cudaSetDevice(device_));
   if (!s) s = stream_;
-  static const double A1[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
-  static const double A3[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
   anel_step_report r{};
   acc_mg_ms_ = acc_sweep_ms_ = 0.0;
   acc_diag_ms_ = 0.0;
@@ -718,78 +807,112 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
   const int64_t launches0 = t_launches;
   ANEL_CUDA_TRY(cudaEventRecord(ev0_, s));
   for (int n = 0; n < nsteps; ++n) {
-    // zero_temps (memManage.F90:844-853).  The accumulators q_u, q_v,
-    // q_w, q_rho, q_s are written, never read, by the first sub-step
-    // (a1 = 0) on every interior cell, and no kernel writes their ghost
-    // cells, so once zeroed they need no zeroing again until set_fields,
-    // reset or a scratch use touches them (temps_clean_); the Poisson
-    // right-hand side is zeroed every step.
-    for (int q : {8, 9, 10, 11, 12, 13})
-      if (q == 13 || !temps_clean_) ANEL_CUDA_TRY(cudaMemsetAsync(d_fields_[q], 0, G_ * sizeof(double), s));
-    temps_clean_ = true;
-    int st = ANEL_OK;
-    const double delt = calcdt(s, &st);
+    double delt = 0.0;
+    int st = step_begin(s, &delt);
     if (st != ANEL_OK) return st;
-    // gravity (Routines.F90:27-52)
-    if (time_ < prm_.gt1) gnow_ = 0.0;
-    else if (time_ > prm_.gt1 && time_ < prm_.gt2) gnow_ = g_orig_ * (time_ - prm_.gt1) / (prm_.gt2 - prm_.gt1);
-    else if (time_ >= prm_.gt2) gnow_ = g_orig_;
-    // LES model coefficients and eddy viscosities (NSsolver.F90:86-100):
-    // les_coeffs on the step cadence, SGSdiff before every sub-step
     const bool les = D_.vles != 0;
-    if (les && nstep_ >= prm_.les_start && nstep_ % prm_.les_freq == 0) {
-      st = les_coeffs(s);
-      if (st != ANEL_OK) return st;
-    }
-    // the scalar models' smoothing of rho and scal1 every 50 steps
-    // (NSsolver.F90:144-164), after the coefficients, before SGSdiff
-    if (time_ > 0.0 && nstep_ % 50 == 0 && (D_.rles || D_.sles)) {
-      st = smooth_scalars(s);
-      if (st != ANEL_OK) return st;
-    }
     const double DTR[3] = {1.0 / 3.0 * delt, 5.0 / 12.0 * delt, 1.0 / 4.0 * delt};
     for (int q = 0; q < 3; ++q) {
       if (les && nstep_ > prm_.les_start) launch_sgs(D_, zrule(NV_CFLUC), s);
       io_last_sub_ = io_out_ && n == nsteps - 1 && q == 2;
-      st = substep(A1[q], 1.0, A3[q], DTR[q], delt, s, &r.mg_iter[q], &r.mg_relmax[q], true);
+      st = substep(kA1[q], 1.0, kA3[q], DTR[q], delt, s, &r.mg_iter[q], &r.mg_relmax[q], true);
       io_last_sub_ = false;
       if (st != ANEL_OK) return st;
     }
-    told_ = time_;  // told = time; time = time + delt (NSsolver.F90:272-274)
-    time_ = time_ + delt;
-    if (diag_on_) {
-      st = ensure_diag();
-      if (st != ANEL_OK) return st;
-      ANEL_CUDA_TRY(cudaEventRecord(dev0_, s));
-      st = compute_diagnostics(s);
-      if (st != ANEL_OK) return st;
-      ANEL_CUDA_TRY(cudaEventRecord(dev1_, s));
-      ANEL_CUDA_TRY(cudaEventSynchronize(dev1_));
-      float dms = 0.f;
-      cudaEventElapsedTime(&dms, dev0_, dev1_);
-      acc_diag_ms_ += dms;
-    }
-    r.nstep = nstep_;
-    r.dt = delt;
-    r.time = time_;
-    nstep_ += 1;
+    st = step_end(delt, s, &r);
+    if (st != ANEL_OK) return st;
   }
   ANEL_CUDA_TRY(cudaEventRecord(ev1_, s));
   ANEL_CUDA_TRY(cudaEventSynchronize(ev1_));
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ev0_, ev1_);
   r.ms = ms;
-  r.mg_ms = acc_mg_ms_;
-  r.fine_sweep_ms = acc_sweep_ms_;
-  r.fine_sweeps = acc_sweeps_;
-  r.diag_ms = acc_diag_ms_;
-  r.launches = t_launches - launches0;
-  double dv[2];
-  const int st = divergence(s, dv);
+  const int st = step_finish(s, launches0, &r);
   if (st != ANEL_OK) return st;
-  r.avg_div = dv[0];
-  r.max_div = dv[1];
   if (rep) *rep = r;
+  return ANEL_OK;
+}
+
+int NSSolver::step_cohort(NSSolver* const* ms, int n, int nsteps, MGSolver* bmg, cudaStream_t s,
+                          anel_step_report* reps) {
+  if (n < 1 || !ms || !bmg || !reps) {
+    set_error("step_cohort: n >= 1 members, a batch solver and reports required");
+    return ANEL_ERR_ARG;
+  }
+  for (int b = 0; b < n; ++b) {
+    NSSolver* m = ms[b];
+    const anel_mg_params& a = m ? m->mg_->params() : bmg->params();
+    const anel_mg_params& c = bmg->params();
+    const bool same_mg = a.precision == c.precision && a.smoother == c.smoother && a.maxcy == c.maxcy &&
+                         a.tolmax == c.tolmax && a.stop == c.stop && a.mode == c.mode &&
+                         std::memcmp(a.pre_relax, c.pre_relax, sizeof(a.pre_relax)) == 0 &&
+                         std::memcmp(a.post_relax, c.post_relax, sizeof(a.post_relax)) == 0 &&
+                         std::memcmp(a.levels, c.levels, sizeof(a.levels)) == 0 &&
+                         std::memcmp(a.tbc, c.tbc, sizeof(a.tbc)) == 0 &&
+                         std::memcmp(a.vbc, c.vbc, sizeof(a.vbc)) == 0;
+    if (!m || m->device_ != bmg->device() || m->nx_ != ms[0]->nx_ || m->ny_ != ms[0]->ny_ ||
+        m->nz_ != ms[0]->nz_ || !same_mg || m->mg_->operator_hash() != bmg->operator_hash()) {
+      set_error("step_cohort: member %d differs in grid, device, multigrid parameters or operator", b);
+      return ANEL_ERR_ARG;
+    }
+    if (m->io_out_ || m->io_wait_p_) {
+      set_error("step_cohort: member %d has a host copy pending", b);
+      return ANEL_ERR_ARG;
+    }
+  }
+  ANEL_CUDA_TRY(cudaSetDevice(bmg->device()));
+  if (!s) s = bmg->stream();
+  std::vector<anel_step_report> r(n);
+  std::vector<int64_t> l0(n);
+  std::vector<double> delt(n);
+  std::vector<double*> phis(n);
+  std::vector<const double*> rhss(n);
+  std::vector<anel_mg_report> mrep(n);
+  for (int b = 0; b < n; ++b) {
+    NSSolver* m = ms[b];
+    m->acc_mg_ms_ = m->acc_sweep_ms_ = m->acc_diag_ms_ = 0.0;
+    m->acc_sweeps_ = 0;
+    l0[b] = t_launches;
+    phis[b] = m->D_.p;
+    rhss[b] = m->D_.psrc;
+  }
+  ANEL_CUDA_TRY(cudaEventRecord(ms[0]->ev0_, s));
+  for (int step = 0; step < nsteps; ++step) {
+    for (int b = 0; b < n; ++b) {
+      const int st = ms[b]->step_begin(s, &delt[b]);
+      if (st != ANEL_OK) return st;
+    }
+    for (int q = 0; q < 3; ++q) {
+      for (int b = 0; b < n; ++b) {
+        NSSolver* m = ms[b];
+        if (m->D_.vles && m->nstep_ > m->prm_.les_start) launch_sgs(m->D_, m->zrule(NV_CFLUC), s);
+        const double DTR[3] = {1.0 / 3.0 * delt[b], 5.0 / 12.0 * delt[b], 1.0 / 4.0 * delt[b]};
+        const int st = m->substep_pre(kA1[q], 1.0, kA3[q], DTR[q], delt[b], s, true);
+        if (st != ANEL_OK) return st;
+      }
+      const int sb = bmg->solve_batch(n, phis.data(), rhss.data(), s, mrep.data());
+      if (sb != ANEL_OK && sb != ANEL_ERR_NOCONV) return sb;
+      for (int b = 0; b < n; ++b) {
+        mrep[b].ms /= n;  // the batch's device time, shared out
+        const int st = ms[b]->substep_post(mrep[b], s, &r[b].mg_iter[q], &r[b].mg_relmax[q]);
+        if (st != ANEL_OK) return st;
+      }
+    }
+    for (int b = 0; b < n; ++b) {
+      const int st = ms[b]->step_end(delt[b], s, &r[b]);
+      if (st != ANEL_OK) return st;
+    }
+  }
+  ANEL_CUDA_TRY(cudaEventRecord(ms[0]->ev1_, s));
+  ANEL_CUDA_TRY(cudaEventSynchronize(ms[0]->ev1_));
+  float tms = 0.f;
+  cudaEventElapsedTime(&tms, ms[0]->ev0_, ms[0]->ev1_);
+  for (int b = 0; b < n; ++b) {
+    r[b].ms = tms;
+    const int st = ms[b]->step_finish(s, l0[b], &r[b]);
+    if (st != ANEL_OK) return st;
+    reps[b] = r[b];
+  }
   return ANEL_OK;
 }
 

@@ -21,6 +21,14 @@ class NSSolver {
   int substep(double a1, double a2, double a3, double dt_rk, double dt, cudaStream_t s, int* iters,
               double* relmax, bool q_zero = false);
   int step(int nsteps, cudaStream_t s, anel_step_report* rep);
+  // nsteps RK3 steps of n members (contexts of one grid, boundary setup
+  // and multigrid parameters; physics, time step and state their own) on
+  // stream s, with each sub-step's n pressure solves as one batched solve
+  // of bmg (MGSolver::solve_batch; a solver of the members' grid and
+  // multigrid parameters).  Each member's fields and report are those of
+  // its own step(); reps: n reports.
+  static int step_cohort(NSSolver* const* ms, int n, int nsteps, MGSolver* bmg, cudaStream_t s,
+                         anel_step_report* reps);
   // nsteps from the host state `in` to the host state `out` (may be the
   // same arrays): the fields are copied in, stepped and copied out, with
   // the copy of p in overlapping sub-step 1 up to its pressure solve and
@@ -70,6 +78,14 @@ class NSSolver {
   int cn_factors(int slot, double rkdt, cudaStream_t s);
   ZRule zrule(int vtype) const;
   double calcdt(cudaStream_t s, int* st);
+  // phases of one RK3 step (step() and step_cohort() run them in order;
+  // the pressure solve of each sub-step sits between pre and post)
+  int step_begin(cudaStream_t s, double* delt);
+  int substep_pre(double a1, double a2, double a3, double dt_rk, double dt, cudaStream_t s, bool q_zero);
+  int substep_post(const anel_mg_report& rep, cudaStream_t s, int* iters, double* relmax);
+  int step_end(double delt, cudaStream_t s, anel_step_report* r);
+  int step_finish(cudaStream_t s, int64_t launches0, anel_step_report* r);
+  double pend_dtrk_ = 0.0;  // the sub-step between substep_pre and substep_post
   int les_coeffs(cudaStream_t s);
 
   anel_ns_params prm_{};

@@ -4,9 +4,18 @@
 //
 // Design:
 //   * requests enter a FIFO queue (anel_serve_submit returns at once);
-//   * max_active worker threads each drive one member at a time on the
-//     member's own CUDA stream, so the kernels of different members overlap
-//     on the device (small members leave most SMs idle on their own);
+//   * max_active worker threads each drive one cohort: the members of one
+//     bucket stepping together.  A worker takes the oldest queued member
+//     whose bucket has no cohort running, sets it up (state, initial
+//     projection) and, when its multigrid is the column-layout mixed
+//     z-line cycle, opens a cohort for its bucket; at every step boundary
+//     the cohort admits the bucket's newly queued members (up to
+//     kMaxCohort) and retires those that are done, and one step of all
+//     members is NSSolver::step_cohort: the members' own kernels, and each
+//     sub-step's pressure solves as one batched multigrid solve (every
+//     kernel of the cycle over all members, one CUDA graph per batch
+//     size).  Other members run alone on their own stream.  Workers of
+//     different buckets overlap on the device;
 //   * a member is admitted when the device memory it needs fits the HBM
 //     budget: an idle context of the same bucket (same grid, models,
 //     multigrid and boundary setup) is re-used without allocating;
@@ -17,14 +26,16 @@
 //   * results (status, queue/run/total latency) are collected by
 //     anel_serve_poll.
 // A member's arithmetic does not depend on what else runs: its kernels
-// read and write only its own buffers, so its fields are bit-identical
-// alone and in the mix.
+// read and write only its own buffers, and in a batched solve every kernel
+// takes each member's work in the one-member order, so its fields are
+// bit-identical alone and in the mix.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -65,6 +76,19 @@ struct ServeCtx {
   std::string key;
   int64_t bytes = 0;
   Clock::time_point last_used;
+};
+
+constexpr int kMaxCohort = 16;  // members per cohort (batched solve size)
+
+// a member being served: its job, context, progress and result
+struct Running {
+  ServeJob* job = nullptr;
+  ServeCtx* ctx = nullptr;
+  bool need_new = false;
+  int done = 0;
+  anel_result res{};
+  anel_step_report rep{};
+  Clock::time_point t0;
 };
 
 class ServeEngine {
@@ -220,18 +244,26 @@ class ServeEngine {
     st->peak_active = peak_active_;
     st->contexts = contexts_;
     st->queued = (int32_t)queue_.size();
+    st->peak_cohort = peak_cohort_;
   }
 
  private:
   // Admit the head of the queue if it fits (mu_ held).  Returns the job and
   // sets ctx (a re-used idle context) or need_new (budget reserved).
-  ServeJob* admit(ServeCtx*& ctx, bool& need_new) {
-    ServeJob* head = queue_.front();
+  ServeJob* admit(ServeCtx*& ctx, bool& need_new, const std::string* only = nullptr) {
+    // the oldest job of bucket *only, or (only null) the oldest job whose
+    // bucket has no cohort running (a running cohort takes its bucket's
+    // jobs at its next step boundary)
+    auto pick = std::find_if(queue_.begin(), queue_.end(), [&](ServeJob* j) {
+      return only ? j->key == *only : cohorts_.count(j->key) == 0;
+    });
+    if (pick == queue_.end()) return nullptr;
+    ServeJob* head = *pick;
     auto it = std::find_if(idle_.begin(), idle_.end(), [&](ServeCtx* c) { return c->key == head->key; });
     if (it != idle_.end()) {
       ctx = *it;
       idle_.erase(it);
-      queue_.pop_front();
+      queue_.erase(pick);
       return head;
     }
     while (used_ + head->est_bytes > budget_ && !idle_.empty()) {
@@ -248,7 +280,7 @@ class ServeEngine {
       used_ += head->est_bytes;
       peak_ = std::max(peak_, used_);
       need_new = true;
-      queue_.pop_front();
+      queue_.erase(pick);
       return head;
     }
     return nullptr;
@@ -257,30 +289,29 @@ class ServeEngine {
   void worker() {
     cudaSetDevice(device_);
     for (;;) {
-      ServeJob* job = nullptr;
-      ServeCtx* ctx = nullptr;
-      bool need_new = false;
+      Running* r = new Running();
       {
         std::unique_lock<std::mutex> lk(mu_);
         for (;;) {
           if (!queue_.empty()) {
-            job = admit(ctx, need_new);
-            if (job) break;
-            if (active_ == 0) {
+            r->job = admit(r->ctx, r->need_new);
+            if (r->job) break;
+            if (active_ == 0 && cohorts_.empty()) {
               // does not fit even with the device to itself
               ServeJob* head = queue_.front();
               queue_.pop_front();
-              anel_result r{};
-              r.id = head->id;
-              r.status = ANEL_ERR_NOMEM;
-              r.nsteps = head->req.nsteps;
-              results_.push_back(r);
+              anel_result res{};
+              res.id = head->id;
+              res.status = ANEL_ERR_NOMEM;
+              res.nsteps = head->req.nsteps;
+              results_.push_back(res);
               ++failed_;
               delete head;
               cv_done_.notify_all();
               continue;
             }
           } else if (stop_) {
+            delete r;
             return;
           }
           cv_work_.wait(lk);
@@ -288,52 +319,38 @@ class ServeEngine {
         ++active_;
         peak_active_ = std::max(peak_active_, active_);
       }
-      anel_result res{};
-      const int st = run(*job, ctx, need_new, res);
-      {
-        std::lock_guard<std::mutex> lk(mu_);
-        --active_;
-        if (ctx) {
-          if (st == ANEL_OK) {
-            ctx->last_used = Clock::now();
-            idle_.push_back(ctx);
-          } else {
-            used_ -= ctx->bytes;
-            --contexts_;
-            delete ctx->s;
-            delete ctx;
-          }
-        } else if (need_new) {
-          used_ -= job->est_bytes;
-        }
-        results_.push_back(res);
-        if (st == ANEL_OK) ++completed_;
-        else ++failed_;
-        delete job;
+      int st = setup(*r);
+      if (st == ANEL_OK && r->job->req.nsteps > 0 && r->ctx->s->mg()->batch_capable()) {
+        run_cohort(r);
+        continue;
       }
-      cv_work_.notify_all();
-      cv_done_.notify_all();
+      if (st == ANEL_OK && r->job->req.nsteps > 0) {
+        st = r->ctx->s->step(r->job->req.nsteps, r->ctx->s->stream(), &r->rep);
+        r->done = r->job->req.nsteps;
+      }
+      finish(r, st);
     }
   }
 
-  int run(ServeJob& job, ServeCtx*& ctx, bool need_new, anel_result& res) {
-    const Clock::time_point t0 = Clock::now();
-    res.id = job.id;
-    res.queue_ms = ms_between(job.t_submit, t0);
-    res.nsteps = job.req.nsteps;
-    res.cells = (int64_t)job.grid.nx * job.grid.ny * job.grid.nz;
+  // Context (new or re-used), reset, initial state and initial projection
+  // of a member, on its own stream.
+  int setup(Running& r) {
+    ServeJob& job = *r.job;
+    r.t0 = Clock::now();
+    r.res.id = job.id;
+    r.res.queue_ms = ms_between(job.t_submit, r.t0);
+    r.res.nsteps = job.req.nsteps;
+    r.res.cells = (int64_t)job.grid.nx * job.grid.ny * job.grid.nz;
     int st = ANEL_OK;
-    if (need_new) {
+    if (r.need_new) {
       NSSolver* s = NSSolver::create(&job.grid, &job.req.mg, &job.req.ns, device_, &st);
-      if (!s) {
-        res.status = st;
-        return st;
-      }
-      ctx = new ServeCtx{s, job.key, job.est_bytes, t0};
+      if (!s) return st;
+      r.ctx = new ServeCtx{s, job.key, job.est_bytes, r.t0};
+      r.need_new = false;
       std::lock_guard<std::mutex> lk(mu_);
       ++contexts_;
     }
-    NSSolver* s = ctx->s;
+    NSSolver* s = r.ctx->s;
     cudaStream_t sm = s->stream();
     st = s->reset(&job.req.ns, sm);
     if (st == ANEL_OK) {
@@ -344,16 +361,134 @@ class ServeEngine {
     double rm = 0.0;
     if (st == ANEL_OK) st = s->project(sm, &it, &rm);
     if (st == ANEL_ERR_NOCONV) st = ANEL_OK;
-    anel_step_report rep{};
-    if (st == ANEL_OK && job.req.nsteps > 0) st = s->step(job.req.nsteps, sm, &rep);
-    if (st == ANEL_OK && job.has_out) st = s->get_fields(&job.fout, ANEL_MEM_HOST, sm);
-    const Clock::time_point t1 = Clock::now();
-    res.status = st;
-    res.run_ms = ms_between(t0, t1);
-    res.latency_ms = ms_between(job.t_submit, t1);
-    res.dt_last = rep.dt;
-    res.max_div = rep.max_div;
     return st;
+  }
+
+  // Fields out, result, context back to the idle pool (or freed on error).
+  void finish(Running* r, int st) {
+    ServeJob& job = *r->job;
+    if (st == ANEL_OK && job.has_out) st = r->ctx->s->get_fields(&job.fout, ANEL_MEM_HOST, r->ctx->s->stream());
+    const Clock::time_point t1 = Clock::now();
+    r->res.status = st;
+    r->res.run_ms = ms_between(r->t0, t1);
+    r->res.latency_ms = ms_between(job.t_submit, t1);
+    r->res.dt_last = r->rep.dt;
+    r->res.max_div = r->rep.max_div;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      --active_;
+      ServeCtx* ctx = r->ctx;
+      if (ctx) {
+        if (st == ANEL_OK) {
+          ctx->last_used = Clock::now();
+          idle_.push_back(ctx);
+        } else {
+          used_ -= ctx->bytes;
+          --contexts_;
+          delete ctx->s;
+          delete ctx;
+        }
+      } else if (r->need_new) {
+        used_ -= job.est_bytes;
+      }
+      results_.push_back(r->res);
+      if (st == ANEL_OK) ++completed_;
+      else ++failed_;
+      delete r->job;
+    }
+    delete r;
+    cv_work_.notify_all();
+    cv_done_.notify_all();
+  }
+
+  // A cohort of the first member's bucket: one step of every member per
+  // round (NSSolver::step_cohort with the bucket's batch solver), members
+  // admitted and retired at step boundaries, until the bucket runs dry.
+  void run_cohort(Running* first) {
+    const std::string key = first->job->key;
+    int st = ANEL_OK;
+    MGSolver* bmg = MGSolver::create(&first->job->grid, &first->job->req.mg, device_, &st);
+    const int64_t G = (int64_t)(first->job->grid.nx + 2) * (first->job->grid.ny + 2) * (first->job->grid.nz + 2);
+    // the batch solver: its own levels plus kMaxCohort members' FP32 levels
+    const int64_t bbytes = G * (24 + 16 * (1 + kMaxCohort)) + ((int64_t)64 << 20);
+    bool fits = false;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      fits = used_ + bbytes <= budget_;
+      if (fits) {
+        cohorts_.insert(key);
+        used_ += bbytes;
+        peak_ = std::max(peak_, used_);
+      }
+    }
+    if (fits && bmg && st == ANEL_OK) st = bmg->batch_reserve(kMaxCohort);
+    if (!fits || !bmg || st != ANEL_OK) {
+      // no room for a batch solver: the member runs alone
+      delete bmg;
+      if (fits) {
+        std::lock_guard<std::mutex> lk(mu_);
+        cohorts_.erase(key);
+        used_ -= bbytes;
+      }
+      const int s2 = first->ctx->s->step(first->job->req.nsteps, first->ctx->s->stream(), &first->rep);
+      first->done = first->job->req.nsteps;
+      finish(first, s2);
+      cv_work_.notify_all();
+      return;
+    }
+    std::vector<Running*> mem{first};
+    for (;;) {
+      // admit the bucket's queued members (each set up on its own stream)
+      for (;;) {
+        if ((int)mem.size() >= kMaxCohort) break;
+        Running* r = new Running();
+        {
+          std::lock_guard<std::mutex> lk(mu_);
+          r->job = queue_.empty() ? nullptr : admit(r->ctx, r->need_new, &key);
+          if (r->job) {
+            ++active_;
+            peak_active_ = std::max(peak_active_, active_);
+          }
+        }
+        if (!r->job) {
+          delete r;
+          break;
+        }
+        const int s1 = setup(*r);
+        if (s1 != ANEL_OK || r->job->req.nsteps == 0) finish(r, s1);
+        else mem.push_back(r);
+      }
+      if (mem.empty()) {
+        std::lock_guard<std::mutex> lk(mu_);
+        const bool more = std::any_of(queue_.begin(), queue_.end(), [&](ServeJob* j) { return j->key == key; });
+        if (!more) {
+          cohorts_.erase(key);
+          used_ -= bbytes;
+          break;
+        }
+        continue;
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        peak_cohort_ = std::max(peak_cohort_, (int)mem.size());
+      }
+      std::vector<NSSolver*> ms(mem.size());
+      std::vector<anel_step_report> reps(mem.size());
+      for (size_t b = 0; b < mem.size(); ++b) ms[b] = mem[b]->ctx->s;
+      const int sc = NSSolver::step_cohort(ms.data(), (int)ms.size(), 1, bmg, bmg->stream(), reps.data());
+      std::vector<Running*> keep;
+      for (size_t b = 0; b < mem.size(); ++b) {
+        Running* r = mem[b];
+        r->rep = reps[b];
+        ++r->done;
+        if (sc != ANEL_OK) finish(r, sc);
+        else if (r->done >= r->job->req.nsteps) finish(r, ANEL_OK);
+        else keep.push_back(r);
+      }
+      mem.swap(keep);
+    }
+    delete bmg;
+    cv_work_.notify_all();
   }
 
   std::mutex mu_;
@@ -367,6 +502,8 @@ class ServeEngine {
   int active_ = 0, peak_active_ = 0, contexts_ = 0;
   int64_t submitted_ = 0, completed_ = 0, failed_ = 0, next_id_ = 1;
   bool stop_ = false;
+  std::set<std::string> cohorts_;  // buckets with a cohort running
+  int peak_cohort_ = 0;
 };
 
 }  // namespace anel

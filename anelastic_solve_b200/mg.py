@@ -83,6 +83,29 @@ class MGSolver:
         self.last_report = rep
         return rep.iter, rep.relmax
 
+    def solve_batch(self, phis, rhss, stream=None, allow_noconv: bool = True):
+        """anel_mg_ctx_solve_batch: the device arrays phis[b] updated in
+        place from rhss[b], all members in one batched solve.  Returns the
+        members' reports."""
+        n = len(phis)
+        if n != len(rhss) or n < 1:
+            raise ValueError("phis and rhss must be non-empty and of equal length")
+        dp = C.POINTER(C.c_double)
+        pp = (dp * n)()
+        pr = (dp * n)()
+        for b in range(n):
+            p1, m1 = _ptr(phis[b])
+            p2, m2 = _ptr(rhss[b])
+            if m1 != abi.MEM_DEVICE or m2 != abi.MEM_DEVICE:
+                raise TypeError("batched solves take device arrays")
+            pp[b] = p1
+            pr[b] = p2
+        s = C.c_void_p(int(stream)) if stream is not None else None
+        reps = (abi.MGReport * n)()
+        allow = (abi.OK, abi.ERR_NOCONV) if allow_noconv else (abi.OK,)
+        check(lib().anel_mg_ctx_solve_batch(self._h, n, pp, pr, s, reps), allow)
+        return list(reps)
+
     def set_profiling(self, on: bool):
         check(lib().anel_mg_ctx_set_profiling(self._h, 1 if on else 0))
 

@@ -82,6 +82,20 @@ class NSSolver:
         check(lib().anel_ns_ctx_step(self._h, int(n), s, C.byref(rep)))
         return rep
 
+    @staticmethod
+    def step_cohort(members, n: int = 1, batch=None, stream=None):
+        """n steps of every NSSolver in members together, the pressure
+        solves of each sub-step batched (anel_ns_ctx_step_cohort); batch: an
+        MGSolver of the members' grid and multigrid parameters, or None for
+        the first member's own.  Returns the members' reports."""
+        k = len(members)
+        hs = (C.c_void_p * k)(*[m._h for m in members])
+        reps = (abi.StepReport * k)()
+        s = C.c_void_p(int(stream)) if stream is not None else None
+        b = batch._h if batch is not None else None
+        check(lib().anel_ns_ctx_step_cohort(hs, k, int(n), b, s, reps))
+        return list(reps)
+
     def step_host(self, fields_in: dict, fields_out: dict, n: int = 1, stream=None) -> abi.StepReport:
         """n steps from host arrays fields_in to host arrays fields_out (may
         be the same dict), copies overlapped with the step where the data

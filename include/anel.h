@@ -168,6 +168,18 @@ int anel_mg_ctx_set_density(anel_mg_ctx* ctx, const double* r, int32_t mem);
  * rhsf is read only (unlike the reference, it is not clobbered). */
 int anel_mg_ctx_solve(anel_mg_ctx* ctx, double* phif, const double* rhsf, int32_t mem,
                       void* stream, anel_mg_report* report);
+/* Batched solve (no reference counterpart: the reference solves one
+ * problem per call): n independent problems on the context's grid, device
+ * arrays d_phis[b] (inout) / d_rhss[b], solved together -- every kernel of
+ * the mixed-precision z-line cycle runs over all members still iterating,
+ * the defect-correction loop is one CUDA graph per batch size, and each
+ * member stops at its own tolerance.  Member b ends bit-identical to
+ * anel_mg_ctx_solve of it alone; reports[b] is its report (ms: the whole
+ * batch).  Needs a mixed-precision ZLINE context on the column layout
+ * (x/y semi-coarsened levels, nz = 32*M), else ANEL_ERR_UNSUPPORTED.
+ * Returns ANEL_ERR_NOCONV if any member did not converge. */
+int anel_mg_ctx_solve_batch(anel_mg_ctx* ctx, int32_t n, double* const* d_phis, const double* const* d_rhss,
+                            void* stream, anel_mg_report* reports);
 /* Profiling: when on, every finest-level smoother launch of the following
  * solves is bracketed by CUDA events on its stream, and the report carries
  * their count and summed time (fine_sweeps, fine_sweep_ms). */
@@ -295,6 +307,16 @@ int anel_ns_ctx_substep(anel_ns_ctx* ctx, double a1, double a2, double a3, doubl
  * output/statistics diagnostics): calcdt, gravity, LES update, three
  * sub-steps.  report (may be NULL) describes the last step. */
 int anel_ns_ctx_step(anel_ns_ctx* ctx, int32_t nsteps, void* stream, anel_step_report* report);
+/* nsteps steps of n contexts together (an ensemble cohort; no reference
+ * counterpart): the contexts share grid, boundary setup and multigrid
+ * parameters (physics, time step and fields are their own), run on one
+ * stream, and every sub-step's n pressure solves are one batched solve
+ * (anel_mg_ctx_solve_batch) of `batch` -- a multigrid context of the same
+ * grid and parameters, or NULL for the first member's own.  Each member's
+ * fields and report equal those of anel_ns_ctx_step on it alone (report
+ * ms and launches: the whole cohort's; mg ms: the batch's shared out). */
+int anel_ns_ctx_step_cohort(anel_ns_ctx* const* ctxs, int32_t n, int32_t nsteps, anel_mg_ctx* batch,
+                            void* stream, anel_step_report* reports);
 /* nsteps from host fields `in` to host fields `out` (the same arrays
  * allowed; null members are skipped): the caller's state stays in host
  * memory, as with the reference's rk_ss on its module arrays.  The copy
@@ -398,12 +420,16 @@ int anel_divergence_noalloc(int32_t nx, int32_t ny, int32_t nz, const double* u,
  * An engine that runs many short, independent shear-layer members (an
  * ensemble, or a request stream) on one GPU.  Not a reference routine:
  * each reference run is its own job.  Requests queue in FIFO order;
- * max_active host threads each drive one member on its own stream, so
- * members overlap on the device; a member is admitted when its device
- * memory fits the HBM budget, re-using an idle context of the same grid /
- * model / multigrid setup or releasing idle contexts of other setups
- * (least recently used first).  A member's fields do not depend on what
- * else runs.  Caller arrays named in a request (fields_in, fields_out) must
+ * max_active host threads each drive a cohort: the members of one bucket
+ * (grid, models, multigrid setup) stepping together, joined by the
+ * bucket's new requests and left by finished members at step boundaries,
+ * with each sub-step's pressure solves batched into one multigrid solve
+ * (up to 16 members; buckets whose multigrid is not the column-layout
+ * mixed z-line cycle run member by member).  Cohorts of different buckets
+ * overlap on the device.  A member is admitted when its device memory
+ * fits the HBM budget, re-using an idle context of the same bucket or
+ * releasing idle contexts of other buckets (least recently used first).
+ * A member's fields do not depend on what else runs.  Caller arrays named in a request (fields_in, fields_out) must
  * stay alive until its result is polled. */
 typedef struct anel_serve anel_serve;
 enum { ANEL_INIT_SHEAR = 0, ANEL_INIT_FIELDS = 1 };
@@ -436,6 +462,8 @@ typedef struct {
   int64_t submitted, completed, failed;
   int64_t bytes_in_use, peak_bytes;  /* admitted context memory (estimates) */
   int32_t active, peak_active, contexts, queued;
+  int32_t peak_cohort;               /* most members stepped together in one cohort */
+  int32_t reserved;
 } anel_serve_stats;
 
 anel_serve* anel_serve_create(int32_t device, int64_t hbm_budget_bytes, int32_t max_active,

@@ -1,5 +1,7 @@
 """Serving engine (anel_serve_*): members queued, admitted against an HBM
-budget and run concurrently on their own streams.
+budget and run concurrently -- as cohorts of one bucket with batched
+pressure solves where the multigrid is the column-layout z-line cycle,
+member by member on their own streams otherwise.
 
 * a served member equals the direct context path (set_fields of the
   shear.py state, project, step) bit for bit, which also pins the device
@@ -93,6 +95,41 @@ def test_same_alone_and_in_mix():
     assert st["peak_active"] > 1  # members overlapped on the device
     for k in FIELDS:
         np.testing.assert_array_equal(res[target]["fields"][k], alone["fields"][k], err_msg=k)
+
+
+def test_cohort_members_equal_direct_contexts():
+    """Six members of one column-cycle bucket (64x32x128), physics and step
+    counts of their own, submitted at once to one worker: they step as a
+    cohort (batched pressure solves; members join and leave at step
+    boundaries), and each equals its own direct context bit for bit."""
+    g = G.shear_layer_grid(64, 32, 128, stretched=True)
+    rng = np.random.default_rng(11)
+    members = [(float(rng.uniform(500, 4000)), float(rng.uniform(0.05, 0.3)), 300 + q, 2 + q % 3)
+               for q in range(6)]
+    e = ServeEngine(hbm_budget_bytes=32 << 30, max_active=1)
+    ids = []
+    for Re, Ri, seed, nsteps in members:
+        mg, ns = _params(g, Re=Re, Ri=Ri)
+        ids.append(e.submit(g, mg, ns, nsteps=nsteps, seed=seed, amp=1e-2, want_fields=True))
+    res = _wait(e, ids)
+    st = e.stats()
+    e.close()
+    print(f"\npeak cohort {st['peak_cohort']}, peak active {st['peak_active']}")
+    assert st["peak_cohort"] > 1
+    for rid, (Re, Ri, seed, nsteps) in zip(ids, members):
+        r = res[rid]
+        assert r["status"] == abi.OK
+        mg, ns = _params(g, Re=Re, Ri=Ri)
+        f = shear.shear_layer_fields(g, amp=1e-2, seed=seed)
+        s = NSSolver(g, mg, ns)
+        s.set_fields({k: f[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
+        s.project()
+        rep = s.step(nsteps)
+        got = s.get_fields(FIELDS)
+        s.close()
+        for k in FIELDS:
+            np.testing.assert_array_equal(r["fields"][k], got[k], err_msg=f"member {rid} {k}")
+        assert r["max_div"] == rep.max_div and r["dt_last"] == rep.dt
 
 
 def test_budget_admission_and_oversized_member():
