@@ -780,6 +780,20 @@ __global__ void __launch_bounds__(128) k_sgs(NSDev D) {
   FA(D.nT, i, j, k) = -(D.CSs[k - 1] + 0.0) * dg2 * modS + 0.0;
 }
 
+// ------------------------------------------------------------ clipVS
+// Routines.F90:301-380 on the interior: below vmin -> vmin, then above
+// vmax -> vmax (NaN passes unchanged, as both comparisons are false).
+__global__ void k_clip(NSDev D, double* a, double vmin, double vmax) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > D.nx + 1) return;
+  double v = FA(a, i, j, k);
+  if (v < vmin) v = vmin;
+  if (v > vmax) v = vmax;
+  FA(a, i, j, k) = v;
+}
+
 // ------------------------------------------------------------ Psource
 // NSsolver.F90:2167-2223 (its ghost pass is not needed: the multigrid
 // reads the interior of the right-hand side only).
@@ -868,26 +882,37 @@ __global__ void __launch_bounds__(256) k_cfl_max(NSDev D, unsigned long long* ou
 // of |div|*vol and vol in a fixed order, and one atomic maximum per block
 // on the bit pattern of max |div| (exact in any order).
 constexpr int kDivRows = 8;
-__global__ void __launch_bounds__(128) k_divergence(NSDev D, unsigned long long* mx, double* part) {
+// With cfl non-null the same pass also takes calcdt's maximum of
+// rdxc |ū| + rdzc |w̄| + rdyc |v̄| (the expression of k_cfl_max, in its
+// order) over the same cells and neighbours, for the next step's time
+// step: one read of u, v, w at the end of a step serves both.
+__global__ void __launch_bounds__(128) k_divergence(NSDev D, unsigned long long* mx, double* part,
+                                                    unsigned long long* cfl) {
   __shared__ double sh[2][4];
-  __shared__ unsigned long long shm[4];
+  __shared__ unsigned long long shm[2][4];
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
   const int k0 = 2 + blockIdx.z * kDivRows;
   double s1 = 0.0, s2 = 0.0;
-  unsigned long long m = 0;
+  unsigned long long m = 0, mc = 0;
   if (i <= D.nx + 1) {
     double wb = FA(D.w, i, j, k0 - 1);
     for (int k = k0; k < k0 + kDivRows && k <= D.nz + 1; ++k) {
       const double wt = FA(D.w, i, j, k);
-      const double d = (FA(D.u, i, j, k) - FA(D.u, i - 1, j, k)) * MT(D.rdxc, i) +
-                       (FA(D.v, i, j, k) - FA(D.v, i, j - 1, k)) * MT(D.rdyc, j) +
-                       (wt - wb) * MT(D.rdzc, k);
+      const double ui = FA(D.u, i, j, k), um = FA(D.u, i - 1, j, k);
+      const double vj = FA(D.v, i, j, k), vm = FA(D.v, i, j - 1, k);
+      const double d = (ui - um) * MT(D.rdxc, i) + (vj - vm) * MT(D.rdyc, j) + (wt - wb) * MT(D.rdzc, k);
       const double vol = 1.0 / (MT(D.rdxc, i) * MT(D.rdyc, j) * MT(D.rdzc, k));
       s1 += fabs(d) * vol;
       s2 += vol;
       const unsigned long long a = __double_as_longlong(fabs(d));
       m = a > m ? a : m;
+      if (cfl) {
+        const double adv = MT(D.rdxc, i) * fabs(0.5 * (ui + um)) + MT(D.rdzc, k) * fabs(0.5 * (wt + wb)) +
+                           MT(D.rdyc, j) * fabs(0.5 * (vj + vm));
+        const unsigned long long b = __double_as_longlong(adv);
+        mc = b > mc ? b : mc;
+      }
       wb = wt;
     }
   }
@@ -896,23 +921,28 @@ __global__ void __launch_bounds__(128) k_divergence(NSDev D, unsigned long long*
     s2 += __shfl_xor_sync(0xffffffffu, s2, o);
     const unsigned long long w = __shfl_xor_sync(0xffffffffu, m, o);
     m = w > m ? w : m;
+    const unsigned long long wc = __shfl_xor_sync(0xffffffffu, mc, o);
+    mc = wc > mc ? wc : mc;
   }
   const int wid = threadIdx.x >> 5;
   if ((threadIdx.x & 31) == 0) {
     sh[0][wid] = s1;
     sh[1][wid] = s2;
-    shm[wid] = m;
+    shm[0][wid] = m;
+    shm[1][wid] = mc;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     double a = 0.0, b = 0.0;
-    unsigned long long mm = 0;
+    unsigned long long mm = 0, mmc = 0;
     for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
       a += sh[0][q];
       b += sh[1][q];
-      mm = shm[q] > mm ? shm[q] : mm;
+      mm = shm[0][q] > mm ? shm[0][q] : mm;
+      mmc = shm[1][q] > mmc ? shm[1][q] : mmc;
     }
     atomicMax(mx, mm);
+    if (cfl) atomicMax(cfl, mmc);
     const int64_t bid = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
     part[2 * bid] = a;
     part[2 * bid + 1] = b;
@@ -1194,6 +1224,11 @@ void launch_init_shear(const NSDev& D, const double* prof, uint32_t seed, double
   count_launch();
 }
 
+void launch_clip(const NSDev& D, double* a, double vmin, double vmax, cudaStream_t s) {
+  k_clip<<<cell_grid(D, 128), 128, 0, s>>>(D, a, vmin, vmax);
+  count_launch();
+}
+
 void launch_psource(const NSDev& D, double dt, cudaStream_t s) {
   const int tx = 128;
   k_psource<<<cell_grid(D, tx), tx, 0, s>>>(D, 1.0 / dt);
@@ -1232,8 +1267,9 @@ int64_t divergence_blocks(const NSDev& D) {
   return (int64_t)g.x * g.y * g.z;
 }
 
-void launch_divergence(const NSDev& D, unsigned long long* mx, double* part, cudaStream_t s) {
-  k_divergence<<<divergence_grid(D), 128, 0, s>>>(D, mx, part);
+void launch_divergence(const NSDev& D, unsigned long long* mx, double* part, cudaStream_t s,
+                       unsigned long long* cfl) {
+  k_divergence<<<divergence_grid(D), 128, 0, s>>>(D, mx, part, cfl);
   count_launch();
 }
 

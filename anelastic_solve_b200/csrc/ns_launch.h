@@ -39,6 +39,8 @@ void launch_init_shear(const NSDev& D, const double* prof, uint32_t seed, double
 void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, const ZRule& Rw,
                   cudaStream_t s);
 void launch_ghost_field(const NSDev& D, double* a, const ZRule& R, cudaStream_t s);
+// clipVS (Routines.F90:301-380) of a cell-centred field's interior
+void launch_clip(const NSDev& D, double* a, double vmin, double vmax, cudaStream_t s);
 void launch_cfl_max(const NSDev& D, unsigned long long* out, cudaStream_t s);
 int64_t divergence_blocks(const NSDev& D);
 // plane statistics (NSsolver.F90:288-395): center_velocity of one
@@ -51,6 +53,9 @@ int64_t plane_part_doubles(const NSDev& D);
 void launch_plane_avg(const NSDev& D, const double* a, const double* wx, const double* wy, double area,
                       double* part, double* out, cudaStream_t s);
 void launch_diag_update(int Z, double dtt, const double* m, double* dg, cudaStream_t s);
-void launch_divergence(const NSDev& D, unsigned long long* mx, double* part, cudaStream_t s);
+// cfl (may be null): also calcdt's CFL maximum of the same fields, as the
+// bit pattern of a non-negative double, atomically maxed into *cfl
+void launch_divergence(const NSDev& D, unsigned long long* mx, double* part, cudaStream_t s,
+                       unsigned long long* cfl = nullptr);
 
 }  // namespace anel

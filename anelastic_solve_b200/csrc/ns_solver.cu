@@ -59,12 +59,22 @@ NSSolver::~NSSolver() {
   if (stream_) cudaStreamDestroy(stream_);
 }
 
+// clip: with scal1 held at zero (scal1_on = 0) its range must keep it there
+static int check_clip(const anel_ns_params* ns) {
+  if (ns->clip && !ns->scal1_on && !(ns->scal1_min <= 0.0 && 0.0 <= ns->scal1_max)) {
+    set_error("clip: with scal1_on = 0 the scal1 range [%g, %g] must contain 0", ns->scal1_min, ns->scal1_max);
+    return ANEL_ERR_ARG;
+  }
+  return ANEL_OK;
+}
+
 int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const anel_ns_params* ns,
                    int device) {
   if (!g || !mgp || !ns) {
     set_error("null grid, mg or ns parameters");
     return ANEL_ERR_ARG;
   }
+  if (check_clip(ns) != ANEL_OK) return ANEL_ERR_ARG;
   prm_ = *ns;
   device_ = device;
   nx_ = g->nx;
@@ -467,6 +477,7 @@ int NSSolver::set_fields(const anel_fields* f, int mem, cudaStream_t s) {
   double* const* src = reinterpret_cast<double* const*>(f);
   const cudaMemcpyKind kind = mem == ANEL_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   bool density = false;
+  fields_changed();
   for (int q = 0; q < 17; ++q) {
     if (!src[q] || !d_fields_[q]) continue;  // LES fields exist only with a subgrid model
     ANEL_CUDA_TRY(cudaMemcpyAsync(d_fields_[q], src[q], G_ * sizeof(double), kind, s));
@@ -537,16 +548,16 @@ int NSSolver::substep_pre(double a1, double a2, double a3, double dt_rk, double 
   const ZRule ru = zrule(NV_U), rv = zrule(NV_V), rw = zrule(NV_W);
   // var_advance_CN_PL: with Vmodel = SSM every variable gets the eddy
   // terms (the LES block is gated on Vmodel, NSsolver.F90:3160-3190)
-  auto cn = [&](int var, double* f, const double* q, int vi, const ZRule& R, const double* kT) {
-    if (D_.vles) launch_cn_les(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, kT, d_cnb_, d_cnc_, s);
-    else launch_cn(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, cnvar_, s);
+  auto cn = [&](int var, double* f, const double* q, int vi, const ZRule& R, const double* kT, cudaStream_t st) {
+    if (D_.vles) launch_cn_les(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, kT, d_cnb_, d_cnc_, st);
+    else launch_cn(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, cnvar_, st);
   };
-  cn(1, D_.u, D_.qu, 0, ru, D_.nuT);
-  cn(2, D_.v, D_.qv, 1, rv, D_.nuT);
-  cn(3, D_.w, D_.qw, 2, rw, D_.nuT);
+  cn(1, D_.u, D_.qu, 0, ru, D_.nuT, s);
+  cn(2, D_.v, D_.qv, 1, rv, D_.nuT, s);
+  cn(3, D_.w, D_.qw, 2, rw, D_.nuT, s);
   launch_psource(D_, dt_rk, s);
-  cn(5, D_.rho, D_.qr, 3, zrule(NV_RHO), D_.kT);
-  if (prm_.scal1_on) cn(8, D_.s, D_.qs, 4, zrule(NV_SCAL1), D_.nT);
+  cn(5, D_.rho, D_.qr, 3, zrule(NV_RHO), D_.kT, s);
+  if (prm_.scal1_on) cn(8, D_.s, D_.qs, 4, zrule(NV_SCAL1), D_.nT, s);
   const size_t fb = G_ * sizeof(double);
   if (io_last_sub_ && io_out_) {
     // rho and scal1 are final: copy them out during the pressure solve
@@ -574,6 +585,7 @@ int NSSolver::substep_post(const anel_mg_report& rep, cudaStream_t s, int* iters
   acc_sweep_ms_ += rep.fine_sweep_ms;
   acc_sweeps_ += rep.fine_sweeps;
   launch_pgrad(D_, pend_dtrk_, zrule(NV_U), zrule(NV_V), zrule(NV_W), s);
+  fields_changed();
   if (iters) *iters = rep.iter;
   if (relmax) *relmax = rep.relmax;
   return check_launch("rk substep");
@@ -606,8 +618,10 @@ int NSSolver::reset(const anel_ns_params* ns, cudaStream_t s) {
     set_error("reset: models, edge-node flag and boundary conditions must match the context");
     return ANEL_ERR_ARG;
   }
+  if (check_clip(ns) != ANEL_OK) return ANEL_ERR_ARG;
   prm_ = *ns;
   temps_clean_ = false;
+  fields_changed();
   rRe_ = 1.0 / ns->Re;
   rPr_ = 1.0 / ns->Pr;
   rSc_ = 1.0 / ns->Sc;
@@ -635,6 +649,7 @@ int NSSolver::reset(const anel_ns_params* ns, cudaStream_t s) {
 int NSSolver::init_shear(uint32_t seed, double amp, double zmax, cudaStream_t s) {
   ANEL_CUDA_TRY(cudaSetDevice(device_));
   if (!s) s = stream_;
+  fields_changed();
   const int Z = nz_ + 2;
   if (!d_ic_) ANEL_CUDA_TRY(cudaMalloc(&d_ic_, 2 * (size_t)Z * sizeof(double)));
   std::vector<double> prof(2 * (size_t)Z);
@@ -706,18 +721,46 @@ int NSSolver::les_coeffs(cudaStream_t s) {
   return ANEL_OK;
 }
 
+// calcdt (Routines.F90:186-258) in two halves: the CFL maximum to the
+// host-mapped word (issue), then, after the stream is synchronised, the
+// time step from it (take)
+void NSSolver::calcdt_issue(cudaStream_t s) {
+  if (cfl_ready_) {
+    // the previous step's divergence pass took it from these fields
+    copy_words(d_red_ + 2, h_red_, 1, s);
+    cfl_ready_ = false;
+  } else {
+    cudaMemsetAsync(d_red_, 0, sizeof(unsigned long long), s);
+    launch_cfl_max(D_, d_red_, s);
+    copy_words(d_red_, h_red_, 1, s);
+  }
+}
+
+double NSSolver::calcdt_take() const {
+  double dt = prm_.cfl / h_red_[0];
+  if (dt >= prm_.dtmax) dt = prm_.dtmax;
+  return dt;
+}
+
 double NSSolver::calcdt(cudaStream_t s, int* st) {
-  cudaMemsetAsync(d_red_, 0, sizeof(unsigned long long), s);
-  launch_cfl_max(D_, d_red_, s);
-  copy_words(d_red_, h_red_, 1, s);
+  calcdt_issue(s);
   if (cudaStreamSynchronize(s) != cudaSuccess) {
     *st = ANEL_ERR_CUDA;
     return 0.0;
   }
-  double dt = prm_.cfl / h_red_[0];
-  if (dt >= prm_.dtmax) dt = prm_.dtmax;
   *st = ANEL_OK;
-  return dt;
+  return calcdt_take();
+}
+
+// The driver's optional clip after each rk_ss (NSsolver.F90:206-211,
+// 235-240, 264-269): clipVS of rho, its ghost pass, clipVS of scal1, its
+// ghost pass.
+void NSSolver::clip_scalars(cudaStream_t s) {
+  if (!prm_.clip) return;
+  launch_clip(D_, D_.rho, prm_.rho_min, prm_.rho_max, s);
+  launch_ghost_field(D_, D_.rho, zrule(NV_RHO), s);
+  launch_clip(D_, D_.s, prm_.scal1_min, prm_.scal1_max, s);
+  launch_ghost_field(D_, D_.s, zrule(NV_SCAL1), s);
 }
 
 static const double kA1[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
@@ -726,6 +769,12 @@ static const double kA3[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
 // Start of a step (NSsolver.F90:63-164): zero_temps, calcdt, gravity, the
 // LES coefficients on their cadence and the scalar smoothing.
 int NSSolver::step_begin(cudaStream_t s, double* delt_out) {
+  step_begin_issue(s);
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  return step_begin_finish(s, delt_out);
+}
+
+void NSSolver::step_begin_issue(cudaStream_t s) {
   // zero_temps (memManage.F90:844-853).  The accumulators q_u, q_v,
   // q_w, q_rho, q_s are written, never read, by the first sub-step
   // (a1 = 0) on every interior cell, and no kernel writes their ghost
@@ -733,11 +782,16 @@ int NSSolver::step_begin(cudaStream_t s, double* delt_out) {
   // reset or a scratch use touches them (temps_clean_); the Poisson
   // right-hand side is zeroed every step.
   for (int q : {8, 9, 10, 11, 12, 13})
-    if (q == 13 || !temps_clean_) ANEL_CUDA_TRY(cudaMemsetAsync(d_fields_[q], 0, G_ * sizeof(double), s));
+    if (q == 13 || !temps_clean_) cudaMemsetAsync(d_fields_[q], 0, G_ * sizeof(double), s);
   temps_clean_ = true;
-  int st = ANEL_OK;
-  const double delt = calcdt(s, &st);
+  calcdt_issue(s);
+}
+
+// (after step_begin_issue and a synchronisation of its stream)
+int NSSolver::step_begin_finish(cudaStream_t s, double* delt_out) {
+  int st = check_launch("step start");
   if (st != ANEL_OK) return st;
+  const double delt = calcdt_take();
   // gravity (Routines.F90:27-52)
   if (time_ < prm_.gt1) gnow_ = 0.0;
   else if (time_ > prm_.gt1 && time_ < prm_.gt2) gnow_ = g_orig_ * (time_ - prm_.gt1) / (prm_.gt2 - prm_.gt1);
@@ -779,6 +833,10 @@ int NSSolver::step_end(double delt, cudaStream_t s, anel_step_report* r) {
   r->dt = delt;
   r->time = time_;
   nstep_ += 1;
+  // divergence of the step's result and the next step's CFL maximum
+  const int st = divergence_pass(s, true);
+  if (st != ANEL_OK) return st;
+  cfl_ready_ = div_ready_ = true;
   return ANEL_OK;
 }
 
@@ -790,7 +848,7 @@ int NSSolver::step_finish(cudaStream_t s, int64_t launches0, anel_step_report* r
   r->diag_ms = acc_diag_ms_;
   r->launches = t_launches - launches0;
   double dv[2];
-  const int st = divergence(s, dv);
+  const int st = div_ready_ ? divergence_read(s, dv) : divergence(s, dv);
   if (st != ANEL_OK) return st;
   r->avg_div = dv[0];
   r->max_div = dv[1];
@@ -818,6 +876,7 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
       st = substep(kA1[q], 1.0, kA3[q], DTR[q], delt, s, &r.mg_iter[q], &r.mg_relmax[q], true);
       io_last_sub_ = false;
       if (st != ANEL_OK) return st;
+      clip_scalars(s);
     }
     st = step_end(delt, s, &r);
     if (st != ANEL_OK) return st;
@@ -878,8 +937,11 @@ int NSSolver::step_cohort(NSSolver* const* ms, int n, int nsteps, MGSolver* bmg,
   }
   ANEL_CUDA_TRY(cudaEventRecord(ms[0]->ev0_, s));
   for (int step = 0; step < nsteps; ++step) {
+    // every member's time step with one synchronisation
+    for (int b = 0; b < n; ++b) ms[b]->step_begin_issue(s);
+    ANEL_CUDA_TRY(cudaStreamSynchronize(s));
     for (int b = 0; b < n; ++b) {
-      const int st = ms[b]->step_begin(s, &delt[b]);
+      const int st = ms[b]->step_begin_finish(s, &delt[b]);
       if (st != ANEL_OK) return st;
     }
     for (int q = 0; q < 3; ++q) {
@@ -896,6 +958,7 @@ int NSSolver::step_cohort(NSSolver* const* ms, int n, int nsteps, MGSolver* bmg,
         mrep[b].ms /= n;  // the batch's device time, shared out
         const int st = ms[b]->substep_post(mrep[b], s, &r[b].mg_iter[q], &r[b].mg_relmax[q]);
         if (st != ANEL_OK) return st;
+        ms[b]->clip_scalars(s);
       }
     }
     for (int b = 0; b < n; ++b) {
@@ -907,11 +970,30 @@ int NSSolver::step_cohort(NSSolver* const* ms, int n, int nsteps, MGSolver* bmg,
   ANEL_CUDA_TRY(cudaEventSynchronize(ms[0]->ev1_));
   float tms = 0.f;
   cudaEventElapsedTime(&tms, ms[0]->ev0_, ms[0]->ev1_);
+  // the divergence of every member's last step (step_end's passes), with
+  // one synchronisation
+  for (int b = 0; b < n; ++b) ms[b]->divergence_issue(s);
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
   for (int b = 0; b < n; ++b) {
-    r[b].ms = tms;
-    const int st = ms[b]->step_finish(s, l0[b], &r[b]);
-    if (st != ANEL_OK) return st;
-    reps[b] = r[b];
+    NSSolver* m = ms[b];
+    anel_step_report& rb = r[b];
+    rb.ms = tms;
+    rb.mg_ms = m->acc_mg_ms_;
+    rb.fine_sweep_ms = m->acc_sweep_ms_;
+    rb.fine_sweeps = m->acc_sweeps_;
+    rb.diag_ms = m->acc_diag_ms_;
+    rb.launches = t_launches - l0[b];
+    double dv[2] = {0.0, 0.0};
+    if (nsteps > 0) {
+      const int st = m->divergence_take(dv);
+      if (st != ANEL_OK) return st;
+    } else {
+      const int st = m->divergence(s, dv);
+      if (st != ANEL_OK) return st;
+    }
+    rb.avg_div = dv[0];
+    rb.max_div = dv[1];
+    reps[b] = rb;
   }
   return ANEL_OK;
 }
@@ -919,6 +1001,7 @@ int NSSolver::step_cohort(NSSolver* const* ms, int n, int nsteps, MGSolver* bmg,
 int NSSolver::ghost_state(cudaStream_t s) {
   ANEL_CUDA_TRY(cudaSetDevice(device_));
   if (!s) s = stream_;
+  fields_changed();
   double* f[6] = {D_.u, D_.v, D_.w, D_.p, D_.rho, D_.s};
   const int vt[6] = {NV_U, NV_V, NV_W, NV_P, NV_RHO, NV_SCAL1};
   for (int q = 0; q < 6; ++q)
@@ -1098,6 +1181,7 @@ int NSSolver::step_host(const anel_fields* in, const anel_fields* out, int nstep
 int NSSolver::project(cudaStream_t s, int* iters, double* relmax) {
   ANEL_CUDA_TRY(cudaSetDevice(device_));
   if (!s) s = stream_;
+  fields_changed();
   // the velocity ghosts first: with the wall values in place the boundary
   // flux of Psource vanishes and the Neumann problem is compatible
   launch_ghost_field(D_, D_.u, zrule(NV_U), s);
@@ -1114,23 +1198,47 @@ int NSSolver::project(cudaStream_t s, int* iters, double* relmax) {
   return check_launch("project");
 }
 
-int NSSolver::divergence(cudaStream_t s, double* out) {
-  ANEL_CUDA_TRY(cudaSetDevice(device_));
-  if (!s) s = stream_;
+// divergence (Routines.F90:54-183) of the current fields into device
+// memory: max |div| in d_red_[1], the volume-weighted sums after the fold;
+// with_cfl also the CFL maximum in d_red_[2]
+int NSSolver::divergence_pass(cudaStream_t s, bool with_cfl) {
   const int64_t nb = divergence_blocks(D_);
   // partial pairs, fold scratch, the two sums
   if (!d_part_)
     ANEL_CUDA_TRY(cudaMalloc(&d_part_, (2 * nb + fold_scratch_doubles() + 2) * sizeof(double)));
   double* sums = d_part_ + 2 * nb + fold_scratch_doubles();
-  ANEL_CUDA_TRY(cudaMemsetAsync(d_red_ + 1, 0, sizeof(unsigned long long), s));
-  launch_divergence(D_, d_red_ + 1, d_part_, s);
+  ANEL_CUDA_TRY(cudaMemsetAsync(d_red_ + 1, 0, (with_cfl ? 2 : 1) * sizeof(unsigned long long), s));
+  launch_divergence(D_, d_red_ + 1, d_part_, s, with_cfl ? d_red_ + 2 : nullptr);
   launch_fold_pairs(d_part_, nb, d_part_ + 2 * nb, sums, s);
+  return ANEL_OK;
+}
+
+void NSSolver::divergence_issue(cudaStream_t s) {
+  const int64_t nb = divergence_blocks(D_);
+  const double* sums = d_part_ + 2 * nb + fold_scratch_doubles();
   copy_words(d_red_ + 1, h_red_ + 1, 1, s);
   copy_words(sums, h_red_ + 2, 2, s);
-  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+}
+
+int NSSolver::divergence_take(double* out) {
   out[0] = h_red_[2] / h_red_[3];
   out[1] = h_red_[1];
   return check_launch("divergence");
+}
+
+int NSSolver::divergence_read(cudaStream_t s, double* out) {
+  divergence_issue(s);
+  ANEL_CUDA_TRY(cudaStreamSynchronize(s));
+  return divergence_take(out);
+}
+
+int NSSolver::divergence(cudaStream_t s, double* out) {
+  ANEL_CUDA_TRY(cudaSetDevice(device_));
+  if (!s) s = stream_;
+  const int st = divergence_pass(s, false);
+  if (st != ANEL_OK) return st;
+  div_ready_ = false;  // d_red_[1] and the sums now hold this pass
+  return divergence_read(s, out);
 }
 
 }  // namespace anel

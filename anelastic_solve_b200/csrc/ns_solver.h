@@ -81,11 +81,28 @@ class NSSolver {
   // phases of one RK3 step (step() and step_cohort() run them in order;
   // the pressure solve of each sub-step sits between pre and post)
   int step_begin(cudaStream_t s, double* delt);
+  void step_begin_issue(cudaStream_t s);
+  int step_begin_finish(cudaStream_t s, double* delt);
+  void calcdt_issue(cudaStream_t s);
+  double calcdt_take() const;
   int substep_pre(double a1, double a2, double a3, double dt_rk, double dt, cudaStream_t s, bool q_zero);
   int substep_post(const anel_mg_report& rep, cudaStream_t s, int* iters, double* relmax);
   int step_end(double delt, cudaStream_t s, anel_step_report* r);
   int step_finish(cudaStream_t s, int64_t launches0, anel_step_report* r);
+  void clip_scalars(cudaStream_t s);
   double pend_dtrk_ = 0.0;  // the sub-step between substep_pre and substep_post
+  // step_end's divergence pass also takes the CFL maximum of the fields it
+  // leaves (d_red_[2]) and its divergence results stay on the device:
+  // cfl_ready_ lets the next calcdt use that maximum, div_ready_ lets
+  // step_finish report those results, without another read of u, v, w.
+  // Every call that changes u, v or w afterwards clears both.
+  bool cfl_ready_ = false, div_ready_ = false;
+
+  void fields_changed() { cfl_ready_ = div_ready_ = false; }
+  int divergence_pass(cudaStream_t s, bool with_cfl);
+  int divergence_read(cudaStream_t s, double* out);
+  void divergence_issue(cudaStream_t s);
+  int divergence_take(double* out);
   int les_coeffs(cudaStream_t s);
 
   anel_ns_params prm_{};

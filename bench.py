@@ -65,6 +65,9 @@ WORKLOADS = {
     "poisson": ("poisson", (512, 256, 512), (9, 8, 9), {}),
     "poisson256": ("poisson", (256, 256, 256), (8, 8, 8), {}),
     "poisson_small": ("poisson", (64, 32, 64), (6, 5, 6), {}),
+    # serving-bucket sizes, for the batched solve (--members)
+    "poisson64": ("poisson", (64, 64, 64), (6, 6, 6), {}),
+    "poisson128": ("poisson", (128, 128, 128), (7, 7, 7), {}),
     # profiling case: 134 MB per FP32 field (above L2), ~1.5 GB on the device
     "poisson_prof": ("poisson", (512, 128, 512), (9, 7, 9), {}),
 }
@@ -168,10 +171,10 @@ def ns_params(phys):
                               interp=abi.DIAG_CORRECTED)
 
 
-def poisson_rhs(g):
+def poisson_rhs(g, seed=1):
     """Seeded N(0,1) right-hand side with the volume mean removed (the
     compatibility condition of the Neumann/periodic problem)."""
-    rng = np.random.default_rng(1)
+    rng = np.random.default_rng(seed)
     f = rng.standard_normal(g.ghosted[::-1])  # (Z,Y,X) C-order == Fortran (X,Y,Z)
     vol = (g.z.dxc[1:-1, None, None] * g.y.dxc[None, 1:-1, None] * g.x.dxc[None, None, 1:-1])
     inner = f[1:-1, 1:-1, 1:-1]
@@ -432,11 +435,54 @@ def run_poisson(args, rank, world, local_rank):
         torch.cuda.synchronize()
         out["e2e_ms"] = e0.elapsed_time(e1) / ne
         out["bytes_io"] = (2 * dsrc.numel() * 8, dsrc.numel() * 8)
+    if args.members > 1:
+        out["batched"] = batched_solves(s, g, args, st, dev)
     s.close()
     out["tuning"] = _lib.tuning_report().splitlines()
     keys = [k for k in ("ms_step", "e2e_ms") if k in out]
     out.update(zip(keys, combine_ranks(world, dev, maxes=[out[k] for k in keys])[0]))
     return out
+
+
+def batched_solves(s, g, args, st, dev):
+    """B = args.members independent right-hand sides (seeds 1..B) of this
+    grid: solved one after another (solve_device each, CUDA events around
+    all B) and as one batched solve (solve_batch); the batched solutions
+    must equal the one-by-one ones bit for bit."""
+    import torch
+
+    B = args.members
+    rhs = [torch.from_numpy(poisson_rhs(g, seed=1 + b)).to(dev) for b in range(B)]
+    one = [torch.zeros_like(rhs[0]) for _ in range(B)]
+    bat = [torch.zeros_like(rhs[0]) for _ in range(B)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def alone():
+        for b in range(B):
+            with torch.cuda.stream(st):
+                one[b].zero_()
+            s.solve(one[b], rhs[b], stream=st.cuda_stream)
+
+    def together():
+        with torch.cuda.stream(st):
+            for b in range(B):
+                bat[b].zero_()
+        return s.solve_batch(bat, rhs, stream=st.cuda_stream)
+
+    alone()
+    together()  # warm-up of both (graphs built)
+    torch.cuda.synchronize()
+    ev[0].record(st)
+    alone()
+    ev[1].record(st)
+    ev[2].record(st)
+    reps = together()
+    ev[3].record(st)
+    torch.cuda.synchronize()
+    t1, tb = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
+    same = all(torch.equal(one[b], bat[b]) for b in range(B))
+    return {"members": B, "ms_one_by_one": round(t1, 3), "ms_batched": round(tb, 3),
+            "speedup": round(t1 / tb, 3), "cycles": [r.iter for r in reps], "bitwise_equal": same}
 
 
 # ------------------------------------------------------------ CPU samples
@@ -730,6 +776,8 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 multigrid companion")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--members", type=int, default=1,
+                    help="poisson workloads: also time this many solves one by one and batched")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the stream")
     ap.add_argument("--rate", type=float, default=50.0, help="serve: arrivals per second")
     ap.add_argument("--serve-steps", type=int, default=10, help="serve: RK3 steps per request")
@@ -888,6 +936,8 @@ def main():
     else:
         line["mg_iters"] = r["iters"][-1]
         line["resid"] = r["resid"]
+        if "batched" in r:
+            line["batched"] = r["batched"]
     if "e2e_ms" in r:
         line["e2e"] = {"value": world * N / (r["e2e_ms"] / 1e3), "unit": unit,
                        "h2d_bytes_per_step": r["bytes_io"][0], "d2h_bytes_per_step": r["bytes_io"][1],

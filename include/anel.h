@@ -254,7 +254,13 @@ typedef struct {
   int32_t filt[3];
   int32_t stretched[3];
   int32_t interp;
-  int32_t reserved2;
+  /* Clip (Parameters::clip, NSsolver.F90:206-211, 235-240, 264-269):
+   * after every sub-step rho and then scal1 are clipped to [min, max]
+   * on the interior (clipVS, Routines.F90:301-380: below min -> min,
+   * then above max -> max) and ghosted.  0 (the runfiles' Clip=no): off.
+   * With scal1_on = 0 the scal1 range must contain 0. */
+  int32_t clip;
+  double rho_min, rho_max, scal1_min, scal1_max;
 } anel_ns_params;
 
 /* Host (or device) pointers to the ghosted FP64 fields of the Flow and

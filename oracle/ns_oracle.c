@@ -1406,6 +1406,20 @@ static void sgsdiff(orc_ns* s) {
 }
 
 /* One NSsolver time step (NSsolver.F90:63-283 minus output/statistics). */
+/* clipVS (Routines.F90:301-380): interior values below vmin become vmin,
+ * then values above vmax become vmax (the clipped-point counts it prints
+ * are not kept). */
+static void clip_vs(const orc_ns* s, double* var, double vmin, double vmax) {
+  const orc_dom* D = &s->d;
+  for (long k = 2; k <= D->nz + 1; ++k)
+    for (long j = 2; j <= D->ny + 1; ++j)
+      for (long i = 2; i <= D->nx + 1; ++i) {
+        double* v = &var[IX(i, j, k)];
+        if (*v < vmin) *v = vmin;
+        if (*v > vmax) *v = vmax;
+      }
+}
+
 int orc_ns_step(orc_ns* s, anel_step_report* rep) {
   const orc_dom* D = &s->d;
   anel_fields* f = &s->f;
@@ -1444,6 +1458,12 @@ int orc_ns_step(orc_ns* s, anel_step_report* rep) {
   for (int q = 0; q < 3; ++q) {
     if (les && s->nstep > s->p.les_start) sgsdiff(s);
     orc_ns_substep(s, A1[q], 1.0, A3[q], DTR[q], delt, &it[q], &rm[q]);
+    if (s->p.clip) { /* NSsolver.F90:206-211 (and :235-240, :264-269) */
+      clip_vs(s, f->rho, s->p.rho_min, s->p.rho_max);
+      ghost(s, f->rho, VT_RHO);
+      clip_vs(s, f->scal1, s->p.scal1_min, s->p.scal1_max);
+      ghost(s, f->scal1, VT_SCAL1);
+    }
   }
   s->told = s->time; /* told = time; time = time + delt (NSsolver.F90:272-274) */
   s->time = s->time + delt;

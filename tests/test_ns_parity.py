@@ -316,3 +316,37 @@ def test_cn_launch_variants_bitwise(variant, monkeypatch):
     got = s.get_fields(CMP)
     for name in CMP:
         np.testing.assert_array_equal(got[name], f[name], err_msg=name)
+
+
+def test_clip_steps_bitwise():
+    """The driver's optional clip (Clip=yes: clipVS of rho and scal1 after
+    every sub-step, NSsolver.F90:206-211, Routines.F90:301-380): three FP64
+    steps with a rho range that cuts the shear layer's tails, GPU == oracle
+    bit for bit; the clipped rho stays in range and differs from the
+    unclipped run."""
+    g_ = G.shear_layer_grid(32, 16, 32, stretched=True)
+    mgp = abi.make_mg_params(levels_for(g_), maxcy=200, tolmax=1e-10, pre=2, post=2,
+                             tbc=(0, 1, 0, 1, 0, 0), mode=abi.MODE_METRIC, stop=abi.STOP_RESID)
+    clip = (-0.8, 0.8, -0.5, 0.5)
+    nsp = abi.make_ns_params(Re=1000.0, Pr=1.0, g=-0.12, dtmax=0.01, ew=1, scal1_on=1, clip=clip)
+    f = shear.shear_layer_fields(g_, amp=1e-3)
+    o = OracleNS(g_, mgp, nsp, f)
+    for name, vt in (("u", 0), ("v", 1), ("w", 2), ("rho", 4), ("scal1", 12)):
+        o.ghost(f[name], vt)
+    o.project()
+    start = {k: v.copy(order="F") for k, v in f.items()}
+    s = NSSolver(g_, mgp, nsp)
+    s.set_fields({k: start[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
+    for _ in range(3):
+        ro = o.step()
+        rg = s.step(1)
+        assert ro.dt == rg.dt and list(ro.mg_iter) == list(rg.mg_iter)
+    got = s.get_fields(CMP)
+    for name in CMP:
+        np.testing.assert_array_equal(got[name], f[name], err_msg=name)
+    rho = got["rho"][1:-1, 1:-1, 1:-1]
+    assert rho.min() >= clip[0] and rho.max() <= clip[1]
+    s2 = NSSolver(g_, mgp, abi.make_ns_params(Re=1000.0, Pr=1.0, g=-0.12, dtmax=0.01, ew=1, scal1_on=1))
+    s2.set_fields({k: start[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
+    s2.step(3)
+    assert s2.get_fields(("rho",))["rho"][1:-1, 1:-1, 1:-1].min() < clip[0]
