@@ -606,8 +606,8 @@ __global__ void __launch_bounds__(TPB) k_cn_column(NSDev D, double* __restrict__
 // c go to per-cell scratch for the back substitution.  Loads of a batch of
 // kCNU rows are issued before its stores.  The arithmetic follows the
 // reference's expressions term by term.
-template <int kVar>
-__global__ void __launch_bounds__(kCNThreads) k_cn_column_les(NSDev D, double* __restrict__ fld,
+template <int kVar, int U = kCNU, int TPB = kCNThreads>
+__global__ void __launch_bounds__(TPB) k_cn_column_les(NSDev D, double* __restrict__ fld,
                                                               const double* __restrict__ q, CNFac F,
                                                               double a3, double rkdt, ZRule R,
                                                               const double* __restrict__ kT,
@@ -660,10 +660,10 @@ __global__ void __launch_bounds__(kCNThreads) k_cn_column_les(NSDev D, double* _
   cc[base] = cprev;
   // kT window: rows k-1 and k of both columns (kn = kc for rho, scal1, w)
   double kcm = kc[0], kcc = kc[XY], knm = kn[0], knc = kn[XY];
-  for (int kb = 2; kb <= n; kb += kCNU) {
-    double up[kCNU], qv[kCNU], kcp[kCNU], knp[kCNU];
+  for (int kb = 2; kb <= n; kb += U) {
+    double up[U], qv[U], kcp[U], knp[U];
 #pragma unroll
-    for (int u = 0; u < kCNU; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int k = kb + u;
       const int64_t o = (int64_t)(k - 1) * XY;
       up[u] = (k < n) ? fld[base + o + XY] : 0.0;
@@ -672,7 +672,7 @@ __global__ void __launch_bounds__(kCNThreads) k_cn_column_les(NSDev D, double* _
       knp[u] = (k < n) ? kn[o + XY] : 0.0;
     }
 #pragma unroll
-    for (int u = 0; u < kCNU; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int k = kb + u;
       if (k <= n) {
         double sub, dia, sup, rhs;
@@ -742,10 +742,10 @@ __global__ void __launch_bounds__(kCNThreads) k_cn_column_les(NSDev D, double* _
   // back substitution: G(n) = G(n)/b(n); G(k) = (G(k) - c(k) G(k+1))/b(k)
   double x = g / b;
   fld[base + (int64_t)(n - 1) * XY] = x;
-  for (int kb = n - 1; kb >= 1; kb -= kCNU) {
-    double gv[kCNU], bv[kCNU], cv[kCNU];
+  for (int kb = n - 1; kb >= 1; kb -= U) {
+    double gv[U], bv[U], cv[U];
 #pragma unroll
-    for (int u = 0; u < kCNU; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int k = kb - u;
       const int64_t o = base + (int64_t)(k - 1) * XY;
       gv[u] = (k >= 1) ? fld[o] : 0.0;
@@ -753,7 +753,7 @@ __global__ void __launch_bounds__(kCNThreads) k_cn_column_les(NSDev D, double* _
       cv[u] = (k >= 1) ? cc[o] : 0.0;
     }
 #pragma unroll
-    for (int u = 0; u < kCNU; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int k = kb - u;
       if (k >= 1) {
         x = (gv[u] - cv[u] * x) / bv[u];
@@ -1005,22 +1005,35 @@ void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFa
   launch_images(D, fld, nullptr, nullptr, s);
 }
 
-void launch_cn_les(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
-                   double rkdt, const ZRule& R, const double* kT, double* b, double* c, cudaStream_t s) {
-  const int tx = kCNThreads;
-  CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc, F.sub, F.diag};
+template <int kVar, int U, int TPB>
+static void cn_les_launch(const NSDev& D, double* fld, const double* q, const CNFac& f, double a3, double rkdt,
+                          const ZRule& R, const double* kT, double* b, double* c, cudaStream_t s) {
   const size_t sm = 10 * (size_t)(D.nz + 3) * sizeof(double);
-  for (const void* f : {(const void*)k_cn_column_les<1>, (const void*)k_cn_column_les<2>,
-                        (const void*)k_cn_column_les<3>, (const void*)k_cn_column_les<5>,
-                        (const void*)k_cn_column_les<8>})
-    set_smem_limit_once(f, 200 * 1024);
-  const dim3 g = col_grid(D, tx);
+  set_smem_limit_once((const void*)k_cn_column_les<kVar, U, TPB>, 200 * 1024);
+  k_cn_column_les<kVar, U, TPB><<<col_grid(D, TPB), TPB, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c);
+}
+
+template <int kVar>
+static void cn_les_variant(const NSDev& D, double* fld, const double* q, const CNFac& f, double a3, double rkdt,
+                           const ZRule& R, const double* kT, double* b, double* c, int variant, cudaStream_t s) {
+  switch (variant) {
+    case 1: cn_les_launch<kVar, 4, 128>(D, fld, q, f, a3, rkdt, R, kT, b, c, s); break;
+    case 2: cn_les_launch<kVar, 8, 128>(D, fld, q, f, a3, rkdt, R, kT, b, c, s); break;
+    case 3: cn_les_launch<kVar, 16, 128>(D, fld, q, f, a3, rkdt, R, kT, b, c, s); break;
+    default: cn_les_launch<kVar, kCNU, kCNThreads>(D, fld, q, f, a3, rkdt, R, kT, b, c, s); break;
+  }
+}
+
+void launch_cn_les(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
+                   double rkdt, const ZRule& R, const double* kT, double* b, double* c, int variant,
+                   cudaStream_t s) {
+  CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc, F.sub, F.diag};
   switch (var) {
-    case 1: k_cn_column_les<1><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
-    case 2: k_cn_column_les<2><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
-    case 3: k_cn_column_les<3><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
-    case 5: k_cn_column_les<5><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
-    default: k_cn_column_les<8><<<g, tx, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c); break;
+    case 1: cn_les_variant<1>(D, fld, q, f, a3, rkdt, R, kT, b, c, variant, s); break;
+    case 2: cn_les_variant<2>(D, fld, q, f, a3, rkdt, R, kT, b, c, variant, s); break;
+    case 3: cn_les_variant<3>(D, fld, q, f, a3, rkdt, R, kT, b, c, variant, s); break;
+    case 5: cn_les_variant<5>(D, fld, q, f, a3, rkdt, R, kT, b, c, variant, s); break;
+    default: cn_les_variant<8>(D, fld, q, f, a3, rkdt, R, kT, b, c, variant, s); break;
   }
   count_launch();
   launch_images(D, fld, nullptr, nullptr, s);

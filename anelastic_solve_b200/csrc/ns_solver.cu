@@ -270,49 +270,69 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
 // fastest kept per (device, grid) for the process.  The variants compute
 // the same bits.
 int NSSolver::tune_cn() {
-  // ANEL_CN_VARIANT=v forces one variant (no timing): for tests
-  const char* force = std::getenv("ANEL_CN_VARIANT");
-  if (force && *force) {
-    const int v = std::atoi(force);
-    if (v < 0 || v >= kCNVariants) {
-      set_error("ANEL_CN_VARIANT=%s: variants are 0..%d", force, kCNVariants - 1);
-      return ANEL_ERR_ARG;
+  // one kernel's variants: forced by the environment variable (no timing;
+  // for tests), looked up in the registry, or timed here on this
+  // context's own u and q (all zero at this point; the factors of a
+  // placeholder rkdt are dropped afterwards)
+  bool timed = false;
+  auto pick = [&](const char* name, int nvar, const char* env, auto run, int* out) -> int {
+    const char* force = std::getenv(env);
+    if (force && *force) {
+      const int v = std::atoi(force);
+      if (v < 0 || v >= nvar) {
+        set_error("%s=%s: variants are 0..%d", env, force, nvar - 1);
+        return ANEL_ERR_ARG;
+      }
+      *out = v;
+      return ANEL_OK;
     }
-    cnvar_ = v;
+    char key[128];
+    std::snprintf(key, sizeof(key), "%s dev%d %dx%dx%d", name, device_, nx_, ny_, nz_);
+    int v = tune_lookup(key);
+    if (v < 0 && !tune_enabled()) v = 0;
+    if (v < 0) {
+      constexpr int kReps = 3;
+      if (!timed) {
+        const int st = cn_factors(0, 1e-3, stream_);
+        if (st != ANEL_OK) return st;
+        timed = true;
+      }
+      std::vector<double> ms(nvar, 0.0);
+      for (int q = 0; q < nvar; ++q) {
+        run(q);
+        ANEL_CUDA_TRY(cudaEventRecord(ev0_, stream_));
+        for (int r = 0; r < kReps; ++r) run(q);
+        ANEL_CUDA_TRY(cudaEventRecord(ev1_, stream_));
+        ANEL_CUDA_TRY(cudaEventSynchronize(ev1_));
+        float t = 0.f;
+        ANEL_CUDA_TRY(cudaEventElapsedTime(&t, ev0_, ev1_));
+        ms[q] = t / kReps;
+      }
+      const int le = check_launch("column solve tuning");
+      if (le != ANEL_OK) return le;
+      v = 0;
+      for (int q = 1; q < nvar; ++q)
+        if (ms[q] < ms[v]) v = q;
+      tune_store(key, v, ms);
+    }
+    *out = v;
     return ANEL_OK;
-  }
-  char key[128];
-  std::snprintf(key, sizeof(key), "k_cn_column dev%d %dx%dx%d", device_, nx_, ny_, nz_);
-  int v = tune_lookup(key);
-  if (v < 0 && !tune_enabled()) v = 0;
-  if (v < 0) {
-    constexpr int kReps = 3;
-    const int st = cn_factors(0, 1e-3, stream_);
-    if (st != ANEL_OK) return st;
-    const ZRule R = zrule(NV_U);
-    std::vector<double> ms(kCNVariants, 0.0);
-    for (int q = 0; q < kCNVariants; ++q) {
-      launch_cn(D_, 1, D_.u, D_.qu, fac(0, 0), 1.0 / 3.0, 1e-3, R, q, stream_);
-      ANEL_CUDA_TRY(cudaEventRecord(ev0_, stream_));
-      for (int r = 0; r < kReps; ++r) launch_cn(D_, 1, D_.u, D_.qu, fac(0, 0), 1.0 / 3.0, 1e-3, R, q, stream_);
-      ANEL_CUDA_TRY(cudaEventRecord(ev1_, stream_));
-      ANEL_CUDA_TRY(cudaEventSynchronize(ev1_));
-      float t = 0.f;
-      ANEL_CUDA_TRY(cudaEventElapsedTime(&t, ev0_, ev1_));
-      ms[q] = t / kReps;
-    }
-    const int le = check_launch("column solve tuning");
-    if (le != ANEL_OK) return le;
-    v = 0;
-    for (int q = 1; q < kCNVariants; ++q)
-      if (ms[q] < ms[v]) v = q;
-    tune_store(key, v, ms);
+  };
+  const ZRule R = zrule(NV_U);
+  int st = pick("k_cn_column", kCNVariants, "ANEL_CN_VARIANT", [&](int q) {
+    launch_cn(D_, 1, D_.u, D_.qu, fac(0, 0), 1.0 / 3.0, 1e-3, R, q, stream_);
+  }, &cnvar_);
+  if (st == ANEL_OK && D_.vles)
+    st = pick("k_cn_column_les", kCNLesVariants, "ANEL_CN_LES_VARIANT", [&](int q) {
+      launch_cn_les(D_, 1, D_.u, D_.qu, fac(0, 0), 1.0 / 3.0, 1e-3, R, D_.nuT, d_cnb_, d_cnc_, q, stream_);
+    }, &cnlesvar_);
+  if (st != ANEL_OK) return st;
+  if (timed) {
     // back to the state of a fresh context
     ANEL_CUDA_TRY(cudaMemsetAsync(D_.u, 0, G_ * sizeof(double), stream_));
     ANEL_CUDA_TRY(cudaStreamSynchronize(stream_));
     cn_rkdt_[0] = -1.0;
   }
-  cnvar_ = v;
   return ANEL_OK;
 }
 
@@ -549,7 +569,7 @@ int NSSolver::substep_pre(double a1, double a2, double a3, double dt_rk, double 
   // var_advance_CN_PL: with Vmodel = SSM every variable gets the eddy
   // terms (the LES block is gated on Vmodel, NSsolver.F90:3160-3190)
   auto cn = [&](int var, double* f, const double* q, int vi, const ZRule& R, const double* kT, cudaStream_t st) {
-    if (D_.vles) launch_cn_les(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, kT, d_cnb_, d_cnc_, st);
+    if (D_.vles) launch_cn_les(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, kT, d_cnb_, d_cnc_, cnlesvar_, st);
     else launch_cn(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, cnvar_, st);
   };
   cn(1, D_.u, D_.qu, 0, ru, D_.nuT, s);

@@ -172,7 +172,8 @@ class NSSolver {
   double* d_cn_ = nullptr;          // CN factors: 3 slots x 5 vars x 9 arrays x (nz+2)
   double* h_cn_ = nullptr;          // pinned staging of the same
   double cn_rkdt_[3] = {-1, -1, -1};
-  int cnvar_ = 0;  // launch variant of the DNS column solve (tune_cn)
+  int cnvar_ = 0;     // launch variant of the DNS column solve (tune_cn)
+  int cnlesvar_ = 0;  // and of the LES column solve
   // the RHS accumulators q_* hold zero ghost cells and the previous step's
   // interior values only (no set_fields, reset or scratch use since the
   // last zeroing): the first sub-step's a1 = 0 form overwrites every

@@ -350,3 +350,20 @@ def test_clip_steps_bitwise():
     s2.set_fields({k: start[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
     s2.step(3)
     assert s2.get_fields(("rho",))["rho"][1:-1, 1:-1, 1:-1].min() < clip[0]
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_les_cn_launch_variants_bitwise(variant, monkeypatch):
+    """Every launch variant of the LES Crank-Nicolson column solve (rows per
+    load batch, columns per block: the autotuner's candidates, forced here
+    through ANEL_CN_LES_VARIANT) gives the oracle's fields bit for bit over
+    two LES steps."""
+    monkeypatch.setenv("ANEL_CN_LES_VARIANT", str(variant))
+    g_, o, s, f, start = setup_case(Re=50000.0, g=-0.1, amp=1e-2, les=True, **LES_CASES[list(LES_CASES)[0]])
+    for _ in range(2):
+        o.step()
+        s.step(1)
+    names = CMP + ("nuT", "kappaT", "nappaT")
+    got = s.get_fields(names)
+    for name in names:
+        np.testing.assert_array_equal(got[name], f[name], err_msg=name)
