@@ -131,7 +131,7 @@ class NSParams(C.Structure):
                 ("les_freq", C.c_int32), ("tb", ((C.c_int32 * 8) * 2) * 3),
                 ("vb", ((C.c_double * 8) * 2) * 3), ("ew", C.c_int32), ("scal1_on", C.c_int32),
                 ("test_ratio", C.c_double), ("filt", C.c_int32 * 3), ("stretched", C.c_int32 * 3),
-                ("interp", C.c_int32), ("clip", C.c_int32),
+                ("interp", C.c_int32), ("clip", C.c_int32), ("pguess", C.c_int32),
                 ("rho_min", C.c_double), ("rho_max", C.c_double),
                 ("scal1_min", C.c_double), ("scal1_max", C.c_double)]
 
@@ -219,7 +219,7 @@ def make_ns_params(Re=1000.0, Pr=1.0, Sc=1.0, cfl=1e6, dtmax=0.01, g=-0.12, les=
                    ssm_const=0.0289, pr_sgs=0.7, les_start=0, les_freq=1,
                    les_damp=DAMP_NONE, les_delta=DELTA_3ROOT, ew=1, scal1_on=1, models=None,
                    test_ratio=2.449489742783178, filt=(1, 1, 1), stretched=(0, 0, 0),
-                   interp=None, clip=None) -> NSParams:
+                   interp=None, clip=None, pguess=0) -> NSParams:
     """Shear-layer parameters: gravity constant g from t = 0 (Ginit = Gfinal
     = g, GT1 = GT2 = 0), free-slip z walls, periodic x and y."""
     p = NSParams()
@@ -240,6 +240,7 @@ def make_ns_params(Re=1000.0, Pr=1.0, Sc=1.0, cfl=1e6, dtmax=0.01, g=-0.12, les=
     p.les_start, p.les_freq = int(les_start), int(les_freq)
     p.ew = int(ew)
     p.scal1_on = int(scal1_on)
+    p.pguess = int(pguess)
     # clip: None (off) or (rho_min, rho_max, scal1_min, scal1_max)
     if clip is not None:
         p.clip = 1

@@ -780,6 +780,17 @@ __global__ void __launch_bounds__(128) k_sgs(NSDev D) {
   FA(D.nT, i, j, k) = -(D.CSs[k - 1] + 0.0) * dg2 * modS + 0.0;
 }
 
+// Pressure initial guess: p = 2 h1 - h2 on the interior (the multigrid's
+// boundary pass rebuilds the ghosts before the first residual).
+__global__ void k_extrap(NSDev D, double* __restrict__ p, const double* __restrict__ h1,
+                         const double* __restrict__ h2) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k = 2 + blockIdx.z;
+  if (i > D.nx + 1) return;
+  FA(p, i, j, k) = 2.0 * FA(h1, i, j, k) - FA(h2, i, j, k);
+}
+
 // ------------------------------------------------------------ clipVS
 // Routines.F90:301-380 on the interior: below vmin -> vmin, then above
 // vmax -> vmax (NaN passes unchanged, as both comparisons are false).
@@ -816,7 +827,9 @@ __global__ void k_psource(NSDev D, double rdt) {
 // Pgrad (NSsolver.F90:2023-2085): one thread per interior cell (the update
 // of a cell reads p only), then ghost(u,'u'), ghost(v,'v'), ghost(w,'w')
 // (NSsolver.F90:572-574) by columns.
-__global__ void __launch_bounds__(128) k_pgrad(NSDev D, double dt) {
+// hist (may be null): the interior of p is also copied there (the history
+// of the pressure initial guess)
+__global__ void __launch_bounds__(128) k_pgrad(NSDev D, double dt, double* __restrict__ hist) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
   const int k = 2 + blockIdx.z;
@@ -825,6 +838,7 @@ __global__ void __launch_bounds__(128) k_pgrad(NSDev D, double dt) {
   const double* __restrict__ p = D.p;
   const double rk = D.rz[k - 1];
   const double pk = FA(p, i, j, k);
+  if (hist) FA(hist, i, j, k) = pk;
   FA(D.u, i, j, k) = FA(D.u, i, j, k) - (FA(p, i + 1, j, k) / rk - pk / rk) * MT(D.rdxe, i) * dt;
   FA(D.v, i, j, k) = FA(D.v, i, j, k) - (FA(p, i, j + 1, k) / rk - pk / rk) * MT(D.rdye, j) * dt;
   if (k <= kend_w)
@@ -1248,9 +1262,14 @@ void launch_psource(const NSDev& D, double dt, cudaStream_t s) {
   count_launch();
 }
 
+void launch_extrap(const NSDev& D, double* p, const double* h1, const double* h2, cudaStream_t s) {
+  k_extrap<<<cell_grid(D, 128), 128, 0, s>>>(D, p, h1, h2);
+  count_launch();
+}
+
 void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, const ZRule& Rw,
-                  cudaStream_t s) {
-  k_pgrad<<<cell_grid(D, 128), 128, 0, s>>>(D, dt);
+                  cudaStream_t s, double* hist) {
+  k_pgrad<<<cell_grid(D, 128), 128, 0, s>>>(D, dt, hist);
   k_pgrad_ghost<<<col_grid(D, 64), 64, 0, s>>>(D, Ru, Rv, Rw);
   count_launch(2);
   launch_images(D, D.u, D.v, D.w, s);

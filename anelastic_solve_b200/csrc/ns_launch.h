@@ -41,8 +41,11 @@ void launch_psource(const NSDev& D, double dt, cudaStream_t s);
 // for u (q = 0), v (1), w (2) at Fortran linear index c.
 void launch_init_shear(const NSDev& D, const double* prof, uint32_t seed, double amp, double zmax,
                        cudaStream_t s);
+// hist (may be null): a copy of p's interior (pressure guess history)
 void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, const ZRule& Rw,
-                  cudaStream_t s);
+                  cudaStream_t s, double* hist = nullptr);
+// p = 2 h1 - h2 on the interior (the extrapolated pressure guess)
+void launch_extrap(const NSDev& D, double* p, const double* h1, const double* h2, cudaStream_t s);
 void launch_ghost_field(const NSDev& D, double* a, const ZRule& R, cudaStream_t s);
 // clipVS (Routines.F90:301-380) of a cell-centred field's interior
 void launch_clip(const NSDev& D, double* a, double vmin, double vmax, cudaStream_t s);

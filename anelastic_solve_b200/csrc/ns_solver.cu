@@ -39,6 +39,8 @@ NSSolver::~NSSolver() {
   cudaFree(d_cnc_);
   cudaFree(d_red_);
   cudaFree(d_part_);
+  for (auto& h : hist_)
+    for (double* a : h) cudaFree(a);
   if (h_cn_) cudaFreeHost(h_cn_);
   if (h_red_) cudaFreeHost(h_red_);
   if (ev0_) cudaEventDestroy(ev0_);
@@ -548,6 +550,16 @@ int NSSolver::get_fields(const anel_fields* f, int mem, cudaStream_t s) {
   return ANEL_OK;
 }
 
+int NSSolver::ensure_hist() {
+  if (hist_[0][0]) return ANEL_OK;
+  for (auto& h : hist_)
+    for (double*& a : h) {
+      ANEL_CUDA_TRY(cudaMalloc(&a, G_ * sizeof(double)));
+      ANEL_CUDA_TRY(cudaMemset(a, 0, G_ * sizeof(double)));
+    }
+  return ANEL_OK;
+}
+
 // --------------------------------------------------------------- rk_ss
 // rk_ss (NSsolver.F90:418-583) in two halves around the pressure solve:
 // RHS, Crank-Nicolson columns and Psource, then (after the solve) Pgrad.
@@ -576,6 +588,10 @@ int NSSolver::substep_pre(double a1, double a2, double a3, double dt_rk, double 
   cn(2, D_.v, D_.qv, 1, rv, D_.nuT, s);
   cn(3, D_.w, D_.qw, 2, rw, D_.nuT, s);
   launch_psource(D_, dt_rk, s);
+  if (prm_.pguess && cur_sub_ >= 0 && nhist_[cur_sub_] >= 2) {
+    const int q = cur_sub_;
+    launch_extrap(D_, D_.p, hist_[q][last_[q]], hist_[q][last_[q] ^ 1], s);
+  }
   cn(5, D_.rho, D_.qr, 3, zrule(NV_RHO), D_.kT, s);
   if (prm_.scal1_on) cn(8, D_.s, D_.qs, 4, zrule(NV_SCAL1), D_.nT, s);
   const size_t fb = G_ * sizeof(double);
@@ -604,7 +620,16 @@ int NSSolver::substep_post(const anel_mg_report& rep, cudaStream_t s, int* iters
   acc_mg_ms_ += rep.ms;
   acc_sweep_ms_ += rep.fine_sweep_ms;
   acc_sweeps_ += rep.fine_sweeps;
-  launch_pgrad(D_, pend_dtrk_, zrule(NV_U), zrule(NV_V), zrule(NV_W), s);
+  double* hist = nullptr;
+  if (prm_.pguess && cur_sub_ >= 0) {
+    const int st = ensure_hist();
+    if (st != ANEL_OK) return st;
+    const int q = cur_sub_;
+    last_[q] ^= 1;  // the older buffer takes this solution
+    hist = hist_[q][last_[q]];
+    nhist_[q] = nhist_[q] < 2 ? nhist_[q] + 1 : 2;
+  }
+  launch_pgrad(D_, pend_dtrk_, zrule(NV_U), zrule(NV_V), zrule(NV_W), s, hist);
   fields_changed();
   if (iters) *iters = rep.iter;
   if (relmax) *relmax = rep.relmax;
@@ -642,6 +667,7 @@ int NSSolver::reset(const anel_ns_params* ns, cudaStream_t s) {
   prm_ = *ns;
   temps_clean_ = false;
   fields_changed();
+  for (int q = 0; q < 3; ++q) nhist_[q] = 0;
   rRe_ = 1.0 / ns->Re;
   rPr_ = 1.0 / ns->Pr;
   rSc_ = 1.0 / ns->Sc;
@@ -893,7 +919,9 @@ int NSSolver::step(int nsteps, cudaStream_t s, anel_step_report* rep) {
     for (int q = 0; q < 3; ++q) {
       if (les && nstep_ > prm_.les_start) launch_sgs(D_, zrule(NV_CFLUC), s);
       io_last_sub_ = io_out_ && n == nsteps - 1 && q == 2;
+      cur_sub_ = q;
       st = substep(kA1[q], 1.0, kA3[q], DTR[q], delt, s, &r.mg_iter[q], &r.mg_relmax[q], true);
+      cur_sub_ = -1;
       io_last_sub_ = false;
       if (st != ANEL_OK) return st;
       clip_scalars(s);
@@ -969,6 +997,7 @@ int NSSolver::step_cohort(NSSolver* const* ms, int n, int nsteps, MGSolver* bmg,
         NSSolver* m = ms[b];
         if (m->D_.vles && m->nstep_ > m->prm_.les_start) launch_sgs(m->D_, m->zrule(NV_CFLUC), s);
         const double DTR[3] = {1.0 / 3.0 * delt[b], 5.0 / 12.0 * delt[b], 1.0 / 4.0 * delt[b]};
+        m->cur_sub_ = q;
         const int st = m->substep_pre(kA1[q], 1.0, kA3[q], DTR[q], delt[b], s, true);
         if (st != ANEL_OK) return st;
       }
@@ -977,6 +1006,7 @@ int NSSolver::step_cohort(NSSolver* const* ms, int n, int nsteps, MGSolver* bmg,
       for (int b = 0; b < n; ++b) {
         mrep[b].ms /= n;  // the batch's device time, shared out
         const int st = ms[b]->substep_post(mrep[b], s, &r[b].mg_iter[q], &r[b].mg_relmax[q]);
+        ms[b]->cur_sub_ = -1;
         if (st != ANEL_OK) return st;
         ms[b]->clip_scalars(s);
       }

@@ -99,6 +99,13 @@ class NSSolver {
   bool cfl_ready_ = false, div_ready_ = false;
 
   void fields_changed() { cfl_ready_ = div_ready_ = false; }
+  // pressure initial guess (prm_.pguess): per sub-step index, the member's
+  // last two solutions (hist_[q][last_[q]] the newest), nhist_[q] of them
+  // valid; cur_sub_ is the sub-step index inside step() (-1 elsewhere)
+  double* hist_[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+  int last_[3] = {0, 0, 0}, nhist_[3] = {0, 0, 0};
+  int cur_sub_ = -1;
+  int ensure_hist();
   int divergence_pass(cudaStream_t s, bool with_cfl);
   int divergence_read(cudaStream_t s, double* out);
   void divergence_issue(cudaStream_t s);

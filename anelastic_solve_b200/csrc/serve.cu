@@ -402,8 +402,9 @@ class ServeEngine {
   }
 
   // A cohort of the first member's bucket: one step of every member per
-  // round (NSSolver::step_cohort with the bucket's batch solver), members
-  // admitted and retired at step boundaries, until the bucket runs dry.
+  // pass of the loop (NSSolver::step_cohort with the bucket's batch
+  // solver), members admitted and retired at step boundaries, until the
+  // bucket runs dry.
   void run_cohort(Running* first) {
     const std::string key = first->job->key;
     int st = ANEL_OK;

@@ -159,7 +159,10 @@ def mg_params(lv, precision, mode=None, smoother=None):
                               mode=abi.MODE_METRIC if mode is None else mode, stop=abi.STOP_RESID)
 
 
-def ns_params(phys):
+def ns_params(phys, pguess=0):
+    """pguess 1: each sub-step's pressure solve starts from the linear
+    extrapolation of the member's solutions of that sub-step in the last
+    two steps (an extension; 0 = the reference's start from the current p)."""
     from anelastic_solve_b200 import abi
 
     # DeltaT_max large: the CFL condition sets the step (calcdt)
@@ -168,7 +171,7 @@ def ns_params(phys):
                               ew=1, scal1_on=0, les=phys.get("les", False), ssm_const=0.0289,
                               pr_sgs=0.7, les_damp=abi.DAMP_NONE, les_start=0, les_freq=1,
                               models=(abi.MODEL_DSM,) * 3 if dsm else None, stretched=(0, 0, 1),
-                              interp=abi.DIAG_CORRECTED)
+                              interp=abi.DIAG_CORRECTED, pguess=pguess)
 
 
 def poisson_rhs(g, seed=1):
@@ -234,7 +237,8 @@ def run_dns(args, rank, world, local_rank):
     g = G.shear_layer_grid(*n, stretched=True)
     N = g.x.n * g.y.n * g.z.n
     prec = abi.PREC_MIXED if args.prec == "mixed" else abi.PREC_FP64
-    s = NSSolver(g, mg_params(lv, prec), ns_params(phys), device=local_rank)
+    s = NSSolver(g, mg_params(lv, prec), ns_params(phys, args.pguess if args.prec == "mixed" else 0),
+                 device=local_rank)
     f = initial_state(g, phys)
     s.set_fields({k: f[k] for k in ("u", "v", "w", "p", "rho", "scal1", "r", "densityBG")})
     del f
@@ -776,6 +780,10 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 multigrid companion")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--pguess", type=int, default=0, choices=[0, 1],
+                    help="mixed runs: 1 = each sub-step's pressure solve starts from the linear "
+                         "extrapolation of that sub-step's last two solutions; 0 = from the current "
+                         "p, as the reference (default)")
     ap.add_argument("--members", type=int, default=1,
                     help="poisson workloads: also time this many solves one by one and batched")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the stream")
@@ -809,6 +817,8 @@ def main():
                               f"Ri={-phys['g']:g}, amp {phys['amp']:g}, CFL {phys['cfl']:g}, "
                               f"MG to ||f-A p||/||f|| <= {TOL:g} each sub-step",
                   "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V({args.pre},{args.post}), metric, {args.prec}",
+                  "p_guess": ("2 p(n-1) - p(n-2) per sub-step (extension)"
+                              if args.pguess and args.prec == "mixed" else "current p (reference)"),
                   "ew": 1, "scal1": "off (zero)", "parallelism": f"replicas x{args.gpus}",
                   "l2": l2note}
     else:

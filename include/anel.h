@@ -260,6 +260,13 @@ typedef struct {
    * then above max -> max) and ghosted.  0 (the runfiles' Clip=no): off.
    * With scal1_on = 0 the scal1 range must contain 0. */
   int32_t clip;
+  /* Initial guess of each sub-step's pressure solve (an extension; the
+   * reference starts from the current p, pguess = 0).  1: the linear
+   * extrapolation 2 p(n-1) - p(n-2) of the member's solutions of the same
+   * sub-step in the last two steps, when both exist.  The solve still
+   * runs to the same stopping test, so it changes which iterate is
+   * returned (within the tolerance), not the accuracy. */
+  int32_t pguess;
   double rho_min, rho_max, scal1_min, scal1_max;
 } anel_ns_params;
 
