@@ -147,6 +147,7 @@ FIELD_NAMES = [n for n, _ in Fields._fields_]
 
 INIT_SHEAR = 0
 INIT_FIELDS = 1
+INIT_POISSON = 2
 
 
 class Request(C.Structure):
@@ -160,7 +161,8 @@ class Request(C.Structure):
 class Result(C.Structure):
     _fields_ = [("id", C.c_int64), ("status", C.c_int32), ("nsteps", C.c_int32),
                 ("cells", C.c_int64), ("queue_ms", C.c_double), ("run_ms", C.c_double),
-                ("latency_ms", C.c_double), ("dt_last", C.c_double), ("max_div", C.c_double)]
+                ("latency_ms", C.c_double), ("dt_last", C.c_double), ("max_div", C.c_double),
+                ("mg_iter", C.c_int32), ("reserved", C.c_int32), ("resid", C.c_double)]
 
 
 class ServeStats(C.Structure):

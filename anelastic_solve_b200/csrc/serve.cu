@@ -23,6 +23,8 @@
 //     used first, until the new context fits;
 //   * contexts stay resident between members of their bucket (fields,
 //     multigrid hierarchy, factor caches, ghost tables);
+//   * standalone pressure solves (ANEL_INIT_POISSON) of one bucket are
+//     solved together, up to kMaxCohort right-hand sides per batched solve;
 //   * results (status, queue/run/total latency) are collected by
 //     anel_serve_poll.
 // A member's arithmetic does not depend on what else runs: its kernels
@@ -130,8 +132,10 @@ class ServeEngine {
       set_error("serve: bad grid sizes or step count");
       return ANEL_ERR_ARG;
     }
-    if (r->init != ANEL_INIT_SHEAR && !(r->init == ANEL_INIT_FIELDS && r->fields_in)) {
-      set_error("serve: init must be ANEL_INIT_SHEAR, or ANEL_INIT_FIELDS with fields_in");
+    if (r->init != ANEL_INIT_SHEAR && !(r->init == ANEL_INIT_FIELDS && r->fields_in) &&
+        !(r->init == ANEL_INIT_POISSON && r->fields_in && r->fields_in->psrc)) {
+      set_error("serve: init must be ANEL_INIT_SHEAR, ANEL_INIT_FIELDS with fields_in, or "
+                "ANEL_INIT_POISSON with fields_in->psrc");
       return ANEL_ERR_ARG;
     }
     auto* job = new ServeJob();
@@ -204,6 +208,9 @@ class ServeEngine {
     const int nf = 14 + (les_any ? 3 : 0) + (nk.vmodel != ANEL_MODEL_DNS ? 2 : 0) + (dyn ? 16 : 0);
     const int64_t mgb = r->mg.precision == ANEL_PREC_MIXED ? 32 : 24;
     job->est_bytes = G * (8 * nf + mgb) + ((int64_t)64 << 20);
+    // a Poisson request holds its FP64 phi and right-hand side on the
+    // device and one member's FP32 levels in its bucket's batch solver
+    if (r->init == ANEL_INIT_POISSON) job->est_bytes = G * (16 + 16) + ((int64_t)1 << 20);
     std::lock_guard<std::mutex> lk(mu_);
     job->id = next_id_++;
     job->t_submit = Clock::now();
@@ -319,6 +326,10 @@ class ServeEngine {
         ++active_;
         peak_active_ = std::max(peak_active_, active_);
       }
+      if (r->job->req.init == ANEL_INIT_POISSON) {
+        run_poisson(r);
+        continue;
+      }
       int st = setup(*r);
       if (st == ANEL_OK && r->job->req.nsteps > 0 && r->ctx->s->mg()->batch_capable()) {
         run_cohort(r);
@@ -391,6 +402,149 @@ class ServeEngine {
       } else if (r->need_new) {
         used_ -= job.est_bytes;
       }
+      results_.push_back(r->res);
+      if (st == ANEL_OK) ++completed_;
+      else ++failed_;
+      delete r->job;
+    }
+    delete r;
+    cv_work_.notify_all();
+    cv_done_.notify_all();
+  }
+
+  // Standalone pressure solves of the first request's bucket: every pass
+  // takes the bucket's queued requests (up to kMaxCohort, admitted against
+  // the budget), copies their right-hand sides and guesses in, solves them
+  // as one batched multigrid solve (one at a time where the multigrid is
+  // not the column-layout mixed cycle) and copies the solutions out.
+  void run_poisson(Running* first) {
+    const std::string key = first->job->key;
+    int st = ANEL_OK;
+    MGSolver* mg = MGSolver::create(&first->job->grid, &first->job->req.mg, device_, &st);
+    const int64_t G = (int64_t)(first->job->grid.nx + 2) * (first->job->grid.ny + 2) *
+                      (first->job->grid.nz + 2);
+    const int64_t mbytes = G * (24 + 16) + ((int64_t)64 << 20);  // the solver's own arrays
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      cohorts_.insert(key);
+      used_ += mbytes;
+      peak_ = std::max(peak_, used_);
+    }
+    cudaStream_t sm = mg ? mg->stream() : nullptr;
+    std::vector<double*> dbuf;  // 2 G-sized device arrays per slot (phi, rhs)
+    std::vector<Running*> mem{first};
+    for (;;) {
+      if (!mg || st != ANEL_OK) {
+        for (Running* r : mem) finish_poisson(r, st != ANEL_OK ? st : ANEL_ERR_CUDA);
+        mem.clear();
+      } else {
+        // admit the bucket's queued requests
+        while ((int)mem.size() < kMaxCohort) {
+          Running* r = new Running();
+          {
+            std::lock_guard<std::mutex> lk(mu_);
+            r->job = queue_.empty() ? nullptr : admit(r->ctx, r->need_new, &key);
+            if (r->job) {
+              ++active_;
+              peak_active_ = std::max(peak_active_, active_);
+            }
+          }
+          if (!r->job) {
+            delete r;
+            break;
+          }
+          mem.push_back(r);
+        }
+      }
+      if (mem.empty()) {
+        std::lock_guard<std::mutex> lk(mu_);
+        const bool more = std::any_of(queue_.begin(), queue_.end(), [&](ServeJob* j) { return j->key == key; });
+        if (!more || !mg || st != ANEL_OK) {
+          cohorts_.erase(key);
+          used_ -= mbytes;
+          break;
+        }
+        continue;
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        peak_cohort_ = std::max(peak_cohort_, (int)mem.size());
+      }
+      const int n = (int)mem.size();
+      int sb = ANEL_OK;
+      while ((int)dbuf.size() < 2 * n && sb == ANEL_OK) {
+        double* a = nullptr;
+        if (cudaMalloc(&a, G * sizeof(double)) != cudaSuccess) {
+          cudaGetLastError();
+          sb = ANEL_ERR_NOMEM;
+        } else {
+          dbuf.push_back(a);
+        }
+      }
+      std::vector<double*> phis(n);
+      std::vector<const double*> rhss(n);
+      std::vector<anel_mg_report> reps(n);
+      const size_t fb = G * sizeof(double);
+      for (int b = 0; b < n && sb == ANEL_OK; ++b) {
+        Running* r = mem[b];
+        r->t0 = Clock::now();
+        phis[b] = dbuf[2 * b];
+        rhss[b] = dbuf[2 * b + 1];
+        const anel_fields& in = r->job->fin;
+        const cudaError_t e1 = in.p ? cudaMemcpyAsync(phis[b], in.p, fb, cudaMemcpyHostToDevice, sm)
+                                    : cudaMemsetAsync(phis[b], 0, fb, sm);
+        const cudaError_t e2 = cudaMemcpyAsync(dbuf[2 * b + 1], in.psrc, fb, cudaMemcpyHostToDevice, sm);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) sb = ANEL_ERR_CUDA;
+      }
+      if (sb == ANEL_OK) {
+        if (mg->batch_capable()) {
+          sb = mg->solve_batch(n, phis.data(), rhss.data(), sm, reps.data());
+        } else {
+          for (int b = 0; b < n && (sb == ANEL_OK || sb == ANEL_ERR_NOCONV); ++b) {
+            const int s1 = mg->solve_device(phis[b], rhss[b], sm, &reps[b]);
+            reps[b].status = s1;
+            if (s1 != ANEL_OK && s1 != ANEL_ERR_NOCONV) sb = s1;
+          }
+        }
+        if (sb == ANEL_ERR_NOCONV) sb = ANEL_OK;  // the members' own status is in their reports
+      }
+      for (int b = 0; b < n; ++b) {
+        Running* r = mem[b];
+        int s1 = sb;
+        if (s1 == ANEL_OK) {
+          r->res.mg_iter = reps[b].iter;
+          r->res.resid = reps[b].resid;
+          if (reps[b].status != ANEL_OK) s1 = reps[b].status;
+          if (r->job->has_out && r->job->fout.p &&
+              cudaMemcpyAsync(r->job->fout.p, phis[b], fb, cudaMemcpyDeviceToHost, sm) != cudaSuccess)
+            s1 = ANEL_ERR_CUDA;
+        }
+        if (sm && cudaStreamSynchronize(sm) != cudaSuccess && s1 == ANEL_OK) s1 = ANEL_ERR_CUDA;
+        finish_poisson(r, s1);
+      }
+      mem.clear();
+    }
+    if (mg) cudaStreamSynchronize(mg->stream());
+    for (double* a : dbuf) cudaFree(a);
+    delete mg;
+    cv_work_.notify_all();
+  }
+
+  // the result of a Poisson request (no stepping context to return)
+  void finish_poisson(Running* r, int st) {
+    ServeJob& job = *r->job;
+    const Clock::time_point t1 = Clock::now();
+    if (r->t0 == Clock::time_point()) r->t0 = t1;
+    r->res.id = job.id;
+    r->res.status = st;
+    r->res.cells = (int64_t)job.grid.nx * job.grid.ny * job.grid.nz;
+    r->res.queue_ms = ms_between(job.t_submit, r->t0);
+    r->res.run_ms = ms_between(r->t0, t1);
+    r->res.latency_ms = ms_between(job.t_submit, t1);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      --active_;
+      if (r->need_new) used_ -= job.est_bytes;
       results_.push_back(r->res);
       if (st == ANEL_OK) ++completed_;
       else ++failed_;

@@ -1,11 +1,13 @@
-"""Serving engine for ensembles of independent shear-layer members.
+"""Serving engine for ensembles of independent shear-layer members and
+standalone pressure solves.
 
 Thin Python face of the native engine of include/anel.h
 (``anel_serve_*``, csrc/serve.cu): requests queue in FIFO order, worker
-threads of the library run one member each on its own CUDA stream, and
-members are admitted against an HBM budget with contexts pooled per grid /
-model / multigrid setup.  Not a reference routine: each reference run is
-its own job.
+threads of the library run them per bucket (grid, models, multigrid setup)
+-- shear-layer members as cohorts stepping together with batched pressure
+solves, standalone solves in batches -- and requests are admitted against
+an HBM budget with contexts pooled per bucket.  Not a reference routine:
+each reference run is its own job.
 """
 from __future__ import annotations
 
@@ -58,6 +60,42 @@ class ServeEngine:
             fo = abi.Fields()
             for k, a in out.items():
                 setattr(fo, k, abi.dptr(a))
+            hold.append(fo)
+            req.fields_out = C.pointer(fo)
+        rid = C.c_int64(0)
+        check(lib().anel_serve_submit(self._h, C.byref(req), C.byref(rid)))
+        self._keep[rid.value] = (hold, out)
+        return rid.value
+
+    def submit_poisson(self, grid, mg: abi.MGParams, rhs, phi0=None, want_solution: bool = True) -> int:
+        """Queue one standalone pressure solve (ANEL_INIT_POISSON): the
+        ghosted FP64 right-hand side rhs, the initial guess phi0 (None:
+        zero).  Requests of one grid and multigrid setup are solved
+        together in batches.  With want_solution the solution comes back
+        from poll() under ``fields["p"]``; ``mg_iter`` and ``resid`` carry
+        the solve's report."""
+        desc, keep = abi.make_grid_desc(grid)
+        req = abi.Request()
+        req.grid = desc
+        req.mg = mg
+        req.ns = abi.make_ns_params()
+        req.init = abi.INIT_POISSON
+        hold = [keep, req]
+        fin = abi.Fields()
+        f = np.asfortranarray(rhs, dtype=np.float64)
+        hold.append(f)
+        fin.psrc = abi.dptr(f)
+        if phi0 is not None:
+            p0 = np.asfortranarray(phi0, dtype=np.float64)
+            hold.append(p0)
+            fin.p = abi.dptr(p0)
+        hold.append(fin)
+        req.fields_in = C.pointer(fin)
+        out = None
+        if want_solution:
+            out = {"p": np.zeros(grid.ghosted, order="F")}
+            fo = abi.Fields()
+            fo.p = abi.dptr(out["p"])
             hold.append(fo)
             req.fields_out = C.pointer(fo)
         rid = C.c_int64(0)

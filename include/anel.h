@@ -445,7 +445,7 @@ int anel_divergence_noalloc(int32_t nx, int32_t ny, int32_t nz, const double* u,
  * A member's fields do not depend on what else runs.  Caller arrays named in a request (fields_in, fields_out) must
  * stay alive until its result is polled. */
 typedef struct anel_serve anel_serve;
-enum { ANEL_INIT_SHEAR = 0, ANEL_INIT_FIELDS = 1 };
+enum { ANEL_INIT_SHEAR = 0, ANEL_INIT_FIELDS = 1, ANEL_INIT_POISSON = 2 };
 typedef struct {
   anel_grid_desc grid;   /* host metric arrays: copied at submit */
   anel_mg_params mg;
@@ -453,7 +453,13 @@ typedef struct {
   int32_t nsteps;        /* RK3 steps after the initial projection */
   int32_t init;          /* ANEL_INIT_SHEAR: shear layer U = tanh(zc), rho = -tanh(zc), noise
                           * amp*(2U-1) on |zc| < 2 from the Park-Miller sequence of seed;
-                          * ANEL_INIT_FIELDS: the host fields of fields_in */
+                          * ANEL_INIT_FIELDS: the host fields of fields_in;
+                          * ANEL_INIT_POISSON: a standalone pressure solve with the
+                          * request's grid and mg parameters (ns, nsteps, seed unused):
+                          * right-hand side fields_in->psrc, initial guess fields_in->p
+                          * (NULL: zero), solution to fields_out->p (may be NULL).
+                          * Requests of one bucket are solved together, up to 16 per
+                          * batched solve. */
   uint32_t seed;
   int32_t reserved;
   double amp;
@@ -470,6 +476,9 @@ typedef struct {
   double latency_ms;     /* submit -> fields ready */
   double dt_last;        /* time step of the last step */
   double max_div;        /* max |div u| after the last step */
+  int32_t mg_iter;       /* Poisson requests: V-cycles of the solve */
+  int32_t reserved;
+  double resid;          /* Poisson requests: final relative residual */
 } anel_result;
 typedef struct {
   int64_t submitted, completed, failed;

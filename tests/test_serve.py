@@ -148,3 +148,40 @@ def test_budget_admission_and_oversized_member():
     assert res[ids[3]]["status"] == abi.ERR_NOMEM
     # one context at a time, re-used by the three members of its bucket
     assert st["peak_active"] == 1 and st["peak_bytes"] <= budget
+
+
+def test_poisson_requests_batched_equal_alone():
+    """Standalone pressure solves served as one bucket (64x32x128, mixed
+    ZLINE, 1e-10): submitted at once to one worker they are solved in one
+    batched solve, and each solution, cycle count and residual equals the
+    one-member solve of its own context, bit for bit; a request with an
+    initial guess starts from it."""
+    import torch
+
+    from anelastic_solve_b200.mg import MGSolver
+
+    from .helpers import compatible, field
+
+    g = G.shear_layer_grid(64, 32, 128, stretched=True)
+    mg, _ = _params(g)
+    rng = np.random.default_rng(17)
+    rhs = [compatible(field(g, rng), g, abi.MODE_METRIC) for _ in range(5)]
+    guess = 1e-3 * field(g, np.random.default_rng(3))
+    e = ServeEngine(hbm_budget_bytes=16 << 30, max_active=1)
+    ids = [e.submit_poisson(g, mg, r, phi0=(guess if q == 2 else None)) for q, r in enumerate(rhs)]
+    res = _wait(e, ids)
+    st = e.stats()
+    e.close()
+    print(f"\npoisson requests: peak cohort {st['peak_cohort']}, cycles {[res[i]['mg_iter'] for i in ids]}")
+    assert st["peak_cohort"] > 1
+    s = MGSolver(g, mg)
+    for q, rid in enumerate(ids):
+        r = res[rid]
+        assert r["status"] == abi.OK and r["resid"] <= 1e-10
+        p0 = guess if q == 2 else np.zeros(g.ghosted, order="F")
+        d = torch.from_numpy(np.ascontiguousarray(p0.T)).cuda()
+        s.solve(d, torch.from_numpy(np.ascontiguousarray(rhs[q].T)).cuda())
+        alone = np.asfortranarray(d.cpu().numpy().T)
+        assert r["mg_iter"] == s.last_report.iter and r["resid"] == s.last_report.resid
+        np.testing.assert_array_equal(r["fields"]["p"], alone, err_msg=f"request {q}")
+    s.close()
