@@ -153,10 +153,25 @@ def mg_params(lv, precision, mode=None, smoother=None):
     zl = (smoother or SMOOTHER["smoother"]) == "zline"
     levels = (lv[0], lv[1], 1) if zl else lv
     pre, post = (SMOOTHER["pre"], SMOOTHER["post"]) if smoother is None else (2, 2)
+    fine = (SMOOTHER.get("fine_pre"), SMOOTHER.get("fine_post")) if smoother is None else (None, None)
+    if fine != (None, None):
+        # per-level counts (coarsest -> finest), the finest level's own
+        ng = max(levels)
+        pre = [pre] * (ng - 1) + [pre if fine[0] is None else fine[0]]
+        post = [post] * (ng - 1) + [post if fine[1] is None else fine[1]]
     return abi.make_mg_params(levels, maxcy=400, tolmax=TOL, pre=pre, post=post,
                               tbc=(0, 1, 0, 1, 0, 0), precision=precision,
                               smoother=abi.SMOOTHER_ZLINE if zl else abi.SMOOTHER_RBPGS,
                               mode=abi.MODE_METRIC if mode is None else mode, stop=abi.STOP_RESID)
+
+
+def fine_note(args):
+    """The finest level's own sweep counts, when set, for the config line."""
+    if args.fine_pre is None and args.fine_post is None:
+        return ""
+    fp = args.pre if args.fine_pre is None else args.fine_pre
+    fq = args.post if args.fine_post is None else args.fine_post
+    return f" (finest level V({fp},{fq}))"
 
 
 def ns_params(phys, pguess=0):
@@ -699,7 +714,7 @@ def main_serve(args, rank, world, local_rank, threads):
                           f"{args.rate:g}/s, grid uniform over {sizes}, Ri~U[0.05,0.3], Re "
                           f"log-uniform [500,4000], {args.serve_steps} RK3 steps each",
               "hbm_budget_gb": args.budget_gb, "workers": args.workers,
-              "mg": f"{args.smoother.upper()} V({args.pre},{args.post}), metric, {args.prec}, to 1e-10",
+              "mg": f"{args.smoother.upper()} V({args.pre},{args.post}){fine_note(args)}, metric, {args.prec}, to 1e-10",
               "parallelism": f"replicas x{world}", "l2": "mixed sizes (32^3 .. 256^3)"}
     if args.impl == "reference":
         if rank != 0:
@@ -777,6 +792,8 @@ def main():
                          "reference's red-black point GS with full coarsening")
     ap.add_argument("--pre", type=int, default=2, help="pre-smoothing sweeps per level")
     ap.add_argument("--post", type=int, default=2, help="post-smoothing sweeps per level")
+    ap.add_argument("--fine-pre", type=int, default=None, help="pre-smoothing sweeps on the finest level")
+    ap.add_argument("--fine-post", type=int, default=None, help="post-smoothing sweeps on the finest level")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 multigrid companion")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
@@ -794,7 +811,8 @@ def main():
     ap.add_argument("--diag", action="store_true",
                     help="dns/les: also time the per-step plane statistics (outside the timed steps)")
     args = ap.parse_args()
-    SMOOTHER.update(smoother=args.smoother, pre=args.pre, post=args.post)
+    SMOOTHER.update(smoother=args.smoother, pre=args.pre, post=args.post, fine_pre=args.fine_pre,
+                    fine_post=args.fine_post)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
@@ -816,7 +834,7 @@ def main():
         config = {"workload": f"{model} shear layer {nx}x{ny}x{nz}: Re={phys['Re']:g}, Pr=1, "
                               f"Ri={-phys['g']:g}, amp {phys['amp']:g}, CFL {phys['cfl']:g}, "
                               f"MG to ||f-A p||/||f|| <= {TOL:g} each sub-step",
-                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V({args.pre},{args.post}), metric, {args.prec}",
+                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V({args.pre},{args.post}){fine_note(args)}, metric, {args.prec}",
                   "p_guess": ("2 p(n-1) - p(n-2) per sub-step (extension)"
                               if args.pguess and args.prec == "mixed" else "current p (reference)"),
                   "ew": 1, "scal1": "off (zero)", "parallelism": f"replicas x{args.gpus}",
@@ -826,7 +844,7 @@ def main():
         unit = "cell-solves/s"
         config = {"workload": f"pressure-Poisson solve {nx}x{ny}x{nz}, tanh-stretched z, periodic "
                               f"x/y, Neumann z, to ||f-A phi||/||f|| <= {TOL:g} from phi0 = 0",
-                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V({args.pre},{args.post}), metric, {args.prec}",
+                  "grid": [nx, ny, nz], "mg_levels": list(lv), "mg": f"{args.smoother.upper()} V({args.pre},{args.post}){fine_note(args)}, metric, {args.prec}",
                   "parallelism": f"replicas x{args.gpus}",
                   "l2": l2note}
     threads = os.cpu_count() or 1
