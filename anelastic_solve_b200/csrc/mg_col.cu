@@ -100,16 +100,12 @@ void launch_col_sweep(const ColLevel& L, int color, const float* fac, int M, int
   count_launch();
 }
 
-static unsigned col_xfer_blocks(int64_t items) {
-  int64_t b = (items + kColXferThreads - 1) / kColXferThreads;
-  const int64_t cap = 148 * 8;
-  if (b > cap) b = cap;
-  if (b < 1) b = 1;
-  return (unsigned)b;
+static dim3 col_xfer_grid(int64_t per_row, int rows, int nm) {
+  return dim3((unsigned)((per_row + kColXferThreads - 1) / kColXferThreads), (unsigned)rows, (unsigned)nm);
 }
 
 void launch_col_restrict(const ColLevel& F, const ColLevel& C, int cdir, cudaStream_t s) {
-  const unsigned g = col_xfer_blocks((int64_t)C.nx * C.ny * (C.nz / 4) * C.nm);
+  const dim3 g = col_xfer_grid((int64_t)C.nx * (C.nz / 4), C.ny, C.nm);
   switch (cdir & 3) {
     case 1: k_col_restrict<1><<<g, kColXferThreads, 0, s>>>(F, C); break;
     case 2: k_col_restrict<2><<<g, kColXferThreads, 0, s>>>(F, C); break;
@@ -119,7 +115,12 @@ void launch_col_restrict(const ColLevel& F, const ColLevel& C, int cdir, cudaStr
 }
 
 void launch_col_prolong(const ColLevel& F, const ColLevel& C, int cdir, cudaStream_t s) {
-  const unsigned g = col_xfer_blocks((int64_t)F.nx * F.ny * (F.nz / 4) * F.nm);
+  // groups of fine columns sharing their coarse columns (k_col_prolong)
+  const int cd = (cdir & 3) ? (cdir & 3) : 3;  // the kernel chosen below
+  const bool cx = cd & 1, cy = cd & 2;
+  const int64_t gx = cx ? F.nx / 2 + 1 : F.nx;
+  const int gy = cy ? F.ny / 2 + 1 : F.ny;
+  const dim3 g = col_xfer_grid(gx * (F.nz / 4), gy, F.nm);
   switch (cdir & 3) {
     case 1: k_col_prolong<1><<<g, kColXferThreads, 0, s>>>(F, C); break;
     case 2: k_col_prolong<2><<<g, kColXferThreads, 0, s>>>(F, C); break;

@@ -666,119 +666,147 @@ __device__ __forceinline__ float4 f4scale(float s, float4 a) {
 
 constexpr int kColXferThreads = 256;
 
+// Grid of the transfer kernels: x runs over (column of a row, 4-row chunk)
+// with the chunk fastest, y over the rows of columns, z over the members of
+// a batch; 32-bit indices (a row holds far fewer than 2^32 chunks).
+
 // mg_restr's x/y variants (z is not coarsened): coarse f of interior cells
 // (ic,jc,k..k+3) from the residuals of their children, in restrict_value's
-// order.  One thread per coarse column and 4-row chunk (grid-stride); the
-// caller zeroes coarse phi.
+// order.  One thread per coarse column and 4-row chunk; the caller zeroes
+// coarse phi.
 template <int CD>
 __global__ void __launch_bounds__(kColXferThreads) k_col_restrict(ColLevel Fb, ColLevel Cb) {
-  const int nch = Cb.nz >> 2;
-  const int64_t items = (int64_t)Cb.nx * Cb.ny * nch;  // of one member
+  const int m = blockIdx.z;
+  if (!col_active(Cb, m)) return;
+  const unsigned nch = (unsigned)Cb.nz >> 2;
+  const unsigned t = blockIdx.x * kColXferThreads + threadIdx.x;
+  if (t >= (unsigned)Cb.nx * nch) return;
   constexpr bool cx = CD & 1, cy = CD & 2;
-  for (int64_t tt = (int64_t)blockIdx.x * kColXferThreads + threadIdx.x; tt < items * Cb.nm;
-       tt += (int64_t)gridDim.x * kColXferThreads) {
-    const int m = Cb.nm == 1 ? 0 : (int)(tt / items);
-    if (!col_active(Cb, m)) continue;
-    const int64_t t = tt - (int64_t)m * items;
-    const ColLevel F = col_member(Fb, m);
-    const ColLevel C = col_member(Cb, m);
-    const int ch = (int)(t % nch);
-    const int64_t col = t / nch;
-    const int ic = 2 + (int)(col % C.nx), jc = 2 + (int)(col / C.nx);
-    const int k = 2 + 4 * ch;
-    const int i = cx ? 2 * ic - 2 : ic;
-    const int j = cy ? 2 * jc - 2 : jc;
-    float4 v;
-    if constexpr (cx && cy) {
-      float4 s = col_resid4(F, i, j, k);
-      s = f4add(s, col_resid4(F, i + 1, j, k));
-      s = f4add(s, col_resid4(F, i, j + 1, k));
-      s = f4add(s, col_resid4(F, i + 1, j + 1, k));
-      v = f4scale(0.25f, s);
-    } else if constexpr (cx) {
-      v = f4scale(0.5f, f4add(col_resid4(F, i, j, k), col_resid4(F, i + 1, j, k)));
-    } else {
-      v = f4scale(0.5f, f4add(col_resid4(F, i, j, k), col_resid4(F, i, j + 1, k)));
-    }
-    *reinterpret_cast<float4*>(C.src + col_cell(C, ic, jc, k)) = v;
+  const ColLevel F = col_member(Fb, m);
+  const ColLevel C = col_member(Cb, m);
+  const unsigned q = t / nch;
+  const int ch = (int)(t - q * nch);
+  const int ic = 2 + (int)q, jc = 2 + (int)blockIdx.y;
+  const int k = 2 + 4 * ch;
+  const int i = cx ? 2 * ic - 2 : ic;
+  const int j = cy ? 2 * jc - 2 : jc;
+  float4 v;
+  if constexpr (cx && cy) {
+    float4 s = col_resid4(F, i, j, k);
+    s = f4add(s, col_resid4(F, i + 1, j, k));
+    s = f4add(s, col_resid4(F, i, j + 1, k));
+    s = f4add(s, col_resid4(F, i + 1, j + 1, k));
+    v = f4scale(0.25f, s);
+  } else if constexpr (cx) {
+    v = f4scale(0.5f, f4add(col_resid4(F, i, j, k), col_resid4(F, i + 1, j, k)));
+  } else {
+    v = f4scale(0.5f, f4add(col_resid4(F, i, j, k), col_resid4(F, i, j + 1, k)));
+  }
+  *reinterpret_cast<float4*>(C.src + col_cell(C, ic, jc, k)) = v;
+}
+
+// Adds the correction chunk corr to rows k..k+3 of fine column (i,j) and
+// writes the sum to the column, to its image columns and, from the first
+// and last chunks, to its z ghosts (the boundary pass of the row-major
+// cycle).
+__device__ __forceinline__ void col_prolong_store(const ColLevel& F, int i, int j, int k, int ch, int nch,
+                                                  float4 corr) {
+  const int64_t c = col_cell(F, i, j, k);
+  float* __restrict__ P = F.phi;
+  const float4 old = *reinterpret_cast<const float4*>(P + c);
+  const float4 v = f4add(old, corr);
+  int d0 = kNoImage, d1 = kNoImage, d2 = kNoImage;
+  if (F.img) {
+    const int* im = F.img + 3 * ((i - 2) + (int64_t)F.nx * (j - 2));
+    d0 = im[0];
+    d1 = im[1];
+    d2 = im[2];
+  }
+  const int64_t o0 = (int64_t)d0 * F.CS, o1 = (int64_t)d1 * F.CS, o2 = (int64_t)d2 * F.CS;
+  *reinterpret_cast<float4*>(P + c) = v;
+  if (d0 != kNoImage) *reinterpret_cast<float4*>(P + c + o0) = v;
+  if (d1 != kNoImage) *reinterpret_cast<float4*>(P + c + o1) = v;
+  if (d2 != kNoImage) *reinterpret_cast<float4*>(P + c + o2) = v;
+  // z ghosts: the first chunk writes the ghosts that copy row k = 2 or
+  // are zero, the last chunk those that copy row k = nz+1
+  const bool h0 = d0 != kNoImage, h1 = d1 != kNoImage, h2 = d2 != kNoImage;
+  const int64_t g1 = c - (k - 1), gZ = c + (F.nz + 2 - k);
+  if (ch == 0) {
+    if (F.z1 != 2) col_put(P, g1, F.z1 == 1 ? v.x : 0.f, o0, o1, o2, h0, h1, h2);
+    if (F.zZ != 2) col_put(P, gZ, F.zZ == 1 ? v.x : 0.f, o0, o1, o2, h0, h1, h2);
+  }
+  if (ch == nch - 1) {
+    if (F.z1 == 2) col_put(P, g1, v.w, o0, o1, o2, h0, h1, h2);
+    if (F.zZ == 2) col_put(P, gZ, v.w, o0, o1, o2, h0, h1, h2);
   }
 }
 
 // mg_cor's x/y variants for the fine interior, in prolong_corr's order,
-// with the ghost copies of the updated cells written alongside (the
-// boundary pass of the row-major cycle).  One thread per fine column and
-// 4-row chunk (grid-stride).
+// with the ghost copies of the updated cells written alongside.  Fine
+// columns i = 2g+1 and 2g+2 both interpolate between coarse columns g+1
+// and g+2 (weights 3:1 and 1:3) when x is coarsened, likewise in y: one
+// thread per 4-row chunk of such a group of up to 2x2 fine columns (the
+// ghost columns i = 1, nx+2 / j = 1, ny+2 of the edge groups are skipped)
+// loads the four coarse chunks once.
 template <int CD>
 __global__ void __launch_bounds__(kColXferThreads) k_col_prolong(ColLevel Fb, ColLevel Cb) {
-  const int nch = Fb.nz >> 2;
-  const int64_t items = (int64_t)Fb.nx * Fb.ny * nch;  // of one member
+  const int m = blockIdx.z;
+  if (!col_active(Fb, m)) return;
   constexpr bool cx = CD & 1, cy = CD & 2;
-  for (int64_t tt = (int64_t)blockIdx.x * kColXferThreads + threadIdx.x; tt < items * Fb.nm;
-       tt += (int64_t)gridDim.x * kColXferThreads) {
-    const int m = Fb.nm == 1 ? 0 : (int)(tt / items);
-    if (!col_active(Fb, m)) continue;
-    const int64_t t = tt - (int64_t)m * items;
-    const ColLevel F = col_member(Fb, m);
-    const ColLevel C = col_member(Cb, m);
-    const int ch = (int)(t % nch);
-    const int64_t col = t / nch;
-    const int i = 2 + (int)(col % F.nx), j = 2 + (int)(col / F.nx);
-    const int k = 2 + 4 * ch;
-    const int ic = cx ? ((i + 1) >> 1) : i;
-    const int jc = cy ? ((j + 1) >> 1) : j;
-    const float wx0 = cx ? ((i & 1) ? 3.f : 1.f) : 1.f, wx1 = cx ? ((i & 1) ? 1.f : 3.f) : 0.f;
-    const float wy0 = cy ? ((j & 1) ? 3.f : 1.f) : 1.f, wy1 = cy ? ((j & 1) ? 1.f : 3.f) : 0.f;
-    const float* __restrict__ pc = C.phi + col_cell(C, ic, jc, k);
-    const int64_t ox = C.CS, oy = (int64_t)C.X * C.CS;
-    const float4 c00 = *reinterpret_cast<const float4*>(pc);
-    float4 corr;
-    if constexpr (cx && cy) {
-      const float4 c10 = *reinterpret_cast<const float4*>(pc + ox);
-      const float4 c01 = *reinterpret_cast<const float4*>(pc + oy);
-      const float4 c11 = *reinterpret_cast<const float4*>(pc + ox + oy);
-      const float w00 = wx0 * wy0, w10 = wx1 * wy0, w01 = wx0 * wy1, w11 = wx1 * wy1;
-      auto one = [&](float a, float b, float c, float d) {
-        float s = w00 * a;
-        s = s + w10 * b;
-        s = s + w01 * c;
-        s = s + w11 * d;
-        return s / 16.f;
-      };
-      corr = make_float4(one(c00.x, c10.x, c01.x, c11.x), one(c00.y, c10.y, c01.y, c11.y),
-                         one(c00.z, c10.z, c01.z, c11.z), one(c00.w, c10.w, c01.w, c11.w));
-    } else {
-      const float4 c1 = *reinterpret_cast<const float4*>(pc + (cx ? ox : oy));
-      const float w0 = cx ? wx0 : wy0, w1 = cx ? wx1 : wy1;
-      corr = make_float4((w0 * c00.x + w1 * c1.x) / 4.f, (w0 * c00.y + w1 * c1.y) / 4.f,
-                         (w0 * c00.z + w1 * c1.z) / 4.f, (w0 * c00.w + w1 * c1.w) / 4.f);
+  const unsigned nch = (unsigned)Fb.nz >> 2;
+  const unsigned gxn = cx ? (unsigned)(Fb.nx >> 1) + 1u : (unsigned)Fb.nx;  // groups per row
+  const unsigned t = blockIdx.x * kColXferThreads + threadIdx.x;
+  if (t >= gxn * nch) return;
+  const ColLevel F = col_member(Fb, m);
+  const ColLevel C = col_member(Cb, m);
+  const unsigned q = t / nch;
+  const int ch = (int)(t - q * nch);
+  const int gx = (int)q, gy = (int)blockIdx.y;
+  const int k = 2 + 4 * ch;
+  const int i0 = cx ? 2 * gx + 1 : gx + 2, j0 = cy ? 2 * gy + 1 : gy + 2;
+  const int ic = cx ? gx + 1 : i0, jc = cy ? gy + 1 : j0;
+  const float* __restrict__ pc = C.phi + col_cell(C, ic, jc, k);
+  const int64_t ox = C.CS, oy = (int64_t)C.X * C.CS;
+  const float4 c00 = *reinterpret_cast<const float4*>(pc);
+  if constexpr (cx && cy) {
+    const float4 c10 = *reinterpret_cast<const float4*>(pc + ox);
+    const float4 c01 = *reinterpret_cast<const float4*>(pc + oy);
+    const float4 c11 = *reinterpret_cast<const float4*>(pc + ox + oy);
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      const int j = j0 + b;
+      if (j < 2 || j > F.ny + 1) continue;
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        const int i = i0 + a;
+        if (i < 2 || i > F.nx + 1) continue;
+        const float wx0 = (i & 1) ? 3.f : 1.f, wx1 = (i & 1) ? 1.f : 3.f;
+        const float wy0 = (j & 1) ? 3.f : 1.f, wy1 = (j & 1) ? 1.f : 3.f;
+        const float w00 = wx0 * wy0, w10 = wx1 * wy0, w01 = wx0 * wy1, w11 = wx1 * wy1;
+        auto one = [&](float p, float r, float u, float d) {
+          float s = w00 * p;
+          s = s + w10 * r;
+          s = s + w01 * u;
+          s = s + w11 * d;
+          return s / 16.f;
+        };
+        const float4 corr = make_float4(one(c00.x, c10.x, c01.x, c11.x), one(c00.y, c10.y, c01.y, c11.y),
+                                        one(c00.z, c10.z, c01.z, c11.z), one(c00.w, c10.w, c01.w, c11.w));
+        col_prolong_store(F, i, j, k, ch, (int)nch, corr);
+      }
     }
-    const int64_t c = col_cell(F, i, j, k);
-    float* __restrict__ P = F.phi;
-    const float4 old = *reinterpret_cast<const float4*>(P + c);
-    const float4 v = f4add(old, corr);
-    int d0 = kNoImage, d1 = kNoImage, d2 = kNoImage;
-    if (F.img) {
-      const int* im = F.img + 3 * ((i - 2) + (int64_t)F.nx * (j - 2));
-      d0 = im[0];
-      d1 = im[1];
-      d2 = im[2];
-    }
-    const int64_t o0 = (int64_t)d0 * F.CS, o1 = (int64_t)d1 * F.CS, o2 = (int64_t)d2 * F.CS;
-    *reinterpret_cast<float4*>(P + c) = v;
-    if (d0 != kNoImage) *reinterpret_cast<float4*>(P + c + o0) = v;
-    if (d1 != kNoImage) *reinterpret_cast<float4*>(P + c + o1) = v;
-    if (d2 != kNoImage) *reinterpret_cast<float4*>(P + c + o2) = v;
-    // z ghosts: the first chunk writes the ghosts that copy row k = 2 or
-    // are zero, the last chunk those that copy row k = nz+1
-    const bool h0 = d0 != kNoImage, h1 = d1 != kNoImage, h2 = d2 != kNoImage;
-    const int64_t g1 = c - (k - 1), gZ = c + (F.nz + 2 - k);
-    if (ch == 0) {
-      if (F.z1 != 2) col_put(P, g1, F.z1 == 1 ? v.x : 0.f, o0, o1, o2, h0, h1, h2);
-      if (F.zZ != 2) col_put(P, gZ, F.zZ == 1 ? v.x : 0.f, o0, o1, o2, h0, h1, h2);
-    }
-    if (ch == nch - 1) {
-      if (F.z1 == 2) col_put(P, g1, v.w, o0, o1, o2, h0, h1, h2);
-      if (F.zZ == 2) col_put(P, gZ, v.w, o0, o1, o2, h0, h1, h2);
+  } else {
+    const float4 c1 = *reinterpret_cast<const float4*>(pc + (cx ? ox : oy));
+    constexpr int n2 = 2;
+#pragma unroll
+    for (int a = 0; a < n2; ++a) {
+      const int i = cx ? i0 + a : i0, j = cx ? j0 : j0 + a;
+      if (cx ? (i < 2 || i > F.nx + 1) : (j < 2 || j > F.ny + 1)) continue;
+      const int par = cx ? (i & 1) : (j & 1);
+      const float w0 = par ? 3.f : 1.f, w1 = par ? 1.f : 3.f;
+      const float4 corr = make_float4((w0 * c00.x + w1 * c1.x) / 4.f, (w0 * c00.y + w1 * c1.y) / 4.f,
+                                      (w0 * c00.z + w1 * c1.z) / 4.f, (w0 * c00.w + w1 * c1.w) / 4.f);
+      col_prolong_store(F, i, j, k, ch, (int)nch, corr);
     }
   }
 }
