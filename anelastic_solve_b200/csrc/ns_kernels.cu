@@ -828,7 +828,9 @@ __global__ void k_psource(NSDev D, double rdt) {
 // of a cell reads p only), then ghost(u,'u'), ghost(v,'v'), ghost(w,'w')
 // (NSsolver.F90:572-574) by columns.
 // hist (may be null): the interior of p is also copied there (the history
-// of the pressure initial guess)
+// of the pressure initial guess).  kU: r is 1 on every plane, so the
+// divisions by r are left out (x / 1.0 == x exactly in IEEE arithmetic).
+template <bool kU>
 __global__ void __launch_bounds__(128) k_pgrad(NSDev D, double dt, double* __restrict__ hist) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
@@ -836,13 +838,18 @@ __global__ void __launch_bounds__(128) k_pgrad(NSDev D, double dt, double* __res
   if (i > D.nx + 1) return;
   const int kend_w = D.nz + 1 - D.ew;
   const double* __restrict__ p = D.p;
-  const double rk = D.rz[k - 1];
+  const double rk = kU ? 1.0 : D.rz[k - 1];
   const double pk = FA(p, i, j, k);
   if (hist) FA(hist, i, j, k) = pk;
-  FA(D.u, i, j, k) = FA(D.u, i, j, k) - (FA(p, i + 1, j, k) / rk - pk / rk) * MT(D.rdxe, i) * dt;
-  FA(D.v, i, j, k) = FA(D.v, i, j, k) - (FA(p, i, j + 1, k) / rk - pk / rk) * MT(D.rdye, j) * dt;
-  if (k <= kend_w)
-    FA(D.w, i, j, k) = FA(D.w, i, j, k) - (FA(p, i, j, k + 1) / D.rz[k] - pk / rk) * MT(D.rdze, k) * dt;
+  const double pr = kU ? pk : pk / rk;
+  const double pe = kU ? FA(p, i + 1, j, k) : FA(p, i + 1, j, k) / rk;
+  const double pn = kU ? FA(p, i, j + 1, k) : FA(p, i, j + 1, k) / rk;
+  FA(D.u, i, j, k) = FA(D.u, i, j, k) - (pe - pr) * MT(D.rdxe, i) * dt;
+  FA(D.v, i, j, k) = FA(D.v, i, j, k) - (pn - pr) * MT(D.rdye, j) * dt;
+  if (k <= kend_w) {
+    const double pt = kU ? FA(p, i, j, k + 1) : FA(p, i, j, k + 1) / D.rz[k];
+    FA(D.w, i, j, k) = FA(D.w, i, j, k) - (pt - pr) * MT(D.rdze, k) * dt;
+  }
 }
 
 __global__ void k_pgrad_ghost(NSDev D, ZRule Ru, ZRule Rv, ZRule Rw) {
@@ -1269,7 +1276,10 @@ void launch_extrap(const NSDev& D, double* p, const double* h1, const double* h2
 
 void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, const ZRule& Rw,
                   cudaStream_t s, double* hist) {
-  k_pgrad<<<cell_grid(D, 128), 128, 0, s>>>(D, dt, hist);
+  if (D.unit_r)
+    k_pgrad<true><<<cell_grid(D, 128), 128, 0, s>>>(D, dt, hist);
+  else
+    k_pgrad<false><<<cell_grid(D, 128), 128, 0, s>>>(D, dt, hist);
   k_pgrad_ghost<<<col_grid(D, 64), 64, 0, s>>>(D, Ru, Rv, Rw);
   count_launch(2);
   launch_images(D, D.u, D.v, D.w, s);
