@@ -602,17 +602,83 @@ __global__ void __launch_bounds__(TPB) k_cn_column(NSDev D, double* __restrict__
 // SSM): every row adds the eddy terms of the column's kT to the DNS
 // coefficients, so the tridiagonal system differs per column and is
 // eliminated here (Thomas of mg_relax.F90:541-595: a = -sub/b(k-1),
-// b = diag + a c(k-1), G = rhs + a G(k-1)).  G stays in the field, b and
-// c go to per-cell scratch for the back substitution.  Loads of a batch of
-// kCNU rows are issued before its stores.  The arithmetic follows the
-// reference's expressions term by term.
-template <int kVar, int U = kCNU, int TPB = kCNThreads>
+// b = diag + a c(k-1), G = rhs + a G(k-1)).  G stays in the field and b
+// goes to per-cell scratch for the back substitution; the super-diagonal
+// c is not stored: the back substitution forms it again from the column's
+// kT rows with the same expressions.  Loads of a batch of U rows are
+// issued before its stores.  The arithmetic follows the reference's
+// expressions term by term.
+//
+// kU: r is 1 on every plane.  Then ra / rk, and the r-weighted average of
+// w's eddy coefficient, leave the coefficient sums unchanged (x * 1.0 and
+// x / 1.0 are exact in IEEE arithmetic), so their divisions are left out.
+
+// Eddy weights of row k: t1 (lower face, rows k-1 and k of kT) and t2
+// (upper face, rows k and k+1), in the reference's pairing per variable
+// (u, v: the four-point average of the two columns; rho: the column's
+// two-point average; scal1: the same without r; w: r-weighted).
+template <int kVar, bool kU>
+__device__ __forceinline__ double les_t1(const double* s_r, int k, double kcc, double knc, double kcm,
+                                         double knm) {
+  constexpr double H = 0.5;
+  if constexpr (kVar == 3) {
+    if constexpr (kU) return -kcc;
+    const double rk = s_r[k - 1], rkp = s_r[k];
+    return -kcc * rk / (H * (rkp + rk));
+  } else if constexpr (kVar == 1 || kVar == 2) {
+    if constexpr (kU) return -0.25 * (kcc + knc + kcm + knm);
+    const double rk = s_r[k - 1];
+    const double ra1 = H * (s_r[k] + rk);
+    return -0.25 * (kcc + knc + kcm + knm) * ra1 / rk;
+  } else if constexpr (kVar == 5) {
+    if constexpr (kU) return -0.5 * (kcc + kcm);
+    const double rk = s_r[k - 1];
+    const double ra1 = H * (s_r[k] + rk);
+    return -0.5 * (kcc + kcm) * ra1 / rk;
+  } else {
+    return -0.5 * (kcc + kcm);
+  }
+}
+
+template <int kVar, bool kU>
+__device__ __forceinline__ double les_t2(const double* s_r, int k, double kcc, double knc, double kcp,
+                                         double knp) {
+  constexpr double H = 0.5;
+  if constexpr (kVar == 3) {
+    if constexpr (kU) return -kcp;
+    const double rk = s_r[k - 1], rkp = s_r[k];
+    return -kcp * rkp / (H * (rkp + rk));
+  } else if constexpr (kVar == 1 || kVar == 2) {
+    if constexpr (kU) return -0.25 * (kcc + knc + kcp + knp);
+    const double rk = s_r[k - 1];
+    const double ra2 = H * (rk + s_r[k - 2]);
+    return -0.25 * (kcc + knc + kcp + knp) * ra2 / rk;
+  } else if constexpr (kVar == 5) {
+    if constexpr (kU) return -0.5 * (kcc + kcp);
+    const double rk = s_r[k - 1];
+    const double ra2 = H * (rk + s_r[k - 2]);
+    return -0.5 * (kcc + kcp) * ra2 / rk;
+  } else {
+    return -0.5 * (kcc + kcp);
+  }
+}
+
+// super-diagonal of an interior (non-wall) row k from its t2
+template <int kVar>
+__device__ __forceinline__ double les_sup(const double* s_c, const double* s_re, const double* s_rc, int k,
+                                          double rkdt, double t2) {
+  if constexpr (kVar != 3)
+    return s_c[k - 1] - 0.5 * rkdt * t2 * s_re[k - 1] * s_rc[k - 1];
+  else
+    return s_c[k - 1] - rkdt * t2 * s_re[k - 1] * s_rc[k];
+}
+
+template <int kVar, bool kU, int U = kCNU, int TPB = kCNThreads>
 __global__ void __launch_bounds__(TPB) k_cn_column_les(NSDev D, double* __restrict__ fld,
                                                               const double* __restrict__ q, CNFac F,
                                                               double a3, double rkdt, ZRule R,
                                                               const double* __restrict__ kT,
-                                                              double* __restrict__ bb,
-                                                              double* __restrict__ cc) {
+                                                              double* __restrict__ bb) {
   extern __shared__ double cn_sm[];
   const int n = D.nz + 2;
   const int S = n + 1;
@@ -648,7 +714,6 @@ __global__ void __launch_bounds__(TPB) k_cn_column_les(NSDev D, double* __restri
   // eddy coefficient columns: u pairs (i, i+1), v pairs (j, j+1)
   const double* kc = kT + base;
   const double* kn = kT + base + (kVar == 1 ? 1 : (kVar == 2 ? D.X : 0));
-  constexpr double H = 0.5;
   double um = fld[base];
   double uk = fld[base + XY];
   // row 1 is a wall row
@@ -657,7 +722,6 @@ __global__ void __launch_bounds__(TPB) k_cn_column_les(NSDev D, double* __restri
   double cprev = s_c[0];
   fld[base] = g;
   bb[base] = b;
-  cc[base] = cprev;
   // kT window: rows k-1 and k of both columns (kn = kc for rho, scal1, w)
   double kcm = kc[0], kcc = kc[XY], knm = kn[0], knc = kn[XY];
   for (int kb = 2; kb <= n; kb += U) {
@@ -683,27 +747,15 @@ __global__ void __launch_bounds__(TPB) k_cn_column_les(NSDev D, double* __restri
           rhs = s_rb[k - 1];
         } else {
           rhs = 1.0 * uk + a3 * qv[u] * 1.0;
-          const double rk = s_r[k - 1];
+          const double t1 = les_t1<kVar, kU>(s_r, k, kcc, knc, kcm, knm);
+          const double t2 = les_t2<kVar, kU>(s_r, k, kcc, knc, kcp[u], knp[u]);
+          sup = les_sup<kVar>(s_c, s_re, s_rc, k, rkdt, t2);
           if (kVar != 3) {
             rhs = rhs + rkdt * 0.5 *
                             (s_t2[k - 1] * (up[u] - uk) * s_re[k - 1] -
                              s_t1[k - 1] * (uk - um) * s_re[k - 2]) *
                             s_rc[k - 1];
-            const double ra1 = H * (s_r[k] + rk);
-            const double ra2 = H * (rk + s_r[k - 2]);
-            double t1, t2;
-            if (kVar == 1 || kVar == 2) {
-              t1 = -0.25 * (kcc + knc + kcm + knm) * ra1 / rk;
-              t2 = -0.25 * (kcc + knc + kcp[u] + knp[u]) * ra2 / rk;
-            } else if (kVar == 5) {
-              t1 = -0.5 * (kcc + kcm) * ra1 / rk;
-              t2 = -0.5 * (kcc + kcp[u]) * ra2 / rk;
-            } else {
-              t1 = -0.5 * (kcc + kcm);
-              t2 = -0.5 * (kcc + kcp[u]);
-            }
             sub = s_sub[k - 1] - 0.5 * rkdt * t1 * s_re[k - 2] * s_rc[k - 1];
-            sup = s_c[k - 1] - 0.5 * rkdt * t2 * s_re[k - 1] * s_rc[k - 1];
             dia = s_dia[k - 1] + 0.5 * rkdt * (t1 * s_re[k - 2] + t2 * s_re[k - 1]) * s_rc[k - 1];
             rhs = rhs + rkdt * 0.5 *
                             (t2 * (up[u] - uk) * s_re[k - 1] - t1 * (uk - um) * s_re[k - 2]) *
@@ -713,11 +765,7 @@ __global__ void __launch_bounds__(TPB) k_cn_column_les(NSDev D, double* __restri
                             (s_t2[k - 1] * (up[u] - uk) * s_rc[k] -
                              s_t1[k - 1] * (uk - um) * s_rc[k - 1]) *
                             s_re[k - 1];
-            const double rkp = s_r[k];
-            const double t1 = -kcc * rk / (H * (rkp + rk));
-            const double t2 = -kcp[u] * rkp / (H * (rkp + rk));
             sub = s_sub[k - 1] - rkdt * t1 * s_re[k - 1] * s_rc[k - 1];
-            sup = s_c[k - 1] - rkdt * t2 * s_re[k - 1] * s_rc[k];
             dia = s_dia[k - 1] + rkdt * (t1 * s_rc[k - 1] + t2 * s_rc[k]) * s_re[k - 1];
             rhs = rhs + rkdt * (t2 * (up[u] - uk) * s_rc[k] - t1 * (uk - um) * s_rc[k - 1]) * s_re[k - 1];
           }
@@ -728,7 +776,6 @@ __global__ void __launch_bounds__(TPB) k_cn_column_les(NSDev D, double* __restri
         const int64_t o = base + (int64_t)(k - 1) * XY;
         fld[o] = g;
         bb[o] = b;
-        cc[o] = sup;
         cprev = sup;
         um = uk;
         uk = up[u];
@@ -739,25 +786,38 @@ __global__ void __launch_bounds__(TPB) k_cn_column_les(NSDev D, double* __restri
       }
     }
   }
-  // back substitution: G(n) = G(n)/b(n); G(k) = (G(k) - c(k) G(k+1))/b(k)
+  // back substitution: G(n) = G(n)/b(n); G(k) = (G(k) - c(k) G(k+1))/b(k),
+  // with c(k) formed again from kT rows k and k+1 (row 1 and the wall rows
+  // take the DNS super-diagonal, as in the forward sweep)
   double x = g / b;
   fld[base + (int64_t)(n - 1) * XY] = x;
+  double kcu = kc[(int64_t)(n - 1) * XY], knu = kn[(int64_t)(n - 1) * XY];  // rows k+1
   for (int kb = n - 1; kb >= 1; kb -= U) {
-    double gv[U], bv[U], cv[U];
+    double gv[U], bv[U], kcv[U], knv[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int k = kb - u;
-      const int64_t o = base + (int64_t)(k - 1) * XY;
-      gv[u] = (k >= 1) ? fld[o] : 0.0;
-      bv[u] = (k >= 1) ? bb[o] : 1.0;
-      cv[u] = (k >= 1) ? cc[o] : 0.0;
+      const int64_t o = (int64_t)(k - 1) * XY;
+      gv[u] = (k >= 1) ? fld[base + o] : 0.0;
+      bv[u] = (k >= 1) ? bb[base + o] : 1.0;
+      kcv[u] = (k >= 2) ? kc[o] : 0.0;
+      knv[u] = (k >= 2) ? kn[o] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int k = kb - u;
       if (k >= 1) {
-        x = (gv[u] - cv[u] * x) / bv[u];
+        double sup;
+        if (k == 1 || s_bc[k - 1] != 0.0) {
+          sup = s_c[k - 1];
+        } else {
+          const double t2 = les_t2<kVar, kU>(s_r, k, kcv[u], knv[u], kcu, knu);
+          sup = les_sup<kVar>(s_c, s_re, s_rc, k, rkdt, t2);
+        }
+        x = (gv[u] - sup * x) / bv[u];
         fld[base + (int64_t)(k - 1) * XY] = x;
+        kcu = kcv[u];
+        knu = knv[u];
       }
     }
   }
@@ -1028,33 +1088,37 @@ void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFa
 
 template <int kVar, int U, int TPB>
 static void cn_les_launch(const NSDev& D, double* fld, const double* q, const CNFac& f, double a3, double rkdt,
-                          const ZRule& R, const double* kT, double* b, double* c, cudaStream_t s) {
+                          const ZRule& R, const double* kT, double* b, cudaStream_t s) {
   const size_t sm = 10 * (size_t)(D.nz + 3) * sizeof(double);
-  set_smem_limit_once((const void*)k_cn_column_les<kVar, U, TPB>, 200 * 1024);
-  k_cn_column_les<kVar, U, TPB><<<col_grid(D, TPB), TPB, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b, c);
+  if (D.unit_r) {
+    set_smem_limit_once((const void*)k_cn_column_les<kVar, true, U, TPB>, 200 * 1024);
+    k_cn_column_les<kVar, true, U, TPB><<<col_grid(D, TPB), TPB, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b);
+  } else {
+    set_smem_limit_once((const void*)k_cn_column_les<kVar, false, U, TPB>, 200 * 1024);
+    k_cn_column_les<kVar, false, U, TPB><<<col_grid(D, TPB), TPB, sm, s>>>(D, fld, q, f, a3, rkdt, R, kT, b);
+  }
 }
 
 template <int kVar>
 static void cn_les_variant(const NSDev& D, double* fld, const double* q, const CNFac& f, double a3, double rkdt,
-                           const ZRule& R, const double* kT, double* b, double* c, int variant, cudaStream_t s) {
+                           const ZRule& R, const double* kT, double* b, int variant, cudaStream_t s) {
   switch (variant) {
-    case 1: cn_les_launch<kVar, 4, 128>(D, fld, q, f, a3, rkdt, R, kT, b, c, s); break;
-    case 2: cn_les_launch<kVar, 8, 128>(D, fld, q, f, a3, rkdt, R, kT, b, c, s); break;
-    case 3: cn_les_launch<kVar, 16, 128>(D, fld, q, f, a3, rkdt, R, kT, b, c, s); break;
-    default: cn_les_launch<kVar, kCNU, kCNThreads>(D, fld, q, f, a3, rkdt, R, kT, b, c, s); break;
+    case 1: cn_les_launch<kVar, 4, 128>(D, fld, q, f, a3, rkdt, R, kT, b, s); break;
+    case 2: cn_les_launch<kVar, 8, 128>(D, fld, q, f, a3, rkdt, R, kT, b, s); break;
+    case 3: cn_les_launch<kVar, 16, 128>(D, fld, q, f, a3, rkdt, R, kT, b, s); break;
+    default: cn_les_launch<kVar, kCNU, kCNThreads>(D, fld, q, f, a3, rkdt, R, kT, b, s); break;
   }
 }
 
 void launch_cn_les(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
-                   double rkdt, const ZRule& R, const double* kT, double* b, double* c, int variant,
-                   cudaStream_t s) {
+                   double rkdt, const ZRule& R, const double* kT, double* b, int variant, cudaStream_t s) {
   CNFac f{F.ap, F.bp, F.c, F.t1, F.t2, F.rb, F.isbc, F.sub, F.diag};
   switch (var) {
-    case 1: cn_les_variant<1>(D, fld, q, f, a3, rkdt, R, kT, b, c, variant, s); break;
-    case 2: cn_les_variant<2>(D, fld, q, f, a3, rkdt, R, kT, b, c, variant, s); break;
-    case 3: cn_les_variant<3>(D, fld, q, f, a3, rkdt, R, kT, b, c, variant, s); break;
-    case 5: cn_les_variant<5>(D, fld, q, f, a3, rkdt, R, kT, b, c, variant, s); break;
-    default: cn_les_variant<8>(D, fld, q, f, a3, rkdt, R, kT, b, c, variant, s); break;
+    case 1: cn_les_variant<1>(D, fld, q, f, a3, rkdt, R, kT, b, variant, s); break;
+    case 2: cn_les_variant<2>(D, fld, q, f, a3, rkdt, R, kT, b, variant, s); break;
+    case 3: cn_les_variant<3>(D, fld, q, f, a3, rkdt, R, kT, b, variant, s); break;
+    case 5: cn_les_variant<5>(D, fld, q, f, a3, rkdt, R, kT, b, variant, s); break;
+    default: cn_les_variant<8>(D, fld, q, f, a3, rkdt, R, kT, b, variant, s); break;
   }
   count_launch();
   launch_images(D, fld, nullptr, nullptr, s);

@@ -23,15 +23,15 @@ constexpr int kCNVariants = 4;
 void launch_cn(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
                double rkdt, const ZRule& R, int variant, cudaStream_t s);
 // var_advance_CN_PL with the eddy terms (Vmodel = SSM): per-column
-// elimination; b, c: G-sized scratch for the eliminated diagonal and the
-// super-diagonal.  kT = nuT (u, v, w), kappaT (rho), nappaT (scal1).
+// elimination; b: G-sized scratch for the eliminated diagonal (the
+// super-diagonal is formed again from kT in the back substitution).
+// kT = nuT (u, v, w), kappaT (rho), nappaT (scal1).
 // variant: rows per load batch and columns per block (0: 8 rows, 256;
 // 1: 4, 128; 2: 8, 128; 3: 16, 128), chosen by the autotuner; every
 // variant computes the same bits
 constexpr int kCNLesVariants = 4;
 void launch_cn_les(const NSDev& D, int var, double* fld, const double* q, const CNFacHost& F, double a3,
-                   double rkdt, const ZRule& R, const double* kT, double* b, double* c, int variant,
-                   cudaStream_t s);
+                   double rkdt, const ZRule& R, const double* kT, double* b, int variant, cudaStream_t s);
 // SGSdiff (straincal.F90:339-414): modS, nuT, kappaT, nappaT on the
 // interior from the model profiles, then their ghosts ('cfluc').
 void launch_sgs(const NSDev& D, const ZRule& cfluc, cudaStream_t s);

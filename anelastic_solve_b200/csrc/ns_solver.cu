@@ -36,7 +36,6 @@ NSSolver::~NSSolver() {
   cudaFree(d_les_);
   cudaFree(d_ic_);
   cudaFree(d_cnb_);
-  cudaFree(d_cnc_);
   cudaFree(d_red_);
   cudaFree(d_part_);
   for (auto& h : hist_)
@@ -185,9 +184,8 @@ int NSSolver::init(const anel_grid_desc* g, const anel_mg_params* mgp, const ane
     ANEL_CUDA_TRY(cudaMemset(d_les_, 0, 4 * (size_t)Z * sizeof(double)));
   }
   if (ns->vmodel != ANEL_MODEL_DNS) {
-    // per-column eliminated diagonal and super-diagonal of the LES CN solve
+    // per-column eliminated diagonal of the LES CN solve
     ANEL_CUDA_TRY(cudaMalloc(&d_cnb_, G_ * sizeof(double)));
-    ANEL_CUDA_TRY(cudaMalloc(&d_cnc_, G_ * sizeof(double)));
   }
   // metrics
   std::vector<double> met;
@@ -326,7 +324,7 @@ int NSSolver::tune_cn() {
   }, &cnvar_);
   if (st == ANEL_OK && D_.vles)
     st = pick("k_cn_column_les", kCNLesVariants, "ANEL_CN_LES_VARIANT", [&](int q) {
-      launch_cn_les(D_, 1, D_.u, D_.qu, fac(0, 0), 1.0 / 3.0, 1e-3, R, D_.nuT, d_cnb_, d_cnc_, q, stream_);
+      launch_cn_les(D_, 1, D_.u, D_.qu, fac(0, 0), 1.0 / 3.0, 1e-3, R, D_.nuT, d_cnb_, q, stream_);
     }, &cnlesvar_);
   if (st != ANEL_OK) return st;
   if (timed) {
@@ -581,7 +579,7 @@ int NSSolver::substep_pre(double a1, double a2, double a3, double dt_rk, double 
   // var_advance_CN_PL: with Vmodel = SSM every variable gets the eddy
   // terms (the LES block is gated on Vmodel, NSsolver.F90:3160-3190)
   auto cn = [&](int var, double* f, const double* q, int vi, const ZRule& R, const double* kT, cudaStream_t st) {
-    if (D_.vles) launch_cn_les(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, kT, d_cnb_, d_cnc_, cnlesvar_, st);
+    if (D_.vles) launch_cn_les(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, kT, d_cnb_, cnlesvar_, st);
     else launch_cn(D_, var, f, q, fac(slot, vi), a3, dt_rk, R, cnvar_, st);
   };
   cn(1, D_.u, D_.qu, 0, ru, D_.nuT, s);

@@ -173,7 +173,6 @@ class NSSolver {
   double* d_les_ = nullptr;         // LES profiles: Csgs CTsgs CSsgs delg^2 (nz+2 each)
   double* d_ic_ = nullptr;          // tanh(zc) and |zc| profiles of init_shear
   double* d_cnb_ = nullptr;         // LES CN: eliminated diagonal per cell
-  double* d_cnc_ = nullptr;         // LES CN: super-diagonal per cell
   bool les_any_ = false;            // a subgrid model is on: nuT/kappaT/nappaT exist
   bool les_coeffs_done_ = false;
   double* d_cn_ = nullptr;          // CN factors: 3 slots x 5 vars x 9 arrays x (nz+2)
