@@ -11,37 +11,24 @@ static constexpr double R12 = 1.0 / 2.0;  // ratios::r_1_2 (modules.F90:203)
 // The right-hand-side functions read their fields through an accessor A_:
 // FU/FV/FW/FR(i+di, j+dj, k+dk) are u, v, w, rho at a constant offset from
 // the cell, FC the scalar of rhs_scalar (rho or scal1), FN/FK the LES
-// eddy coefficients.  The floating-point expressions are the same for every
-// accessor; only where the values come from differs (global memory around
-// the cell, or the shared-memory planes of the tiled kernel).
+// eddy coefficients (nuT; kappaT for rho, nappaT for scal1).  The accessor
+// (TileAcc) reads the shared-memory planes of the tiled kernel or global
+// memory around the cell; the floating-point expressions do not depend on
+// where the values come from.
 #undef FA
 #define FU(I, J, K) A_.u((I) - i, (J) - j, (K) - k)
 #define FV(I, J, K) A_.v((I) - i, (J) - j, (K) - k)
 #define FW(I, J, K) A_.w((I) - i, (J) - j, (K) - k)
 #define FR(I, J, K) A_.r((I) - i, (J) - j, (K) - k)
 #define FC(I, J, K) (kRho ? A_.r((I) - i, (J) - j, (K) - k) : A_.g(D.s, (I) - i, (J) - j, (K) - k))
-#define FN(I, J, K) A_.g(D.nuT, (I) - i, (J) - j, (K) - k)
-#define FK(I, J, K) A_.g(kT, (I) - i, (J) - j, (K) - k)
+#define FN(I, J, K) A_.nu((I) - i, (J) - j, (K) - k)
+#define FK(I, J, K) A_.template kap<kRho>(kT, (I) - i, (J) - j, (K) - k)
 // r(z) and densityBG(z) at profile index q; with kU (both identically 1,
 // the Boussinesq configurations) the constant 1.0, so that products with
 // them and quotients by them fold away: x*1 and x/1 are exact, so the
 // results are the same bits as with the profile values.
 #define RZ(q) (kU ? 1.0 : D.rz[q])
 #define BG(q) (kU ? 1.0 : D.bgz[q])
-
-// Every field from global memory around the cell c0.
-struct GlobalAcc {
-  const NSDev& D;
-  int64_t c0;
-  __device__ __forceinline__ int64_t o(int di, int dj, int dk) const {
-    return c0 + di + (int64_t)D.X * dj + D.XY * dk;
-  }
-  __device__ __forceinline__ double u(int a, int b, int c) const { return D.u[o(a, b, c)]; }
-  __device__ __forceinline__ double v(int a, int b, int c) const { return D.v[o(a, b, c)]; }
-  __device__ __forceinline__ double w(int a, int b, int c) const { return D.w[o(a, b, c)]; }
-  __device__ __forceinline__ double r(int a, int b, int c) const { return D.rho[o(a, b, c)]; }
-  __device__ __forceinline__ double g(const double* p, int a, int b, int c) const { return p[o(a, b, c)]; }
-};
 
 // u1_rhs (NSsolver.F90:646-804): returns Utemp(i,j,k) before ghosting.
 template <bool kU, class Acc>
@@ -276,16 +263,18 @@ __device__ __forceinline__ double rhs_scalar(const NSDev& D, const Acc& A_, int 
 // tile plus a one-cell halo), four planes per field in a ring: the
 // functions read planes k-1, k, k+1 while the block brings plane k+2 in
 // with asynchronous copies, so every field value is read from global memory once
-// per tile instead of once per use.  scal1 and the LES coefficients are
-// read from global memory.
+// per tile instead of once per use.  kL (the eddy coefficients exist):
+// nuT and kappaT are staged in the same ring; scal1 and nappaT are read
+// from global memory.
 constexpr int kRT_I = 32, kRT_J = 8, kRT_K = 32;
 constexpr int kRT_W = kRT_I + 2, kRT_PL = kRT_W * (kRT_J + 2);
 constexpr int kRT_PER = (kRT_PL + kRT_I * kRT_J - 1) / (kRT_I * kRT_J);  // plane elements per thread
 
-// u, v, w, rho from the ring of shared planes (slot of plane k = k & 3),
-// the rest from global memory around c0.
+// u, v, w, rho (and with kL nuT and kappaT) from the ring of shared planes
+// (slot of plane k = k & 3), the rest from global memory around c0.
+template <bool kL>
 struct TileAcc {
-  const double* sm;  // [field u v w rho][slot][j + 1][i + 1]
+  const double* sm;  // [field u v w rho (nuT kappaT)][slot][j + 1][i + 1]
   int idx;           // (ty + 1) * kRT_W + tx + 1
   int k;
   const NSDev& D;
@@ -300,17 +289,29 @@ struct TileAcc {
   __device__ __forceinline__ double g(const double* p, int a, int b, int c) const {
     return p[c0 + a + (int64_t)D.X * b + D.XY * c];
   }
+  __device__ __forceinline__ double nu(int a, int b, int c) const {
+    return kL ? f(4, a, b, c) : g(D.nuT, a, b, c);
+  }
+  // p: kappaT for rho (staged with kL), nappaT for scal1 (global)
+  template <bool kR>
+  __device__ __forceinline__ double kap(const double* p, int a, int b, int c) const {
+    return (kL && kR) ? f(5, a, b, c) : g(p, a, b, c);
+  }
 };
 
-template <bool kFirst, bool kU>
+// shared-memory bytes of k_rhs_accum: four planes of 4 (6 with kL) fields
+constexpr size_t rhs_smem_bytes(bool les) { return (size_t)(les ? 6 : 4) * 4 * kRT_PL * sizeof(double); }
+
+template <bool kFirst, bool kU, bool kL>
 __global__ void __launch_bounds__(kRT_I * kRT_J, 2) k_rhs_accum(NSDev D, double a1, double a2, double dt) {
-  __shared__ double sm[4 * 4 * kRT_PL];
+  extern __shared__ double sm[];
+  constexpr int NF = kL ? 6 : 4;
   const int t = threadIdx.x;
   const int tx = t & 31, ty = t >> 5;
   const int i0 = 2 + blockIdx.x * kRT_I, j0 = 2 + blockIdx.y * kRT_J, k0 = 2 + blockIdx.z * kRT_K;
   const int i = i0 + tx, j = j0 + ty;
   const int kend = min(k0 + kRT_K, D.nz + 2);  // exclusive
-  const double* fld[4] = {D.u, D.v, D.w, D.rho};
+  const double* fld[6] = {D.u, D.v, D.w, D.rho, D.nuT, D.kT};
   // plane element e of the tile (halo included) -> global offset, or -1
   int64_t off[kRT_PER];
 #pragma unroll
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(kRT_I * kRT_J, 2) k_rhs_accum(NSDev D, double 
       if (off[q] < 0) continue;
       const int e = t + q * kRT_I * kRT_J;
 #pragma unroll
-      for (int f = 0; f < 4; ++f) {
+      for (int f = 0; f < NF; ++f) {
         const unsigned dst =
             (unsigned)__cvta_generic_to_shared(&sm[(f * 4 + (p & 3)) * kRT_PL + e]);
         const double* src = fld[f] + off[q] + D.XY * (p - 1);
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(kRT_I * kRT_J, 2) k_rhs_accum(NSDev D, double 
       const double q0v = kFirst ? 0.0 : D.qv[c];
       const double q0w = kFirst ? 0.0 : D.qw[c];
       const double q0r = kFirst ? 0.0 : D.qr[c];
-      const TileAcc A{sm, (ty + 1) * kRT_W + tx + 1, k, D, c};
+      const TileAcc<kL> A{sm, (ty + 1) * kRT_W + tx + 1, k, D, c};
       const double fu = rhs_u<kU>(D, A, i, j, k);
       const double fv = rhs_v<kU>(D, A, i, j, k);
       const double fw = rhs_w<kU>(D, A, i, j, k);
@@ -1045,15 +1046,27 @@ static dim3 col_grid(const NSDev& D, int tx) {
   return dim3((unsigned)((D.nx + tx - 1) / tx), (unsigned)D.ny, 1u);
 }
 
+template <bool kFirst, bool kU, bool kL>
+static void rhs_launch(const NSDev& D, dim3 g, double a1, double a2, double dt, cudaStream_t s) {
+  const size_t sm = rhs_smem_bytes(kL);
+  if (kL) set_smem_limit_once((const void*)k_rhs_accum<kFirst, kU, kL>, (int)sm);
+  k_rhs_accum<kFirst, kU, kL><<<g, kRT_I * kRT_J, sm, s>>>(D, a1, a2, dt);
+}
+
 void launch_rhs_accum(const NSDev& D, double a1, double a2, double dt, bool first, cudaStream_t s) {
   const dim3 g((unsigned)((D.nx + kRT_I - 1) / kRT_I), (unsigned)((D.ny + kRT_J - 1) / kRT_J),
                (unsigned)((D.nz + kRT_K - 1) / kRT_K));
-  const int sel = (first ? 2 : 0) + (D.unit_r ? 1 : 0);
+  const bool les = D.nuT && D.kT;
+  const int sel = (first ? 4 : 0) + (D.unit_r ? 2 : 0) + (les ? 1 : 0);
   switch (sel) {
-    case 0: k_rhs_accum<false, false><<<g, kRT_I * kRT_J, 0, s>>>(D, a1, a2, dt); break;
-    case 1: k_rhs_accum<false, true><<<g, kRT_I * kRT_J, 0, s>>>(D, a1, a2, dt); break;
-    case 2: k_rhs_accum<true, false><<<g, kRT_I * kRT_J, 0, s>>>(D, a1, a2, dt); break;
-    default: k_rhs_accum<true, true><<<g, kRT_I * kRT_J, 0, s>>>(D, a1, a2, dt); break;
+    case 0: rhs_launch<false, false, false>(D, g, a1, a2, dt, s); break;
+    case 1: rhs_launch<false, false, true>(D, g, a1, a2, dt, s); break;
+    case 2: rhs_launch<false, true, false>(D, g, a1, a2, dt, s); break;
+    case 3: rhs_launch<false, true, true>(D, g, a1, a2, dt, s); break;
+    case 4: rhs_launch<true, false, false>(D, g, a1, a2, dt, s); break;
+    case 5: rhs_launch<true, false, true>(D, g, a1, a2, dt, s); break;
+    case 6: rhs_launch<true, true, false>(D, g, a1, a2, dt, s); break;
+    default: rhs_launch<true, true, true>(D, g, a1, a2, dt, s); break;
   }
   count_launch();
 }
