@@ -74,39 +74,69 @@ __global__ void k_dyn_comp(NSDev D, int ij, double* __restrict__ out) {
   out[o] = r;
 }
 
-// One direction of the test filter (hf = 0: filter with weights 1/4, 1/2,
-// 1/4, written with the source's zero weights, sx and ex boundary
-// formulas) or of filterHF (hf = 1: a strict local extremum of the pencil
-// takes the 3-point average when that is still an extremum of the same
-// kind), src -> dst on the interior.
-__global__ void k_dyn_pass(NSDev D, const double* __restrict__ src, double* __restrict__ dst, int dir, int hf) {
-  DYN_CELL();
-  const int q = dir == 0 ? i : (dir == 1 ? j : k);
-  const int n = dir == 0 ? D.nx : (dir == 1 ? D.ny : D.nz);
-  const int64_t st = dir == 0 ? 1 : (dir == 1 ? (int64_t)D.X : D.XY);
-  const double* p = src + o;
-  if (!hf) {
-    const double w0 = 0.0, w1 = 1.0 / 4.0, w2 = 1.0 / 2.0, w3 = 1.0 / 4.0, w4 = 0.0;
-    double r;
-    if (q == 2)
-      r = w1 * p[-st] + w2 * p[0] + w3 * p[st] + w4 * p[2 * st] + w0 * p[3 * st];
-    else if (q == n + 1)
-      r = w1 * p[st] + w2 * p[0] + w3 * p[-st] + w4 * p[-2 * st] + w0 * p[-3 * st];
-    else
-      r = w0 * p[-2 * st] + w1 * p[-st] + w2 * p[0] + w3 * p[st] + w4 * p[2 * st];
-    dst[o] = r;
-  } else {
-    const double p0 = p[0], pm = p[-st], pp = p[st];
-    double r = p0;
-    if (p0 < pp && p0 < pm) {
-      const double x = 1.0 / 4.0 * pm + 1.0 / 2.0 * p0 + 1.0 / 4.0 * pp;
-      if (x < pp && x < pm) r = x;
-    } else if (p0 > pp && p0 > pm) {
-      const double x = 1.0 / 4.0 * pm + 1.0 / 2.0 * p0 + 1.0 / 4.0 * pp;
-      if (x > pp && x > pm) r = x;
+// One direction of the test filter (HF = false: filter with weights 1/4,
+// 1/2, 1/4, written with the source's zero weights, sx and ex boundary
+// formulas) or of filterHF (HF = true: a strict local extremum of the
+// pencil takes the 3-point average when that is still an extremum of the
+// same kind), src -> dst on the interior.  A thread does kDynK planes of
+// one (i, j): for the z direction the planes its next cell reads are the
+// ones it has just read, so they come from L1.
+constexpr int kDynK = 8;
+template <int DIR, bool HF>
+__global__ void __launch_bounds__(128) k_dyn_pass(NSDev D, const double* __restrict__ src,
+                                                  double* __restrict__ dst) {
+  const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 2 + blockIdx.y;
+  const int k0 = 2 + blockIdx.z * kDynK;
+  if (i > D.nx + 1) return;
+  const int kend = min(k0 + kDynK, D.nz + 2);  // exclusive
+  const int n = DIR == 0 ? D.nx : (DIR == 1 ? D.ny : D.nz);
+  const int64_t st = DIR == 0 ? 1 : (DIR == 1 ? (int64_t)D.X : D.XY);
+  for (int k = k0; k < kend; ++k) {
+    const int64_t o = NS_IX(i, j, k);
+    const int q = DIR == 0 ? i : (DIR == 1 ? j : k);
+    const double* p = src + o;
+    if constexpr (!HF) {
+      const double w0 = 0.0, w1 = 1.0 / 4.0, w2 = 1.0 / 2.0, w3 = 1.0 / 4.0, w4 = 0.0;
+      double r;
+      if (q == 2)
+        r = w1 * p[-st] + w2 * p[0] + w3 * p[st] + w4 * p[2 * st] + w0 * p[3 * st];
+      else if (q == n + 1)
+        r = w1 * p[st] + w2 * p[0] + w3 * p[-st] + w4 * p[-2 * st] + w0 * p[-3 * st];
+      else
+        r = w0 * p[-2 * st] + w1 * p[-st] + w2 * p[0] + w3 * p[st] + w4 * p[2 * st];
+      dst[o] = r;
+    } else {
+      const double p0 = p[0], pm = p[-st], pp = p[st];
+      double r = p0;
+      if (p0 < pp && p0 < pm) {
+        const double x = 1.0 / 4.0 * pm + 1.0 / 2.0 * p0 + 1.0 / 4.0 * pp;
+        if (x < pp && x < pm) r = x;
+      } else if (p0 > pp && p0 > pm) {
+        const double x = 1.0 / 4.0 * pm + 1.0 / 2.0 * p0 + 1.0 / 4.0 * pp;
+        if (x > pp && x > pm) r = x;
+      }
+      dst[o] = r;
     }
-    dst[o] = r;
   }
+}
+
+template <int DIR>
+void dyn_pass_launch(const NSDev& D, const double* src, double* dst, int hf, cudaStream_t s) {
+  const dim3 g((unsigned)((D.nx + 127) / 128), (unsigned)D.ny, (unsigned)((D.nz + kDynK - 1) / kDynK));
+  if (hf)
+    k_dyn_pass<DIR, true><<<g, 128, 0, s>>>(D, src, dst);
+  else
+    k_dyn_pass<DIR, false><<<g, 128, 0, s>>>(D, src, dst);
+}
+
+void launch_dyn_pass(const NSDev& D, const double* src, double* dst, int dir, int hf, cudaStream_t s) {
+  if (dir == 0)
+    dyn_pass_launch<0>(D, src, dst, hf, s);
+  else if (dir == 1)
+    dyn_pass_launch<1>(D, src, dst, hf, s);
+  else
+    dyn_pass_launch<2>(D, src, dst, hf, s);
 }
 
 // whole-array assignments of the source (ghost cells included)
@@ -249,7 +279,7 @@ void NSSolver::dyn_filter(const double* in, double* out, int vt, int hf, cudaStr
   for (int d = 0; d < 3; ++d) {
     if (hf || prm_.filt[d]) {
       double* dst = (cur == out) ? tmp : out;
-      k_dyn_pass<<<interior_grid(D_), 128, 0, s>>>(D_, cur, dst, d, hf);
+      launch_dyn_pass(D_, cur, dst, d, hf, s);
       count_launch();
       cur = dst;
     } else if (cur == in) {
