@@ -6,6 +6,9 @@
 namespace anel {
 
 static constexpr double R12 = 1.0 / 2.0;  // ratios::r_1_2 (modules.F90:203)
+// planes of one (i, j) per thread in the one-cell kernels (SGS, Psource,
+// Pgrad): the z-neighbours a thread reads next are the ones it just read
+static constexpr int kCellK = 8;
 
 // --------------------------------------------------------------- RHS
 // The right-hand-side functions read their fields through an accessor A_:
@@ -832,13 +835,16 @@ __global__ void __launch_bounds__(TPB) k_cn_column_les(NSDev D, double* __restri
 __global__ void __launch_bounds__(128) k_sgs(NSDev D) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
-  const int k = 2 + blockIdx.z;
+  const int k0 = 2 + blockIdx.z * kCellK;
   if (i > D.nx + 1) return;
-  const double modS = strain_mag(D, D.u, D.v, D.w, i, j, k);
-  const double dg2 = D.delg2[k - 1];
-  FA(D.nuT, i, j, k) = -(D.Cs[k - 1] + 0.0) * dg2 * modS + 0.0;
-  FA(D.kT, i, j, k) = -(D.CTs[k - 1] + 0.0) * dg2 * modS + 0.0;
-  FA(D.nT, i, j, k) = -(D.CSs[k - 1] + 0.0) * dg2 * modS + 0.0;
+  const int kend = min(k0 + kCellK, D.nz + 2);  // exclusive
+  for (int k = k0; k < kend; ++k) {
+    const double modS = strain_mag(D, D.u, D.v, D.w, i, j, k);
+    const double dg2 = D.delg2[k - 1];
+    FA(D.nuT, i, j, k) = -(D.Cs[k - 1] + 0.0) * dg2 * modS + 0.0;
+    FA(D.kT, i, j, k) = -(D.CTs[k - 1] + 0.0) * dg2 * modS + 0.0;
+    FA(D.nT, i, j, k) = -(D.CSs[k - 1] + 0.0) * dg2 * modS + 0.0;
+  }
 }
 
 // Pressure initial guess: p = 2 h1 - h2 on the interior (the multigrid's
@@ -872,16 +878,19 @@ __global__ void k_clip(NSDev D, double* a, double vmin, double vmax) {
 __global__ void k_psource(NSDev D, double rdt) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
-  const int k = 2 + blockIdx.z;
+  const int k0 = 2 + blockIdx.z * kCellK;
   if (i > D.nx + 1) return;
-  const double rk = D.rz[k - 1];
-  const double H = 0.5;
-  const double v = ((rk * FA(D.u, i, j, k) - rk * FA(D.u, i - 1, j, k)) * MT(D.rdxc, i) +
-                    (rk * FA(D.v, i, j, k) - rk * FA(D.v, i, j - 1, k)) * MT(D.rdyc, j) +
-                    (H * (D.rz[k] + rk) * FA(D.w, i, j, k) - H * (rk + D.rz[k - 2]) * FA(D.w, i, j, k - 1)) *
-                        MT(D.rdzc, k)) *
-                   rdt;
-  FA(D.psrc, i, j, k) = 0.0 + v;
+  const int kend = min(k0 + kCellK, D.nz + 2);  // exclusive
+  for (int k = k0; k < kend; ++k) {
+    const double rk = D.rz[k - 1];
+    const double H = 0.5;
+    const double v = ((rk * FA(D.u, i, j, k) - rk * FA(D.u, i - 1, j, k)) * MT(D.rdxc, i) +
+                      (rk * FA(D.v, i, j, k) - rk * FA(D.v, i, j - 1, k)) * MT(D.rdyc, j) +
+                      (H * (D.rz[k] + rk) * FA(D.w, i, j, k) - H * (rk + D.rz[k - 2]) * FA(D.w, i, j, k - 1)) *
+                          MT(D.rdzc, k)) *
+                     rdt;
+    FA(D.psrc, i, j, k) = 0.0 + v;
+  }
 }
 
 // ------------------------------------------------------ Pgrad + ghosts
@@ -895,21 +904,24 @@ template <bool kU>
 __global__ void __launch_bounds__(128) k_pgrad(NSDev D, double dt, double* __restrict__ hist) {
   const int i = 2 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 2 + blockIdx.y;
-  const int k = 2 + blockIdx.z;
+  const int k0 = 2 + blockIdx.z * kCellK;
   if (i > D.nx + 1) return;
+  const int kend = min(k0 + kCellK, D.nz + 2);  // exclusive
   const int kend_w = D.nz + 1 - D.ew;
   const double* __restrict__ p = D.p;
-  const double rk = kU ? 1.0 : D.rz[k - 1];
-  const double pk = FA(p, i, j, k);
-  if (hist) FA(hist, i, j, k) = pk;
-  const double pr = kU ? pk : pk / rk;
-  const double pe = kU ? FA(p, i + 1, j, k) : FA(p, i + 1, j, k) / rk;
-  const double pn = kU ? FA(p, i, j + 1, k) : FA(p, i, j + 1, k) / rk;
-  FA(D.u, i, j, k) = FA(D.u, i, j, k) - (pe - pr) * MT(D.rdxe, i) * dt;
-  FA(D.v, i, j, k) = FA(D.v, i, j, k) - (pn - pr) * MT(D.rdye, j) * dt;
-  if (k <= kend_w) {
-    const double pt = kU ? FA(p, i, j, k + 1) : FA(p, i, j, k + 1) / D.rz[k];
-    FA(D.w, i, j, k) = FA(D.w, i, j, k) - (pt - pr) * MT(D.rdze, k) * dt;
+  for (int k = k0; k < kend; ++k) {
+    const double rk = kU ? 1.0 : D.rz[k - 1];
+    const double pk = FA(p, i, j, k);
+    if (hist) FA(hist, i, j, k) = pk;
+    const double pr = kU ? pk : pk / rk;
+    const double pe = kU ? FA(p, i + 1, j, k) : FA(p, i + 1, j, k) / rk;
+    const double pn = kU ? FA(p, i, j + 1, k) : FA(p, i, j + 1, k) / rk;
+    FA(D.u, i, j, k) = FA(D.u, i, j, k) - (pe - pr) * MT(D.rdxe, i) * dt;
+    FA(D.v, i, j, k) = FA(D.v, i, j, k) - (pn - pr) * MT(D.rdye, j) * dt;
+    if (k <= kend_w) {
+      const double pt = kU ? FA(p, i, j, k + 1) : FA(p, i, j, k + 1) / D.rz[k];
+      FA(D.w, i, j, k) = FA(D.w, i, j, k) - (pt - pr) * MT(D.rdze, k) * dt;
+    }
   }
 }
 
@@ -1042,6 +1054,10 @@ static void launch_images(const NSDev& D, double* a0, double* a1, double* a2, cu
 static dim3 cell_grid(const NSDev& D, int tx) {
   return dim3((unsigned)((D.nx + tx - 1) / tx), (unsigned)D.ny, (unsigned)D.nz);
 }
+// kernels whose thread does kCellK planes of one (i, j)
+static dim3 cell_grid_k(const NSDev& D, int tx) {
+  return dim3((unsigned)((D.nx + tx - 1) / tx), (unsigned)D.ny, (unsigned)((D.nz + kCellK - 1) / kCellK));
+}
 static dim3 col_grid(const NSDev& D, int tx) {
   return dim3((unsigned)((D.nx + tx - 1) / tx), (unsigned)D.ny, 1u);
 }
@@ -1138,7 +1154,7 @@ void launch_cn_les(const NSDev& D, int var, double* fld, const double* q, const 
 }
 
 void launch_sgs(const NSDev& D, const ZRule& cfluc, cudaStream_t s) {
-  k_sgs<<<cell_grid(D, 128), 128, 0, s>>>(D);
+  k_sgs<<<cell_grid_k(D, 128), 128, 0, s>>>(D);
   for (double* a : {D.nuT, D.kT, D.nT}) k_ghost_field<<<col_grid(D, 64), 64, 0, s>>>(D, a, cfluc);
   count_launch(4);
   launch_images(D, D.nuT, D.kT, D.nT, s);
@@ -1342,7 +1358,7 @@ void launch_clip(const NSDev& D, double* a, double vmin, double vmax, cudaStream
 
 void launch_psource(const NSDev& D, double dt, cudaStream_t s) {
   const int tx = 128;
-  k_psource<<<cell_grid(D, tx), tx, 0, s>>>(D, 1.0 / dt);
+  k_psource<<<cell_grid_k(D, tx), tx, 0, s>>>(D, 1.0 / dt);
   count_launch();
 }
 
@@ -1354,9 +1370,9 @@ void launch_extrap(const NSDev& D, double* p, const double* h1, const double* h2
 void launch_pgrad(const NSDev& D, double dt, const ZRule& Ru, const ZRule& Rv, const ZRule& Rw,
                   cudaStream_t s, double* hist) {
   if (D.unit_r)
-    k_pgrad<true><<<cell_grid(D, 128), 128, 0, s>>>(D, dt, hist);
+    k_pgrad<true><<<cell_grid_k(D, 128), 128, 0, s>>>(D, dt, hist);
   else
-    k_pgrad<false><<<cell_grid(D, 128), 128, 0, s>>>(D, dt, hist);
+    k_pgrad<false><<<cell_grid_k(D, 128), 128, 0, s>>>(D, dt, hist);
   k_pgrad_ghost<<<col_grid(D, 64), 64, 0, s>>>(D, Ru, Rv, Rw);
   count_launch(2);
   launch_images(D, D.u, D.v, D.w, s);
